@@ -1,0 +1,488 @@
+// CPU oracle C interface — TEST INFRASTRUCTURE ONLY.
+// Loaded by tests/ (ctypes) and by bench.py's CPU baseline leg; the shipped
+// library never links it. All values cross the boundary as double; the world
+// computes in float (precision 0, the reference's default f32 build) or in
+// double (precision 1, the reference's `--features f64` build).
+#include <cstring>
+#include <memory>
+#include "oracle_world.hpp"
+
+using namespace oracle;
+
+namespace {
+
+struct Handle {
+    int f64 = 0;
+    std::unique_ptr<World<float>> wf;
+    std::unique_ptr<World<double>> wd;
+};
+
+template <class R>
+Shape<R> make_shape(uint32_t type, const double* p, const double* pts, uint32_t npts) {
+    switch (type) {
+        case SHAPE_SPHERE: return Shape<R>::sphere(static_cast<R>(p[0]));
+        case SHAPE_BOX: return Shape<R>::box(V3<R>(static_cast<R>(p[0]), static_cast<R>(p[1]), static_cast<R>(p[2])));
+        case SHAPE_CAPSULE: return Shape<R>::capsule(static_cast<R>(p[0]), static_cast<R>(p[1]));
+        case SHAPE_PLANE: return Shape<R>::plane(V3<R>(static_cast<R>(p[0]), static_cast<R>(p[1]), static_cast<R>(p[2])), static_cast<R>(p[3]));
+        default: {
+            std::vector<V3<R>> v;
+            for (uint32_t i = 0; i < npts; ++i) v.push_back(V3<R>(static_cast<R>(pts[3 * i]), static_cast<R>(pts[3 * i + 1]), static_cast<R>(pts[3 * i + 2])));
+            return Shape<R>::hull(v);
+        }
+    }
+}
+
+// Body descriptor layout (doubles), shared with tests/oracle_api.py:
+//  0 shape, 1-3 pos, 4-7 quat xyzw, 8-10 linvel, 11-13 angvel, 14 mass (0 = static),
+//  15 friction, 16 restitution, 17 flags, 18 group, 19 mask, 20 lin damping,
+//  21 ang damping, 22 activation override (0 = default), 23 kinematic (0/1)
+constexpr int DESC = 24;
+
+template <class R>
+uint32_t add_body(World<R>& w, const double* d) {
+    uint32_t shape = uint32_t(d[0]);
+    V3<R> pos(static_cast<R>(d[1]), static_cast<R>(d[2]), static_cast<R>(d[3]));
+    Body<R> b = d[14] > 0 ? w.make_dynamic(shape, pos, static_cast<R>(d[14])) : w.make_static(shape, pos);
+    b.orientation = Quat<R>(static_cast<R>(d[4]), static_cast<R>(d[5]), static_cast<R>(d[6]), static_cast<R>(d[7]));
+    b.linear_velocity = V3<R>(static_cast<R>(d[8]), static_cast<R>(d[9]), static_cast<R>(d[10]));
+    b.angular_velocity = V3<R>(static_cast<R>(d[11]), static_cast<R>(d[12]), static_cast<R>(d[13]));
+    b.friction = static_cast<R>(d[15]);
+    b.restitution = static_cast<R>(d[16]);
+    b.flags = uint32_t(d[17]);
+    b.group = uint16_t(d[18]);
+    b.mask = uint16_t(d[19]);
+    b.linear_damping = static_cast<R>(d[20]);
+    b.angular_damping = static_cast<R>(d[21]);
+    if (d[23] != 0) {  // body.rs:440-449 new_kinematic: a static body turned kinematic
+        b = w.make_static(shape, pos);
+        b.orientation = Quat<R>(static_cast<R>(d[4]), static_cast<R>(d[5]), static_cast<R>(d[6]), static_cast<R>(d[7]));
+        b.linear_velocity = V3<R>(static_cast<R>(d[8]), static_cast<R>(d[9]), static_cast<R>(d[10]));
+        b.angular_velocity = V3<R>(static_cast<R>(d[11]), static_cast<R>(d[12]), static_cast<R>(d[13]));
+        b.friction = static_cast<R>(d[15]);
+        b.restitution = static_cast<R>(d[16]);
+        b.is_static = false;
+        b.flags = uint32_t(d[17]) | CF_KINEMATIC;
+        b.activation = ACT_DISABLE_DEACTIVATION;
+    }
+    if (d[22] != 0) b.activation = uint32_t(d[22]);
+    return w.add_body(b);
+}
+
+// Body state layout (doubles): pos3, quat4, linvel3, angvel3, activation, deactivation_time = 15
+constexpr int STATE = 15;
+
+template <class R>
+void get_state(const World<R>& w, double* out) {
+    for (size_t i = 0; i < w.bodies.size(); ++i) {
+        const Body<R>& b = w.bodies[i];
+        double* o = out + i * STATE;
+        o[0] = b.position.x; o[1] = b.position.y; o[2] = b.position.z;
+        o[3] = b.orientation.x; o[4] = b.orientation.y; o[5] = b.orientation.z; o[6] = b.orientation.w;
+        o[7] = b.linear_velocity.x; o[8] = b.linear_velocity.y; o[9] = b.linear_velocity.z;
+        o[10] = b.angular_velocity.x; o[11] = b.angular_velocity.y; o[12] = b.angular_velocity.z;
+        o[13] = b.activation; o[14] = b.deactivation_time;
+    }
+}
+
+template <class R>
+void set_state(World<R>& w, const double* in) {
+    for (size_t i = 0; i < w.bodies.size(); ++i) {
+        Body<R>& b = w.bodies[i];
+        const double* o = in + i * STATE;
+        b.position = V3<R>(static_cast<R>(o[0]), static_cast<R>(o[1]), static_cast<R>(o[2]));
+        b.orientation = Quat<R>(static_cast<R>(o[3]), static_cast<R>(o[4]), static_cast<R>(o[5]), static_cast<R>(o[6]));
+        b.linear_velocity = V3<R>(static_cast<R>(o[7]), static_cast<R>(o[8]), static_cast<R>(o[9]));
+        b.angular_velocity = V3<R>(static_cast<R>(o[10]), static_cast<R>(o[11]), static_cast<R>(o[12]));
+        b.activation = uint32_t(o[13]);
+        b.deactivation_time = static_cast<R>(o[14]);
+    }
+}
+
+// Row layout (doubles): body_a, body_b, point_index, normal3, r_a3, r_b3,
+// penetration, normal_impulse, tangent1_impulse, tangent2_impulse, push_impulse,
+// split_active, friction, restitution, normal_mass, tangent1_mass, tangent2_mass,
+// baumgarte_span, normal_cfm, erp = 26
+constexpr int ROW = 26;
+
+template <class R>
+void get_rows(const std::vector<ContactConstraint<R>>& rows, double* out) {
+    for (size_t i = 0; i < rows.size(); ++i) {
+        const ContactConstraint<R>& c = rows[i];
+        double* o = out + i * ROW;
+        o[0] = c.body_a; o[1] = c.body_b; o[2] = c.point_index;
+        o[3] = c.normal.x; o[4] = c.normal.y; o[5] = c.normal.z;
+        o[6] = c.r_a.x; o[7] = c.r_a.y; o[8] = c.r_a.z;
+        o[9] = c.r_b.x; o[10] = c.r_b.y; o[11] = c.r_b.z;
+        o[12] = c.penetration; o[13] = c.normal_impulse; o[14] = c.tangent1_impulse; o[15] = c.tangent2_impulse;
+        o[16] = c.push_impulse; o[17] = c.split_active ? 1 : 0; o[18] = c.friction; o[19] = c.restitution;
+        o[20] = c.normal_mass; o[21] = c.tangent1_mass; o[22] = c.tangent2_mass;
+        o[23] = c.baumgarte_span; o[24] = c.normal_cfm; o[25] = c.erp;
+    }
+}
+
+template <class R>
+Quat<R> q_of(const double* p) { return Quat<R>(static_cast<R>(p[3]), static_cast<R>(p[4]), static_cast<R>(p[5]), static_cast<R>(p[6])); }
+template <class R>
+V3<R> v_of(const double* p) { return V3<R>(static_cast<R>(p[0]), static_cast<R>(p[1]), static_cast<R>(p[2])); }
+
+template <class R>
+int collide_impl(World<R>& w, uint32_t sa, const double* pose_a, uint32_t sb, const double* pose_b, const double* seed,
+                 double* out) {
+    Manifold<R> m;
+    V3<R> s;
+    bool has_seed = seed != nullptr;
+    if (has_seed) s = V3<R>(static_cast<R>(seed[0]), static_cast<R>(seed[1]), static_cast<R>(seed[2]));
+    if (!collide(w.shapes[sa], v_of<R>(pose_a), q_of<R>(pose_a), w.shapes[sb], v_of<R>(pose_b), q_of<R>(pose_b), has_seed, s, m))
+        return 0;
+    int n = 0;
+    for (auto& cp : m.points) {
+        double* o = out + n * 7;
+        o[0] = cp.position.x; o[1] = cp.position.y; o[2] = cp.position.z;
+        o[3] = cp.normal.x; o[4] = cp.normal.y; o[5] = cp.normal.z;
+        o[6] = cp.penetration;
+        if (++n == 8) break;
+    }
+    return n;
+}
+
+template <class R>
+int convex_impl(World<R>& w, uint32_t sa, const double* pose_a, uint32_t sb, const double* pose_b, double* out) {
+    Manifold<R> m;
+    R thr = pair_threshold(w.shapes[sa], w.shapes[sb]);
+    if (!convex_convex(w.shapes[sa], v_of<R>(pose_a), q_of<R>(pose_a), w.shapes[sb], v_of<R>(pose_b), q_of<R>(pose_b),
+                       false, V3<R>(), thr, m))
+        return 0;
+    const ContactPoint<R>& cp = m.points[0];
+    out[0] = cp.position.x; out[1] = cp.position.y; out[2] = cp.position.z;
+    out[3] = cp.normal.x; out[4] = cp.normal.y; out[5] = cp.normal.z;
+    out[6] = cp.penetration;
+    return 1;
+}
+
+template <class R>
+int gjk_kind_impl(World<R>& w, uint32_t sa, const double* pa, uint32_t sb, const double* pb) {
+    R thr = pair_threshold(w.shapes[sa], w.shapes[sb]);
+    GjkOutcome<R> g = gjk_contact(w.shapes[sa], v_of<R>(pa), q_of<R>(pa), w.shapes[sb], v_of<R>(pb), q_of<R>(pb), false,
+                                  V3<R>(), thr);
+    return g.kind;
+}
+
+template <class R>
+void pairs_impl(const double* aabbs, uint32_t n, int method, std::vector<std::pair<uint32_t, uint32_t>>& out) {
+    std::vector<Aabb<R>> a(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const double* p = aabbs + 6 * i;
+        a[i] = Aabb<R>(V3<R>(static_cast<R>(p[0]), static_cast<R>(p[1]), static_cast<R>(p[2])), V3<R>(static_cast<R>(p[3]), static_cast<R>(p[4]), static_cast<R>(p[5])));
+    }
+    if (method == 0) brute_force_pairs(a, out);
+    else sweep_pairs(a, out);
+}
+
+// Contacts layout for a standalone solve (doubles): body_a, body_b, pos3, normal3,
+// penetration, normal_impulse = 10
+template <class R>
+void solve_impl(World<R>& w, const double* contacts, uint32_t n, double inv_dt, double* out_rows) {
+    std::vector<ContactConstraint<R>> rows;
+    for (uint32_t i = 0; i < n; ++i) {
+        const double* c = contacts + 10 * i;
+        uint32_t ia = uint32_t(c[0]), ib = uint32_t(c[1]);
+        ContactPoint<R> cp(V3<R>(static_cast<R>(c[2]), static_cast<R>(c[3]), static_cast<R>(c[4])), V3<R>(static_cast<R>(c[5]), static_cast<R>(c[6]), static_cast<R>(c[7])), static_cast<R>(c[8]));
+        cp.normal_impulse = static_cast<R>(c[9]);
+        rows.push_back(prepare_contact(ia, ib, cp, w.bodies[ia], w.bodies[ib], i, static_cast<R>(inv_dt), w.info));
+    }
+    solve(w.bodies, rows, static_cast<R>(inv_dt), w.info);
+    if (out_rows) get_rows(rows, out_rows);
+}
+
+template <class R>
+void push_impl(const World<R>& w, double* out) {
+    for (size_t i = 0; i < w.bodies.size(); ++i) {
+        const Body<R>& b = w.bodies[i];
+        out[6 * i + 0] = b.push_linear.x; out[6 * i + 1] = b.push_linear.y; out[6 * i + 2] = b.push_linear.z;
+        out[6 * i + 3] = b.push_angular.x; out[6 * i + 4] = b.push_angular.y; out[6 * i + 5] = b.push_angular.z;
+    }
+}
+
+#define DISPATCH(h, expr)                  \
+    do {                                   \
+        if ((h)->f64) { auto& w = *(h)->wd; expr; } \
+        else { auto& w = *(h)->wf; expr; } \
+    } while (0)
+
+}  // namespace
+
+extern "C" {
+
+void* orc_world_new(int f64) {
+    Handle* h = new Handle();
+    h->f64 = f64;
+    if (f64) h->wd.reset(new World<double>());
+    else h->wf.reset(new World<float>());
+    return h;
+}
+
+void orc_world_free(void* p) { delete static_cast<Handle*>(p); }
+
+void orc_world_set_gravity(void* p, double gx, double gy, double gz) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, { using R = std::remove_reference_t<decltype(w.gravity.x)>; w.gravity = V3<R>(static_cast<R>(gx), static_cast<R>(gy), static_cast<R>(gz)); });
+}
+
+// params: erp2, linear_slop, restitution_threshold, split_impulse, split_threshold,
+// split_turn_erp, warmstarting_factor, global_cfm, sor, num_iterations
+void orc_world_set_solver(void* p, const double* s) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, {
+        using R = std::remove_reference_t<decltype(w.gravity.x)>;
+        w.info.erp2 = static_cast<R>(s[0]); w.info.linear_slop = static_cast<R>(s[1]); w.info.restitution_velocity_threshold = static_cast<R>(s[2]);
+        w.info.split_impulse = s[3] != 0; w.info.split_impulse_penetration_threshold = static_cast<R>(s[4]);
+        w.info.split_impulse_turn_erp = static_cast<R>(s[5]); w.info.warmstarting_factor = static_cast<R>(s[6]); w.info.global_cfm = static_cast<R>(s[7]);
+        w.info.sor = static_cast<R>(s[8]); w.info.num_iterations = uint32_t(s[9]);
+    });
+}
+
+void orc_world_set_brute_force(void* p, int on) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, { w.brute_force_broadphase = on != 0; });
+}
+
+uint32_t orc_world_add_shape(void* p, uint32_t type, const double* params, const double* pts, uint32_t npts) {
+    Handle* h = static_cast<Handle*>(p);
+    uint32_t r = 0;
+    DISPATCH(h, {
+        using R = std::remove_reference_t<decltype(w.gravity.x)>;
+        w.shapes.push_back(make_shape<R>(type, params, pts, npts));
+        r = uint32_t(w.shapes.size() - 1);
+    });
+    return r;
+}
+
+double orc_shape_threshold(void* p, uint32_t s) {
+    Handle* h = static_cast<Handle*>(p);
+    double r = 0;
+    DISPATCH(h, { r = double(w.shapes[s].contact_breaking_threshold()); });
+    return r;
+}
+
+void orc_shape_world_aabb(void* p, uint32_t s, const double* pose, double* out6) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, {
+        using R = std::remove_reference_t<decltype(w.gravity.x)>;
+        Aabb<R> a = w.shapes[s].world_aabb(v_of<R>(pose), q_of<R>(pose));
+        out6[0] = a.min.x; out6[1] = a.min.y; out6[2] = a.min.z; out6[3] = a.max.x; out6[4] = a.max.y; out6[5] = a.max.z;
+    });
+}
+
+void orc_shape_inertia(void* p, uint32_t s, double mass, double* out3) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, {
+        using R = std::remove_reference_t<decltype(w.gravity.x)>;
+        V3<R> in = w.shapes[s].local_inertia(static_cast<R>(mass));
+        out3[0] = in.x; out3[1] = in.y; out3[2] = in.z;
+    });
+}
+
+uint32_t orc_world_add_body(void* p, const double* desc) {
+    Handle* h = static_cast<Handle*>(p);
+    uint32_t r = 0;
+    DISPATCH(h, { r = add_body(w, desc); });
+    return r;
+}
+
+uint32_t orc_world_num_bodies(void* p) {
+    Handle* h = static_cast<Handle*>(p);
+    uint32_t r = 0;
+    DISPATCH(h, { r = uint32_t(w.bodies.size()); });
+    return r;
+}
+
+void orc_world_step(void* p, double dt) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, {
+        using R = std::remove_reference_t<decltype(w.gravity.x)>;
+        w.step(static_cast<R>(dt));
+    });
+}
+
+void orc_world_get_state(void* p, double* out) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, { get_state(w, out); });
+}
+
+void orc_world_set_state(void* p, const double* in) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, { set_state(w, in); });
+}
+
+void orc_world_get_push(void* p, double* out) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, { push_impl(w, out); });
+}
+
+uint32_t orc_world_num_pairs(void* p) {
+    Handle* h = static_cast<Handle*>(p);
+    uint32_t r = 0;
+    DISPATCH(h, { r = uint32_t(w.last_pairs.size()); });
+    return r;
+}
+
+void orc_world_get_pairs(void* p, uint32_t* out) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, {
+        for (size_t i = 0; i < w.last_pairs.size(); ++i) { out[2 * i] = w.last_pairs[i].first; out[2 * i + 1] = w.last_pairs[i].second; }
+    });
+}
+
+uint32_t orc_world_num_rows(void* p) {
+    Handle* h = static_cast<Handle*>(p);
+    uint32_t r = 0;
+    DISPATCH(h, { r = uint32_t(w.last_rows.size()); });
+    return r;
+}
+
+// which: 0 = after the solve, 1 = as prepared (before the solve)
+void orc_world_get_rows(void* p, int which, double* out) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, { get_rows(which ? w.last_rows_pre : w.last_rows, out); });
+}
+
+uint32_t orc_world_narrowphase_calls(void* p) {
+    Handle* h = static_cast<Handle*>(p);
+    uint32_t r = 0;
+    DISPATCH(h, { r = w.last_narrowphase_calls; });
+    return r;
+}
+
+uint32_t orc_world_num_manifolds(void* p) {
+    Handle* h = static_cast<Handle*>(p);
+    uint32_t r = 0;
+    DISPATCH(h, { r = uint32_t(w.cache.size()); });
+    return r;
+}
+
+void orc_world_set_solve_order(void* p, const uint64_t* keys, uint32_t n) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, { w.solve_order.assign(keys, keys + n); });
+}
+
+int orc_collide(void* p, uint32_t sa, const double* pose_a, uint32_t sb, const double* pose_b, const double* seed,
+                double* out) {
+    Handle* h = static_cast<Handle*>(p);
+    int r = 0;
+    DISPATCH(h, { r = collide_impl(w, sa, pose_a, sb, pose_b, seed, out); });
+    return r;
+}
+
+// The generic GJK/EPA path (convex_convex.rs:30) regardless of the shape pair.
+int orc_convex_convex(void* p, uint32_t sa, const double* pose_a, uint32_t sb, const double* pose_b, double* out) {
+    Handle* h = static_cast<Handle*>(p);
+    int r = 0;
+    DISPATCH(h, { r = convex_impl(w, sa, pose_a, sb, pose_b, out); });
+    return r;
+}
+
+int orc_gjk_kind(void* p, uint32_t sa, const double* pose_a, uint32_t sb, const double* pose_b) {
+    Handle* h = static_cast<Handle*>(p);
+    int r = 0;
+    DISPATCH(h, { r = gjk_kind_impl(w, sa, pose_a, sb, pose_b); });
+    return r;
+}
+
+void orc_solve_contacts(void* p, const double* contacts, uint32_t n, double inv_dt, double* out_rows) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, { solve_impl(w, contacts, n, inv_dt, out_rows); });
+}
+
+// Pairs of an AABB set (n x [min3, max3]); method 0 = brute force, 1 = sweep.
+// Returns the pair count; writes up to cap pairs.
+uint64_t orc_pairs(int f64, const double* aabbs, uint32_t n, int method, uint32_t* out, uint64_t cap) {
+    std::vector<std::pair<uint32_t, uint32_t>> pr;
+    if (f64) pairs_impl<double>(aabbs, n, method, pr);
+    else pairs_impl<float>(aabbs, n, method, pr);
+    for (size_t i = 0; i < pr.size() && i < cap; ++i) { out[2 * i] = pr[i].first; out[2 * i + 1] = pr[i].second; }
+    return pr.size();
+}
+
+// Persistent manifold handle (float or double).
+struct PmHandle { int f64; PersistentManifold<float> f; PersistentManifold<double> d; };
+
+void* orc_pm_new(int f64) { PmHandle* h = new PmHandle(); h->f64 = f64; return h; }
+void orc_pm_free(void* p) { delete static_cast<PmHandle*>(p); }
+
+// points: n x (pos3, normal3, penetration)
+void orc_pm_capture(void* p, const double* pts, uint32_t n, const double* pose_a, const double* pose_b, double thr) {
+    PmHandle* h = static_cast<PmHandle*>(p);
+    auto run = [&](auto& pm, auto zero) {
+        using R = decltype(zero);
+        Manifold<R> m;
+        for (uint32_t i = 0; i < n; ++i) {
+            const double* c = pts + 7 * i;
+            m.points.push_back(ContactPoint<R>(V3<R>(static_cast<R>(c[0]), static_cast<R>(c[1]), static_cast<R>(c[2])), V3<R>(static_cast<R>(c[3]), static_cast<R>(c[4]), static_cast<R>(c[5])), static_cast<R>(c[6])));
+        }
+        pm.capture(m, v_of<R>(pose_a), q_of<R>(pose_a), v_of<R>(pose_b), q_of<R>(pose_b), static_cast<R>(thr));
+    };
+    if (h->f64) run(h->d, 0.0); else run(h->f, 0.0f);
+}
+
+// out: n x (pos3, normal3, penetration, normal_impulse, lifetime); returns n
+uint32_t orc_pm_refresh(void* p, const double* pose_a, const double* pose_b, double* out) {
+    PmHandle* h = static_cast<PmHandle*>(p);
+    uint32_t n = 0;
+    auto run = [&](auto& pm, auto zero) {
+        using R = decltype(zero);
+        std::vector<ContactPoint<R>> o;
+        pm.refresh(v_of<R>(pose_a), q_of<R>(pose_a), v_of<R>(pose_b), q_of<R>(pose_b), o);
+        for (auto& cp : o) {
+            double* d = out + 9 * n;
+            d[0] = cp.position.x; d[1] = cp.position.y; d[2] = cp.position.z;
+            d[3] = cp.normal.x; d[4] = cp.normal.y; d[5] = cp.normal.z;
+            d[6] = cp.penetration; d[7] = cp.normal_impulse; d[8] = cp.lifetime;
+            ++n;
+        }
+    };
+    if (h->f64) run(h->d, 0.0); else run(h->f, 0.0f);
+    return n;
+}
+
+int orc_pm_needs_redetect(void* p, const double* pose_a, const double* pose_b) {
+    PmHandle* h = static_cast<PmHandle*>(p);
+    if (h->f64) return h->d.needs_redetect(v_of<double>(pose_a), q_of<double>(pose_a), v_of<double>(pose_b), q_of<double>(pose_b));
+    return h->f.needs_redetect(v_of<float>(pose_a), q_of<float>(pose_a), v_of<float>(pose_b), q_of<float>(pose_b));
+}
+
+void orc_pm_set_impulse(void* p, uint32_t k, double imp) {
+    PmHandle* h = static_cast<PmHandle*>(p);
+    if (h->f64) h->d.points[k].normal_impulse = imp; else h->f.points[k].normal_impulse = float(imp);
+}
+
+// out: n x (local_a3, local_b3, normal3, penetration, impulse, lifetime)
+uint32_t orc_pm_points(void* p, double* out) {
+    PmHandle* h = static_cast<PmHandle*>(p);
+    uint32_t n = 0;
+    auto run = [&](auto& pm) {
+        for (auto& q : pm.points) {
+            double* d = out + 12 * n;
+            d[0] = q.local_a.x; d[1] = q.local_a.y; d[2] = q.local_a.z;
+            d[3] = q.local_b.x; d[4] = q.local_b.y; d[5] = q.local_b.z;
+            d[6] = q.normal.x; d[7] = q.normal.y; d[8] = q.normal.z;
+            d[9] = q.penetration; d[10] = q.normal_impulse; d[11] = q.lifetime;
+            ++n;
+        }
+    };
+    if (h->f64) run(h->d); else run(h->f);
+    return n;
+}
+
+// Pose integration (body.rs:92-137): in = pos3, quat4, linvel3, angvel3; out = pos3, quat4
+void orc_interpolate_pose(int f64, const double* in, double dt, double* out) {
+    auto run = [&](auto zero) {
+        using R = decltype(zero);
+        V3<R> np; Quat<R> nq;
+        interpolate_pose(V3<R>(static_cast<R>(in[0]), static_cast<R>(in[1]), static_cast<R>(in[2])), Quat<R>(static_cast<R>(in[3]), static_cast<R>(in[4]), static_cast<R>(in[5]), static_cast<R>(in[6])),
+                         V3<R>(static_cast<R>(in[7]), static_cast<R>(in[8]), static_cast<R>(in[9])), V3<R>(static_cast<R>(in[10]), static_cast<R>(in[11]), static_cast<R>(in[12])), static_cast<R>(dt), np, nq);
+        out[0] = np.x; out[1] = np.y; out[2] = np.z; out[3] = nq.x; out[4] = nq.y; out[5] = nq.z; out[6] = nq.w;
+    };
+    if (f64) run(0.0); else run(0.0f);
+}
+
+}  // extern "C"

@@ -1,0 +1,300 @@
+"""ctypes wrapper of the CPU oracle (oracle/liboracle.so) — test infrastructure.
+
+Only tests, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module; the product library never does.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(ROOT, "oracle", "liboracle.so")
+
+SPHERE, BOX, CAPSULE, HULL, PLANE = 0, 1, 2, 3, 4
+ACTIVE, ISLAND_SLEEPING, WANTS_DEACTIVATION, DISABLE_DEACTIVATION, DISABLE_SIMULATION = 1, 2, 3, 4, 5
+NO_CONTACT_RESPONSE, DISABLE_WORLD_GRAVITY, KINEMATIC = 0x1, 0x2, 0x4
+
+DESC = 24   # body descriptor doubles (oracle_capi.cpp)
+STATE = 15  # body state doubles
+ROW = 26    # contact row doubles
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("oracle/liboracle.so is not built (run __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        D = ctypes.POINTER(ctypes.c_double)
+        U32 = ctypes.c_uint32
+        sig = {
+            "orc_world_new": (P, [ctypes.c_int]),
+            "orc_world_free": (None, [P]),
+            "orc_world_set_gravity": (None, [P, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
+            "orc_world_set_solver": (None, [P, D]),
+            "orc_world_set_brute_force": (None, [P, ctypes.c_int]),
+            "orc_world_add_shape": (U32, [P, U32, D, D, U32]),
+            "orc_shape_threshold": (ctypes.c_double, [P, U32]),
+            "orc_shape_world_aabb": (None, [P, U32, D, D]),
+            "orc_shape_inertia": (None, [P, U32, ctypes.c_double, D]),
+            "orc_world_add_body": (U32, [P, D]),
+            "orc_world_num_bodies": (U32, [P]),
+            "orc_world_step": (None, [P, ctypes.c_double]),
+            "orc_world_get_state": (None, [P, D]),
+            "orc_world_set_state": (None, [P, D]),
+            "orc_world_get_push": (None, [P, D]),
+            "orc_world_num_pairs": (U32, [P]),
+            "orc_world_get_pairs": (None, [P, ctypes.POINTER(U32)]),
+            "orc_world_num_rows": (U32, [P]),
+            "orc_world_get_rows": (None, [P, ctypes.c_int, D]),
+            "orc_world_narrowphase_calls": (U32, [P]),
+            "orc_world_num_manifolds": (U32, [P]),
+            "orc_world_set_solve_order": (None, [P, ctypes.POINTER(ctypes.c_uint64), U32]),
+            "orc_collide": (ctypes.c_int, [P, U32, D, U32, D, D, D]),
+            "orc_gjk_kind": (ctypes.c_int, [P, U32, D, U32, D]),
+            "orc_convex_convex": (ctypes.c_int, [P, U32, D, U32, D, D]),
+            "orc_solve_contacts": (None, [P, D, U32, ctypes.c_double, D]),
+            "orc_pairs": (ctypes.c_uint64, [ctypes.c_int, D, U32, ctypes.c_int, ctypes.POINTER(U32), ctypes.c_uint64]),
+            "orc_pm_new": (P, [ctypes.c_int]),
+            "orc_pm_free": (None, [P]),
+            "orc_pm_capture": (None, [P, D, U32, D, D, ctypes.c_double]),
+            "orc_pm_refresh": (U32, [P, D, D, D]),
+            "orc_pm_needs_redetect": (ctypes.c_int, [P, D, D]),
+            "orc_pm_set_impulse": (None, [P, U32, ctypes.c_double]),
+            "orc_pm_points": (U32, [P, D]),
+            "orc_interpolate_pose": (None, [ctypes.c_int, D, ctypes.c_double, D]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def pose(p=(0, 0, 0), q=(0, 0, 0, 1)):
+    return f64(list(p) + list(q))
+
+
+def body_desc(shape, pos, quat=(0, 0, 0, 1), linvel=(0, 0, 0), angvel=(0, 0, 0), mass=1.0, friction=0.5,
+              restitution=0.0, flags=0, group=1, mask=0xFFFF, lin_damping=0.0, ang_damping=0.0, activation=0,
+              kinematic=0):
+    d = np.zeros(DESC)
+    d[0] = shape
+    d[1:4] = pos
+    d[4:8] = quat
+    d[8:11] = linvel
+    d[11:14] = angvel
+    d[14] = mass
+    d[15] = friction
+    d[16] = restitution
+    d[17] = flags
+    d[18] = group
+    d[19] = mask
+    d[20] = lin_damping
+    d[21] = ang_damping
+    d[22] = activation
+    d[23] = kinematic
+    return d
+
+
+class OracleWorld:
+    """One oracle world (precision 'f32' or 'f64')."""
+
+    def __init__(self, precision="f32"):
+        self.L = lib()
+        self.h = self.L.orc_world_new(1 if precision == "f64" else 0)
+        self.precision = precision
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.L.orc_world_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def set_gravity(self, g):
+        self.L.orc_world_set_gravity(self.h, *map(float, g))
+
+    def set_solver(self, erp2=0.2, linear_slop=0.005, restitution_threshold=1.0, split_impulse=True,
+                   split_threshold=-0.04, split_turn_erp=0.1, warmstarting_factor=0.85, global_cfm=0.0, sor=1.0,
+                   num_iterations=10):
+        s = f64([erp2, linear_slop, restitution_threshold, 1.0 if split_impulse else 0.0, split_threshold,
+                 split_turn_erp, warmstarting_factor, global_cfm, sor, num_iterations])
+        self.L.orc_world_set_solver(self.h, dptr(s))
+
+    def set_brute_force(self, on=True):
+        self.L.orc_world_set_brute_force(self.h, 1 if on else 0)
+
+    def add_shape(self, kind, params=(), points=None):
+        p = f64(list(params) + [0.0] * (4 - len(params)))
+        if points is not None:
+            pts = f64(np.asarray(points).reshape(-1, 3))
+            return self.L.orc_world_add_shape(self.h, kind, dptr(p), dptr(pts), len(pts))
+        return self.L.orc_world_add_shape(self.h, kind, dptr(p), None, 0)
+
+    def sphere(self, r):
+        return self.add_shape(SPHERE, [r])
+
+    def box(self, h):
+        return self.add_shape(BOX, list(h))
+
+    def capsule(self, r, hh):
+        return self.add_shape(CAPSULE, [r, hh])
+
+    def plane(self, n, c):
+        return self.add_shape(PLANE, list(n) + [c])
+
+    def hull(self, pts):
+        return self.add_shape(HULL, [], pts)
+
+    def threshold(self, s):
+        return self.L.orc_shape_threshold(self.h, s)
+
+    def world_aabb(self, s, p):
+        out = np.zeros(6)
+        self.L.orc_shape_world_aabb(self.h, s, dptr(f64(p)), dptr(out))
+        return out
+
+    def inertia(self, s, mass):
+        out = np.zeros(3)
+        self.L.orc_shape_inertia(self.h, s, mass, dptr(out))
+        return out
+
+    def add_body(self, *args, **kw):
+        d = f64(body_desc(*args, **kw))
+        return self.L.orc_world_add_body(self.h, dptr(d))
+
+    def add_desc(self, d):
+        return self.L.orc_world_add_body(self.h, dptr(f64(d)))
+
+    @property
+    def num_bodies(self):
+        return self.L.orc_world_num_bodies(self.h)
+
+    def step(self, dt):
+        self.L.orc_world_step(self.h, dt)
+
+    def state(self):
+        out = np.zeros((self.num_bodies, STATE))
+        self.L.orc_world_get_state(self.h, dptr(out))
+        return out
+
+    def set_state(self, s):
+        s = f64(s)
+        self.L.orc_world_set_state(self.h, dptr(s))
+
+    def push(self):
+        out = np.zeros((self.num_bodies, 6))
+        self.L.orc_world_get_push(self.h, dptr(out))
+        return out
+
+    def pairs(self):
+        n = self.L.orc_world_num_pairs(self.h)
+        out = np.zeros((n, 2), dtype=np.uint32)
+        if n:
+            self.L.orc_world_get_pairs(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+        return out
+
+    def rows(self, pre=False):
+        n = self.L.orc_world_num_rows(self.h)
+        out = np.zeros((n, ROW))
+        if n:
+            self.L.orc_world_get_rows(self.h, 1 if pre else 0, dptr(out))
+        return out
+
+    def narrowphase_calls(self):
+        return self.L.orc_world_narrowphase_calls(self.h)
+
+    def num_manifolds(self):
+        return self.L.orc_world_num_manifolds(self.h)
+
+    def set_solve_order(self, keys):
+        k = np.ascontiguousarray(keys, dtype=np.uint64)
+        self.L.orc_world_set_solve_order(self.h, k.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), len(k))
+
+    def collide(self, sa, pa, sb, pb, seed=None):
+        out = np.zeros((8, 7))
+        sd = dptr(f64(seed)) if seed is not None else None
+        n = self.L.orc_collide(self.h, sa, dptr(f64(pa)), sb, dptr(f64(pb)), sd, dptr(out))
+        return out[:n]
+
+    def convex_convex(self, sa, pa, sb, pb):
+        out = np.zeros(7)
+        n = self.L.orc_convex_convex(self.h, sa, dptr(f64(pa)), sb, dptr(f64(pb)), dptr(out))
+        return out if n else None
+
+    def gjk_kind(self, sa, pa, sb, pb):
+        return self.L.orc_gjk_kind(self.h, sa, dptr(f64(pa)), sb, dptr(f64(pb)))
+
+    def solve_contacts(self, contacts, inv_dt):
+        c = f64(np.asarray(contacts).reshape(-1, 10))
+        out = np.zeros((len(c), ROW))
+        self.L.orc_solve_contacts(self.h, dptr(c), len(c), inv_dt, dptr(out))
+        return out
+
+
+def oracle_pairs(aabbs, method=0, precision="f32"):
+    """Pairs of an (n, 6) AABB array: method 0 brute force, 1 sweep."""
+    a = f64(np.asarray(aabbs).reshape(-1, 6))
+    L = lib()
+    n = L.orc_pairs(1 if precision == "f64" else 0, dptr(a), len(a), method, None, 0)
+    out = np.zeros((n, 2), dtype=np.uint32)
+    if n:
+        L.orc_pairs(1 if precision == "f64" else 0, dptr(a), len(a), method,
+                    out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), n)
+    return out
+
+
+class OracleManifold:
+    def __init__(self, precision="f32"):
+        self.L = lib()
+        self.h = self.L.orc_pm_new(1 if precision == "f64" else 0)
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.L.orc_pm_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def capture(self, points, pa, pb, thr):
+        p = f64(np.asarray(points).reshape(-1, 7))
+        self.L.orc_pm_capture(self.h, dptr(p), len(p), dptr(f64(pa)), dptr(f64(pb)), thr)
+
+    def refresh(self, pa, pb):
+        out = np.zeros((16, 9))
+        n = self.L.orc_pm_refresh(self.h, dptr(f64(pa)), dptr(f64(pb)), dptr(out))
+        return out[:n]
+
+    def needs_redetect(self, pa, pb):
+        return bool(self.L.orc_pm_needs_redetect(self.h, dptr(f64(pa)), dptr(f64(pb))))
+
+    def set_impulse(self, k, v):
+        self.L.orc_pm_set_impulse(self.h, k, v)
+
+    def points(self):
+        out = np.zeros((16, 12))
+        n = self.L.orc_pm_points(self.h, dptr(out))
+        return out[:n]
+
+
+def interpolate_pose(pos, quat, linvel, angvel, dt, precision="f32"):
+    inp = f64(list(pos) + list(quat) + list(linvel) + list(angvel))
+    out = np.zeros(7)
+    lib().orc_interpolate_pose(1 if precision == "f64" else 0, dptr(inp), dt, dptr(out))
+    return out
