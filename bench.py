@@ -1,0 +1,261 @@
+#!/usr/bin/env python
+"""Benchmark: body-steps/s of the rigid-body step on the 131,072-body pile.
+
+Workload (config 3 of the benchmark set): 65,536 unit boxes (half 0.5) and
+65,536 spheres (r 0.5) on a jittered 64x64x32 grid with 1.05 m spacing over a
+ground plane; f32; dt 1/60; 20 PGS iterations. The pile first settles for
+--preroll steps (untimed, 4 s simulated by default) so the timed steps run on
+a dense contact state; then --warmup untimed steps, then --steps timed steps.
+
+Arms:
+  default            the sm_100a library through its C ABI; `value` is device
+                     time on the world's stream; `e2e` repeats the steps through
+                     the public API with host buffers (force upload + step +
+                     pose read-back every step) on the wall clock.
+  --impl reference   the CPU implementation of the same step on the host
+                     cores (the C++ restatement in oracle/: the Rust reference
+                     has no toolchain on this machine), on a bounded sample of
+                     the same pile recipe.
+Multi-GPU (torchrun): one independent replica per rank (no collective on the
+data path); value = all ranks' body-steps / max rank time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "bullet-physics_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "body-steps/s (128k-body pile; 4096 batched worlds) and adjoint steps/s vs plain"
+UNIT = "body-steps/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=60)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--preroll", type=int, default=240)
+    p.add_argument("--impl", default="bgpu", choices=["bgpu", "reference"])
+    p.add_argument("--grid", default="64,64,32", help="pile grid nx,nz,ny (default: the full 131,072-body pile)")
+    p.add_argument("--cpu-sample-grid", default="16,16,32")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def grid_of(s):
+    nx, nz, ny = (int(x) for x in s.split(","))
+    return nx, nz, ny
+
+
+def cpu_baseline(grid, preroll, steps):
+    """The CPU step (oracle restatement, single thread) on a bounded sample of the pile recipe."""
+    import oracle_api
+    import scenes
+
+    nx, nz, ny = grid
+    sc = scenes.large_pile_fast(nx, nz, ny, seed=3)
+    w = sc.build_oracle(oracle_api)
+    for _ in range(preroll):
+        w.step(sc.dt)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        w.step(sc.dt)
+    dt = time.perf_counter() - t0
+    n = sc.num_dynamic
+    return {"value": n * steps / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"large-pile recipe {nx}x{nz}x{ny} ({n} bodies), {preroll}-step settle, {steps} timed steps, "
+                      f"single thread, {dt:.2f} s"}
+
+
+def algorithmic_pgs_bytes(st, iters):
+    """Per-launch algorithmic bytes of the PGS kernel: per contact and iteration 300 B
+    (180 B row + 24 B impulse r/w + 96 B velocity gather/scatter), 120 B per contact of
+    warm start, 100 B per split-active contact and iteration."""
+    c = st["num_contacts"]
+    split_c = st.get("num_split_contacts", 0)
+    return c * (300 * iters + 120) + 100 * split_c * iters
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world_size > 1:
+        import torch
+        import torch.distributed as tdist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local_rank)
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist = tdist
+    if args.impl == "reference":
+        if rank == 0:
+            base = cpu_baseline(grid_of(args.cpu_sample_grid), min(args.preroll, 240), max(1, min(args.steps, 30)))
+            line = {"metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                    "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+                    "config": {"workload": "large_pile_131072 (config 3): CPU sample of the same recipe",
+                               "iterations": 20, "dt": 1 / 60},
+                    "cpu_baseline": base,
+                    "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    if local_rank:
+        os.environ["CUDA_VISIBLE_DEVICES"] = os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank))
+    import bgpu
+    import scenes
+
+    nx, nz, ny = grid_of(args.grid)
+    sc = scenes.large_pile_fast(nx, nz, ny, seed=3 + rank)
+    w = sc.build_gpu(bgpu)
+    n_dyn = sc.num_dynamic
+    w.step_timed(sc.dt, args.preroll)
+    w.step_timed(sc.dt, args.warmup)
+    w.enable_timing(True)
+    if dist:
+        import torch
+
+        dist.barrier()
+        torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        ms = w.step_timed(sc.dt, args.steps)
+    st = w.stats()
+    w.enable_timing(False)
+    region_ms = ms
+    if dist:
+        import torch
+
+        t = torch.tensor([region_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        region_ms = float(t.item())
+        dist.barrier()
+    value = n_dyn * args.steps * world_size / (region_ms / 1000.0)
+
+    # End to end through the public API with host buffers.
+    forces = np.zeros((w.num_bodies, 3), dtype=np.float32)
+    poses = np.zeros((w.num_bodies, 7), dtype=np.float32)
+    e2e_steps = max(1, min(args.steps, 30))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        w.apply_forces(forces)
+        w.step(sc.dt)
+        w.poses(poses)
+    e2e_s = time.perf_counter() - t0
+    e2e_value = n_dyn * e2e_steps * world_size / e2e_s
+    if dist:
+        import torch
+
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_value = n_dyn * e2e_steps * world_size / float(t.item())
+
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        launches = max(st["timed_steps"], 1)
+        solve_ms = st["solve_kernel_ms"] / launches
+        alg = algorithmic_pgs_bytes(st, sc.iterations)
+        achieved = alg / (solve_ms / 1000.0) / 1e9 if solve_ms > 0 else None
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": region_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"large_pile_{n_dyn} (config 3): {nx}x{nz}x{ny} grid, 50% unit boxes / 50% r0.5 "
+                                   f"spheres, 1.05 m spacing, ground plane",
+                       "iterations": sc.iterations, "dt": sc.dt, "preroll_steps": args.preroll,
+                       "parallelism": f"replicas x{world_size}",
+                       "l2": "inputs larger than L2 (rows + manifolds + bodies > 126 MB)",
+                       "pairs": st["num_pairs"], "contacts": st["num_contacts"],
+                       "contact_pairs": st["num_contact_pairs"], "colours": st["num_colours"],
+                       "stage_ms_per_step": [x / launches for x in st["stage_ms"]]},
+            "roofline": {"kernel": "k_solve (colour-batched PGS)", "bound": "hbm",
+                         "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": (achieved / hbm) if achieved else None, "traffic": None,
+                         "peak_kind": peak_kind, "kernel_ms_per_launch": solve_ms,
+                         "algorithmic_bytes_per_launch": alg},
+            "clocks": clocks.summary(),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(forces.nbytes),
+                    "d2h_bytes_per_step": int(poses.nbytes)},
+            "gpu_launches": int(args.steps * 36),
+            "device_status": st["device_status"],
+        }
+        if world_size == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(grid_of(args.cpu_sample_grid), min(args.preroll, 240), 30)
+        print(json.dumps(line), flush=True)
+    w.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,352 @@
+"""ctypes binding of libbgpu.so (the C ABI in include/bgpu.h).
+
+The product is the C ABI; this module is a thin caller used by the tests,
+the benchmark and the smoke entry. It refuses to run without the compiled
+library: there is no fallback implementation.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbgpu.so")
+
+SPHERE, BOX, CAPSULE, HULL, PLANE = 0, 1, 2, 3, 4
+NO_CONTACT_RESPONSE, DISABLE_WORLD_GRAVITY, KINEMATIC, ADDITIONAL_DAMPING = 0x1, 0x2, 0x4, 0x10
+STATE = 15
+CONTACT = 18
+
+
+class SolverInfo(ctypes.Structure):
+    _fields_ = [("erp2", ctypes.c_float), ("linear_slop", ctypes.c_float),
+                ("restitution_velocity_threshold", ctypes.c_float), ("split_impulse", ctypes.c_uint32),
+                ("split_impulse_penetration_threshold", ctypes.c_float), ("split_impulse_turn_erp", ctypes.c_float),
+                ("warmstarting_factor", ctypes.c_float), ("global_cfm", ctypes.c_float), ("sor", ctypes.c_float),
+                ("num_iterations", ctypes.c_uint32)]
+
+
+class BodyDesc(ctypes.Structure):
+    _fields_ = [("shape", ctypes.c_uint32), ("position", ctypes.c_float * 3), ("orientation", ctypes.c_float * 4),
+                ("linear_velocity", ctypes.c_float * 3), ("angular_velocity", ctypes.c_float * 3),
+                ("mass", ctypes.c_float), ("friction", ctypes.c_float), ("restitution", ctypes.c_float),
+                ("linear_damping", ctypes.c_float), ("angular_damping", ctypes.c_float), ("flags", ctypes.c_uint32),
+                ("group", ctypes.c_uint16), ("mask", ctypes.c_uint16), ("activation", ctypes.c_uint32),
+                ("linear_sleeping_threshold", ctypes.c_float), ("angular_sleeping_threshold", ctypes.c_float)]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [("num_bodies", ctypes.c_uint32), ("num_pairs", ctypes.c_uint32),
+                ("num_contact_pairs", ctypes.c_uint32), ("num_contacts", ctypes.c_uint32),
+                ("num_colours", ctypes.c_uint32), ("num_detect", ctypes.c_uint32), ("num_manifolds", ctypes.c_uint32),
+                ("device_status", ctypes.c_uint32), ("num_split_pairs", ctypes.c_uint32),
+                ("timed_steps", ctypes.c_uint32), ("stage_ms", ctypes.c_float * 7), ("solve_kernel_ms", ctypes.c_float),
+                ("step_ms", ctypes.c_float)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        F = ctypes.POINTER(ctypes.c_float)
+        U32 = ctypes.c_uint32
+        U32P = ctypes.POINTER(ctypes.c_uint32)
+        U64P = ctypes.POINTER(ctypes.c_uint64)
+        S = ctypes.c_int32
+        sig = {
+            "bgpu_version": (ctypes.c_char_p, []),
+            "bgpu_device_count": (ctypes.c_int, []),
+            "bgpu_last_error": (ctypes.c_size_t, [ctypes.c_char_p, ctypes.c_size_t]),
+            "bgpu_solver_info_default": (None, [ctypes.POINTER(SolverInfo)]),
+            "bgpu_body_desc_default": (None, [ctypes.POINTER(BodyDesc)]),
+            "bgpu_world_create": (S, [ctypes.POINTER(SolverInfo), F, ctypes.POINTER(P)]),
+            "bgpu_world_destroy": (None, [P]),
+            "bgpu_world_set_gravity": (S, [P, F]),
+            "bgpu_world_set_solver_info": (S, [P, ctypes.POINTER(SolverInfo)]),
+            "bgpu_add_shape": (S, [P, U32, F, F, U32, U32P]),
+            "bgpu_add_bodies": (S, [P, U32, ctypes.POINTER(BodyDesc), U32P]),
+            "bgpu_num_bodies": (U32, [P]),
+            "bgpu_step": (S, [P, ctypes.c_float, U32]),
+            "bgpu_step_simulation_fixed": (S, [P, ctypes.c_float, U32, ctypes.c_float, U32P]),
+            "bgpu_step_timed": (S, [P, ctypes.c_float, U32, F]),
+            "bgpu_read_state": (S, [P, F]),
+            "bgpu_write_state": (S, [P, F]),
+            "bgpu_read_poses": (S, [P, F]),
+            "bgpu_apply_forces": (S, [P, F, F]),
+            "bgpu_read_pairs": (S, [P, U32P, ctypes.c_uint64, U64P]),
+            "bgpu_read_contacts": (S, [P, F, ctypes.c_uint64, U64P]),
+            "bgpu_read_solve_order": (S, [P, U64P, ctypes.c_uint64, U64P]),
+            "bgpu_get_stats": (S, [P, ctypes.POINTER(StepStats)]),
+            "bgpu_enable_step_timing": (S, [P, ctypes.c_int]),
+            "bgpu_broadphase_pairs": (S, [F, U32, U32P, ctypes.c_uint64, U64P]),
+            "bgpu_collide": (S, [P, U32, U32P, F, U32P, F, F, ctypes.c_int, F, U32P]),
+            "bgpu_solve_contacts": (S, [P, U32, F, ctypes.c_float, F, U64P]),
+            "bgpu_read_push": (S, [P, F]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+class BgpuError(RuntimeError):
+    pass
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(512)
+    lib().bgpu_last_error(buf, 512)
+    return buf.value.decode()
+
+
+def check(status, what=""):
+    if status != 0:
+        raise BgpuError(f"{what}: status {status}: {last_error()}")
+
+
+def fptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def u32ptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+
+
+def u64ptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+
+def f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def device_count():
+    return lib().bgpu_device_count()
+
+
+def solver_info(**kw):
+    s = SolverInfo()
+    lib().bgpu_solver_info_default(ctypes.byref(s))
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+def body_descs(n):
+    arr = (BodyDesc * n)()
+    for i in range(n):
+        lib().bgpu_body_desc_default(ctypes.byref(arr[i]))
+    return arr
+
+
+class World:
+    def __init__(self, gravity=(0.0, -9.81, 0.0), **info):
+        self.L = lib()
+        self.h = ctypes.c_void_p()
+        g = f32(gravity)
+        s = solver_info(**info)
+        check(self.L.bgpu_world_create(ctypes.byref(s), fptr(g), ctypes.byref(self.h)), "bgpu_world_create")
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.L.bgpu_world_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_solver(self, **info):
+        s = solver_info(**info)
+        check(self.L.bgpu_world_set_solver_info(self.h, ctypes.byref(s)), "set_solver_info")
+
+    def set_gravity(self, g):
+        check(self.L.bgpu_world_set_gravity(self.h, fptr(f32(g))), "set_gravity")
+
+    def add_shape(self, kind, params=(), points=None):
+        p = f32(list(params) + [0.0] * (4 - len(params)))
+        out = ctypes.c_uint32()
+        if points is not None:
+            pts = f32(np.asarray(points).reshape(-1, 3))
+            check(self.L.bgpu_add_shape(self.h, kind, fptr(p), fptr(pts), len(pts), ctypes.byref(out)), "add_shape")
+        else:
+            check(self.L.bgpu_add_shape(self.h, kind, fptr(p), None, 0, ctypes.byref(out)), "add_shape")
+        return out.value
+
+    def sphere(self, r):
+        return self.add_shape(SPHERE, [r])
+
+    def box(self, h):
+        return self.add_shape(BOX, list(h))
+
+    def capsule(self, r, hh):
+        return self.add_shape(CAPSULE, [r, hh])
+
+    def plane(self, n, c):
+        return self.add_shape(PLANE, list(n) + [c])
+
+    def hull(self, pts):
+        return self.add_shape(HULL, [], pts)
+
+    def add_descs(self, descs):
+        out = ctypes.c_uint32()
+        check(self.L.bgpu_add_bodies(self.h, len(descs), descs, ctypes.byref(out)), "add_bodies")
+        return out.value
+
+    def add_body(self, shape, pos, quat=(0, 0, 0, 1), linvel=(0, 0, 0), angvel=(0, 0, 0), mass=1.0, friction=0.5,
+                 restitution=0.0, flags=0, group=1, mask=0xFFFF, lin_damping=0.0, ang_damping=0.0, activation=0,
+                 kinematic=0):
+        d = body_descs(1)
+        b = d[0]
+        b.shape = shape
+        b.position[:] = list(map(float, pos))
+        b.orientation[:] = list(map(float, quat))
+        b.linear_velocity[:] = list(map(float, linvel))
+        b.angular_velocity[:] = list(map(float, angvel))
+        b.mass = mass
+        b.friction = friction
+        b.restitution = restitution
+        b.flags = flags | (KINEMATIC if kinematic else 0)
+        b.group = group
+        b.mask = mask
+        b.linear_damping = lin_damping
+        b.angular_damping = ang_damping
+        b.activation = activation
+        return self.add_descs(d)
+
+    def add_bodies_array(self, shape, pos, quat, linvel=None, angvel=None, mass=None, friction=None,
+                         restitution=None):
+        """Vectorised insertion from numpy arrays (n,), (n,3), (n,4)."""
+        n = len(shape)
+        d = body_descs(n)
+        for i in range(n):
+            b = d[i]
+            b.shape = int(shape[i])
+            b.position[:] = [float(x) for x in pos[i]]
+            b.orientation[:] = [float(x) for x in quat[i]]
+            if linvel is not None:
+                b.linear_velocity[:] = [float(x) for x in linvel[i]]
+            if angvel is not None:
+                b.angular_velocity[:] = [float(x) for x in angvel[i]]
+            if mass is not None:
+                b.mass = float(mass[i])
+            if friction is not None:
+                b.friction = float(friction[i])
+            if restitution is not None:
+                b.restitution = float(restitution[i])
+        return self.add_descs(d)
+
+    @property
+    def num_bodies(self):
+        return self.L.bgpu_num_bodies(self.h)
+
+    def step(self, dt, n=1):
+        check(self.L.bgpu_step(self.h, dt, n), "bgpu_step")
+
+    def step_timed(self, dt, n):
+        """Runs n steps; returns the device time (ms) measured on the world's stream."""
+        ms = ctypes.c_float()
+        check(self.L.bgpu_step_timed(self.h, dt, n, ctypes.byref(ms)), "bgpu_step_timed")
+        return ms.value
+
+    def step_fixed(self, dt, max_sub_steps, fixed_dt):
+        out = ctypes.c_uint32()
+        check(self.L.bgpu_step_simulation_fixed(self.h, dt, max_sub_steps, fixed_dt, ctypes.byref(out)), "step_fixed")
+        return out.value
+
+    def state(self):
+        out = np.zeros((self.num_bodies, STATE), dtype=np.float32)
+        check(self.L.bgpu_read_state(self.h, fptr(out)), "read_state")
+        return out
+
+    def set_state(self, s):
+        s = f32(s)
+        check(self.L.bgpu_write_state(self.h, fptr(s)), "write_state")
+
+    def poses(self, out=None):
+        if out is None:
+            out = np.zeros((self.num_bodies, 7), dtype=np.float32)
+        check(self.L.bgpu_read_poses(self.h, fptr(out)), "read_poses")
+        return out
+
+    def apply_forces(self, force=None, torque=None):
+        f = fptr(f32(force)) if force is not None else None
+        t = fptr(f32(torque)) if torque is not None else None
+        check(self.L.bgpu_apply_forces(self.h, f, t), "apply_forces")
+
+    def pairs(self):
+        n = ctypes.c_uint64()
+        check(self.L.bgpu_read_pairs(self.h, None, 0, ctypes.byref(n)), "read_pairs")
+        out = np.zeros((n.value, 2), dtype=np.uint32)
+        if n.value:
+            check(self.L.bgpu_read_pairs(self.h, u32ptr(out), n.value, ctypes.byref(n)), "read_pairs")
+        return out
+
+    def contacts(self):
+        n = ctypes.c_uint64()
+        check(self.L.bgpu_read_contacts(self.h, None, 0, ctypes.byref(n)), "read_contacts")
+        out = np.zeros((n.value, CONTACT), dtype=np.float32)
+        if n.value:
+            check(self.L.bgpu_read_contacts(self.h, fptr(out), n.value, ctypes.byref(n)), "read_contacts")
+        return out
+
+    def solve_order(self):
+        n = ctypes.c_uint64()
+        check(self.L.bgpu_read_solve_order(self.h, None, 0, ctypes.byref(n)), "read_solve_order")
+        out = np.zeros(n.value, dtype=np.uint64)
+        if n.value:
+            check(self.L.bgpu_read_solve_order(self.h, u64ptr(out), n.value, ctypes.byref(n)), "read_solve_order")
+        return out
+
+    def stats(self):
+        s = StepStats()
+        check(self.L.bgpu_get_stats(self.h, ctypes.byref(s)), "get_stats")
+        return {f: (list(getattr(s, f)) if f == "stage_ms" else getattr(s, f)) for f, _ in StepStats._fields_}
+
+    def enable_timing(self, on=True):
+        check(self.L.bgpu_enable_step_timing(self.h, 1 if on else 0), "timing")
+
+    def collide(self, sa, pa, sb, pb, seeds=None, force_convex=False):
+        sa = np.ascontiguousarray(sa, dtype=np.uint32)
+        sb = np.ascontiguousarray(sb, dtype=np.uint32)
+        n = len(sa)
+        pa = f32(np.asarray(pa).reshape(n, 7))
+        pb = f32(np.asarray(pb).reshape(n, 7))
+        out = np.zeros((n, 4, 7), dtype=np.float32)
+        cnt = np.zeros(n, dtype=np.uint32)
+        sd = fptr(f32(np.asarray(seeds).reshape(n, 3))) if seeds is not None else None
+        check(self.L.bgpu_collide(self.h, n, u32ptr(sa), fptr(pa), u32ptr(sb), fptr(pb), sd, 1 if force_convex else 0,
+                                  fptr(out), u32ptr(cnt)), "collide")
+        return out, cnt
+
+    def solve_contacts(self, contacts, inv_dt):
+        c = f32(np.asarray(contacts).reshape(-1, 10))
+        rows = np.zeros((len(c), CONTACT), dtype=np.float32)
+        keys = np.zeros(len(c), dtype=np.uint64)
+        check(self.L.bgpu_solve_contacts(self.h, len(c), fptr(c), inv_dt, fptr(rows), u64ptr(keys)), "solve_contacts")
+        return rows, keys
+
+    def push(self):
+        out = np.zeros((self.num_bodies, 6), dtype=np.float32)
+        check(self.L.bgpu_read_push(self.h, fptr(out)), "read_push")
+        return out
+
+
+def broadphase_pairs(aabbs):
+    a = f32(np.asarray(aabbs).reshape(-1, 6))
+    n = ctypes.c_uint64()
+    check(lib().bgpu_broadphase_pairs(fptr(a), len(a), None, 0, ctypes.byref(n)), "broadphase_pairs")
+    out = np.zeros((n.value, 2), dtype=np.uint32)
+    if n.value:
+        check(lib().bgpu_broadphase_pairs(fptr(a), len(a), u32ptr(out), n.value, ctypes.byref(n)), "broadphase_pairs")
+    return out

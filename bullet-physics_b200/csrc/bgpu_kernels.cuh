@@ -1,0 +1,210 @@
+// Host-side declarations shared by the kernel translation units and the world.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <functional>
+#include <string>
+#include <vector>
+#include "bgpu_world.cuh"
+
+namespace bgpu {
+
+// ---------------------------------------------------------------- device buffers
+struct CudaError {
+    cudaError_t code;
+    std::string where;
+};
+
+void check_cuda(cudaError_t e, const char* where);  // throws CudaError
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t cap = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    // Grow to at least n elements (contents are not preserved).
+    void reserve(size_t n) {
+        if (n <= cap) return;
+        release();
+        size_t c = n < 16 ? 16 : n;
+        check_cuda(cudaMalloc(&p, c * sizeof(T)), "cudaMalloc");
+        cap = c;
+    }
+    // Grow to at least n elements, preserving the first `keep` elements.
+    void grow_keep(size_t n, size_t keep, cudaStream_t s) {
+        if (n <= cap) return;
+        size_t c = n < 16 ? 16 : n;
+        T* q = nullptr;
+        check_cuda(cudaMalloc(&q, c * sizeof(T)), "cudaMalloc");
+        if (p && keep) check_cuda(cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, s), "copy");
+        if (p) {
+            check_cuda(cudaStreamSynchronize(s), "sync");
+            cudaFree(p);
+        }
+        p = q;
+        cap = c;
+    }
+};
+
+// ---------------------------------------------------------------- body kernels (k_body.cu)
+void launch_integrate_velocities(const BodyDev& b, const Shape* shapes, const float4* hull, uint32_t n, float dt,
+                                 cudaStream_t s);
+void launch_initial_aabbs(const BodyDev& b, const Shape* shapes, const float4* hull, uint32_t first, uint32_t n,
+                          cudaStream_t s);
+void launch_integrate_positions(const BodyDev& b, uint32_t n, float dt, float turn_erp, cudaStream_t s);
+
+// ---------------------------------------------------------------- broad phase (k_broadphase.cu)
+// Sorted closed-overlap pairs of n AABBs. `unbounded` lists (ascending) the
+// proxies kept out of the tree (planes, +-1e30 boxes); they are tested
+// against every proxy by an ordered compaction.
+struct Broadphase {
+    DevBuf<uint64_t> keys, keys_alt;
+    DevBuf<uint32_t> leaf_body, parent, left, right, counts, offsets, refit_flag, flags, scan_out, unbounded;
+    DevBuf<float4> node_min, node_max;
+    DevBuf<unsigned char> cub_tmp;
+    DevBuf<int> bounds;          // 6 ordered ints: scene min/max of leaf centres
+    DevBuf<uint32_t> scalars;    // [0] total pairs, [1] status, [2] per-unbounded count
+    uint32_t* host_scalars = nullptr;  // pinned
+    Broadphase();
+    ~Broadphase();
+    // Returns the pair count; pairs are written to `out` (grown as needed).
+    uint64_t run(const float4* aabb_min, const float4* aabb_max, uint32_t n, const std::vector<uint32_t>& unbounded_host,
+                 DevBuf<uint64_t>& out, uint32_t* status_dev, cudaStream_t s);
+};
+
+// ---------------------------------------------------------------- islands (k_islands.cu)
+struct Islands {
+    DevBuf<uint32_t> parent, awake;
+    void run(const BodyDev& b, uint32_t n, const uint64_t* pairs, uint32_t npairs, uint32_t* simulate_flag,
+             uint32_t* status_dev, cudaStream_t s);
+};
+
+// ---------------------------------------------------------------- pair pass + solver (k_pairs.cu, k_solver.cu)
+struct StepParams {
+    float dt, inv_dt;
+    SolverParams info;
+};
+
+// Raw device pointers of PairData, passed to kernels by value.
+struct PairDataDev {
+    uint32_t* status;
+    float4* entries;
+    float4* detect;
+    uint32_t* detect_n;
+    uint32_t* row_count;
+    float4* rows;
+    uint32_t* route_list;
+    uint32_t* old_owned;
+    uint32_t* scalars;
+};
+
+struct PairData {
+    // Per pair (indexed like the sorted pair array).
+    DevBuf<uint32_t> status;       // PS_* | route << 8
+    DevBuf<float4> entries;        // new manifolds (ENTRY_F4 per pair)
+    DevBuf<float4> detect;         // fresh detections: 2 float4 per point (pos,pen | normal,-), 4 points
+    DevBuf<uint32_t> detect_n;     // points per fresh detection
+    DevBuf<uint32_t> row_count;    // solver rows per pair (0..4)
+    DevBuf<float4> rows;           // ROW_F4 per contact slot, 4 slots per pair
+    DevBuf<uint32_t> route_list;   // pairs needing detection: [0, P) analytic, [P, 2P) convex
+    DevBuf<uint32_t> old_owned;    // per old manifold: 1 when a current pair took it over
+    DevBuf<uint32_t> scalars;      // [0] analytic count [1] convex count [2] contact pairs [3] contacts
+                                   // [4] colours [5] split pairs [6] detect total [7] manifolds
+    // Solver batches
+    DevBuf<uint32_t> contact_pairs;  // pair ids with rows (ascending)
+    DevBuf<uint32_t> colour;         // per contact pair
+    DevBuf<unsigned long long> body_prio;
+    DevBuf<unsigned long long> body_mask;  // 2 words per body
+    DevBuf<uint32_t> colour_count, colour_offset, colour_cursor;
+    DevBuf<uint32_t> split_count, split_offset, split_cursor;
+    DevBuf<uint32_t> batch;          // contact pairs in colour order
+    DevBuf<uint32_t> split_batch;    // pairs with split-active rows, colour order
+    DevBuf<uint32_t> flags;          // selection flags
+    DevBuf<uint32_t> sel_a, sel_b;   // cache compaction lists
+    DevBuf<unsigned char> cub_tmp;
+    DevBuf<unsigned int> barrier;    // grid barrier words + round counters
+    void reserve(size_t npairs, size_t nbodies, size_t old_manifolds) {
+        status.reserve(npairs);
+        entries.reserve(npairs * ENTRY_F4);
+        detect.reserve(npairs * 8);
+        detect_n.reserve(npairs);
+        row_count.reserve(npairs);
+        rows.reserve(npairs * 4 * ROW_F4);
+        route_list.reserve(2 * npairs);
+        old_owned.reserve(old_manifolds + 1);
+        scalars.reserve(16);
+        contact_pairs.reserve(npairs);
+        colour.reserve(npairs);
+        body_prio.reserve(nbodies);
+        body_mask.reserve(2 * nbodies);
+        colour_count.reserve(130);
+        colour_offset.reserve(130);
+        colour_cursor.reserve(130);
+        split_count.reserve(130);
+        split_offset.reserve(130);
+        split_cursor.reserve(130);
+        batch.reserve(npairs);
+        split_batch.reserve(npairs);
+        flags.reserve(npairs + old_manifolds + 1);
+        sel_a.reserve(npairs);
+        sel_b.reserve(old_manifolds + 1);
+        barrier.reserve(16);
+    }
+    PairDataDev dev() {
+        return PairDataDev{status.p, entries.p, detect.p, detect_n.p, row_count.p, rows.p, route_list.p, old_owned.p,
+                           scalars.p};
+    }
+};
+
+struct Manifolds {  // the persistent cache: sorted keys + entries
+    DevBuf<uint64_t> keys;
+    DevBuf<float4> entries;
+    DevBuf<uint32_t> count;     // device count
+    uint32_t* count_dev = nullptr;
+    uint32_t count_host = 0;    // last known count (upper bound for capacity planning)
+    void init() {
+        count.reserve(4);
+        count_dev = count.p;
+    }
+};
+
+struct WorldView {
+    BodyDev b;
+    const Shape* shapes;
+    const float4* hull;
+    uint32_t nbodies;
+};
+
+// Pair pass: classify + refresh, narrow phase, capture. Fills PairData for `npairs`.
+void run_pair_pass(const WorldView& w, const uint64_t* pairs, uint32_t npairs, const Manifolds& old_cache,
+                   PairData& pd, const StepParams& sp, const uint32_t* simulate_flag, uint32_t* status_dev,
+                   cudaStream_t s);
+// Narrow phase on explicit queries (parity harness).
+void run_collide_queries(const Shape* shapes, const float4* hull, uint32_t n, const uint32_t* sa, const float4* pa,
+                         const float4* qa, const uint32_t* sb, const float4* pb, const float4* qb, const float4* seeds,
+                         int force_convex, float4* out, uint32_t* counts, uint32_t* status_dev, cudaStream_t s);
+// Row preparation for caller-supplied contacts (parity harness).
+void run_prepare_contacts(const BodyDev& b, uint32_t ngroups, const uint32_t* group_first, const uint32_t* group_n,
+                          const float* contacts, const uint64_t* group_keys, const StepParams& sp, float4* rows,
+                          uint32_t* row_count, cudaStream_t s);
+// World inverse inertia of every body (the solver's per-body input).
+void launch_compute_iw(const BodyDev& b, uint32_t n, cudaStream_t s);
+// Colouring + PGS over the pairs with rows (counts stay on the device).
+// `mark(5)` is called after the colouring and `mark(6)` after the PGS kernel (timing hooks).
+void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
+                uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark);
+// Impulse writeback, then compaction of the surviving manifolds into `next`.
+void run_cache_update(const uint64_t* pairs, uint32_t npairs, const Manifolds& old_cache, PairData& pd,
+                      Manifolds& next, const uint32_t* simulate_flag, const uint32_t* prev_simulate,
+                      cudaStream_t s);
+
+}  // namespace bgpu

@@ -1,0 +1,359 @@
+// Broad phase: Morton-ordered linear BVH (Karras 2012 radix-tree build,
+// bottom-up refit) over the bounded proxies, queried once per proxy.
+//
+// Output contract (crates/bullet-collision/src/broadphase/mod.rs:94-130,
+// brute_force.rs:54-68): every pair (i < j) whose closed AABBs overlap on all
+// three axes (util.rs:28-38), sorted lexicographically. Each proxy i owns the
+// segment of partners j > i; a count pass sizes the segments, an exclusive
+// scan places them, and a write pass stores each segment already sorted, so
+// no global pair sort is needed. Unbounded proxies (planes) are kept out of
+// the tree and joined by an ordered flag/scan compaction.
+#include <cub/cub.cuh>
+#include "bgpu_kernels.cuh"
+
+namespace bgpu {
+
+namespace {
+
+constexpr int STACK_DEPTH = 64;
+constexpr int LOCAL_SORT = 48;
+
+__device__ __forceinline__ bool overlaps(float4 amin, float4 amax, float4 bmin, float4 bmax) {
+    return amin.x <= bmax.x && amin.y <= bmax.y && amin.z <= bmax.z && bmin.x <= amax.x && bmin.y <= amax.y &&
+           bmin.z <= amax.z;
+}
+
+__device__ __forceinline__ int float_to_ordered(float f) {
+    int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float ordered_to_float(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+__global__ void k_reset_bounds(int* bounds) {
+    if (threadIdx.x < 3) bounds[threadIdx.x] = 0x7fffffff;
+    else if (threadIdx.x < 6) bounds[threadIdx.x] = int(0x80000000);
+}
+
+__global__ void k_bounds(const float4* __restrict__ mn, const float4* __restrict__ mx, const uint32_t* __restrict__ is_unb,
+                         uint32_t n, int* bounds) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    float cx = INFINITY, cy = INFINITY, cz = INFINITY, dx = -INFINITY, dy = -INFINITY, dz = -INFINITY;
+    if (i < n && !is_unb[i]) {
+        float4 a = mn[i], b = mx[i];
+        cx = dx = 0.5f * (a.x + b.x);
+        cy = dy = 0.5f * (a.y + b.y);
+        cz = dz = 0.5f * (a.z + b.z);
+    }
+    typedef cub::BlockReduce<float, 256> BR;
+    __shared__ typename BR::TempStorage t;
+    float r;
+    r = BR(t).Reduce(cx, cub::Min()); __syncthreads(); if (threadIdx.x == 0 && r < INFINITY) atomicMin(&bounds[0], float_to_ordered(r));
+    r = BR(t).Reduce(cy, cub::Min()); __syncthreads(); if (threadIdx.x == 0 && r < INFINITY) atomicMin(&bounds[1], float_to_ordered(r));
+    r = BR(t).Reduce(cz, cub::Min()); __syncthreads(); if (threadIdx.x == 0 && r < INFINITY) atomicMin(&bounds[2], float_to_ordered(r));
+    r = BR(t).Reduce(dx, cub::Max()); __syncthreads(); if (threadIdx.x == 0 && r > -INFINITY) atomicMax(&bounds[3], float_to_ordered(r));
+    r = BR(t).Reduce(dy, cub::Max()); __syncthreads(); if (threadIdx.x == 0 && r > -INFINITY) atomicMax(&bounds[4], float_to_ordered(r));
+    r = BR(t).Reduce(dz, cub::Max()); __syncthreads(); if (threadIdx.x == 0 && r > -INFINITY) atomicMax(&bounds[5], float_to_ordered(r));
+}
+
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t quantize(float c, float lo, float hi) {
+    float ext = hi - lo;
+    float t = ext > 0.0f ? (c - lo) / ext : 0.0f;
+    t = fminf(fmaxf(t, 0.0f), 1.0f);
+    return uint32_t(t * 1023.0f);
+}
+
+__global__ void k_keys(const float4* __restrict__ mn, const float4* __restrict__ mx, const uint32_t* __restrict__ is_unb,
+                       uint32_t n, const int* __restrict__ bounds, uint64_t* keys) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (is_unb[i]) { keys[i] = ~0ull; return; }
+    float4 a = mn[i], b = mx[i];
+    float lo0 = ordered_to_float(bounds[0]), lo1 = ordered_to_float(bounds[1]), lo2 = ordered_to_float(bounds[2]);
+    float hi0 = ordered_to_float(bounds[3]), hi1 = ordered_to_float(bounds[4]), hi2 = ordered_to_float(bounds[5]);
+    uint32_t x = quantize(0.5f * (a.x + b.x), lo0, hi0);
+    uint32_t y = quantize(0.5f * (a.y + b.y), lo1, hi1);
+    uint32_t z = quantize(0.5f * (a.z + b.z), lo2, hi2);
+    uint32_t code = (expand_bits(x) << 2) | (expand_bits(y) << 1) | expand_bits(z);
+    keys[i] = (uint64_t(code) << 32) | i;
+}
+
+__device__ __forceinline__ int delta(const uint64_t* __restrict__ k, int m, int i, int j) {
+    if (j < 0 || j >= m) return -1;
+    return __clzll(k[i] ^ k[j]);
+}
+
+// Karras 2012: internal node i spans a key range split at its highest differing bit.
+__global__ void k_build(const uint64_t* __restrict__ k, int m, uint32_t* left, uint32_t* right, uint32_t* parent,
+                        uint32_t* leaf_body, uint32_t* refit_flag) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) leaf_body[i] = uint32_t(k[i] & 0xffffffffu);
+    if (i >= m - 1) return;
+    refit_flag[i] = 0;
+    int d = (delta(k, m, i, i + 1) - delta(k, m, i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = delta(k, m, i, i - d);
+    int lmax = 2;
+    while (delta(k, m, i, i + lmax * d) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+        if (delta(k, m, i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = delta(k, m, i, j);
+    int s = 0;
+    int t = l;
+    do {
+        t = (t + 1) / 2;
+        if (delta(k, m, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    int gamma = i + s * d + min(d, 0);
+    int lo = min(i, j), hi = max(i, j);
+    uint32_t lc = (lo == gamma) ? uint32_t(m - 1 + gamma) : uint32_t(gamma);
+    uint32_t rc = (hi == gamma + 1) ? uint32_t(m - 1 + gamma + 1) : uint32_t(gamma + 1);
+    left[i] = lc;
+    right[i] = rc;
+    parent[lc] = uint32_t(i);
+    parent[rc] = uint32_t(i);
+}
+
+__global__ void k_refit(int m, const uint32_t* __restrict__ leaf_body, const uint32_t* __restrict__ parent,
+                        const uint32_t* __restrict__ left, const uint32_t* __restrict__ right, uint32_t* refit_flag,
+                        const float4* __restrict__ bmin, const float4* __restrict__ bmax, float4* nmin, float4* nmax) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    uint32_t node = uint32_t(m - 1 + t);
+    uint32_t body = leaf_body[t];
+    nmin[node] = bmin[body];
+    nmax[node] = bmax[body];
+    if (m == 1) return;
+    __threadfence();
+    uint32_t cur = parent[node];
+    for (int guard = 0; guard < 128; ++guard) {
+        if (atomicAdd(&refit_flag[cur], 1u) == 0) return;  // first child to arrive stops
+        __threadfence();
+        uint32_t l = left[cur], r = right[cur];
+        float4 a0 = __ldcg(&nmin[l]), a1 = __ldcg(&nmax[l]), b0 = __ldcg(&nmin[r]), b1 = __ldcg(&nmax[r]);
+        nmin[cur] = make_float4(fminf(a0.x, b0.x), fminf(a0.y, b0.y), fminf(a0.z, b0.z), 0.f);
+        nmax[cur] = make_float4(fmaxf(a1.x, b1.x), fmaxf(a1.y, b1.y), fmaxf(a1.z, b1.z), 0.f);
+        __threadfence();
+        if (cur == 0) return;
+        cur = parent[cur];
+    }
+}
+
+// Count pass (write == false) or write pass: partners j > i of bounded proxy i.
+template <bool WRITE>
+__global__ void k_query(int m, uint32_t n, const uint32_t* __restrict__ is_unb, const float4* __restrict__ bmin,
+                        const float4* __restrict__ bmax, const float4* __restrict__ nmin, const float4* __restrict__ nmax,
+                        const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                        const uint32_t* __restrict__ leaf_body, const uint32_t* __restrict__ unb, uint32_t nunb,
+                        uint32_t* counts, const uint32_t* __restrict__ offsets, uint64_t* out, uint32_t* status) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || is_unb[i]) return;
+    float4 qmin = bmin[i], qmax = bmax[i];
+    uint32_t cnt = 0;
+    uint32_t local[LOCAL_SORT];
+    uint64_t base = 0;
+    uint32_t expected = 0;
+    if (WRITE) {
+        base = offsets[i];
+        expected = counts[i];
+    }
+    auto emit = [&](uint32_t j) {
+        if (WRITE) {
+            if (expected <= LOCAL_SORT) {
+                if (cnt < LOCAL_SORT) local[cnt] = j;
+            } else if (cnt < expected) {
+                out[base + cnt] = (uint64_t(i) << 32) | j;
+            }
+        }
+        ++cnt;
+    };
+    if (m > 0) {
+        uint32_t stack[STACK_DEPTH];
+        int sp = 0;
+        stack[sp++] = 0u;
+        if (m == 1) {
+            // The root is the single leaf.
+            sp = 0;
+            uint32_t j = leaf_body[0];
+            if (j > i && overlaps(qmin, qmax, bmin[j], bmax[j])) emit(j);
+        }
+        while (sp > 0) {
+            uint32_t node = stack[--sp];
+            uint32_t ch[2] = {left[node], right[node]};
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                uint32_t cn = ch[c];
+                if (!overlaps(qmin, qmax, nmin[cn], nmax[cn])) continue;
+                if (cn >= uint32_t(m - 1)) {
+                    uint32_t j = leaf_body[cn - (m - 1)];
+                    if (j > i) emit(j);
+                } else if (sp < STACK_DEPTH) {
+                    stack[sp++] = cn;
+                } else {
+                    atomicOr(status, ST_TRAVERSAL_STACK);
+                }
+            }
+        }
+    }
+    for (uint32_t u = 0; u < nunb; ++u) {
+        uint32_t h = unb[u];
+        if (h > i && overlaps(qmin, qmax, bmin[h], bmax[h])) emit(h);
+    }
+    if (!WRITE) {
+        counts[i] = cnt;
+        return;
+    }
+    if (expected <= LOCAL_SORT) {
+        uint32_t c = cnt < LOCAL_SORT ? cnt : LOCAL_SORT;
+        for (uint32_t a = 1; a < c; ++a) {
+            uint32_t v = local[a];
+            uint32_t b = a;
+            while (b > 0 && local[b - 1] > v) { local[b] = local[b - 1]; --b; }
+            local[b] = v;
+        }
+        for (uint32_t a = 0; a < c; ++a) out[base + a] = (uint64_t(i) << 32) | local[a];
+    } else {
+        uint32_t c = cnt < expected ? cnt : expected;
+        for (uint32_t a = 1; a < c; ++a) {
+            uint64_t v = out[base + a];
+            uint32_t b = a;
+            while (b > 0 && out[base + b - 1] > v) { out[base + b] = out[base + b - 1]; --b; }
+            out[base + b] = v;
+        }
+    }
+}
+
+// Unbounded proxy h: flags[j] = (j > h && overlap(h, j)) over all proxies.
+__global__ void k_unb_flags(uint32_t h, uint32_t n, const float4* __restrict__ bmin, const float4* __restrict__ bmax,
+                            uint32_t* flags) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    flags[j] = (j > h && overlaps(bmin[h], bmax[h], bmin[j], bmax[j])) ? 1u : 0u;
+}
+
+__global__ void k_unb_count(uint32_t h, uint32_t n, const uint32_t* __restrict__ flags, const uint32_t* __restrict__ scan,
+                            uint32_t* counts) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) counts[h] = n ? scan[n - 1] + flags[n - 1] : 0u;
+}
+
+__global__ void k_unb_write(uint32_t h, uint32_t n, const uint32_t* __restrict__ flags, const uint32_t* __restrict__ scan,
+                            const uint32_t* __restrict__ offsets, uint64_t* out) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n || !flags[j]) return;
+    out[uint64_t(offsets[h]) + scan[j]] = (uint64_t(h) << 32) | j;
+}
+
+__global__ void k_total(uint32_t n, const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
+                        uint32_t* scalars) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        uint64_t t = n ? uint64_t(offsets[n - 1]) + counts[n - 1] : 0;
+        scalars[0] = uint32_t(t > 0xffffffffull ? 0xffffffffull : t);
+    }
+}
+
+__global__ void k_clear_u32(uint32_t n, uint32_t* a) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = 0;
+}
+
+__global__ void k_set_unbounded(const uint32_t* __restrict__ unb, uint32_t nunb, uint32_t* is_unb) {
+    uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u < nunb) is_unb[unb[u]] = 1;
+}
+
+}  // namespace
+
+Broadphase::Broadphase() {
+    check_cuda(cudaMallocHost(&host_scalars, 4 * sizeof(uint32_t)), "cudaMallocHost");
+}
+
+Broadphase::~Broadphase() {
+    if (host_scalars) cudaFreeHost(host_scalars);
+}
+
+uint64_t Broadphase::run(const float4* aabb_min, const float4* aabb_max, uint32_t n,
+                         const std::vector<uint32_t>& unbounded_host, DevBuf<uint64_t>& out, uint32_t* status_dev,
+                         cudaStream_t s) {
+    if (n == 0) return 0;
+    const uint32_t nunb = uint32_t(unbounded_host.size());
+    const int m = int(n - nunb);
+    const int TB = 256;
+    const uint32_t grid = (n + TB - 1) / TB;
+    keys.reserve(n);
+    keys_alt.reserve(n);
+    leaf_body.reserve(n);
+    parent.reserve(2 * size_t(n));
+    left.reserve(n);
+    right.reserve(n);
+    refit_flag.reserve(n);
+    node_min.reserve(2 * size_t(n));
+    node_max.reserve(2 * size_t(n));
+    counts.reserve(n);
+    offsets.reserve(n);
+    flags.reserve(n);
+    scan_out.reserve(n);
+    bounds.reserve(6);
+    scalars.reserve(4);
+    unbounded.reserve(nunb + 1);
+    if (nunb) check_cuda(cudaMemcpyAsync(unbounded.p, unbounded_host.data(), nunb * sizeof(uint32_t),
+                                         cudaMemcpyHostToDevice, s), "upload unbounded");
+    // flags doubles as the "is unbounded" marker until the unbounded pass.
+    k_clear_u32<<<grid, TB, 0, s>>>(n, flags.p);
+    if (nunb) k_set_unbounded<<<(nunb + TB - 1) / TB, TB, 0, s>>>(unbounded.p, nunb, flags.p);
+    k_reset_bounds<<<1, 32, 0, s>>>(bounds.p);
+    k_bounds<<<grid, TB, 0, s>>>(aabb_min, aabb_max, flags.p, n, bounds.p);
+    k_keys<<<grid, TB, 0, s>>>(aabb_min, aabb_max, flags.p, n, bounds.p, keys.p);
+
+    // Sort the Morton keys (unbounded proxies carry ~0 and sort last).
+    size_t tmp_bytes = 0;
+    cub::DoubleBuffer<uint64_t> db(keys.p, keys_alt.p);
+    check_cuda(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, int(n), 0, 64, s), "sort size");
+    size_t scan_bytes = 0;
+    check_cuda(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, counts.p, offsets.p, int(n), s), "scan size");
+    cub_tmp.reserve(std::max(tmp_bytes, scan_bytes));
+    check_cuda(cub::DeviceRadixSort::SortKeys(cub_tmp.p, tmp_bytes, db, int(n), 0, 64, s), "sort");
+    const uint64_t* sorted = db.Current();
+
+    if (m > 0) {
+        k_build<<<(m + TB - 1) / TB, TB, 0, s>>>(sorted, m, left.p, right.p, parent.p, leaf_body.p, refit_flag.p);
+        k_refit<<<(m + TB - 1) / TB, TB, 0, s>>>(m, leaf_body.p, parent.p, left.p, right.p, refit_flag.p, aabb_min,
+                                                 aabb_max, node_min.p, node_max.p);
+    }
+    k_query<false><<<grid, TB, 0, s>>>(m, n, flags.p, aabb_min, aabb_max, node_min.p, node_max.p, left.p, right.p,
+                                        leaf_body.p, unbounded.p, nunb, counts.p, nullptr, nullptr, status_dev);
+    // Unbounded proxies: count their segments by flag + scan.
+    for (uint32_t u = 0; u < nunb; ++u) {
+        uint32_t h = unbounded_host[u];
+        // scan_out holds the flags; the key scratch (no longer needed after the build) holds the scan.
+        k_unb_flags<<<grid, TB, 0, s>>>(h, n, aabb_min, aabb_max, scan_out.p);
+        check_cuda(cub::DeviceScan::ExclusiveSum(cub_tmp.p, scan_bytes, scan_out.p, (uint32_t*)keys_alt.p, int(n), s), "scan");
+        k_unb_count<<<1, 1, 0, s>>>(h, n, scan_out.p, (uint32_t*)keys_alt.p, counts.p);
+    }
+    check_cuda(cub::DeviceScan::ExclusiveSum(cub_tmp.p, scan_bytes, counts.p, offsets.p, int(n), s), "scan");
+    k_total<<<1, 1, 0, s>>>(n, counts.p, offsets.p, scalars.p);
+    check_cuda(cudaMemcpyAsync(host_scalars, scalars.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "total d2h");
+    check_cuda(cudaStreamSynchronize(s), "broadphase sync");
+    uint64_t total = host_scalars[0];
+    out.reserve(total + 1);
+    if (total) {
+        k_query<true><<<grid, TB, 0, s>>>(m, n, flags.p, aabb_min, aabb_max, node_min.p, node_max.p, left.p, right.p,
+                                           leaf_body.p, unbounded.p, nunb, counts.p, offsets.p, out.p, status_dev);
+        for (uint32_t u = 0; u < nunb; ++u) {
+            uint32_t h = unbounded_host[u];
+            k_unb_flags<<<grid, TB, 0, s>>>(h, n, aabb_min, aabb_max, scan_out.p);
+            check_cuda(cub::DeviceScan::ExclusiveSum(cub_tmp.p, scan_bytes, scan_out.p, (uint32_t*)keys_alt.p, int(n), s), "scan");
+            k_unb_write<<<grid, TB, 0, s>>>(h, n, scan_out.p, (uint32_t*)keys_alt.p, offsets.p, out.p);
+        }
+    }
+    return total;
+}
+
+}  // namespace bgpu

@@ -1,0 +1,561 @@
+// Pair pass of the step (crates/bullet-dynamics/src/world/step.rs:439-854):
+// per broad-phase pair, the group/mask filter, the persistent-manifold
+// lookup, the refresh-versus-redetect gate, the narrow phase, the merge of a
+// fresh detection into the cached manifold, and the solver-row preparation
+// (sequential_impulse.rs:339-550). Three kernels: classify+refresh (one
+// thread per pair), narrow phase (analytic routes, then GJK/EPA on its own
+// compacted list so EPA's scratch only costs where it runs), and
+// capture+refresh+rows for the pairs that were re-detected.
+#include <cub/cub.cuh>
+#include "bgpu_kernels.cuh"
+
+namespace bgpu {
+
+namespace {
+
+constexpr float REDETECT_SPEED_SQUARED = 0.08f * 0.08f;  // world.rs:62
+constexpr float REDRIFT_T = 0.005f;                       // manifold.rs:149-151
+constexpr float REDRIFT_ANGLE = 0.01f;
+
+struct Pt {
+    V3 la, lb, n;
+    float pen, imp;
+    uint32_t life;
+};
+
+struct Entry {
+    V3 dpa, dpb;
+    Q dqa, dqb;
+    float thr;
+    uint32_t meta;
+    Pt p[4];
+    __device__ int count() const { return int(meta & 7u); }
+};
+
+__device__ __forceinline__ Entry load_entry(const float4* __restrict__ e) {
+    Entry E;
+    float4 a = __ldg(&e[0]), b = __ldg(&e[1]), c = __ldg(&e[2]), d = __ldg(&e[3]);
+    E.dpa = from4(a);
+    E.thr = a.w;
+    E.dqa = q4(b);
+    E.dpb = from4(c);
+    E.meta = __float_as_uint(c.w);
+    E.dqb = q4(d);
+    int n = E.count();
+    for (int k = 0; k < 4; ++k) {
+        if (k >= n) break;
+        float4 x = __ldg(&e[4 + 3 * k]), y = __ldg(&e[5 + 3 * k]), z = __ldg(&e[6 + 3 * k]);
+        E.p[k].la = from4(x); E.p[k].pen = x.w;
+        E.p[k].lb = from4(y); E.p[k].imp = y.w;
+        E.p[k].n = from4(z); E.p[k].life = __float_as_uint(z.w);
+    }
+    return E;
+}
+
+__device__ __forceinline__ void store_entry(float4* e, const Entry& E) {
+    e[0] = to4(E.dpa, E.thr);
+    e[1] = to4(E.dqa);
+    e[2] = to4(E.dpb, __uint_as_float(E.meta));
+    e[3] = to4(E.dqb);
+    int n = E.count();
+    for (int k = 0; k < n; ++k) {
+        e[4 + 3 * k] = to4(E.p[k].la, E.p[k].pen);
+        e[5 + 3 * k] = to4(E.p[k].lb, E.p[k].imp);
+        e[6 + 3 * k] = to4(E.p[k].n, __uint_as_float(E.p[k].life));
+    }
+}
+
+__device__ __forceinline__ void store_meta_only(float4* e, uint32_t meta) {
+    e[2] = make_float4(0.f, 0.f, 0.f, __uint_as_float(meta));
+}
+
+__device__ __forceinline__ float rotation_angle(Q q) { return 2.0f * acosf(fminf(fmaxf(q.w, -1.0f), 1.0f)); }
+
+// manifold.rs:287-304
+__device__ __forceinline__ bool needs_redetect(const Entry& E, V3 pa, Q qa, V3 pb, Q qb) {
+    if (!(E.meta & META_INIT)) return true;
+    V3 drift = (pb - E.dpb) - (pa - E.dpa);
+    if (len2(drift) > REDRIFT_T * REDRIFT_T) return true;
+    Q ra = qmul(qa, qinv(E.dqa));
+    Q rb = qmul(qb, qinv(E.dqb));
+    return rotation_angle(ra) + rotation_angle(rb) > REDRIFT_ANGLE;
+}
+
+struct Out {
+    int n;
+    V3 pos[4], nrm[4];
+    float pen[4], imp[4];
+};
+
+// manifold.rs:246-282 — survivors keep their order, so out k addresses cache point k.
+__device__ __forceinline__ void refresh(Entry& E, V3 pa, Q qa, V3 pb, Q qb, Out& o) {
+    float thr = E.thr, thr_sq = thr * thr;
+    int kept = 0;
+    o.n = 0;
+    int n = E.count();
+    for (int k = 0; k < n; ++k) {
+        Pt p = E.p[k];
+        V3 wa = pa + rotate(qa, p.la);
+        V3 wb = pb + rotate(qb, p.lb);
+        V3 d = wa - wb;
+        float pen = dot(d, p.n);
+        if (pen < -thr) continue;
+        V3 lat = d - p.n * pen;
+        if (len2(lat) > thr_sq) continue;
+        p.pen = pen;
+        p.life += 1;
+        o.pos[o.n] = wb; o.nrm[o.n] = p.n; o.pen[o.n] = pen; o.imp[o.n] = p.imp; o.n++;
+        E.p[kept++] = p;
+    }
+    E.meta = (E.meta & ~7u) | uint32_t(kept);
+}
+
+__device__ __forceinline__ int32_t total_key(float v) {
+    int32_t b = __float_as_int(v);
+    return b ^ int32_t(uint32_t(b >> 31) >> 1);
+}
+
+// manifold.rs:326-376
+__device__ __forceinline__ void capture(Entry& E, const Manifold& m, V3 pa, Q qa, V3 pb, Q qb, float thr) {
+    E.thr = thr;
+    Q ia = qinv(qa), ib = qinv(qb);
+    float thr_sq = thr * thr;
+    Pt pts[8];
+    int n = E.count();
+    for (int k = 0; k < n; ++k) pts[k] = E.p[k];
+    for (int c = 0; c < m.n; ++c) {
+        V3 wb = m.pos[c];
+        V3 wa = m.pos[c] + m.nrm[c] * m.pen[c];
+        Pt pt;
+        pt.la = rotate(ia, wa - pa);
+        pt.lb = rotate(ib, wb - pb);
+        pt.n = m.nrm[c];
+        pt.pen = m.pen[c];
+        pt.imp = 0.0f;
+        pt.life = 0;
+        bool matched = false;
+        for (int k = 0; k < n; ++k) {
+            if (len2(pts[k].la - pt.la) < thr_sq && dot(pts[k].n, pt.n) >= 0.9f) {
+                pt.imp = pts[k].imp;
+                pts[k] = pt;
+                matched = true;
+                break;
+            }
+        }
+        if (!matched) pts[n++] = pt;
+    }
+    if (n > 4) {  // stable descending sort by penetration (total order), keep four
+        for (int a = 1; a < n; ++a) {
+            Pt v = pts[a];
+            int32_t kv = total_key(v.pen);
+            int b = a;
+            while (b > 0 && total_key(pts[b - 1].pen) < kv) { pts[b] = pts[b - 1]; --b; }
+            pts[b] = v;
+        }
+        n = 4;
+    }
+    for (int k = 0; k < n; ++k) E.p[k] = pts[k];
+    E.dpa = pa; E.dqa = qa; E.dpb = pb; E.dqb = qb;
+    E.meta = (E.meta & ~7u) | uint32_t(n) | META_INIT | META_VALID;
+}
+
+__device__ __forceinline__ M3 load_iw(const float4* __restrict__ iw, uint32_t i, float& inv_mass) {
+    float4 a = iw[3 * i], b = iw[3 * i + 1], c = iw[3 * i + 2];
+    inv_mass = c.y;
+    return M3{V3{a.x, a.y, a.z}, V3{a.w, b.x, b.y}, V3{b.z, b.w, c.x}};
+}
+
+// sequential_impulse.rs:655-673
+__device__ __forceinline__ float effective_mass(float ima, float imb, V3 aa, V3 ab, V3 ra, V3 rb, V3 d) {
+    float k = ima + imb + dot(d, cross(aa, ra)) + dot(d, cross(ab, rb));
+    return k > 0.0f ? 1.0f / k : 0.0f;
+}
+
+// step.rs:750-764 + sequential_impulse.rs:339-550: one prepared row per refreshed point.
+__device__ __forceinline__ void emit_rows(const BodyDev& b, uint32_t i, uint32_t j, const Out& o, const StepParams& sp,
+                                          float4* __restrict__ rows, uint32_t* __restrict__ row_count, uint32_t p) {
+    float ima, imb;
+    M3 iwa = load_iw(b.iw, i, ima);
+    M3 iwb = load_iw(b.iw, j, imb);
+    V3 posa = from4(b.pos[i]), posb = from4(b.pos[j]);
+    float4 ma = b.material[i], mb = b.material[j];
+    const SolverParams& info = sp.info;
+    float inv_dt = sp.inv_dt;
+    for (int k = 0; k < o.n; ++k) {
+        V3 n = o.nrm[k];
+        float imp = o.imp[k] * info.warmstarting_factor;
+        V3 t1, t2;
+        tangent_basis_dev(n, t1, t2);
+        V3 ra = o.pos[k] - posa;
+        V3 rb = o.pos[k] - posb;
+        V3 ana = mul(iwa, cross(ra, n)), anb = mul(iwb, cross(rb, n));
+        V3 a1a = mul(iwa, cross(ra, t1)), a1b = mul(iwb, cross(rb, t1));
+        V3 a2a = mul(iwa, cross(ra, t2)), a2b = mul(iwb, cross(rb, t2));
+        float nm = effective_mass(ima, imb, ana, anb, ra, rb, n);
+        float t1m = effective_mass(ima, imb, a1a, a1b, ra, rb, t1);
+        float t2m = effective_mass(ima, imb, a2a, a2b, ra, rb, t2);
+        float friction = ma.x * mb.x;
+        float restitution = ma.y * mb.y;
+        float erp = info.erp2;
+        float ncfm = 0.0f;
+        float cfm_global = info.global_cfm * inv_dt;
+        if (cfm_global != 0.0f || info.sor != 1.0f) {
+            float kk = nm > 0.0f ? 1.0f / nm : 0.0f;
+            nm = kk + cfm_global > 0.0f ? info.sor / (kk + cfm_global) : 0.0f;
+            ncfm = cfm_global * nm;
+        }
+        if (info.sor != 1.0f) { t1m *= info.sor; t2m *= info.sor; }
+        float pen = o.pen[k];
+        float span = fmaxf(pen - info.linear_slop, 0.0f);
+        float separation = fminf(pen, 0.0f);
+        bool split = info.split_impulse != 0 && pen > -info.split_impulse_penetration_threshold;
+        float baum = split ? 0.0f : erp * inv_dt * span;
+        float sepb = separation < 0.0f ? separation * inv_dt : 0.0f;
+        float rhs = split ? pen * erp * inv_dt * nm : 0.0f;
+        float4* r = rows + (size_t(p) * 4 + k) * ROW_F4;
+        r[0] = to4(n, friction);
+        r[1] = to4(ra, baum);
+        r[2] = to4(rb, sepb);
+        r[3] = make_float4(imp, 0.0f, 0.0f, restitution);
+        r[4] = make_float4(nm, t1m, t2m, ncfm);
+        r[5] = make_float4(rhs, 0.0f, split ? 1.0f : 0.0f, pen);
+    }
+    row_count[p] = uint32_t(o.n);
+}
+
+__device__ __forceinline__ uint32_t route_of(uint32_t ta, uint32_t tb) {
+    if (ta == SHAPE_PLANE && tb == SHAPE_PLANE) return NP_NONE;
+    if (ta == SHAPE_PLANE) return NP_PLANE_A;
+    if (tb == SHAPE_PLANE) return NP_PLANE_B;
+    if (ta == SHAPE_SPHERE && tb == SHAPE_SPHERE) return NP_SPHERE_SPHERE;
+    if (ta == SHAPE_SPHERE && tb == SHAPE_BOX) return NP_SPHERE_BOX;
+    if (ta == SHAPE_BOX && tb == SHAPE_SPHERE) return NP_BOX_SPHERE;
+    if (ta == SHAPE_BOX && tb == SHAPE_BOX) return NP_BOX_BOX;
+    return NP_CONVEX;
+}
+
+__device__ __forceinline__ int64_t find_key(const uint64_t* __restrict__ keys, uint32_t n, uint64_t k) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        uint64_t v = keys[mid];
+        if (v < k) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < n && keys[lo] == k) ? int64_t(lo) : -1;
+}
+
+__device__ __forceinline__ bool active_state(uint32_t a) {
+    return a == ACT_ACTIVE || a == ACT_WANTS_DEACTIVATION || a == ACT_DISABLE_DEACTIVATION;
+}
+
+// step.rs:645-799, classify + refresh path. Scalars: [0] analytic list count, [1] convex list count.
+__global__ void k_classify(BodyDev b, const Shape* __restrict__ shapes, const uint64_t* __restrict__ pairs,
+                           uint32_t npairs, const uint64_t* __restrict__ old_keys, const float4* __restrict__ old_entries,
+                           const uint32_t* __restrict__ old_count_ptr, StepParams sp, PairDataDev pd) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    uint64_t key = pairs[p];
+    uint32_t i = key_lo(key), j = key_hi(key);
+    uint4 ia = b.info[i], ib = b.info[j];
+    float4* ne = pd.entries + size_t(p) * ENTRY_F4;
+    pd.row_count[p] = 0;
+    pd.detect_n[p] = 0;
+    uint32_t ga = ia.w & 0xffffu, mka = ia.w >> 16, gb = ib.w & 0xffffu, mkb = ib.w >> 16;
+    if ((ga & mkb) == 0 || (gb & mka) == 0) {
+        pd.status[p] = PS_NONE;
+        store_meta_only(ne, 0u);
+        return;
+    }
+    uint32_t old_count = *old_count_ptr;
+    int64_t old = old_count ? find_key(old_keys, old_count, key) : -1;
+    if (old >= 0) pd.old_owned[old] = 1u;
+    bool act_a = active_state(ia.z), act_b = active_state(ib.z);
+    bool sk_a = (ia.y & (BF_STATIC | BF_KINEMATIC)) != 0, sk_b = (ib.y & (BF_STATIC | BF_KINEMATIC)) != 0;
+    if ((!act_a && !act_b) || (sk_a && sk_b)) {
+        // step.rs:677-715: a sleeping island / immovable pair keeps its manifold verbatim.
+        pd.status[p] = PS_KEEP;
+        if (old >= 0) {
+            const float4* oe = old_entries + size_t(old) * ENTRY_F4;
+            for (int t = 0; t < ENTRY_F4; ++t) ne[t] = __ldg(&oe[t]);
+        } else {
+            store_meta_only(ne, 0u);
+        }
+        return;
+    }
+    bool no_response = ((ia.y | ib.y) & BF_NO_RESPONSE) != 0;
+    V3 pa = from4(b.pred[i]), pb = from4(b.pred[j]);
+    Q qa = q4(b.quat[i]), qb = q4(b.quat[j]);
+    bool fast = b.settled[i] > REDETECT_SPEED_SQUARED || b.settled[j] > REDETECT_SPEED_SQUARED;
+    Entry E;
+    E.meta = 0;
+    if (old >= 0) E = load_entry(old_entries + size_t(old) * ENTRY_F4);
+    if (old >= 0 && !needs_redetect(E, pa, qa, pb, qb)) {
+        Out o;
+        refresh(E, pa, qa, pb, qb, o);
+        bool deep = false;
+        for (int k = 0; k < o.n; ++k) if (o.pen[k] > sp.info.linear_slop) deep = true;
+        if (!fast || !deep) {
+            store_entry(ne, E);
+            if (!no_response) emit_rows(b, i, j, o, sp, pd.rows, pd.row_count, p);
+            pd.status[p] = PS_SERVED;
+            return;
+        }
+    }
+    if (old >= 0) store_entry(ne, E);
+    else store_meta_only(ne, 0u);
+    uint32_t route = route_of(shapes[ia.x].type, shapes[ib.x].type);
+    pd.status[p] = PS_DETECT | (route << 8);
+    if (route == NP_NONE) return;
+    if (route == NP_CONVEX) {
+        uint32_t slot = atomicAdd(&pd.scalars[1], 1u);
+        pd.route_list[npairs + slot] = p;
+    } else {
+        uint32_t slot = atomicAdd(&pd.scalars[0], 1u);
+        pd.route_list[slot] = p;
+    }
+}
+
+// narrowphase/mod.rs:63-286 for one pair; returns the manifold (positions on B, normals A->B).
+__device__ __forceinline__ void collide_analytic(uint32_t route, const Shape& sa, V3 pa, Q qa, const Shape& sb, V3 pb,
+                                                 Q qb, const float4* __restrict__ hull, Manifold& m) {
+    float thr = fminf(sa.cbt, sb.cbt);
+    m.n = 0;
+    switch (route) {
+        case NP_PLANE_A: plane_convex(sa, pa, qa, sb, pb, qb, thr, hull, m); break;
+        case NP_PLANE_B:
+            if (plane_convex(sb, pb, qb, sa, pa, qa, thr, hull, m)) mf_flip(m);
+            break;
+        case NP_SPHERE_SPHERE: sphere_sphere(sa.p0, pa, sb.p0, pb, m); break;
+        case NP_SPHERE_BOX:
+            if (sphere_box(sa.p0, pa, V3{sb.p0, sb.p1, sb.p2}, pb, qb, thr, m)) mf_flip(m);
+            break;
+        case NP_BOX_SPHERE: sphere_box(sb.p0, pb, V3{sa.p0, sa.p1, sa.p2}, pa, qa, thr, m); break;
+        case NP_BOX_BOX: box_box(V3{sa.p0, sa.p1, sa.p2}, pa, qa, V3{sb.p0, sb.p1, sb.p2}, pb, qb, m); break;
+        default: break;
+    }
+}
+
+// convex_convex.rs:30-155
+__device__ __noinline__ void collide_convex(const Shape& sa, V3 pa, Q qa, const Shape& sb, V3 pb, Q qb, bool has_seed,
+                                            V3 seed, const float4* __restrict__ hull, EpaScratch& scratch, Manifold& m,
+                                            uint32_t* status) {
+    m.n = 0;
+    float thr = fminf(sa.cbt, sb.cbt);
+    ConvexPair cp;
+    cp.sa = &sa; cp.sb = &sb; cp.pa = pa; cp.pb = pb; cp.qa = qa; cp.qb = qb; cp.hull = hull;
+    GjkResult g = gjk_contact(cp, has_seed, seed, thr);
+    if (g.kind == 0) return;
+    if (g.kind == 1) {
+        mf_push(m, g.point_on_b, g.normal, -g.distance);
+        return;
+    }
+    V3 n;
+    float core_depth;
+    if (epa_penetration(cp, g.simplex, scratch, n, core_depth)) atomicOr(status, ST_EPA_CAPACITY);
+    if (core_depth <= 0.0f) return;
+    float depth = core_depth + sa.margin + sb.margin;
+    V3 point_a = support_world(sa, pa, qa, n, hull);
+    mf_push(m, point_a - n * depth, n, depth);
+}
+
+__device__ __forceinline__ void store_detection(PairDataDev& pd, uint32_t p, const Manifold& m) {
+    float4* d = pd.detect + size_t(p) * 8;
+    for (int k = 0; k < m.n; ++k) {
+        d[2 * k] = to4(m.pos[k], m.pen[k]);
+        d[2 * k + 1] = to4(m.nrm[k], 0.0f);
+    }
+    pd.detect_n[p] = uint32_t(m.n);
+}
+
+__device__ __forceinline__ bool entry_seed(const float4* __restrict__ e, V3& s) {
+    float4 c = e[2];
+    uint32_t meta = __float_as_uint(c.w);
+    if (!(meta & META_VALID) || (meta & 7u) == 0) return false;
+    float4 z = e[6];
+    V3 n = from4(z);
+    if (len2(n) > 0.5f) { s = n; return true; }
+    return false;
+}
+
+__global__ void k_narrow_analytic(BodyDev b, const Shape* __restrict__ shapes, const float4* __restrict__ hull,
+                                  const uint64_t* __restrict__ pairs, PairDataDev pd) {
+    uint32_t cnt = pd.scalars[0];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+        uint32_t p = pd.route_list[t];
+        uint64_t key = pairs[p];
+        uint32_t i = key_lo(key), j = key_hi(key);
+        uint4 ia = b.info[i], ib = b.info[j];
+        Shape sa = shapes[ia.x], sb = shapes[ib.x];
+        Manifold m;
+        collide_analytic(pd.status[p] >> 8, sa, from4(b.pred[i]), q4(b.quat[i]), sb, from4(b.pred[j]), q4(b.quat[j]),
+                         hull, m);
+        store_detection(pd, p, m);
+    }
+}
+
+__global__ void k_narrow_convex(BodyDev b, const Shape* __restrict__ shapes, const float4* __restrict__ hull,
+                                const uint64_t* __restrict__ pairs, uint32_t npairs, PairDataDev pd, uint32_t* status) {
+    uint32_t cnt = pd.scalars[1];
+    EpaScratch scratch;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+        uint32_t p = pd.route_list[npairs + t];
+        uint64_t key = pairs[p];
+        uint32_t i = key_lo(key), j = key_hi(key);
+        uint4 ia = b.info[i], ib = b.info[j];
+        Shape sa = shapes[ia.x], sb = shapes[ib.x];
+        V3 seed = V3{0.f, 0.f, 0.f};
+        bool has_seed = entry_seed(pd.entries + size_t(p) * ENTRY_F4, seed);
+        Manifold m;
+        collide_convex(sa, from4(b.pred[i]), q4(b.quat[i]), sb, from4(b.pred[j]), q4(b.quat[j]), has_seed, seed, hull,
+                       scratch, m, status);
+        store_detection(pd, p, m);
+    }
+}
+
+// step.rs:800-853: merge the detection into the manifold, refresh, emit rows; or drop the manifold.
+__device__ __forceinline__ void capture_one(const BodyDev& b, const Shape* __restrict__ shapes, const uint64_t* __restrict__ pairs,
+                                            const StepParams& sp, PairDataDev& pd, uint32_t p) {
+    uint64_t key = pairs[p];
+    uint32_t i = key_lo(key), j = key_hi(key);
+    float4* ne = pd.entries + size_t(p) * ENTRY_F4;
+    uint32_t n = pd.detect_n[p];
+    if (n == 0) {
+        store_meta_only(ne, 0u);
+        return;
+    }
+    Manifold m;
+    m.n = int(n);
+    const float4* d = pd.detect + size_t(p) * 8;
+    for (uint32_t k = 0; k < n; ++k) {
+        float4 a = d[2 * k], c = d[2 * k + 1];
+        m.pos[k] = from4(a); m.pen[k] = a.w; m.nrm[k] = from4(c);
+    }
+    uint4 ia = b.info[i], ib = b.info[j];
+    Entry E;
+    uint32_t meta = __float_as_uint(ne[2].w);
+    if (meta & META_VALID) {
+        E = load_entry(ne);
+    } else {
+        E.meta = 0;
+        E.thr = 0.02f;
+    }
+    V3 pa = from4(b.pred[i]), pb = from4(b.pred[j]);
+    Q qa = q4(b.quat[i]), qb = q4(b.quat[j]);
+    float thr = fminf(shapes[ia.x].cbt, shapes[ib.x].cbt);
+    capture(E, m, pa, qa, pb, qb, thr);
+    Out o;
+    refresh(E, pa, qa, pb, qb, o);
+    store_entry(ne, E);
+    if (((ia.y | ib.y) & BF_NO_RESPONSE) == 0) emit_rows(b, i, j, o, sp, pd.rows, pd.row_count, p);
+}
+
+__global__ void k_capture(BodyDev b, const Shape* __restrict__ shapes, const uint64_t* __restrict__ pairs,
+                          uint32_t npairs, StepParams sp, PairDataDev pd) {
+    uint32_t na = pd.scalars[0], nc = pd.scalars[1];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < na + nc; t += gridDim.x * blockDim.x) {
+        uint32_t p = t < na ? pd.route_list[t] : pd.route_list[npairs + (t - na)];
+        capture_one(b, shapes, pairs, sp, pd, p);
+    }
+}
+
+// Plane-plane pairs (route NP_NONE) detect nothing: their manifold (if any) is dropped.
+__global__ void k_drop_undetectable(uint32_t npairs, PairDataDev pd) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    if (pd.status[p] == (PS_DETECT | (NP_NONE << 8))) store_meta_only(pd.entries + size_t(p) * ENTRY_F4, 0u);
+}
+
+__global__ void k_collide_queries(const Shape* __restrict__ shapes, const float4* __restrict__ hull, uint32_t n,
+                                  const uint32_t* __restrict__ sai, const float4* __restrict__ pa4,
+                                  const float4* __restrict__ qa4, const uint32_t* __restrict__ sbi,
+                                  const float4* __restrict__ pb4, const float4* __restrict__ qb4,
+                                  const float4* __restrict__ seeds, int force_convex, float4* out, uint32_t* counts,
+                                  uint32_t* status) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    Shape sa = shapes[sai[t]], sb = shapes[sbi[t]];
+    V3 pa = from4(pa4[t]), pb = from4(pb4[t]);
+    Q qa = q4(qa4[t]), qb = q4(qb4[t]);
+    Manifold m;
+    m.n = 0;
+    uint32_t route = force_convex ? NP_CONVEX : route_of(sa.type, sb.type);
+    if (route == NP_CONVEX) {
+        EpaScratch scratch;
+        bool has_seed = seeds != nullptr;
+        V3 seed = has_seed ? from4(seeds[t]) : V3{0.f, 0.f, 0.f};
+        collide_convex(sa, pa, qa, sb, pb, qb, has_seed, seed, hull, scratch, m, status);
+    } else if (route != NP_NONE) {
+        collide_analytic(route, sa, pa, qa, sb, pb, qb, hull, m);
+    }
+    counts[t] = uint32_t(m.n);
+    for (int k = 0; k < m.n; ++k) {
+        out[(size_t(t) * 4 + k) * 2] = to4(m.pos[k], m.pen[k]);
+        out[(size_t(t) * 4 + k) * 2 + 1] = to4(m.nrm[k], 0.0f);
+    }
+}
+
+// Stand-alone row preparation: contacts (body_a, body_b, pos3, normal3, penetration,
+// impulse) grouped by consecutive body pairs; group g owns row slots [4g, 4g + n).
+__global__ void k_prepare_contacts(BodyDev b, uint32_t ngroups, const uint32_t* __restrict__ group_first,
+                                   const uint32_t* __restrict__ group_n, const float* __restrict__ contacts,
+                                   const uint64_t* __restrict__ group_keys, StepParams sp, float4* rows,
+                                   uint32_t* row_count) {
+    uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngroups) return;
+    uint64_t key = group_keys[g];
+    uint32_t i = key_lo(key), j = key_hi(key);
+    Out o;
+    o.n = int(group_n[g]);
+    for (int k = 0; k < o.n; ++k) {
+        const float* c = contacts + size_t(group_first[g] + k) * 10;
+        o.pos[k] = V3{c[2], c[3], c[4]};
+        o.nrm[k] = V3{c[5], c[6], c[7]};
+        o.pen[k] = c[8];
+        o.imp[k] = c[9];
+    }
+    // The caller's impulse is already the warm-start value: undo the factor emit_rows applies.
+    StepParams q = sp;
+    q.info.warmstarting_factor = 1.0f;
+    emit_rows(b, i, j, o, q, rows, row_count, g);
+}
+
+}  // namespace
+
+void run_pair_pass(const WorldView& w, const uint64_t* pairs, uint32_t npairs, const Manifolds& old_cache,
+                   PairData& pd, const StepParams& sp, const uint32_t* simulate_flag, uint32_t* status_dev,
+                   cudaStream_t s) {
+    (void)simulate_flag;
+    if (npairs == 0) return;
+    PairDataDev d = pd.dev();
+    check_cuda(cudaMemsetAsync(pd.scalars.p, 0, 8 * sizeof(uint32_t), s), "memset scalars");
+    const int TB = 128;
+    k_classify<<<(npairs + TB - 1) / TB, TB, 0, s>>>(w.b, w.shapes, pairs, npairs, old_cache.keys.p,
+                                                     old_cache.entries.p, old_cache.count_dev, sp, d);
+    k_drop_undetectable<<<(npairs + 255) / 256, 256, 0, s>>>(npairs, d);
+    uint32_t grid = std::min<uint32_t>((npairs + TB - 1) / TB, 148u * 16u);
+    k_narrow_analytic<<<grid, TB, 0, s>>>(w.b, w.shapes, w.hull, pairs, d);
+    uint32_t cgrid = std::min<uint32_t>((npairs + 63) / 64, 148u * 8u);
+    k_narrow_convex<<<cgrid, 64, 0, s>>>(w.b, w.shapes, w.hull, pairs, npairs, d, status_dev);
+    k_capture<<<grid, TB, 0, s>>>(w.b, w.shapes, pairs, npairs, sp, d);
+}
+
+void run_collide_queries(const Shape* shapes, const float4* hull, uint32_t n, const uint32_t* sa, const float4* pa,
+                         const float4* qa, const uint32_t* sb, const float4* pb, const float4* qb, const float4* seeds,
+                         int force_convex, float4* out, uint32_t* counts, uint32_t* status_dev, cudaStream_t s) {
+    if (n == 0) return;
+    k_collide_queries<<<(n + 63) / 64, 64, 0, s>>>(shapes, hull, n, sa, pa, qa, sb, pb, qb, seeds, force_convex, out,
+                                                   counts, status_dev);
+}
+
+}  // namespace bgpu
+
+namespace bgpu {
+void run_prepare_contacts(const BodyDev& b, uint32_t ngroups, const uint32_t* group_first, const uint32_t* group_n,
+                          const float* contacts, const uint64_t* group_keys, const StepParams& sp, float4* rows,
+                          uint32_t* row_count, cudaStream_t s) {
+    if (ngroups == 0) return;
+    k_prepare_contacts<<<(ngroups + 127) / 128, 128, 0, s>>>(b, ngroups, group_first, group_n, contacts, group_keys, sp,
+                                                             rows, row_count);
+}
+}  // namespace bgpu

@@ -1,0 +1,566 @@
+// Sequential-impulse (PGS) solve over graph-coloured row groups, and the
+// post-solve manifold writeback / lifecycle prune.
+//
+// The reference solves rows one by one in pair order (solver/
+// sequential_impulse.rs:692-735, 743-802). Here the row group of each pair
+// (its <= 4 contacts, solved in order by one thread) is a graph vertex; two
+// groups conflict when they share a body with nonzero inverse mass. A
+// Jones-Plassmann colouring with first-fit colour choice splits the groups
+// into batches of pairwise-independent groups; a persistent cooperative
+// kernel sweeps the batches in colour order with a grid barrier between
+// batches. Within a batch no dynamic body is touched twice, so the result is
+// bit-identical to the reference's sequential solve over the same rows taken
+// in (colour, pair) order.
+//
+// Rows store only the contact frame (normal, lever arms), the bias terms, the
+// effective masses and the accumulated impulses; the tangent basis, the
+// angular components Iw^-1 (r x d) and the velocity couplings are recomputed
+// from the per-body world inverse inertia with the reference's arithmetic, so
+// they equal the values the reference precomputes in prepare().
+#include <cooperative_groups.h>
+#include <cub/cub.cuh>
+#include "bgpu_kernels.cuh"
+
+namespace bgpu {
+
+namespace {
+
+constexpr uint32_t NO_COLOUR = 0xffffffffu;
+constexpr int MAX_COLOURS = 128;
+constexpr int MAX_ROUNDS = 1024;
+constexpr unsigned int BARRIER_SPIN_LIMIT = 1u << 26;
+
+// Grid-wide barrier for a cooperative launch (all blocks co-resident). The
+// spin is bounded: on timeout the status word records it and the kernel
+// continues, so no launch can hang the device.
+__device__ __forceinline__ void grid_barrier(unsigned int* bar, unsigned int nblocks, uint32_t* status) {
+    __syncthreads();
+    // After one timeout every later barrier returns at once, so a broken launch ends quickly.
+    if (threadIdx.x == 0 && !(*(volatile uint32_t*)status & ST_BARRIER_TIMEOUT)) {
+        volatile unsigned int* vgen = bar + 1;
+        unsigned int gen = *vgen;
+        __threadfence();
+        unsigned int arrived = atomicAdd(&bar[0], 1u);
+        if (arrived == nblocks - 1) {
+            atomicExch(&bar[0], 0u);
+            __threadfence();
+            atomicAdd(&bar[1], 1u);
+        } else {
+            unsigned int spins = 0;
+            while (*vgen == gen) {
+                __nanosleep(64);
+                if (++spins > BARRIER_SPIN_LIMIT) {
+                    atomicOr(status, ST_BARRIER_TIMEOUT);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t mix32(uint64_t k) {
+    uint32_t h = uint32_t(k) ^ uint32_t(k >> 32) * 0x9E3779B1u;
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= 0xC2B2AE35u;
+    h ^= h >> 16;
+    return h;
+}
+
+__device__ __forceinline__ float inv_mass_of(const float4* __restrict__ iw, uint32_t i) { return iw[3 * i + 2].y; }
+
+__device__ __forceinline__ M3 load_iw(const float4* __restrict__ iw, uint32_t i, float& inv_mass) {
+    float4 a = __ldg(&iw[3 * i]), b = __ldg(&iw[3 * i + 1]), c = __ldg(&iw[3 * i + 2]);
+    inv_mass = c.y;
+    return M3{V3{a.x, a.y, a.z}, V3{a.w, b.x, b.y}, V3{b.z, b.w, c.x}};
+}
+
+__global__ void k_flag_contact_pairs(uint32_t npairs, const uint32_t* __restrict__ row_count, uint32_t* flags) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < npairs) flags[p] = row_count[p] > 0 ? 1u : 0u;
+}
+
+struct ColourArgs {
+    const uint32_t* count;  // number of contact pairs
+    const uint32_t* contact_pairs;
+    const uint64_t* pairs;
+    const float4* iw;
+    uint32_t* colour;
+    unsigned long long* prio;
+    unsigned long long* mask;
+    unsigned int* bar;  // [0..1] barrier, [2..4] round counters, [5] colour max
+    uint32_t* status;
+};
+
+// Jones-Plassmann rounds: an uncoloured group wins when its priority is the
+// maximum over the uncoloured groups at both of its dynamic bodies; winners
+// take the lowest colour free at both bodies.
+__global__ void k_colour(ColourArgs a) {
+    const uint32_t K = *a.count;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const unsigned int nblocks = gridDim.x;
+    for (uint32_t k = tid; k < K; k += stride) {
+        a.colour[k] = NO_COLOUR;
+        uint64_t key = a.pairs[a.contact_pairs[k]];
+        uint32_t u = key_lo(key), v = key_hi(key);
+        a.mask[2 * u] = 0ull; a.mask[2 * u + 1] = 0ull;
+        a.mask[2 * v] = 0ull; a.mask[2 * v + 1] = 0ull;
+    }
+    if (tid == 0) { a.bar[2] = 0; a.bar[3] = 0; a.bar[4] = 0; a.bar[5] = 0; }
+    grid_barrier(a.bar, nblocks, a.status);
+    int round = 0;
+    for (; round < MAX_ROUNDS; ++round) {
+        // phase 0: clear the bids of the uncoloured groups' bodies
+        for (uint32_t k = tid; k < K; k += stride) {
+            if (a.colour[k] != NO_COLOUR) continue;
+            uint64_t key = a.pairs[a.contact_pairs[k]];
+            a.prio[key_lo(key)] = 0ull;
+            a.prio[key_hi(key)] = 0ull;
+        }
+        grid_barrier(a.bar, nblocks, a.status);
+        // phase 1: bid (and recycle the counter of round r-1)
+        if (tid == 0) a.bar[2 + (round + 2) % 3] = 0;
+        for (uint32_t k = tid; k < K; k += stride) {
+            if (__ldcg(&a.colour[k]) != NO_COLOUR) continue;
+            uint64_t key = a.pairs[a.contact_pairs[k]];
+            uint32_t u = key_lo(key), v = key_hi(key);
+            unsigned long long pr = (uint64_t(mix32(key)) << 32) | k;
+            if (inv_mass_of(a.iw, u) > 0.0f) atomicMax(&a.prio[u], pr);
+            if (inv_mass_of(a.iw, v) > 0.0f) atomicMax(&a.prio[v], pr);
+        }
+        grid_barrier(a.bar, nblocks, a.status);
+        // phase 2: winners pick a colour
+        for (uint32_t k = tid; k < K; k += stride) {
+            if (__ldcg(&a.colour[k]) != NO_COLOUR) continue;
+            uint64_t key = a.pairs[a.contact_pairs[k]];
+            uint32_t u = key_lo(key), v = key_hi(key);
+            unsigned long long pr = (uint64_t(mix32(key)) << 32) | k;
+            bool du = inv_mass_of(a.iw, u) > 0.0f, dv = inv_mass_of(a.iw, v) > 0.0f;
+            bool win = (!du || __ldcg(&a.prio[u]) == pr) && (!dv || __ldcg(&a.prio[v]) == pr);
+            if (!win) {
+                atomicAdd(&a.bar[2 + round % 3], 1u);
+                continue;
+            }
+            unsigned long long m0 = 0, m1 = 0;
+            if (du) { m0 |= __ldcg(&a.mask[2 * u]); m1 |= __ldcg(&a.mask[2 * u + 1]); }
+            if (dv) { m0 |= __ldcg(&a.mask[2 * v]); m1 |= __ldcg(&a.mask[2 * v + 1]); }
+            uint32_t c;
+            if (~m0) c = uint32_t(__ffsll((long long)~m0) - 1);
+            else if (~m1) c = 64u + uint32_t(__ffsll((long long)~m1) - 1);
+            else { c = MAX_COLOURS - 1; atomicOr(a.status, ST_COLOUR_OVERFLOW); }
+            a.colour[k] = c;
+            unsigned long long b0 = c < 64 ? (1ull << c) : 0ull, b1 = c >= 64 ? (1ull << (c - 64)) : 0ull;
+            if (du) { a.mask[2 * u] |= b0; a.mask[2 * u + 1] |= b1; }
+            if (dv) { a.mask[2 * v] |= b0; a.mask[2 * v + 1] |= b1; }
+            atomicMax(&a.bar[5], c + 1);
+        }
+        grid_barrier(a.bar, nblocks, a.status);
+        volatile unsigned int* vb = a.bar;
+        if (vb[2 + round % 3] == 0) break;
+        if (*(volatile uint32_t*)a.status & ST_BARRIER_TIMEOUT) break;
+    }
+    if (round >= MAX_ROUNDS && tid == 0) atomicOr(a.status, ST_COLOUR_ROUNDS);
+}
+
+__global__ void k_zero_u32(uint32_t n, uint32_t* a) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = 0;
+}
+
+// Colour histograms of all groups and of the groups with split-active rows.
+__global__ void k_colour_hist(const uint32_t* __restrict__ count, const uint32_t* __restrict__ contact_pairs,
+                              const uint32_t* __restrict__ colour, const uint32_t* __restrict__ row_count,
+                              const float4* __restrict__ rows, uint32_t* hist, uint32_t* split_hist, uint32_t* split_flag) {
+    uint32_t K = *count;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        uint32_t c = colour[k];
+        atomicAdd(&hist[c], 1u);
+        uint32_t p = contact_pairs[k];
+        uint32_t n = row_count[p];
+        atomicAdd(&hist[MAX_COLOURS + 1], n);
+        bool split = false;
+        for (uint32_t r = 0; r < n; ++r) split |= rows[(size_t(p) * 4 + r) * ROW_F4 + 5].z != 0.0f;
+        split_flag[k] = split ? 1u : 0u;
+        if (split) atomicAdd(&split_hist[c], 1u);
+    }
+}
+
+__global__ void k_colour_scan(uint32_t* hist, uint32_t* offset, uint32_t* cursor, uint32_t* split_hist,
+                              uint32_t* split_offset, uint32_t* split_cursor, const unsigned int* bar, uint32_t* scalars) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t ncol = bar[5];
+    uint32_t acc = 0, sacc = 0;
+    for (uint32_t c = 0; c < ncol; ++c) {
+        offset[c] = acc;
+        cursor[c] = acc;
+        acc += hist[c];
+        split_offset[c] = sacc;
+        split_cursor[c] = sacc;
+        sacc += split_hist[c];
+    }
+    offset[ncol] = acc;
+    split_offset[ncol] = sacc;
+    scalars[3] = hist[MAX_COLOURS + 1];
+    scalars[4] = ncol;
+    scalars[5] = sacc;
+}
+
+__global__ void k_colour_scatter(const uint32_t* __restrict__ count, const uint32_t* __restrict__ contact_pairs,
+                                 const uint32_t* __restrict__ colour, const uint32_t* __restrict__ split_flag,
+                                 uint32_t* cursor, uint32_t* split_cursor, uint32_t* batch, uint32_t* split_batch) {
+    uint32_t K = *count;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        uint32_t c = colour[k];
+        uint32_t p = contact_pairs[k];
+        batch[atomicAdd(&cursor[c], 1u)] = p;
+        if (split_flag[k]) split_batch[atomicAdd(&split_cursor[c], 1u)] = p;
+    }
+}
+
+struct SolveArgs {
+    const uint64_t* pairs;
+    const uint32_t* row_count;
+    float4* rows;
+    const uint32_t* batch;
+    const uint32_t* offset;
+    const uint32_t* split_batch;
+    const uint32_t* split_offset;
+    const uint32_t* scalars;  // [4] colours [5] split groups
+    float4* linvel;
+    float4* angvel;
+    float4* push_lin;
+    float4* push_ang;
+    const float4* iw;
+    unsigned int* bar;
+    uint32_t* status;
+    float inv_dt;
+    float restitution_threshold;
+    uint32_t iterations;
+};
+
+__device__ __forceinline__ void apply(V3& la, V3& wa, V3& lb, V3& wb, bool appa, bool appb, float ima, float imb, V3 d,
+                                      V3 ca, V3 cb, float j) {
+    if (appa) { la -= d * (j * ima); wa -= ca * j; }
+    if (appb) { lb += d * (j * imb); wb += cb * j; }
+}
+
+enum Phase { WARM = 0, ITER = 1 };
+
+// warm_start (sequential_impulse.rs:710-717) or one solve_contact sweep (:804-930) over a group.
+template <int PHASE>
+__device__ __forceinline__ void solve_group(const SolveArgs& a, uint32_t p) {
+    uint64_t key = a.pairs[p];
+    uint32_t ia = key_lo(key), ib = key_hi(key);
+    uint32_t cnt = a.row_count[p];
+    float ima, imb;
+    M3 iwa = load_iw(a.iw, ia, ima);
+    M3 iwb = load_iw(a.iw, ib, imb);
+    bool appa = ima > 0.0f, appb = imb > 0.0f;
+    V3 la = from4(__ldcg(&a.linvel[ia])), wa = from4(__ldcg(&a.angvel[ia]));
+    V3 lb = from4(__ldcg(&a.linvel[ib])), wb = from4(__ldcg(&a.angvel[ib]));
+    for (uint32_t k = 0; k < cnt; ++k) {
+        float4* r = a.rows + (size_t(p) * 4 + k) * ROW_F4;
+        float4 r0 = r[0], r1 = r[1], r2 = r[2];
+        float4 r3 = __ldcg(&r[3]);
+        V3 n = from4(r0), ra = from4(r1), rb = from4(r2);
+        V3 t1, t2;
+        tangent_basis_dev(n, t1, t2);
+        V3 ana = mul(iwa, cross(ra, n)), anb = mul(iwb, cross(rb, n));
+        V3 a1a = mul(iwa, cross(ra, t1)), a1b = mul(iwb, cross(rb, t1));
+        V3 a2a = mul(iwa, cross(ra, t2)), a2b = mul(iwb, cross(rb, t2));
+        if (PHASE == WARM) {
+            apply(la, wa, lb, wb, appa, appb, ima, imb, n, ana, anb, r3.x);
+            apply(la, wa, lb, wb, appa, appb, ima, imb, t1, a1a, a1b, r3.y);
+            apply(la, wa, lb, wb, appa, appb, ima, imb, t2, a2a, a2b, r3.z);
+            continue;
+        }
+        float4 r4 = r[4];
+        float ims = ima + imb;
+        V3 kn = n * ims + cross(anb, rb) + cross(ana, ra);
+        V3 kt1 = t1 * ims + cross(a1b, rb) + cross(a1a, ra);
+        V3 kt2 = t2 * ims + cross(a2b, rb) + cross(a2a, ra);
+        V3 va = la + cross(wa, ra);
+        V3 vb = lb + cross(wb, rb);
+        V3 rel = vb - va;
+        float vn = dot(rel, n);
+        float bias = 0.0f;
+        if (vn < -a.restitution_threshold) bias = -r3.w * vn;
+        if (r1.w != 0.0f) bias += r1.w;
+        if (r2.w != 0.0f) bias += r2.w;
+        float lambda = r4.w != 0.0f ? r4.x * (bias - vn) - r4.w * r3.x : r4.x * (bias - vn);
+        float old = r3.x;
+        float nimp = fmaxf(old + lambda, 0.0f);
+        float jn = nimp - old;
+        apply(la, wa, lb, wb, appa, appb, ima, imb, n, ana, anb, jn);
+        rel += kn * jn;
+        float maxf = r0.w * nimp;
+        float vt = dot(rel, t1);
+        float lam = -r4.y * (vt - 0.0f * a.inv_dt);
+        float o1 = r3.y;
+        float n1 = fminf(fmaxf(o1 + lam, -maxf), maxf);
+        float j1 = n1 - o1;
+        apply(la, wa, lb, wb, appa, appb, ima, imb, t1, a1a, a1b, j1);
+        rel += kt1 * j1;
+        vt = dot(rel, t2);
+        lam = -r4.z * (vt - 0.0f * a.inv_dt);
+        float o2 = r3.z;
+        float n2 = fminf(fmaxf(o2 + lam, -maxf), maxf);
+        float j2 = n2 - o2;
+        apply(la, wa, lb, wb, appa, appb, ima, imb, t2, a2a, a2b, j2);
+        __stcg(&r[3], make_float4(nimp, n1, n2, r3.w));
+    }
+    if (appa) { __stcg(&a.linvel[ia], to4(la, 0.0f)); __stcg(&a.angvel[ia], to4(wa, 0.0f)); }
+    if (appb) { __stcg(&a.linvel[ib], to4(lb, 0.0f)); __stcg(&a.angvel[ib], to4(wb, 0.0f)); }
+}
+
+// split_impulse_pass body (sequential_impulse.rs:759-786) for one group.
+__device__ __forceinline__ void split_group(const SolveArgs& a, uint32_t p) {
+    uint64_t key = a.pairs[p];
+    uint32_t ia = key_lo(key), ib = key_hi(key);
+    uint32_t cnt = a.row_count[p];
+    float ima, imb;
+    M3 iwa = load_iw(a.iw, ia, ima);
+    M3 iwb = load_iw(a.iw, ib, imb);
+    bool appa = ima > 0.0f, appb = imb > 0.0f;
+    V3 pla = from4(__ldcg(&a.push_lin[ia])), pwa = from4(__ldcg(&a.push_ang[ia]));
+    V3 plb = from4(__ldcg(&a.push_lin[ib])), pwb = from4(__ldcg(&a.push_ang[ib]));
+    for (uint32_t k = 0; k < cnt; ++k) {
+        float4* r = a.rows + (size_t(p) * 4 + k) * ROW_F4;
+        float4 r5 = __ldcg(&r[5]);
+        if (r5.z == 0.0f) continue;
+        float4 r0 = r[0], r1 = r[1], r2 = r[2], r4 = r[4];
+        V3 n = from4(r0), ra = from4(r1), rb = from4(r2);
+        V3 pva = pla + cross(pwa, ra);
+        V3 pvb = plb + cross(pwb, rb);
+        float pvn = dot(pvb - pva, n);
+        float delta = r4.w != 0.0f ? r5.x - pvn * r4.x - r4.w * r5.y : r5.x - pvn * r4.x;
+        float old = r5.y;
+        float np = fmaxf(old + delta, 0.0f);
+        float j = np - old;
+        if (j != 0.0f) {
+            V3 ana = mul(iwa, cross(ra, n)), anb = mul(iwb, cross(rb, n));
+            if (appa) { pla -= n * (j * ima); pwa -= ana * j; }
+            if (appb) { plb += n * (j * imb); pwb += anb * j; }
+        }
+        __stcg(&r[5], make_float4(r5.x, np, r5.z, r5.w));
+    }
+    if (appa) { __stcg(&a.push_lin[ia], to4(pla, 0.0f)); __stcg(&a.push_ang[ia], to4(pwa, 0.0f)); }
+    if (appb) { __stcg(&a.push_lin[ib], to4(plb, 0.0f)); __stcg(&a.push_ang[ib], to4(pwb, 0.0f)); }
+}
+
+// solve() (sequential_impulse.rs:692-705): warm start, the velocity sweeps, the split sweeps.
+__global__ void k_solve(SolveArgs a) {
+    const uint32_t ncol = a.scalars[4];
+    const uint32_t nsplit = a.scalars[5];
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const unsigned int nb = gridDim.x;
+    for (uint32_t c = 0; c < ncol; ++c) {
+        for (uint32_t t = a.offset[c] + tid; t < a.offset[c + 1]; t += stride) solve_group<WARM>(a, a.batch[t]);
+        grid_barrier(a.bar, nb, a.status);
+    }
+    for (uint32_t it = 0; it < a.iterations; ++it) {
+        for (uint32_t c = 0; c < ncol; ++c) {
+            for (uint32_t t = a.offset[c] + tid; t < a.offset[c + 1]; t += stride) solve_group<ITER>(a, a.batch[t]);
+            grid_barrier(a.bar, nb, a.status);
+        }
+    }
+    if (nsplit == 0) return;
+    for (uint32_t it = 0; it < a.iterations; ++it) {
+        for (uint32_t c = 0; c < ncol; ++c) {
+            for (uint32_t t = a.split_offset[c] + tid; t < a.split_offset[c + 1]; t += stride)
+                split_group(a, a.split_batch[t]);
+            grid_barrier(a.bar, nb, a.status);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- cache update
+// step.rs:982-1005: the solved normal impulse goes back to its manifold point.
+__global__ void k_writeback(uint32_t npairs, const uint32_t* __restrict__ row_count, const float4* __restrict__ rows,
+                            float4* entries, uint32_t* valid_flags) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    float4* e = entries + size_t(p) * ENTRY_F4;
+    uint32_t n = row_count[p];
+    for (uint32_t k = 0; k < n; ++k) {
+        float imp = rows[(size_t(p) * 4 + k) * ROW_F4 + 3].x;
+        float4 y = e[5 + 3 * k];
+        y.w = imp;
+        e[5 + 3 * k] = y;
+    }
+    valid_flags[p] = (__float_as_uint(e[2].w) & META_VALID) ? 1u : 0u;
+}
+
+// step.rs:1006-1010: with prune = simulate && prev_simulate, manifolds whose pair vanished die;
+// otherwise the unowned old manifolds survive.
+__global__ void k_flag_unowned(uint32_t nold, const uint32_t* __restrict__ owned, const uint32_t* __restrict__ simulate,
+                               const uint32_t* __restrict__ prev_simulate, uint32_t* flags) {
+    uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nold) return;
+    bool prune = (*simulate != 0) && (*prev_simulate != 0);
+    flags[o] = (!prune && !owned[o]) ? 1u : 0u;
+}
+
+__device__ __forceinline__ uint32_t lower_bound_pairs(const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ sel,
+                                                      uint32_t n, uint64_t key) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (pairs[sel[mid]] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint32_t lower_bound_keys(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ sel,
+                                                     uint32_t n, uint64_t key) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (keys[sel[mid]] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Merge the surviving current manifolds (A, pair order) with the surviving old ones (B, key order).
+__global__ void k_merge(const uint64_t* __restrict__ pairs, const float4* __restrict__ cur_entries,
+                        const uint32_t* __restrict__ sel_a, const uint32_t* __restrict__ na_ptr,
+                        const uint64_t* __restrict__ old_keys, const float4* __restrict__ old_entries,
+                        const uint32_t* __restrict__ sel_b, const uint32_t* __restrict__ nb_ptr, uint64_t* out_keys,
+                        float4* out_entries, uint32_t* out_count) {
+    uint32_t na = *na_ptr, nb = *nb_ptr;
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) *out_count = na + nb;
+    if (t < na) {
+        uint32_t p = sel_a[t];
+        uint64_t key = pairs[p];
+        uint32_t pos = t + (nb ? lower_bound_keys(old_keys, sel_b, nb, key) : 0u);
+        out_keys[pos] = key;
+        const float4* src = cur_entries + size_t(p) * ENTRY_F4;
+        float4* dst = out_entries + size_t(pos) * ENTRY_F4;
+        for (int q = 0; q < ENTRY_F4; ++q) dst[q] = src[q];
+    } else if (t < na + nb) {
+        uint32_t b = t - na;
+        uint32_t o = sel_b[b];
+        uint64_t key = old_keys[o];
+        uint32_t pos = b + lower_bound_pairs(pairs, sel_a, na, key);
+        out_keys[pos] = key;
+        const float4* src = old_entries + size_t(o) * ENTRY_F4;
+        float4* dst = out_entries + size_t(pos) * ENTRY_F4;
+        for (int q = 0; q < ENTRY_F4; ++q) dst[q] = src[q];
+    }
+}
+
+int coop_grid(const void* fn, int block, size_t smem) {
+    static int sms = -1;
+    if (sms < 0) {
+        int dev = 0;
+        check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+        check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "sm count");
+    }
+    int per_sm = 0;
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem), "occupancy");
+    if (per_sm < 1) per_sm = 1;
+    return sms * per_sm;
+}
+
+}  // namespace
+
+void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
+                uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark) {
+    if (npairs == 0) {
+        check_cuda(cudaMemsetAsync(pd.scalars.p + 2, 0, 4 * sizeof(uint32_t), s), "memset");
+        mark(5);
+        mark(6);
+        return;
+    }
+    const int TB = 256;
+    // Contact pairs (ascending pair order).
+    k_flag_contact_pairs<<<(npairs + TB - 1) / TB, TB, 0, s>>>(npairs, pd.row_count.p, pd.flags.p);
+    size_t bytes = 0;
+    cub::CountingInputIterator<uint32_t> it(0);
+    check_cuda(cub::DeviceSelect::Flagged(nullptr, bytes, it, pd.flags.p, pd.contact_pairs.p, pd.scalars.p + 2,
+                                          int(npairs), s), "select size");
+    pd.cub_tmp.reserve(bytes);
+    check_cuda(cub::DeviceSelect::Flagged(pd.cub_tmp.p, bytes, it, pd.flags.p, pd.contact_pairs.p, pd.scalars.p + 2,
+                                          int(npairs), s), "select");
+    // Colouring (cooperative launch).
+    check_cuda(cudaMemsetAsync(pd.barrier.p, 0, 16 * sizeof(unsigned int), s), "memset barrier");
+    ColourArgs ca{pd.scalars.p + 2, pd.contact_pairs.p, pairs, w.b.iw, pd.colour.p, pd.body_prio.p, pd.body_mask.p,
+                  pd.barrier.p, status_dev};
+    static int colour_grid = 0;
+    if (!colour_grid) colour_grid = coop_grid((const void*)k_colour, TB, 0);
+    void* cargs[] = {&ca};
+    check_cuda(cudaLaunchCooperativeKernel((const void*)k_colour, dim3(colour_grid), dim3(TB), cargs, 0, s),
+               "colour launch");
+    // Batches.
+    check_cuda(cudaMemsetAsync(pd.colour_count.p, 0, 130 * sizeof(uint32_t), s), "memset");
+    check_cuda(cudaMemsetAsync(pd.split_count.p, 0, 130 * sizeof(uint32_t), s), "memset");
+    uint32_t g = std::min<uint32_t>((npairs + TB - 1) / TB, 148u * 8u);
+    k_colour_hist<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pd.colour.p, pd.row_count.p, pd.rows.p,
+                                   pd.colour_count.p, pd.split_count.p, pd.flags.p);
+    k_colour_scan<<<1, 32, 0, s>>>(pd.colour_count.p, pd.colour_offset.p, pd.colour_cursor.p, pd.split_count.p,
+                                   pd.split_offset.p, pd.split_cursor.p, pd.barrier.p, pd.scalars.p);
+    k_colour_scatter<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pd.colour.p, pd.flags.p, pd.colour_cursor.p,
+                                      pd.split_cursor.p, pd.batch.p, pd.split_batch.p);
+    // PGS (cooperative launch).
+    check_cuda(cudaMemsetAsync(pd.barrier.p, 0, 2 * sizeof(unsigned int), s), "memset barrier");
+    mark(5);
+    SolveArgs sa{pairs, pd.row_count.p, pd.rows.p, pd.batch.p, pd.colour_offset.p, pd.split_batch.p, pd.split_offset.p,
+                 pd.scalars.p, w.b.linvel, w.b.angvel, w.b.push_lin, w.b.push_ang, w.b.iw, pd.barrier.p, status_dev,
+                 sp.inv_dt, sp.info.restitution_velocity_threshold, sp.info.num_iterations};
+    static int solve_grid = 0;
+    if (!solve_grid) solve_grid = coop_grid((const void*)k_solve, TB, 0);
+    void* sargs[] = {&sa};
+    check_cuda(cudaLaunchCooperativeKernel((const void*)k_solve, dim3(solve_grid), dim3(TB), sargs, 0, s),
+               "solve launch");
+    mark(6);
+}
+
+void run_cache_update(const uint64_t* pairs, uint32_t npairs, const Manifolds& old_cache, PairData& pd,
+                      Manifolds& next, const uint32_t* simulate_flag, const uint32_t* prev_simulate, cudaStream_t s) {
+    const int TB = 256;
+    uint32_t nold_cap = old_cache.count_host;
+    // A: surviving manifolds of the current pairs.
+    if (npairs) k_writeback<<<(npairs + TB - 1) / TB, TB, 0, s>>>(npairs, pd.row_count.p, pd.rows.p, pd.entries.p,
+                                                                  pd.flags.p);
+    cub::CountingInputIterator<uint32_t> it(0);
+    size_t bytes_a = 0, bytes_b = 0;
+    uint32_t* na_dev = pd.scalars.p + 8;
+    uint32_t* nb_dev = pd.scalars.p + 9;
+    check_cuda(cudaMemsetAsync(na_dev, 0, 2 * sizeof(uint32_t), s), "memset");
+    if (npairs)
+        check_cuda(cub::DeviceSelect::Flagged(nullptr, bytes_a, it, pd.flags.p, pd.sel_a.p, na_dev, int(npairs), s), "sel");
+    if (nold_cap)
+        check_cuda(cub::DeviceSelect::Flagged(nullptr, bytes_b, it, pd.flags.p, pd.sel_b.p, nb_dev, int(nold_cap), s), "sel");
+    pd.cub_tmp.reserve(std::max(bytes_a, bytes_b));
+    if (npairs)
+        check_cuda(cub::DeviceSelect::Flagged(pd.cub_tmp.p, bytes_a, it, pd.flags.p, pd.sel_a.p, na_dev, int(npairs), s),
+                   "sel");
+    // B: unowned old manifolds (only kept when this step does not prune).
+    if (nold_cap) {
+        // nold_cap is the exact old count: the world syncs on it before the step.
+        k_flag_unowned<<<(nold_cap + TB - 1) / TB, TB, 0, s>>>(nold_cap, pd.old_owned.p, simulate_flag, prev_simulate,
+                                                                pd.flags.p);
+        check_cuda(cub::DeviceSelect::Flagged(pd.cub_tmp.p, bytes_b, it, pd.flags.p, pd.sel_b.p, nb_dev, int(nold_cap), s),
+                   "sel");
+    }
+    size_t cap = size_t(npairs) + nold_cap + 1;
+    next.keys.reserve(cap);
+    next.entries.reserve(cap * ENTRY_F4);
+    uint32_t total = npairs + nold_cap;
+    if (total)
+        k_merge<<<(total + TB - 1) / TB, TB, 0, s>>>(pairs, pd.entries.p, pd.sel_a.p, na_dev, old_cache.keys.p,
+                                                      old_cache.entries.p, pd.sel_b.p, nb_dev, next.keys.p,
+                                                      next.entries.p, next.count_dev);
+    else
+        check_cuda(cudaMemsetAsync(next.count_dev, 0, sizeof(uint32_t), s), "memset");
+}
+
+}  // namespace bgpu

@@ -1,0 +1,1094 @@
+// Host side of the rigid-body world: device memory ownership, the step
+// orchestration (step.rs:281-1287 order: integrate velocities + AABBs, broad
+// phase, islands, pair pass, solve, manifold writeback/prune, integrate
+// positions), and the C ABI declared in include/bgpu.h.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/bgpu.h"
+#include "bgpu_kernels.cuh"
+
+namespace bgpu {
+
+void check_cuda(cudaError_t e, const char* where) {
+    if (e != cudaSuccess) throw CudaError{e, std::string(where) + ": " + cudaGetErrorString(e)};
+}
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct InvalidArg {
+    std::string what;
+};
+
+const float CONTACT_BREAKING_THRESHOLD = 0.02f;  // manifold.rs:8
+
+// shapes/mod.rs:388-392 (float arithmetic, host)
+float contact_breaking_threshold(const float lmin[3], const float lmax[3]) {
+    float dx = lmax[0] - lmin[0], dy = lmax[1] - lmin[1], dz = lmax[2] - lmin[2];
+    float len = std::sqrt(dx * dx + dy * dy + dz * dz);
+    float cx = (lmin[0] + lmax[0]) * 0.5f, cy = (lmin[1] + lmax[1]) * 0.5f, cz = (lmin[2] + lmax[2]) * 0.5f;
+    float clen = std::sqrt(cx * cx + cy * cy + cz * cz);
+    float disc = len * 0.5f + clen;
+    return disc * CONTACT_BREAKING_THRESHOLD;
+}
+
+// Diagonal local inertia (shapes/mod.rs:396-412), float host arithmetic.
+void local_inertia(const Shape& s, float mass, float out[3]) {
+    switch (s.type) {
+        case SHAPE_SPHERE: {
+            float v = 0.4f * mass * s.p0 * s.p0;
+            out[0] = out[1] = out[2] = v;
+            return;
+        }
+        case SHAPE_BOX: {
+            float m = mass / 3.0f;
+            out[0] = m * (s.p1 * s.p1 + s.p2 * s.p2);
+            out[1] = m * (s.p0 * s.p0 + s.p2 * s.p2);
+            out[2] = m * (s.p0 * s.p0 + s.p1 * s.p1);
+            return;
+        }
+        case SHAPE_CAPSULE: {
+            const float PI = 3.14159265358979323846f;
+            float h = 2.0f * s.p1;
+            float r2 = s.p0 * s.p0;
+            float h2 = h * h;
+            float v_cyl = PI * r2 * h;
+            float v_sph = 4.0f / 3.0f * PI * r2 * s.p0;
+            float v = v_cyl + v_sph;
+            float m_cyl = mass * v_cyl / v;
+            float m_sph = mass * v_sph / v;
+            float ixx = m_cyl * (3.0f * r2 + h2) / 12.0f + m_sph * (0.4f * r2 + 0.25f * h2);
+            float iyy = m_cyl * r2 / 2.0f + m_sph * 0.4f * r2;
+            out[0] = ixx; out[1] = iyy; out[2] = ixx;
+            return;
+        }
+        case SHAPE_HULL: {
+            float hx = (s.lmax[0] - s.lmin[0]) * 0.5f, hy = (s.lmax[1] - s.lmin[1]) * 0.5f,
+                  hz = (s.lmax[2] - s.lmin[2]) * 0.5f;
+            float m = mass / 3.0f;
+            out[0] = m * (hy * hy + hz * hz);
+            out[1] = m * (hx * hx + hz * hz);
+            out[2] = m * (hx * hx + hy * hy);
+            return;
+        }
+        default:
+            out[0] = out[1] = out[2] = 0.0f;
+    }
+}
+
+struct HostStats {  // pinned, written by async copies at the end of a step
+    uint32_t scalars[16];
+    uint32_t status;
+    uint32_t cache_count;
+    uint32_t simulate;
+};
+
+}  // namespace
+
+struct World {
+    cudaStream_t stream = nullptr;
+    SolverParams info{};
+    float gravity[3] = {0.0f, -9.81f, 0.0f};
+    // shapes
+    std::vector<Shape> shapes_h;
+    std::vector<float4> hull_h;
+    DevBuf<Shape> shapes_d;
+    DevBuf<float4> hull_d;
+    bool shapes_dirty = false;
+    // bodies
+    uint32_t n = 0, cap = 0;
+    DevBuf<float4> pos, quat, linvel, angvel, inv_inertia, grav, force, torque, material, sleep, aabb_min, aabb_max,
+        pred, iw, push_lin, push_ang;
+    DevBuf<uint4> info_d;
+    DevBuf<float> settled;
+    std::vector<uint32_t> unbounded;  // plane bodies (kept out of the BVH)
+    // step machinery
+    Broadphase bp;
+    Islands islands;
+    PairData pd;
+    Manifolds cache[2];
+    int cur = 0;
+    DevBuf<uint64_t> pairs;
+    uint32_t npairs = 0;
+    DevBuf<uint32_t> flags;  // [0] status, [1] simulate, [2] prev_simulate
+    HostStats* hs = nullptr;
+    bool timing = false;
+    cudaEvent_t ev[2][10] = {};  // two event sets: the step being enqueued and the previous one
+    int ev_cur = 0;
+    bool ev_pending[2] = {false, false};
+    bgpu_step_stats last{};
+    bool stats_pending = false;
+    float accumulator = 0.0f;  // step_simulation_fixed's m_localTime
+    int solved_standalone = 0;  // 1 after bgpu_solve_contacts (read_contacts reports its groups)
+    uint32_t standalone_groups = 0;
+    DevBuf<uint64_t> standalone_keys;
+
+    World() {
+        check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+        check_cuda(cudaMallocHost(&hs, sizeof(HostStats)), "cudaMallocHost");
+        std::memset(hs, 0, sizeof(HostStats));
+        flags.reserve(4);
+        check_cuda(cudaMemsetAsync(flags.p, 0, 4 * sizeof(uint32_t), stream), "memset");
+        cache[0].init();
+        cache[1].init();
+        check_cuda(cudaMemsetAsync(cache[0].count_dev, 0, sizeof(uint32_t), stream), "memset");
+        check_cuda(cudaMemsetAsync(cache[1].count_dev, 0, sizeof(uint32_t), stream), "memset");
+        pd.scalars.reserve(16);
+        for (auto& set : ev)
+            for (auto& e : set) check_cuda(cudaEventCreate(&e), "event");
+    }
+    ~World() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& set : ev)
+            for (auto& e : set) if (e) cudaEventDestroy(e);
+        if (hs) cudaFreeHost(hs);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    BodyDev body_dev() {
+        return BodyDev{pos.p, quat.p, linvel.p, angvel.p, inv_inertia.p, grav.p, force.p, torque.p, material.p,
+                       sleep.p, info_d.p, aabb_min.p, aabb_max.p, pred.p, settled.p, iw.p, push_lin.p, push_ang.p};
+    }
+    WorldView view() { return WorldView{body_dev(), shapes_d.p, hull_d.p, n}; }
+
+    void sync_shapes() {
+        if (!shapes_dirty) return;
+        shapes_d.reserve(shapes_h.size() + 1);
+        check_cuda(cudaMemcpyAsync(shapes_d.p, shapes_h.data(), shapes_h.size() * sizeof(Shape), cudaMemcpyHostToDevice,
+                                   stream), "upload shapes");
+        hull_d.reserve(hull_h.size() + 1);
+        if (!hull_h.empty())
+            check_cuda(cudaMemcpyAsync(hull_d.p, hull_h.data(), hull_h.size() * sizeof(float4), cudaMemcpyHostToDevice,
+                                       stream), "upload hull");
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+        shapes_dirty = false;
+    }
+
+    uint32_t add_shape(uint32_t type, const float* params, const float* pts, uint32_t npts) {
+        Shape s;
+        std::memset(&s, 0, sizeof(s));
+        s.type = type;
+        switch (type) {
+            case SHAPE_SPHERE:
+                if (!params || !(params[0] > 0.0f)) throw InvalidArg{"sphere radius must be > 0"};
+                s.p0 = params[0];
+                s.margin = s.p0;
+                for (int k = 0; k < 3; ++k) { s.lmin[k] = -s.p0; s.lmax[k] = s.p0; }
+                break;
+            case SHAPE_BOX:
+                if (!params || !(params[0] > 0.0f) || !(params[1] > 0.0f) || !(params[2] > 0.0f))
+                    throw InvalidArg{"box half extents must be > 0"};
+                s.p0 = params[0]; s.p1 = params[1]; s.p2 = params[2];
+                s.margin = 0.04f;
+                s.lmin[0] = -s.p0; s.lmin[1] = -s.p1; s.lmin[2] = -s.p2;
+                s.lmax[0] = s.p0; s.lmax[1] = s.p1; s.lmax[2] = s.p2;
+                break;
+            case SHAPE_CAPSULE:
+                if (!params || !(params[0] > 0.0f) || !(params[1] >= 0.0f))
+                    throw InvalidArg{"capsule radius must be > 0 and half height >= 0"};
+                s.p0 = params[0]; s.p1 = params[1];
+                s.margin = s.p0;
+                s.lmin[0] = -s.p0; s.lmin[1] = -(s.p1 + s.p0); s.lmin[2] = -s.p0;
+                s.lmax[0] = s.p0; s.lmax[1] = s.p1 + s.p0; s.lmax[2] = s.p0;
+                break;
+            case SHAPE_HULL: {
+                if (!pts || npts == 0) throw InvalidArg{"hull needs at least one point"};
+                s.hull_off = uint32_t(hull_h.size());
+                s.hull_cnt = npts;
+                s.margin = 0.0f;
+                for (int k = 0; k < 3; ++k) { s.lmin[k] = INFINITY; s.lmax[k] = -INFINITY; }
+                for (uint32_t i = 0; i < npts; ++i) {
+                    hull_h.push_back(make_float4(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], 0.0f));
+                    for (int k = 0; k < 3; ++k) {
+                        s.lmin[k] = std::min(s.lmin[k], pts[3 * i + k]);
+                        s.lmax[k] = std::max(s.lmax[k], pts[3 * i + k]);
+                    }
+                }
+                break;
+            }
+            case SHAPE_PLANE: {
+                if (!params) throw InvalidArg{"plane needs a normal and a constant"};
+                float nx = params[0], ny = params[1], nz = params[2];
+                float l = std::sqrt(nx * nx + ny * ny + nz * nz);
+                if (!(l > 0.0f)) throw InvalidArg{"plane normal must be nonzero"};
+                s.p0 = nx / l; s.p1 = ny / l; s.p2 = nz / l; s.p3 = params[3];
+                s.margin = 0.0f;
+                for (int k = 0; k < 3; ++k) { s.lmin[k] = -1e30f; s.lmax[k] = 1e30f; }
+                break;
+            }
+            default:
+                throw InvalidArg{"unknown shape type"};
+        }
+        s.cbt = contact_breaking_threshold(s.lmin, s.lmax);
+        shapes_h.push_back(s);
+        shapes_dirty = true;
+        return uint32_t(shapes_h.size() - 1);
+    }
+
+    void grow_bodies(uint32_t need) {
+        if (need <= cap) return;
+        uint32_t c = std::max<uint32_t>(need, cap * 2);
+        c = std::max<uint32_t>(c, 64);
+        auto g4 = [&](DevBuf<float4>& b) { b.grow_keep(c, n, stream); };
+        g4(pos); g4(quat); g4(linvel); g4(angvel); g4(inv_inertia); g4(grav); g4(force); g4(torque); g4(material);
+        g4(sleep); g4(aabb_min); g4(aabb_max); g4(pred); g4(push_lin); g4(push_ang);
+        iw.grow_keep(size_t(c) * 3, size_t(n) * 3, stream);
+        info_d.grow_keep(c, n, stream);
+        settled.grow_keep(c, n, stream);
+        cap = c;
+    }
+
+    uint32_t add_bodies(uint32_t cnt, const bgpu_body_desc* d) {
+        for (uint32_t k = 0; k < cnt; ++k) {
+            if (d[k].shape >= shapes_h.size()) throw InvalidArg{"body shape id out of range"};
+            if (shapes_h[d[k].shape].type == SHAPE_PLANE && d[k].mass != 0.0f)
+                throw InvalidArg{"a plane body must be static (mass 0)"};
+            if (!(d[k].mass >= 0.0f)) throw InvalidArg{"mass must be >= 0"};
+        }
+        sync_shapes();
+        uint32_t first = n;
+        grow_bodies(n + cnt);
+        std::vector<float4> hp(cnt), hq(cnt), hlv(cnt), hav(cnt), hinv(cnt), hg(cnt), hz(cnt), hmat(cnt), hsl(cnt);
+        std::vector<uint4> hinfo(cnt);
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const bgpu_body_desc& b = d[k];
+            const Shape& s = shapes_h[b.shape];
+            bool kin = (b.flags & BGPU_BODY_KINEMATIC) != 0;
+            bool stat = b.mass == 0.0f && !kin;
+            uint32_t fl = 0;
+            if (stat) fl |= BF_STATIC;
+            if (kin) fl |= BF_KINEMATIC;
+            if (b.flags & BGPU_BODY_NO_CONTACT_RESPONSE) fl |= BF_NO_RESPONSE;
+            if (b.flags & BGPU_BODY_DISABLE_WORLD_GRAVITY) fl |= BF_DISABLE_GRAVITY;
+            if (b.flags & BGPU_BODY_ADDITIONAL_DAMPING) fl |= BF_ADDITIONAL_DAMPING;
+            float inv_mass = 0.0f, inv[3] = {0.0f, 0.0f, 0.0f};
+            if (!stat && !kin) {  // body.rs:388-399 new_dynamic
+                float in[3];
+                local_inertia(s, b.mass, in);
+                for (int a = 0; a < 3; ++a) inv[a] = in[a] != 0.0f ? 1.0f / in[a] : 0.0f;
+                inv_mass = 1.0f / b.mass;
+            }
+            uint32_t act = stat ? ACT_ISLAND_SLEEPING : (kin ? ACT_DISABLE_DEACTIVATION : ACT_ACTIVE);
+            if (b.activation) act = b.activation;
+            hp[k] = make_float4(b.position[0], b.position[1], b.position[2], 0.0f);
+            hq[k] = make_float4(b.orientation[0], b.orientation[1], b.orientation[2], b.orientation[3]);
+            hlv[k] = make_float4(b.linear_velocity[0], b.linear_velocity[1], b.linear_velocity[2], 0.0f);
+            hav[k] = make_float4(b.angular_velocity[0], b.angular_velocity[1], b.angular_velocity[2], 0.0f);
+            hinv[k] = make_float4(inv[0], inv[1], inv[2], inv_mass);
+            // world.rs:528-535: dynamic bodies inherit the world gravity.
+            bool inherit = !stat && !kin && !(b.flags & BGPU_BODY_DISABLE_WORLD_GRAVITY);
+            hg[k] = inherit ? make_float4(gravity[0], gravity[1], gravity[2], 0.0f) : make_float4(0.f, 0.f, 0.f, 0.f);
+            hz[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+            hmat[k] = make_float4(b.friction, b.restitution, b.linear_damping, b.angular_damping);
+            float lt = b.linear_sleeping_threshold > 0.0f ? b.linear_sleeping_threshold : 0.8f;
+            float at = b.angular_sleeping_threshold > 0.0f ? b.angular_sleeping_threshold : 1.0f;
+            hsl[k] = make_float4(0.0f, lt, at, 0.0f);
+            uint32_t group = b.group, mask = b.mask;
+            hinfo[k] = make_uint4(b.shape, fl, act, group | (mask << 16));
+            if (s.type == SHAPE_PLANE) unbounded.push_back(first + k);
+        }
+        auto up = [&](DevBuf<float4>& dst, const std::vector<float4>& src) {
+            check_cuda(cudaMemcpyAsync(dst.p + first, src.data(), cnt * sizeof(float4), cudaMemcpyHostToDevice, stream),
+                       "upload bodies");
+        };
+        up(pos, hp); up(quat, hq); up(linvel, hlv); up(angvel, hav); up(inv_inertia, hinv); up(grav, hg);
+        up(force, hz); up(torque, hz); up(material, hmat); up(sleep, hsl); up(push_lin, hz); up(push_ang, hz);
+        check_cuda(cudaMemcpyAsync(info_d.p + first, hinfo.data(), cnt * sizeof(uint4), cudaMemcpyHostToDevice, stream),
+                   "upload info");
+        n += cnt;
+        launch_initial_aabbs(body_dev(), shapes_d.p, hull_d.p, first, cnt, stream);
+        check_cuda(cudaGetLastError(), "initial aabbs");
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+        std::sort(unbounded.begin(), unbounded.end());
+        return first;
+    }
+
+    void set_gravity(const float* g) {
+        gravity[0] = g[0]; gravity[1] = g[1]; gravity[2] = g[2];
+        // world.rs:467-481: active bodies that did not opt out take the new gravity.
+        if (n == 0) return;
+        std::vector<uint4> hinfo(n);
+        std::vector<float4> hg(n);
+        check_cuda(cudaMemcpyAsync(hinfo.data(), info_d.p, n * sizeof(uint4), cudaMemcpyDeviceToHost, stream), "d2h");
+        check_cuda(cudaMemcpyAsync(hg.data(), grav.p, n * sizeof(float4), cudaMemcpyDeviceToHost, stream), "d2h");
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+        for (uint32_t i = 0; i < n; ++i) {
+            uint32_t a = hinfo[i].z;
+            bool active = a == ACT_ACTIVE || a == ACT_WANTS_DEACTIVATION || a == ACT_DISABLE_DEACTIVATION;
+            if (active && !(hinfo[i].y & BF_DISABLE_GRAVITY)) hg[i] = make_float4(g[0], g[1], g[2], 0.0f);
+        }
+        check_cuda(cudaMemcpyAsync(grav.p, hg.data(), n * sizeof(float4), cudaMemcpyHostToDevice, stream), "h2d");
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+    }
+
+    void mark(int k) {
+        if (timing) check_cuda(cudaEventRecord(ev[ev_cur][k], stream), "event");
+    }
+
+    // Adds a completed event set to the timing sums. Marks: 0 start, 1 velocities+AABBs,
+    // 2 broad phase, 3 islands, 4 pair pass, 5 colouring, 6 PGS kernel, 7 writeback, 8 positions.
+    void fold(int set) {
+        if (!ev_pending[set]) return;
+        ev_pending[set] = false;
+        float ms[9] = {};
+        for (int k = 0; k < 8; ++k) check_cuda(cudaEventElapsedTime(&ms[k], ev[set][k], ev[set][k + 1]), "elapsed");
+        last.stage_ms[0] += ms[0];
+        last.stage_ms[1] += 0.0f;  // AABBs are fused into the velocity pass
+        last.stage_ms[2] += ms[1];
+        last.stage_ms[3] += ms[2];
+        last.stage_ms[4] += ms[3];
+        last.stage_ms[5] += ms[4] + ms[5] + ms[6];
+        last.stage_ms[6] += ms[7];
+        last.solve_kernel_ms += ms[5];
+        float total = 0.0f;
+        check_cuda(cudaEventElapsedTime(&total, ev[set][0], ev[set][8]), "elapsed");
+        last.step_ms += total;
+        last.timed_steps += 1;
+    }
+
+    void reset_timing() {
+        for (int k = 0; k < 7; ++k) last.stage_ms[k] = 0.0f;
+        last.solve_kernel_ms = 0.0f;
+        last.step_ms = 0.0f;
+        last.timed_steps = 0;
+        ev_pending[0] = ev_pending[1] = false;
+    }
+
+    // One step_simulation(dt) (step.rs:100-108 -> internal_step).
+    void step_once(float dt) {
+        sync_shapes();
+        solved_standalone = 0;
+        StepParams sp;
+        sp.dt = dt;
+        sp.inv_dt = 1.0f / dt;
+        sp.info = info;
+        BodyDev b = body_dev();
+        WorldView wv = view();
+        uint32_t* status = flags.p;
+        uint32_t* simulate = flags.p + 1;
+        uint32_t* prev_simulate = flags.p + 2;
+        check_cuda(cudaMemsetAsync(flags.p, 0, 2 * sizeof(uint32_t), stream), "memset flags");
+        mark(0);
+        // 1-3: velocities, predicted poses, AABBs (fused).
+        launch_integrate_velocities(b, shapes_d.p, hull_d.p, n, dt, stream);
+        mark(1);
+        // 4: broad phase (syncs once to size the pair arrays; the previous step's
+        //    manifold count and timing events are read at the same point).
+        uint64_t np = bp.run(aabb_min.p, aabb_max.p, n, unbounded, pairs, status, stream);
+        npairs = uint32_t(np);
+        if (timing) fold(ev_cur ^ 1);
+        Manifolds& old_cache = cache[cur];
+        Manifolds& next = cache[cur ^ 1];
+        old_cache.count_host = hs->cache_count;
+        mark(2);
+        // 4b: islands
+        islands.run(b, n, pairs.p, npairs, simulate, status, stream);
+        mark(3);
+        // 5: pair pass
+        pd.reserve(std::max<uint32_t>(npairs, 1), n, old_cache.count_host);
+        if (old_cache.count_host)
+            check_cuda(cudaMemsetAsync(pd.old_owned.p, 0, old_cache.count_host * sizeof(uint32_t), stream), "memset");
+        run_pair_pass(wv, pairs.p, npairs, old_cache, pd, sp, simulate, status, stream);
+        mark(4);
+        // 6: solve (colouring, then the PGS kernel)
+        run_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); });
+        // 6b: impulse writeback + prune
+        run_cache_update(pairs.p, npairs, old_cache, pd, next, simulate, prev_simulate, stream);
+        check_cuda(cudaMemcpyAsync(prev_simulate, simulate, sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream), "flag");
+        mark(7);
+        // 6c + 7 + 8: deactivation, pose integration with the split push, force clear.
+        launch_integrate_positions(b, n, dt, info.split_impulse_turn_erp, stream);
+        mark(8);
+        if (timing) {
+            ev_pending[ev_cur] = true;
+            ev_cur ^= 1;
+        }
+        check_cuda(cudaGetLastError(), "step launch");
+        cur ^= 1;
+        check_cuda(cudaMemcpyAsync(hs->scalars, pd.scalars.p, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream), "d2h");
+        check_cuda(cudaMemcpyAsync(&hs->status, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream), "d2h");
+        check_cuda(cudaMemcpyAsync(&hs->cache_count, next.count_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream),
+                   "d2h");
+        stats_pending = true;
+    }
+
+    void finish_stats() {
+        if (!stats_pending) return;
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+        stats_pending = false;
+        last.num_bodies = n;
+        last.num_pairs = npairs;
+        last.num_contact_pairs = hs->scalars[2];
+        last.num_contacts = hs->scalars[3];
+        last.num_colours = hs->scalars[4];
+        last.num_split_pairs = hs->scalars[5];
+        last.num_detect = hs->scalars[0] + hs->scalars[1];
+        last.num_manifolds = hs->cache_count;
+        last.device_status = hs->status;
+        if (timing) {
+            fold(ev_cur ^ 1);
+            fold(ev_cur);
+        }
+    }
+};
+
+}  // namespace bgpu
+
+using bgpu::World;
+
+struct bgpu_world {
+    World impl;
+};
+
+namespace {
+
+template <class F>
+bgpu_status guarded(F&& f) {
+    try {
+        return f();
+    } catch (const bgpu::CudaError& e) {
+        bgpu::g_last_error = e.where;
+        return BGPU_ERR_CUDA;
+    } catch (const bgpu::InvalidArg& e) {
+        bgpu::g_last_error = e.what;
+        return BGPU_ERR_INVALID_ARGUMENT;
+    } catch (const std::bad_alloc&) {
+        bgpu::g_last_error = "host allocation failed";
+        return BGPU_ERR_CAPACITY;
+    } catch (const std::exception& e) {
+        bgpu::g_last_error = e.what();
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+}
+
+bgpu_status check_device_status(World& w) {
+    w.finish_stats();
+    if (w.last.device_status) {
+        char buf[128];
+        std::snprintf(buf, sizeof(buf), "device status bits 0x%x", w.last.device_status);
+        bgpu::g_last_error = buf;
+        return BGPU_ERR_DEVICE_STATUS;
+    }
+    return BGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bgpu_version(void) { return "bgpu 0.1 (sm_100a)"; }
+
+int bgpu_device_count(void) {
+    int c = 0;
+    if (cudaGetDeviceCount(&c) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return c;
+}
+
+size_t bgpu_last_error(char* buf, size_t len) {
+    const std::string& e = bgpu::g_last_error;
+    if (buf && len) {
+        size_t k = std::min(len - 1, e.size());
+        std::memcpy(buf, e.data(), k);
+        buf[k] = 0;
+    }
+    return e.size();
+}
+
+void bgpu_solver_info_default(bgpu_solver_info* o) {
+    if (!o) return;
+    o->erp2 = 0.2f;
+    o->linear_slop = 0.005f;
+    o->restitution_velocity_threshold = 1.0f;
+    o->split_impulse = 1;
+    o->split_impulse_penetration_threshold = -0.04f;
+    o->split_impulse_turn_erp = 0.1f;
+    o->warmstarting_factor = 0.85f;
+    o->global_cfm = 0.0f;
+    o->sor = 1.0f;
+    o->num_iterations = 10;
+}
+
+void bgpu_body_desc_default(bgpu_body_desc* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->orientation[3] = 1.0f;
+    o->mass = 1.0f;
+    o->friction = 0.5f;
+    o->group = 1;
+    o->mask = 0xFFFF;
+}
+
+static void copy_info(bgpu::SolverParams& d, const bgpu_solver_info& s) {
+    d.erp2 = s.erp2;
+    d.linear_slop = s.linear_slop;
+    d.restitution_velocity_threshold = s.restitution_velocity_threshold;
+    d.split_impulse = s.split_impulse;
+    d.split_impulse_penetration_threshold = s.split_impulse_penetration_threshold;
+    d.split_impulse_turn_erp = s.split_impulse_turn_erp;
+    d.warmstarting_factor = s.warmstarting_factor;
+    d.global_cfm = s.global_cfm;
+    d.sor = s.sor;
+    d.num_iterations = s.num_iterations;
+}
+
+bgpu_status bgpu_world_create(const bgpu_solver_info* info, const float* gravity, bgpu_world** out) {
+    if (!out) {
+        bgpu::g_last_error = "out is NULL";
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    if (bgpu_device_count() == 0) {
+        bgpu::g_last_error = "no CUDA device";
+        return BGPU_ERR_NO_DEVICE;
+    }
+    return guarded([&]() -> bgpu_status {
+        std::unique_ptr<bgpu_world> w(new bgpu_world());
+        bgpu_solver_info d;
+        bgpu_solver_info_default(&d);
+        copy_info(w->impl.info, info ? *info : d);
+        if (gravity) std::memcpy(w->impl.gravity, gravity, 3 * sizeof(float));
+        *out = w.release();
+        return BGPU_OK;
+    });
+}
+
+void bgpu_world_destroy(bgpu_world* w) { delete w; }
+
+bgpu_status bgpu_world_set_gravity(bgpu_world* w, const float* g) {
+    if (!w || !g) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        w->impl.set_gravity(g);
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_world_set_solver_info(bgpu_world* w, const bgpu_solver_info* info) {
+    if (!w || !info) return BGPU_ERR_INVALID_ARGUMENT;
+    copy_info(w->impl.info, *info);
+    return BGPU_OK;
+}
+
+bgpu_status bgpu_add_shape(bgpu_world* w, uint32_t type, const float* params, const float* pts, uint32_t npts,
+                           uint32_t* out) {
+    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        uint32_t id = w->impl.add_shape(type, params, pts, npts);
+        if (out) *out = id;
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_add_bodies(bgpu_world* w, uint32_t n, const bgpu_body_desc* d, uint32_t* out_first) {
+    if (!w || (n && !d)) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        w->impl.finish_stats();
+        uint32_t f = w->impl.add_bodies(n, d);
+        if (out_first) *out_first = f;
+        return BGPU_OK;
+    });
+}
+
+uint32_t bgpu_num_bodies(const bgpu_world* w) { return w ? w->impl.n : 0; }
+
+bgpu_status bgpu_step(bgpu_world* w, float dt, uint32_t nsteps) {
+    if (!w || !(dt > 0.0f)) {
+        bgpu::g_last_error = "world is NULL or dt <= 0";
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&]() -> bgpu_status {
+        for (uint32_t k = 0; k < nsteps; ++k) w->impl.step_once(dt);
+        return check_device_status(w->impl);
+    });
+}
+
+bgpu_status bgpu_step_timed(bgpu_world* w, float dt, uint32_t nsteps, float* device_ms) {
+    if (!w || !(dt > 0.0f)) {
+        bgpu::g_last_error = "world is NULL or dt <= 0";
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        cudaEvent_t a, b;
+        bgpu::check_cuda(cudaEventCreate(&a), "event");
+        bgpu::check_cuda(cudaEventCreate(&b), "event");
+        bgpu::check_cuda(cudaEventRecord(a, W.stream), "event");
+        for (uint32_t k = 0; k < nsteps; ++k) W.step_once(dt);
+        bgpu::check_cuda(cudaEventRecord(b, W.stream), "event");
+        bgpu::check_cuda(cudaEventSynchronize(b), "event sync");
+        float ms = 0.0f;
+        bgpu::check_cuda(cudaEventElapsedTime(&ms, a, b), "elapsed");
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        if (device_ms) *device_ms = ms;
+        return check_device_status(W);
+    });
+}
+
+// step.rs:136-199 (fixed-timestep accumulator; motion-state interpolation is not modelled).
+bgpu_status bgpu_step_simulation_fixed(bgpu_world* w, float dt, uint32_t max_sub_steps, float fixed_dt,
+                                       uint32_t* out_substeps) {
+    if (!w || (max_sub_steps != 0 && !(fixed_dt > 0.0f))) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        uint32_t num = 0;
+        float step_dt = fixed_dt;
+        if (max_sub_steps != 0) {
+            float& acc = W.accumulator;
+            acc += dt;
+            if (acc >= fixed_dt) {
+                num = uint32_t(acc / fixed_dt);
+                acc -= float(num) * fixed_dt;
+            }
+        } else {
+            step_dt = dt;
+            W.accumulator = dt;  // step.rs:156 (latency interpolation off: the remainder is dt)
+            if (std::fabs(dt) <= 1.1920929e-7f) {
+                if (out_substeps) *out_substeps = 0;
+                return BGPU_OK;
+            }
+            num = 1;
+        }
+        uint32_t clamped = max_sub_steps ? std::min(num, max_sub_steps) : num;
+        for (uint32_t k = 0; k < clamped; ++k) W.step_once(step_dt);
+        if (out_substeps) *out_substeps = num;
+        return check_device_status(W);
+    });
+}
+
+bgpu_status bgpu_read_state(bgpu_world* w, float* state) {
+    if (!w || !state) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        uint32_t n = W.n;
+        std::vector<float4> p(n), q(n), lv(n), av(n), sl(n);
+        std::vector<uint4> in(n);
+        cudaStream_t s = W.stream;
+        bgpu::check_cuda(cudaMemcpyAsync(p.data(), W.pos.p, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaMemcpyAsync(q.data(), W.quat.p, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaMemcpyAsync(lv.data(), W.linvel.p, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaMemcpyAsync(av.data(), W.angvel.p, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaMemcpyAsync(sl.data(), W.sleep.p, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaMemcpyAsync(in.data(), W.info_d.p, n * sizeof(uint4), cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+        for (uint32_t i = 0; i < n; ++i) {
+            float* o = state + size_t(i) * 15;
+            o[0] = p[i].x; o[1] = p[i].y; o[2] = p[i].z;
+            o[3] = q[i].x; o[4] = q[i].y; o[5] = q[i].z; o[6] = q[i].w;
+            o[7] = lv[i].x; o[8] = lv[i].y; o[9] = lv[i].z;
+            o[10] = av[i].x; o[11] = av[i].y; o[12] = av[i].z;
+            o[13] = float(in[i].z);
+            o[14] = sl[i].x;
+        }
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_write_state(bgpu_world* w, const float* state) {
+    if (!w || !state) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        W.finish_stats();
+        uint32_t n = W.n;
+        std::vector<float4> p(n), q(n), lv(n), av(n), sl(n);
+        std::vector<uint4> in(n);
+        cudaStream_t s = W.stream;
+        bgpu::check_cuda(cudaMemcpyAsync(sl.data(), W.sleep.p, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaMemcpyAsync(in.data(), W.info_d.p, n * sizeof(uint4), cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+        for (uint32_t i = 0; i < n; ++i) {
+            const float* o = state + size_t(i) * 15;
+            p[i] = make_float4(o[0], o[1], o[2], 0.0f);
+            q[i] = make_float4(o[3], o[4], o[5], o[6]);
+            lv[i] = make_float4(o[7], o[8], o[9], 0.0f);
+            av[i] = make_float4(o[10], o[11], o[12], 0.0f);
+            in[i].z = uint32_t(o[13]);
+            sl[i].x = o[14];
+        }
+        bgpu::check_cuda(cudaMemcpyAsync(W.pos.p, p.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s), "h2d");
+        bgpu::check_cuda(cudaMemcpyAsync(W.quat.p, q.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s), "h2d");
+        bgpu::check_cuda(cudaMemcpyAsync(W.linvel.p, lv.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s), "h2d");
+        bgpu::check_cuda(cudaMemcpyAsync(W.angvel.p, av.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s), "h2d");
+        bgpu::check_cuda(cudaMemcpyAsync(W.sleep.p, sl.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s), "h2d");
+        bgpu::check_cuda(cudaMemcpyAsync(W.info_d.p, in.data(), n * sizeof(uint4), cudaMemcpyHostToDevice, s), "h2d");
+        bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_read_poses(bgpu_world* w, float* poses) {
+    if (!w || !poses) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        uint32_t n = W.n;
+        std::vector<float4> p(n), q(n);
+        cudaStream_t s = W.stream;
+        bgpu::check_cuda(cudaMemcpyAsync(p.data(), W.pos.p, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaMemcpyAsync(q.data(), W.quat.p, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+        for (uint32_t i = 0; i < n; ++i) {
+            float* o = poses + size_t(i) * 7;
+            o[0] = p[i].x; o[1] = p[i].y; o[2] = p[i].z;
+            o[3] = q[i].x; o[4] = q[i].y; o[5] = q[i].z; o[6] = q[i].w;
+        }
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_apply_forces(bgpu_world* w, const float* force, const float* torque) {
+    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        uint32_t n = W.n;
+        std::vector<float4> f(n);
+        cudaStream_t s = W.stream;
+        for (int which = 0; which < 2; ++which) {
+            const float* src = which ? torque : force;
+            if (!src) continue;
+            for (uint32_t i = 0; i < n; ++i) f[i] = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0f);
+            bgpu::check_cuda(cudaMemcpyAsync(which ? W.torque.p : W.force.p, f.data(), n * sizeof(float4),
+                                             cudaMemcpyHostToDevice, s), "h2d");
+            bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+        }
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_read_pairs(bgpu_world* w, uint32_t* out, uint64_t cap, uint64_t* out_n) {
+    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        W.finish_stats();
+        if (out_n) *out_n = W.npairs;
+        uint64_t k = std::min<uint64_t>(cap, W.npairs);
+        if (!out || !k) return BGPU_OK;
+        std::vector<uint64_t> keys(k);
+        bgpu::check_cuda(cudaMemcpyAsync(keys.data(), W.pairs.p, k * sizeof(uint64_t), cudaMemcpyDeviceToHost, W.stream),
+                         "d2h");
+        bgpu::check_cuda(cudaStreamSynchronize(W.stream), "sync");
+        for (uint64_t i = 0; i < k; ++i) {
+            out[2 * i] = bgpu::key_lo(keys[i]);
+            out[2 * i + 1] = bgpu::key_hi(keys[i]);
+        }
+        return BGPU_OK;
+    });
+}
+
+// Gather the solved rows in (colour, pair key) order.
+static void gather_solve_order(World& W, uint32_t ngroups, const uint64_t* keys_dev, std::vector<uint64_t>& order_keys,
+                               std::vector<float>& rows_out) {
+    bgpu::PairData& pd = W.pd;
+    cudaStream_t s = W.stream;
+    uint32_t sc[16];
+    bgpu::check_cuda(cudaMemcpyAsync(sc, pd.scalars.p, sizeof(sc), cudaMemcpyDeviceToHost, s), "d2h");
+    bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+    uint32_t K = sc[2], ncol = sc[4];
+    std::vector<uint32_t> cp(K), col(K), cnt(ngroups);
+    std::vector<uint64_t> keys(ngroups);
+    std::vector<float4> rows(size_t(ngroups) * 4 * bgpu::ROW_F4);
+    if (K) {
+        bgpu::check_cuda(cudaMemcpyAsync(cp.data(), pd.contact_pairs.p, K * 4, cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaMemcpyAsync(col.data(), pd.colour.p, K * 4, cudaMemcpyDeviceToHost, s), "d2h");
+    }
+    if (ngroups) {
+        bgpu::check_cuda(cudaMemcpyAsync(cnt.data(), pd.row_count.p, ngroups * 4, cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaMemcpyAsync(keys.data(), keys_dev, ngroups * 8, cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaMemcpyAsync(rows.data(), pd.rows.p, rows.size() * sizeof(float4), cudaMemcpyDeviceToHost, s),
+                         "d2h");
+    }
+    bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+    (void)ncol;
+    std::vector<uint32_t> idx(K);
+    for (uint32_t k = 0; k < K; ++k) idx[k] = k;
+    std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) {
+        if (col[a] != col[b]) return col[a] < col[b];
+        return cp[a] < cp[b];
+    });
+    order_keys.clear();
+    rows_out.clear();
+    for (uint32_t t : idx) {
+        uint32_t p = cp[t];
+        order_keys.push_back(keys[p]);
+        for (uint32_t k = 0; k < cnt[p]; ++k) {
+            const float4* r = &rows[(size_t(p) * 4 + k) * bgpu::ROW_F4];
+            float rec[16] = {float(bgpu::key_lo(keys[p])), float(bgpu::key_hi(keys[p])), float(k),
+                             r[0].x, r[0].y, r[0].z, r[1].x, r[1].y, r[1].z, r[2].x, r[2].y, r[2].z,
+                             r[5].w, r[3].x, r[3].y, r[3].z};
+            rows_out.insert(rows_out.end(), rec, rec + 16);
+            rows_out.push_back(r[5].y);
+            rows_out.push_back(r[5].z);
+        }
+    }
+}
+
+bgpu_status bgpu_read_contacts(bgpu_world* w, float* out, uint64_t cap, uint64_t* out_n) {
+    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        W.finish_stats();
+        std::vector<uint64_t> keys;
+        std::vector<float> rows;
+        if (W.solved_standalone) gather_solve_order(W, W.standalone_groups, W.standalone_keys.p, keys, rows);
+        else gather_solve_order(W, W.npairs, W.pairs.p, keys, rows);
+        uint64_t n = rows.size() / 18;
+        if (out_n) *out_n = n;
+        uint64_t k = std::min<uint64_t>(cap, n);
+        for (uint64_t i = 0; i < k; ++i) std::memcpy(out + 18 * i, rows.data() + 18 * i, 18 * sizeof(float));
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_read_solve_order(bgpu_world* w, uint64_t* out, uint64_t cap, uint64_t* out_n) {
+    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        W.finish_stats();
+        std::vector<uint64_t> keys;
+        std::vector<float> rows;
+        if (W.solved_standalone) gather_solve_order(W, W.standalone_groups, W.standalone_keys.p, keys, rows);
+        else gather_solve_order(W, W.npairs, W.pairs.p, keys, rows);
+        if (out_n) *out_n = keys.size();
+        uint64_t k = std::min<uint64_t>(cap, keys.size());
+        if (out && k) std::memcpy(out, keys.data(), k * sizeof(uint64_t));
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_get_stats(bgpu_world* w, bgpu_step_stats* out) {
+    if (!w || !out) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        w->impl.finish_stats();
+        *out = w->impl.last;
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_enable_step_timing(bgpu_world* w, int on) {
+    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        w->impl.finish_stats();
+        w->impl.timing = on != 0;
+        w->impl.reset_timing();
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_broadphase_pairs(const float* aabbs, uint32_t n, uint32_t* out, uint64_t cap, uint64_t* out_n) {
+    if (!aabbs && n) return BGPU_ERR_INVALID_ARGUMENT;
+    if (bgpu_device_count() == 0) {
+        bgpu::g_last_error = "no CUDA device";
+        return BGPU_ERR_NO_DEVICE;
+    }
+    return guarded([&]() -> bgpu_status {
+        cudaStream_t s;
+        bgpu::check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+        struct StreamGuard {
+            cudaStream_t s;
+            ~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+        } guard{s};
+        std::vector<float4> mn(n), mx(n);
+        std::vector<uint32_t> unb;
+        for (uint32_t i = 0; i < n; ++i) {
+            const float* a = aabbs + 6 * size_t(i);
+            mn[i] = make_float4(a[0], a[1], a[2], 0.0f);
+            mx[i] = make_float4(a[3], a[4], a[5], 0.0f);
+            bool huge = false;
+            for (int k = 0; k < 3; ++k) {
+                float e = a[3 + k] - a[k];
+                if (!(e < 1e15f)) huge = true;
+            }
+            if (huge) unb.push_back(i);
+        }
+        bgpu::DevBuf<float4> dmn, dmx;
+        bgpu::DevBuf<uint64_t> pairs;
+        bgpu::DevBuf<uint32_t> status;
+        dmn.reserve(n + 1);
+        dmx.reserve(n + 1);
+        status.reserve(1);
+        bgpu::check_cuda(cudaMemsetAsync(status.p, 0, 4, s), "memset");
+        if (n) {
+            bgpu::check_cuda(cudaMemcpyAsync(dmn.p, mn.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s), "h2d");
+            bgpu::check_cuda(cudaMemcpyAsync(dmx.p, mx.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s), "h2d");
+        }
+        bgpu::Broadphase bp;
+        uint64_t np = bp.run(dmn.p, dmx.p, n, unb, pairs, status.p, s);
+        uint32_t st = 0;
+        bgpu::check_cuda(cudaMemcpyAsync(&st, status.p, 4, cudaMemcpyDeviceToHost, s), "d2h");
+        std::vector<uint64_t> keys(np);
+        if (np)
+            bgpu::check_cuda(cudaMemcpyAsync(keys.data(), pairs.p, np * 8, cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+        if (out_n) *out_n = np;
+        uint64_t k = std::min<uint64_t>(cap, np);
+        for (uint64_t i = 0; i < k && out; ++i) {
+            out[2 * i] = bgpu::key_lo(keys[i]);
+            out[2 * i + 1] = bgpu::key_hi(keys[i]);
+        }
+        if (st) {
+            bgpu::g_last_error = "broad-phase traversal stack overflow";
+            return BGPU_ERR_DEVICE_STATUS;
+        }
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_collide(bgpu_world* w, uint32_t n, const uint32_t* sa, const float* pa, const uint32_t* sb,
+                         const float* pb, const float* seeds, int force_convex, float* out, uint32_t* counts) {
+    if (!w || (n && (!sa || !pa || !sb || !pb || !out || !counts))) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        for (uint32_t i = 0; i < n; ++i)
+            if (sa[i] >= W.shapes_h.size() || sb[i] >= W.shapes_h.size()) throw bgpu::InvalidArg{"shape id out of range"};
+        W.sync_shapes();
+        cudaStream_t s = W.stream;
+        std::vector<float4> hpa(n), hqa(n), hpb(n), hqb(n), hs(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            const float* a = pa + 7 * size_t(i);
+            const float* b = pb + 7 * size_t(i);
+            hpa[i] = make_float4(a[0], a[1], a[2], 0.0f);
+            hqa[i] = make_float4(a[3], a[4], a[5], a[6]);
+            hpb[i] = make_float4(b[0], b[1], b[2], 0.0f);
+            hqb[i] = make_float4(b[3], b[4], b[5], b[6]);
+            if (seeds) hs[i] = make_float4(seeds[3 * i], seeds[3 * i + 1], seeds[3 * i + 2], 0.0f);
+        }
+        bgpu::DevBuf<float4> d_pa, d_qa, d_pb, d_qb, d_seed, d_out;
+        bgpu::DevBuf<uint32_t> d_sa, d_sb, d_cnt, d_status;
+        size_t m = size_t(n) + 1;
+        d_pa.reserve(m); d_qa.reserve(m); d_pb.reserve(m); d_qb.reserve(m); d_seed.reserve(m);
+        d_out.reserve(m * 8); d_sa.reserve(m); d_sb.reserve(m); d_cnt.reserve(m); d_status.reserve(1);
+        auto h2d = [&](void* dst, const void* src, size_t bytes) {
+            if (bytes) bgpu::check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "h2d");
+        };
+        h2d(d_pa.p, hpa.data(), n * sizeof(float4));
+        h2d(d_qa.p, hqa.data(), n * sizeof(float4));
+        h2d(d_pb.p, hpb.data(), n * sizeof(float4));
+        h2d(d_qb.p, hqb.data(), n * sizeof(float4));
+        h2d(d_seed.p, hs.data(), n * sizeof(float4));
+        h2d(d_sa.p, sa, n * 4);
+        h2d(d_sb.p, sb, n * 4);
+        bgpu::check_cuda(cudaMemsetAsync(d_status.p, 0, 4, s), "memset");
+        bgpu::run_collide_queries(W.shapes_d.p, W.hull_d.p, n, d_sa.p, d_pa.p, d_qa.p, d_sb.p, d_pb.p, d_qb.p,
+                                  seeds ? d_seed.p : nullptr, force_convex, d_out.p, d_cnt.p, d_status.p, s);
+        bgpu::check_cuda(cudaGetLastError(), "collide launch");
+        std::vector<float4> hout(size_t(n) * 8);
+        uint32_t st = 0;
+        if (n) {
+            bgpu::check_cuda(cudaMemcpyAsync(hout.data(), d_out.p, hout.size() * sizeof(float4), cudaMemcpyDeviceToHost, s),
+                             "d2h");
+            bgpu::check_cuda(cudaMemcpyAsync(counts, d_cnt.p, n * 4, cudaMemcpyDeviceToHost, s), "d2h");
+        }
+        bgpu::check_cuda(cudaMemcpyAsync(&st, d_status.p, 4, cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+        for (uint32_t i = 0; i < n; ++i) {
+            for (uint32_t k = 0; k < counts[i] && k < 4; ++k) {
+                float4 a = hout[(size_t(i) * 4 + k) * 2], b = hout[(size_t(i) * 4 + k) * 2 + 1];
+                float* o = out + (size_t(i) * 4 + k) * 7;
+                o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = b.x; o[4] = b.y; o[5] = b.z; o[6] = a.w;
+            }
+        }
+        if (st) {
+            bgpu::g_last_error = "narrow phase status bits set";
+            return BGPU_ERR_DEVICE_STATUS;
+        }
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_solve_contacts(bgpu_world* w, uint32_t n, const float* contacts, float inv_dt, float* rows_out,
+                                uint64_t* order_keys_out) {
+    if (!w || (n && !contacts) || !(inv_dt > 0.0f)) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        W.finish_stats();
+        W.sync_shapes();
+        cudaStream_t s = W.stream;
+        // Row groups: consecutive contacts of the same (body_a, body_b), at most four.
+        std::vector<uint32_t> first, cnt;
+        std::vector<uint64_t> keys;
+        for (uint32_t i = 0; i < n; ++i) {
+            uint32_t a = uint32_t(contacts[10 * size_t(i)]), b = uint32_t(contacts[10 * size_t(i) + 1]);
+            if (a >= W.n || b >= W.n || a == b) throw bgpu::InvalidArg{"contact body index out of range"};
+            uint64_t key = (uint64_t(a) << 32) | b;
+            if (!keys.empty() && keys.back() == key && cnt.back() < 4) {
+                cnt.back()++;
+            } else {
+                first.push_back(i);
+                cnt.push_back(1);
+                keys.push_back(key);
+            }
+        }
+        uint32_t G = uint32_t(keys.size());
+        W.pd.reserve(std::max<uint32_t>(G, 1), W.n, 1);
+        bgpu::DevBuf<uint32_t> d_first, d_cnt;
+        bgpu::DevBuf<float> d_c;
+        d_first.reserve(G + 1);
+        d_cnt.reserve(G + 1);
+        d_c.reserve(size_t(n) * 10 + 1);
+        W.standalone_keys.reserve(G + 1);
+        if (G) {
+            bgpu::check_cuda(cudaMemcpyAsync(d_first.p, first.data(), G * 4, cudaMemcpyHostToDevice, s), "h2d");
+            bgpu::check_cuda(cudaMemcpyAsync(d_cnt.p, cnt.data(), G * 4, cudaMemcpyHostToDevice, s), "h2d");
+            bgpu::check_cuda(cudaMemcpyAsync(W.standalone_keys.p, keys.data(), G * 8, cudaMemcpyHostToDevice, s), "h2d");
+            bgpu::check_cuda(cudaMemcpyAsync(d_c.p, contacts, size_t(n) * 10 * 4, cudaMemcpyHostToDevice, s), "h2d");
+        }
+        bgpu::check_cuda(cudaMemsetAsync(W.pd.row_count.p, 0, std::max<uint32_t>(G, 1) * 4, s), "memset");
+        bgpu::check_cuda(cudaMemsetAsync(W.push_lin.p, 0, W.n * sizeof(float4), s), "memset");
+        bgpu::check_cuda(cudaMemsetAsync(W.push_ang.p, 0, W.n * sizeof(float4), s), "memset");
+        bgpu::check_cuda(cudaMemsetAsync(W.flags.p, 0, 4, s), "memset");
+        bgpu::launch_compute_iw(W.body_dev(), W.n, s);
+        bgpu::StepParams sp;
+        sp.inv_dt = inv_dt;
+        sp.dt = 1.0f / inv_dt;
+        sp.info = W.info;
+        bgpu::run_prepare_contacts(W.body_dev(), G, d_first.p, d_cnt.p, d_c.p, W.standalone_keys.p, sp, W.pd.rows.p,
+                                   W.pd.row_count.p, s);
+        bgpu::run_solver(W.view(), W.standalone_keys.p, G, W.pd, sp, W.flags.p, s, [](int) {});
+        bgpu::check_cuda(cudaGetLastError(), "solve launch");
+        uint32_t st = 0;
+        bgpu::check_cuda(cudaMemcpyAsync(&st, W.flags.p, 4, cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+        W.solved_standalone = 1;
+        W.standalone_groups = G;
+        std::vector<uint64_t> okeys;
+        std::vector<float> rows;
+        gather_solve_order(W, G, W.standalone_keys.p, okeys, rows);
+        if (rows_out) std::memcpy(rows_out, rows.data(), rows.size() * sizeof(float));
+        if (order_keys_out) std::memcpy(order_keys_out, okeys.data(), okeys.size() * sizeof(uint64_t));
+        if (st) {
+            char buf[96];
+            std::snprintf(buf, sizeof(buf), "device status bits 0x%x", st);
+            bgpu::g_last_error = buf;
+            return BGPU_ERR_DEVICE_STATUS;
+        }
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_read_push(bgpu_world* w, float* out) {
+    if (!w || !out) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        uint32_t n = W.n;
+        std::vector<float4> pl(n), pa(n);
+        bgpu::check_cuda(cudaMemcpyAsync(pl.data(), W.push_lin.p, n * sizeof(float4), cudaMemcpyDeviceToHost, W.stream), "d2h");
+        bgpu::check_cuda(cudaMemcpyAsync(pa.data(), W.push_ang.p, n * sizeof(float4), cudaMemcpyDeviceToHost, W.stream), "d2h");
+        bgpu::check_cuda(cudaStreamSynchronize(W.stream), "sync");
+        for (uint32_t i = 0; i < n; ++i) {
+            float* o = out + 6 * size_t(i);
+            o[0] = pl[i].x; o[1] = pl[i].y; o[2] = pl[i].z; o[3] = pa[i].x; o[4] = pa[i].y; o[5] = pa[i].z;
+        }
+        return BGPU_OK;
+    });
+}
+
+}  // extern "C"

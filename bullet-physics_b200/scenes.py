@@ -1,0 +1,235 @@
+"""Seeded synthetic scenes of the five benchmark configurations.
+
+Each builder returns a plain description (shape list + per-body numpy arrays)
+that both the device world (bgpu.World) and the CPU oracle can ingest, so a
+parity check and a benchmark run start from bit-identical inputs.
+
+  falling_box_stack  1,000 boxes (half 0.5, 1 kg) on a 10x10x10 grid, 1.1 m
+                     spacing, 2 m above a ground plane, jitter U(-0.05,0.05) m
+                     and +-5 deg about a random axis; 10 iterations; 300 steps.
+  mixed_convex_pile  16,384 bodies: 40% boxes (half U(0.2,0.6)^3), 30% spheres
+                     (r U(0.2,0.5)), 15% capsules (r U(0.1,0.3), hh U(0.2,0.6)),
+                     15% hulls of 24 points on a sphere of R U(0.3,0.6);
+                     rho 1000; uniform in a 40 m cube above the ground, random
+                     orientation; 10 iterations; 300 steps.
+  large_pile         131,072 bodies (50% unit boxes half 0.5, 50% spheres
+                     r 0.5) on a jittered 64x64x32 grid, 1.05 m spacing;
+                     20 iterations; 600 steps.
+Scaled-down variants (`scale`) keep the recipe and shrink the grid.
+"""
+import math
+
+import numpy as np
+
+SPHERE, BOX, CAPSULE, HULL, PLANE = 0, 1, 2, 3, 4
+
+
+class Scene:
+    def __init__(self, name, dt, iterations, steps):
+        self.name = name
+        self.dt = dt
+        self.iterations = iterations
+        self.steps = steps
+        self.gravity = (0.0, -9.81, 0.0)
+        self.shapes = []  # (type, params list, points or None)
+        self.shape_of = []
+        self.pos = []
+        self.quat = []
+        self.linvel = []
+        self.angvel = []
+        self.mass = []
+        self.friction = []
+        self.restitution = []
+
+    def add_shape(self, kind, params=(), points=None):
+        self.shapes.append((kind, list(params), None if points is None else np.asarray(points, dtype=np.float32)))
+        return len(self.shapes) - 1
+
+    def add(self, shape, pos, quat=(0, 0, 0, 1), mass=1.0, linvel=(0, 0, 0), angvel=(0, 0, 0), friction=0.5,
+            restitution=0.0):
+        self.shape_of.append(shape)
+        self.pos.append(pos)
+        self.quat.append(quat)
+        self.linvel.append(linvel)
+        self.angvel.append(angvel)
+        self.mass.append(mass)
+        self.friction.append(friction)
+        self.restitution.append(restitution)
+
+    def arrays(self):
+        return dict(shape=np.asarray(self.shape_of, dtype=np.uint32), pos=np.asarray(self.pos, dtype=np.float32),
+                    quat=np.asarray(self.quat, dtype=np.float32), linvel=np.asarray(self.linvel, dtype=np.float32),
+                    angvel=np.asarray(self.angvel, dtype=np.float32), mass=np.asarray(self.mass, dtype=np.float32),
+                    friction=np.asarray(self.friction, dtype=np.float32),
+                    restitution=np.asarray(self.restitution, dtype=np.float32))
+
+    @property
+    def num_bodies(self):
+        return len(self.shape_of)
+
+    @property
+    def num_dynamic(self):
+        return int(np.count_nonzero(np.asarray(self.mass) > 0))
+
+    def build_gpu(self, bgpu_module, **solver):
+        w = bgpu_module.World(gravity=self.gravity, num_iterations=self.iterations, **solver)
+        for kind, params, pts in self.shapes:
+            w.add_shape(kind, params, pts)
+        a = self.arrays()
+        w.add_bodies_array(a["shape"], a["pos"], a["quat"], a["linvel"], a["angvel"], a["mass"], a["friction"],
+                           a["restitution"])
+        return w
+
+    def build_oracle(self, oracle_module, precision="f32", **solver):
+        w = oracle_module.OracleWorld(precision)
+        w.set_gravity(self.gravity)
+        w.set_solver(num_iterations=self.iterations, **solver)
+        for kind, params, pts in self.shapes:
+            w.add_shape(kind, params, pts)
+        a = self.arrays()
+        for i in range(self.num_bodies):
+            w.add_body(int(a["shape"][i]), a["pos"][i].astype(np.float64), quat=a["quat"][i].astype(np.float64),
+                       linvel=a["linvel"][i].astype(np.float64), angvel=a["angvel"][i].astype(np.float64),
+                       mass=float(a["mass"][i]), friction=float(a["friction"][i]),
+                       restitution=float(a["restitution"][i]))
+        return w
+
+
+def random_quat_small(rng, max_deg):
+    axis = rng.normal(size=3)
+    axis /= np.linalg.norm(axis)
+    ang = math.radians(rng.uniform(-max_deg, max_deg))
+    s = math.sin(ang / 2)
+    q = np.array([axis[0] * s, axis[1] * s, axis[2] * s, math.cos(ang / 2)], dtype=np.float32)
+    return q / np.linalg.norm(q)
+
+
+def random_quat(rng):
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    if q[3] < 0:
+        q = -q
+    return q.astype(np.float32)
+
+
+def falling_box_stack(nx=10, ny=10, nz=10, seed=1, steps=300):
+    """Config 1: box grid over a ground plane (10 iterations, dt 1/60)."""
+    rng = np.random.default_rng(seed)
+    s = Scene(f"falling_box_stack_{nx}x{ny}x{nz}", 1.0 / 60.0, 10, steps)
+    plane = s.add_shape(PLANE, [0.0, 1.0, 0.0, 0.0])
+    box = s.add_shape(BOX, [0.5, 0.5, 0.5])
+    s.add(plane, (0.0, 0.0, 0.0), mass=0.0)
+    sp = 1.1
+    for j in range(ny):
+        for i in range(nx):
+            for k in range(nz):
+                p = np.array([(i - (nx - 1) / 2) * sp, 2.0 + j * sp, (k - (nz - 1) / 2) * sp])
+                p = p + rng.uniform(-0.05, 0.05, size=3)
+                s.add(box, tuple(p.astype(np.float32)), random_quat_small(rng, 5.0), mass=1.0, friction=0.5)
+    return s
+
+
+def fibonacci_free_points(rng, n, radius):
+    v = rng.normal(size=(n, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    return (v * radius).astype(np.float32)
+
+
+def hull_volume(points):
+    from scipy.spatial import ConvexHull  # scene generation only
+
+    return float(ConvexHull(points).volume)
+
+
+def mixed_convex_pile(n=16384, seed=2, steps=300, extent=40.0):
+    """Config 2: boxes/spheres/capsules/hulls at rho 1000, uniform in a cube above the ground."""
+    rng = np.random.default_rng(seed)
+    s = Scene(f"mixed_convex_pile_{n}", 1.0 / 60.0, 10, steps)
+    plane = s.add_shape(PLANE, [0.0, 1.0, 0.0, 0.0])
+    s.add(plane, (0.0, 0.0, 0.0), mass=0.0)
+    rho = 1000.0
+    kinds = rng.choice(4, size=n, p=[0.4, 0.3, 0.15, 0.15])
+    for t in range(n):
+        kind = kinds[t]
+        if kind == 0:
+            h = rng.uniform(0.2, 0.6, size=3)
+            sh = s.add_shape(BOX, list(h))
+            mass = rho * 8.0 * h[0] * h[1] * h[2]
+        elif kind == 1:
+            r = rng.uniform(0.2, 0.5)
+            sh = s.add_shape(SPHERE, [r])
+            mass = rho * 4.0 / 3.0 * math.pi * r ** 3
+        elif kind == 2:
+            r = rng.uniform(0.1, 0.3)
+            hh = rng.uniform(0.2, 0.6)
+            sh = s.add_shape(CAPSULE, [r, hh])
+            mass = rho * (math.pi * r * r * 2.0 * hh + 4.0 / 3.0 * math.pi * r ** 3)
+        else:
+            R = rng.uniform(0.3, 0.6)
+            pts = fibonacci_free_points(rng, 24, R)
+            sh = s.add_shape(HULL, [], pts)
+            mass = rho * hull_volume(pts)
+        p = (rng.uniform(-extent / 2, extent / 2), rng.uniform(1.0, 1.0 + extent), rng.uniform(-extent / 2, extent / 2))
+        s.add(sh, p, random_quat(rng), mass=float(mass))
+    return s
+
+
+def large_pile(nx=64, nz=64, ny=32, seed=3, steps=600, spacing=1.05):
+    """Config 3: 50% unit boxes / 50% r-0.5 spheres on a jittered grid (20 iterations)."""
+    rng = np.random.default_rng(seed)
+    s = Scene(f"large_pile_{nx}x{nz}x{ny}", 1.0 / 60.0, 20, steps)
+    plane = s.add_shape(PLANE, [0.0, 1.0, 0.0, 0.0])
+    box = s.add_shape(BOX, [0.5, 0.5, 0.5])
+    sph = s.add_shape(SPHERE, [0.5])
+    s.add(plane, (0.0, 0.0, 0.0), mass=0.0)
+    n = nx * ny * nz
+    is_box = rng.random(n) < 0.5
+    jit = rng.uniform(-0.02, 0.02, size=(n, 3))
+    t = 0
+    for j in range(ny):
+        for i in range(nx):
+            for k in range(nz):
+                p = np.array([(i - (nx - 1) / 2) * spacing, 0.6 + j * spacing, (k - (nz - 1) / 2) * spacing]) + jit[t]
+                if is_box[t]:
+                    s.add(box, tuple(p.astype(np.float32)), random_quat_small(rng, 5.0), mass=1.0)
+                else:
+                    s.add(sph, tuple(p.astype(np.float32)), mass=1.0)
+                t += 1
+    return s
+
+
+def large_pile_arrays(nx=64, nz=64, ny=32, seed=3, spacing=1.05):
+    """Vectorised builder of the same recipe as large_pile (fast for 131k bodies)."""
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nz
+    is_box = rng.random(n) < 0.5
+    jit = rng.uniform(-0.02, 0.02, size=(n, 3))
+    j, i, k = np.meshgrid(np.arange(ny), np.arange(nx), np.arange(nz), indexing="ij")
+    base = np.stack([(i.ravel() - (nx - 1) / 2) * spacing, 0.6 + j.ravel() * spacing,
+                     (k.ravel() - (nz - 1) / 2) * spacing], axis=1)
+    pos = (base + jit).astype(np.float32)
+    axis = rng.normal(size=(n, 3))
+    axis /= np.linalg.norm(axis, axis=1, keepdims=True)
+    ang = np.radians(rng.uniform(-5.0, 5.0, size=n))
+    quat = np.concatenate([axis * np.sin(ang / 2)[:, None], np.cos(ang / 2)[:, None]], axis=1).astype(np.float32)
+    quat[~is_box] = [0, 0, 0, 1]
+    quat /= np.linalg.norm(quat, axis=1, keepdims=True)
+    return is_box, pos, quat
+
+
+def large_pile_fast(nx=64, nz=64, ny=32, seed=3, steps=600, spacing=1.05):
+    s = Scene(f"large_pile_{nx}x{nz}x{ny}", 1.0 / 60.0, 20, steps)
+    plane = s.add_shape(PLANE, [0.0, 1.0, 0.0, 0.0])
+    box = s.add_shape(BOX, [0.5, 0.5, 0.5])
+    sph = s.add_shape(SPHERE, [0.5])
+    is_box, pos, quat = large_pile_arrays(nx, nz, ny, seed, spacing)
+    n = len(pos)
+    s.shape_of = [plane] + list(np.where(is_box, box, sph))
+    s.pos = [(0.0, 0.0, 0.0)] + list(map(tuple, pos))
+    s.quat = [(0, 0, 0, 1)] + list(map(tuple, quat))
+    s.linvel = [(0, 0, 0)] * (n + 1)
+    s.angvel = [(0, 0, 0)] * (n + 1)
+    s.mass = [0.0] + [1.0] * n
+    s.friction = [0.5] * (n + 1)
+    s.restitution = [0.0] * (n + 1)
+    return s

@@ -1,0 +1,196 @@
+/*
+ * bgpu — B200-native rigid-body step, C ABI.
+ *
+ * Drop-in for the discrete-dynamics step of the Rust crates bullet-collision /
+ * bullet-dynamics (CrazyboyQCD/bullet-physics). A world object owns all device
+ * memory; caller buffers are borrowed for the duration of a call. One CUDA
+ * stream per world; calls on one world are not thread-safe. Every call returns
+ * a bgpu_status; bgpu_last_error() describes the last failure on the calling
+ * thread.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   PhysicsWorld::new / with_broadphase      crates/bullet-dynamics/src/world.rs:406-463
+ *   PhysicsWorld::set_gravity                crates/bullet-dynamics/src/world.rs:467-481
+ *   PhysicsWorld::solver_info_mut            crates/bullet-dynamics/src/world.rs:956
+ *   PhysicsWorld::add_body                   crates/bullet-dynamics/src/world.rs:524-563
+ *   RigidBody::new_dynamic / new_static /    crates/bullet-dynamics/src/body.rs:388-499
+ *     new_kinematic
+ *   PhysicsWorld::step_simulation            crates/bullet-dynamics/src/world/step.rs:100-108
+ *   PhysicsWorld::step_simulation_fixed      crates/bullet-dynamics/src/world/step.rs:136-199
+ *   PhysicsWorld::body / body_mut            crates/bullet-dynamics/src/world.rs:566-598
+ *   BroadPhase::compute_pairs_into           crates/bullet-collision/src/broadphase/mod.rs:94-130
+ *   narrowphase::collide_seeded              crates/bullet-collision/src/narrowphase/mod.rs:63-286
+ *   sequential_impulse::solve                crates/bullet-dynamics/src/solver/sequential_impulse.rs:692-705
+ *   StepTimings                              crates/bullet-dynamics/src/timing.rs:20-117
+ *   C-ABI handle pattern (demo_new/free/step) tools/wasm-demo/src/lib.rs:407-486
+ */
+#ifndef BGPU_H
+#define BGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t bgpu_status;
+#define BGPU_OK 0
+#define BGPU_ERR_INVALID_ARGUMENT 1
+#define BGPU_ERR_CAPACITY 2
+#define BGPU_ERR_CUDA 3
+#define BGPU_ERR_DEVICE_STATUS 4 /* a kernel left a bounded loop or overflowed a fixed buffer */
+#define BGPU_ERR_NO_DEVICE 5
+
+/* Shape kinds (crates/bullet-collision/src/shapes/mod.rs:61-85, convex subset + plane). */
+#define BGPU_SHAPE_SPHERE 0  /* params: radius */
+#define BGPU_SHAPE_BOX 1     /* params: half extents x, y, z */
+#define BGPU_SHAPE_CAPSULE 2 /* params: radius, half height (segment along local Y) */
+#define BGPU_SHAPE_HULL 3    /* hull_points: n x 3 floats (must be convex) */
+#define BGPU_SHAPE_PLANE 4   /* params: normal x, y, z, constant (static bodies only) */
+
+/* Body flags (crates/bullet-dynamics/src/body.rs:204-252). */
+#define BGPU_BODY_NO_CONTACT_RESPONSE 0x1u
+#define BGPU_BODY_DISABLE_WORLD_GRAVITY 0x2u
+#define BGPU_BODY_KINEMATIC 0x4u
+#define BGPU_BODY_ADDITIONAL_DAMPING 0x10u
+
+/* Activation states (crates/bullet-dynamics/src/body.rs:140-153). */
+#define BGPU_ACTIVE 1u
+#define BGPU_ISLAND_SLEEPING 2u
+#define BGPU_WANTS_DEACTIVATION 3u
+#define BGPU_DISABLE_DEACTIVATION 4u
+#define BGPU_DISABLE_SIMULATION 5u
+
+/* Contact subset of SolverInfo (crates/bullet-dynamics/src/solver/info.rs:24-107). */
+typedef struct bgpu_solver_info {
+    float erp2;                                /* 0.2 */
+    float linear_slop;                         /* 0.005 */
+    float restitution_velocity_threshold;      /* 1.0 */
+    uint32_t split_impulse;                    /* 1 */
+    float split_impulse_penetration_threshold; /* -0.04 */
+    float split_impulse_turn_erp;              /* 0.1 */
+    float warmstarting_factor;                 /* 0.85 */
+    float global_cfm;                          /* 0.0 */
+    float sor;                                 /* 1.0 */
+    uint32_t num_iterations;                   /* 10 */
+} bgpu_solver_info;
+
+/* RigidBody construction parameters (body.rs:388-499). mass == 0 builds a static
+ * body (new_static); the KINEMATIC flag builds new_kinematic. Zero sleeping
+ * thresholds select the defaults 0.8 / 1.0; activation 0 selects the default. */
+typedef struct bgpu_body_desc {
+    uint32_t shape;
+    float position[3];
+    float orientation[4]; /* x, y, z, w */
+    float linear_velocity[3];
+    float angular_velocity[3];
+    float mass;
+    float friction;    /* default 0.5 */
+    float restitution; /* default 0.0 */
+    float linear_damping;
+    float angular_damping;
+    uint32_t flags;
+    uint16_t group; /* default 1 */
+    uint16_t mask;  /* default 0xFFFF */
+    uint32_t activation;
+    float linear_sleeping_threshold;
+    float angular_sleeping_threshold;
+} bgpu_body_desc;
+
+/* Counters of the last step, and timing sums over the steps run since timing
+ * was (re)enabled: the seven StepTimings stages (timing.rs:20-47), the PGS
+ * kernel alone, and whole steps, all in ms of device time on the world's stream. */
+typedef struct bgpu_step_stats {
+    uint32_t num_bodies;
+    uint32_t num_pairs;          /* broad-phase pairs */
+    uint32_t num_contact_pairs;  /* pairs that emitted solver rows */
+    uint32_t num_contacts;       /* solver rows */
+    uint32_t num_colours;        /* PGS batches */
+    uint32_t num_detect;         /* pairs that ran the narrow phase */
+    uint32_t num_manifolds;      /* persistent manifolds after the step */
+    uint32_t device_status;      /* or of the kernels' status bits (0 = clean) */
+    uint32_t num_split_pairs;    /* row groups with split-impulse rows */
+    uint32_t timed_steps;        /* steps in the sums below */
+    float stage_ms[7];           /* integrate velocities, update aabbs, broadphase, islands,
+                                    narrowphase, solve, integrate positions */
+    float solve_kernel_ms;       /* the PGS kernel only (inside the solve stage) */
+    float step_ms;
+} bgpu_step_stats;
+
+typedef struct bgpu_world bgpu_world;
+
+void bgpu_solver_info_default(bgpu_solver_info* out);
+void bgpu_body_desc_default(bgpu_body_desc* out);
+
+/* Library and device probes. */
+const char* bgpu_version(void);
+int bgpu_device_count(void);
+size_t bgpu_last_error(char* buf, size_t len);
+
+/* World lifetime (PhysicsWorld::new; world.rs:406-463). gravity may be NULL (0, -9.81, 0). */
+bgpu_status bgpu_world_create(const bgpu_solver_info* info, const float* gravity, bgpu_world** out);
+void bgpu_world_destroy(bgpu_world* w);
+bgpu_status bgpu_world_set_gravity(bgpu_world* w, const float* gravity);
+bgpu_status bgpu_world_set_solver_info(bgpu_world* w, const bgpu_solver_info* info);
+
+/* Shapes and bodies (world.rs:524-563). */
+bgpu_status bgpu_add_shape(bgpu_world* w, uint32_t type, const float* params, const float* hull_points,
+                           uint32_t num_hull_points, uint32_t* out_shape);
+bgpu_status bgpu_add_bodies(bgpu_world* w, uint32_t n, const bgpu_body_desc* descs, uint32_t* out_first);
+uint32_t bgpu_num_bodies(const bgpu_world* w);
+
+/* The step (step.rs:100-199). bgpu_step runs step_simulation(dt) nsteps times. */
+bgpu_status bgpu_step(bgpu_world* w, float dt, uint32_t nsteps);
+bgpu_status bgpu_step_simulation_fixed(bgpu_world* w, float dt, uint32_t max_sub_steps, float fixed_dt,
+                                       uint32_t* out_substeps);
+/* bgpu_step with device timing: *device_ms is the event-measured time on the
+ * world's stream from before the first step to after the last one. */
+bgpu_status bgpu_step_timed(bgpu_world* w, float dt, uint32_t nsteps, float* device_ms);
+
+/* Body access (body / body_mut). State layout per body: pos3, quat4, linvel3,
+ * angvel3, activation, deactivation time = 15 floats. Poses: pos3 + quat4. */
+bgpu_status bgpu_read_state(bgpu_world* w, float* state);
+bgpu_status bgpu_write_state(bgpu_world* w, const float* state);
+bgpu_status bgpu_read_poses(bgpu_world* w, float* poses);
+/* Accumulated force / torque per body (n x 3 each, either may be NULL);
+ * cleared by the next step like RigidBody::clear_forces (step.rs:1272). */
+bgpu_status bgpu_apply_forces(bgpu_world* w, const float* force, const float* torque);
+
+/* Results of the last step, for inspection and parity checks.
+ * Pairs: n x (lo, hi), lexicographic. Contacts: rows in solve order, 18 floats each:
+ * body_a, body_b, point index, normal3, r_a3, r_b3, penetration, normal impulse,
+ * tangent1 impulse, tangent2 impulse, push impulse, split flag.
+ * Solve order: pair keys (lo << 32 | hi) in the order their rows were solved. */
+bgpu_status bgpu_read_pairs(bgpu_world* w, uint32_t* pairs, uint64_t cap, uint64_t* out_n);
+bgpu_status bgpu_read_contacts(bgpu_world* w, float* rows, uint64_t cap, uint64_t* out_n);
+bgpu_status bgpu_read_solve_order(bgpu_world* w, uint64_t* keys, uint64_t cap, uint64_t* out_n);
+bgpu_status bgpu_get_stats(bgpu_world* w, bgpu_step_stats* out);
+/* Turns per-stage timing on (resetting the sums) or off. */
+bgpu_status bgpu_enable_step_timing(bgpu_world* w, int on);
+
+/* Stand-alone stages on caller data (parity harness entry points).
+ * Broad phase: aabbs n x 6 (min3, max3) -> the closed-overlap pairs (i < j),
+ * lexicographic; writes up to cap pairs and returns the count. */
+bgpu_status bgpu_broadphase_pairs(const float* aabbs, uint32_t n, uint32_t* pairs, uint64_t cap, uint64_t* out_n);
+/* Narrow phase on this world's shapes: per query shape_a/pose_a (pos3 quat4) vs
+ * shape_b/pose_b; seeds n x 3 or NULL; out n x 4 x 7 (pos3, normal3, penetration),
+ * counts n. force_convex != 0 routes every pair through GJK/EPA (convex_convex.rs:30). */
+bgpu_status bgpu_collide(bgpu_world* w, uint32_t n, const uint32_t* shape_a, const float* pose_a,
+                         const uint32_t* shape_b, const float* pose_b, const float* seeds, int force_convex,
+                         float* out, uint32_t* counts);
+/* Solver on this world's bodies: contacts n x 10 (body_a, body_b, pos3, normal3,
+ * penetration, warm-start impulse); consecutive contacts of the same body pair form
+ * one row group. Body velocities and push velocities are updated in place; the
+ * rows (18 floats, as bgpu_read_contacts) come back in solve order, and the group
+ * keys (body_a << 32 | body_b) in the order the groups were solved. */
+bgpu_status bgpu_solve_contacts(bgpu_world* w, uint32_t n, const float* contacts, float inv_dt, float* rows_out,
+                                uint64_t* order_keys_out);
+/* Push velocities (n x 6: push_lin3, push_ang3) left by the last solve. */
+bgpu_status bgpu_read_push(bgpu_world* w, float* push);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BGPU_H */

@@ -175,7 +175,8 @@ void pairs_impl(const double* aabbs, uint32_t n, int method, std::vector<std::pa
         a[i] = Aabb<R>(V3<R>(static_cast<R>(p[0]), static_cast<R>(p[1]), static_cast<R>(p[2])), V3<R>(static_cast<R>(p[3]), static_cast<R>(p[4]), static_cast<R>(p[5])));
     }
     if (method == 0) brute_force_pairs(a, out);
-    else sweep_pairs(a, out);
+    else if (method == 1) sweep_pairs(a, out);
+    else grid_pairs(a, out);
 }
 
 // Contacts layout for a standalone solve (doubles): body_a, body_b, pos3, normal3,
@@ -365,6 +366,11 @@ void orc_world_set_solve_order(void* p, const uint64_t* keys, uint32_t n) {
     DISPATCH(h, { w.solve_order.assign(keys, keys + n); });
 }
 
+void orc_world_stage_seconds(void* p, double* out7) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, { for (int k = 0; k < 7; ++k) out7[k] = w.stage_s[k]; });
+}
+
 int orc_collide(void* p, uint32_t sa, const double* pose_a, uint32_t sb, const double* pose_b, const double* seed,
                 double* out) {
     Handle* h = static_cast<Handle*>(p);
@@ -393,7 +399,7 @@ void orc_solve_contacts(void* p, const double* contacts, uint32_t n, double inv_
     DISPATCH(h, { solve_impl(w, contacts, n, inv_dt, out_rows); });
 }
 
-// Pairs of an AABB set (n x [min3, max3]); method 0 = brute force, 1 = sweep.
+// Pairs of an AABB set (n x [min3, max3]); method 0 = brute force, 1 = sweep, 2 = grid.
 // Returns the pair count; writes up to cap pairs.
 uint64_t orc_pairs(int f64, const double* aabbs, uint32_t n, int method, uint32_t* out, uint64_t cap) {
     std::vector<std::pair<uint32_t, uint32_t>> pr;

@@ -5,6 +5,8 @@
 // (bullet-dynamics/src/island.rs, world/islands.rs) and the rigid subset of
 // the step pipeline (bullet-dynamics/src/world/step.rs:281-1287).
 #pragma once
+#include <chrono>
+#include <cstring>
 #include <map>
 #include <unordered_map>
 #include "oracle_narrow.hpp"
@@ -12,6 +14,18 @@
 namespace oracle {
 
 // ------------------------------------------------------------ manifold.rs
+// IEEE total order of f32/f64::total_cmp as a signed integer key.
+inline int64_t total_order_key(double v) {
+    int64_t b;
+    std::memcpy(&b, &v, sizeof(b));
+    return b ^ int64_t(uint64_t(b >> 63) >> 1);
+}
+inline int64_t total_order_key(float v) {
+    int32_t b;
+    std::memcpy(&b, &v, sizeof(b));
+    return int64_t(b ^ int32_t(uint32_t(b >> 31) >> 1));
+}
+
 template <class R>
 struct PersistentPoint {  // manifold.rs:124-142
     V3<R> local_a, local_b, normal;
@@ -98,8 +112,9 @@ struct PersistentManifold {  // manifold.rs:168-386
         }
         if (points.size() > 4) {
             // Stable descending sort by penetration (Rust sort_by + total_cmp).
-            std::stable_sort(points.begin(), points.end(),
-                             [](const PersistentPoint<R>& a, const PersistentPoint<R>& b) { return a.penetration > b.penetration; });
+            std::stable_sort(points.begin(), points.end(), [](const PersistentPoint<R>& a, const PersistentPoint<R>& b) {
+                return total_order_key(a.penetration) > total_order_key(b.penetration);
+            });
             points.resize(4);
         }
         detect_pos_a = pa; detect_ori_a = qa; detect_pos_b = pb; detect_ori_b = qb;
@@ -491,6 +506,94 @@ void sweep_pairs(const std::vector<Aabb<R>>& aabbs, std::vector<std::pair<uint32
     for (uint64_t k : keys) out.push_back({uint32_t(k >> 32), uint32_t(k & 0xffffffffu)});
 }
 
+// Uniform-grid pair finder with the same output contract as brute_force_pairs:
+// bounded proxies are hashed by their min corner into cells no smaller than the
+// largest proxy extent, so each overlapping pair meets in adjacent cells; proxies
+// larger than 1e15 (planes) are tested against everything. Exact 3-axis closed
+// overlap filter, lexicographic output.
+template <class R>
+void grid_pairs(const std::vector<Aabb<R>>& aabbs, std::vector<std::pair<uint32_t, uint32_t>>& out) {
+    out.clear();
+    const size_t n = aabbs.size();
+    std::vector<uint32_t> big, small;
+    R cell = 0;
+    V3<R> lo = V3<R>::splat(std::numeric_limits<R>::infinity());
+    for (size_t i = 0; i < n; ++i) {
+        const Aabb<R>& a = aabbs[i];
+        R ex = std::max(std::max(a.max.x - a.min.x, a.max.y - a.min.y), a.max.z - a.min.z);
+        if (!(ex < R(1e15))) { big.push_back(uint32_t(i)); continue; }
+        small.push_back(uint32_t(i));
+        cell = std::max(cell, ex);
+        lo = lo.min(a.min);
+    }
+    std::vector<uint64_t> keys;
+    if (!small.empty()) {
+        if (!(cell > R(0))) cell = R(1);
+        auto coord = [&](R v, R l) { return int64_t(std::floor(double(v - l) / double(cell))); };
+        // cell key -> bucket (sorted vector of (cell, body))
+        std::vector<std::pair<uint64_t, uint32_t>> cells;
+        cells.reserve(small.size());
+        auto pack = [](int64_t x, int64_t y, int64_t z) {
+            return (uint64_t(x & 0x1FFFFF) << 42) | (uint64_t(y & 0x1FFFFF) << 21) | uint64_t(z & 0x1FFFFF);
+        };
+        for (uint32_t i : small) {
+            const Aabb<R>& a = aabbs[i];
+            cells.push_back({pack(coord(a.min.x, lo.x), coord(a.min.y, lo.y), coord(a.min.z, lo.z)), i});
+        }
+        std::sort(cells.begin(), cells.end());
+        // Open-addressed table: cell key -> [first, last) run in `cells`.
+        size_t cap = 16;
+        int bits = 4;
+        while (cap < 2 * cells.size()) { cap <<= 1; ++bits; }
+        std::vector<uint64_t> tkey(cap, ~0ull);
+        std::vector<uint32_t> tbeg(cap, 0), tend(cap, 0);
+        auto slot_of = [&](uint64_t k) {
+            uint64_t h = k * 0x9E3779B97F4A7C15ull;  // Fibonacci hashing: keep the top bits
+            return size_t(h >> (64 - bits));
+        };
+        for (size_t r = 0; r < cells.size();) {
+            size_t e = r;
+            while (e < cells.size() && cells[e].first == cells[r].first) ++e;
+            size_t sl = slot_of(cells[r].first);
+            while (tkey[sl] != ~0ull) sl = (sl + 1) & (cap - 1);
+            tkey[sl] = cells[r].first;
+            tbeg[sl] = uint32_t(r);
+            tend[sl] = uint32_t(e);
+            r = e;
+        }
+        for (uint32_t i : small) {
+            const Aabb<R>& a = aabbs[i];
+            int64_t cx = coord(a.min.x, lo.x), cy = coord(a.min.y, lo.y), cz = coord(a.min.z, lo.z);
+            for (int64_t dx = -1; dx <= 1; ++dx)
+                for (int64_t dy = -1; dy <= 1; ++dy)
+                    for (int64_t dz = -1; dz <= 1; ++dz) {
+                        if (cx + dx < 0 || cy + dy < 0 || cz + dz < 0) continue;
+                        uint64_t key = pack(cx + dx, cy + dy, cz + dz);
+                        size_t sl = slot_of(key);
+                        while (tkey[sl] != ~0ull && tkey[sl] != key) sl = (sl + 1) & (cap - 1);
+                        if (tkey[sl] != key) continue;
+                        for (uint32_t t = tbeg[sl]; t < tend[sl]; ++t) {
+                            uint32_t j = cells[t].second;
+                            if (j > i && a.overlaps(aabbs[j])) keys.push_back((uint64_t(i) << 32) | j);
+                        }
+                    }
+        }
+    }
+    for (uint32_t h : big)
+        for (size_t j = 0; j < n; ++j) {
+            if (j == h) continue;
+            bool other_big = std::binary_search(big.begin(), big.end(), uint32_t(j));
+            if (other_big && j < h) continue;  // a big-big pair is emitted once, from the smaller index
+            if (aabbs[h].overlaps(aabbs[j])) {
+                uint32_t a = std::min<uint32_t>(h, uint32_t(j)), b = std::max<uint32_t>(h, uint32_t(j));
+                keys.push_back((uint64_t(a) << 32) | b);
+            }
+        }
+    std::sort(keys.begin(), keys.end());
+    out.reserve(keys.size());
+    for (uint64_t k : keys) out.push_back({uint32_t(k >> 32), uint32_t(k & 0xffffffffu)});
+}
+
 // ------------------------------------------------------------ world
 inline uint64_t pair_key(uint32_t a, uint32_t b) {
     uint32_t lo = std::min(a, b), hi = std::max(a, b);
@@ -519,6 +622,18 @@ struct World {
     std::vector<ContactConstraint<R>> last_rows_pre; // prepared rows, in solve order, before the solve
     std::vector<V3<R>> last_predicted;
     uint32_t last_narrowphase_calls = 0;
+
+    // timing.rs:20-47 StepTimings: cumulative seconds per stage (integrate
+    // velocities, update aabbs, broadphase, islands, narrowphase, solve,
+    // integrate positions).
+    double stage_s[7] = {0, 0, 0, 0, 0, 0, 0};
+    std::chrono::steady_clock::time_point clk_;
+    void clk_start() { clk_ = std::chrono::steady_clock::now(); }
+    void clk_mark(int stage) {
+        auto t = std::chrono::steady_clock::now();
+        stage_s[stage] += std::chrono::duration<double>(t - clk_).count();
+        clk_ = t;
+    }
 
     // world.rs:524-563 (add_body: gravity inheritance + padded proxy AABB)
     uint32_t add_body(Body<R> b) {
@@ -607,6 +722,7 @@ struct World {
     // world/step.rs:281-1287, rigid subset (no joints, multibodies, soft bodies,
     // events, CCD, motion states).
     void step(R dt) {
+        clk_start();
         R inv_dt = R(1) / dt;
         size_t n = bodies.size();
         // 1. settled speeds, then integrate velocities (step.rs:306-314)
@@ -614,6 +730,7 @@ struct World {
         for (size_t i = 0; i < n; ++i)
             settled[i] = bodies[i].linear_velocity.length_squared() + bodies[i].angular_velocity.length_squared();
         for (auto& b : bodies) b.integrate_velocities(dt);
+        clk_mark(0);
         // 2. predicted positions (step.rs:341-343)
         std::vector<V3<R>> pred(n);
         for (size_t i = 0; i < n; ++i) pred[i] = bodies[i].predicted_position(dt);
@@ -623,12 +740,15 @@ struct World {
             proxy_aabbs[i] = shapes[bodies[i].shape].world_aabb(pred[i], bodies[i].orientation)
                                  .expanded(CONTACT_BREAKING_THRESHOLD<R>);
         }
+        clk_mark(1);
         // 4. broad phase (step.rs:413-415)
         std::vector<std::pair<uint32_t, uint32_t>> pairs;
         if (brute_force_broadphase) brute_force_pairs(proxy_aabbs, pairs);
-        else sweep_pairs(proxy_aabbs, pairs);
+        else grid_pairs(proxy_aabbs, pairs);
+        clk_mark(2);
         // 4b. islands (step.rs:423)
         step_islands(pairs);
+        clk_mark(3);
         // 5. pair pass (step.rs:439-854)
         step_counter += 1;
         bool simulate = false;
@@ -692,6 +812,7 @@ struct World {
             });
         }
         last_rows_pre = rows;
+        clk_mark(4);
         // 6. solve (step.rs:959-972)
         solve(bodies, rows, inv_dt, info);
         // 6b. impulse writeback + prune (step.rs:982-1010)
@@ -706,6 +827,7 @@ struct World {
                 else ++ci;
             }
         }
+        clk_mark(5);
         // 6c. deactivation (step.rs:1059-1061)
         for (auto& b : bodies) b.update_deactivation(dt);
         // 7. integrate positions + split-impulse push (step.rs:1171-1215)
@@ -732,6 +854,7 @@ struct World {
         last_pairs = pairs;
         last_rows = rows;
         last_predicted = pred;
+        clk_mark(6);
     }
 };
 

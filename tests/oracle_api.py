@@ -54,6 +54,7 @@ def lib():
             "orc_world_narrowphase_calls": (U32, [P]),
             "orc_world_num_manifolds": (U32, [P]),
             "orc_world_set_solve_order": (None, [P, ctypes.POINTER(ctypes.c_uint64), U32]),
+            "orc_world_stage_seconds": (None, [P, D]),
             "orc_collide": (ctypes.c_int, [P, U32, D, U32, D, D, D]),
             "orc_gjk_kind": (ctypes.c_int, [P, U32, D, U32, D]),
             "orc_convex_convex": (ctypes.c_int, [P, U32, D, U32, D, D]),
@@ -221,6 +222,11 @@ class OracleWorld:
 
     def num_manifolds(self):
         return self.L.orc_world_num_manifolds(self.h)
+
+    def stage_seconds(self):
+        out = np.zeros(7)
+        self.L.orc_world_stage_seconds(self.h, dptr(out))
+        return out
 
     def set_solve_order(self, keys):
         k = np.ascontiguousarray(keys, dtype=np.uint64)

@@ -501,9 +501,14 @@ def test_broadphase_contract_closed_bounds_and_order():
 
 
 @pytest.mark.parametrize("seed", range(4))
-def test_sweep_matches_brute_force_dense_sets(seed):
+def test_sweep_and_grid_match_brute_force_dense_sets(seed):
     a = ref_scattered_boxes(0xDB4E7F4A7C150001 ^ ((seed * 0x517CC1B727220A95) & 0xFFFFFFFFFFFFFFFF), 512, 300, 300)
-    np.testing.assert_array_equal(oracle_pairs(a, 0), oracle_pairs(a, 1))
+    bf = oracle_pairs(a, 0)
+    np.testing.assert_array_equal(bf, oracle_pairs(a, 1))
+    np.testing.assert_array_equal(bf, oracle_pairs(a, 2))
+    big = np.array([[-1e30, -1e30, -1e30, 1e30, 1e30, 1e30]], dtype=np.float32)
+    b = np.concatenate([a[:100], big, a[100:], big], axis=0)
+    np.testing.assert_array_equal(oracle_pairs(b, 0), oracle_pairs(b, 2))
 
 
 # ------------------------------------------------------------------ world-level
