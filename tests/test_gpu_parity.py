@@ -160,8 +160,12 @@ def _solver_scene(rng, nbodies=120, ngroups=400):
                            v=rng.normal(size=3), w=rng.normal(size=3), mass=0.0 if static else rng.uniform(0.5, 3.0),
                            mu=rng.uniform(0.2, 0.9), e=rng.uniform(0.0, 0.5)))
     contacts = []
+    used = set()
     for g in range(ngroups):
         a, b = rng.choice(nbodies, size=2, replace=False)
+        while (int(a), int(b)) in used:  # unique (body_a, body_b) keys: one row group each
+            a, b = rng.choice(nbodies, size=2, replace=False)
+        used.add((int(a), int(b)))
         n = np.array([0.0, 1.0, 0.0]) + rng.normal(size=3) * 0.3
         n /= np.linalg.norm(n)
         for k in range(int(rng.integers(1, 5))):
