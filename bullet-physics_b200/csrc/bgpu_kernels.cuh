@@ -17,6 +17,7 @@ struct CudaError {
 };
 
 void check_cuda(cudaError_t e, const char* where);  // throws CudaError
+void set_last_error(const std::string& msg);         // text returned by bgpu_last_error
 
 template <class T>
 struct DevBuf {

@@ -357,3 +357,220 @@ uint64_t Broadphase::run(const float4* aabb_min, const float4* aabb_max, uint32_
 }
 
 }  // namespace bgpu
+
+// ---------------------------------------------------------------- allocation-free entry point
+//
+// For callers that cannot allocate device memory while they run: game and robotics
+// loops with a fixed device-memory budget, code running inside another runtime
+// that owns the allocator, or callers on a hard deadline that cannot afford a
+// cudaMalloc / cudaFree round trip (both may synchronise the device). They pass
+// device buffers for the input AABBs and the output pairs; every scratch array
+// of the broad phase lives in one fixed file-scope device array instead.
+//
+// Limits: at most BGPU_NOALLOC_MAX_PROXIES proxies and BGPU_NOALLOC_MAX_UNBOUNDED
+// unbounded proxies (extent >= 1e15, e.g. planes); larger inputs are rejected.
+// The array is shared by every call in the process and keeps the last call's
+// contents, so two calls that overlap on the GPU (different streams, or
+// different host threads) race on it and must be serialised by the caller.
+// Each GPU that loads the library holds the array until the process exits.
+#include <mutex>
+#include "../../include/bgpu.h"
+
+namespace bgpu {
+namespace {
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(24) << 20;
+static __device__ __align__(256) unsigned char g_bp_scratch[NOALLOC_SCRATCH_BYTES];
+
+std::mutex g_bp_scratch_mutex;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+unsigned char* g_bp_scratch_addr[NOALLOC_MAX_DEVICES] = {};
+
+// Device address of the scratch array for the current device. In host code the
+// array's name is only a stand-in, so the address comes from the runtime, once
+// per device (the first call on a device does this lookup).
+unsigned char* noalloc_scratch_address(int dev) {
+    std::lock_guard<std::mutex> lock(g_bp_scratch_mutex);
+    if (!g_bp_scratch_addr[dev]) {
+        void* ptr = nullptr;
+        check_cuda(cudaGetSymbolAddress(&ptr, g_bp_scratch), "cudaGetSymbolAddress(g_bp_scratch)");
+        g_bp_scratch_addr[dev] = static_cast<unsigned char*>(ptr);
+    }
+    return g_bp_scratch_addr[dev];
+}
+
+struct Bump {
+    unsigned char* base;
+    size_t used, cap;
+    template <class T>
+    T* take(size_t n) {
+        size_t off = (used + 255) & ~size_t(255);
+        size_t bytes = n * sizeof(T);
+        if (off + bytes > cap) return nullptr;
+        used = off + bytes;
+        return reinterpret_cast<T*>(base + off);
+    }
+};
+
+__global__ void k_noalloc_unpack(const float* __restrict__ aabbs, uint32_t n, float4* mn, float4* mx,
+                                 uint32_t* is_unb) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* a = aabbs + 6 * size_t(i);
+    mn[i] = make_float4(a[0], a[1], a[2], 0.0f);
+    mx[i] = make_float4(a[3], a[4], a[5], 0.0f);
+    bool huge = !(a[3] - a[0] < 1e15f) || !(a[4] - a[1] < 1e15f) || !(a[5] - a[2] < 1e15f);
+    is_unb[i] = huge ? 1u : 0u;
+}
+
+__global__ void k_unb_write_list(uint32_t n, const uint32_t* __restrict__ is_unb, const uint32_t* __restrict__ scan,
+                                 uint32_t* list) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && is_unb[i]) list[scan[i]] = i;
+}
+
+// Keys (lo << 32 | hi) become (lo, hi) uint32 pairs in place.
+__global__ void k_noalloc_keys_to_pairs(uint64_t* buf, uint64_t n) {
+    uint64_t k = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    uint64_t key = buf[k];
+    uint32_t* p = reinterpret_cast<uint32_t*>(buf + k);
+    p[0] = uint32_t(key >> 32);
+    p[1] = uint32_t(key & 0xffffffffu);
+}
+
+}  // namespace
+}  // namespace bgpu
+
+extern "C" bgpu_status bgpu_broadphase_pairs_noalloc(const float* aabbs_dev, uint32_t n, uint32_t* pairs_dev,
+                                                     uint64_t cap, uint64_t* out_n, void* stream) {
+    using namespace bgpu;
+    if (out_n) *out_n = 0;
+    if ((n && !aabbs_dev) || (cap && !pairs_dev) || (reinterpret_cast<uintptr_t>(pairs_dev) & 7u)) {
+        set_last_error("allocation-free broad phase: NULL buffer or pairs buffer not 8-byte aligned");
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+    if (n > BGPU_NOALLOC_MAX_PROXIES) {
+        set_last_error("allocation-free broad phase: more than BGPU_NOALLOC_MAX_PROXIES (65536) proxies");
+        return BGPU_ERR_CAPACITY;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    try {
+        int dev = 0;
+        check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+        if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+            set_last_error("allocation-free broad phase: device ordinal out of range");
+            return BGPU_ERR_CAPACITY;
+        }
+        if (n == 0) return BGPU_OK;
+        Bump sb{noalloc_scratch_address(dev), 0, NOALLOC_SCRATCH_BYTES};
+        float4* mn = sb.take<float4>(n);
+        float4* mx = sb.take<float4>(n);
+        uint64_t* keys = sb.take<uint64_t>(n);
+        uint64_t* keys_alt = sb.take<uint64_t>(n);
+        uint32_t* is_unb = sb.take<uint32_t>(n);
+        uint32_t* leaf_body = sb.take<uint32_t>(n);
+        uint32_t* parent = sb.take<uint32_t>(2 * size_t(n));
+        uint32_t* left = sb.take<uint32_t>(n);
+        uint32_t* right = sb.take<uint32_t>(n);
+        uint32_t* refit_flag = sb.take<uint32_t>(n);
+        uint32_t* counts = sb.take<uint32_t>(n);
+        uint32_t* offsets = sb.take<uint32_t>(n);
+        uint32_t* flags = sb.take<uint32_t>(n);
+        uint32_t* scan = sb.take<uint32_t>(n);
+        uint32_t* unb_list = sb.take<uint32_t>(BGPU_NOALLOC_MAX_UNBOUNDED + 1);
+        float4* node_min = sb.take<float4>(2 * size_t(n));
+        float4* node_max = sb.take<float4>(2 * size_t(n));
+        int* bounds = sb.take<int>(8);
+        uint32_t* scalars = sb.take<uint32_t>(8);
+        size_t sort_bytes = 0, scan_bytes = 0;
+        cub::DoubleBuffer<uint64_t> db(keys, keys_alt);
+        check_cuda(cub::DeviceRadixSort::SortKeys(nullptr, sort_bytes, db, int(n), 0, 64, s), "sort size");
+        check_cuda(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, counts, offsets, int(n), s), "scan size");
+        size_t tmp_bytes = std::max(sort_bytes, scan_bytes);
+        unsigned char* tmp = sb.take<unsigned char>(tmp_bytes);
+        if (!tmp) {
+            set_last_error("allocation-free broad phase: scratch array too small");
+            return BGPU_ERR_CAPACITY;
+        }
+        const int TB = 256;
+        const uint32_t grid = (n + TB - 1) / TB;
+        // Nothing below relies on the previous call's contents; the status word and the
+        // counters are cleared here, every other array is fully rewritten before it is read.
+        check_cuda(cudaMemsetAsync(scalars, 0, 8 * sizeof(uint32_t), s), "memset");
+        k_noalloc_unpack<<<grid, TB, 0, s>>>(aabbs_dev, n, mn, mx, is_unb);
+        // Unbounded proxies, listed in index order (few by contract).
+        check_cuda(cub::DeviceScan::ExclusiveSum(tmp, scan_bytes, is_unb, scan, int(n), s), "scan");
+        uint32_t host_scan_last[2] = {0, 0};
+        check_cuda(cudaMemcpyAsync(&host_scan_last[0], scan + (n - 1), 4, cudaMemcpyDeviceToHost, s), "d2h");
+        check_cuda(cudaMemcpyAsync(&host_scan_last[1], is_unb + (n - 1), 4, cudaMemcpyDeviceToHost, s), "d2h");
+        check_cuda(cudaStreamSynchronize(s), "sync");
+        uint32_t nunb = host_scan_last[0] + host_scan_last[1];
+        if (nunb > BGPU_NOALLOC_MAX_UNBOUNDED) {
+            set_last_error("allocation-free broad phase: more than BGPU_NOALLOC_MAX_UNBOUNDED (16) unbounded proxies");
+            return BGPU_ERR_CAPACITY;
+        }
+        uint32_t unb_host[BGPU_NOALLOC_MAX_UNBOUNDED + 1];
+        if (nunb) {
+            k_unb_write_list<<<grid, TB, 0, s>>>(n, is_unb, scan, unb_list);
+            check_cuda(cudaMemcpyAsync(unb_host, unb_list, nunb * 4, cudaMemcpyDeviceToHost, s), "d2h");
+        }
+        const int m = int(n - nunb);
+        k_reset_bounds<<<1, 32, 0, s>>>(bounds);
+        k_bounds<<<grid, TB, 0, s>>>(mn, mx, is_unb, n, bounds);
+        k_keys<<<grid, TB, 0, s>>>(mn, mx, is_unb, n, bounds, keys);
+        check_cuda(cub::DeviceRadixSort::SortKeys(tmp, sort_bytes, db, int(n), 0, 64, s), "sort");
+        const uint64_t* sorted = db.Current();
+        if (m > 0) {
+            k_build<<<(m + TB - 1) / TB, TB, 0, s>>>(sorted, m, left, right, parent, leaf_body, refit_flag);
+            k_refit<<<(m + TB - 1) / TB, TB, 0, s>>>(m, leaf_body, parent, left, right, refit_flag, mn, mx, node_min,
+                                                     node_max);
+        }
+        uint32_t* status = scalars + 1;
+        k_query<false><<<grid, TB, 0, s>>>(m, n, is_unb, mn, mx, node_min, node_max, left, right, leaf_body, unb_list,
+                                            nunb, counts, nullptr, nullptr, status);
+        uint32_t* unb_scan = reinterpret_cast<uint32_t*>(db.Alternate());  // free after the build
+        check_cuda(cudaStreamSynchronize(s), "sync");
+        for (uint32_t u = 0; u < nunb; ++u) {
+            uint32_t h = unb_host[u];
+            k_unb_flags<<<grid, TB, 0, s>>>(h, n, mn, mx, flags);
+            check_cuda(cub::DeviceScan::ExclusiveSum(tmp, scan_bytes, flags, unb_scan, int(n), s), "scan");
+            k_unb_count<<<1, 1, 0, s>>>(h, n, flags, unb_scan, counts);
+        }
+        check_cuda(cub::DeviceScan::ExclusiveSum(tmp, scan_bytes, counts, offsets, int(n), s), "scan");
+        k_total<<<1, 1, 0, s>>>(n, counts, offsets, scalars);
+        uint32_t host_scalars[2] = {0, 0};
+        check_cuda(cudaMemcpyAsync(host_scalars, scalars, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "d2h");
+        check_cuda(cudaStreamSynchronize(s), "sync");
+        uint64_t total = host_scalars[0];
+        if (out_n) *out_n = total;
+        if (total > cap) {
+            set_last_error("allocation-free broad phase: output capacity too small (out_n holds the pair count)");
+            return BGPU_ERR_CAPACITY;
+        }
+        uint64_t* out = reinterpret_cast<uint64_t*>(pairs_dev);
+        if (total) {
+            k_query<true><<<grid, TB, 0, s>>>(m, n, is_unb, mn, mx, node_min, node_max, left, right, leaf_body,
+                                               unb_list, nunb, counts, offsets, out, status);
+            for (uint32_t u = 0; u < nunb; ++u) {
+                uint32_t h = unb_host[u];
+                k_unb_flags<<<grid, TB, 0, s>>>(h, n, mn, mx, flags);
+                check_cuda(cub::DeviceScan::ExclusiveSum(tmp, scan_bytes, flags, unb_scan, int(n), s), "scan");
+                k_unb_write<<<grid, TB, 0, s>>>(h, n, flags, unb_scan, offsets, out);
+            }
+            k_noalloc_keys_to_pairs<<<uint32_t((total + TB - 1) / TB), TB, 0, s>>>(out, total);
+        }
+        uint32_t st = 0;
+        check_cuda(cudaMemcpyAsync(&st, status, 4, cudaMemcpyDeviceToHost, s), "d2h");
+        check_cuda(cudaStreamSynchronize(s), "sync");
+        check_cuda(cudaGetLastError(), "launch");
+        if (st) {
+            set_last_error("allocation-free broad phase: traversal stack overflow");
+            return BGPU_ERR_DEVICE_STATUS;
+        }
+        return BGPU_OK;
+    } catch (const CudaError& e) {
+        set_last_error(e.where);
+        return BGPU_ERR_CUDA;
+    }
+}

@@ -28,6 +28,12 @@ struct InvalidArg {
     std::string what;
 };
 
+}  // namespace
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+
 const float CONTACT_BREAKING_THRESHOLD = 0.02f;  // manifold.rs:8
 
 // shapes/mod.rs:388-392 (float arithmetic, host)

@@ -189,6 +189,28 @@ bgpu_status bgpu_solve_contacts(bgpu_world* w, uint32_t n, const float* contacts
 /* Push velocities (n x 6: push_lin3, push_ang3) left by the last solve. */
 bgpu_status bgpu_read_push(bgpu_world* w, float* push);
 
+/* Broad phase that allocates nothing (no counterpart in the reference), for
+ * callers that cannot allocate device memory while they run: loops with a fixed
+ * device-memory budget, code inside a host runtime that owns the allocator, and
+ * deadline-bound callers that cannot afford cudaMalloc / cudaFree (both may
+ * synchronise the device). Same output as bgpu_broadphase_pairs, but the inputs
+ * and outputs are device buffers: aabbs_dev n x 6 floats (min3, max3); pairs_dev
+ * room for cap pairs of 2 x uint32, 8-byte aligned. *out_n receives the pair
+ * count (also when it exceeds cap, which returns BGPU_ERR_CAPACITY). All scratch
+ * lives in one fixed file-scope device array of the library (24 MiB on every GPU
+ * that loads the library, held until exit), which limits n to
+ * BGPU_NOALLOC_MAX_PROXIES and the unbounded proxies (extent >= 1e15, such as
+ * planes) to BGPU_NOALLOC_MAX_UNBOUNDED; larger inputs return BGPU_ERR_CAPACITY.
+ * The first call on a device looks up the array's device address: make it
+ * before any stream capture. Every call shares the array, so calls that overlap
+ * on the GPU race and must be serialised by the caller. stream is a
+ * cudaStream_t (NULL = the default stream); the call returns after its work on
+ * that stream has finished. */
+#define BGPU_NOALLOC_MAX_PROXIES 65536u
+#define BGPU_NOALLOC_MAX_UNBOUNDED 16u
+bgpu_status bgpu_broadphase_pairs_noalloc(const float* aabbs_dev, uint32_t n, uint32_t* pairs_dev, uint64_t cap,
+                                          uint64_t* out_n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
