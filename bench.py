@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--grid", default="64,64,32", help="pile grid nx,nz,ny (default: the full 131,072-body pile)")
     p.add_argument("--cpu-sample-grid", default="16,16,32")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--batch-worlds", type=int, default=4096, help="batched-worlds leg: number of worlds (0: skip)")
+    p.add_argument("--batch-steps", type=int, default=30)
     return p.parse_args()
 
 
@@ -129,6 +131,83 @@ def algorithmic_pgs_bytes(st, iters):
     c = st["num_contacts"]
     split_c = st.get("num_split_contacts", 0)
     return c * (300 * iters + 120) + 100 * split_c * iters
+
+
+def count_launches(w, dt, nsteps=2):
+    """Kernels the library launches per step, counted by CUPTI (torch.profiler) over
+    `nsteps` untimed steps run after the timed region; memcpy/memset are not counted."""
+    try:
+        import torch
+        from torch.autograd import DeviceType
+        from torch.profiler import ProfilerActivity, profile
+
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            w.step(dt, nsteps)
+            torch.cuda.synchronize()
+        names = {}
+        for e in prof.events():
+            if e.device_type != DeviceType.CUDA or e.name.startswith(("Memcpy", "Memset")):
+                continue
+            names[e.name] = names.get(e.name, 0) + 1
+        total = sum(names.values())
+        return (total / nsteps if total else None), len(names)
+    except Exception:  # profiler unavailable: report no count rather than a guess
+        return None, 0
+
+
+def solve_traffic(contacts):
+    """DRAM bytes per k_solve launch, from the committed ncu capture of the same kernel
+    (profiles/k_solve_large_pile_131072.md, a shorter-settled pile), scaled to this
+    launch by its contact count (the kernel's traffic grows with the rows it sweeps)."""
+    import re
+
+    path = os.path.join(ROOT, "profiles", "k_solve_large_pile_131072.md")
+    try:
+        text = open(path).read()
+        dram = float(re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", text).group(1))
+        cap_contacts = float(re.search(r"capture_contacts:\s*([0-9]+)", text).group(1))
+    except (OSError, AttributeError, ValueError):
+        return None, None
+    return dram * contacts / cap_contacts, {"captured_bytes": dram, "captured_contacts": int(cap_contacts)}
+
+
+def bench_batched(bgpu, scenes, n_worlds, steps, warmup, sample_worlds=32, sample_steps=20):
+    """Batched-worlds leg: body-steps/s of n_worlds independent worlds stepped as one batch,
+    against the same worlds stepped one world at a time as plain worlds (a sample of the
+    worlds, scaled to the whole batch by its body count)."""
+    sc = scenes.batched_worlds(n_worlds=n_worlds, seed=4)
+    w = sc.build_gpu(bgpu)
+    n_dyn = sc.num_dynamic
+    w.step_timed(sc.dt, 60)  # settle
+    w.step_timed(sc.dt, warmup)
+    w.enable_timing(True)
+    ms = w.step_timed(sc.dt, steps)
+    st = w.stats()
+    w.enable_timing(False)
+    w.close()
+    batched = n_dyn * steps / (ms / 1000.0)
+    # one plain world per world, stepped one after another (a sample of the worlds)
+    idx = np.linspace(0, n_worlds - 1, min(sample_worlds, n_worlds)).astype(int)
+    total_ms, sample_dyn = 0.0, 0
+    for k in idx:
+        ws = sc.world_scene(int(k))
+        pw = ws.build_gpu(bgpu)
+        pw.step_timed(ws.dt, 60)
+        total_ms += pw.step_timed(ws.dt, sample_steps)
+        sample_dyn += ws.num_dynamic
+        pw.close()
+    per_world = sample_dyn * sample_steps / (total_ms / 1000.0)
+    return {"workload": f"batched_worlds_{n_worlds} (config 4): {n_dyn} dynamic bodies, "
+                        f"{sc.num_bodies} bodies, 8-255 per world, 10 iterations",
+            "value": batched, "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+            "pairs": st["num_pairs"], "contacts": st["num_contacts"], "colours": st["num_colours"],
+            "stage_ms_per_step": [x / max(st["timed_steps"], 1) for x in st["stage_ms"]],
+            "one_world_per_launch": {"value": per_world, "unit": UNIT,
+                                     "sample": f"{len(idx)} of the worlds as plain worlds, {sample_steps} steps each, "
+                                               f"device time summed"},
+            "speedup_vs_one_world_per_launch": batched / per_world if per_world else None,
+            "device_status": st["device_status"]}
 
 
 def peaks():
@@ -219,12 +298,15 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_value = n_dyn * e2e_steps * world_size / float(t.item())
 
+    launches_per_step, kernel_kinds = count_launches(w, sc.dt) if rank == 0 else (None, 0)
+
     if rank == 0:
         hbm, peak_kind = peaks()
         launches = max(st["timed_steps"], 1)
         solve_ms = st["solve_kernel_ms"] / launches
         alg = algorithmic_pgs_bytes(st, sc.iterations)
         achieved = alg / (solve_ms / 1000.0) / 1e9 if solve_ms > 0 else None
+        traffic, traffic_src = solve_traffic(st["num_contacts"])
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": region_ms / args.steps, "higher_is_better": True,
@@ -239,15 +321,19 @@ def main():
                        "stage_ms_per_step": [x / launches for x in st["stage_ms"]]},
             "roofline": {"kernel": "k_solve (colour-batched PGS)", "bound": "hbm",
                          "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": (achieved / hbm) if achieved else None, "traffic": None,
-                         "peak_kind": peak_kind, "kernel_ms_per_launch": solve_ms,
-                         "algorithmic_bytes_per_launch": alg},
+                         "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
+                         "traffic_source": traffic_src, "peak_kind": peak_kind,
+                         "kernel_ms_per_launch": solve_ms, "algorithmic_bytes_per_launch": alg,
+                         "split_contacts": st["num_split_contacts"]},
             "clocks": clocks.summary(),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(forces.nbytes),
                     "d2h_bytes_per_step": int(poses.nbytes)},
-            "gpu_launches": int(args.steps * 36),
+            "gpu_launches": int(round(launches_per_step * args.steps)) if launches_per_step else None,
+            "gpu_launches_note": f"CUPTI count of one step x steps ({kernel_kinds} kernel kinds)",
             "device_status": st["device_status"],
         }
+        if args.batch_worlds > 0:
+            line["batched_worlds"] = bench_batched(bgpu, scenes, args.batch_worlds, args.batch_steps, args.warmup)
         if world_size == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(grid_of(args.cpu_sample_grid), min(args.preroll, 240), 30)
         print(json.dumps(line), flush=True)

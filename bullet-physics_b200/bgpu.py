@@ -41,8 +41,17 @@ class StepStats(ctypes.Structure):
                 ("num_colours", ctypes.c_uint32), ("num_detect", ctypes.c_uint32), ("num_manifolds", ctypes.c_uint32),
                 ("device_status", ctypes.c_uint32), ("num_split_pairs", ctypes.c_uint32),
                 ("timed_steps", ctypes.c_uint32), ("stage_ms", ctypes.c_float * 7), ("solve_kernel_ms", ctypes.c_float),
-                ("step_ms", ctypes.c_float)]
+                ("step_ms", ctypes.c_float), ("num_split_contacts", ctypes.c_uint32)]
 
+
+# numpy view of bgpu_body_desc (96 bytes), for building many descriptors at once
+DESC_DTYPE = np.dtype([("shape", "<u4"), ("position", "<f4", 3), ("orientation", "<f4", 4),
+                       ("linear_velocity", "<f4", 3), ("angular_velocity", "<f4", 3), ("mass", "<f4"),
+                       ("friction", "<f4"), ("restitution", "<f4"), ("linear_damping", "<f4"),
+                       ("angular_damping", "<f4"), ("flags", "<u4"), ("group", "<u2"), ("mask", "<u2"),
+                       ("activation", "<u4"), ("linear_sleeping_threshold", "<f4"),
+                       ("angular_sleeping_threshold", "<f4")])
+assert DESC_DTYPE.itemsize == ctypes.sizeof(BodyDesc)
 
 _lib = None
 
@@ -88,6 +97,11 @@ def lib():
             "bgpu_collide": (S, [P, U32, U32P, F, U32P, F, F, ctypes.c_int, F, U32P]),
             "bgpu_solve_contacts": (S, [P, U32, F, ctypes.c_float, F, U64P]),
             "bgpu_read_push": (S, [P, F]),
+            "bgpu_batch_create": (S, [ctypes.POINTER(SolverInfo), F, ctypes.POINTER(P)]),
+            "bgpu_batch_add_worlds": (S, [P, U32, U32P, ctypes.c_void_p, U32P]),
+            "bgpu_batch_num_worlds": (U32, [P]),
+            "bgpu_batch_world_offsets": (S, [P, U32P]),
+            "bgpu_batch_step": (S, [P, ctypes.c_float, U32]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -147,13 +161,38 @@ def body_descs(n):
     return arr
 
 
+def desc_array(shape, pos, quat, linvel=None, angvel=None, mass=None, friction=None, restitution=None):
+    """bgpu_body_desc records for n bodies from numpy arrays (n,), (n,3), (n,4); other fields default."""
+    n = len(shape)
+    base = body_descs(1)
+    d = np.repeat(np.frombuffer(bytes(base), dtype=DESC_DTYPE), n)
+    d["shape"] = np.asarray(shape, dtype=np.uint32)
+    d["position"] = np.asarray(pos, dtype=np.float32).reshape(n, 3)
+    d["orientation"] = np.asarray(quat, dtype=np.float32).reshape(n, 4)
+    if linvel is not None:
+        d["linear_velocity"] = np.asarray(linvel, dtype=np.float32).reshape(n, 3)
+    if angvel is not None:
+        d["angular_velocity"] = np.asarray(angvel, dtype=np.float32).reshape(n, 3)
+    if mass is not None:
+        d["mass"] = np.asarray(mass, dtype=np.float32)
+    if friction is not None:
+        d["friction"] = np.asarray(friction, dtype=np.float32)
+    if restitution is not None:
+        d["restitution"] = np.asarray(restitution, dtype=np.float32)
+    return d
+
+
 class World:
-    def __init__(self, gravity=(0.0, -9.81, 0.0), **info):
+    """One world, or with batch=True a batch of independent worlds (bgpu_batch_*)."""
+
+    def __init__(self, gravity=(0.0, -9.81, 0.0), batch=False, **info):
         self.L = lib()
         self.h = ctypes.c_void_p()
         g = f32(gravity)
         s = solver_info(**info)
-        check(self.L.bgpu_world_create(ctypes.byref(s), fptr(g), ctypes.byref(self.h)), "bgpu_world_create")
+        create = self.L.bgpu_batch_create if batch else self.L.bgpu_world_create
+        check(create(ctypes.byref(s), fptr(g), ctypes.byref(self.h)), "bgpu_world_create")
+        self.batch = batch
 
     def close(self):
         if getattr(self, "h", None) and self.h.value:
@@ -227,24 +266,31 @@ class World:
     def add_bodies_array(self, shape, pos, quat, linvel=None, angvel=None, mass=None, friction=None,
                          restitution=None):
         """Vectorised insertion from numpy arrays (n,), (n,3), (n,4)."""
-        n = len(shape)
-        d = body_descs(n)
-        for i in range(n):
-            b = d[i]
-            b.shape = int(shape[i])
-            b.position[:] = [float(x) for x in pos[i]]
-            b.orientation[:] = [float(x) for x in quat[i]]
-            if linvel is not None:
-                b.linear_velocity[:] = [float(x) for x in linvel[i]]
-            if angvel is not None:
-                b.angular_velocity[:] = [float(x) for x in angvel[i]]
-            if mass is not None:
-                b.mass = float(mass[i])
-            if friction is not None:
-                b.friction = float(friction[i])
-            if restitution is not None:
-                b.restitution = float(restitution[i])
-        return self.add_descs(d)
+        d = desc_array(shape, pos, quat, linvel, angvel, mass, friction, restitution)
+        out = ctypes.c_uint32()
+        check(self.L.bgpu_add_bodies(self.h, len(d), d.ctypes.data_as(ctypes.POINTER(BodyDesc)), ctypes.byref(out)),
+              "add_bodies")
+        return out.value
+
+    def add_worlds_array(self, bodies_per_world, shape, pos, quat, linvel=None, angvel=None, mass=None,
+                         friction=None, restitution=None):
+        """Batched worlds: append worlds whose bodies follow each other in the arrays."""
+        counts = np.ascontiguousarray(bodies_per_world, dtype=np.uint32)
+        d = desc_array(shape, pos, quat, linvel, angvel, mass, friction, restitution)
+        assert len(d) == int(counts.sum())
+        out = ctypes.c_uint32()
+        check(self.L.bgpu_batch_add_worlds(self.h, len(counts), u32ptr(counts), d.ctypes.data, ctypes.byref(out)),
+              "batch_add_worlds")
+        return out.value
+
+    @property
+    def num_worlds(self):
+        return self.L.bgpu_batch_num_worlds(self.h)
+
+    def world_offsets(self):
+        out = np.zeros(self.num_worlds + 1, dtype=np.uint32)
+        check(self.L.bgpu_batch_world_offsets(self.h, u32ptr(out)), "batch_world_offsets")
+        return out
 
     @property
     def num_bodies(self):

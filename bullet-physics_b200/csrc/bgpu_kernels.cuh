@@ -80,13 +80,18 @@ struct Broadphase {
     // Returns the pair count; pairs are written to `out` (grown as needed).
     uint64_t run(const float4* aabb_min, const float4* aabb_max, uint32_t n, const std::vector<uint32_t>& unbounded_host,
                  DevBuf<uint64_t>& out, uint32_t* status_dev, cudaStream_t s);
+    // Batched worlds: pairs only inside each world [world_off[k], world_off[k + 1]) (device array).
+    uint64_t run_worlds(const float4* aabb_min, const float4* aabb_max, uint32_t n, const uint32_t* world_off,
+                        uint32_t n_worlds, DevBuf<uint64_t>& out, cudaStream_t s);
 };
 
 // ---------------------------------------------------------------- islands (k_islands.cu)
 struct Islands {
     DevBuf<uint32_t> parent, awake;
-    void run(const BodyDev& b, uint32_t n, const uint64_t* pairs, uint32_t npairs, uint32_t* simulate_flag,
-             uint32_t* status_dev, cudaStream_t s);
+    // simulate_flag[world] is raised when the world has an active body; world_of
+    // (per body) is null for a single world.
+    void run(const BodyDev& b, uint32_t n, const uint64_t* pairs, uint32_t npairs, const uint32_t* world_of,
+             uint32_t* simulate_flag, uint32_t* status_dev, cudaStream_t s);
 };
 
 // ---------------------------------------------------------------- pair pass + solver (k_pairs.cu, k_solver.cu)
@@ -120,15 +125,16 @@ struct PairData {
     DevBuf<uint32_t> old_owned;    // per old manifold: 1 when a current pair took it over
     DevBuf<uint32_t> scalars;      // [0] analytic count [1] convex count [2] contact pairs [3] contacts
                                    // [4] colours [5] split pairs [6] detect total [7] manifolds
+                                   // [8] [9] cache compaction counts [10] split contacts [11] largest split batch
     // Solver batches
     DevBuf<uint32_t> contact_pairs;  // pair ids with rows (ascending)
     DevBuf<uint32_t> colour;         // per contact pair
     DevBuf<unsigned long long> body_prio;
-    DevBuf<unsigned long long> body_mask;  // 2 words per body
+    DevBuf<unsigned long long> body_mask;  // 2 words per body: colours taken at the body
     DevBuf<uint32_t> colour_count, colour_offset, colour_cursor;
     DevBuf<uint32_t> split_count, split_offset, split_cursor;
-    DevBuf<uint32_t> batch;          // contact pairs in colour order
-    DevBuf<uint32_t> split_batch;    // pairs with split-active rows, colour order
+    DevBuf<uint4> batch_rec;         // contact pairs in colour order: body a, body b, pair | rows << 29, 0
+    DevBuf<uint4> split_rec;         // the same for the pairs with split-active rows
     DevBuf<uint32_t> flags;          // selection flags
     DevBuf<uint32_t> sel_a, sel_b;   // cache compaction lists
     DevBuf<unsigned char> cub_tmp;
@@ -147,14 +153,14 @@ struct PairData {
         colour.reserve(npairs);
         body_prio.reserve(nbodies);
         body_mask.reserve(2 * nbodies);
-        colour_count.reserve(130);
-        colour_offset.reserve(130);
-        colour_cursor.reserve(130);
-        split_count.reserve(130);
-        split_offset.reserve(130);
-        split_cursor.reserve(130);
-        batch.reserve(npairs);
-        split_batch.reserve(npairs);
+        colour_count.reserve(132);
+        colour_offset.reserve(132);
+        colour_cursor.reserve(132);
+        split_count.reserve(132);
+        split_offset.reserve(132);
+        split_cursor.reserve(132);
+        batch_rec.reserve(npairs);
+        split_rec.reserve(npairs);
         flags.reserve(npairs + old_manifolds + 1);
         sel_a.reserve(npairs);
         sel_b.reserve(old_manifolds + 1);
@@ -204,8 +210,9 @@ void launch_compute_iw(const BodyDev& b, uint32_t n, cudaStream_t s);
 void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
                 uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark);
 // Impulse writeback, then compaction of the surviving manifolds into `next`.
+// simulate / prev_simulate hold one flag per world, indexed through world_of (null: one world).
 void run_cache_update(const uint64_t* pairs, uint32_t npairs, const Manifolds& old_cache, PairData& pd,
-                      Manifolds& next, const uint32_t* simulate_flag, const uint32_t* prev_simulate,
-                      cudaStream_t s);
+                      Manifolds& next, const uint32_t* world_of, const uint32_t* simulate_flag,
+                      const uint32_t* prev_simulate, cudaStream_t s);
 
 }  // namespace bgpu

@@ -269,7 +269,71 @@ __global__ void k_set_unbounded(const uint32_t* __restrict__ unb, uint32_t nunb,
     if (u < nunb) is_unb[unb[u]] = 1;
 }
 
+// Batched worlds: world k owns proxies [off[k], off[k + 1]) and pairs only form
+// inside a world. One CTA per world tests every (i < j) of the world against
+// the other proxies staged in shared memory, tile by tile in ascending j, so
+// each proxy's segment comes out sorted, as in the tree query. The count pass
+// (WRITE false) fills counts[i]; the write pass stores at offsets[i].
+constexpr int WP_TILE = 64;
+
+template <bool WRITE>
+__global__ void __launch_bounds__(WP_TILE) k_world_pairs(const float4* __restrict__ bmin, const float4* __restrict__ bmax,
+                                                           const uint32_t* __restrict__ off, uint32_t n_worlds,
+                                                           uint32_t* counts, const uint32_t* __restrict__ offsets,
+                                                           uint64_t* out) {
+    __shared__ float4 smin[WP_TILE], smax[WP_TILE];
+    for (uint32_t w = blockIdx.x; w < n_worlds; w += gridDim.x) {
+        const uint32_t lo = off[w], hi = off[w + 1];
+        for (uint32_t ibase = lo; ibase < hi; ibase += WP_TILE) {
+            const uint32_t i = ibase + threadIdx.x;
+            const bool has = i < hi;
+            float4 qmin = make_float4(0.f, 0.f, 0.f, 0.f), qmax = qmin;
+            if (has) { qmin = bmin[i]; qmax = bmax[i]; }
+            uint32_t cnt = 0;
+            uint64_t pos = (WRITE && has) ? uint64_t(offsets[i]) : 0ull;
+            for (uint32_t jbase = ibase; jbase < hi; jbase += WP_TILE) {
+                __syncthreads();
+                const uint32_t j = jbase + threadIdx.x;
+                if (j < hi) { smin[threadIdx.x] = bmin[j]; smax[threadIdx.x] = bmax[j]; }
+                __syncthreads();
+                const uint32_t jn = min(uint32_t(WP_TILE), hi - jbase);
+                if (!has) continue;
+                for (uint32_t q = 0; q < jn; ++q) {
+                    const uint32_t jj = jbase + q;
+                    if (jj > i && overlaps(qmin, qmax, smin[q], smax[q])) {
+                        if (WRITE) out[pos++] = (uint64_t(i) << 32) | jj;
+                        else ++cnt;
+                    }
+                }
+            }
+            if (!WRITE && has) counts[i] = cnt;
+        }
+    }
+}
+
 }  // namespace
+
+uint64_t Broadphase::run_worlds(const float4* aabb_min, const float4* aabb_max, uint32_t n, const uint32_t* world_off,
+                                uint32_t n_worlds, DevBuf<uint64_t>& out, cudaStream_t s) {
+    if (n == 0 || n_worlds == 0) return 0;
+    counts.reserve(n);
+    offsets.reserve(n);
+    scalars.reserve(4);
+    const uint32_t grid = std::min<uint32_t>(n_worlds, 148u * 32u);
+    k_world_pairs<false><<<grid, WP_TILE, 0, s>>>(aabb_min, aabb_max, world_off, n_worlds, counts.p, nullptr, nullptr);
+    size_t scan_bytes = 0;
+    check_cuda(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, counts.p, offsets.p, int(n), s), "scan size");
+    cub_tmp.reserve(scan_bytes);
+    check_cuda(cub::DeviceScan::ExclusiveSum(cub_tmp.p, scan_bytes, counts.p, offsets.p, int(n), s), "scan");
+    k_total<<<1, 1, 0, s>>>(n, counts.p, offsets.p, scalars.p);
+    check_cuda(cudaMemcpyAsync(host_scalars, scalars.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "total d2h");
+    check_cuda(cudaStreamSynchronize(s), "broadphase sync");
+    uint64_t total = host_scalars[0];
+    out.reserve(total + 1);
+    if (total)
+        k_world_pairs<true><<<grid, WP_TILE, 0, s>>>(aabb_min, aabb_max, world_off, n_worlds, counts.p, offsets.p, out.p);
+    return total;
+}
 
 Broadphase::Broadphase() {
     check_cuda(cudaMallocHost(&host_scalars, 4 * sizeof(uint32_t)), "cudaMallocHost");

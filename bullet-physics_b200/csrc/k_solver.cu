@@ -6,11 +6,17 @@
 // (its <= 4 contacts, solved in order by one thread) is a graph vertex; two
 // groups conflict when they share a body with nonzero inverse mass. A
 // Jones-Plassmann colouring with first-fit colour choice splits the groups
-// into batches of pairwise-independent groups; a persistent cooperative
-// kernel sweeps the batches in colour order with a grid barrier between
-// batches. Within a batch no dynamic body is touched twice, so the result is
-// bit-identical to the reference's sequential solve over the same rows taken
-// in (colour, pair) order.
+// into batches of pairwise-independent groups. Within a batch no dynamic body
+// is touched twice, so the result is bit-identical to the reference's
+// sequential solve over the same rows taken in (colour, pair) order.
+//
+// The PGS kernel is a persistent cooperative launch split into two teams of
+// blocks with their own grid barriers: the velocity team runs the warm start
+// and the velocity sweeps, the split team the split-impulse sweeps, which
+// touch only the push velocities and so run at the same time. Before waiting
+// at a barrier each thread loads its next group's slot record and prefetches
+// that group's rows and inertia, so after the barrier only the velocities are
+// fetched.
 //
 // Rows store only the contact frame (normal, lever arms), the bias terms, the
 // effective masses and the accumulated impulses; the tangent basis, the
@@ -30,29 +36,22 @@ constexpr int MAX_COLOURS = 128;
 constexpr int MAX_ROUNDS = 1024;
 constexpr unsigned int BARRIER_SPIN_LIMIT = 1u << 26;
 
-// Grid-wide barrier for a cooperative launch (all blocks co-resident). The
-// spin is bounded: on timeout the status word records it and the kernel
-// continues, so no launch can hang the device.
-__device__ __forceinline__ void grid_barrier(unsigned int* bar, unsigned int nblocks, uint32_t* status) {
+// Barrier of a team of co-resident blocks (a cooperative launch) on a counter
+// that only grows during the launch: the k-th barrier (k from 1) of a team of
+// n blocks completes when the counter reaches k * n. One atomic per block,
+// then a tight spin. The spin is bounded: on timeout the status word records
+// it and every later barrier returns at once, so no launch can hang the device.
+__device__ __forceinline__ void team_barrier(unsigned int* ctr, unsigned int target, uint32_t* status) {
     __syncthreads();
-    // After one timeout every later barrier returns at once, so a broken launch ends quickly.
     if (threadIdx.x == 0 && !(*(volatile uint32_t*)status & ST_BARRIER_TIMEOUT)) {
-        volatile unsigned int* vgen = bar + 1;
-        unsigned int gen = *vgen;
         __threadfence();
-        unsigned int arrived = atomicAdd(&bar[0], 1u);
-        if (arrived == nblocks - 1) {
-            atomicExch(&bar[0], 0u);
-            __threadfence();
-            atomicAdd(&bar[1], 1u);
-        } else {
-            unsigned int spins = 0;
-            while (*vgen == gen) {
-                __nanosleep(64);
-                if (++spins > BARRIER_SPIN_LIMIT) {
-                    atomicOr(status, ST_BARRIER_TIMEOUT);
-                    break;
-                }
+        atomicAdd(ctr, 1u);
+        volatile unsigned int* vc = ctr;
+        unsigned int spins = 0;
+        while (*vc < target) {
+            if (++spins > BARRIER_SPIN_LIMIT) {
+                atomicOr(status, ST_BARRIER_TIMEOUT);
+                break;
             }
         }
         __threadfence();
@@ -91,7 +90,7 @@ struct ColourArgs {
     uint32_t* colour;
     unsigned long long* prio;
     unsigned long long* mask;
-    unsigned int* bar;  // [0..1] barrier, [2..4] round counters, [5] colour max
+    unsigned int* bar;  // [0] barrier counter, [2..4] round counters, [5] colour max
     uint32_t* status;
 };
 
@@ -103,6 +102,7 @@ __global__ void k_colour(ColourArgs a) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t stride = gridDim.x * blockDim.x;
     const unsigned int nblocks = gridDim.x;
+    unsigned int nbar = 0;
     for (uint32_t k = tid; k < K; k += stride) {
         a.colour[k] = NO_COLOUR;
         uint64_t key = a.pairs[a.contact_pairs[k]];
@@ -111,7 +111,7 @@ __global__ void k_colour(ColourArgs a) {
         a.mask[2 * v] = 0ull; a.mask[2 * v + 1] = 0ull;
     }
     if (tid == 0) { a.bar[2] = 0; a.bar[3] = 0; a.bar[4] = 0; a.bar[5] = 0; }
-    grid_barrier(a.bar, nblocks, a.status);
+    team_barrier(a.bar, ++nbar * nblocks, a.status);
     int round = 0;
     for (; round < MAX_ROUNDS; ++round) {
         // phase 0: clear the bids of the uncoloured groups' bodies
@@ -121,7 +121,7 @@ __global__ void k_colour(ColourArgs a) {
             a.prio[key_lo(key)] = 0ull;
             a.prio[key_hi(key)] = 0ull;
         }
-        grid_barrier(a.bar, nblocks, a.status);
+        team_barrier(a.bar, ++nbar * nblocks, a.status);
         // phase 1: bid (and recycle the counter of round r-1)
         if (tid == 0) a.bar[2 + (round + 2) % 3] = 0;
         for (uint32_t k = tid; k < K; k += stride) {
@@ -132,7 +132,7 @@ __global__ void k_colour(ColourArgs a) {
             if (inv_mass_of(a.iw, u) > 0.0f) atomicMax(&a.prio[u], pr);
             if (inv_mass_of(a.iw, v) > 0.0f) atomicMax(&a.prio[v], pr);
         }
-        grid_barrier(a.bar, nblocks, a.status);
+        team_barrier(a.bar, ++nbar * nblocks, a.status);
         // phase 2: winners pick a colour
         for (uint32_t k = tid; k < K; k += stride) {
             if (__ldcg(&a.colour[k]) != NO_COLOUR) continue;
@@ -158,7 +158,7 @@ __global__ void k_colour(ColourArgs a) {
             if (dv) { a.mask[2 * v] |= b0; a.mask[2 * v + 1] |= b1; }
             atomicMax(&a.bar[5], c + 1);
         }
-        grid_barrier(a.bar, nblocks, a.status);
+        team_barrier(a.bar, ++nbar * nblocks, a.status);
         volatile unsigned int* vb = a.bar;
         if (vb[2 + round % 3] == 0) break;
         if (*(volatile uint32_t*)a.status & ST_BARRIER_TIMEOUT) break;
@@ -166,34 +166,56 @@ __global__ void k_colour(ColourArgs a) {
     if (round >= MAX_ROUNDS && tid == 0) atomicOr(a.status, ST_COLOUR_ROUNDS);
 }
 
-__global__ void k_zero_u32(uint32_t n, uint32_t* a) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) a[i] = 0;
-}
-
-// Colour histograms of all groups and of the groups with split-active rows.
+// Colour histograms of all groups and of the groups with split-active rows,
+// plus the row and split-row totals.
 __global__ void k_colour_hist(const uint32_t* __restrict__ count, const uint32_t* __restrict__ contact_pairs,
                               const uint32_t* __restrict__ colour, const uint32_t* __restrict__ row_count,
                               const float4* __restrict__ rows, uint32_t* hist, uint32_t* split_hist, uint32_t* split_flag) {
+    // Block-local histograms; [MAX_COLOURS] rows, [MAX_COLOURS + 1] split-active rows.
+    __shared__ uint32_t sh[MAX_COLOURS + 2], ssh[MAX_COLOURS];
+    for (uint32_t i = threadIdx.x; i < MAX_COLOURS + 2; i += blockDim.x) sh[i] = 0;
+    for (uint32_t i = threadIdx.x; i < MAX_COLOURS; i += blockDim.x) ssh[i] = 0;
+    __syncthreads();
     uint32_t K = *count;
+    uint32_t nrows = 0, nsplit_rows = 0;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
         uint32_t c = colour[k];
-        atomicAdd(&hist[c], 1u);
+        atomicAdd(&sh[c], 1u);
         uint32_t p = contact_pairs[k];
         uint32_t n = row_count[p];
-        atomicAdd(&hist[MAX_COLOURS + 1], n);
-        bool split = false;
-        for (uint32_t r = 0; r < n; ++r) split |= rows[(size_t(p) * 4 + r) * ROW_F4 + 5].z != 0.0f;
-        split_flag[k] = split ? 1u : 0u;
-        if (split) atomicAdd(&split_hist[c], 1u);
+        nrows += n;
+        uint32_t nsr = 0;  // split-active rows
+        for (uint32_t r = 0; r < n; ++r) nsr += rows[(size_t(p) * 4 + r) * ROW_F4 + 5].z != 0.0f ? 1u : 0u;
+        split_flag[k] = nsr ? 1u : 0u;
+        if (nsr) {
+            nsplit_rows += nsr;
+            atomicAdd(&ssh[c], 1u);
+        }
+    }
+    nrows = __reduce_add_sync(0xffffffffu, nrows);
+    nsplit_rows = __reduce_add_sync(0xffffffffu, nsplit_rows);
+    if ((threadIdx.x & 31u) == 0u) {
+        if (nrows) atomicAdd(&sh[MAX_COLOURS], nrows);
+        if (nsplit_rows) atomicAdd(&sh[MAX_COLOURS + 1], nsplit_rows);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < MAX_COLOURS; i += blockDim.x) {
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+        if (ssh[i]) atomicAdd(&split_hist[i], ssh[i]);
+    }
+    if (threadIdx.x == 0) {
+        if (sh[MAX_COLOURS]) atomicAdd(&hist[MAX_COLOURS + 1], sh[MAX_COLOURS]);
+        if (sh[MAX_COLOURS + 1]) atomicAdd(&hist[MAX_COLOURS + 2], sh[MAX_COLOURS + 1]);
     }
 }
 
+// Offsets of the colour batches; scalars [3] rows [4] colours [5] split groups
+// [10] split rows [11] largest split batch.
 __global__ void k_colour_scan(uint32_t* hist, uint32_t* offset, uint32_t* cursor, uint32_t* split_hist,
                               uint32_t* split_offset, uint32_t* split_cursor, const unsigned int* bar, uint32_t* scalars) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     uint32_t ncol = bar[5];
-    uint32_t acc = 0, sacc = 0;
+    uint32_t acc = 0, sacc = 0, smax = 0;
     for (uint32_t c = 0; c < ncol; ++c) {
         offset[c] = acc;
         cursor[c] = acc;
@@ -201,41 +223,60 @@ __global__ void k_colour_scan(uint32_t* hist, uint32_t* offset, uint32_t* cursor
         split_offset[c] = sacc;
         split_cursor[c] = sacc;
         sacc += split_hist[c];
+        smax = max(smax, split_hist[c]);
     }
     offset[ncol] = acc;
     split_offset[ncol] = sacc;
     scalars[3] = hist[MAX_COLOURS + 1];
     scalars[4] = ncol;
     scalars[5] = sacc;
+    scalars[10] = hist[MAX_COLOURS + 2];
+    scalars[11] = smax;
 }
 
+// One atomicAdd per distinct colour among the calling lanes of a warp.
+__device__ __forceinline__ uint32_t claim_slot(uint32_t* cursor, uint32_t c) {
+    uint32_t active = __activemask();
+    uint32_t peers = __match_any_sync(active, c);
+    uint32_t lane = threadIdx.x & 31u;
+    uint32_t leader = uint32_t(__ffs(int(peers)) - 1);
+    uint32_t rank = uint32_t(__popc(peers & ((1u << lane) - 1u)));
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&cursor[c], uint32_t(__popc(int(peers))));
+    base = __shfl_sync(peers, base, int(leader));
+    return base + rank;
+}
+
+// Slot record of a group: its two bodies and its pair index with the row count
+// in the top three bits.
 __global__ void k_colour_scatter(const uint32_t* __restrict__ count, const uint32_t* __restrict__ contact_pairs,
+                                 const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ row_count,
                                  const uint32_t* __restrict__ colour, const uint32_t* __restrict__ split_flag,
-                                 uint32_t* cursor, uint32_t* split_cursor, uint32_t* batch, uint32_t* split_batch) {
+                                 uint32_t* cursor, uint32_t* split_cursor, uint4* batch_rec, uint4* split_rec) {
     uint32_t K = *count;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
         uint32_t c = colour[k];
         uint32_t p = contact_pairs[k];
-        batch[atomicAdd(&cursor[c], 1u)] = p;
-        if (split_flag[k]) split_batch[atomicAdd(&split_cursor[c], 1u)] = p;
+        uint64_t key = pairs[p];
+        uint4 rec = make_uint4(key_lo(key), key_hi(key), p | (row_count[p] << 29), 0u);
+        batch_rec[claim_slot(cursor, c)] = rec;
+        if (split_flag[k]) split_rec[claim_slot(split_cursor, c)] = rec;
     }
 }
 
 struct SolveArgs {
-    const uint64_t* pairs;
-    const uint32_t* row_count;
     float4* rows;
-    const uint32_t* batch;
+    const uint4* batch_rec;
     const uint32_t* offset;
-    const uint32_t* split_batch;
+    const uint4* split_rec;
     const uint32_t* split_offset;
-    const uint32_t* scalars;  // [4] colours [5] split groups
+    const uint32_t* scalars;  // [4] colours [5] split groups [11] largest split batch
     float4* linvel;
     float4* angvel;
     float4* push_lin;
     float4* push_ang;
     const float4* iw;
-    unsigned int* bar;
+    unsigned int* bar;        // [0] velocity-team barrier counter, [1] split-team counter
     uint32_t* status;
     float inv_dt;
     float restitution_threshold;
@@ -248,31 +289,24 @@ __device__ __forceinline__ void apply(V3& la, V3& wa, V3& lb, V3& wb, bool appa,
     if (appb) { lb += d * (j * imb); wb += cb * j; }
 }
 
-enum Phase { WARM = 0, ITER = 1 };
+enum Kind { WARM = 0, ITER = 1, SPLIT = 2 };
 
 // warm_start (sequential_impulse.rs:710-717) or one solve_contact sweep (:804-930) over a group.
-template <int PHASE>
-__device__ __forceinline__ void solve_group(const SolveArgs& a, uint32_t p) {
-    uint64_t key = a.pairs[p];
-    uint32_t ia = key_lo(key), ib = key_hi(key);
-    uint32_t cnt = a.row_count[p];
-    float ima, imb;
-    M3 iwa = load_iw(a.iw, ia, ima);
-    M3 iwb = load_iw(a.iw, ib, imb);
+template <int KIND>
+__device__ __forceinline__ void solve_group(const SolveArgs& a, uint32_t p, uint32_t cnt, const M3& iwa, const M3& iwb,
+                                            float ima, float imb, V3& la, V3& wa, V3& lb, V3& wb) {
     bool appa = ima > 0.0f, appb = imb > 0.0f;
-    V3 la = from4(__ldcg(&a.linvel[ia])), wa = from4(__ldcg(&a.angvel[ia]));
-    V3 lb = from4(__ldcg(&a.linvel[ib])), wb = from4(__ldcg(&a.angvel[ib]));
     for (uint32_t k = 0; k < cnt; ++k) {
         float4* r = a.rows + (size_t(p) * 4 + k) * ROW_F4;
         float4 r0 = r[0], r1 = r[1], r2 = r[2];
-        float4 r3 = __ldcg(&r[3]);
+        float4 r3 = r[3];
         V3 n = from4(r0), ra = from4(r1), rb = from4(r2);
         V3 t1, t2;
         tangent_basis_dev(n, t1, t2);
         V3 ana = mul(iwa, cross(ra, n)), anb = mul(iwb, cross(rb, n));
         V3 a1a = mul(iwa, cross(ra, t1)), a1b = mul(iwb, cross(rb, t1));
         V3 a2a = mul(iwa, cross(ra, t2)), a2b = mul(iwb, cross(rb, t2));
-        if (PHASE == WARM) {
+        if (KIND == WARM) {
             apply(la, wa, lb, wb, appa, appb, ima, imb, n, ana, anb, r3.x);
             apply(la, wa, lb, wb, appa, appb, ima, imb, t1, a1a, a1b, r3.y);
             apply(la, wa, lb, wb, appa, appb, ima, imb, t2, a2a, a2b, r3.z);
@@ -311,26 +345,17 @@ __device__ __forceinline__ void solve_group(const SolveArgs& a, uint32_t p) {
         float n2 = fminf(fmaxf(o2 + lam, -maxf), maxf);
         float j2 = n2 - o2;
         apply(la, wa, lb, wb, appa, appb, ima, imb, t2, a2a, a2b, j2);
-        __stcg(&r[3], make_float4(nimp, n1, n2, r3.w));
+        r[3] = make_float4(nimp, n1, n2, r3.w);
     }
-    if (appa) { __stcg(&a.linvel[ia], to4(la, 0.0f)); __stcg(&a.angvel[ia], to4(wa, 0.0f)); }
-    if (appb) { __stcg(&a.linvel[ib], to4(lb, 0.0f)); __stcg(&a.angvel[ib], to4(wb, 0.0f)); }
 }
 
 // split_impulse_pass body (sequential_impulse.rs:759-786) for one group.
-__device__ __forceinline__ void split_group(const SolveArgs& a, uint32_t p) {
-    uint64_t key = a.pairs[p];
-    uint32_t ia = key_lo(key), ib = key_hi(key);
-    uint32_t cnt = a.row_count[p];
-    float ima, imb;
-    M3 iwa = load_iw(a.iw, ia, ima);
-    M3 iwb = load_iw(a.iw, ib, imb);
+__device__ __forceinline__ void split_group(const SolveArgs& a, uint32_t p, uint32_t cnt, const M3& iwa, const M3& iwb,
+                                            float ima, float imb, V3& pla, V3& pwa, V3& plb, V3& pwb) {
     bool appa = ima > 0.0f, appb = imb > 0.0f;
-    V3 pla = from4(__ldcg(&a.push_lin[ia])), pwa = from4(__ldcg(&a.push_ang[ia]));
-    V3 plb = from4(__ldcg(&a.push_lin[ib])), pwb = from4(__ldcg(&a.push_ang[ib]));
     for (uint32_t k = 0; k < cnt; ++k) {
         float4* r = a.rows + (size_t(p) * 4 + k) * ROW_F4;
-        float4 r5 = __ldcg(&r[5]);
+        float4 r5 = r[5];
         if (r5.z == 0.0f) continue;
         float4 r0 = r[0], r1 = r[1], r2 = r[2], r4 = r[4];
         V3 n = from4(r0), ra = from4(r1), rb = from4(r2);
@@ -346,36 +371,111 @@ __device__ __forceinline__ void split_group(const SolveArgs& a, uint32_t p) {
             if (appa) { pla -= n * (j * ima); pwa -= ana * j; }
             if (appb) { plb += n * (j * imb); pwb += anb * j; }
         }
-        __stcg(&r[5], make_float4(r5.x, np, r5.z, r5.w));
+        r[5] = make_float4(r5.x, np, r5.z, r5.w);
     }
-    if (appa) { __stcg(&a.push_lin[ia], to4(pla, 0.0f)); __stcg(&a.push_ang[ia], to4(pwa, 0.0f)); }
-    if (appb) { __stcg(&a.push_lin[ib], to4(plb, 0.0f)); __stcg(&a.push_ang[ib], to4(pwb, 0.0f)); }
 }
 
-// solve() (sequential_impulse.rs:692-705): warm start, the velocity sweeps, the split sweeps.
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// Bring a group's rows (a pair's four row slots start on a 128-byte line) and
+// both bodies' inverse inertia into L1 ahead of its turn.
+__device__ __forceinline__ void prefetch_group(const SolveArgs& a, uint4 rec) {
+    const uint32_t p = rec.z & 0x1fffffffu, cnt = rec.z >> 29;
+    const char* r = reinterpret_cast<const char*>(a.rows + size_t(p) * 4 * ROW_F4);
+    for (uint32_t off = 0; off < cnt * ROW_F4 * 16u; off += 128u) prefetch_l1(r + off);
+    const char* ia = reinterpret_cast<const char*>(a.iw + 3 * size_t(rec.x));
+    const char* ib = reinterpret_cast<const char*>(a.iw + 3 * size_t(rec.y));
+    prefetch_l1(ia);
+    prefetch_l1(ia + 47);
+    prefetch_l1(ib);
+    prefetch_l1(ib + 47);
+}
+
+// One group: velocities (or push velocities) from L2, the group's rows, the
+// dynamic bodies' new velocities back to L2.
+template <int KIND>
+__device__ __forceinline__ void run_group(const SolveArgs& a, uint4 rec) {
+    const uint32_t ia = rec.x, ib = rec.y, p = rec.z & 0x1fffffffu, cnt = rec.z >> 29;
+    float4* plin = KIND == SPLIT ? a.push_lin : a.linvel;
+    float4* pang = KIND == SPLIT ? a.push_ang : a.angvel;
+    float ima, imb;
+    M3 iwa = load_iw(a.iw, ia, ima);
+    M3 iwb = load_iw(a.iw, ib, imb);
+    V3 la = from4(__ldcg(&plin[ia])), wa = from4(__ldcg(&pang[ia]));
+    V3 lb = from4(__ldcg(&plin[ib])), wb = from4(__ldcg(&pang[ib]));
+    if (KIND == SPLIT) split_group(a, p, cnt, iwa, iwb, ima, imb, la, wa, lb, wb);
+    else solve_group<KIND>(a, p, cnt, iwa, iwb, ima, imb, la, wa, lb, wb);
+    if (ima > 0.0f) { __stcg(&plin[ia], to4(la, 0.0f)); __stcg(&pang[ia], to4(wa, 0.0f)); }
+    if (imb > 0.0f) { __stcg(&plin[ib], to4(lb, 0.0f)); __stcg(&pang[ib], to4(wb, 0.0f)); }
+}
+
+// Phases first .. last-1 of a team: phase q is colour q % ncol of sweep
+// q / ncol. The team's threads deal the batch slots of each phase among
+// themselves; between phases the team meets at its barrier, and before it
+// each thread fetches its next slot record and prefetches that group.
+template <bool VELOCITY>
+__device__ __forceinline__ void run_phases(const SolveArgs& a, const uint4* __restrict__ recs,
+                                           const uint32_t* __restrict__ off, uint32_t ncol, uint32_t nphases,
+                                           uint32_t tid, uint32_t stride, unsigned int* ctr, uint32_t team_blocks,
+                                           uint32_t& nbar) {
+    if (ncol == 0) return;
+    uint4 rec = make_uint4(0u, 0u, 0u, 0u);
+    bool has = false;
+    {
+        uint32_t t = off[0] + tid;
+        if (nphases && t < off[1]) { rec = __ldg(&recs[t]); prefetch_group(a, rec); has = true; }
+    }
+    for (uint32_t q = 0; q < nphases; ++q) {
+        const uint32_t c = q % ncol, sweep = q / ncol;
+        const uint32_t end = off[c + 1];
+        if (has) {
+            if (!VELOCITY) run_group<SPLIT>(a, rec);
+            else if (sweep == 0) run_group<WARM>(a, rec);
+            else run_group<ITER>(a, rec);
+            for (uint32_t t = off[c] + tid + stride; t < end; t += stride) {
+                uint4 r2 = __ldg(&recs[t]);
+                if (!VELOCITY) run_group<SPLIT>(a, r2);
+                else if (sweep == 0) run_group<WARM>(a, r2);
+                else run_group<ITER>(a, r2);
+            }
+        }
+        if (q + 1 == nphases) break;
+        const uint32_t cn = (q + 1) % ncol;
+        const uint32_t tn = off[cn] + tid;
+        has = tn < off[cn + 1];
+        if (has) { rec = __ldg(&recs[tn]); prefetch_group(a, rec); }
+        team_barrier(ctr, ++nbar * team_blocks, a.status);
+    }
+}
+
+// solve() (sequential_impulse.rs:692-705): warm start and velocity sweeps on
+// the velocity team; the split sweeps on the split team, which has enough
+// blocks for the largest split batch and at most a quarter of the grid (none
+// on a grid too small to split, where the velocity team runs them last).
 __global__ void k_solve(SolveArgs a) {
     const uint32_t ncol = a.scalars[4];
     const uint32_t nsplit = a.scalars[5];
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    const unsigned int nb = gridDim.x;
-    for (uint32_t c = 0; c < ncol; ++c) {
-        for (uint32_t t = a.offset[c] + tid; t < a.offset[c + 1]; t += stride) solve_group<WARM>(a, a.batch[t]);
-        grid_barrier(a.bar, nb, a.status);
+    const uint32_t iters = a.iterations;
+    const uint32_t G = gridDim.x;
+    uint32_t split_blocks = 0;
+    if (nsplit && iters && G >= 4) {
+        uint32_t need = (a.scalars[11] + blockDim.x - 1) / blockDim.x;
+        split_blocks = min(max(need, 1u), G / 4);
     }
-    for (uint32_t it = 0; it < a.iterations; ++it) {
-        for (uint32_t c = 0; c < ncol; ++c) {
-            for (uint32_t t = a.offset[c] + tid; t < a.offset[c + 1]; t += stride) solve_group<ITER>(a, a.batch[t]);
-            grid_barrier(a.bar, nb, a.status);
-        }
+    const bool split_team = blockIdx.x >= G - split_blocks;
+    const uint32_t team_blocks = split_team ? split_blocks : G - split_blocks;
+    const uint32_t team_block = split_team ? blockIdx.x - (G - split_blocks) : blockIdx.x;
+    const uint32_t tid = team_block * blockDim.x + threadIdx.x;
+    const uint32_t stride = team_blocks * blockDim.x;
+    uint32_t nbar = 0;
+    if (split_team) {
+        run_phases<false>(a, a.split_rec, a.split_offset, ncol, iters * ncol, tid, stride, a.bar + 1, team_blocks, nbar);
+        return;
     }
-    if (nsplit == 0) return;
-    for (uint32_t it = 0; it < a.iterations; ++it) {
-        for (uint32_t c = 0; c < ncol; ++c) {
-            for (uint32_t t = a.split_offset[c] + tid; t < a.split_offset[c + 1]; t += stride)
-                split_group(a, a.split_batch[t]);
-            grid_barrier(a.bar, nb, a.status);
-        }
+    run_phases<true>(a, a.batch_rec, a.offset, ncol, (iters + 1) * ncol, tid, stride, a.bar, team_blocks, nbar);
+    if (nsplit && iters && split_blocks == 0) {
+        team_barrier(a.bar, ++nbar * team_blocks, a.status);
+        run_phases<false>(a, a.split_rec, a.split_offset, ncol, iters * ncol, tid, stride, a.bar, team_blocks, nbar);
     }
 }
 
@@ -396,13 +496,15 @@ __global__ void k_writeback(uint32_t npairs, const uint32_t* __restrict__ row_co
     valid_flags[p] = (__float_as_uint(e[2].w) & META_VALID) ? 1u : 0u;
 }
 
-// step.rs:1006-1010: with prune = simulate && prev_simulate, manifolds whose pair vanished die;
-// otherwise the unowned old manifolds survive.
-__global__ void k_flag_unowned(uint32_t nold, const uint32_t* __restrict__ owned, const uint32_t* __restrict__ simulate,
+// step.rs:1006-1010: with prune = simulate && prev_simulate (of the manifold's world), manifolds
+// whose pair vanished die; otherwise the unowned old manifolds survive.
+__global__ void k_flag_unowned(uint32_t nold, const uint32_t* __restrict__ owned, const uint64_t* __restrict__ old_keys,
+                               const uint32_t* __restrict__ world_of, const uint32_t* __restrict__ simulate,
                                const uint32_t* __restrict__ prev_simulate, uint32_t* flags) {
     uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= nold) return;
-    bool prune = (*simulate != 0) && (*prev_simulate != 0);
+    uint32_t w = world_of ? world_of[key_lo(old_keys[o])] : 0u;
+    bool prune = (simulate[w] != 0) && (prev_simulate[w] != 0);
     flags[o] = (!prune && !owned[o]) ? 1u : 0u;
 }
 
@@ -476,11 +578,13 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
                 uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark) {
     if (npairs == 0) {
         check_cuda(cudaMemsetAsync(pd.scalars.p + 2, 0, 4 * sizeof(uint32_t), s), "memset");
+        check_cuda(cudaMemsetAsync(pd.scalars.p + 10, 0, 2 * sizeof(uint32_t), s), "memset");
         mark(5);
         mark(6);
         return;
     }
     const int TB = 256;
+    if (npairs >= (1u << 29)) throw CudaError{cudaErrorInvalidValue, "more than 2^29 pairs for the solver's slot records"};
     // Contact pairs (ascending pair order).
     k_flag_contact_pairs<<<(npairs + TB - 1) / TB, TB, 0, s>>>(npairs, pd.row_count.p, pd.flags.p);
     size_t bytes = 0;
@@ -500,21 +604,22 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
     check_cuda(cudaLaunchCooperativeKernel((const void*)k_colour, dim3(colour_grid), dim3(TB), cargs, 0, s),
                "colour launch");
     // Batches.
-    check_cuda(cudaMemsetAsync(pd.colour_count.p, 0, 130 * sizeof(uint32_t), s), "memset");
-    check_cuda(cudaMemsetAsync(pd.split_count.p, 0, 130 * sizeof(uint32_t), s), "memset");
+    check_cuda(cudaMemsetAsync(pd.colour_count.p, 0, (MAX_COLOURS + 3) * sizeof(uint32_t), s), "memset");
+    check_cuda(cudaMemsetAsync(pd.split_count.p, 0, (MAX_COLOURS + 3) * sizeof(uint32_t), s), "memset");
     uint32_t g = std::min<uint32_t>((npairs + TB - 1) / TB, 148u * 8u);
     k_colour_hist<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pd.colour.p, pd.row_count.p, pd.rows.p,
                                    pd.colour_count.p, pd.split_count.p, pd.flags.p);
     k_colour_scan<<<1, 32, 0, s>>>(pd.colour_count.p, pd.colour_offset.p, pd.colour_cursor.p, pd.split_count.p,
                                    pd.split_offset.p, pd.split_cursor.p, pd.barrier.p, pd.scalars.p);
-    k_colour_scatter<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pd.colour.p, pd.flags.p, pd.colour_cursor.p,
-                                      pd.split_cursor.p, pd.batch.p, pd.split_batch.p);
-    // PGS (cooperative launch).
+    k_colour_scatter<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pairs, pd.row_count.p, pd.colour.p,
+                                      pd.flags.p, pd.colour_cursor.p, pd.split_cursor.p, pd.batch_rec.p,
+                                      pd.split_rec.p);
+    // PGS (cooperative launch: the teams' barriers need every block resident).
     check_cuda(cudaMemsetAsync(pd.barrier.p, 0, 2 * sizeof(unsigned int), s), "memset barrier");
     mark(5);
-    SolveArgs sa{pairs, pd.row_count.p, pd.rows.p, pd.batch.p, pd.colour_offset.p, pd.split_batch.p, pd.split_offset.p,
-                 pd.scalars.p, w.b.linvel, w.b.angvel, w.b.push_lin, w.b.push_ang, w.b.iw, pd.barrier.p, status_dev,
-                 sp.inv_dt, sp.info.restitution_velocity_threshold, sp.info.num_iterations};
+    SolveArgs sa{pd.rows.p, pd.batch_rec.p, pd.colour_offset.p, pd.split_rec.p, pd.split_offset.p, pd.scalars.p,
+                 w.b.linvel, w.b.angvel, w.b.push_lin, w.b.push_ang, w.b.iw, pd.barrier.p, status_dev, sp.inv_dt,
+                 sp.info.restitution_velocity_threshold, sp.info.num_iterations};
     static int solve_grid = 0;
     if (!solve_grid) solve_grid = coop_grid((const void*)k_solve, TB, 0);
     void* sargs[] = {&sa};
@@ -524,7 +629,8 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
 }
 
 void run_cache_update(const uint64_t* pairs, uint32_t npairs, const Manifolds& old_cache, PairData& pd,
-                      Manifolds& next, const uint32_t* simulate_flag, const uint32_t* prev_simulate, cudaStream_t s) {
+                      Manifolds& next, const uint32_t* world_of, const uint32_t* simulate_flag,
+                      const uint32_t* prev_simulate, cudaStream_t s) {
     const int TB = 256;
     uint32_t nold_cap = old_cache.count_host;
     // A: surviving manifolds of the current pairs.
@@ -546,8 +652,8 @@ void run_cache_update(const uint64_t* pairs, uint32_t npairs, const Manifolds& o
     // B: unowned old manifolds (only kept when this step does not prune).
     if (nold_cap) {
         // nold_cap is the exact old count: the world syncs on it before the step.
-        k_flag_unowned<<<(nold_cap + TB - 1) / TB, TB, 0, s>>>(nold_cap, pd.old_owned.p, simulate_flag, prev_simulate,
-                                                                pd.flags.p);
+        k_flag_unowned<<<(nold_cap + TB - 1) / TB, TB, 0, s>>>(nold_cap, pd.old_owned.p, old_cache.keys.p, world_of,
+                                                                simulate_flag, prev_simulate, pd.flags.p);
         check_cuda(cub::DeviceSelect::Flagged(pd.cub_tmp.p, bytes_b, it, pd.flags.p, pd.sel_b.p, nb_dev, int(nold_cap), s),
                    "sel");
     }

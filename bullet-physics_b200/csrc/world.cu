@@ -116,6 +116,11 @@ struct World {
     DevBuf<uint4> info_d;
     DevBuf<float> settled;
     std::vector<uint32_t> unbounded;  // plane bodies (kept out of the BVH)
+    // batched worlds: world k owns bodies [world_off_h[k], world_off_h[k + 1])
+    bool batch = false;
+    std::vector<uint32_t> world_off_h{0u};
+    DevBuf<uint32_t> world_off_d, world_of_d;
+    DevBuf<uint32_t> world_sim;  // [0, W) simulate, [W, 2W) prev_simulate, per world
     // step machinery
     Broadphase bp;
     Islands islands;
@@ -124,7 +129,7 @@ struct World {
     int cur = 0;
     DevBuf<uint64_t> pairs;
     uint32_t npairs = 0;
-    DevBuf<uint32_t> flags;  // [0] status, [1] simulate, [2] prev_simulate
+    DevBuf<uint32_t> flags;  // [0] status
     HostStats* hs = nullptr;
     bool timing = false;
     cudaEvent_t ev[2][10] = {};  // two event sets: the step being enqueued and the previous one
@@ -143,6 +148,8 @@ struct World {
         std::memset(hs, 0, sizeof(HostStats));
         flags.reserve(4);
         check_cuda(cudaMemsetAsync(flags.p, 0, 4 * sizeof(uint32_t), stream), "memset");
+        world_sim.reserve(2);
+        check_cuda(cudaMemsetAsync(world_sim.p, 0, 2 * sizeof(uint32_t), stream), "memset");
         cache[0].init();
         cache[1].init();
         check_cuda(cudaMemsetAsync(cache[0].count_dev, 0, sizeof(uint32_t), stream), "memset");
@@ -253,6 +260,11 @@ struct World {
     }
 
     uint32_t add_bodies(uint32_t cnt, const bgpu_body_desc* d) {
+        if (batch) throw InvalidArg{"a batched world takes bodies through bgpu_batch_add_worlds"};
+        return add_bodies_impl(cnt, d);
+    }
+
+    uint32_t add_bodies_impl(uint32_t cnt, const bgpu_body_desc* d) {
         for (uint32_t k = 0; k < cnt; ++k) {
             if (d[k].shape >= shapes_h.size()) throw InvalidArg{"body shape id out of range"};
             if (shapes_h[d[k].shape].type == SHAPE_PLANE && d[k].mass != 0.0f)
@@ -317,6 +329,47 @@ struct World {
         return first;
     }
 
+    uint32_t num_worlds() const { return batch ? uint32_t(world_off_h.size() - 1) : 1u; }
+
+    // Batched worlds: append worlds whose bodies are given back to back.
+    uint32_t add_worlds(uint32_t nw, const uint32_t* bodies_per_world, const bgpu_body_desc* d) {
+        if (!batch) throw InvalidArg{"bgpu_batch_add_worlds needs a world made by bgpu_batch_create"};
+        uint64_t total = 0;
+        for (uint32_t k = 0; k < nw; ++k) total += bodies_per_world[k];
+        if (uint64_t(n) + total > 0xfffffff0ull) throw InvalidArg{"too many bodies"};
+        const uint32_t first_world = num_worlds();
+        const uint32_t first_body = n;
+        if (total) add_bodies_impl(uint32_t(total), d);
+        uint32_t acc = first_body;
+        for (uint32_t k = 0; k < nw; ++k) {
+            acc += bodies_per_world[k];
+            world_off_h.push_back(acc);
+        }
+        const uint32_t W = num_worlds();
+        // world offsets and per-body world ids (kept in step with the body arrays)
+        world_off_d.grow_keep(W + 1, 0, stream);
+        check_cuda(cudaMemcpyAsync(world_off_d.p, world_off_h.data(), (W + 1) * sizeof(uint32_t),
+                                   cudaMemcpyHostToDevice, stream), "upload world offsets");
+        std::vector<uint32_t> wof(total);
+        for (uint32_t k = 0, i = 0; k < nw; ++k)
+            for (uint32_t j = 0; j < bodies_per_world[k]; ++j) wof[i++] = first_world + k;
+        world_of_d.grow_keep(std::max<uint32_t>(cap, 1), first_body, stream);
+        if (total)
+            check_cuda(cudaMemcpyAsync(world_of_d.p + first_body, wof.data(), total * sizeof(uint32_t),
+                                       cudaMemcpyHostToDevice, stream), "upload world ids");
+        // per-world simulate flags: new worlds start with prev_simulate = 0
+        DevBuf<uint32_t> fresh;
+        fresh.reserve(2 * size_t(W));
+        check_cuda(cudaMemsetAsync(fresh.p, 0, 2 * size_t(W) * sizeof(uint32_t), stream), "memset");
+        const uint32_t W0 = first_world;
+        if (W0) check_cuda(cudaMemcpyAsync(fresh.p + W, world_sim.p + W0, W0 * sizeof(uint32_t),
+                                           cudaMemcpyDeviceToDevice, stream), "copy flags");
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+        std::swap(world_sim.p, fresh.p);
+        std::swap(world_sim.cap, fresh.cap);
+        return first_world;
+    }
+
     void set_gravity(const float* g) {
         gravity[0] = g[0]; gravity[1] = g[1]; gravity[2] = g[2];
         // world.rs:467-481: active bodies that did not opt out take the new gravity.
@@ -379,16 +432,20 @@ struct World {
         BodyDev b = body_dev();
         WorldView wv = view();
         uint32_t* status = flags.p;
-        uint32_t* simulate = flags.p + 1;
-        uint32_t* prev_simulate = flags.p + 2;
-        check_cuda(cudaMemsetAsync(flags.p, 0, 2 * sizeof(uint32_t), stream), "memset flags");
+        const uint32_t nw = num_worlds();
+        uint32_t* simulate = world_sim.p;
+        uint32_t* prev_simulate = world_sim.p + nw;
+        const uint32_t* world_of = batch ? world_of_d.p : nullptr;
+        check_cuda(cudaMemsetAsync(flags.p, 0, sizeof(uint32_t), stream), "memset flags");
+        check_cuda(cudaMemsetAsync(simulate, 0, nw * sizeof(uint32_t), stream), "memset flags");
         mark(0);
         // 1-3: velocities, predicted poses, AABBs (fused).
         launch_integrate_velocities(b, shapes_d.p, hull_d.p, n, dt, stream);
         mark(1);
         // 4: broad phase (syncs once to size the pair arrays; the previous step's
         //    manifold count and timing events are read at the same point).
-        uint64_t np = bp.run(aabb_min.p, aabb_max.p, n, unbounded, pairs, status, stream);
+        uint64_t np = batch ? bp.run_worlds(aabb_min.p, aabb_max.p, n, world_off_d.p, nw, pairs, stream)
+                            : bp.run(aabb_min.p, aabb_max.p, n, unbounded, pairs, status, stream);
         npairs = uint32_t(np);
         if (timing) fold(ev_cur ^ 1);
         Manifolds& old_cache = cache[cur];
@@ -396,7 +453,7 @@ struct World {
         old_cache.count_host = hs->cache_count;
         mark(2);
         // 4b: islands
-        islands.run(b, n, pairs.p, npairs, simulate, status, stream);
+        islands.run(b, n, pairs.p, npairs, world_of, simulate, status, stream);
         mark(3);
         // 5: pair pass
         pd.reserve(std::max<uint32_t>(npairs, 1), n, old_cache.count_host);
@@ -407,8 +464,9 @@ struct World {
         // 6: solve (colouring, then the PGS kernel)
         run_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); });
         // 6b: impulse writeback + prune
-        run_cache_update(pairs.p, npairs, old_cache, pd, next, simulate, prev_simulate, stream);
-        check_cuda(cudaMemcpyAsync(prev_simulate, simulate, sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream), "flag");
+        run_cache_update(pairs.p, npairs, old_cache, pd, next, world_of, simulate, prev_simulate, stream);
+        check_cuda(cudaMemcpyAsync(prev_simulate, simulate, nw * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream),
+                   "flag");
         mark(7);
         // 6c + 7 + 8: deactivation, pose integration with the split push, force clear.
         launch_integrate_positions(b, n, dt, info.split_impulse_turn_erp, stream);
@@ -436,6 +494,7 @@ struct World {
         last.num_contacts = hs->scalars[3];
         last.num_colours = hs->scalars[4];
         last.num_split_pairs = hs->scalars[5];
+        last.num_split_contacts = hs->scalars[10];
         last.num_detect = hs->scalars[0] + hs->scalars[1];
         last.num_manifolds = hs->cache_count;
         last.device_status = hs->status;
@@ -606,6 +665,52 @@ bgpu_status bgpu_add_bodies(bgpu_world* w, uint32_t n, const bgpu_body_desc* d, 
 }
 
 uint32_t bgpu_num_bodies(const bgpu_world* w) { return w ? w->impl.n : 0; }
+
+bgpu_status bgpu_batch_create(const bgpu_solver_info* info, const float* gravity, bgpu_world** out) {
+    bgpu_status st = bgpu_world_create(info, gravity, out);
+    if (st != BGPU_OK) return st;
+    (*out)->impl.batch = true;
+    return BGPU_OK;
+}
+
+bgpu_status bgpu_batch_add_worlds(bgpu_world* w, uint32_t n_worlds, const uint32_t* bodies_per_world,
+                                  const bgpu_body_desc* descs, uint32_t* out_first_world) {
+    if (!w || (n_worlds && !bodies_per_world)) {
+        bgpu::g_last_error = "world is NULL or bodies_per_world is NULL";
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+    uint64_t total = 0;
+    for (uint32_t k = 0; k < n_worlds; ++k) total += bodies_per_world[k];
+    if (total && !descs) {
+        bgpu::g_last_error = "descs is NULL";
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&]() -> bgpu_status {
+        w->impl.finish_stats();
+        uint32_t f = w->impl.add_worlds(n_worlds, bodies_per_world, descs);
+        if (out_first_world) *out_first_world = f;
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_batch_step(bgpu_world* w, float dt, uint32_t nsteps) {
+    if (!w || !w->impl.batch) {
+        bgpu::g_last_error = "world is NULL or not batched";
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+    return bgpu_step(w, dt, nsteps);
+}
+
+uint32_t bgpu_batch_num_worlds(const bgpu_world* w) { return (w && w->impl.batch) ? w->impl.num_worlds() : 0u; }
+
+bgpu_status bgpu_batch_world_offsets(bgpu_world* w, uint32_t* offsets) {
+    if (!w || !offsets || !w->impl.batch) {
+        bgpu::g_last_error = "world is NULL, not batched, or offsets is NULL";
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+    std::memcpy(offsets, w->impl.world_off_h.data(), w->impl.world_off_h.size() * sizeof(uint32_t));
+    return BGPU_OK;
+}
 
 bgpu_status bgpu_step(bgpu_world* w, float dt, uint32_t nsteps) {
     if (!w || !(dt > 0.0f)) {

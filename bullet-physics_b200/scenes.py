@@ -15,6 +15,10 @@ parity check and a benchmark run start from bit-identical inputs.
   large_pile         131,072 bodies (50% unit boxes half 0.5, 50% spheres
                      r 0.5) on a jittered 64x64x32 grid, 1.05 m spacing;
                      20 iterations; 600 steps.
+  batched_worlds     4,096 independent worlds of n = floor(exp(U(ln 8, ln 256)))
+                     dynamic bodies each, half of them columns of 1-16 unit
+                     boxes, half jittered sphere piles (r 0.5), every world on
+                     its own ground plane; 10 iterations; 500 steps.
 Scaled-down variants (`scale`) keep the recipe and shrink the grid.
 """
 import math
@@ -232,4 +236,122 @@ def large_pile_fast(nx=64, nz=64, ny=32, seed=3, steps=600, spacing=1.05):
     s.mass = [0.0] + [1.0] * n
     s.friction = [0.5] * (n + 1)
     s.restitution = [0.0] * (n + 1)
+    return s
+
+
+class BatchScene:
+    """Independent worlds sharing one shape list (batched-worlds configuration)."""
+
+    FIELDS = ("shape", "pos", "quat", "linvel", "angvel", "mass", "friction", "restitution")
+
+    def __init__(self, name, dt, iterations, steps):
+        self.name = name
+        self.dt = dt
+        self.iterations = iterations
+        self.steps = steps
+        self.gravity = (0.0, -9.81, 0.0)
+        self.shapes = []
+        self.worlds = []  # per world: dict of the FIELDS arrays
+
+    def add_shape(self, kind, params=(), points=None):
+        self.shapes.append((kind, list(params), None if points is None else np.asarray(points, dtype=np.float32)))
+        return len(self.shapes) - 1
+
+    def add_world(self, shape, pos, quat, mass):
+        n = len(shape)
+        self.worlds.append(dict(shape=np.asarray(shape, dtype=np.uint32), pos=np.asarray(pos, dtype=np.float32),
+                                quat=np.asarray(quat, dtype=np.float32), linvel=np.zeros((n, 3), np.float32),
+                                angvel=np.zeros((n, 3), np.float32), mass=np.asarray(mass, dtype=np.float32),
+                                friction=np.full(n, 0.5, np.float32), restitution=np.zeros(n, np.float32)))
+
+    @property
+    def bodies_per_world(self):
+        return np.array([len(w["shape"]) for w in self.worlds], dtype=np.uint32)
+
+    @property
+    def num_bodies(self):
+        return int(self.bodies_per_world.sum())
+
+    @property
+    def num_dynamic(self):
+        return int(sum(np.count_nonzero(w["mass"] > 0) for w in self.worlds))
+
+    def arrays(self):
+        return {f: np.concatenate([w[f] for w in self.worlds]) for f in self.FIELDS}
+
+    def build_gpu(self, bgpu_module, **solver):
+        w = bgpu_module.World(gravity=self.gravity, batch=True, num_iterations=self.iterations, **solver)
+        for kind, params, pts in self.shapes:
+            w.add_shape(kind, params, pts)
+        a = self.arrays()
+        w.add_worlds_array(self.bodies_per_world, a["shape"], a["pos"], a["quat"], a["linvel"], a["angvel"],
+                           a["mass"], a["friction"], a["restitution"])
+        return w
+
+    def world_scene(self, k):
+        """World k alone, as a Scene with the same shape list (for the oracle or a plain GPU world)."""
+        s = Scene(f"{self.name}_world{k}", self.dt, self.iterations, self.steps)
+        s.gravity = self.gravity
+        s.shapes = list(self.shapes)
+        w = self.worlds[k]
+        s.shape_of = [int(x) for x in w["shape"]]
+        s.pos = list(map(tuple, w["pos"]))
+        s.quat = list(map(tuple, w["quat"]))
+        s.linvel = list(map(tuple, w["linvel"]))
+        s.angvel = list(map(tuple, w["angvel"]))
+        s.mass = [float(x) for x in w["mass"]]
+        s.friction = [float(x) for x in w["friction"]]
+        s.restitution = [float(x) for x in w["restitution"]]
+        return s
+
+
+def _small_rotations(rng, n, max_deg):
+    axis = rng.normal(size=(n, 3))
+    axis /= np.linalg.norm(axis, axis=1, keepdims=True)
+    ang = np.radians(rng.uniform(-max_deg, max_deg, size=n))
+    q = np.concatenate([axis * np.sin(ang / 2)[:, None], np.cos(ang / 2)[:, None]], axis=1)
+    return (q / np.linalg.norm(q, axis=1, keepdims=True)).astype(np.float32)
+
+
+def batched_worlds(n_worlds=4096, seed=4, steps=500, min_bodies=8, max_bodies=256):
+    """Batched-worlds configuration: n = floor(exp(U(ln 8, ln 256))) dynamic bodies per world,
+    box columns (heights U{1..16}, 1.5 m apart) or a jittered sphere pile, each on its own plane."""
+    rng = np.random.default_rng(seed)
+    s = BatchScene(f"batched_worlds_{n_worlds}", 1.0 / 60.0, 10, steps)
+    plane = s.add_shape(PLANE, [0.0, 1.0, 0.0, 0.0])
+    box = s.add_shape(BOX, [0.5, 0.5, 0.5])
+    sph = s.add_shape(SPHERE, [0.5])
+    for _ in range(n_worlds):
+        nb = int(math.floor(math.exp(rng.uniform(math.log(min_bodies), math.log(max_bodies)))))
+        if rng.random() < 0.5:  # columns of boxes
+            heights = []
+            left = nb
+            while left > 0:
+                h = min(int(rng.integers(1, 17)), left)
+                heights.append(h)
+                left -= h
+            side = int(math.ceil(math.sqrt(len(heights))))
+            col = np.repeat(np.arange(len(heights)), heights)
+            lvl = np.concatenate([np.arange(h) for h in heights])
+            x = (col % side - (side - 1) / 2) * 1.5
+            z = (col // side - (side - 1) / 2) * 1.5
+            y = 0.55 + lvl * 1.05
+            pos = np.stack([x, y, z], axis=1) + np.concatenate(
+                [rng.uniform(-0.02, 0.02, size=(nb, 1)), np.zeros((nb, 1)), rng.uniform(-0.02, 0.02, size=(nb, 1))],
+                axis=1)
+            quat = _small_rotations(rng, nb, 2.0)
+            kind = box
+        else:  # sphere pile
+            side = int(math.ceil(nb ** (1.0 / 3.0)))
+            t = np.arange(nb)
+            gx, gz, gy = t % side, (t // side) % side, t // (side * side)
+            pos = np.stack([(gx - (side - 1) / 2) * 1.05, 0.6 + gy * 1.05, (gz - (side - 1) / 2) * 1.05], axis=1)
+            pos = pos + rng.uniform(-0.05, 0.05, size=(nb, 3))
+            quat = np.tile(np.array([0, 0, 0, 1], np.float32), (nb, 1))
+            kind = sph
+        shape = np.concatenate([[plane], np.full(nb, kind)])
+        pos = np.concatenate([np.zeros((1, 3)), pos]).astype(np.float32)
+        quat = np.concatenate([np.array([[0, 0, 0, 1]], np.float32), quat])
+        mass = np.concatenate([[0.0], np.ones(nb)])
+        s.add_world(shape, pos, quat, mass)
     return s

@@ -42,6 +42,16 @@ typedef int32_t bgpu_status;
 #define BGPU_ERR_DEVICE_STATUS 4 /* a kernel left a bounded loop or overflowed a fixed buffer */
 #define BGPU_ERR_NO_DEVICE 5
 
+/* Bits of bgpu_step_stats.device_status (no counterpart in the reference, whose
+ * step cannot fail: they report a bounded device loop or a fixed buffer that ran out). */
+#define BGPU_DEVSTAT_UNION_FIND_LIMIT 0x002u  /* island union-find retries */
+#define BGPU_DEVSTAT_BARRIER_TIMEOUT 0x004u   /* a grid barrier gave up waiting */
+#define BGPU_DEVSTAT_COLOUR_OVERFLOW 0x008u   /* more than 128 PGS colours needed */
+#define BGPU_DEVSTAT_EPA_CAPACITY 0x010u      /* EPA vertex/face budget */
+#define BGPU_DEVSTAT_TRAVERSAL_STACK 0x040u   /* BVH traversal stack */
+#define BGPU_DEVSTAT_COLOUR_ROUNDS 0x080u     /* colouring did not converge */
+#define BGPU_DEVSTAT_SOLVE_TIMEOUT 0x100u     /* a PGS row group gave up waiting for its turn */
+
 /* Shape kinds (crates/bullet-collision/src/shapes/mod.rs:61-85, convex subset + plane). */
 #define BGPU_SHAPE_SPHERE 0  /* params: radius */
 #define BGPU_SHAPE_BOX 1     /* params: half extents x, y, z */
@@ -116,6 +126,7 @@ typedef struct bgpu_step_stats {
                                     narrowphase, solve, integrate positions */
     float solve_kernel_ms;       /* the PGS kernel only (inside the solve stage) */
     float step_ms;
+    uint32_t num_split_contacts; /* solver rows with an active split-impulse term */
 } bgpu_step_stats;
 
 typedef struct bgpu_world bgpu_world;
@@ -139,6 +150,25 @@ bgpu_status bgpu_add_shape(bgpu_world* w, uint32_t type, const float* params, co
                            uint32_t num_hull_points, uint32_t* out_shape);
 bgpu_status bgpu_add_bodies(bgpu_world* w, uint32_t n, const bgpu_body_desc* descs, uint32_t* out_first);
 uint32_t bgpu_num_bodies(const bgpu_world* w);
+
+/* Batched worlds (no counterpart in the reference, where every world is one
+ * PhysicsWorld stepped on its own). A batch holds many independent worlds that
+ * one sequence of kernel launches steps together: world k owns a contiguous
+ * range of bodies, pairs only form inside a world (per-world all-pairs broad
+ * phase), and each world keeps its own islands, sleeping and manifold-prune
+ * state (step.rs:1006-1010 per world). Shapes are shared by all worlds. Every
+ * other call (bgpu_step, bgpu_read_state, bgpu_apply_forces, ...) sees the batch
+ * as one body array in world order. */
+bgpu_status bgpu_batch_create(const bgpu_solver_info* info, const float* gravity, bgpu_world** out);
+/* Appends n_worlds worlds whose bodies follow each other in descs (world k has
+ * bodies_per_world[k] bodies); *out_first_world receives the first new world id. */
+bgpu_status bgpu_batch_add_worlds(bgpu_world* w, uint32_t n_worlds, const uint32_t* bodies_per_world,
+                                  const bgpu_body_desc* descs, uint32_t* out_first_world);
+uint32_t bgpu_batch_num_worlds(const bgpu_world* w);
+/* Writes num_worlds + 1 body offsets (world k owns bodies [offsets[k], offsets[k + 1])). */
+bgpu_status bgpu_batch_world_offsets(bgpu_world* w, uint32_t* offsets);
+/* Steps every world of the batch nsteps times (the same as bgpu_step). */
+bgpu_status bgpu_batch_step(bgpu_world* w, float dt, uint32_t nsteps);
 
 /* The step (step.rs:100-199). bgpu_step runs step_simulation(dt) nsteps times. */
 bgpu_status bgpu_step(bgpu_world* w, float dt, uint32_t nsteps);
