@@ -135,6 +135,7 @@ struct PairData {
     DevBuf<uint32_t> split_count, split_offset, split_cursor;
     DevBuf<uint4> batch_rec;         // contact pairs in colour order: body a, body b, pair | rows << 29, 0
     DevBuf<uint4> split_rec;         // the same for the pairs with split-active rows
+    DevBuf<float4> vtab, stab;       // solver contact tables in batch-slot order (k_solver.cu)
     DevBuf<uint32_t> flags;          // selection flags
     DevBuf<uint32_t> sel_a, sel_b;   // cache compaction lists
     DevBuf<unsigned char> cub_tmp;
@@ -159,8 +160,8 @@ struct PairData {
         split_count.reserve(132);
         split_offset.reserve(132);
         split_cursor.reserve(132);
-        batch_rec.reserve(npairs);
-        split_rec.reserve(npairs);
+        batch_rec.reserve(npairs + 32 * 130);  // batches start on multiples of 32
+        split_rec.reserve(npairs + 32 * 130);
         flags.reserve(npairs + old_manifolds + 1);
         sel_a.reserve(npairs);
         sel_b.reserve(old_manifolds + 1);

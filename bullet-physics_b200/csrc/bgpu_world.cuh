@@ -34,7 +34,6 @@ enum : uint32_t {
     ST_NONFINITE = 1u << 5,
     ST_TRAVERSAL_STACK = 1u << 6,
     ST_COLOUR_ROUNDS = 1u << 7,
-    ST_SOLVE_TIMEOUT = 1u << 8,  // a PGS row group gave up waiting for its turn at a body
 };
 
 // Pair status codes written by the classify pass.

@@ -13,10 +13,11 @@
 // The PGS kernel is a persistent cooperative launch split into two teams of
 // blocks with their own grid barriers: the velocity team runs the warm start
 // and the velocity sweeps, the split team the split-impulse sweeps, which
-// touch only the push velocities and so run at the same time. Before waiting
-// at a barrier each thread loads its next group's slot record and prefetches
-// that group's rows and inertia, so after the barrier only the velocities are
-// fetched.
+// touch only the push velocities and so run at the same time. The first
+// sweep of each team computes the per-contact terms that stay fixed during the
+// solve (tangent basis, Iw^-1 (r x d), the velocity couplings kn/kt1/kt2) once
+// and stores them in a contact table in batch-slot order, so the later sweeps
+// run only the impulse update, reading the table with coalesced loads.
 //
 // Rows store only the contact frame (normal, lever arms), the bias terms, the
 // effective masses and the accumulated impulses; the tangent basis, the
@@ -44,17 +45,18 @@ constexpr unsigned int BARRIER_SPIN_LIMIT = 1u << 26;
 __device__ __forceinline__ void team_barrier(unsigned int* ctr, unsigned int target, uint32_t* status) {
     __syncthreads();
     if (threadIdx.x == 0 && !(*(volatile uint32_t*)status & ST_BARRIER_TIMEOUT)) {
-        __threadfence();
-        atomicAdd(ctr, 1u);
-        volatile unsigned int* vc = ctr;
-        unsigned int spins = 0;
-        while (*vc < target) {
+        // The release add publishes the block's writes (ordered before it by the
+        // bar.sync above); the acquire load makes the other blocks' writes visible.
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(ctr) : "memory");
+        unsigned int v, spins = 0;
+        for (;;) {
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(ctr) : "memory");
+            if (v >= target) break;
             if (++spins > BARRIER_SPIN_LIMIT) {
                 atomicOr(status, ST_BARRIER_TIMEOUT);
                 break;
             }
         }
-        __threadfence();
     }
     __syncthreads();
 }
@@ -216,10 +218,14 @@ __global__ void k_colour_scan(uint32_t* hist, uint32_t* offset, uint32_t* cursor
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     uint32_t ncol = bar[5];
     uint32_t acc = 0, sacc = 0, smax = 0;
+    // Batches start on multiples of 32 (one warp's slots never straddle two
+    // batches); after the scatter the cursors hold the batch ends.
     for (uint32_t c = 0; c < ncol; ++c) {
+        acc = (acc + 31u) & ~31u;
         offset[c] = acc;
         cursor[c] = acc;
         acc += hist[c];
+        sacc = (sacc + 31u) & ~31u;
         split_offset[c] = sacc;
         split_cursor[c] = sacc;
         sacc += split_hist[c];
@@ -227,9 +233,11 @@ __global__ void k_colour_scan(uint32_t* hist, uint32_t* offset, uint32_t* cursor
     }
     offset[ncol] = acc;
     split_offset[ncol] = sacc;
+    uint32_t split_groups = 0;
+    for (uint32_t c = 0; c < ncol; ++c) split_groups += split_hist[c];
     scalars[3] = hist[MAX_COLOURS + 1];
     scalars[4] = ncol;
-    scalars[5] = sacc;
+    scalars[5] = split_groups;
     scalars[10] = hist[MAX_COLOURS + 2];
     scalars[11] = smax;
 }
@@ -267,15 +275,19 @@ __global__ void k_colour_scatter(const uint32_t* __restrict__ count, const uint3
 struct SolveArgs {
     float4* rows;
     const uint4* batch_rec;
-    const uint32_t* offset;
+    const uint32_t* offset;   // colour batch starts (multiples of 32)
+    const uint32_t* end;      // colour batch ends
     const uint4* split_rec;
     const uint32_t* split_offset;
+    const uint32_t* split_end;
     const uint32_t* scalars;  // [4] colours [5] split groups [11] largest split batch
     float4* linvel;
     float4* angvel;
     float4* push_lin;
     float4* push_ang;
     const float4* iw;
+    float4* vtab;             // velocity contact table (VT_PLANES planes)
+    float4* stab;             // split contact table (ST_PLANES planes)
     unsigned int* bar;        // [0] velocity-team barrier counter, [1] split-team counter
     uint32_t* status;
     float inv_dt;
@@ -291,38 +303,118 @@ __device__ __forceinline__ void apply(V3& la, V3& wa, V3& lb, V3& wb, bool appa,
 
 enum Kind { WARM = 0, ITER = 1, SPLIT = 2 };
 
-// warm_start (sequential_impulse.rs:710-717) or one solve_contact sweep (:804-930) over a group.
-template <int KIND>
-__device__ __forceinline__ void solve_group(const SolveArgs& a, uint32_t p, uint32_t cnt, const M3& iwa, const M3& iwb,
-                                            float ima, float imb, V3& la, V3& wa, V3& lb, V3& wb) {
-    bool appa = ima > 0.0f, appb = imb > 0.0f;
+// Per-step contact tables in batch-slot order. Slots are grouped 32 at a time
+// (colour batches start on a multiple of 32, so a warp's lanes hold exactly one
+// such group), and each group stores field ("plane") by field and contact by
+// contact, 32 float4 per (plane, contact): element (plane, k, t) sits at
+// ((t / 32 * PLANES + plane) * 4 + k) * 32 + t % 32. A warp's loads are
+// coalesced and everything one warp reads in a sweep lies in one contiguous
+// span of at most 30 KB, so scattered page (TLB) lookups stay few. The first
+// sweep of each team fills its table from the rows and the bodies' inverse
+// inertia; the later sweeps read only the table and the velocities. A slot's
+// table entries are written and read by the same thread only (the slot-to-thread
+// deal is fixed for the launch), so plain L1-cached loads see them; they are
+// never read through the read-only (non-coherent) path, since this kernel
+// writes them.
+//
+// Velocity table planes: 0 n|friction 1 r_a|bias 2 r_b|bias 3 t1|1/m_a
+// 4 t2|1/m_b 5 Iw_a(r_a x n)|normal mass 6 Iw_b(r_b x n)|t1 mass
+// 7 Iw_a(r_a x t1)|t2 mass 8 Iw_b(r_b x t1)|cfm 9 Iw_a(r_a x t2)|restitution
+// 10 Iw_b(r_b x t2) 11 kn 12 kt1 13 kt2 14 accumulated impulses (row 3).
+// Split table planes: 0 n|normal mass 1 r_a|cfm 2 r_b 3 Iw_a(r_a x n)|1/m_a
+// 4 Iw_b(r_b x n)|1/m_b 5 row 5 (rhs, push impulse, active, penetration).
+constexpr uint32_t VT_PLANES = 15;
+constexpr uint32_t ST_PLANES = 6;
+
+template <uint32_t PLANES>
+__device__ __forceinline__ size_t tix(uint32_t plane, uint32_t k, uint32_t t) {
+    return ((size_t(t >> 5) * PLANES + plane) * 4 + k) * 32 + (t & 31u);
+}
+
+__device__ __forceinline__ float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
+
+// warm_start (sequential_impulse.rs:710-717) for group slot t, which also
+// fills the slot's velocity table with the prepared terms the sweeps use
+// (sequential_impulse.rs:352-520 computes the same values in prepare()).
+__device__ __forceinline__ void warm_group(const SolveArgs& a, uint32_t t, uint32_t p, uint32_t cnt, uint32_t ia,
+                                           uint32_t ib, V3& la, V3& wa, V3& lb, V3& wb, bool& appa, bool& appb) {
+    float ima, imb;
+    const M3 iwa = load_iw(a.iw, ia, ima);
+    const M3 iwb = load_iw(a.iw, ib, imb);
+    appa = ima > 0.0f;
+    appb = imb > 0.0f;
     for (uint32_t k = 0; k < cnt; ++k) {
-        float4* r = a.rows + (size_t(p) * 4 + k) * ROW_F4;
-        float4 r0 = r[0], r1 = r[1], r2 = r[2];
-        float4 r3 = r[3];
-        V3 n = from4(r0), ra = from4(r1), rb = from4(r2);
+        const float4* r = a.rows + (size_t(p) * 4 + k) * ROW_F4;
+        const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
+        const V3 n = from4(r0), ra = from4(r1), rb = from4(r2);
         V3 t1, t2;
         tangent_basis_dev(n, t1, t2);
-        V3 ana = mul(iwa, cross(ra, n)), anb = mul(iwb, cross(rb, n));
-        V3 a1a = mul(iwa, cross(ra, t1)), a1b = mul(iwb, cross(rb, t1));
-        V3 a2a = mul(iwa, cross(ra, t2)), a2b = mul(iwb, cross(rb, t2));
-        if (KIND == WARM) {
-            apply(la, wa, lb, wb, appa, appb, ima, imb, n, ana, anb, r3.x);
-            apply(la, wa, lb, wb, appa, appb, ima, imb, t1, a1a, a1b, r3.y);
-            apply(la, wa, lb, wb, appa, appb, ima, imb, t2, a2a, a2b, r3.z);
-            continue;
-        }
-        float4 r4 = r[4];
-        float ims = ima + imb;
-        V3 kn = n * ims + cross(anb, rb) + cross(ana, ra);
-        V3 kt1 = t1 * ims + cross(a1b, rb) + cross(a1a, ra);
-        V3 kt2 = t2 * ims + cross(a2b, rb) + cross(a2a, ra);
+        const V3 ana = mul(iwa, cross(ra, n)), anb = mul(iwb, cross(rb, n));
+        const V3 a1a = mul(iwa, cross(ra, t1)), a1b = mul(iwb, cross(rb, t1));
+        const V3 a2a = mul(iwa, cross(ra, t2)), a2b = mul(iwb, cross(rb, t2));
+        const float ims = ima + imb;
+        const V3 kn = n * ims + cross(anb, rb) + cross(ana, ra);
+        const V3 kt1 = t1 * ims + cross(a1b, rb) + cross(a1a, ra);
+        const V3 kt2 = t2 * ims + cross(a2b, rb) + cross(a2a, ra);
+        apply(la, wa, lb, wb, appa, appb, ima, imb, n, ana, anb, r3.x);
+        apply(la, wa, lb, wb, appa, appb, ima, imb, t1, a1a, a1b, r3.y);
+        apply(la, wa, lb, wb, appa, appb, ima, imb, t2, a2a, a2b, r3.z);
+        float4* v = a.vtab;
+        v[tix<VT_PLANES>(0, k, t)] = r0;
+        v[tix<VT_PLANES>(1, k, t)] = r1;
+        v[tix<VT_PLANES>(2, k, t)] = r2;
+        v[tix<VT_PLANES>(3, k, t)] = f4(t1, ima);
+        v[tix<VT_PLANES>(4, k, t)] = f4(t2, imb);
+        v[tix<VT_PLANES>(5, k, t)] = f4(ana, r4.x);
+        v[tix<VT_PLANES>(6, k, t)] = f4(anb, r4.y);
+        v[tix<VT_PLANES>(7, k, t)] = f4(a1a, r4.z);
+        v[tix<VT_PLANES>(8, k, t)] = f4(a1b, r4.w);
+        v[tix<VT_PLANES>(9, k, t)] = f4(a2a, r3.w);
+        v[tix<VT_PLANES>(10, k, t)] = f4(a2b, 0.0f);
+        v[tix<VT_PLANES>(11, k, t)] = f4(kn, 0.0f);
+        v[tix<VT_PLANES>(12, k, t)] = f4(kt1, 0.0f);
+        v[tix<VT_PLANES>(13, k, t)] = f4(kt2, 0.0f);
+        v[tix<VT_PLANES>(14, k, t)] = r3;
+    }
+}
+
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
+// Bring contact k of slot t's velocity-table entries into L1 (all planes).
+__device__ __forceinline__ void prefetch_contact_l1(const float4* v, uint32_t k, uint32_t t) {
+    for (uint32_t pl = 0; pl < VT_PLANES; ++pl) prefetch_l1(&v[tix<VT_PLANES>(pl, k, t)]);
+}
+
+// One solve_contact sweep (sequential_impulse.rs:804-930) over group slot t;
+// on the last sweep the impulses also go back to the pair's rows.
+__device__ __forceinline__ void iter_group(const SolveArgs& a, uint32_t t, uint32_t p, uint32_t cnt, bool last, V3& la,
+                                           V3& wa, V3& lb, V3& wb, bool& appa, bool& appb) {
+    const float4* v = a.vtab;
+    const float ima = v[tix<VT_PLANES>(3, 0, t)].w, imb = v[tix<VT_PLANES>(4, 0, t)].w;
+    appa = ima > 0.0f;
+    appb = imb > 0.0f;
+    for (uint32_t k = 0; k < cnt; ++k) {
+        if (k + 1 < cnt) prefetch_contact_l1(v, k + 1, t);
+        const float4 r0 = v[tix<VT_PLANES>(0, k, t)], r1 = v[tix<VT_PLANES>(1, k, t)],
+                     r2 = v[tix<VT_PLANES>(2, k, t)];
+        const float4 q3 = v[tix<VT_PLANES>(3, k, t)], q4 = v[tix<VT_PLANES>(4, k, t)];
+        const float4 q5 = v[tix<VT_PLANES>(5, k, t)], q6 = v[tix<VT_PLANES>(6, k, t)];
+        const float4 q7 = v[tix<VT_PLANES>(7, k, t)], q8 = v[tix<VT_PLANES>(8, k, t)];
+        const float4 q9 = v[tix<VT_PLANES>(9, k, t)], q10 = v[tix<VT_PLANES>(10, k, t)];
+        const float4 q11 = v[tix<VT_PLANES>(11, k, t)], q12 = v[tix<VT_PLANES>(12, k, t)];
+        const float4 q13 = v[tix<VT_PLANES>(13, k, t)];
+        const float4 r3 = v[tix<VT_PLANES>(14, k, t)];
+        const V3 n = from4(r0), ra = from4(r1), rb = from4(r2), t1 = from4(q3), t2 = from4(q4);
+        const V3 ana = from4(q5), anb = from4(q6), a1a = from4(q7), a1b = from4(q8), a2a = from4(q9), a2b = from4(q10);
+        const V3 kn = from4(q11), kt1 = from4(q12), kt2 = from4(q13);
+        const float4 r4 = make_float4(q5.w, q6.w, q7.w, q8.w);
         V3 va = la + cross(wa, ra);
         V3 vb = lb + cross(wb, rb);
         V3 rel = vb - va;
         float vn = dot(rel, n);
         float bias = 0.0f;
-        if (vn < -a.restitution_threshold) bias = -r3.w * vn;
+        if (vn < -a.restitution_threshold) bias = -q9.w * vn;
         if (r1.w != 0.0f) bias += r1.w;
         if (r2.w != 0.0f) bias += r2.w;
         float lambda = r4.w != 0.0f ? r4.x * (bias - vn) - r4.w * r3.x : r4.x * (bias - vn);
@@ -345,106 +437,142 @@ __device__ __forceinline__ void solve_group(const SolveArgs& a, uint32_t p, uint
         float n2 = fminf(fmaxf(o2 + lam, -maxf), maxf);
         float j2 = n2 - o2;
         apply(la, wa, lb, wb, appa, appb, ima, imb, t2, a2a, a2b, j2);
-        r[3] = make_float4(nimp, n1, n2, r3.w);
+        const float4 nr3 = make_float4(nimp, n1, n2, r3.w);
+        a.vtab[tix<VT_PLANES>(14, k, t)] = nr3;
+        if (last) a.rows[(size_t(p) * 4 + k) * ROW_F4 + 3] = nr3;
     }
 }
 
-// split_impulse_pass body (sequential_impulse.rs:759-786) for one group.
-__device__ __forceinline__ void split_group(const SolveArgs& a, uint32_t p, uint32_t cnt, const M3& iwa, const M3& iwb,
-                                            float ima, float imb, V3& pla, V3& pwa, V3& plb, V3& pwb) {
-    bool appa = ima > 0.0f, appb = imb > 0.0f;
+// split_impulse_pass body (sequential_impulse.rs:759-786) for split slot t; the
+// first sweep fills the slot's split table, the last writes row 5 back.
+__device__ __forceinline__ void split_group(const SolveArgs& a, uint32_t t, uint32_t p, uint32_t cnt, uint32_t ia,
+                                            uint32_t ib, bool first, bool last, V3& pla, V3& pwa, V3& plb, V3& pwb,
+                                            bool& appa, bool& appb) {
+    float4* s = a.stab;
+    float ima, imb;
+    M3 iwa, iwb;
+    if (first) {
+        iwa = load_iw(a.iw, ia, ima);
+        iwb = load_iw(a.iw, ib, imb);
+    } else {
+        ima = s[tix<ST_PLANES>(3, 0, t)].w;
+        imb = s[tix<ST_PLANES>(4, 0, t)].w;
+    }
+    appa = ima > 0.0f;
+    appb = imb > 0.0f;
     for (uint32_t k = 0; k < cnt; ++k) {
-        float4* r = a.rows + (size_t(p) * 4 + k) * ROW_F4;
-        float4 r5 = r[5];
-        if (r5.z == 0.0f) continue;
-        float4 r0 = r[0], r1 = r[1], r2 = r[2], r4 = r[4];
-        V3 n = from4(r0), ra = from4(r1), rb = from4(r2);
+        float4 q0, q1, q2, q3, q4, r5;
+        if (first) {
+            const float4* r = a.rows + (size_t(p) * 4 + k) * ROW_F4;
+            const float4 r0 = r[0], r1 = r[1], r2 = r[2], r4 = r[4];
+            r5 = r[5];
+            const V3 n = from4(r0), ra = from4(r1), rb = from4(r2);
+            const V3 ana = mul(iwa, cross(ra, n)), anb = mul(iwb, cross(rb, n));
+            q0 = f4(n, r4.x);
+            q1 = f4(ra, r4.w);
+            q2 = f4(rb, 0.0f);
+            q3 = f4(ana, ima);
+            q4 = f4(anb, imb);
+            s[tix<ST_PLANES>(0, k, t)] = q0;
+            s[tix<ST_PLANES>(1, k, t)] = q1;
+            s[tix<ST_PLANES>(2, k, t)] = q2;
+            s[tix<ST_PLANES>(3, k, t)] = q3;
+            s[tix<ST_PLANES>(4, k, t)] = q4;
+        } else {
+            r5 = s[tix<ST_PLANES>(5, k, t)];
+        }
+        if (r5.z == 0.0f) {
+            if (first) s[tix<ST_PLANES>(5, k, t)] = r5;
+            continue;
+        }
+        if (!first) {
+            q0 = s[tix<ST_PLANES>(0, k, t)];
+            q1 = s[tix<ST_PLANES>(1, k, t)];
+            q2 = s[tix<ST_PLANES>(2, k, t)];
+            q3 = s[tix<ST_PLANES>(3, k, t)];
+            q4 = s[tix<ST_PLANES>(4, k, t)];
+        }
+        const V3 n = from4(q0), ra = from4(q1), rb = from4(q2), ana = from4(q3), anb = from4(q4);
+        const float nmass = q0.w, cfm = q1.w;
         V3 pva = pla + cross(pwa, ra);
         V3 pvb = plb + cross(pwb, rb);
         float pvn = dot(pvb - pva, n);
-        float delta = r4.w != 0.0f ? r5.x - pvn * r4.x - r4.w * r5.y : r5.x - pvn * r4.x;
+        float delta = cfm != 0.0f ? r5.x - pvn * nmass - cfm * r5.y : r5.x - pvn * nmass;
         float old = r5.y;
         float np = fmaxf(old + delta, 0.0f);
         float j = np - old;
         if (j != 0.0f) {
-            V3 ana = mul(iwa, cross(ra, n)), anb = mul(iwb, cross(rb, n));
             if (appa) { pla -= n * (j * ima); pwa -= ana * j; }
             if (appb) { plb += n * (j * imb); pwb += anb * j; }
         }
-        r[5] = make_float4(r5.x, np, r5.z, r5.w);
+        const float4 nr5 = make_float4(r5.x, np, r5.z, r5.w);
+        s[tix<ST_PLANES>(5, k, t)] = nr5;
+        if (last) a.rows[(size_t(p) * 4 + k) * ROW_F4 + 5] = nr5;
     }
 }
 
-__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
-
-// Bring a group's rows (a pair's four row slots start on a 128-byte line) and
-// both bodies' inverse inertia into L1 ahead of its turn.
-__device__ __forceinline__ void prefetch_group(const SolveArgs& a, uint4 rec) {
-    const uint32_t p = rec.z & 0x1fffffffu, cnt = rec.z >> 29;
-    const char* r = reinterpret_cast<const char*>(a.rows + size_t(p) * 4 * ROW_F4);
-    for (uint32_t off = 0; off < cnt * ROW_F4 * 16u; off += 128u) prefetch_l1(r + off);
-    const char* ia = reinterpret_cast<const char*>(a.iw + 3 * size_t(rec.x));
-    const char* ib = reinterpret_cast<const char*>(a.iw + 3 * size_t(rec.y));
-    prefetch_l1(ia);
-    prefetch_l1(ia + 47);
-    prefetch_l1(ib);
-    prefetch_l1(ib + 47);
-}
-
-// One group: velocities (or push velocities) from L2, the group's rows, the
+// One group: velocities (or push velocities) from L2, the group's solve, the
 // dynamic bodies' new velocities back to L2.
 template <int KIND>
-__device__ __forceinline__ void run_group(const SolveArgs& a, uint4 rec) {
+__device__ __forceinline__ void run_group(const SolveArgs& a, uint32_t t, uint4 rec, uint32_t sweep, uint32_t last) {
     const uint32_t ia = rec.x, ib = rec.y, p = rec.z & 0x1fffffffu, cnt = rec.z >> 29;
     float4* plin = KIND == SPLIT ? a.push_lin : a.linvel;
     float4* pang = KIND == SPLIT ? a.push_ang : a.angvel;
-    float ima, imb;
-    M3 iwa = load_iw(a.iw, ia, ima);
-    M3 iwb = load_iw(a.iw, ib, imb);
     V3 la = from4(__ldcg(&plin[ia])), wa = from4(__ldcg(&pang[ia]));
     V3 lb = from4(__ldcg(&plin[ib])), wb = from4(__ldcg(&pang[ib]));
-    if (KIND == SPLIT) split_group(a, p, cnt, iwa, iwb, ima, imb, la, wa, lb, wb);
-    else solve_group<KIND>(a, p, cnt, iwa, iwb, ima, imb, la, wa, lb, wb);
-    if (ima > 0.0f) { __stcg(&plin[ia], to4(la, 0.0f)); __stcg(&pang[ia], to4(wa, 0.0f)); }
-    if (imb > 0.0f) { __stcg(&plin[ib], to4(lb, 0.0f)); __stcg(&pang[ib], to4(wb, 0.0f)); }
+    bool appa, appb;  // only dynamic bodies move
+    if (KIND == WARM) warm_group(a, t, p, cnt, ia, ib, la, wa, lb, wb, appa, appb);
+    else if (KIND == ITER) iter_group(a, t, p, cnt, sweep == last, la, wa, lb, wb, appa, appb);
+    else split_group(a, t, p, cnt, ia, ib, sweep == 0, sweep == last, la, wa, lb, wb, appa, appb);
+    if (appa) { __stcg(&plin[ia], to4(la, 0.0f)); __stcg(&pang[ia], to4(wa, 0.0f)); }
+    if (appb) { __stcg(&plin[ib], to4(lb, 0.0f)); __stcg(&pang[ib], to4(wb, 0.0f)); }
 }
 
-// Phases first .. last-1 of a team: phase q is colour q % ncol of sweep
-// q / ncol. The team's threads deal the batch slots of each phase among
-// themselves; between phases the team meets at its barrier, and before it
-// each thread fetches its next slot record and prefetches that group.
 template <bool VELOCITY>
-__device__ __forceinline__ void run_phases(const SolveArgs& a, const uint4* __restrict__ recs,
-                                           const uint32_t* __restrict__ off, uint32_t ncol, uint32_t nphases,
-                                           uint32_t tid, uint32_t stride, unsigned int* ctr, uint32_t team_blocks,
-                                           uint32_t& nbar) {
-    if (ncol == 0) return;
-    uint4 rec = make_uint4(0u, 0u, 0u, 0u);
-    bool has = false;
-    {
-        uint32_t t = off[0] + tid;
-        if (nphases && t < off[1]) { rec = __ldg(&recs[t]); prefetch_group(a, rec); has = true; }
+__device__ __forceinline__ void prefetch_slot_l2(const SolveArgs& a, uint32_t t, uint32_t cnt) {
+    for (uint32_t k = 0; k < cnt; ++k) {
+        if (VELOCITY)
+            for (uint32_t pl = 0; pl < VT_PLANES; ++pl) prefetch_l2(&a.vtab[tix<VT_PLANES>(pl, k, t)]);
+        else
+            for (uint32_t pl = 0; pl < ST_PLANES; ++pl) prefetch_l2(&a.stab[tix<ST_PLANES>(pl, k, t)]);
     }
+}
+
+template <bool VELOCITY>
+__device__ __forceinline__ void run_item(const SolveArgs& a, uint32_t sweep, uint32_t last, uint32_t t, uint4 rec) {
+    if (!VELOCITY) run_group<SPLIT>(a, t, rec, sweep, last);
+    else if (sweep == 0) run_group<WARM>(a, t, rec, sweep, last);
+    else run_group<ITER>(a, t, rec, sweep, last);
+}
+
+// Phases 0 .. nphases-1 of a team: phase q is colour q % ncol of sweep q / ncol.
+// The team's threads deal the batch slots of each phase among themselves and
+// meet at the team barrier between phases; each thread reads its next slot
+// record while it solves the current one.
+template <bool VELOCITY>
+__device__ __forceinline__ void run_phases(const SolveArgs& a, const uint4* __restrict__ recs, const uint32_t* soff,
+                                           const uint32_t* send, uint32_t ncol, uint32_t nphases, uint32_t last, uint32_t tid,
+                                           uint32_t stride, unsigned int* ctr, uint32_t team_blocks, uint32_t& nbar) {
+    if (ncol == 0 || nphases == 0) return;
+    auto first_rec = [&](uint32_t c) -> uint4 {
+        const uint32_t t = soff[c] + tid;
+        return t < send[c] ? __ldg(&recs[t]) : make_uint4(0u, 0u, 0u, 0u);
+    };
+    uint4 rec = first_rec(0);  // rec.z == 0 (no rows): no slot for this thread
     for (uint32_t q = 0; q < nphases; ++q) {
         const uint32_t c = q % ncol, sweep = q / ncol;
-        const uint32_t end = off[c + 1];
-        if (has) {
-            if (!VELOCITY) run_group<SPLIT>(a, rec);
-            else if (sweep == 0) run_group<WARM>(a, rec);
-            else run_group<ITER>(a, rec);
-            for (uint32_t t = off[c] + tid + stride; t < end; t += stride) {
-                uint4 r2 = __ldg(&recs[t]);
-                if (!VELOCITY) run_group<SPLIT>(a, r2);
-                else if (sweep == 0) run_group<WARM>(a, r2);
-                else run_group<ITER>(a, r2);
-            }
+        const uint4 next = q + 1 < nphases ? first_rec((q + 1) % ncol) : make_uint4(0u, 0u, 0u, 0u);
+        if (rec.z) {
+            run_item<VELOCITY>(a, sweep, last, soff[c] + tid, rec);
+            for (uint32_t t = soff[c] + tid + stride; t < send[c]; t += stride)
+                run_item<VELOCITY>(a, sweep, last, t, __ldg(&recs[t]));
         }
-        if (q + 1 == nphases) break;
-        const uint32_t cn = (q + 1) % ncol;
-        const uint32_t tn = off[cn] + tid;
-        has = tn < off[cn + 1];
-        if (has) { rec = __ldg(&recs[tn]); prefetch_group(a, rec); }
-        team_barrier(ctr, ++nbar * team_blocks, a.status);
+        rec = next;
+        if (q + 1 < nphases) {
+            // The next phase's table entries (written in sweep 0) head for L2 while the team waits.
+            if (rec.z && (q + 1) >= ncol) prefetch_slot_l2<VELOCITY>(a, soff[(q + 1) % ncol] + tid, rec.z >> 29);
+            team_barrier(ctr, ++nbar * team_blocks, a.status);
+        }
     }
 }
 
@@ -452,7 +580,7 @@ __device__ __forceinline__ void run_phases(const SolveArgs& a, const uint4* __re
 // the velocity team; the split sweeps on the split team, which has enough
 // blocks for the largest split batch and at most a quarter of the grid (none
 // on a grid too small to split, where the velocity team runs them last).
-__global__ void k_solve(SolveArgs a) {
+__global__ void __launch_bounds__(256, 2) k_solve(SolveArgs a) {
     const uint32_t ncol = a.scalars[4];
     const uint32_t nsplit = a.scalars[5];
     const uint32_t iters = a.iterations;
@@ -467,15 +595,25 @@ __global__ void k_solve(SolveArgs a) {
     const uint32_t team_block = split_team ? blockIdx.x - (G - split_blocks) : blockIdx.x;
     const uint32_t tid = team_block * blockDim.x + threadIdx.x;
     const uint32_t stride = team_blocks * blockDim.x;
+    __shared__ uint32_t s_off[MAX_COLOURS], s_end[MAX_COLOURS], s_split_off[MAX_COLOURS], s_split_end[MAX_COLOURS];
+    for (uint32_t c = threadIdx.x; c < ncol; c += blockDim.x) {
+        s_off[c] = a.offset[c];
+        s_end[c] = a.end[c];
+        s_split_off[c] = a.split_offset[c];
+        s_split_end[c] = a.split_end[c];
+    }
+    __syncthreads();
     uint32_t nbar = 0;
     if (split_team) {
-        run_phases<false>(a, a.split_rec, a.split_offset, ncol, iters * ncol, tid, stride, a.bar + 1, team_blocks, nbar);
+        run_phases<false>(a, a.split_rec, s_split_off, s_split_end, ncol, iters * ncol, iters - 1u, tid, stride, a.bar + 1,
+                          team_blocks, nbar);
         return;
     }
-    run_phases<true>(a, a.batch_rec, a.offset, ncol, (iters + 1) * ncol, tid, stride, a.bar, team_blocks, nbar);
+    run_phases<true>(a, a.batch_rec, s_off, s_end, ncol, (iters + 1) * ncol, iters, tid, stride, a.bar, team_blocks, nbar);
     if (nsplit && iters && split_blocks == 0) {
         team_barrier(a.bar, ++nbar * team_blocks, a.status);
-        run_phases<false>(a, a.split_rec, a.split_offset, ncol, iters * ncol, tid, stride, a.bar, team_blocks, nbar);
+        run_phases<false>(a, a.split_rec, s_split_off, s_split_end, ncol, iters * ncol, iters - 1u, tid, stride, a.bar, team_blocks,
+                          nbar);
     }
 }
 
@@ -617,9 +755,15 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
     // PGS (cooperative launch: the teams' barriers need every block resident).
     check_cuda(cudaMemsetAsync(pd.barrier.p, 0, 2 * sizeof(unsigned int), s), "memset barrier");
     mark(5);
-    SolveArgs sa{pd.rows.p, pd.batch_rec.p, pd.colour_offset.p, pd.split_rec.p, pd.split_offset.p, pd.scalars.p,
-                 w.b.linvel, w.b.angvel, w.b.push_lin, w.b.push_ang, w.b.iw, pd.barrier.p, status_dev, sp.inv_dt,
-                 sp.info.restitution_velocity_threshold, sp.info.num_iterations};
+    // Slot capacity: every group plus the 32-alignment padding of each batch.
+    const size_t slots = (size_t(npairs) + 32u * (MAX_COLOURS + 1) + 31u) & ~size_t(31);
+    pd.vtab.reserve(size_t(VT_PLANES) * 4 * slots);
+    pd.stab.reserve(size_t(ST_PLANES) * 4 * slots);
+    SolveArgs sa{pd.rows.p, pd.batch_rec.p, pd.colour_offset.p, pd.colour_cursor.p, pd.split_rec.p,
+                 pd.split_offset.p, pd.split_cursor.p, pd.scalars.p, w.b.linvel, w.b.angvel, w.b.push_lin,
+                 w.b.push_ang, w.b.iw, pd.vtab.p, pd.stab.p,
+                 pd.barrier.p, status_dev, sp.inv_dt, sp.info.restitution_velocity_threshold,
+                 sp.info.num_iterations};
     static int solve_grid = 0;
     if (!solve_grid) solve_grid = coop_grid((const void*)k_solve, TB, 0);
     void* sargs[] = {&sa};

@@ -50,7 +50,6 @@ typedef int32_t bgpu_status;
 #define BGPU_DEVSTAT_EPA_CAPACITY 0x010u      /* EPA vertex/face budget */
 #define BGPU_DEVSTAT_TRAVERSAL_STACK 0x040u   /* BVH traversal stack */
 #define BGPU_DEVSTAT_COLOUR_ROUNDS 0x080u     /* colouring did not converge */
-#define BGPU_DEVSTAT_SOLVE_TIMEOUT 0x100u     /* a PGS row group gave up waiting for its turn */
 
 /* Shape kinds (crates/bullet-collision/src/shapes/mod.rs:61-85, convex subset + plane). */
 #define BGPU_SHAPE_SPHERE 0  /* params: radius */
