@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--batch-worlds", type=int, default=4096, help="batched-worlds leg: number of worlds (0: skip)")
     p.add_argument("--batch-steps", type=int, default=30)
+    p.add_argument("--adjoint-worlds", type=int, default=1024, help="adjoint leg: number of worlds (0: skip)")
     return p.parse_args()
 
 
@@ -210,6 +211,37 @@ def bench_batched(bgpu, scenes, n_worlds, steps, warmup, sample_worlds=32, sampl
             "device_status": st["device_status"]}
 
 
+def bench_adjoint(bgpu, scenes, n_worlds, steps=120, every=20):
+    """Adjoint leg: 1,024 worlds x 64 thrown boxes, 120 steps at dt 1/120. Times the plain
+    forward (bgpu_step), the taped forward (with checkpoints) and the backward pass (replay of
+    every segment with recording, then the reverse sweeps), all device time."""
+    sc = scenes.adjoint_worlds(n_worlds=n_worlds, seed=5, steps=steps)
+    w = sc.build_gpu(bgpu)
+    tape = bgpu.Tape(w, every)
+    tape.forward(sc.dt, steps)  # first pass: grows the world's buffers
+    tape.rewind()
+    plain_ms = w.step_timed(sc.dt, steps)  # the same rollout, plain steps
+    tape.rewind()
+    tape.forward(sc.dt, steps)
+    st = w.state()
+    loss, gx = scenes.com_loss(st[:, 0:3], sc.arrays()["mass"], w.world_offsets(), sc.targets)
+    g = tape.backward(gx.astype(np.float32))  # first call: allocates the segment records
+    fwd_ms, cold_bwd_ms = tape.timing()
+    g = tape.backward(gx.astype(np.float32))
+    _, bwd_ms = tape.timing()
+    tape.close()
+    w.close()
+    n_dyn = sc.num_dynamic
+    return {"workload": f"adjoint_worlds_{n_worlds} (config 5): {n_dyn} boxes, {steps} steps, dt 1/120, "
+                        f"10 iterations, checkpoint every {every} steps",
+            "value": steps / (bwd_ms / 1000.0), "unit": "adjoint steps/s",
+            "plain_forward_ms": plain_ms, "taped_forward_ms": fwd_ms, "backward_ms": bwd_ms,
+            "backward_first_call_ms": cold_bwd_ms,
+            "backward_over_plain_forward": bwd_ms / plain_ms if plain_ms > 0 else None,
+            "plain_steps_per_s": steps / (plain_ms / 1000.0), "loss": loss,
+            "grad_norms": {k: float(np.linalg.norm(v)) for k, v in g.items()}}
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -334,6 +366,8 @@ def main():
         }
         if args.batch_worlds > 0:
             line["batched_worlds"] = bench_batched(bgpu, scenes, args.batch_worlds, args.batch_steps, args.warmup)
+        if args.adjoint_worlds > 0:
+            line["adjoint"] = bench_adjoint(bgpu, scenes, args.adjoint_worlds)
         if world_size == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(grid_of(args.cpu_sample_grid), min(args.preroll, 240), 30)
         print(json.dumps(line), flush=True)

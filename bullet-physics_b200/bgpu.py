@@ -102,6 +102,12 @@ def lib():
             "bgpu_batch_num_worlds": (U32, [P]),
             "bgpu_batch_world_offsets": (S, [P, U32P]),
             "bgpu_batch_step": (S, [P, ctypes.c_float, U32]),
+            "bgpu_tape_create": (S, [P, U32, ctypes.POINTER(P)]),
+            "bgpu_tape_destroy": (None, [P]),
+            "bgpu_tape_forward": (S, [P, ctypes.c_float, U32]),
+            "bgpu_tape_backward": (S, [P, F, F, F, F, F]),
+            "bgpu_tape_timing": (S, [P, F, F]),
+            "bgpu_tape_rewind": (S, [P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -386,6 +392,56 @@ class World:
         out = np.zeros((self.num_bodies, 6), dtype=np.float32)
         check(self.L.bgpu_read_push(self.h, fptr(out)), "read_push")
         return out
+
+
+class Tape:
+    """Adjoint of a world's steps (bgpu_tape_*): forward with checkpoints, then gradients
+    of a loss of the final state w.r.t. initial velocities, friction and restitution."""
+
+    def __init__(self, world, checkpoint_every=20):
+        self.L = lib()
+        self.world = world  # the world must outlive the tape
+        self.h = ctypes.c_void_p()
+        check(self.L.bgpu_tape_create(world.h, checkpoint_every, ctypes.byref(self.h)), "bgpu_tape_create")
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.L.bgpu_tape_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self, dt, nsteps):
+        check(self.L.bgpu_tape_forward(self.h, dt, nsteps), "bgpu_tape_forward")
+
+    def backward(self, grad_x, grad_v=None, grad_w=None):
+        """grad_x, grad_v, grad_w: (n, 3) dL/d(final position, linear, angular velocity).
+        Returns dict of gradients: v0 (n,3), w0 (n,3), friction (n,), restitution (n,)."""
+        n = self.world.num_bodies
+        g = np.zeros((n, 9), dtype=np.float32)
+        g[:, 0:3] = grad_x
+        if grad_v is not None:
+            g[:, 3:6] = grad_v
+        if grad_w is not None:
+            g[:, 6:9] = grad_w
+        out = {"v0": np.zeros((n, 3), np.float32), "w0": np.zeros((n, 3), np.float32),
+               "friction": np.zeros(n, np.float32), "restitution": np.zeros(n, np.float32)}
+        check(self.L.bgpu_tape_backward(self.h, fptr(g), fptr(out["v0"]), fptr(out["w0"]), fptr(out["friction"]),
+                                        fptr(out["restitution"])), "bgpu_tape_backward")
+        return out
+
+    def rewind(self):
+        check(self.L.bgpu_tape_rewind(self.h), "bgpu_tape_rewind")
+
+    def timing(self):
+        f = ctypes.c_float()
+        b = ctypes.c_float()
+        check(self.L.bgpu_tape_timing(self.h, ctypes.byref(f), ctypes.byref(b)), "bgpu_tape_timing")
+        return f.value, b.value
 
 
 def broadphase_pairs(aabbs):

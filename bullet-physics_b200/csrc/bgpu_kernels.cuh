@@ -23,6 +23,7 @@ template <class T>
 struct DevBuf {
     T* p = nullptr;
     size_t cap = 0;
+    size_t cap_hint = 0;  // capacity before the last growth
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
@@ -31,12 +32,22 @@ struct DevBuf {
         if (p) cudaFree(p);
         p = nullptr;
         cap = 0;
+        cap_hint = 0;
     }
-    // Grow to at least n elements (contents are not preserved).
+    void release_keep_cap() {
+        cap_hint = cap;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    // Grow to at least n elements (contents are not preserved). Growth is
+    // geometric, so a scene whose pair or contact counts creep up step by step
+    // reallocates (and synchronises in cudaFree) only a few times.
     void reserve(size_t n) {
         if (n <= cap) return;
-        release();
+        release_keep_cap();
         size_t c = n < 16 ? 16 : n;
+        if (c < cap_hint + cap_hint / 2) c = cap_hint + cap_hint / 2;
         check_cuda(cudaMalloc(&p, c * sizeof(T)), "cudaMalloc");
         cap = c;
     }
@@ -55,6 +66,66 @@ struct DevBuf {
         cap = c;
     }
 };
+
+// ---------------------------------------------------------------- device helpers shared by the solver and its adjoint
+constexpr unsigned int BARRIER_SPIN_LIMIT = 1u << 26;
+
+// Barrier of a team of co-resident blocks (a cooperative launch) on a counter
+// that only grows during the launch: the k-th barrier (k from 1) of a team of
+// n blocks completes when the counter reaches k * n. One atomic per block,
+// then a tight spin. The spin is bounded: on timeout the status word records
+// it and every later barrier returns at once, so no launch can hang the device.
+__device__ __forceinline__ void team_barrier(unsigned int* ctr, unsigned int target, uint32_t* status) {
+    __syncthreads();
+    if (threadIdx.x == 0 && !(*(volatile uint32_t*)status & ST_BARRIER_TIMEOUT)) {
+        // The release add publishes the block's writes (ordered before it by the
+        // bar.sync above); the acquire load makes the other blocks' writes visible.
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(ctr) : "memory");
+        unsigned int v, spins = 0;
+        for (;;) {
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(ctr) : "memory");
+            if (v >= target) break;
+            if (++spins > BARRIER_SPIN_LIMIT) {
+                atomicOr(status, ST_BARRIER_TIMEOUT);
+                break;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Per-step contact tables in batch-slot order. Slots are grouped 32 at a time
+// (colour batches start on a multiple of 32, so a warp's lanes hold exactly one
+// such group), and each group stores field ("plane") by field and contact by
+// contact, 32 float4 per (plane, contact): element (plane, k, t) sits at
+// ((t / 32 * PLANES + plane) * 4 + k) * 32 + t % 32. A warp's loads are
+// coalesced and everything one warp reads in a sweep lies in one contiguous
+// span of at most 30 KB, so scattered page (TLB) lookups stay few. The first
+// sweep of each team fills its table from the rows and the bodies' inverse
+// inertia; the later sweeps read only the table and the velocities. A slot's
+// table entries are written and read by the same thread only (the slot-to-thread
+// deal is fixed for the launch), so plain L1-cached loads see them; they are
+// never read through the read-only (non-coherent) path, since this kernel
+// writes them.
+//
+// Velocity table planes: 0 n|friction 1 r_a|bias 2 r_b|bias 3 t1|1/m_a
+// 4 t2|1/m_b 5 Iw_a(r_a x n)|normal mass 6 Iw_b(r_b x n)|t1 mass
+// 7 Iw_a(r_a x t1)|t2 mass 8 Iw_b(r_b x t1)|cfm 9 Iw_a(r_a x t2)|restitution
+// 10 Iw_b(r_b x t2) 11 kn 12 kt1 13 kt2 14 accumulated impulses (row 3).
+// Split table planes: 0 n|normal mass 1 r_a|cfm 2 r_b 3 Iw_a(r_a x n)|1/m_a
+// 4 Iw_b(r_b x n)|1/m_b 5 row 5 (rhs, push impulse, active, penetration).
+constexpr uint32_t VT_PLANES = 15;
+constexpr uint32_t ST_PLANES = 6;
+
+// Adjoint sweep record of (sweep >= 1, contact k, slot t), in 32-slot blocks like the tables.
+__device__ __forceinline__ size_t sweep_index(uint32_t sweep, uint32_t k, uint32_t t, uint32_t iters) {
+    return ((size_t(t >> 5) * iters + (sweep - 1)) * 4 + k) * 32 + (t & 31u);
+}
+
+template <uint32_t PLANES>
+__device__ __forceinline__ size_t tix(uint32_t plane, uint32_t k, uint32_t t) {
+    return ((size_t(t >> 5) * PLANES + plane) * 4 + k) * 32 + (t & 31u);
+}
 
 // ---------------------------------------------------------------- body kernels (k_body.cu)
 void launch_integrate_velocities(const BodyDev& b, const Shape* shapes, const float4* hull, uint32_t n, float dt,
@@ -100,6 +171,19 @@ struct StepParams {
     SolverParams info;
 };
 
+constexpr uint32_t REC_NONE = 0xffffffffu;
+
+// Records of one forward step for the adjoint (every pointer null when not recording).
+struct RecordDev {
+    uint8_t* pt_src = nullptr;    // per pair x 4: index, in the old cache entry, of each point the pair pass
+                                  // stored before the narrow phase (0xff: none)
+    uint32_t* pair_old = nullptr;  // per pair: position of its manifold in the old cache, or REC_NONE
+    uint32_t* row_src = nullptr;   // per pair x 4: old cache position * 4 + point whose impulse warm-started
+                                   // the row, or REC_NONE
+    uint32_t* merge_pos = nullptr;  // per pair: position of its manifold in the merged cache, or REC_NONE
+    float4* sweeps = nullptr;       // per (sweep, slot, contact): normal velocity, normal impulse, clamp bits
+};
+
 // Raw device pointers of PairData, passed to kernels by value.
 struct PairDataDev {
     uint32_t* status;
@@ -111,6 +195,7 @@ struct PairDataDev {
     uint32_t* route_list;
     uint32_t* old_owned;
     uint32_t* scalars;
+    RecordDev rec;
 };
 
 struct PairData {
@@ -140,6 +225,7 @@ struct PairData {
     DevBuf<uint32_t> sel_a, sel_b;   // cache compaction lists
     DevBuf<unsigned char> cub_tmp;
     DevBuf<unsigned int> barrier;    // grid barrier words + round counters
+    RecordDev rec;                   // set by an adjoint tape while it records a step
     void reserve(size_t npairs, size_t nbodies, size_t old_manifolds) {
         status.reserve(npairs);
         entries.reserve(npairs * ENTRY_F4);
@@ -169,7 +255,7 @@ struct PairData {
     }
     PairDataDev dev() {
         return PairDataDev{status.p, entries.p, detect.p, detect_n.p, row_count.p, rows.p, route_list.p, old_owned.p,
-                           scalars.p};
+                           scalars.p, rec};
     }
 };
 
@@ -215,5 +301,25 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
 void run_cache_update(const uint64_t* pairs, uint32_t npairs, const Manifolds& old_cache, PairData& pd,
                       Manifolds& next, const uint32_t* world_of, const uint32_t* simulate_flag,
                       const uint32_t* prev_simulate, cudaStream_t s);
+
+// ---------------------------------------------------------------- adjoint (k_adjoint.cu)
+// One recorded step as the reverse solve reads it (device pointers).
+struct AdjStep {
+    const uint4* recs;          // batch slot records
+    const uint32_t* off;        // colour batch starts (ncol)
+    const uint32_t* end;        // colour batch ends (ncol)
+    uint32_t ncol;
+    uint32_t iters;
+    const float4* tab;          // velocity contact table
+    const float4* sweeps;       // per-sweep records
+    const uint32_t* merge_pos;  // pair -> merged cache position
+    const uint32_t* row_src;    // row -> old cache position * 4 + point
+};
+void launch_adj_positions(uint32_t n, float dt, const uint8_t* flags, const float4* xbar, float4* vbar, cudaStream_t s);
+void launch_adj_velocities(uint32_t n, float dt, const uint8_t* flags, const float4* material, float4* vbar,
+                           float4* wbar, cudaStream_t s);
+void run_adj_solve(const AdjStep& st, float4* lbar, float4* vbar, float4* wbar, float* mubar, float* ebar,
+                   const float4* material, const float* carry_in, float* carry_out, float restitution_threshold,
+                   float warm_factor, unsigned int* bar, uint32_t* status_dev, cudaStream_t s);
 
 }  // namespace bgpu

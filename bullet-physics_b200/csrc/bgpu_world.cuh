@@ -74,6 +74,14 @@ struct BodyDev {
     float4* iw;           // world inverse inertia: 3 float4 per body (9 entries column-major + inv mass)
     float4* push_lin;
     float4* push_ang;
+    uint8_t* rec_flags = nullptr;  // adjoint recording only: RF_* bits per body for the step
+};
+
+// Per-body bits of a recorded step (the adjoint's frozen sleep / integration decisions).
+enum : uint8_t {
+    RF_INTEGRATED = 1,  // integrate_velocities ran (dynamic and active)
+    RF_ZEROED = 2,      // the island went to sleep: velocities were zeroed before the solve
+    RF_MOVED = 4,       // the pose was integrated with the solved velocities
 };
 
 // Persistent manifold entry: 16 float4 (manifold.rs:168-186 + 4 points of manifold.rs:124-142).

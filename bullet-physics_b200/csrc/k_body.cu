@@ -75,6 +75,7 @@ __global__ void k_integrate_velocities(BodyDev b, const Shape* __restrict__ shap
         w += gyroscopic_implicit(inv_local, q, w, dt);
         b.linvel[i] = to4(v, 0.0f);
         b.angvel[i] = to4(w, 0.0f);
+        if (b.rec_flags) b.rec_flags[i] |= RF_INTEGRATED;
     }
     V3 p = from4(p4);
     V3 pred = (stat || !active) ? p : p + v * dt;
@@ -161,6 +162,7 @@ __global__ void k_integrate_positions(BodyDev b, uint32_t n, float dt, float tur
     if (!stat && active) {
         interpolate_pose(p, q, v, w, dt);
         moved = true;
+        if (b.rec_flags) b.rec_flags[i] |= RF_MOVED;
     }
     V3 pl = from4(b.push_lin[i]), pw = from4(b.push_ang[i]);
     if (active && !stat && !kin && (pl.x != 0.0f || pl.y != 0.0f || pl.z != 0.0f)) {

@@ -104,7 +104,8 @@ __global__ void k_kinematic_wake(const uint4* __restrict__ info, const float4* _
 // islands.rs:281-294 + body.rs:578-624; also raises the `simulate` flag (step.rs:440) of the
 // body's world (world_of is null for a single world).
 __global__ void k_uf_apply(uint4* info, float4* lv, float4* av, float4* sleep, uint32_t n, const uint32_t* __restrict__ root,
-                           const uint32_t* __restrict__ awake, const uint32_t* __restrict__ world_of, uint32_t* simulate) {
+                           const uint32_t* __restrict__ awake, const uint32_t* __restrict__ world_of, uint32_t* simulate,
+                           uint8_t* rec_flags) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint4 in = info[i];
@@ -125,6 +126,7 @@ __global__ void k_uf_apply(uint4* info, float4* lv, float4* av, float4* sleep, u
         }
         lv[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         av[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (rec_flags) rec_flags[i] |= RF_ZEROED;
     }
     bool active = in.z == ACT_ACTIVE || in.z == ACT_WANTS_DEACTIVATION || in.z == ACT_DISABLE_DEACTIVATION;
     if (active) atomicOr(&simulate[world_of ? world_of[i] : 0u], 1u);
@@ -146,7 +148,7 @@ void Islands::run(const BodyDev& b, uint32_t n, const uint64_t* pairs, uint32_t 
         k_kinematic_wake<<<(npairs + TB - 1) / TB, TB, 0, s>>>(b.info, b.linvel, b.angvel, pairs, npairs, parent.p,
                                                                 awake.p);
     k_uf_apply<<<(n + TB - 1) / TB, TB, 0, s>>>(b.info, b.linvel, b.angvel, b.sleep, n, parent.p, awake.p, world_of,
-                                                 simulate_flag);
+                                                 simulate_flag, b.rec_flags);
 }
 
 }  // namespace bgpu

@@ -21,6 +21,7 @@ struct Pt {
     V3 la, lb, n;
     float pen, imp;
     uint32_t life;
+    uint32_t src;  // index of the point in the entry it was loaded from (0xff: new); not stored
 };
 
 struct Entry {
@@ -48,6 +49,7 @@ __device__ __forceinline__ Entry load_entry(const float4* __restrict__ e) {
         E.p[k].la = from4(x); E.p[k].pen = x.w;
         E.p[k].lb = from4(y); E.p[k].imp = y.w;
         E.p[k].n = from4(z); E.p[k].life = __float_as_uint(z.w);
+        E.p[k].src = uint32_t(k);
     }
     return E;
 }
@@ -85,6 +87,7 @@ struct Out {
     int n;
     V3 pos[4], nrm[4];
     float pen[4], imp[4];
+    uint32_t src[4];  // the loaded entry's index of the point each row comes from (0xff: new point)
 };
 
 // manifold.rs:246-282 — survivors keep their order, so out k addresses cache point k.
@@ -104,7 +107,7 @@ __device__ __forceinline__ void refresh(Entry& E, V3 pa, Q qa, V3 pb, Q qb, Out&
         if (len2(lat) > thr_sq) continue;
         p.pen = pen;
         p.life += 1;
-        o.pos[o.n] = wb; o.nrm[o.n] = p.n; o.pen[o.n] = pen; o.imp[o.n] = p.imp; o.n++;
+        o.pos[o.n] = wb; o.nrm[o.n] = p.n; o.pen[o.n] = pen; o.imp[o.n] = p.imp; o.src[o.n] = p.src; o.n++;
         E.p[kept++] = p;
     }
     E.meta = (E.meta & ~7u) | uint32_t(kept);
@@ -133,10 +136,12 @@ __device__ __forceinline__ void capture(Entry& E, const Manifold& m, V3 pa, Q qa
         pt.pen = m.pen[c];
         pt.imp = 0.0f;
         pt.life = 0;
+        pt.src = 0xffu;
         bool matched = false;
         for (int k = 0; k < n; ++k) {
             if (len2(pts[k].la - pt.la) < thr_sq && dot(pts[k].n, pt.n) >= 0.9f) {
                 pt.imp = pts[k].imp;
+                pt.src = pts[k].src;
                 pts[k] = pt;
                 matched = true;
                 break;
@@ -172,8 +177,11 @@ __device__ __forceinline__ float effective_mass(float ima, float imb, V3 aa, V3 
 }
 
 // step.rs:750-764 + sequential_impulse.rs:339-550: one prepared row per refreshed point.
+// rec_row_src (adjoint recording, else null) receives, per row, the old cache position * 4 + point
+// index that supplied its warm-start impulse (old: the pair's old cache position, or -1).
 __device__ __forceinline__ void emit_rows(const BodyDev& b, uint32_t i, uint32_t j, const Out& o, const StepParams& sp,
-                                          float4* __restrict__ rows, uint32_t* __restrict__ row_count, uint32_t p) {
+                                          float4* __restrict__ rows, uint32_t* __restrict__ row_count, uint32_t p,
+                                          uint32_t* rec_row_src, int64_t old) {
     float ima, imb;
     M3 iwa = load_iw(b.iw, i, ima);
     M3 iwb = load_iw(b.iw, j, imb);
@@ -219,6 +227,8 @@ __device__ __forceinline__ void emit_rows(const BodyDev& b, uint32_t i, uint32_t
         r[3] = make_float4(imp, 0.0f, 0.0f, restitution);
         r[4] = make_float4(nm, t1m, t2m, ncfm);
         r[5] = make_float4(rhs, 0.0f, split ? 1.0f : 0.0f, pen);
+        if (rec_row_src)
+            rec_row_src[size_t(p) * 4 + k] = (old >= 0 && o.src[k] < 4u) ? uint32_t(old) * 4u + o.src[k] : REC_NONE;
     }
     row_count[p] = uint32_t(o.n);
 }
@@ -297,13 +307,17 @@ __global__ void k_classify(BodyDev b, const Shape* __restrict__ shapes, const ui
         for (int k = 0; k < o.n; ++k) if (o.pen[k] > sp.info.linear_slop) deep = true;
         if (!fast || !deep) {
             store_entry(ne, E);
-            if (!no_response) emit_rows(b, i, j, o, sp, pd.rows, pd.row_count, p);
+            if (!no_response) emit_rows(b, i, j, o, sp, pd.rows, pd.row_count, p, pd.rec.row_src, old);
             pd.status[p] = PS_SERVED;
             return;
         }
     }
     if (old >= 0) store_entry(ne, E);
     else store_meta_only(ne, 0u);
+    if (pd.rec.pt_src) {  // where the stored points came from, for the capture pass
+        pd.rec.pair_old[p] = old >= 0 ? uint32_t(old) : REC_NONE;
+        for (int k = 0; k < 4; ++k) pd.rec.pt_src[size_t(p) * 4 + k] = (old >= 0 && k < E.count()) ? uint8_t(E.p[k].src) : uint8_t(0xff);
+    }
     uint32_t route = route_of(shapes[ia.x].type, shapes[ib.x].type);
     pd.status[p] = PS_DETECT | (route << 8);
     if (route == NP_NONE) return;
@@ -436,6 +450,8 @@ __device__ __forceinline__ void capture_one(const BodyDev& b, const Shape* __res
     uint32_t meta = __float_as_uint(ne[2].w);
     if (meta & META_VALID) {
         E = load_entry(ne);
+        if (pd.rec.pt_src)
+            for (int k = 0; k < E.count(); ++k) E.p[k].src = pd.rec.pt_src[size_t(p) * 4 + k];
     } else {
         E.meta = 0;
         E.thr = 0.02f;
@@ -447,7 +463,10 @@ __device__ __forceinline__ void capture_one(const BodyDev& b, const Shape* __res
     Out o;
     refresh(E, pa, qa, pb, qb, o);
     store_entry(ne, E);
-    if (((ia.y | ib.y) & BF_NO_RESPONSE) == 0) emit_rows(b, i, j, o, sp, pd.rows, pd.row_count, p);
+    if (((ia.y | ib.y) & BF_NO_RESPONSE) == 0) {
+        const int64_t old = pd.rec.pair_old ? (pd.rec.pair_old[p] == REC_NONE ? -1 : int64_t(pd.rec.pair_old[p])) : -1;
+        emit_rows(b, i, j, o, sp, pd.rows, pd.row_count, p, pd.rec.row_src, old);
+    }
 }
 
 __global__ void k_capture(BodyDev b, const Shape* __restrict__ shapes, const uint64_t* __restrict__ pairs,
@@ -517,7 +536,7 @@ __global__ void k_prepare_contacts(BodyDev b, uint32_t ngroups, const uint32_t* 
     // The caller's impulse is already the warm-start value: undo the factor emit_rows applies.
     StepParams q = sp;
     q.info.warmstarting_factor = 1.0f;
-    emit_rows(b, i, j, o, q, rows, row_count, g);
+    emit_rows(b, i, j, o, q, rows, row_count, g, nullptr, -1);
 }
 
 }  // namespace

@@ -35,31 +35,6 @@ namespace {
 constexpr uint32_t NO_COLOUR = 0xffffffffu;
 constexpr int MAX_COLOURS = 128;
 constexpr int MAX_ROUNDS = 1024;
-constexpr unsigned int BARRIER_SPIN_LIMIT = 1u << 26;
-
-// Barrier of a team of co-resident blocks (a cooperative launch) on a counter
-// that only grows during the launch: the k-th barrier (k from 1) of a team of
-// n blocks completes when the counter reaches k * n. One atomic per block,
-// then a tight spin. The spin is bounded: on timeout the status word records
-// it and every later barrier returns at once, so no launch can hang the device.
-__device__ __forceinline__ void team_barrier(unsigned int* ctr, unsigned int target, uint32_t* status) {
-    __syncthreads();
-    if (threadIdx.x == 0 && !(*(volatile uint32_t*)status & ST_BARRIER_TIMEOUT)) {
-        // The release add publishes the block's writes (ordered before it by the
-        // bar.sync above); the acquire load makes the other blocks' writes visible.
-        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(ctr) : "memory");
-        unsigned int v, spins = 0;
-        for (;;) {
-            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(ctr) : "memory");
-            if (v >= target) break;
-            if (++spins > BARRIER_SPIN_LIMIT) {
-                atomicOr(status, ST_BARRIER_TIMEOUT);
-                break;
-            }
-        }
-    }
-    __syncthreads();
-}
 
 __device__ __forceinline__ uint32_t mix32(uint64_t k) {
     uint32_t h = uint32_t(k) ^ uint32_t(k >> 32) * 0x9E3779B1u;
@@ -288,6 +263,7 @@ struct SolveArgs {
     const float4* iw;
     float4* vtab;             // velocity contact table (VT_PLANES planes)
     float4* stab;             // split contact table (ST_PLANES planes)
+    float4* srec;             // adjoint recording (else null): per (sweep, slot, contact) vn, impulse, clamp bits
     unsigned int* bar;        // [0] velocity-team barrier counter, [1] split-team counter
     uint32_t* status;
     float inv_dt;
@@ -302,34 +278,6 @@ __device__ __forceinline__ void apply(V3& la, V3& wa, V3& lb, V3& wb, bool appa,
 }
 
 enum Kind { WARM = 0, ITER = 1, SPLIT = 2 };
-
-// Per-step contact tables in batch-slot order. Slots are grouped 32 at a time
-// (colour batches start on a multiple of 32, so a warp's lanes hold exactly one
-// such group), and each group stores field ("plane") by field and contact by
-// contact, 32 float4 per (plane, contact): element (plane, k, t) sits at
-// ((t / 32 * PLANES + plane) * 4 + k) * 32 + t % 32. A warp's loads are
-// coalesced and everything one warp reads in a sweep lies in one contiguous
-// span of at most 30 KB, so scattered page (TLB) lookups stay few. The first
-// sweep of each team fills its table from the rows and the bodies' inverse
-// inertia; the later sweeps read only the table and the velocities. A slot's
-// table entries are written and read by the same thread only (the slot-to-thread
-// deal is fixed for the launch), so plain L1-cached loads see them; they are
-// never read through the read-only (non-coherent) path, since this kernel
-// writes them.
-//
-// Velocity table planes: 0 n|friction 1 r_a|bias 2 r_b|bias 3 t1|1/m_a
-// 4 t2|1/m_b 5 Iw_a(r_a x n)|normal mass 6 Iw_b(r_b x n)|t1 mass
-// 7 Iw_a(r_a x t1)|t2 mass 8 Iw_b(r_b x t1)|cfm 9 Iw_a(r_a x t2)|restitution
-// 10 Iw_b(r_b x t2) 11 kn 12 kt1 13 kt2 14 accumulated impulses (row 3).
-// Split table planes: 0 n|normal mass 1 r_a|cfm 2 r_b 3 Iw_a(r_a x n)|1/m_a
-// 4 Iw_b(r_b x n)|1/m_b 5 row 5 (rhs, push impulse, active, penetration).
-constexpr uint32_t VT_PLANES = 15;
-constexpr uint32_t ST_PLANES = 6;
-
-template <uint32_t PLANES>
-__device__ __forceinline__ size_t tix(uint32_t plane, uint32_t k, uint32_t t) {
-    return ((size_t(t >> 5) * PLANES + plane) * 4 + k) * 32 + (t & 31u);
-}
 
 __device__ __forceinline__ float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
 
@@ -388,8 +336,8 @@ __device__ __forceinline__ void prefetch_contact_l1(const float4* v, uint32_t k,
 
 // One solve_contact sweep (sequential_impulse.rs:804-930) over group slot t;
 // on the last sweep the impulses also go back to the pair's rows.
-__device__ __forceinline__ void iter_group(const SolveArgs& a, uint32_t t, uint32_t p, uint32_t cnt, bool last, V3& la,
-                                           V3& wa, V3& lb, V3& wb, bool& appa, bool& appb) {
+__device__ __forceinline__ void iter_group(const SolveArgs& a, uint32_t t, uint32_t p, uint32_t cnt, uint32_t sweep,
+                                           bool last, V3& la, V3& wa, V3& lb, V3& wb, bool& appa, bool& appb) {
     const float4* v = a.vtab;
     const float ima = v[tix<VT_PLANES>(3, 0, t)].w, imb = v[tix<VT_PLANES>(4, 0, t)].w;
     appa = ima > 0.0f;
@@ -427,17 +375,24 @@ __device__ __forceinline__ void iter_group(const SolveArgs& a, uint32_t t, uint3
         float vt = dot(rel, t1);
         float lam = -r4.y * (vt - 0.0f * a.inv_dt);
         float o1 = r3.y;
-        float n1 = fminf(fmaxf(o1 + lam, -maxf), maxf);
+        const float u1 = o1 + lam;
+        float n1 = fminf(fmaxf(u1, -maxf), maxf);
         float j1 = n1 - o1;
         apply(la, wa, lb, wb, appa, appb, ima, imb, t1, a1a, a1b, j1);
         rel += kt1 * j1;
         vt = dot(rel, t2);
         lam = -r4.z * (vt - 0.0f * a.inv_dt);
         float o2 = r3.z;
-        float n2 = fminf(fmaxf(o2 + lam, -maxf), maxf);
+        const float u2 = o2 + lam;
+        float n2 = fminf(fmaxf(u2, -maxf), maxf);
         float j2 = n2 - o2;
         apply(la, wa, lb, wb, appa, appb, ima, imb, t2, a2a, a2b, j2);
         const float4 nr3 = make_float4(nimp, n1, n2, r3.w);
+        if (a.srec) {  // the forward values the adjoint's frozen linearisation needs
+            const uint32_t s1 = u1 > maxf ? 1u : (u1 < -maxf ? 2u : 0u);
+            const uint32_t s2 = u2 > maxf ? 1u : (u2 < -maxf ? 2u : 0u);
+            a.srec[sweep_index(sweep, k, t, a.iterations)] = make_float4(vn, nimp, __uint_as_float(s1 | (s2 << 2)), 0.0f);
+        }
         a.vtab[tix<VT_PLANES>(14, k, t)] = nr3;
         if (last) a.rows[(size_t(p) * 4 + k) * ROW_F4 + 3] = nr3;
     }
@@ -522,7 +477,7 @@ __device__ __forceinline__ void run_group(const SolveArgs& a, uint32_t t, uint4 
     V3 lb = from4(__ldcg(&plin[ib])), wb = from4(__ldcg(&pang[ib]));
     bool appa, appb;  // only dynamic bodies move
     if (KIND == WARM) warm_group(a, t, p, cnt, ia, ib, la, wa, lb, wb, appa, appb);
-    else if (KIND == ITER) iter_group(a, t, p, cnt, sweep == last, la, wa, lb, wb, appa, appb);
+    else if (KIND == ITER) iter_group(a, t, p, cnt, sweep, sweep == last, la, wa, lb, wb, appa, appb);
     else split_group(a, t, p, cnt, ia, ib, sweep == 0, sweep == last, la, wa, lb, wb, appa, appb);
     if (appa) { __stcg(&plin[ia], to4(la, 0.0f)); __stcg(&pang[ia], to4(wa, 0.0f)); }
     if (appb) { __stcg(&plin[ib], to4(lb, 0.0f)); __stcg(&pang[ib], to4(wb, 0.0f)); }
@@ -673,7 +628,7 @@ __global__ void k_merge(const uint64_t* __restrict__ pairs, const float4* __rest
                         const uint32_t* __restrict__ sel_a, const uint32_t* __restrict__ na_ptr,
                         const uint64_t* __restrict__ old_keys, const float4* __restrict__ old_entries,
                         const uint32_t* __restrict__ sel_b, const uint32_t* __restrict__ nb_ptr, uint64_t* out_keys,
-                        float4* out_entries, uint32_t* out_count) {
+                        float4* out_entries, uint32_t* out_count, uint32_t* rec_merge_pos) {
     uint32_t na = *na_ptr, nb = *nb_ptr;
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t == 0) *out_count = na + nb;
@@ -682,6 +637,7 @@ __global__ void k_merge(const uint64_t* __restrict__ pairs, const float4* __rest
         uint64_t key = pairs[p];
         uint32_t pos = t + (nb ? lower_bound_keys(old_keys, sel_b, nb, key) : 0u);
         out_keys[pos] = key;
+        if (rec_merge_pos) rec_merge_pos[p] = pos;
         const float4* src = cur_entries + size_t(p) * ENTRY_F4;
         float4* dst = out_entries + size_t(pos) * ENTRY_F4;
         for (int q = 0; q < ENTRY_F4; ++q) dst[q] = src[q];
@@ -761,7 +717,7 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
     pd.stab.reserve(size_t(ST_PLANES) * 4 * slots);
     SolveArgs sa{pd.rows.p, pd.batch_rec.p, pd.colour_offset.p, pd.colour_cursor.p, pd.split_rec.p,
                  pd.split_offset.p, pd.split_cursor.p, pd.scalars.p, w.b.linvel, w.b.angvel, w.b.push_lin,
-                 w.b.push_ang, w.b.iw, pd.vtab.p, pd.stab.p,
+                 w.b.push_ang, w.b.iw, pd.vtab.p, pd.stab.p, pd.rec.sweeps,
                  pd.barrier.p, status_dev, sp.inv_dt, sp.info.restitution_velocity_threshold,
                  sp.info.num_iterations};
     static int solve_grid = 0;
@@ -808,7 +764,7 @@ void run_cache_update(const uint64_t* pairs, uint32_t npairs, const Manifolds& o
     if (total)
         k_merge<<<(total + TB - 1) / TB, TB, 0, s>>>(pairs, pd.entries.p, pd.sel_a.p, na_dev, old_cache.keys.p,
                                                       old_cache.entries.p, pd.sel_b.p, nb_dev, next.keys.p,
-                                                      next.entries.p, next.count_dev);
+                                                      next.entries.p, next.count_dev, pd.rec.merge_pos);
     else
         check_cuda(cudaMemsetAsync(next.count_dev, 0, sizeof(uint32_t), s), "memset");
 }

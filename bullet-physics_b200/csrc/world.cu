@@ -99,6 +99,19 @@ struct HostStats {  // pinned, written by async copies at the end of a step
 
 }  // namespace
 
+// One forward step recorded for the adjoint (the reverse solve's inputs).
+struct StepRecord {
+    uint32_t ncol = 0, iters = 0, slots = 0, npairs = 0, nold = 0;
+    DevBuf<uint4> recs;                  // batch slot records (colour order)
+    DevBuf<float4> tab, sweeps;          // velocity contact table, per-sweep records
+    DevBuf<uint32_t> row_src, merge_pos; // warm-start sources, merged cache positions
+    DevBuf<uint32_t> off, end;           // colour batch starts / ends
+    DevBuf<uint8_t> flags;               // RF_* per body
+    AdjStep view() const {
+        return AdjStep{recs.p, off.p, end.p, ncol, iters, tab.p, sweeps.p, merge_pos.p, row_src.p};
+    }
+};
+
 struct World {
     cudaStream_t stream = nullptr;
     SolverParams info{};
@@ -141,6 +154,10 @@ struct World {
     int solved_standalone = 0;  // 1 after bgpu_solve_contacts (read_contacts reports its groups)
     uint32_t standalone_groups = 0;
     DevBuf<uint64_t> standalone_keys;
+    // adjoint recording: the step being recorded (null otherwise) and the pair pass's scratch
+    StepRecord* rec_step = nullptr;
+    DevBuf<uint8_t> rec_pt_src;
+    DevBuf<uint32_t> rec_pair_old;
 
     World() {
         check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
@@ -168,7 +185,8 @@ struct World {
 
     BodyDev body_dev() {
         return BodyDev{pos.p, quat.p, linvel.p, angvel.p, inv_inertia.p, grav.p, force.p, torque.p, material.p,
-                       sleep.p, info_d.p, aabb_min.p, aabb_max.p, pred.p, settled.p, iw.p, push_lin.p, push_ang.p};
+                       sleep.p, info_d.p, aabb_min.p, aabb_max.p, pred.p, settled.p, iw.p, push_lin.p, push_ang.p,
+                       rec_step ? rec_step->flags.p : nullptr};
     }
     WorldView view() { return WorldView{body_dev(), shapes_d.p, hull_d.p, n}; }
 
@@ -429,6 +447,10 @@ struct World {
         sp.dt = dt;
         sp.inv_dt = 1.0f / dt;
         sp.info = info;
+        if (rec_step) {
+            rec_step->flags.reserve(std::max<uint32_t>(n, 1));
+            check_cuda(cudaMemsetAsync(rec_step->flags.p, 0, std::max<uint32_t>(n, 1), stream), "memset");
+        }
         BodyDev b = body_dev();
         WorldView wv = view();
         uint32_t* status = flags.p;
@@ -451,6 +473,7 @@ struct World {
         Manifolds& old_cache = cache[cur];
         Manifolds& next = cache[cur ^ 1];
         old_cache.count_host = hs->cache_count;
+        if (rec_step) prepare_record(old_cache.count_host);
         mark(2);
         // 4b: islands
         islands.run(b, n, pairs.p, npairs, world_of, simulate, status, stream);
@@ -482,6 +505,53 @@ struct World {
         check_cuda(cudaMemcpyAsync(&hs->cache_count, next.count_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream),
                    "d2h");
         stats_pending = true;
+        if (rec_step) finish_record();
+    }
+
+    // Adjoint recording: point the pair pass, the solver and the merge at the record's arrays.
+    void prepare_record(uint32_t nold) {
+        StepRecord& R = *rec_step;
+        R.npairs = npairs;
+        R.nold = nold;
+        R.iters = info.num_iterations;
+        const size_t np = std::max<uint32_t>(npairs, 1);
+        rec_pt_src.reserve(np * 4);
+        rec_pair_old.reserve(np);
+        R.row_src.reserve(np * 4);
+        R.merge_pos.reserve(np);
+        check_cuda(cudaMemsetAsync(R.merge_pos.p, 0xff, np * sizeof(uint32_t), stream), "memset");
+        const size_t slots_cap = (size_t(npairs) + 32u * 130u + 31u) & ~size_t(31);
+        if (R.iters) R.sweeps.reserve(size_t(R.iters) * 4 * slots_cap);
+        pd.rec = RecordDev{rec_pt_src.p, rec_pair_old.p, R.row_src.p, R.merge_pos.p, R.iters ? R.sweeps.p : nullptr};
+    }
+
+    // Keep the step's batch records, colour offsets and contact table (they are overwritten next step).
+    void finish_record() {
+        StepRecord& R = *rec_step;
+        pd.rec = RecordDev{};
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+        R.ncol = hs->scalars[4];
+        R.slots = 0;
+        if (npairs == 0 || R.ncol == 0) {
+            R.ncol = 0;
+            return;
+        }
+        std::vector<uint32_t> off(R.ncol + 1);
+        check_cuda(cudaMemcpy(off.data(), pd.colour_offset.p, (R.ncol + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost),
+                   "d2h");
+        R.slots = (off[R.ncol] + 31u) & ~31u;
+        R.off.reserve(R.ncol);
+        R.end.reserve(R.ncol);
+        R.recs.reserve(R.slots);
+        R.tab.reserve(size_t(R.slots) * VT_PLANES * 4);
+        auto d2d = [&](void* dst, const void* src, size_t bytes) {
+            check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream), "record copy");
+        };
+        d2d(R.off.p, pd.colour_offset.p, R.ncol * sizeof(uint32_t));
+        d2d(R.end.p, pd.colour_cursor.p, R.ncol * sizeof(uint32_t));
+        d2d(R.recs.p, pd.batch_rec.p, size_t(R.slots) * sizeof(uint4));
+        d2d(R.tab.p, pd.vtab.p, size_t(R.slots) * VT_PLANES * 4 * sizeof(float4));
+        check_cuda(cudaStreamSynchronize(stream), "sync");
     }
 
     void finish_stats() {
@@ -501,6 +571,203 @@ struct World {
         if (timing) {
             fold(ev_cur ^ 1);
             fold(ev_cur);
+        }
+    }
+};
+
+// ---------------------------------------------------------------- adjoint tape
+// World state a replay starts from: the body arrays a step reads, the current
+// manifold cache, the per-world simulate flags.
+struct Snapshot {
+    uint32_t n = 0, count = 0, nsim = 0;
+    int cur = 0;
+    DevBuf<float4> f4[10];
+    DevBuf<uint4> info;
+    DevBuf<uint64_t> keys;
+    DevBuf<float4> entries;
+    DevBuf<uint32_t> sim;
+};
+
+static float4* body_array(World& W, int k) {
+    float4* a[10] = {W.pos.p,    W.quat.p,   W.linvel.p,   W.angvel.p,   W.sleep.p,
+                     W.force.p,  W.torque.p, W.aabb_min.p, W.aabb_max.p, W.grav.p};
+    return a[k];
+}
+
+static void save_snapshot(World& W, Snapshot& S) {
+    check_cuda(cudaStreamSynchronize(W.stream), "sync");
+    S.n = W.n;
+    S.cur = W.cur;
+    S.count = W.hs->cache_count;  // entries of cache[cur], written back at the end of every step
+    S.nsim = 2 * W.num_worlds();
+    auto d2d = [&](void* dst, const void* src, size_t bytes) {
+        if (bytes) check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, W.stream), "snapshot copy");
+    };
+    for (int k = 0; k < 10; ++k) {
+        S.f4[k].reserve(std::max<uint32_t>(S.n, 1));
+        d2d(S.f4[k].p, body_array(W, k), S.n * sizeof(float4));
+    }
+    S.info.reserve(std::max<uint32_t>(S.n, 1));
+    d2d(S.info.p, W.info_d.p, S.n * sizeof(uint4));
+    const Manifolds& c = W.cache[W.cur];
+    S.keys.reserve(S.count + 1);
+    S.entries.reserve((size_t(S.count) + 1) * ENTRY_F4);
+    d2d(S.keys.p, c.keys.p, S.count * sizeof(uint64_t));
+    d2d(S.entries.p, c.entries.p, size_t(S.count) * ENTRY_F4 * sizeof(float4));
+    S.sim.reserve(S.nsim);
+    d2d(S.sim.p, W.world_sim.p, S.nsim * sizeof(uint32_t));
+    check_cuda(cudaStreamSynchronize(W.stream), "sync");
+}
+
+static void restore_snapshot(World& W, const Snapshot& S) {
+    if (S.n != W.n || S.nsim != 2 * W.num_worlds()) throw InvalidArg{"bodies or worlds were added after the tape's forward pass"};
+    auto d2d = [&](void* dst, const void* src, size_t bytes) {
+        if (bytes) check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, W.stream), "restore copy");
+    };
+    for (int k = 0; k < 10; ++k) d2d(body_array(W, k), S.f4[k].p, S.n * sizeof(float4));
+    d2d(W.info_d.p, S.info.p, S.n * sizeof(uint4));
+    W.cur = S.cur;
+    Manifolds& c = W.cache[W.cur];
+    c.keys.reserve(S.count + 1);
+    c.entries.reserve((size_t(S.count) + 1) * ENTRY_F4);
+    d2d(c.keys.p, S.keys.p, S.count * sizeof(uint64_t));
+    d2d(c.entries.p, S.entries.p, size_t(S.count) * ENTRY_F4 * sizeof(float4));
+    check_cuda(cudaMemcpyAsync(c.count_dev, &S.count, sizeof(uint32_t), cudaMemcpyHostToDevice, W.stream), "h2d");
+    d2d(W.world_sim.p, S.sim.p, S.nsim * sizeof(uint32_t));
+    check_cuda(cudaStreamSynchronize(W.stream), "sync");
+    c.count_host = S.count;
+    W.hs->cache_count = S.count;
+    W.stats_pending = false;
+}
+
+// Tape::backward of the rigid-body step: a forward pass that keeps a
+// checkpoint every `every` steps, and a backward pass that replays each
+// segment from its checkpoint with recording on, then runs the segment's
+// steps in reverse (k_adjoint.cu).
+struct Tape {
+    World* W;
+    uint32_t every;
+    float dt = 0.0f;
+    uint32_t nsteps = 0;
+    std::vector<std::unique_ptr<Snapshot>> cps;
+    Snapshot final_state;
+    std::vector<std::unique_ptr<StepRecord>> recs;
+    DevBuf<float4> xbar, vbar, wbar, lbar;
+    DevBuf<float> mubar, ebar, carry[2];
+    DevBuf<unsigned int> bar;
+    DevBuf<uint32_t> status;
+    cudaEvent_t ev[4] = {};
+    float forward_ms = 0.0f, backward_ms = 0.0f;
+
+    Tape(World* w, uint32_t k) : W(w), every(k) {
+        for (auto& e : ev) check_cuda(cudaEventCreate(&e), "event");
+    }
+    ~Tape() {
+        for (auto& e : ev) if (e) cudaEventDestroy(e);
+    }
+
+    void forward(float step_dt, uint32_t steps) {
+        W->finish_stats();
+        dt = step_dt;
+        nsteps = steps;
+        cps.clear();
+        check_cuda(cudaEventRecord(ev[0], W->stream), "event");
+        for (uint32_t s = 0; s < steps; ++s) {
+            if (s % every == 0) {
+                cps.emplace_back(new Snapshot);
+                save_snapshot(*W, *cps.back());
+            }
+            W->step_once(dt);
+        }
+        save_snapshot(*W, final_state);
+        check_cuda(cudaEventRecord(ev[1], W->stream), "event");
+        check_cuda(cudaEventSynchronize(ev[1]), "sync");
+        check_cuda(cudaEventElapsedTime(&forward_ms, ev[0], ev[1]), "elapsed");
+    }
+
+    // Back to the state at the start of the last forward pass (its first checkpoint).
+    void rewind() {
+        if (cps.empty()) throw InvalidArg{"the tape has no forward pass"};
+        restore_snapshot(*W, *cps[0]);
+    }
+
+    // grad_state: n x 9 floats (dL/dx, dL/dv, dL/dw of the final state). Outputs may be null.
+    void backward(const float* grad_state, float* gv0, float* gw0, float* gmu, float* ge) {
+        if (cps.empty()) throw InvalidArg{"the tape has no forward pass"};
+        const uint32_t n = W->n;
+        cudaStream_t s = W->stream;
+        std::vector<float4> hx(n), hv(n), hw(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            const float* g = grad_state + size_t(i) * 9;
+            hx[i] = make_float4(g[0], g[1], g[2], 0.0f);
+            hv[i] = make_float4(g[3], g[4], g[5], 0.0f);
+            hw[i] = make_float4(g[6], g[7], g[8], 0.0f);
+        }
+        const size_t nn = std::max<uint32_t>(n, 1);
+        xbar.reserve(nn); vbar.reserve(nn); wbar.reserve(nn); mubar.reserve(nn); ebar.reserve(nn);
+        bar.reserve(4);
+        status.reserve(4);
+        check_cuda(cudaMemcpyAsync(xbar.p, hx.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s), "h2d");
+        check_cuda(cudaMemcpyAsync(vbar.p, hv.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s), "h2d");
+        check_cuda(cudaMemcpyAsync(wbar.p, hw.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s), "h2d");
+        check_cuda(cudaMemsetAsync(mubar.p, 0, nn * sizeof(float), s), "memset");
+        check_cuda(cudaMemsetAsync(ebar.p, 0, nn * sizeof(float), s), "memset");
+        check_cuda(cudaMemsetAsync(status.p, 0, sizeof(uint32_t), s), "memset");
+        check_cuda(cudaEventRecord(ev[2], s), "event");
+        while (recs.size() < every) recs.emplace_back(new StepRecord);
+        const float* carry_in = nullptr;
+        int o = 0;
+        for (size_t seg = cps.size(); seg-- > 0;) {
+            const uint32_t s0 = uint32_t(seg) * every, s1 = std::min(s0 + every, nsteps);
+            restore_snapshot(*W, *cps[seg]);
+            for (uint32_t st = s0; st < s1; ++st) {
+                W->rec_step = recs[st - s0].get();
+                try {
+                    W->step_once(dt);
+                } catch (...) {
+                    W->rec_step = nullptr;
+                    throw;
+                }
+                W->rec_step = nullptr;
+            }
+            if (W->hs->status) throw InvalidArg{"device status set while replaying a segment"};
+            for (uint32_t st = s1; st-- > s0;) {
+                const StepRecord& R = *recs[st - s0];
+                launch_adj_positions(n, dt, R.flags.p, xbar.p, vbar.p, s);
+                float* cout = nullptr;
+                if (R.nold) {
+                    carry[o].reserve(size_t(R.nold) * 4);
+                    check_cuda(cudaMemsetAsync(carry[o].p, 0, size_t(R.nold) * 4 * sizeof(float), s), "memset");
+                    cout = carry[o].p;
+                }
+                if (R.ncol) {
+                    lbar.reserve(size_t(R.slots) * 4);
+                    run_adj_solve(R.view(), lbar.p, vbar.p, wbar.p, mubar.p, ebar.p, W->material.p, carry_in, cout,
+                                  W->info.restitution_velocity_threshold, W->info.warmstarting_factor, bar.p, status.p,
+                                  s);
+                }
+                launch_adj_velocities(n, dt, R.flags.p, W->material.p, vbar.p, wbar.p, s);
+                check_cuda(cudaGetLastError(), "adjoint launch");
+                carry_in = cout;
+                o ^= 1;
+            }
+        }
+        check_cuda(cudaEventRecord(ev[3], s), "event");
+        restore_snapshot(*W, final_state);
+        check_cuda(cudaEventElapsedTime(&backward_ms, ev[2], ev[3]), "elapsed");
+        uint32_t st = 0;
+        check_cuda(cudaMemcpy(&st, status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost), "d2h");
+        if (st) throw InvalidArg{"device status set in the adjoint solve (barrier timeout)"};
+        std::vector<float> hm(n), he(n);
+        check_cuda(cudaMemcpy(hv.data(), vbar.p, n * sizeof(float4), cudaMemcpyDeviceToHost), "d2h");
+        check_cuda(cudaMemcpy(hw.data(), wbar.p, n * sizeof(float4), cudaMemcpyDeviceToHost), "d2h");
+        check_cuda(cudaMemcpy(hm.data(), mubar.p, n * sizeof(float), cudaMemcpyDeviceToHost), "d2h");
+        check_cuda(cudaMemcpy(he.data(), ebar.p, n * sizeof(float), cudaMemcpyDeviceToHost), "d2h");
+        for (uint32_t i = 0; i < n; ++i) {
+            if (gv0) { gv0[3 * i] = hv[i].x; gv0[3 * i + 1] = hv[i].y; gv0[3 * i + 2] = hv[i].z; }
+            if (gw0) { gw0[3 * i] = hw[i].x; gw0[3 * i + 1] = hw[i].y; gw0[3 * i + 2] = hw[i].z; }
+            if (gmu) gmu[i] = hm[i];
+            if (ge) ge[i] = he[i];
         }
     }
 };
@@ -699,6 +966,67 @@ bgpu_status bgpu_batch_step(bgpu_world* w, float dt, uint32_t nsteps) {
         return BGPU_ERR_INVALID_ARGUMENT;
     }
     return bgpu_step(w, dt, nsteps);
+}
+
+struct bgpu_tape {
+    std::unique_ptr<bgpu::Tape> impl;
+};
+
+bgpu_status bgpu_tape_create(bgpu_world* w, uint32_t checkpoint_every, bgpu_tape** out) {
+    if (!w || !out || checkpoint_every == 0) {
+        bgpu::g_last_error = "world or out is NULL, or checkpoint_every is 0";
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    return guarded([&]() -> bgpu_status {
+        std::unique_ptr<bgpu_tape> t(new bgpu_tape());
+        t->impl.reset(new bgpu::Tape(&w->impl, checkpoint_every));
+        *out = t.release();
+        return BGPU_OK;
+    });
+}
+
+void bgpu_tape_destroy(bgpu_tape* t) { delete t; }
+
+bgpu_status bgpu_tape_forward(bgpu_tape* t, float dt, uint32_t nsteps) {
+    if (!t || !(dt > 0.0f)) {
+        bgpu::g_last_error = "tape is NULL or dt <= 0";
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&]() -> bgpu_status {
+        t->impl->forward(dt, nsteps);
+        return check_device_status(*t->impl->W);
+    });
+}
+
+bgpu_status bgpu_tape_backward(bgpu_tape* t, const float* grad_state, float* grad_v0, float* grad_w0,
+                               float* grad_friction, float* grad_restitution) {
+    if (!t || !grad_state) {
+        bgpu::g_last_error = "tape or grad_state is NULL";
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&]() -> bgpu_status {
+        t->impl->backward(grad_state, grad_v0, grad_w0, grad_friction, grad_restitution);
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_tape_rewind(bgpu_tape* t) {
+    if (!t) {
+        bgpu::g_last_error = "tape is NULL";
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&]() -> bgpu_status {
+        t->impl->rewind();
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_tape_timing(const bgpu_tape* t, float* forward_ms, float* backward_ms) {
+    if (!t) return BGPU_ERR_INVALID_ARGUMENT;
+    if (forward_ms) *forward_ms = t->impl->forward_ms;
+    if (backward_ms) *backward_ms = t->impl->backward_ms;
+    return BGPU_OK;
 }
 
 uint32_t bgpu_batch_num_worlds(const bgpu_world* w) { return (w && w->impl.batch) ? w->impl.num_worlds() : 0u; }

@@ -19,6 +19,11 @@ parity check and a benchmark run start from bit-identical inputs.
                      dynamic bodies each, half of them columns of 1-16 unit
                      boxes, half jittered sphere piles (r 0.5), every world on
                      its own ground plane; 10 iterations; 500 steps.
+  adjoint_worlds     1,024 worlds of 64 unit boxes (4x4x4, 1.2 m apart) thrown
+                     with v0 U(-2,2)^3, friction U(0.2,0.9), restitution
+                     U(0,0.3); ground plane with friction and restitution 1 (so
+                     a ground contact's coefficients are the box's); dt 1/120;
+                     10 iterations; 120 steps; loss sum_w |com_w - target_w|^2.
 Scaled-down variants (`scale`) keep the recipe and shrink the grid.
 """
 import math
@@ -257,12 +262,17 @@ class BatchScene:
         self.shapes.append((kind, list(params), None if points is None else np.asarray(points, dtype=np.float32)))
         return len(self.shapes) - 1
 
-    def add_world(self, shape, pos, quat, mass):
+    def add_world(self, shape, pos, quat, mass, linvel=None, friction=None, restitution=None):
         n = len(shape)
         self.worlds.append(dict(shape=np.asarray(shape, dtype=np.uint32), pos=np.asarray(pos, dtype=np.float32),
-                                quat=np.asarray(quat, dtype=np.float32), linvel=np.zeros((n, 3), np.float32),
+                                quat=np.asarray(quat, dtype=np.float32),
+                                linvel=(np.zeros((n, 3), np.float32) if linvel is None
+                                        else np.asarray(linvel, dtype=np.float32).reshape(n, 3)),
                                 angvel=np.zeros((n, 3), np.float32), mass=np.asarray(mass, dtype=np.float32),
-                                friction=np.full(n, 0.5, np.float32), restitution=np.zeros(n, np.float32)))
+                                friction=(np.full(n, 0.5, np.float32) if friction is None
+                                          else np.asarray(friction, dtype=np.float32)),
+                                restitution=(np.zeros(n, np.float32) if restitution is None
+                                             else np.asarray(restitution, dtype=np.float32))))
 
     @property
     def bodies_per_world(self):
@@ -355,3 +365,47 @@ def batched_worlds(n_worlds=4096, seed=4, steps=500, min_bodies=8, max_bodies=25
         mass = np.concatenate([[0.0], np.ones(nb)])
         s.add_world(shape, pos, quat, mass)
     return s
+
+
+def adjoint_worlds(n_worlds=1024, seed=5, steps=120, side=4):
+    """Adjoint configuration: boxes thrown in independent worlds; world targets for the loss."""
+    rng = np.random.default_rng(seed)
+    s = BatchScene(f"adjoint_worlds_{n_worlds}", 1.0 / 120.0, 10, steps)
+    plane = s.add_shape(PLANE, [0.0, 1.0, 0.0, 0.0])
+    box = s.add_shape(BOX, [0.5, 0.5, 0.5])
+    nb = side ** 3
+    t = np.arange(nb)
+    gx, gz, gy = t % side, (t // side) % side, t // (side * side)
+    base = np.stack([(gx - (side - 1) / 2) * 1.2, 0.6 + gy * 1.2, (gz - (side - 1) / 2) * 1.2], axis=1)
+    s.targets = []
+    for _ in range(n_worlds):
+        pos = base + rng.uniform(-0.05, 0.05, size=(nb, 3))
+        v0 = rng.uniform(-2.0, 2.0, size=(nb, 3))
+        mu = rng.uniform(0.2, 0.9, size=nb)
+        e = rng.uniform(0.0, 0.3, size=nb)
+        s.add_world(np.concatenate([[plane], np.full(nb, box)]),
+                    np.concatenate([np.zeros((1, 3)), pos]).astype(np.float32),
+                    np.tile(np.array([0, 0, 0, 1], np.float32), (nb + 1, 1)),
+                    np.concatenate([[0.0], np.ones(nb)]),
+                    linvel=np.concatenate([np.zeros((1, 3)), v0]),
+                    friction=np.concatenate([[1.0], mu]), restitution=np.concatenate([[1.0], e]))
+        s.targets.append(pos.mean(axis=0) + np.array([1.0, 0.0, 0.5]))
+    s.targets = np.asarray(s.targets, dtype=np.float64)
+    return s
+
+
+def com_loss(positions, masses, offsets, targets):
+    """sum_w |com_w - target_w|^2 over the dynamic bodies of each world, and dL/dx per body."""
+    x = np.asarray(positions, dtype=np.float64)
+    m = np.asarray(masses, dtype=np.float64)
+    g = np.zeros_like(x)
+    loss = 0.0
+    for k in range(len(offsets) - 1):
+        lo, hi = int(offsets[k]), int(offsets[k + 1])
+        mk = m[lo:hi]
+        M = mk.sum()
+        com = (mk[:, None] * x[lo:hi]).sum(axis=0) / M
+        d = com - targets[k]
+        loss += float(d @ d)
+        g[lo:hi] = 2.0 * d[None, :] * (mk / M)[:, None]
+    return loss, g

@@ -169,6 +169,34 @@ bgpu_status bgpu_batch_world_offsets(bgpu_world* w, uint32_t* offsets);
 /* Steps every world of the batch nsteps times (the same as bgpu_step). */
 bgpu_status bgpu_batch_step(bgpu_world* w, float dt, uint32_t nsteps);
 
+/* Adjoint (no counterpart in the reference, whose world is not differentiable).
+ * A tape steps its world forward, keeping a checkpoint of the world state every
+ * checkpoint_every steps, then returns gradients of a loss of the final state with
+ * respect to every body's initial linear and angular velocity, friction and
+ * restitution. The differentiated model holds each step's contact geometry (rows,
+ * world inverse inertia), its clamp decisions and its sleep decisions at their
+ * forward values, and follows the warm start across steps (step.rs:751, 821); the
+ * gyroscopic term is held fixed (it vanishes for isotropic inertia). The backward
+ * pass replays each segment from its checkpoint, so its cost is about one extra
+ * forward pass plus the reverse sweeps, and memory holds one segment's records.
+ * The world must outlive the tape; bodies must not be added between forward and
+ * backward. After backward the world is back in its state at the end of forward. */
+typedef struct bgpu_tape bgpu_tape;
+bgpu_status bgpu_tape_create(bgpu_world* w, uint32_t checkpoint_every, bgpu_tape** out);
+void bgpu_tape_destroy(bgpu_tape* t);
+/* Runs step_simulation(dt) nsteps times on the tape's world, recording checkpoints. */
+bgpu_status bgpu_tape_forward(bgpu_tape* t, float dt, uint32_t nsteps);
+/* grad_state: n x 9 floats per body, dL/d(position, linear velocity, angular velocity) of
+ * the final state. Outputs (each may be NULL): grad_v0 and grad_w0 n x 3, grad_friction and
+ * grad_restitution n (for the body's material coefficient; contacts combine them as products). */
+bgpu_status bgpu_tape_backward(bgpu_tape* t, const float* grad_state, float* grad_v0, float* grad_w0,
+                               float* grad_friction, float* grad_restitution);
+/* Puts the world back in its state at the start of the last forward pass (body state and
+ * manifold cache), e.g. to run the same rollout again after changing initial velocities. */
+bgpu_status bgpu_tape_rewind(bgpu_tape* t);
+/* Device time of the last forward and backward calls, in ms on the world's stream. */
+bgpu_status bgpu_tape_timing(const bgpu_tape* t, float* forward_ms, float* backward_ms);
+
 /* The step (step.rs:100-199). bgpu_step runs step_simulation(dt) nsteps times. */
 bgpu_status bgpu_step(bgpu_world* w, float dt, uint32_t nsteps);
 bgpu_status bgpu_step_simulation_fixed(bgpu_world* w, float dt, uint32_t max_sub_steps, float fixed_dt,
