@@ -216,6 +216,8 @@ struct PairData {
     DevBuf<uint32_t> colour;         // per contact pair
     DevBuf<unsigned long long> body_prio;
     DevBuf<unsigned long long> body_mask;  // 2 words per body: colours taken at the body
+    DevBuf<unsigned long long> body_dup;   // 2 words per body: colours seeded twice at the body
+    DevBuf<uint32_t> colour_remap;         // colour -> dense colour (empty colours dropped)
     DevBuf<uint32_t> colour_count, colour_offset, colour_cursor;
     DevBuf<uint32_t> split_count, split_offset, split_cursor;
     DevBuf<uint4> batch_rec;         // contact pairs in colour order: body a, body b, pair | rows << 29, 0
@@ -240,6 +242,8 @@ struct PairData {
         colour.reserve(npairs);
         body_prio.reserve(nbodies);
         body_mask.reserve(2 * nbodies);
+        body_dup.reserve(2 * nbodies);
+        colour_remap.reserve(132);
         colour_count.reserve(132);
         colour_offset.reserve(132);
         colour_cursor.reserve(132);
@@ -294,8 +298,9 @@ void run_prepare_contacts(const BodyDev& b, uint32_t ngroups, const uint32_t* gr
 void launch_compute_iw(const BodyDev& b, uint32_t n, cudaStream_t s);
 // Colouring + PGS over the pairs with rows (counts stay on the device).
 // `mark(5)` is called after the colouring and `mark(6)` after the PGS kernel (timing hooks).
+// seed_colours: start the colouring from the colours the pairs' manifolds carry from last step.
 void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
-                uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark);
+                uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark, bool seed_colours);
 // Impulse writeback, then compaction of the surviving manifolds into `next`.
 // simulate / prev_simulate hold one flag per world, indexed through world_of (null: one world).
 void run_cache_update(const uint64_t* pairs, uint32_t npairs, const Manifolds& old_cache, PairData& pd,

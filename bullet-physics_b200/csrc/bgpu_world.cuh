@@ -93,6 +93,7 @@ enum : uint8_t {
 constexpr int ENTRY_F4 = 16;
 constexpr uint32_t META_INIT = 1u << 8;
 constexpr uint32_t META_VALID = 1u << 9;
+constexpr uint32_t META_COLOUR_SHIFT = 16;  // bits 16-23: last PGS colour + 1 (0: none)
 
 // Contact row slot: 6 float4 per contact, 4 slots per pair.
 //  r[0] normal.xyz, friction                 r[1] r_a.xyz, Baumgarte bias

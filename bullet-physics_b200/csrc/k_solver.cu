@@ -67,13 +67,25 @@ struct ColourArgs {
     uint32_t* colour;
     unsigned long long* prio;
     unsigned long long* mask;
+    unsigned long long* dup;      // 2 words per body: colours seeded twice at the body
+    const float4* entries;        // this step's manifold entries (their meta carries last step's colour)
+    uint32_t seed;                // 1: start from last step's colours
     unsigned int* bar;  // [0] barrier counter, [2..4] round counters, [5] colour max
     uint32_t* status;
 };
 
-// Jones-Plassmann rounds: an uncoloured group wins when its priority is the
-// maximum over the uncoloured groups at both of its dynamic bodies; winners
-// take the lowest colour free at both bodies.
+__device__ __forceinline__ unsigned long long* colour_word(unsigned long long* m, uint32_t x, uint32_t c) {
+    return &m[2 * x + (c >> 6)];
+}
+
+// Seeding, then Jones-Plassmann rounds. Seeding: a group whose pair kept its
+// manifold starts from the colour it had last step (kept in the entry's meta
+// bits); a seed is dropped, for every group that claims it, when two groups
+// claim the same colour at one dynamic body - so the result does not depend on
+// the order of the atomics. The bits of dropped seeds stay in the masks and
+// only make those colours unavailable there. Jones-Plassmann: an uncoloured
+// group wins when its priority is the maximum over the uncoloured groups at
+// both of its dynamic bodies; winners take the lowest colour free at both.
 __global__ void k_colour(ColourArgs a) {
     const uint32_t K = *a.count;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -86,9 +98,45 @@ __global__ void k_colour(ColourArgs a) {
         uint32_t u = key_lo(key), v = key_hi(key);
         a.mask[2 * u] = 0ull; a.mask[2 * u + 1] = 0ull;
         a.mask[2 * v] = 0ull; a.mask[2 * v + 1] = 0ull;
+        if (a.seed) {
+            a.dup[2 * u] = 0ull; a.dup[2 * u + 1] = 0ull;
+            a.dup[2 * v] = 0ull; a.dup[2 * v + 1] = 0ull;
+        }
     }
     if (tid == 0) { a.bar[2] = 0; a.bar[3] = 0; a.bar[4] = 0; a.bar[5] = 0; }
     team_barrier(a.bar, ++nbar * nblocks, a.status);
+    if (a.seed) {
+        for (uint32_t k = tid; k < K; k += stride) {  // claim last step's colour at both bodies
+            const uint32_t p = a.contact_pairs[k];
+            const uint32_t cs = (__float_as_uint(a.entries[size_t(p) * ENTRY_F4 + 2].w) >> META_COLOUR_SHIFT) & 0xffu;
+            if (cs == 0u || cs > MAX_COLOURS) continue;
+            const uint32_t c = cs - 1u;
+            const unsigned long long bit = 1ull << (c & 63u);
+            const uint64_t key = a.pairs[p];
+            const uint32_t u = key_lo(key), v = key_hi(key);
+            if (inv_mass_of(a.iw, u) > 0.0f && (atomicOr(colour_word(a.mask, u, c), bit) & bit))
+                atomicOr(colour_word(a.dup, u, c), bit);
+            if (inv_mass_of(a.iw, v) > 0.0f && (atomicOr(colour_word(a.mask, v, c), bit) & bit))
+                atomicOr(colour_word(a.dup, v, c), bit);
+        }
+        team_barrier(a.bar, ++nbar * nblocks, a.status);
+        for (uint32_t k = tid; k < K; k += stride) {  // keep the seeds claimed once at each body
+            const uint32_t p = a.contact_pairs[k];
+            const uint32_t cs = (__float_as_uint(a.entries[size_t(p) * ENTRY_F4 + 2].w) >> META_COLOUR_SHIFT) & 0xffu;
+            if (cs == 0u || cs > MAX_COLOURS) continue;
+            const uint32_t c = cs - 1u;
+            const unsigned long long bit = 1ull << (c & 63u);
+            const uint64_t key = a.pairs[p];
+            const uint32_t u = key_lo(key), v = key_hi(key);
+            const bool du = inv_mass_of(a.iw, u) > 0.0f && (__ldcg(colour_word(a.dup, u, c)) & bit);
+            const bool dv = inv_mass_of(a.iw, v) > 0.0f && (__ldcg(colour_word(a.dup, v, c)) & bit);
+            if (!du && !dv) {
+                a.colour[k] = c;
+                atomicMax(&a.bar[5], c + 1u);
+            }
+        }
+        team_barrier(a.bar, ++nbar * nblocks, a.status);
+    }
     int round = 0;
     for (; round < MAX_ROUNDS; ++round) {
         // phase 0: clear the bids of the uncoloured groups' bodies
@@ -157,6 +205,10 @@ __global__ void k_colour_hist(const uint32_t* __restrict__ count, const uint32_t
     uint32_t nrows = 0, nsplit_rows = 0;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
         uint32_t c = colour[k];
+        if (c >= MAX_COLOURS) {  // colouring gave up (its status bit is set): the group is not solved
+            split_flag[k] = 0u;
+            continue;
+        }
         atomicAdd(&sh[c], 1u);
         uint32_t p = contact_pairs[k];
         uint32_t n = row_count[p];
@@ -189,29 +241,33 @@ __global__ void k_colour_hist(const uint32_t* __restrict__ count, const uint32_t
 // Offsets of the colour batches; scalars [3] rows [4] colours [5] split groups
 // [10] split rows [11] largest split batch.
 __global__ void k_colour_scan(uint32_t* hist, uint32_t* offset, uint32_t* cursor, uint32_t* split_hist,
-                              uint32_t* split_offset, uint32_t* split_cursor, const unsigned int* bar, uint32_t* scalars) {
+                              uint32_t* split_offset, uint32_t* split_cursor, const unsigned int* bar, uint32_t* scalars,
+                              uint32_t* remap) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    uint32_t ncol = bar[5];
-    uint32_t acc = 0, sacc = 0, smax = 0;
-    // Batches start on multiples of 32 (one warp's slots never straddle two
-    // batches); after the scatter the cursors hold the batch ends.
-    for (uint32_t c = 0; c < ncol; ++c) {
+    const uint32_t nraw = bar[5];
+    uint32_t acc = 0, sacc = 0, smax = 0, split_groups = 0, d = 0;
+    // Colours without groups are dropped (remap: colour -> dense colour), batches start on
+    // multiples of 32 (one warp's slots never straddle two batches); after the scatter the
+    // cursors hold the batch ends.
+    for (uint32_t c = 0; c < nraw; ++c) {
+        if (hist[c] == 0) continue;
+        remap[c] = d;
         acc = (acc + 31u) & ~31u;
-        offset[c] = acc;
-        cursor[c] = acc;
+        offset[d] = acc;
+        cursor[d] = acc;
         acc += hist[c];
         sacc = (sacc + 31u) & ~31u;
-        split_offset[c] = sacc;
-        split_cursor[c] = sacc;
+        split_offset[d] = sacc;
+        split_cursor[d] = sacc;
         sacc += split_hist[c];
         smax = max(smax, split_hist[c]);
+        split_groups += split_hist[c];
+        ++d;
     }
-    offset[ncol] = acc;
-    split_offset[ncol] = sacc;
-    uint32_t split_groups = 0;
-    for (uint32_t c = 0; c < ncol; ++c) split_groups += split_hist[c];
+    offset[d] = acc;
+    split_offset[d] = sacc;
     scalars[3] = hist[MAX_COLOURS + 1];
-    scalars[4] = ncol;
+    scalars[4] = d;
     scalars[5] = split_groups;
     scalars[10] = hist[MAX_COLOURS + 2];
     scalars[11] = smax;
@@ -235,13 +291,18 @@ __device__ __forceinline__ uint32_t claim_slot(uint32_t* cursor, uint32_t c) {
 __global__ void k_colour_scatter(const uint32_t* __restrict__ count, const uint32_t* __restrict__ contact_pairs,
                                  const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ row_count,
                                  const uint32_t* __restrict__ colour, const uint32_t* __restrict__ split_flag,
-                                 uint32_t* cursor, uint32_t* split_cursor, uint4* batch_rec, uint4* split_rec) {
+                                 uint32_t* cursor, uint32_t* split_cursor, uint4* batch_rec, uint4* split_rec,
+                                 float4* entries, const uint32_t* __restrict__ remap) {
     uint32_t K = *count;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
-        uint32_t c = colour[k];
+        if (colour[k] >= MAX_COLOURS) continue;  // colouring gave up (its status bit is set)
+        uint32_t c = remap[colour[k]];
         uint32_t p = contact_pairs[k];
         uint64_t key = pairs[p];
         uint4 rec = make_uint4(key_lo(key), key_hi(key), p | (row_count[p] << 29), 0u);
+        // The colour rides in the manifold's meta bits to seed next step's colouring.
+        float* mw = &entries[size_t(p) * ENTRY_F4 + 2].w;
+        *mw = __uint_as_float((__float_as_uint(*mw) & ~(0xffu << META_COLOUR_SHIFT)) | ((c + 1u) << META_COLOUR_SHIFT));
         batch_rec[claim_slot(cursor, c)] = rec;
         if (split_flag[k]) split_rec[claim_slot(split_cursor, c)] = rec;
     }
@@ -669,7 +730,7 @@ int coop_grid(const void* fn, int block, size_t smem) {
 }  // namespace
 
 void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
-                uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark) {
+                uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark, bool seed_colours) {
     if (npairs == 0) {
         check_cuda(cudaMemsetAsync(pd.scalars.p + 2, 0, 4 * sizeof(uint32_t), s), "memset");
         check_cuda(cudaMemsetAsync(pd.scalars.p + 10, 0, 2 * sizeof(uint32_t), s), "memset");
@@ -691,7 +752,7 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
     // Colouring (cooperative launch).
     check_cuda(cudaMemsetAsync(pd.barrier.p, 0, 16 * sizeof(unsigned int), s), "memset barrier");
     ColourArgs ca{pd.scalars.p + 2, pd.contact_pairs.p, pairs, w.b.iw, pd.colour.p, pd.body_prio.p, pd.body_mask.p,
-                  pd.barrier.p, status_dev};
+                  pd.body_dup.p, pd.entries.p, seed_colours ? 1u : 0u, pd.barrier.p, status_dev};
     static int colour_grid = 0;
     if (!colour_grid) colour_grid = coop_grid((const void*)k_colour, TB, 0);
     void* cargs[] = {&ca};
@@ -704,10 +765,10 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
     k_colour_hist<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pd.colour.p, pd.row_count.p, pd.rows.p,
                                    pd.colour_count.p, pd.split_count.p, pd.flags.p);
     k_colour_scan<<<1, 32, 0, s>>>(pd.colour_count.p, pd.colour_offset.p, pd.colour_cursor.p, pd.split_count.p,
-                                   pd.split_offset.p, pd.split_cursor.p, pd.barrier.p, pd.scalars.p);
+                                   pd.split_offset.p, pd.split_cursor.p, pd.barrier.p, pd.scalars.p, pd.colour_remap.p);
     k_colour_scatter<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pairs, pd.row_count.p, pd.colour.p,
                                       pd.flags.p, pd.colour_cursor.p, pd.split_cursor.p, pd.batch_rec.p,
-                                      pd.split_rec.p);
+                                      pd.split_rec.p, pd.entries.p, pd.colour_remap.p);
     // PGS (cooperative launch: the teams' barriers need every block resident).
     check_cuda(cudaMemsetAsync(pd.barrier.p, 0, 2 * sizeof(unsigned int), s), "memset barrier");
     mark(5);

@@ -154,6 +154,8 @@ struct World {
     int solved_standalone = 0;  // 1 after bgpu_solve_contacts (read_contacts reports its groups)
     uint32_t standalone_groups = 0;
     DevBuf<uint64_t> standalone_keys;
+    uint64_t step_count = 0;  // steps taken (seeded vs full colouring)
+    static constexpr uint64_t RECOLOUR_PERIOD = 64;
     // adjoint recording: the step being recorded (null otherwise) and the pair pass's scratch
     StepRecord* rec_step = nullptr;
     DevBuf<uint8_t> rec_pt_src;
@@ -485,7 +487,10 @@ struct World {
         run_pair_pass(wv, pairs.p, npairs, old_cache, pd, sp, simulate, status, stream);
         mark(4);
         // 6: solve (colouring, then the PGS kernel)
-        run_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); });
+        // The colouring starts from last step's colours, except every RECOLOUR_PERIOD-th step.
+        run_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); },
+                   step_count % RECOLOUR_PERIOD != 0);
+        ++step_count;
         // 6b: impulse writeback + prune
         run_cache_update(pairs.p, npairs, old_cache, pd, next, world_of, simulate, prev_simulate, stream);
         check_cuda(cudaMemcpyAsync(prev_simulate, simulate, nw * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream),
@@ -581,6 +586,7 @@ struct World {
 struct Snapshot {
     uint32_t n = 0, count = 0, nsim = 0;
     int cur = 0;
+    uint64_t step_count = 0;
     DevBuf<float4> f4[10];
     DevBuf<uint4> info;
     DevBuf<uint64_t> keys;
@@ -598,6 +604,7 @@ static void save_snapshot(World& W, Snapshot& S) {
     check_cuda(cudaStreamSynchronize(W.stream), "sync");
     S.n = W.n;
     S.cur = W.cur;
+    S.step_count = W.step_count;
     S.count = W.hs->cache_count;  // entries of cache[cur], written back at the end of every step
     S.nsim = 2 * W.num_worlds();
     auto d2d = [&](void* dst, const void* src, size_t bytes) {
@@ -627,6 +634,7 @@ static void restore_snapshot(World& W, const Snapshot& S) {
     for (int k = 0; k < 10; ++k) d2d(body_array(W, k), S.f4[k].p, S.n * sizeof(float4));
     d2d(W.info_d.p, S.info.p, S.n * sizeof(uint4));
     W.cur = S.cur;
+    W.step_count = S.step_count;
     Manifolds& c = W.cache[W.cur];
     c.keys.reserve(S.count + 1);
     c.entries.reserve((size_t(S.count) + 1) * ENTRY_F4);
@@ -1491,7 +1499,7 @@ bgpu_status bgpu_solve_contacts(bgpu_world* w, uint32_t n, const float* contacts
         sp.info = W.info;
         bgpu::run_prepare_contacts(W.body_dev(), G, d_first.p, d_cnt.p, d_c.p, W.standalone_keys.p, sp, W.pd.rows.p,
                                    W.pd.row_count.p, s);
-        bgpu::run_solver(W.view(), W.standalone_keys.p, G, W.pd, sp, W.flags.p, s, [](int) {});
+        bgpu::run_solver(W.view(), W.standalone_keys.p, G, W.pd, sp, W.flags.p, s, [](int) {}, false);
         bgpu::check_cuda(cudaGetLastError(), "solve launch");
         uint32_t st = 0;
         bgpu::check_cuda(cudaMemcpyAsync(&st, W.flags.p, 4, cudaMemcpyDeviceToHost, s), "d2h");

@@ -289,3 +289,32 @@ def test_world_single_step_from_identical_state(gpu):
     o.step(s.dt)
     np.testing.assert_array_equal(w.pairs(), o.pairs())
     assert w.stats()["device_status"] == 0
+
+
+def test_world_mixed_convex_pile_matches_oracle(gpu):
+    """Config 2 recipe at small scale (boxes, spheres, capsules, 24-point hulls): the world step
+    with GJK/EPA manifolds against the oracle, in windows of 10 steps from a shared state."""
+    import bgpu
+    import scenes
+
+    s = scenes.mixed_convex_pile(n=96, seed=21, steps=90, extent=6.0)
+    w = s.build_gpu(bgpu)
+    o = s.build_oracle(orc)
+    convex_pairs = 0
+    for step in range(90):
+        if step % 10 == 0:
+            o.set_state(w.state().astype(np.float64))
+        w.step(s.dt)
+        o.set_solve_order(w.solve_order())
+        o.step(s.dt)
+        st = w.stats()
+        assert st["device_status"] == 0, st
+        convex_pairs = max(convex_pairs, st["num_detect"])
+        if step % 10 == 9:
+            g = w.state()
+            r = o.state()
+            np.testing.assert_array_equal(g[:, 13], r[:, 13])
+            err = float(np.abs(g[:, :13] - r[:, :13]).max())
+            assert err <= 1e-3, f"step {step}: {err}"
+            _pairs_equal(w.pairs(), o.pairs())
+    assert convex_pairs > 0
