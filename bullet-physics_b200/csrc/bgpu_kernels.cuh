@@ -158,7 +158,7 @@ struct Broadphase {
 
 // ---------------------------------------------------------------- islands (k_islands.cu)
 struct Islands {
-    DevBuf<uint32_t> parent, awake;
+    DevBuf<uint32_t> parent, awake, need;
     // simulate_flag[world] is raised when the world has an active body; world_of
     // (per body) is null for a single world.
     void run(const BodyDev& b, uint32_t n, const uint64_t* pairs, uint32_t npairs, const uint32_t* world_of,

@@ -154,8 +154,11 @@ __global__ void k_query(int m, uint32_t n, const uint32_t* __restrict__ is_unb, 
                         const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
                         const uint32_t* __restrict__ leaf_body, const uint32_t* __restrict__ unb, uint32_t nunb,
                         uint32_t* counts, const uint32_t* __restrict__ offsets, uint64_t* out, uint32_t* status) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || is_unb[i]) return;
+    // Threads take the bounded proxies in Morton (leaf) order, so a warp's
+    // queries are neighbours in space and walk much the same part of the tree.
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= uint32_t(m)) return;
+    const uint32_t i = leaf_body[t];
     float4 qmin = bmin[i], qmax = bmax[i];
     uint32_t cnt = 0;
     uint32_t local[LOCAL_SORT];
@@ -391,7 +394,8 @@ uint64_t Broadphase::run(const float4* aabb_min, const float4* aabb_max, uint32_
         k_refit<<<(m + TB - 1) / TB, TB, 0, s>>>(m, leaf_body.p, parent.p, left.p, right.p, refit_flag.p, aabb_min,
                                                  aabb_max, node_min.p, node_max.p);
     }
-    k_query<false><<<grid, TB, 0, s>>>(m, n, flags.p, aabb_min, aabb_max, node_min.p, node_max.p, left.p, right.p,
+    const uint32_t qgrid = m > 0 ? (uint32_t(m) + TB - 1) / TB : 1u;
+    k_query<false><<<qgrid, TB, 0, s>>>(m, n, flags.p, aabb_min, aabb_max, node_min.p, node_max.p, left.p, right.p,
                                         leaf_body.p, unbounded.p, nunb, counts.p, nullptr, nullptr, status_dev);
     // Unbounded proxies: count their segments by flag + scan.
     for (uint32_t u = 0; u < nunb; ++u) {
@@ -408,7 +412,7 @@ uint64_t Broadphase::run(const float4* aabb_min, const float4* aabb_max, uint32_
     uint64_t total = host_scalars[0];
     out.reserve(total + 1);
     if (total) {
-        k_query<true><<<grid, TB, 0, s>>>(m, n, flags.p, aabb_min, aabb_max, node_min.p, node_max.p, left.p, right.p,
+        k_query<true><<<qgrid, TB, 0, s>>>(m, n, flags.p, aabb_min, aabb_max, node_min.p, node_max.p, left.p, right.p,
                                            leaf_body.p, unbounded.p, nunb, counts.p, offsets.p, out.p, status_dev);
         for (uint32_t u = 0; u < nunb; ++u) {
             uint32_t h = unbounded_host[u];
@@ -591,8 +595,9 @@ extern "C" bgpu_status bgpu_broadphase_pairs_noalloc(const float* aabbs_dev, uin
                                                      node_max);
         }
         uint32_t* status = scalars + 1;
-        k_query<false><<<grid, TB, 0, s>>>(m, n, is_unb, mn, mx, node_min, node_max, left, right, leaf_body, unb_list,
-                                            nunb, counts, nullptr, nullptr, status);
+        const uint32_t qgrid = m > 0 ? (uint32_t(m) + TB - 1) / TB : 1u;
+        k_query<false><<<qgrid, TB, 0, s>>>(m, n, is_unb, mn, mx, node_min, node_max, left, right, leaf_body,
+                                            unb_list, nunb, counts, nullptr, nullptr, status);
         uint32_t* unb_scan = reinterpret_cast<uint32_t*>(db.Alternate());  // free after the build
         check_cuda(cudaStreamSynchronize(s), "sync");
         for (uint32_t u = 0; u < nunb; ++u) {
@@ -614,7 +619,7 @@ extern "C" bgpu_status bgpu_broadphase_pairs_noalloc(const float* aabbs_dev, uin
         }
         uint64_t* out = reinterpret_cast<uint64_t*>(pairs_dev);
         if (total) {
-            k_query<true><<<grid, TB, 0, s>>>(m, n, is_unb, mn, mx, node_min, node_max, left, right, leaf_body,
+            k_query<true><<<qgrid, TB, 0, s>>>(m, n, is_unb, mn, mx, node_min, node_max, left, right, leaf_body,
                                                unb_list, nunb, counts, offsets, out, status);
             for (uint32_t u = 0; u < nunb; ++u) {
                 uint32_t h = unb_host[u];

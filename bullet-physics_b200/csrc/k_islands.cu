@@ -9,6 +9,10 @@
 // union-by-size. An island with any Active / DisableDeactivation member —
 // or touching a moving kinematic body — wakes its sleepers; an island with
 // none sleeps as a unit.
+//
+// When no dynamic body is asleep or wants deactivation, every island that has
+// a dynamic body is awake and the decision changes nothing, so the union-find
+// is skipped (k_island_need raises the flag that the other kernels test).
 #include "bgpu_kernels.cuh"
 
 namespace bgpu {
@@ -35,6 +39,33 @@ __device__ __forceinline__ uint32_t find_root(const uint32_t* parent, uint32_t x
     return x;
 }
 
+// need = 1 when some dynamic body is island-sleeping or wants deactivation.
+// find with path halving: every visited node is pointed at its grandparent.
+// Only roots are ever linked (atomicCAS) and a node that stopped being a root
+// never becomes one again, so the grandparent is always an ancestor and the
+// plain store keeps every path leading to the current root.
+__device__ __forceinline__ uint32_t find_halving(uint32_t* parent, uint32_t x, uint32_t* status) {
+    for (int g = 0; g < UF_LIMIT; ++g) {
+        uint32_t p = __ldcg(&parent[x]);
+        if (p == x) return x;
+        uint32_t gp = __ldcg(&parent[p]);
+        if (gp != p) __stcg(&parent[x], gp);
+        x = gp;
+    }
+    atomicOr(status, ST_UNION_FIND_LIMIT);
+    return x;
+}
+
+__global__ void k_island_need(const uint4* __restrict__ info, uint32_t n, uint32_t* need) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool c = false;
+    if (i < n) {
+        uint4 in = info[i];
+        c = participates(in.y) && (in.z == ACT_ISLAND_SLEEPING || in.z == ACT_WANTS_DEACTIVATION);
+    }
+    if (__ballot_sync(0xffffffffu, c) && (threadIdx.x & 31u) == 0u) atomicOr(need, 1u);
+}
+
 __global__ void k_uf_init(uint32_t n, uint32_t* parent, uint32_t* awake) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -43,15 +74,15 @@ __global__ void k_uf_init(uint32_t n, uint32_t* parent, uint32_t* awake) {
 }
 
 __global__ void k_uf_link(const uint4* __restrict__ info, const uint64_t* __restrict__ pairs, uint32_t npairs,
-                          uint32_t* parent, uint32_t* status) {
+                          uint32_t* parent, uint32_t* status, const uint32_t* __restrict__ need) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= npairs) return;
+    if (p >= npairs || !*need) return;
     uint64_t k = pairs[p];
     uint32_t a = key_lo(k), b = key_hi(k);
     uint4 ia = info[a], ib = info[b];
     if (!eligible(ia, ib) || !participates(ia.y) || !participates(ib.y)) return;
     for (int g = 0; g < UF_LIMIT; ++g) {
-        uint32_t ra = find_root(parent, a, status), rb = find_root(parent, b, status);
+        uint32_t ra = find_halving(parent, a, status), rb = find_halving(parent, b, status);
         if (ra == rb) return;
         if (ra > rb) { uint32_t t = ra; ra = rb; rb = t; }
         if (atomicCAS(&parent[rb], rb, ra) == rb) return;
@@ -60,29 +91,28 @@ __global__ void k_uf_link(const uint4* __restrict__ info, const uint64_t* __rest
 }
 
 __global__ void k_uf_flatten_awake(const uint4* __restrict__ info, uint32_t n, uint32_t* parent, uint32_t* awake,
-                                   uint32_t* status) {
+                                   uint32_t* status, const uint32_t* __restrict__ need) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || !*need) return;
     uint32_t r = find_root(parent, i, status);
     uint4 in = info[i];
     // body.rs:602-608 (is_island_awake): Active or DisableDeactivation.
     if (participates(in.y) && (in.z == ACT_ACTIVE || in.z == ACT_DISABLE_DEACTIVATION)) awake[r] = 1u;
 }
 
-__global__ void k_uf_store_roots(uint32_t n, uint32_t* parent, uint32_t* status) {
+__global__ void k_uf_store_roots(uint32_t n, uint32_t* parent, uint32_t* status, const uint32_t* __restrict__ need) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    uint32_t r = find_root(parent, i, status);
-    __syncwarp();
-    parent[i] = r;
+    if (i >= n || !*need) return;
+    // Writing the root is safe while other threads still walk: every pointer still leads to it.
+    parent[i] = find_root(parent, i, status);
 }
 
 // islands.rs:232-279 — a moving kinematic wakes every eligible island it pairs with.
 __global__ void k_kinematic_wake(const uint4* __restrict__ info, const float4* __restrict__ lv, const float4* __restrict__ av,
                                  const uint64_t* __restrict__ pairs, uint32_t npairs, const uint32_t* __restrict__ root,
-                                 uint32_t* awake) {
+                                 uint32_t* awake, const uint32_t* __restrict__ need) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= npairs) return;
+    if (p >= npairs || !*need) return;
     uint64_t k = pairs[p];
     uint32_t ends[2] = {key_lo(k), key_hi(k)};
     int ks = -1;
@@ -105,11 +135,11 @@ __global__ void k_kinematic_wake(const uint4* __restrict__ info, const float4* _
 // body's world (world_of is null for a single world).
 __global__ void k_uf_apply(uint4* info, float4* lv, float4* av, float4* sleep, uint32_t n, const uint32_t* __restrict__ root,
                            const uint32_t* __restrict__ awake, const uint32_t* __restrict__ world_of, uint32_t* simulate,
-                           uint8_t* rec_flags) {
+                           uint8_t* rec_flags, const uint32_t* __restrict__ need) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint4 in = info[i];
-    bool aw = awake[root[i]] != 0;
+    bool aw = !*need || awake[root[i]] != 0;
     bool part = participates(in.y);
     if (aw) {
         if (!(in.y & BF_STATIC) && in.z == ACT_ISLAND_SLEEPING) {  // island_wake
@@ -139,16 +169,19 @@ void Islands::run(const BodyDev& b, uint32_t n, const uint64_t* pairs, uint32_t 
     if (n == 0) return;
     parent.reserve(n);
     awake.reserve(n);
+    need.reserve(1);
+    check_cuda(cudaMemsetAsync(need.p, 0, sizeof(uint32_t), s), "memset");
     const int TB = 256;
+    k_island_need<<<(n + TB - 1) / TB, TB, 0, s>>>(b.info, n, need.p);
     k_uf_init<<<(n + TB - 1) / TB, TB, 0, s>>>(n, parent.p, awake.p);
-    if (npairs) k_uf_link<<<(npairs + TB - 1) / TB, TB, 0, s>>>(b.info, pairs, npairs, parent.p, status_dev);
-    k_uf_flatten_awake<<<(n + TB - 1) / TB, TB, 0, s>>>(b.info, n, parent.p, awake.p, status_dev);
-    k_uf_store_roots<<<(n + TB - 1) / TB, TB, 0, s>>>(n, parent.p, status_dev);
+    if (npairs) k_uf_link<<<(npairs + TB - 1) / TB, TB, 0, s>>>(b.info, pairs, npairs, parent.p, status_dev, need.p);
+    k_uf_flatten_awake<<<(n + TB - 1) / TB, TB, 0, s>>>(b.info, n, parent.p, awake.p, status_dev, need.p);
+    k_uf_store_roots<<<(n + TB - 1) / TB, TB, 0, s>>>(n, parent.p, status_dev, need.p);
     if (npairs)
         k_kinematic_wake<<<(npairs + TB - 1) / TB, TB, 0, s>>>(b.info, b.linvel, b.angvel, pairs, npairs, parent.p,
-                                                                awake.p);
+                                                                awake.p, need.p);
     k_uf_apply<<<(n + TB - 1) / TB, TB, 0, s>>>(b.info, b.linvel, b.angvel, b.sleep, n, parent.p, awake.p, world_of,
-                                                 simulate_flag, b.rec_flags);
+                                                 simulate_flag, b.rec_flags, need.p);
 }
 
 }  // namespace bgpu
