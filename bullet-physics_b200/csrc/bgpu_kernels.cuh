@@ -127,6 +127,10 @@ __device__ __forceinline__ size_t tix(uint32_t plane, uint32_t k, uint32_t t) {
     return ((size_t(t >> 5) * PLANES + plane) * 4 + k) * 32 + (t & 31u);
 }
 
+// float4 between consecutive planes of one (contact, slot): plane p of (k, t) is
+// tab[tix<PLANES>(0, k, t) + p * PLANE_STRIDE], a constant offset the loads fold in.
+constexpr uint32_t PLANE_STRIDE = 4 * 32;
+
 // ---------------------------------------------------------------- body kernels (k_body.cu)
 void launch_integrate_velocities(const BodyDev& b, const Shape* shapes, const float4* hull, uint32_t n, float dt,
                                  cudaStream_t s);

@@ -89,8 +89,8 @@ __device__ __forceinline__ size_t lix(uint32_t k, uint32_t t) { return tix<1>(0,
 __device__ __forceinline__ void reverse_group(const AdjArgs& a, uint32_t t, uint32_t sweep) {
     const uint4 rec = a.recs[t];
     const uint32_t ia = rec.x, ib = rec.y, p = rec.z & 0x1fffffffu, cnt = rec.z >> 29;
-    const float4* v = a.tab;
-    const float ima = v[tix<VT_PLANES>(3, 0, t)].w, imb = v[tix<VT_PLANES>(4, 0, t)].w;
+    const float4* e0 = a.tab + tix<VT_PLANES>(0, 0, t);
+    const float ima = e0[3 * PLANE_STRIDE].w, imb = e0[4 * PLANE_STRIDE].w;
     const bool appa = ima > 0.0f, appb = imb > 0.0f;
     V3 La = from4(__ldcg(&a.vbar[ia])), Wa = from4(__ldcg(&a.wbar[ia]));
     V3 Lb = from4(__ldcg(&a.vbar[ib])), Wb = from4(__ldcg(&a.wbar[ib]));
@@ -111,8 +111,9 @@ __device__ __forceinline__ void reverse_group(const AdjArgs& a, uint32_t t, uint
     float mub = 0.0f, eb = 0.0f;
     for (int kk = int(cnt) - 1; kk >= 0; --kk) {
         const uint32_t k = uint32_t(kk);
-        const V3 n = from4(v[tix<VT_PLANES>(0, k, t)]);
-        const V3 ana = from4(v[tix<VT_PLANES>(5, k, t)]), anb = from4(v[tix<VT_PLANES>(6, k, t)]);
+        const float4* e = a.tab + tix<VT_PLANES>(0, k, t);
+        const V3 n = from4(e[0 * PLANE_STRIDE]);
+        const V3 ana = from4(e[5 * PLANE_STRIDE]), anb = from4(e[6 * PLANE_STRIDE]);
         float4 lb = a.lbar[lix(k, t)];
         if (sweep == 0) {  // warm start: only the normal impulse is nonzero (step.rs:751)
             const float lin = lb.x + japp(n, ana, anb);
@@ -120,14 +121,14 @@ __device__ __forceinline__ void reverse_group(const AdjArgs& a, uint32_t t, uint
             if (src != REC_NONE && a.carry_out) atomicAdd(&a.carry_out[src], a.warm_factor * lin);
             continue;
         }
-        const float4 r0 = v[tix<VT_PLANES>(0, k, t)], r1 = v[tix<VT_PLANES>(1, k, t)], r2 = v[tix<VT_PLANES>(2, k, t)];
-        const float4 q3 = v[tix<VT_PLANES>(3, k, t)], q4 = v[tix<VT_PLANES>(4, k, t)];
-        const float4 q5 = v[tix<VT_PLANES>(5, k, t)], q6 = v[tix<VT_PLANES>(6, k, t)];
-        const float4 q7 = v[tix<VT_PLANES>(7, k, t)], q8 = v[tix<VT_PLANES>(8, k, t)];
-        const float4 q9 = v[tix<VT_PLANES>(9, k, t)], q10 = v[tix<VT_PLANES>(10, k, t)];
+        const float4 r0 = e[0 * PLANE_STRIDE], r1 = e[1 * PLANE_STRIDE], r2 = e[2 * PLANE_STRIDE];
+        const float4 q3 = e[3 * PLANE_STRIDE], q4 = e[4 * PLANE_STRIDE];
+        const float4 q5 = e[5 * PLANE_STRIDE], q6 = e[6 * PLANE_STRIDE];
+        const float4 q7 = e[7 * PLANE_STRIDE], q8 = e[8 * PLANE_STRIDE];
+        const float4 q9 = e[9 * PLANE_STRIDE], q10 = e[10 * PLANE_STRIDE];
         const V3 ra = from4(r1), rb = from4(r2), t1 = from4(q3), t2 = from4(q4);
         const V3 a1a = from4(q7), a1b = from4(q8), a2a = from4(q9), a2b = from4(q10);
-        const V3 kn = from4(v[tix<VT_PLANES>(11, k, t)]), kt1 = from4(v[tix<VT_PLANES>(12, k, t)]);
+        const V3 kn = from4(e[11 * PLANE_STRIDE]), kt1 = from4(e[12 * PLANE_STRIDE]);
         const float mn = q5.w, m1 = q6.w, m2 = q7.w, cfm = q8.w, e_ab = q9.w, mu_ab = r0.w;
         const float4 sr = a.sweeps[sweep_index(sweep, k, t, a.iters)];
         const float vn = sr.x, nimp = sr.y;

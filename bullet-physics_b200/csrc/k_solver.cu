@@ -353,6 +353,7 @@ __device__ __forceinline__ void warm_group(const SolveArgs& a, uint32_t t, uint3
     appa = ima > 0.0f;
     appb = imb > 0.0f;
     for (uint32_t k = 0; k < cnt; ++k) {
+        float4* e = a.vtab + tix<VT_PLANES>(0, k, t);
         const float4* r = a.rows + (size_t(p) * 4 + k) * ROW_F4;
         const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
         const V3 n = from4(r0), ra = from4(r1), rb = from4(r2);
@@ -369,51 +370,46 @@ __device__ __forceinline__ void warm_group(const SolveArgs& a, uint32_t t, uint3
         apply(la, wa, lb, wb, appa, appb, ima, imb, t1, a1a, a1b, r3.y);
         apply(la, wa, lb, wb, appa, appb, ima, imb, t2, a2a, a2b, r3.z);
         float4* v = a.vtab;
-        v[tix<VT_PLANES>(0, k, t)] = r0;
-        v[tix<VT_PLANES>(1, k, t)] = r1;
-        v[tix<VT_PLANES>(2, k, t)] = r2;
-        v[tix<VT_PLANES>(3, k, t)] = f4(t1, ima);
-        v[tix<VT_PLANES>(4, k, t)] = f4(t2, imb);
-        v[tix<VT_PLANES>(5, k, t)] = f4(ana, r4.x);
-        v[tix<VT_PLANES>(6, k, t)] = f4(anb, r4.y);
-        v[tix<VT_PLANES>(7, k, t)] = f4(a1a, r4.z);
-        v[tix<VT_PLANES>(8, k, t)] = f4(a1b, r4.w);
-        v[tix<VT_PLANES>(9, k, t)] = f4(a2a, r3.w);
-        v[tix<VT_PLANES>(10, k, t)] = f4(a2b, 0.0f);
-        v[tix<VT_PLANES>(11, k, t)] = f4(kn, 0.0f);
-        v[tix<VT_PLANES>(12, k, t)] = f4(kt1, 0.0f);
-        v[tix<VT_PLANES>(13, k, t)] = f4(kt2, 0.0f);
-        v[tix<VT_PLANES>(14, k, t)] = r3;
+        e[0 * PLANE_STRIDE] = r0;
+        e[1 * PLANE_STRIDE] = r1;
+        e[2 * PLANE_STRIDE] = r2;
+        e[3 * PLANE_STRIDE] = f4(t1, ima);
+        e[4 * PLANE_STRIDE] = f4(t2, imb);
+        e[5 * PLANE_STRIDE] = f4(ana, r4.x);
+        e[6 * PLANE_STRIDE] = f4(anb, r4.y);
+        e[7 * PLANE_STRIDE] = f4(a1a, r4.z);
+        e[8 * PLANE_STRIDE] = f4(a1b, r4.w);
+        e[9 * PLANE_STRIDE] = f4(a2a, r3.w);
+        e[10 * PLANE_STRIDE] = f4(a2b, 0.0f);
+        e[11 * PLANE_STRIDE] = f4(kn, 0.0f);
+        e[12 * PLANE_STRIDE] = f4(kt1, 0.0f);
+        e[13 * PLANE_STRIDE] = f4(kt2, 0.0f);
+        e[14 * PLANE_STRIDE] = r3;
     }
 }
 
 __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
-__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
-// Bring contact k of slot t's velocity-table entries into L1 (all planes).
-__device__ __forceinline__ void prefetch_contact_l1(const float4* v, uint32_t k, uint32_t t) {
-    for (uint32_t pl = 0; pl < VT_PLANES; ++pl) prefetch_l1(&v[tix<VT_PLANES>(pl, k, t)]);
-}
 
 // One solve_contact sweep (sequential_impulse.rs:804-930) over group slot t;
 // on the last sweep the impulses also go back to the pair's rows.
 __device__ __forceinline__ void iter_group(const SolveArgs& a, uint32_t t, uint32_t p, uint32_t cnt, uint32_t sweep,
                                            bool last, V3& la, V3& wa, V3& lb, V3& wb, bool& appa, bool& appb) {
-    const float4* v = a.vtab;
-    const float ima = v[tix<VT_PLANES>(3, 0, t)].w, imb = v[tix<VT_PLANES>(4, 0, t)].w;
+    const float4* e0 = a.vtab + tix<VT_PLANES>(0, 0, t);
+    const float ima = e0[3 * PLANE_STRIDE].w, imb = e0[4 * PLANE_STRIDE].w;
     appa = ima > 0.0f;
     appb = imb > 0.0f;
     for (uint32_t k = 0; k < cnt; ++k) {
-        if (k + 1 < cnt) prefetch_contact_l1(v, k + 1, t);
-        const float4 r0 = v[tix<VT_PLANES>(0, k, t)], r1 = v[tix<VT_PLANES>(1, k, t)],
-                     r2 = v[tix<VT_PLANES>(2, k, t)];
-        const float4 q3 = v[tix<VT_PLANES>(3, k, t)], q4 = v[tix<VT_PLANES>(4, k, t)];
-        const float4 q5 = v[tix<VT_PLANES>(5, k, t)], q6 = v[tix<VT_PLANES>(6, k, t)];
-        const float4 q7 = v[tix<VT_PLANES>(7, k, t)], q8 = v[tix<VT_PLANES>(8, k, t)];
-        const float4 q9 = v[tix<VT_PLANES>(9, k, t)], q10 = v[tix<VT_PLANES>(10, k, t)];
-        const float4 q11 = v[tix<VT_PLANES>(11, k, t)], q12 = v[tix<VT_PLANES>(12, k, t)];
-        const float4 q13 = v[tix<VT_PLANES>(13, k, t)];
-        const float4 r3 = v[tix<VT_PLANES>(14, k, t)];
+        float4* e = a.vtab + tix<VT_PLANES>(0, k, t);
+        const float4 r0 = e[0 * PLANE_STRIDE], r1 = e[1 * PLANE_STRIDE],
+                     r2 = e[2 * PLANE_STRIDE];
+        const float4 q3 = e[3 * PLANE_STRIDE], q4 = e[4 * PLANE_STRIDE];
+        const float4 q5 = e[5 * PLANE_STRIDE], q6 = e[6 * PLANE_STRIDE];
+        const float4 q7 = e[7 * PLANE_STRIDE], q8 = e[8 * PLANE_STRIDE];
+        const float4 q9 = e[9 * PLANE_STRIDE], q10 = e[10 * PLANE_STRIDE];
+        const float4 q11 = e[11 * PLANE_STRIDE], q12 = e[12 * PLANE_STRIDE];
+        const float4 q13 = e[13 * PLANE_STRIDE];
+        const float4 r3 = e[14 * PLANE_STRIDE];
         const V3 n = from4(r0), ra = from4(r1), rb = from4(r2), t1 = from4(q3), t2 = from4(q4);
         const V3 ana = from4(q5), anb = from4(q6), a1a = from4(q7), a1b = from4(q8), a2a = from4(q9), a2b = from4(q10);
         const V3 kn = from4(q11), kt1 = from4(q12), kt2 = from4(q13);
@@ -454,7 +450,7 @@ __device__ __forceinline__ void iter_group(const SolveArgs& a, uint32_t t, uint3
             const uint32_t s2 = u2 > maxf ? 1u : (u2 < -maxf ? 2u : 0u);
             a.srec[sweep_index(sweep, k, t, a.iterations)] = make_float4(vn, nimp, __uint_as_float(s1 | (s2 << 2)), 0.0f);
         }
-        a.vtab[tix<VT_PLANES>(14, k, t)] = nr3;
+        e[14 * PLANE_STRIDE] = nr3;
         if (last) a.rows[(size_t(p) * 4 + k) * ROW_F4 + 3] = nr3;
     }
 }
@@ -464,19 +460,20 @@ __device__ __forceinline__ void iter_group(const SolveArgs& a, uint32_t t, uint3
 __device__ __forceinline__ void split_group(const SolveArgs& a, uint32_t t, uint32_t p, uint32_t cnt, uint32_t ia,
                                             uint32_t ib, bool first, bool last, V3& pla, V3& pwa, V3& plb, V3& pwb,
                                             bool& appa, bool& appb) {
-    float4* s = a.stab;
+    const float4* e0 = a.stab + tix<ST_PLANES>(0, 0, t);
     float ima, imb;
     M3 iwa, iwb;
     if (first) {
         iwa = load_iw(a.iw, ia, ima);
         iwb = load_iw(a.iw, ib, imb);
     } else {
-        ima = s[tix<ST_PLANES>(3, 0, t)].w;
-        imb = s[tix<ST_PLANES>(4, 0, t)].w;
+        ima = e0[3 * PLANE_STRIDE].w;
+        imb = e0[4 * PLANE_STRIDE].w;
     }
     appa = ima > 0.0f;
     appb = imb > 0.0f;
     for (uint32_t k = 0; k < cnt; ++k) {
+        float4* e = a.stab + tix<ST_PLANES>(0, k, t);
         float4 q0, q1, q2, q3, q4, r5;
         if (first) {
             const float4* r = a.rows + (size_t(p) * 4 + k) * ROW_F4;
@@ -489,24 +486,24 @@ __device__ __forceinline__ void split_group(const SolveArgs& a, uint32_t t, uint
             q2 = f4(rb, 0.0f);
             q3 = f4(ana, ima);
             q4 = f4(anb, imb);
-            s[tix<ST_PLANES>(0, k, t)] = q0;
-            s[tix<ST_PLANES>(1, k, t)] = q1;
-            s[tix<ST_PLANES>(2, k, t)] = q2;
-            s[tix<ST_PLANES>(3, k, t)] = q3;
-            s[tix<ST_PLANES>(4, k, t)] = q4;
+            e[0 * PLANE_STRIDE] = q0;
+            e[1 * PLANE_STRIDE] = q1;
+            e[2 * PLANE_STRIDE] = q2;
+            e[3 * PLANE_STRIDE] = q3;
+            e[4 * PLANE_STRIDE] = q4;
         } else {
-            r5 = s[tix<ST_PLANES>(5, k, t)];
+            r5 = e[5 * PLANE_STRIDE];
         }
         if (r5.z == 0.0f) {
-            if (first) s[tix<ST_PLANES>(5, k, t)] = r5;
+            if (first) e[5 * PLANE_STRIDE] = r5;
             continue;
         }
         if (!first) {
-            q0 = s[tix<ST_PLANES>(0, k, t)];
-            q1 = s[tix<ST_PLANES>(1, k, t)];
-            q2 = s[tix<ST_PLANES>(2, k, t)];
-            q3 = s[tix<ST_PLANES>(3, k, t)];
-            q4 = s[tix<ST_PLANES>(4, k, t)];
+            q0 = e[0 * PLANE_STRIDE];
+            q1 = e[1 * PLANE_STRIDE];
+            q2 = e[2 * PLANE_STRIDE];
+            q3 = e[3 * PLANE_STRIDE];
+            q4 = e[4 * PLANE_STRIDE];
         }
         const V3 n = from4(q0), ra = from4(q1), rb = from4(q2), ana = from4(q3), anb = from4(q4);
         const float nmass = q0.w, cfm = q1.w;
@@ -522,7 +519,7 @@ __device__ __forceinline__ void split_group(const SolveArgs& a, uint32_t t, uint
             if (appb) { plb += n * (j * imb); pwb += anb * j; }
         }
         const float4 nr5 = make_float4(r5.x, np, r5.z, r5.w);
-        s[tix<ST_PLANES>(5, k, t)] = nr5;
+        e[5 * PLANE_STRIDE] = nr5;
         if (last) a.rows[(size_t(p) * 4 + k) * ROW_F4 + 5] = nr5;
     }
 }
@@ -544,13 +541,19 @@ __device__ __forceinline__ void run_group(const SolveArgs& a, uint32_t t, uint4 
     if (appb) { __stcg(&plin[ib], to4(lb, 0.0f)); __stcg(&pang[ib], to4(wb, 0.0f)); }
 }
 
+// Bring all of a slot's table entries into L1 (the next phase's group, while the
+// team waits at the barrier: a phase's entries, ~1.5 contacts x 240 B per slot,
+// fit in L1 next to nothing else the solve keeps there).
 template <bool VELOCITY>
-__device__ __forceinline__ void prefetch_slot_l2(const SolveArgs& a, uint32_t t, uint32_t cnt) {
+__device__ __forceinline__ void prefetch_slot_l1(const SolveArgs& a, uint32_t t, uint32_t cnt) {
     for (uint32_t k = 0; k < cnt; ++k) {
-        if (VELOCITY)
-            for (uint32_t pl = 0; pl < VT_PLANES; ++pl) prefetch_l2(&a.vtab[tix<VT_PLANES>(pl, k, t)]);
-        else
-            for (uint32_t pl = 0; pl < ST_PLANES; ++pl) prefetch_l2(&a.stab[tix<ST_PLANES>(pl, k, t)]);
+        if (VELOCITY) {
+            const float4* e = a.vtab + tix<VT_PLANES>(0, k, t);
+            for (uint32_t pl = 0; pl < VT_PLANES; ++pl) prefetch_l1(e + pl * PLANE_STRIDE);
+        } else {
+            const float4* e = a.stab + tix<ST_PLANES>(0, k, t);
+            for (uint32_t pl = 0; pl < ST_PLANES; ++pl) prefetch_l1(e + pl * PLANE_STRIDE);
+        }
     }
 }
 
@@ -585,8 +588,8 @@ __device__ __forceinline__ void run_phases(const SolveArgs& a, const uint4* __re
         }
         rec = next;
         if (q + 1 < nphases) {
-            // The next phase's table entries (written in sweep 0) head for L2 while the team waits.
-            if (rec.z && (q + 1) >= ncol) prefetch_slot_l2<VELOCITY>(a, soff[(q + 1) % ncol] + tid, rec.z >> 29);
+            // The next phase's table entries (written in sweep 0) head for L1 while the team waits.
+            if (rec.z && (q + 1) >= ncol) prefetch_slot_l1<VELOCITY>(a, soff[(q + 1) % ncol] + tid, rec.z >> 29);
             team_barrier(ctr, ++nbar * team_blocks, a.status);
         }
     }
