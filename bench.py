@@ -134,6 +134,16 @@ def algorithmic_pgs_bytes(st, iters):
     return c * (300 * iters + 120) + 100 * split_c * iters
 
 
+def pinned_array(shape):
+    """A float32 host array in page-locked memory (falls back to pageable if torch cannot pin)."""
+    try:
+        import torch
+
+        return torch.zeros(shape, dtype=torch.float32, pin_memory=True).numpy()
+    except Exception:
+        return np.zeros(shape, dtype=np.float32)
+
+
 def count_launches(w, dt, nsteps=2):
     """Kernels the library launches per step, counted by CUPTI (torch.profiler) over
     `nsteps` untimed steps run after the timed region; memcpy/memset are not counted."""
@@ -312,9 +322,9 @@ def main():
         dist.barrier()
     value = n_dyn * args.steps * world_size / (region_ms / 1000.0)
 
-    # End to end through the public API with host buffers.
-    forces = np.zeros((w.num_bodies, 3), dtype=np.float32)
-    poses = np.zeros((w.num_bodies, 7), dtype=np.float32)
+    # End to end through the public API with pinned host buffers (force upload, step, pose read-back).
+    forces = pinned_array((w.num_bodies, 3))
+    poses = pinned_array((w.num_bodies, 7))
     e2e_steps = max(1, min(args.steps, 30))
     t0 = time.perf_counter()
     for _ in range(e2e_steps):

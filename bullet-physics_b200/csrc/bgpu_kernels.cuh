@@ -137,6 +137,9 @@ void launch_integrate_velocities(const BodyDev& b, const Shape* shapes, const fl
 void launch_initial_aabbs(const BodyDev& b, const Shape* shapes, const float4* hull, uint32_t first, uint32_t n,
                           cudaStream_t s);
 void launch_integrate_positions(const BodyDev& b, uint32_t n, float dt, float turn_erp, cudaStream_t s);
+// Host-facing layouts: n x 3 floats -> float4 lanes, and poses -> n x 7 floats.
+void launch_unpack3(uint32_t n, const float* src, float4* dst, cudaStream_t s);
+void launch_pack_poses(uint32_t n, const float4* pos, const float4* quat, float* out, cudaStream_t s);
 
 // ---------------------------------------------------------------- broad phase (k_broadphase.cu)
 // Sorted closed-overlap pairs of n AABBs. `unbounded` lists (ascending) the

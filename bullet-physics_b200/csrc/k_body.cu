@@ -219,4 +219,32 @@ void launch_integrate_positions(const BodyDev& b, uint32_t n, float dt, float tu
     k_integrate_positions<<<(n + 255) / 256, 256, 0, s>>>(b, n, dt, turn_erp);
 }
 
+namespace {
+
+// n x 3 floats (the caller's layout) -> float4 lanes.
+__global__ void k_unpack3(uint32_t n, const float* __restrict__ src, float4* dst) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dst[i] = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0f);
+}
+
+// position + orientation -> n x 7 floats (x y z qx qy qz qw).
+__global__ void k_pack_poses(uint32_t n, const float4* __restrict__ pos, const float4* __restrict__ quat, float* out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = pos[i], q = quat[i];
+    float* o = out + size_t(i) * 7;
+    o[0] = p.x; o[1] = p.y; o[2] = p.z; o[3] = q.x; o[4] = q.y; o[5] = q.z; o[6] = q.w;
+}
+
+}  // namespace
+
+void launch_unpack3(uint32_t n, const float* src, float4* dst, cudaStream_t s) {
+    if (n) k_unpack3<<<(n + 255) / 256, 256, 0, s>>>(n, src, dst);
+}
+
+void launch_pack_poses(uint32_t n, const float4* pos, const float4* quat, float* out, cudaStream_t s) {
+    if (n) k_pack_poses<<<(n + 255) / 256, 256, 0, s>>>(n, pos, quat, out);
+}
+
 }  // namespace bgpu

@@ -158,6 +158,7 @@ struct World {
     static constexpr uint64_t RECOLOUR_PERIOD = 64;
     // adjoint recording: the step being recorded (null otherwise) and the pair pass's scratch
     StepRecord* rec_step = nullptr;
+    DevBuf<float> host_io;  // device staging for the caller-layout force / pose buffers
     DevBuf<uint8_t> rec_pt_src;
     DevBuf<uint32_t> rec_pair_old;
 
@@ -1178,16 +1179,14 @@ bgpu_status bgpu_read_poses(bgpu_world* w, float* poses) {
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         uint32_t n = W.n;
-        std::vector<float4> p(n), q(n);
+        if (!n) return BGPU_OK;
         cudaStream_t s = W.stream;
-        bgpu::check_cuda(cudaMemcpyAsync(p.data(), W.pos.p, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "d2h");
-        bgpu::check_cuda(cudaMemcpyAsync(q.data(), W.quat.p, n * sizeof(float4), cudaMemcpyDeviceToHost, s), "d2h");
+        // Packed on the device, one copy into the caller's buffer (direct DMA when it is pinned).
+        W.host_io.reserve(size_t(n) * 7);
+        bgpu::launch_pack_poses(n, W.pos.p, W.quat.p, W.host_io.p, s);
+        bgpu::check_cuda(cudaMemcpyAsync(poses, W.host_io.p, size_t(n) * 7 * sizeof(float), cudaMemcpyDeviceToHost, s),
+                         "d2h");
         bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
-        for (uint32_t i = 0; i < n; ++i) {
-            float* o = poses + size_t(i) * 7;
-            o[0] = p[i].x; o[1] = p[i].y; o[2] = p[i].z;
-            o[3] = q[i].x; o[4] = q[i].y; o[5] = q[i].z; o[6] = q[i].w;
-        }
         return BGPU_OK;
     });
 }
@@ -1197,16 +1196,20 @@ bgpu_status bgpu_apply_forces(bgpu_world* w, const float* force, const float* to
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         uint32_t n = W.n;
-        std::vector<float4> f(n);
+        if (!n) return BGPU_OK;
         cudaStream_t s = W.stream;
+        // One copy of the caller's n x 3 floats each, widened on the device; the sync at the
+        // end returns the caller's buffers (the copies may read them asynchronously when pinned).
+        W.host_io.reserve(size_t(n) * 6);
         for (int which = 0; which < 2; ++which) {
             const float* src = which ? torque : force;
             if (!src) continue;
-            for (uint32_t i = 0; i < n; ++i) f[i] = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0f);
-            bgpu::check_cuda(cudaMemcpyAsync(which ? W.torque.p : W.force.p, f.data(), n * sizeof(float4),
-                                             cudaMemcpyHostToDevice, s), "h2d");
-            bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+            float* stage = W.host_io.p + size_t(which) * 3 * n;
+            bgpu::check_cuda(cudaMemcpyAsync(stage, src, size_t(n) * 3 * sizeof(float), cudaMemcpyHostToDevice, s),
+                             "h2d");
+            bgpu::launch_unpack3(n, stage, which ? W.torque.p : W.force.p, s);
         }
+        bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
         return BGPU_OK;
     });
 }
