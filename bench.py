@@ -134,6 +134,22 @@ def algorithmic_pgs_bytes(st, iters):
     return c * (300 * iters + 120) + 100 * split_c * iters
 
 
+def max_over_ranks(dist, x, device=None):
+    """The largest of every rank's x (the job's time is its slowest replica's); x itself on one rank."""
+    if not dist:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device or ("cuda" if torch.cuda.is_available() else "cpu"))
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank, steps, world_size, seconds):
+    """Whole-job throughput of independent replicas: all ranks' units x steps over the slowest rank's time."""
+    return units_per_rank * steps * world_size / seconds
+
+
 def pinned_array(shape):
     """A float32 host array in page-locked memory (falls back to pageable if torch cannot pin)."""
     try:
@@ -312,15 +328,10 @@ def main():
         ms = w.step_timed(sc.dt, args.steps)
     st = w.stats()
     w.enable_timing(False)
-    region_ms = ms
+    region_ms = max_over_ranks(dist, ms)
     if dist:
-        import torch
-
-        t = torch.tensor([region_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        region_ms = float(t.item())
         dist.barrier()
-    value = n_dyn * args.steps * world_size / (region_ms / 1000.0)
+    value = replica_throughput(n_dyn, args.steps, world_size, region_ms / 1000.0)
 
     # End to end through the public API with pinned host buffers (force upload, step, pose read-back).
     forces = pinned_array((w.num_bodies, 3))
@@ -331,14 +342,8 @@ def main():
         w.apply_forces(forces)
         w.step(sc.dt)
         w.poses(poses)
-    e2e_s = time.perf_counter() - t0
-    e2e_value = n_dyn * e2e_steps * world_size / e2e_s
-    if dist:
-        import torch
-
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_value = n_dyn * e2e_steps * world_size / float(t.item())
+    e2e_s = max_over_ranks(dist, time.perf_counter() - t0)
+    e2e_value = replica_throughput(n_dyn, e2e_steps, world_size, e2e_s)
 
     launches_per_step, kernel_kinds = count_launches(w, sc.dt) if rank == 0 else (None, 0)
 
