@@ -91,6 +91,7 @@ def lib():
             "bgpu_read_pairs": (S, [P, U32P, ctypes.c_uint64, U64P]),
             "bgpu_read_contacts": (S, [P, F, ctypes.c_uint64, U64P]),
             "bgpu_read_solve_order": (S, [P, U64P, ctypes.c_uint64, U64P]),
+            "bgpu_read_colour_batches": (S, [P, U32P, U32P, U32, U32P]),
             "bgpu_get_stats": (S, [P, ctypes.POINTER(StepStats)]),
             "bgpu_enable_step_timing": (S, [P, ctypes.c_int]),
             "bgpu_broadphase_pairs": (S, [F, U32, U32P, ctypes.c_uint64, U64P]),
@@ -359,6 +360,17 @@ class World:
         if n.value:
             check(self.L.bgpu_read_solve_order(self.h, u64ptr(out), n.value, ctypes.byref(n)), "read_solve_order")
         return out
+
+    def colour_batches(self):
+        """Per colour of the last step's PGS: (row groups, row groups with split-impulse rows)."""
+        n = ctypes.c_uint32()
+        check(self.L.bgpu_read_colour_batches(self.h, None, None, 0, ctypes.byref(n)), "read_colour_batches")
+        g = np.zeros(n.value, dtype=np.uint32)
+        sg = np.zeros(n.value, dtype=np.uint32)
+        if n.value:
+            check(self.L.bgpu_read_colour_batches(self.h, u32ptr(g), u32ptr(sg), n.value, ctypes.byref(n)),
+                  "read_colour_batches")
+        return g, sg
 
     def stats(self):
         s = StepStats()

@@ -75,6 +75,7 @@ constexpr unsigned int BARRIER_SPIN_LIMIT = 1u << 26;
 // n blocks completes when the counter reaches k * n. One atomic per block,
 // then a tight spin. The spin is bounded: on timeout the status word records
 // it and every later barrier returns at once, so no launch can hang the device.
+// (Spinning on relaxed loads with one acquire fence at the end measured slower.)
 __device__ __forceinline__ void team_barrier(unsigned int* ctr, unsigned int target, uint32_t* status) {
     __syncthreads();
     if (threadIdx.x == 0 && !(*(volatile uint32_t*)status & ST_BARRIER_TIMEOUT)) {
@@ -93,6 +94,9 @@ __device__ __forceinline__ void team_barrier(unsigned int* ctr, unsigned int tar
     }
     __syncthreads();
 }
+
+// PGS colours per step (a colouring that needs more records ST_COLOUR_OVERFLOW).
+constexpr int MAX_COLOURS = 128;
 
 // Per-step contact tables in batch-slot order. Slots are grouped 32 at a time
 // (colour batches start on a multiple of 32, so a warp's lanes hold exactly one
@@ -148,10 +152,11 @@ void launch_pack_poses(uint32_t n, const float4* pos, const float4* quat, float*
 struct Broadphase {
     DevBuf<uint64_t> keys, keys_alt;
     DevBuf<uint32_t> leaf_body, parent, left, right, counts, offsets, refit_flag, flags, scan_out, unbounded;
+    DevBuf<uint32_t> stash, overflow;  // partners of proxies with few of them; proxies with many
     DevBuf<float4> node_min, node_max;
     DevBuf<unsigned char> cub_tmp;
     DevBuf<int> bounds;          // 6 ordered ints: scene min/max of leaf centres
-    DevBuf<uint32_t> scalars;    // [0] total pairs, [1] status, [2] per-unbounded count
+    DevBuf<uint32_t> scalars;    // [0] total pairs, [1] proxies with more partners than the stash holds
     uint32_t* host_scalars = nullptr;  // pinned
     Broadphase();
     ~Broadphase();
@@ -205,6 +210,8 @@ struct PairDataDev {
     RecordDev rec;
 };
 
+constexpr uint32_t ROUTE_COUNT0 = 16;  // first per-route counter in PairData::scalars
+
 struct PairData {
     // Per pair (indexed like the sorted pair array).
     DevBuf<uint32_t> status;       // PS_* | route << 8
@@ -213,11 +220,12 @@ struct PairData {
     DevBuf<uint32_t> detect_n;     // points per fresh detection
     DevBuf<uint32_t> row_count;    // solver rows per pair (0..4)
     DevBuf<float4> rows;           // ROW_F4 per contact slot, 4 slots per pair
-    DevBuf<uint32_t> route_list;   // pairs needing detection: [0, P) analytic, [P, 2P) convex
+    DevBuf<uint32_t> route_list;   // pairs needing detection, one list per route r: [(r - 1) P, r P)
     DevBuf<uint32_t> old_owned;    // per old manifold: 1 when a current pair took it over
     DevBuf<uint32_t> scalars;      // [0] analytic count [1] convex count [2] contact pairs [3] contacts
                                    // [4] colours [5] split pairs [6] detect total [7] manifolds
                                    // [8] [9] cache compaction counts [10] split contacts [11] largest split batch
+                                   // [ROUTE_COUNT0 + r] pairs on narrow-phase route r
     // Solver batches
     DevBuf<uint32_t> contact_pairs;  // pair ids with rows (ascending)
     DevBuf<uint32_t> colour;         // per contact pair
@@ -225,6 +233,7 @@ struct PairData {
     DevBuf<unsigned long long> body_mask;  // 2 words per body: colours taken at the body
     DevBuf<unsigned long long> body_dup;   // 2 words per body: colours seeded twice at the body
     DevBuf<uint32_t> colour_remap;         // colour -> dense colour (empty colours dropped)
+    DevBuf<uint32_t> colour_work;          // two lists of uncoloured groups (Jones-Plassmann rounds)
     DevBuf<uint32_t> colour_count, colour_offset, colour_cursor;
     DevBuf<uint32_t> split_count, split_offset, split_cursor;
     DevBuf<uint4> batch_rec;         // contact pairs in colour order: body a, body b, pair | rows << 29, 0
@@ -242,9 +251,9 @@ struct PairData {
         detect_n.reserve(npairs);
         row_count.reserve(npairs);
         rows.reserve(npairs * 4 * ROW_F4);
-        route_list.reserve(2 * npairs);
+        route_list.reserve(size_t(NP_CONVEX) * npairs);
         old_owned.reserve(old_manifolds + 1);
-        scalars.reserve(16);
+        scalars.reserve(ROUTE_COUNT0 + NP_CONVEX + 1);
         contact_pairs.reserve(npairs);
         colour.reserve(npairs);
         body_prio.reserve(nbodies);

@@ -4,10 +4,13 @@
 // Output contract (crates/bullet-collision/src/broadphase/mod.rs:94-130,
 // brute_force.rs:54-68): every pair (i < j) whose closed AABBs overlap on all
 // three axes (util.rs:28-38), sorted lexicographically. Each proxy i owns the
-// segment of partners j > i; a count pass sizes the segments, an exclusive
-// scan places them, and a write pass stores each segment already sorted, so
-// no global pair sort is needed. Unbounded proxies (planes) are kept out of
-// the tree and joined by an ordered flag/scan compaction.
+// segment of partners j > i. One tree walk per proxy counts its partners and
+// keeps them, sorted, in a fixed number of stash slots; an exclusive scan of
+// the counts places the segments and a copy pass moves the stashed ones into
+// place, so no global pair sort is needed. The few proxies with more partners
+// than slots walk the tree a second time and write their segment directly.
+// Unbounded proxies (planes) are kept out of the tree and joined by an ordered
+// flag/scan compaction.
 #include <cub/cub.cuh>
 #include "bgpu_kernels.cuh"
 
@@ -147,18 +150,37 @@ __global__ void k_refit(int m, const uint32_t* __restrict__ leaf_body, const uin
     }
 }
 
-// Count pass (write == false) or write pass: partners j > i of bounded proxy i.
-template <bool WRITE>
+// Partners j > i of bounded proxy i, in one of three modes:
+//   Q_COUNT  counts[i] only;
+//   Q_WRITE  the segment at offsets[i] (counts[i] from an earlier pass), sorted;
+//   Q_STASH  counts[i], and when it is at most STASH_SLOTS the sorted partners in
+//            stash slot a of Morton position t (stash[a * m + t], so a warp's
+//            writes of one slot are contiguous); a proxy with more partners is
+//            appended to `list` (its length in list_len) for a Q_WRITE pass.
+// Q_COUNT and Q_WRITE take the proxies from `list` when it is given (t < list_len).
+constexpr int Q_COUNT = 0, Q_WRITE = 1, Q_STASH = 2;
+constexpr uint32_t STASH_SLOTS = 32;
+
+template <int MODE>
 __global__ void k_query(int m, uint32_t n, const uint32_t* __restrict__ is_unb, const float4* __restrict__ bmin,
                         const float4* __restrict__ bmax, const float4* __restrict__ nmin, const float4* __restrict__ nmax,
                         const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
                         const uint32_t* __restrict__ leaf_body, const uint32_t* __restrict__ unb, uint32_t nunb,
-                        uint32_t* counts, const uint32_t* __restrict__ offsets, uint64_t* out, uint32_t* status) {
+                        uint32_t* counts, const uint32_t* __restrict__ offsets, uint64_t* out, uint32_t* status,
+                        uint32_t* list, uint32_t* list_len, uint32_t* stash) {
+    constexpr bool WRITE = MODE == Q_WRITE;
+    constexpr bool KEEP = MODE != Q_COUNT;
     // Threads take the bounded proxies in Morton (leaf) order, so a warp's
     // queries are neighbours in space and walk much the same part of the tree.
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= uint32_t(m)) return;
-    const uint32_t i = leaf_body[t];
+    uint32_t i;
+    if (MODE != Q_STASH && list) {
+        if (t >= *list_len) return;
+        i = list[t];
+    } else {
+        if (t >= uint32_t(m)) return;
+        i = leaf_body[t];
+    }
     float4 qmin = bmin[i], qmax = bmax[i];
     uint32_t cnt = 0;
     uint32_t local[LOCAL_SORT];
@@ -169,7 +191,9 @@ __global__ void k_query(int m, uint32_t n, const uint32_t* __restrict__ is_unb, 
         expected = counts[i];
     }
     auto emit = [&](uint32_t j) {
-        if (WRITE) {
+        if (MODE == Q_STASH) {
+            if (cnt < STASH_SLOTS) local[cnt] = j;
+        } else if (WRITE) {
             if (expected <= LOCAL_SORT) {
                 if (cnt < LOCAL_SORT) local[cnt] = j;
             } else if (cnt < expected) {
@@ -210,11 +234,18 @@ __global__ void k_query(int m, uint32_t n, const uint32_t* __restrict__ is_unb, 
         uint32_t h = unb[u];
         if (h > i && overlaps(qmin, qmax, bmin[h], bmax[h])) emit(h);
     }
-    if (!WRITE) {
+    if (!KEEP) {
         counts[i] = cnt;
         return;
     }
-    if (expected <= LOCAL_SORT) {
+    if (MODE == Q_STASH) {
+        counts[i] = cnt;
+        if (cnt > STASH_SLOTS) {
+            list[atomicAdd(list_len, 1u)] = i;
+            return;
+        }
+    }
+    if (MODE == Q_STASH || expected <= LOCAL_SORT) {
         uint32_t c = cnt < LOCAL_SORT ? cnt : LOCAL_SORT;
         for (uint32_t a = 1; a < c; ++a) {
             uint32_t v = local[a];
@@ -222,7 +253,10 @@ __global__ void k_query(int m, uint32_t n, const uint32_t* __restrict__ is_unb, 
             while (b > 0 && local[b - 1] > v) { local[b] = local[b - 1]; --b; }
             local[b] = v;
         }
-        for (uint32_t a = 0; a < c; ++a) out[base + a] = (uint64_t(i) << 32) | local[a];
+        if (MODE == Q_STASH)
+            for (uint32_t a = 0; a < c; ++a) stash[size_t(a) * uint32_t(m) + t] = local[a];
+        else
+            for (uint32_t a = 0; a < c; ++a) out[base + a] = (uint64_t(i) << 32) | local[a];
     } else {
         uint32_t c = cnt < expected ? cnt : expected;
         for (uint32_t a = 1; a < c; ++a) {
@@ -232,6 +266,18 @@ __global__ void k_query(int m, uint32_t n, const uint32_t* __restrict__ is_unb, 
             out[base + b] = v;
         }
     }
+}
+
+// Stashed segments (at most STASH_SLOTS partners) to their place in the pair list.
+__global__ void k_stash_copy(int m, const uint32_t* __restrict__ leaf_body, const uint32_t* __restrict__ counts,
+                             const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ stash, uint64_t* out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= uint32_t(m)) return;
+    const uint32_t i = leaf_body[t];
+    const uint32_t c = counts[i];
+    if (c > STASH_SLOTS) return;
+    const uint64_t base = offsets[i];
+    for (uint32_t a = 0; a < c; ++a) out[base + a] = (uint64_t(i) << 32) | stash[size_t(a) * uint32_t(m) + t];
 }
 
 // Unbounded proxy h: flags[j] = (j > h && overlap(h, j)) over all proxies.
@@ -395,8 +441,14 @@ uint64_t Broadphase::run(const float4* aabb_min, const float4* aabb_max, uint32_
                                                  aabb_max, node_min.p, node_max.p);
     }
     const uint32_t qgrid = m > 0 ? (uint32_t(m) + TB - 1) / TB : 1u;
-    k_query<false><<<qgrid, TB, 0, s>>>(m, n, flags.p, aabb_min, aabb_max, node_min.p, node_max.p, left.p, right.p,
-                                        leaf_body.p, unbounded.p, nunb, counts.p, nullptr, nullptr, status_dev);
+    // One traversal per proxy: counts, plus the sorted partners of every proxy with at
+    // most STASH_SLOTS of them; the rest are listed and walk the tree again below.
+    stash.reserve(size_t(STASH_SLOTS) * uint32_t(m > 0 ? m : 1));
+    overflow.reserve(uint32_t(m > 0 ? m : 1));
+    check_cuda(cudaMemsetAsync(scalars.p, 0, 2 * sizeof(uint32_t), s), "memset");
+    k_query<Q_STASH><<<qgrid, TB, 0, s>>>(m, n, flags.p, aabb_min, aabb_max, node_min.p, node_max.p, left.p, right.p,
+                                          leaf_body.p, unbounded.p, nunb, counts.p, nullptr, nullptr, status_dev,
+                                          overflow.p, scalars.p + 1, stash.p);
     // Unbounded proxies: count their segments by flag + scan.
     for (uint32_t u = 0; u < nunb; ++u) {
         uint32_t h = unbounded_host[u];
@@ -407,13 +459,17 @@ uint64_t Broadphase::run(const float4* aabb_min, const float4* aabb_max, uint32_
     }
     check_cuda(cub::DeviceScan::ExclusiveSum(cub_tmp.p, scan_bytes, counts.p, offsets.p, int(n), s), "scan");
     k_total<<<1, 1, 0, s>>>(n, counts.p, offsets.p, scalars.p);
-    check_cuda(cudaMemcpyAsync(host_scalars, scalars.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "total d2h");
+    check_cuda(cudaMemcpyAsync(host_scalars, scalars.p, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "total d2h");
     check_cuda(cudaStreamSynchronize(s), "broadphase sync");
     uint64_t total = host_scalars[0];
+    const uint32_t n_overflow = host_scalars[1];
     out.reserve(total + 1);
     if (total) {
-        k_query<true><<<qgrid, TB, 0, s>>>(m, n, flags.p, aabb_min, aabb_max, node_min.p, node_max.p, left.p, right.p,
-                                           leaf_body.p, unbounded.p, nunb, counts.p, offsets.p, out.p, status_dev);
+        if (m > 0) k_stash_copy<<<qgrid, TB, 0, s>>>(m, leaf_body.p, counts.p, offsets.p, stash.p, out.p);
+        if (n_overflow)
+            k_query<Q_WRITE><<<(n_overflow + TB - 1) / TB, TB, 0, s>>>(
+                m, n, flags.p, aabb_min, aabb_max, node_min.p, node_max.p, left.p, right.p, leaf_body.p, unbounded.p,
+                nunb, counts.p, offsets.p, out.p, status_dev, overflow.p, scalars.p + 1, nullptr);
         for (uint32_t u = 0; u < nunb; ++u) {
             uint32_t h = unbounded_host[u];
             k_unb_flags<<<grid, TB, 0, s>>>(h, n, aabb_min, aabb_max, scan_out.p);
@@ -596,8 +652,9 @@ extern "C" bgpu_status bgpu_broadphase_pairs_noalloc(const float* aabbs_dev, uin
         }
         uint32_t* status = scalars + 1;
         const uint32_t qgrid = m > 0 ? (uint32_t(m) + TB - 1) / TB : 1u;
-        k_query<false><<<qgrid, TB, 0, s>>>(m, n, is_unb, mn, mx, node_min, node_max, left, right, leaf_body,
-                                            unb_list, nunb, counts, nullptr, nullptr, status);
+        k_query<Q_COUNT><<<qgrid, TB, 0, s>>>(m, n, is_unb, mn, mx, node_min, node_max, left, right, leaf_body,
+                                              unb_list, nunb, counts, nullptr, nullptr, status, nullptr, nullptr,
+                                              nullptr);
         uint32_t* unb_scan = reinterpret_cast<uint32_t*>(db.Alternate());  // free after the build
         check_cuda(cudaStreamSynchronize(s), "sync");
         for (uint32_t u = 0; u < nunb; ++u) {
@@ -619,8 +676,9 @@ extern "C" bgpu_status bgpu_broadphase_pairs_noalloc(const float* aabbs_dev, uin
         }
         uint64_t* out = reinterpret_cast<uint64_t*>(pairs_dev);
         if (total) {
-            k_query<true><<<qgrid, TB, 0, s>>>(m, n, is_unb, mn, mx, node_min, node_max, left, right, leaf_body,
-                                               unb_list, nunb, counts, offsets, out, status);
+            k_query<Q_WRITE><<<qgrid, TB, 0, s>>>(m, n, is_unb, mn, mx, node_min, node_max, left, right, leaf_body,
+                                                  unb_list, nunb, counts, offsets, out, status, nullptr, nullptr,
+                                                  nullptr);
             for (uint32_t u = 0; u < nunb; ++u) {
                 uint32_t h = unb_host[u];
                 k_unb_flags<<<grid, TB, 0, s>>>(h, n, mn, mx, flags);

@@ -13,6 +13,15 @@
 // When no dynamic body is asleep or wants deactivation, every island that has
 // a dynamic body is awake and the decision changes nothing, so the union-find
 // is skipped (k_island_need raises the flag that the other kernels test).
+//
+// Pairs whose two bodies are both awake (Active / DisableDeactivation) are not
+// linked. That cannot change any body's decision: a set of the thinner
+// partition that has no awake member loses no pair (each dropped pair has
+// awake ends), so it is a whole island of the full partition; and a set cut
+// out of an island with an awake member was cut along a dropped pair, one of
+// whose awake ends it holds. So every body lands in a set with an awake member
+// exactly when its island has one, and a set with none (touched by a moving
+// kinematic or not) is the whole island.
 #include "bgpu_kernels.cuh"
 
 namespace bgpu {
@@ -22,6 +31,11 @@ namespace {
 constexpr int UF_LIMIT = 1 << 16;
 
 __device__ __forceinline__ bool participates(uint32_t flags) { return (flags & (BF_STATIC | BF_KINEMATIC)) == 0; }
+
+// body.rs:602-608 (is_island_awake): Active or DisableDeactivation.
+__device__ __forceinline__ bool awake_member(uint4 in) {
+    return participates(in.y) && (in.z == ACT_ACTIVE || in.z == ACT_DISABLE_DEACTIVATION);
+}
 
 __device__ __forceinline__ bool eligible(uint4 a, uint4 b) {
     if ((a.y | b.y) & BF_NO_RESPONSE) return false;
@@ -81,6 +95,7 @@ __global__ void k_uf_link(const uint4* __restrict__ info, const uint64_t* __rest
     uint32_t a = key_lo(k), b = key_hi(k);
     uint4 ia = info[a], ib = info[b];
     if (!eligible(ia, ib) || !participates(ia.y) || !participates(ib.y)) return;
+    if (awake_member(ia) && awake_member(ib)) return;
     for (int g = 0; g < UF_LIMIT; ++g) {
         uint32_t ra = find_halving(parent, a, status), rb = find_halving(parent, b, status);
         if (ra == rb) return;
@@ -96,8 +111,7 @@ __global__ void k_uf_flatten_awake(const uint4* __restrict__ info, uint32_t n, u
     if (i >= n || !*need) return;
     uint32_t r = find_root(parent, i, status);
     uint4 in = info[i];
-    // body.rs:602-608 (is_island_awake): Active or DisableDeactivation.
-    if (participates(in.y) && (in.z == ACT_ACTIVE || in.z == ACT_DISABLE_DEACTIVATION)) awake[r] = 1u;
+    if (awake_member(in)) awake[r] = 1u;
 }
 
 __global__ void k_uf_store_roots(uint32_t n, uint32_t* parent, uint32_t* status, const uint32_t* __restrict__ need) {

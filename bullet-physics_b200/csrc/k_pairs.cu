@@ -259,6 +259,29 @@ __device__ __forceinline__ bool active_state(uint32_t a) {
     return a == ACT_ACTIVE || a == ACT_WANTS_DEACTIVATION || a == ACT_DISABLE_DEACTIVATION;
 }
 
+// One atomicAdd per distinct route among the calling lanes of a warp.
+__device__ __forceinline__ uint32_t claim_route_slot(uint32_t* counts, uint32_t route) {
+    const uint32_t active = __activemask();
+    const uint32_t peers = __match_any_sync(active, route);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t leader = uint32_t(__ffs(int(peers)) - 1);
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&counts[route], uint32_t(__popc(int(peers))));
+    base = __shfl_sync(peers, base, int(leader));
+    return base + uint32_t(__popc(peers & ((1u << lane) - 1u)));
+}
+
+// Position t of the detection lists (the analytic routes in route order, then the
+// convex list) -> pair id. counts = the scalars from ROUTE_COUNT0 (index = route).
+__device__ __forceinline__ uint32_t detect_list_pair(const uint32_t* __restrict__ list, const uint32_t* counts,
+                                                     uint32_t npairs, uint32_t t, uint32_t last_route) {
+    for (uint32_t r = NP_PLANE_A; r <= last_route; ++r) {
+        if (t < counts[r]) return list[size_t(r - 1) * npairs + t];
+        t -= counts[r];
+    }
+    return 0xffffffffu;
+}
+
 // step.rs:645-799, classify + refresh path. Scalars: [0] analytic list count, [1] convex list count.
 __global__ void k_classify(BodyDev b, const Shape* __restrict__ shapes, const uint64_t* __restrict__ pairs,
                            uint32_t npairs, const uint64_t* __restrict__ old_keys, const float4* __restrict__ old_entries,
@@ -321,13 +344,10 @@ __global__ void k_classify(BodyDev b, const Shape* __restrict__ shapes, const ui
     uint32_t route = route_of(shapes[ia.x].type, shapes[ib.x].type);
     pd.status[p] = PS_DETECT | (route << 8);
     if (route == NP_NONE) return;
-    if (route == NP_CONVEX) {
-        uint32_t slot = atomicAdd(&pd.scalars[1], 1u);
-        pd.route_list[npairs + slot] = p;
-    } else {
-        uint32_t slot = atomicAdd(&pd.scalars[0], 1u);
-        pd.route_list[slot] = p;
-    }
+    // One list per route (route r in [(r - 1) P, r P), P = npairs), so that the narrow
+    // phase's warps run one shape routine each instead of every route their lanes hold.
+    const uint32_t slot = claim_route_slot(&pd.scalars[ROUTE_COUNT0], route);
+    pd.route_list[size_t(route - 1) * npairs + slot] = p;
 }
 
 // narrowphase/mod.rs:63-286 for one pair; returns the manifold (positions on B, normals A->B).
@@ -393,10 +413,17 @@ __device__ __forceinline__ bool entry_seed(const float4* __restrict__ e, V3& s) 
 }
 
 __global__ void k_narrow_analytic(BodyDev b, const Shape* __restrict__ shapes, const float4* __restrict__ hull,
-                                  const uint64_t* __restrict__ pairs, PairDataDev pd) {
-    uint32_t cnt = pd.scalars[0];
+                                  const uint64_t* __restrict__ pairs, uint32_t npairs, PairDataDev pd) {
+    uint32_t counts[NP_CONVEX + 1];
+    uint32_t cnt = 0;
+#pragma unroll
+    for (uint32_t r = 0; r <= NP_CONVEX; ++r) {
+        counts[r] = pd.scalars[ROUTE_COUNT0 + r];
+        if (r >= NP_PLANE_A && r < NP_CONVEX) cnt += counts[r];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) pd.scalars[0] = cnt;  // analytic detections (step statistics)
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
-        uint32_t p = pd.route_list[t];
+        uint32_t p = detect_list_pair(pd.route_list, counts, npairs, t, NP_BOX_BOX);
         uint64_t key = pairs[p];
         uint32_t i = key_lo(key), j = key_hi(key);
         uint4 ia = b.info[i], ib = b.info[j];
@@ -410,10 +437,11 @@ __global__ void k_narrow_analytic(BodyDev b, const Shape* __restrict__ shapes, c
 
 __global__ void k_narrow_convex(BodyDev b, const Shape* __restrict__ shapes, const float4* __restrict__ hull,
                                 const uint64_t* __restrict__ pairs, uint32_t npairs, PairDataDev pd, uint32_t* status) {
-    uint32_t cnt = pd.scalars[1];
+    uint32_t cnt = pd.scalars[ROUTE_COUNT0 + NP_CONVEX];
+    if (blockIdx.x == 0 && threadIdx.x == 0) pd.scalars[1] = cnt;  // convex detections (step statistics)
     EpaScratch scratch;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
-        uint32_t p = pd.route_list[npairs + t];
+        uint32_t p = pd.route_list[size_t(NP_CONVEX - 1) * npairs + t];
         uint64_t key = pairs[p];
         uint32_t i = key_lo(key), j = key_hi(key);
         uint4 ia = b.info[i], ib = b.info[j];
@@ -471,9 +499,15 @@ __device__ __forceinline__ void capture_one(const BodyDev& b, const Shape* __res
 
 __global__ void k_capture(BodyDev b, const Shape* __restrict__ shapes, const uint64_t* __restrict__ pairs,
                           uint32_t npairs, StepParams sp, PairDataDev pd) {
-    uint32_t na = pd.scalars[0], nc = pd.scalars[1];
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < na + nc; t += gridDim.x * blockDim.x) {
-        uint32_t p = t < na ? pd.route_list[t] : pd.route_list[npairs + (t - na)];
+    uint32_t counts[NP_CONVEX + 1];
+    uint32_t cnt = 0;
+#pragma unroll
+    for (uint32_t r = 0; r <= NP_CONVEX; ++r) {
+        counts[r] = pd.scalars[ROUTE_COUNT0 + r];
+        if (r >= NP_PLANE_A) cnt += counts[r];
+    }
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+        const uint32_t p = detect_list_pair(pd.route_list, counts, npairs, t, NP_CONVEX);
         capture_one(b, shapes, pairs, sp, pd, p);
     }
 }
@@ -548,12 +582,13 @@ void run_pair_pass(const WorldView& w, const uint64_t* pairs, uint32_t npairs, c
     if (npairs == 0) return;
     PairDataDev d = pd.dev();
     check_cuda(cudaMemsetAsync(pd.scalars.p, 0, 8 * sizeof(uint32_t), s), "memset scalars");
+    check_cuda(cudaMemsetAsync(pd.scalars.p + ROUTE_COUNT0, 0, (NP_CONVEX + 1) * sizeof(uint32_t), s), "memset scalars");
     const int TB = 128;
     k_classify<<<(npairs + TB - 1) / TB, TB, 0, s>>>(w.b, w.shapes, pairs, npairs, old_cache.keys.p,
                                                      old_cache.entries.p, old_cache.count_dev, sp, d);
     k_drop_undetectable<<<(npairs + 255) / 256, 256, 0, s>>>(npairs, d);
     uint32_t grid = std::min<uint32_t>((npairs + TB - 1) / TB, 148u * 16u);
-    k_narrow_analytic<<<grid, TB, 0, s>>>(w.b, w.shapes, w.hull, pairs, d);
+    k_narrow_analytic<<<grid, TB, 0, s>>>(w.b, w.shapes, w.hull, pairs, npairs, d);
     uint32_t cgrid = std::min<uint32_t>((npairs + 63) / 64, 148u * 8u);
     k_narrow_convex<<<cgrid, 64, 0, s>>>(w.b, w.shapes, w.hull, pairs, npairs, d, status_dev);
     k_capture<<<grid, TB, 0, s>>>(w.b, w.shapes, pairs, npairs, sp, d);

@@ -33,7 +33,6 @@ namespace bgpu {
 namespace {
 
 constexpr uint32_t NO_COLOUR = 0xffffffffu;
-constexpr int MAX_COLOURS = 128;
 constexpr int MAX_ROUNDS = 1024;
 
 __device__ __forceinline__ uint32_t mix32(uint64_t k) {
@@ -70,7 +69,7 @@ struct ColourArgs {
     unsigned long long* dup;      // 2 words per body: colours seeded twice at the body
     const float4* entries;        // this step's manifold entries (their meta carries last step's colour)
     uint32_t seed;                // 1: start from last step's colours
-    unsigned int* bar;  // [0] barrier counter, [2..4] round counters, [5] colour max
+    unsigned int* bar;  // [0] barrier counter, [5] colour max, [6] [7] uncoloured-list lengths
     uint32_t* status;
 };
 
@@ -86,7 +85,77 @@ __device__ __forceinline__ unsigned long long* colour_word(unsigned long long* m
 // only make those colours unavailable there. Jones-Plassmann: an uncoloured
 // group wins when its priority is the maximum over the uncoloured groups at
 // both of its dynamic bodies; winners take the lowest colour free at both.
-__global__ void k_colour(ColourArgs a) {
+//
+// The rounds walk a list of the still-uncoloured groups (rebuilt by each round
+// from its losers), so a round costs what is left to colour, not the whole
+// set; once the list fits one block, that block finishes the rounds alone with
+// block-local syncs and the rest of the grid exits. Which groups win in a
+// round depends only on the priorities, so the colours do not depend on the
+// list order or on which threads run the rounds.
+struct JpList {
+    uint32_t* items[2];
+    unsigned int* len[2];
+};
+
+// Appends k to a list: one atomicAdd per group of lanes that append together.
+__device__ __forceinline__ void list_append(uint32_t* items, unsigned int* len, uint32_t k) {
+    cooperative_groups::coalesced_group g = cooperative_groups::coalesced_threads();
+    unsigned int base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(len, g.size());
+    base = g.shfl(base, 0);
+    items[base + g.thread_rank()] = k;
+}
+
+// One Jones-Plassmann round over list r & 1; losers go to list (r + 1) & 1.
+// [lo, n) with step `step` is this thread's share of the list.
+__device__ __forceinline__ void jp_clear(const ColourArgs& a, const uint32_t* list, uint32_t n, uint32_t lo, uint32_t step) {
+    for (uint32_t i = lo; i < n; i += step) {
+        const uint64_t key = a.pairs[a.contact_pairs[list[i]]];
+        a.prio[key_lo(key)] = 0ull;
+        a.prio[key_hi(key)] = 0ull;
+    }
+}
+
+__device__ __forceinline__ void jp_bid(const ColourArgs& a, const uint32_t* list, uint32_t n, uint32_t lo, uint32_t step) {
+    for (uint32_t i = lo; i < n; i += step) {
+        const uint32_t k = list[i];
+        const uint64_t key = a.pairs[a.contact_pairs[k]];
+        const uint32_t u = key_lo(key), v = key_hi(key);
+        const unsigned long long pr = (uint64_t(mix32(key)) << 32) | k;
+        if (inv_mass_of(a.iw, u) > 0.0f) atomicMax(&a.prio[u], pr);
+        if (inv_mass_of(a.iw, v) > 0.0f) atomicMax(&a.prio[v], pr);
+    }
+}
+
+__device__ __forceinline__ void jp_pick(const ColourArgs& a, const uint32_t* list, uint32_t n, uint32_t lo, uint32_t step,
+                                        uint32_t* losers, unsigned int* nlosers) {
+    for (uint32_t i = lo; i < n; i += step) {
+        const uint32_t k = list[i];
+        const uint64_t key = a.pairs[a.contact_pairs[k]];
+        const uint32_t u = key_lo(key), v = key_hi(key);
+        const unsigned long long pr = (uint64_t(mix32(key)) << 32) | k;
+        const bool du = inv_mass_of(a.iw, u) > 0.0f, dv = inv_mass_of(a.iw, v) > 0.0f;
+        const bool win = (!du || __ldcg(&a.prio[u]) == pr) && (!dv || __ldcg(&a.prio[v]) == pr);
+        if (!win) {
+            list_append(losers, nlosers, k);
+            continue;
+        }
+        unsigned long long m0 = 0, m1 = 0;
+        if (du) { m0 |= __ldcg(&a.mask[2 * u]); m1 |= __ldcg(&a.mask[2 * u + 1]); }
+        if (dv) { m0 |= __ldcg(&a.mask[2 * v]); m1 |= __ldcg(&a.mask[2 * v + 1]); }
+        uint32_t c;
+        if (~m0) c = uint32_t(__ffsll((long long)~m0) - 1);
+        else if (~m1) c = 64u + uint32_t(__ffsll((long long)~m1) - 1);
+        else { c = MAX_COLOURS - 1; atomicOr(a.status, ST_COLOUR_OVERFLOW); }
+        a.colour[k] = c;
+        const unsigned long long b0 = c < 64 ? (1ull << c) : 0ull, b1 = c >= 64 ? (1ull << (c - 64)) : 0ull;
+        if (du) { a.mask[2 * u] |= b0; a.mask[2 * u + 1] |= b1; }
+        if (dv) { a.mask[2 * v] |= b0; a.mask[2 * v + 1] |= b1; }
+        atomicMax(&a.bar[5], c + 1);
+    }
+}
+
+__global__ void k_colour(ColourArgs a, JpList wl) {
     const uint32_t K = *a.count;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -101,9 +170,15 @@ __global__ void k_colour(ColourArgs a) {
         if (a.seed) {
             a.dup[2 * u] = 0ull; a.dup[2 * u + 1] = 0ull;
             a.dup[2 * v] = 0ull; a.dup[2 * v + 1] = 0ull;
+        } else {
+            wl.items[0][k] = k;  // every group starts uncoloured
         }
     }
-    if (tid == 0) { a.bar[2] = 0; a.bar[3] = 0; a.bar[4] = 0; a.bar[5] = 0; }
+    if (tid == 0) {
+        a.bar[5] = 0;
+        *wl.len[0] = a.seed ? 0u : K;
+        *wl.len[1] = 0u;
+    }
     team_barrier(a.bar, ++nbar * nblocks, a.status);
     if (a.seed) {
         for (uint32_t k = tid; k < K; k += stride) {  // claim last step's colour at both bodies
@@ -123,72 +198,56 @@ __global__ void k_colour(ColourArgs a) {
         for (uint32_t k = tid; k < K; k += stride) {  // keep the seeds claimed once at each body
             const uint32_t p = a.contact_pairs[k];
             const uint32_t cs = (__float_as_uint(a.entries[size_t(p) * ENTRY_F4 + 2].w) >> META_COLOUR_SHIFT) & 0xffu;
-            if (cs == 0u || cs > MAX_COLOURS) continue;
-            const uint32_t c = cs - 1u;
-            const unsigned long long bit = 1ull << (c & 63u);
-            const uint64_t key = a.pairs[p];
-            const uint32_t u = key_lo(key), v = key_hi(key);
-            const bool du = inv_mass_of(a.iw, u) > 0.0f && (__ldcg(colour_word(a.dup, u, c)) & bit);
-            const bool dv = inv_mass_of(a.iw, v) > 0.0f && (__ldcg(colour_word(a.dup, v, c)) & bit);
-            if (!du && !dv) {
+            bool keep = false;
+            uint32_t c = 0;
+            if (cs != 0u && cs <= MAX_COLOURS) {
+                c = cs - 1u;
+                const unsigned long long bit = 1ull << (c & 63u);
+                const uint64_t key = a.pairs[p];
+                const uint32_t u = key_lo(key), v = key_hi(key);
+                const bool du = inv_mass_of(a.iw, u) > 0.0f && (__ldcg(colour_word(a.dup, u, c)) & bit);
+                const bool dv = inv_mass_of(a.iw, v) > 0.0f && (__ldcg(colour_word(a.dup, v, c)) & bit);
+                keep = !du && !dv;
+            }
+            if (keep) {
                 a.colour[k] = c;
                 atomicMax(&a.bar[5], c + 1u);
+            } else {
+                list_append(wl.items[0], wl.len[0], k);
             }
         }
         team_barrier(a.bar, ++nbar * nblocks, a.status);
     }
+    // Rounds on the whole grid while the list is longer than one block.
     int round = 0;
     for (; round < MAX_ROUNDS; ++round) {
-        // phase 0: clear the bids of the uncoloured groups' bodies
-        for (uint32_t k = tid; k < K; k += stride) {
-            if (a.colour[k] != NO_COLOUR) continue;
-            uint64_t key = a.pairs[a.contact_pairs[k]];
-            a.prio[key_lo(key)] = 0ull;
-            a.prio[key_hi(key)] = 0ull;
-        }
+        const uint32_t cur = uint32_t(round) & 1u, nxt = cur ^ 1u;
+        const uint32_t n = *(volatile unsigned int*)wl.len[cur];
+        if (n <= blockDim.x) break;
+        jp_clear(a, wl.items[cur], n, tid, stride);
+        if (tid == 0) *wl.len[nxt] = 0u;  // last read (as this list's length) before the previous barrier
         team_barrier(a.bar, ++nbar * nblocks, a.status);
-        // phase 1: bid (and recycle the counter of round r-1)
-        if (tid == 0) a.bar[2 + (round + 2) % 3] = 0;
-        for (uint32_t k = tid; k < K; k += stride) {
-            if (__ldcg(&a.colour[k]) != NO_COLOUR) continue;
-            uint64_t key = a.pairs[a.contact_pairs[k]];
-            uint32_t u = key_lo(key), v = key_hi(key);
-            unsigned long long pr = (uint64_t(mix32(key)) << 32) | k;
-            if (inv_mass_of(a.iw, u) > 0.0f) atomicMax(&a.prio[u], pr);
-            if (inv_mass_of(a.iw, v) > 0.0f) atomicMax(&a.prio[v], pr);
-        }
+        jp_bid(a, wl.items[cur], n, tid, stride);
         team_barrier(a.bar, ++nbar * nblocks, a.status);
-        // phase 2: winners pick a colour
-        for (uint32_t k = tid; k < K; k += stride) {
-            if (__ldcg(&a.colour[k]) != NO_COLOUR) continue;
-            uint64_t key = a.pairs[a.contact_pairs[k]];
-            uint32_t u = key_lo(key), v = key_hi(key);
-            unsigned long long pr = (uint64_t(mix32(key)) << 32) | k;
-            bool du = inv_mass_of(a.iw, u) > 0.0f, dv = inv_mass_of(a.iw, v) > 0.0f;
-            bool win = (!du || __ldcg(&a.prio[u]) == pr) && (!dv || __ldcg(&a.prio[v]) == pr);
-            if (!win) {
-                atomicAdd(&a.bar[2 + round % 3], 1u);
-                continue;
-            }
-            unsigned long long m0 = 0, m1 = 0;
-            if (du) { m0 |= __ldcg(&a.mask[2 * u]); m1 |= __ldcg(&a.mask[2 * u + 1]); }
-            if (dv) { m0 |= __ldcg(&a.mask[2 * v]); m1 |= __ldcg(&a.mask[2 * v + 1]); }
-            uint32_t c;
-            if (~m0) c = uint32_t(__ffsll((long long)~m0) - 1);
-            else if (~m1) c = 64u + uint32_t(__ffsll((long long)~m1) - 1);
-            else { c = MAX_COLOURS - 1; atomicOr(a.status, ST_COLOUR_OVERFLOW); }
-            a.colour[k] = c;
-            unsigned long long b0 = c < 64 ? (1ull << c) : 0ull, b1 = c >= 64 ? (1ull << (c - 64)) : 0ull;
-            if (du) { a.mask[2 * u] |= b0; a.mask[2 * u + 1] |= b1; }
-            if (dv) { a.mask[2 * v] |= b0; a.mask[2 * v + 1] |= b1; }
-            atomicMax(&a.bar[5], c + 1);
-        }
+        jp_pick(a, wl.items[cur], n, tid, stride, wl.items[nxt], wl.len[nxt]);
         team_barrier(a.bar, ++nbar * nblocks, a.status);
-        volatile unsigned int* vb = a.bar;
-        if (vb[2 + round % 3] == 0) break;
-        if (*(volatile uint32_t*)a.status & ST_BARRIER_TIMEOUT) break;
+        if (*(volatile uint32_t*)a.status & ST_BARRIER_TIMEOUT) return;
     }
-    if (round >= MAX_ROUNDS && tid == 0) atomicOr(a.status, ST_COLOUR_ROUNDS);
+    // The short tail: block 0 alone, one group per thread.
+    if (blockIdx.x != 0) return;
+    for (; round < MAX_ROUNDS; ++round) {
+        const uint32_t cur = uint32_t(round) & 1u, nxt = cur ^ 1u;
+        const uint32_t n = *(volatile unsigned int*)wl.len[cur];
+        if (n == 0) break;
+        jp_clear(a, wl.items[cur], n, threadIdx.x, blockDim.x);
+        if (threadIdx.x == 0) *wl.len[nxt] = 0u;
+        __syncthreads();
+        jp_bid(a, wl.items[cur], n, threadIdx.x, blockDim.x);
+        __syncthreads();
+        jp_pick(a, wl.items[cur], n, threadIdx.x, blockDim.x, wl.items[nxt], wl.len[nxt]);
+        __syncthreads();
+    }
+    if (round >= MAX_ROUNDS && threadIdx.x == 0) atomicOr(a.status, ST_COLOUR_ROUNDS);
 }
 
 // Colour histograms of all groups and of the groups with split-active rows,
@@ -342,6 +401,8 @@ enum Kind { WARM = 0, ITER = 1, SPLIT = 2 };
 
 __device__ __forceinline__ float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
 
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // warm_start (sequential_impulse.rs:710-717) for group slot t, which also
 // fills the slot's velocity table with the prepared terms the sweeps use
 // (sequential_impulse.rs:352-520 computes the same values in prepare()).
@@ -388,7 +449,6 @@ __device__ __forceinline__ void warm_group(const SolveArgs& a, uint32_t t, uint3
     }
 }
 
-__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
 
 // One solve_contact sweep (sequential_impulse.rs:804-930) over group slot t;
@@ -541,18 +601,20 @@ __device__ __forceinline__ void run_group(const SolveArgs& a, uint32_t t, uint4 
     if (appb) { __stcg(&plin[ib], to4(lb, 0.0f)); __stcg(&pang[ib], to4(wb, 0.0f)); }
 }
 
-// Bring all of a slot's table entries into L1 (the next phase's group, while the
-// team waits at the barrier: a phase's entries, ~1.5 contacts x 240 B per slot,
-// fit in L1 next to nothing else the solve keeps there).
+// Bring all of a slot's table entries into L2 (the next phase's group, while the
+// team waits at the barrier): the tables of a large pile outgrow L2, so without
+// this the first loads after the barrier would wait for DRAM. (Into L1 instead
+// measured the same: the barrier's acquire drops L1. Asking for a group's later
+// contacts into L1 at the start of its solve measured slower.)
 template <bool VELOCITY>
-__device__ __forceinline__ void prefetch_slot_l1(const SolveArgs& a, uint32_t t, uint32_t cnt) {
+__device__ __forceinline__ void prefetch_slot_l2(const SolveArgs& a, uint32_t t, uint32_t cnt) {
     for (uint32_t k = 0; k < cnt; ++k) {
         if (VELOCITY) {
             const float4* e = a.vtab + tix<VT_PLANES>(0, k, t);
-            for (uint32_t pl = 0; pl < VT_PLANES; ++pl) prefetch_l1(e + pl * PLANE_STRIDE);
+            for (uint32_t pl = 0; pl < VT_PLANES; ++pl) prefetch_l2(e + pl * PLANE_STRIDE);
         } else {
             const float4* e = a.stab + tix<ST_PLANES>(0, k, t);
-            for (uint32_t pl = 0; pl < ST_PLANES; ++pl) prefetch_l1(e + pl * PLANE_STRIDE);
+            for (uint32_t pl = 0; pl < ST_PLANES; ++pl) prefetch_l2(e + pl * PLANE_STRIDE);
         }
     }
 }
@@ -568,13 +630,25 @@ __device__ __forceinline__ void run_item(const SolveArgs& a, uint32_t sweep, uin
 // The team's threads deal the batch slots of each phase among themselves and
 // meet at the team barrier between phases; each thread reads its next slot
 // record while it solves the current one.
+//
+// A colour with at most one block's worth of groups (the tail colours of a
+// pile, or every colour of a small scene) is solved by the team's first block
+// alone, one group per thread. Between two such colours the block syncs
+// locally instead of the team meeting at a barrier: the other blocks go on to
+// the next barrier and wait there.
 template <bool VELOCITY>
 __device__ __forceinline__ void run_phases(const SolveArgs& a, const uint4* __restrict__ recs, const uint32_t* soff,
                                            const uint32_t* send, uint32_t ncol, uint32_t nphases, uint32_t last, uint32_t tid,
-                                           uint32_t stride, unsigned int* ctr, uint32_t team_blocks, uint32_t& nbar) {
+                                           uint32_t stride, unsigned int* ctr, uint32_t team_blocks, uint32_t team_block,
+                                           uint32_t& nbar) {
     if (ncol == 0 || nphases == 0) return;
+    auto small = [&](uint32_t c) { return send[c] - soff[c] <= blockDim.x; };
+    auto first_slot = [&](uint32_t c) -> uint32_t {
+        if (!small(c)) return soff[c] + tid;
+        return team_block == 0 ? soff[c] + threadIdx.x : send[c];
+    };
     auto first_rec = [&](uint32_t c) -> uint4 {
-        const uint32_t t = soff[c] + tid;
+        const uint32_t t = first_slot(c);
         return t < send[c] ? __ldg(&recs[t]) : make_uint4(0u, 0u, 0u, 0u);
     };
     uint4 rec = first_rec(0);  // rec.z == 0 (no rows): no slot for this thread
@@ -582,14 +656,20 @@ __device__ __forceinline__ void run_phases(const SolveArgs& a, const uint4* __re
         const uint32_t c = q % ncol, sweep = q / ncol;
         const uint4 next = q + 1 < nphases ? first_rec((q + 1) % ncol) : make_uint4(0u, 0u, 0u, 0u);
         if (rec.z) {
-            run_item<VELOCITY>(a, sweep, last, soff[c] + tid, rec);
-            for (uint32_t t = soff[c] + tid + stride; t < send[c]; t += stride)
-                run_item<VELOCITY>(a, sweep, last, t, __ldg(&recs[t]));
+            const uint32_t t0 = first_slot(c);
+            run_item<VELOCITY>(a, sweep, last, t0, rec);
+            if (!small(c))
+                for (uint32_t t = t0 + stride; t < send[c]; t += stride) run_item<VELOCITY>(a, sweep, last, t, __ldg(&recs[t]));
         }
         rec = next;
         if (q + 1 < nphases) {
-            // The next phase's table entries (written in sweep 0) head for L1 while the team waits.
-            if (rec.z && (q + 1) >= ncol) prefetch_slot_l1<VELOCITY>(a, soff[(q + 1) % ncol] + tid, rec.z >> 29);
+            const uint32_t cn = (q + 1) % ncol;
+            if (small(c) && small(cn)) {
+                __syncthreads();  // global writes of the block are visible to the block after it
+                continue;
+            }
+            // The next phase's table entries (written in sweep 0) head for L2 while the team waits.
+            if (rec.z && (q + 1) >= ncol) prefetch_slot_l2<VELOCITY>(a, first_slot(cn), rec.z >> 29);
             team_barrier(ctr, ++nbar * team_blocks, a.status);
         }
     }
@@ -625,14 +705,15 @@ __global__ void __launch_bounds__(256, 2) k_solve(SolveArgs a) {
     uint32_t nbar = 0;
     if (split_team) {
         run_phases<false>(a, a.split_rec, s_split_off, s_split_end, ncol, iters * ncol, iters - 1u, tid, stride, a.bar + 1,
-                          team_blocks, nbar);
+                          team_blocks, team_block, nbar);
         return;
     }
-    run_phases<true>(a, a.batch_rec, s_off, s_end, ncol, (iters + 1) * ncol, iters, tid, stride, a.bar, team_blocks, nbar);
+    run_phases<true>(a, a.batch_rec, s_off, s_end, ncol, (iters + 1) * ncol, iters, tid, stride, a.bar, team_blocks,
+                     team_block, nbar);
     if (nsplit && iters && split_blocks == 0) {
         team_barrier(a.bar, ++nbar * team_blocks, a.status);
         run_phases<false>(a, a.split_rec, s_split_off, s_split_end, ncol, iters * ncol, iters - 1u, tid, stride, a.bar, team_blocks,
-                          nbar);
+                          team_block, nbar);
     }
 }
 
@@ -758,7 +839,9 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
                   pd.body_dup.p, pd.entries.p, seed_colours ? 1u : 0u, pd.barrier.p, status_dev};
     static int colour_grid = 0;
     if (!colour_grid) colour_grid = coop_grid((const void*)k_colour, TB, 0);
-    void* cargs[] = {&ca};
+    pd.colour_work.reserve(2 * size_t(npairs) + 2);
+    JpList wl{{pd.colour_work.p, pd.colour_work.p + npairs}, {pd.barrier.p + 6, pd.barrier.p + 7}};
+    void* cargs[] = {&ca, &wl};
     check_cuda(cudaLaunchCooperativeKernel((const void*)k_colour, dim3(colour_grid), dim3(TB), cargs, 0, s),
                "colour launch");
     // Batches.

@@ -1314,6 +1314,38 @@ bgpu_status bgpu_read_solve_order(bgpu_world* w, uint64_t* out, uint64_t cap, ui
     });
 }
 
+bgpu_status bgpu_read_colour_batches(bgpu_world* w, uint32_t* groups, uint32_t* split_groups, uint32_t cap,
+                                     uint32_t* out_n) {
+    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        W.finish_stats();
+        bgpu::PairData& pd = W.pd;
+        cudaStream_t s = W.stream;
+        uint32_t ncol = 0;
+        if (W.npairs && pd.scalars.p && pd.colour_offset.p) {
+            uint32_t sc[16];
+            bgpu::check_cuda(cudaMemcpyAsync(sc, pd.scalars.p, sizeof(sc), cudaMemcpyDeviceToHost, s), "d2h");
+            bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+            ncol = std::min<uint32_t>(sc[4], uint32_t(bgpu::MAX_COLOURS));
+        }
+        if (out_n) *out_n = ncol;
+        const uint32_t k = std::min(cap, ncol);
+        if (!k) return BGPU_OK;
+        std::vector<uint32_t> off(k), end(k), soff(k), send(k);
+        bgpu::check_cuda(cudaMemcpyAsync(off.data(), pd.colour_offset.p, k * 4, cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaMemcpyAsync(end.data(), pd.colour_cursor.p, k * 4, cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaMemcpyAsync(soff.data(), pd.split_offset.p, k * 4, cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaMemcpyAsync(send.data(), pd.split_cursor.p, k * 4, cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+        for (uint32_t c = 0; c < k; ++c) {
+            if (groups) groups[c] = end[c] - off[c];
+            if (split_groups) split_groups[c] = send[c] - soff[c];
+        }
+        return BGPU_OK;
+    });
+}
+
 bgpu_status bgpu_get_stats(bgpu_world* w, bgpu_step_stats* out) {
     if (!w || !out) return BGPU_ERR_INVALID_ARGUMENT;
     return guarded([&]() -> bgpu_status {

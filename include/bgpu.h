@@ -222,6 +222,12 @@ bgpu_status bgpu_apply_forces(bgpu_world* w, const float* force, const float* to
 bgpu_status bgpu_read_pairs(bgpu_world* w, uint32_t* pairs, uint64_t cap, uint64_t* out_n);
 bgpu_status bgpu_read_contacts(bgpu_world* w, float* rows, uint64_t cap, uint64_t* out_n);
 bgpu_status bgpu_read_solve_order(bgpu_world* w, uint64_t* keys, uint64_t cap, uint64_t* out_n);
+/* PGS batches of the last step, one entry per colour in solve order: contact pairs
+ * (row groups) in the batch, and those of them with split-impulse rows. Each solver
+ * iteration runs one phase per colour, so these sizes set how the work spreads over
+ * the device. Either array may be NULL; out_n receives the colour count. */
+bgpu_status bgpu_read_colour_batches(bgpu_world* w, uint32_t* groups, uint32_t* split_groups, uint32_t cap,
+                                     uint32_t* out_n);
 bgpu_status bgpu_get_stats(bgpu_world* w, bgpu_step_stats* out);
 /* Turns per-stage timing on (resetting the sums) or off. */
 bgpu_status bgpu_enable_step_timing(bgpu_world* w, int on);

@@ -318,3 +318,59 @@ def test_world_mixed_convex_pile_matches_oracle(gpu):
             assert err <= 1e-3, f"step {step}: {err}"
             _pairs_equal(w.pairs(), o.pairs())
     assert convex_pairs > 0
+
+
+def test_world_sleeping_chain_wakes_like_the_oracle(gpu):
+    """Islands: a chain of touching boxes settles and falls asleep as one island, a lone box
+    sleeps on its own, and a box dropped onto the chain's end (landing after the chain slept)
+    wakes the whole chain but not the lone box. Activation states equal the oracle's at every
+    step; the rest of the state within 1e-3."""
+    import bgpu
+    import scenes
+
+    s = scenes.Scene("sleeping_chain", 1 / 120, 10, 420)
+    p = s.add_shape(scenes.PLANE, [0, 1, 0, 0])
+    b = s.add_shape(scenes.BOX, [0.5, 0.5, 0.5])
+    s.add(p, (0, 0, 0), mass=0.0)
+    chain = list(range(1, 6))
+    for k in range(5):
+        s.add(b, (1.0 * k, 0.5, 0.0))
+    lone = 6
+    s.add(b, (10.0, 0.5, 0.0))
+    drop = 7
+    s.add(b, (4.0, 40.0, 0.0))
+    w = s.build_gpu(bgpu)
+    o = s.build_oracle(orc)
+    history = []
+    for step in range(s.steps):
+        w.step(s.dt)
+        o.set_solve_order(w.solve_order())
+        o.step(s.dt)
+        assert w.stats()["device_status"] == 0
+        g, r = w.state(), o.state()
+        np.testing.assert_array_equal(g[:, 13], r[:, 13], err_msg=f"step {step}")
+        err = float(np.abs(g[:, :13] - r[:, :13]).max())
+        assert err <= 1e-3, f"step {step}: max abs state error {err}"
+        history.append(g[:, 13].copy())
+    h = np.array(history)
+    asleep = h[:, chain] == 2
+    slept = np.flatnonzero(asleep.all(axis=1))
+    assert len(slept) > 0, "the chain never slept"
+    assert not asleep[-1].any(), "the dropped box did not wake the chain"
+    assert h[-1, lone] == 2 and h[slept[0]:, lone].min() == 2
+    assert h[slept[0], drop] != 2  # still falling while the chain slept
+
+
+def test_colour_batches_cover_every_row_group(gpu):
+    import bgpu
+    import scenes
+
+    s = scenes.falling_box_stack(4, 4, 4, seed=6, steps=40)
+    w = s.build_gpu(bgpu)
+    w.step(s.dt, 40)
+    st = w.stats()
+    groups, split = w.colour_batches()
+    assert len(groups) == st["num_colours"] > 0
+    assert int(groups.sum()) == st["num_contact_pairs"]
+    assert int(split.sum()) == st["num_split_pairs"]
+    assert np.all(groups > 0) and np.all(split <= groups)
