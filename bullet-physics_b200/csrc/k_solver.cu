@@ -127,8 +127,21 @@ __device__ __forceinline__ void jp_bid(const ColourArgs& a, const uint32_t* list
     }
 }
 
+// The colour count (bar[5]) is raised once per block: each warp folds its lanes'
+// colours into the block's shared maximum, which colour_max_flush publishes.
+__device__ __forceinline__ void warp_colour_max(unsigned int* s_cmax, uint32_t top) {
+    top = __reduce_max_sync(0xffffffffu, top);
+    if ((threadIdx.x & 31u) == 0 && top) atomicMax(s_cmax, top);
+}
+
+__device__ __forceinline__ void colour_max_flush(const unsigned int* s_cmax, unsigned int* bar5) {
+    __syncthreads();
+    if (threadIdx.x == 0 && *s_cmax) atomicMax(bar5, *s_cmax);
+}
+
 __device__ __forceinline__ void jp_pick(const ColourArgs& a, const uint32_t* list, uint32_t n, uint32_t lo, uint32_t step,
-                                        uint32_t* losers, unsigned int* nlosers) {
+                                        uint32_t* losers, unsigned int* nlosers, unsigned int* s_cmax) {
+    uint32_t top = 0;
     for (uint32_t i = lo; i < n; i += step) {
         const uint32_t k = list[i];
         const uint64_t key = a.pairs[a.contact_pairs[k]];
@@ -151,8 +164,9 @@ __device__ __forceinline__ void jp_pick(const ColourArgs& a, const uint32_t* lis
         const unsigned long long b0 = c < 64 ? (1ull << c) : 0ull, b1 = c >= 64 ? (1ull << (c - 64)) : 0ull;
         if (du) { a.mask[2 * u] |= b0; a.mask[2 * u + 1] |= b1; }
         if (dv) { a.mask[2 * v] |= b0; a.mask[2 * v + 1] |= b1; }
-        atomicMax(&a.bar[5], c + 1);
+        top = max(top, c + 1u);
     }
+    warp_colour_max(s_cmax, top);
 }
 
 __global__ void k_colour(ColourArgs a, JpList wl) {
@@ -161,6 +175,8 @@ __global__ void k_colour(ColourArgs a, JpList wl) {
     const uint32_t stride = gridDim.x * blockDim.x;
     const unsigned int nblocks = gridDim.x;
     unsigned int nbar = 0;
+    __shared__ unsigned int s_cmax;
+    if (threadIdx.x == 0) s_cmax = 0u;
     for (uint32_t k = tid; k < K; k += stride) {
         a.colour[k] = NO_COLOUR;
         uint64_t key = a.pairs[a.contact_pairs[k]];
@@ -195,6 +211,7 @@ __global__ void k_colour(ColourArgs a, JpList wl) {
                 atomicOr(colour_word(a.dup, v, c), bit);
         }
         team_barrier(a.bar, ++nbar * nblocks, a.status);
+        uint32_t top = 0;
         for (uint32_t k = tid; k < K; k += stride) {  // keep the seeds claimed once at each body
             const uint32_t p = a.contact_pairs[k];
             const uint32_t cs = (__float_as_uint(a.entries[size_t(p) * ENTRY_F4 + 2].w) >> META_COLOUR_SHIFT) & 0xffu;
@@ -211,42 +228,56 @@ __global__ void k_colour(ColourArgs a, JpList wl) {
             }
             if (keep) {
                 a.colour[k] = c;
-                atomicMax(&a.bar[5], c + 1u);
+                top = max(top, c + 1u);
             } else {
                 list_append(wl.items[0], wl.len[0], k);
             }
         }
+        warp_colour_max(&s_cmax, top);
+        colour_max_flush(&s_cmax, &a.bar[5]);
         team_barrier(a.bar, ++nbar * nblocks, a.status);
     }
-    // Rounds on the whole grid while the list is longer than one block.
+    // Rounds on the whole grid while the list is longer than one block. The list
+    // length is read once per block, so every thread of a block takes the same path
+    // (even after a barrier timeout, when lengths may still be changing).
+    __shared__ unsigned int s_len;
+    auto list_len = [&](uint32_t which) -> uint32_t {
+        if (threadIdx.x == 0) s_len = *(volatile unsigned int*)wl.len[which];
+        __syncthreads();
+        const uint32_t v = s_len;
+        __syncthreads();
+        return v;
+    };
     int round = 0;
     for (; round < MAX_ROUNDS; ++round) {
         const uint32_t cur = uint32_t(round) & 1u, nxt = cur ^ 1u;
-        const uint32_t n = *(volatile unsigned int*)wl.len[cur];
+        const uint32_t n = list_len(cur);
         if (n <= blockDim.x) break;
         jp_clear(a, wl.items[cur], n, tid, stride);
         if (tid == 0) *wl.len[nxt] = 0u;  // last read (as this list's length) before the previous barrier
         team_barrier(a.bar, ++nbar * nblocks, a.status);
         jp_bid(a, wl.items[cur], n, tid, stride);
         team_barrier(a.bar, ++nbar * nblocks, a.status);
-        jp_pick(a, wl.items[cur], n, tid, stride, wl.items[nxt], wl.len[nxt]);
+        jp_pick(a, wl.items[cur], n, tid, stride, wl.items[nxt], wl.len[nxt], &s_cmax);
+        colour_max_flush(&s_cmax, &a.bar[5]);
         team_barrier(a.bar, ++nbar * nblocks, a.status);
-        if (*(volatile uint32_t*)a.status & ST_BARRIER_TIMEOUT) return;
+        if (__syncthreads_or((*(volatile uint32_t*)a.status & ST_BARRIER_TIMEOUT) != 0u)) return;
     }
     // The short tail: block 0 alone, one group per thread.
     if (blockIdx.x != 0) return;
     for (; round < MAX_ROUNDS; ++round) {
         const uint32_t cur = uint32_t(round) & 1u, nxt = cur ^ 1u;
-        const uint32_t n = *(volatile unsigned int*)wl.len[cur];
+        const uint32_t n = list_len(cur);
         if (n == 0) break;
         jp_clear(a, wl.items[cur], n, threadIdx.x, blockDim.x);
         if (threadIdx.x == 0) *wl.len[nxt] = 0u;
         __syncthreads();
         jp_bid(a, wl.items[cur], n, threadIdx.x, blockDim.x);
         __syncthreads();
-        jp_pick(a, wl.items[cur], n, threadIdx.x, blockDim.x, wl.items[nxt], wl.len[nxt]);
+        jp_pick(a, wl.items[cur], n, threadIdx.x, blockDim.x, wl.items[nxt], wl.len[nxt], &s_cmax);
         __syncthreads();
     }
+    colour_max_flush(&s_cmax, &a.bar[5]);
     if (round >= MAX_ROUNDS && threadIdx.x == 0) atomicOr(a.status, ST_COLOUR_ROUNDS);
 }
 
