@@ -92,6 +92,7 @@ def lib():
             "bgpu_read_contacts": (S, [P, F, ctypes.c_uint64, U64P]),
             "bgpu_read_solve_order": (S, [P, U64P, ctypes.c_uint64, U64P]),
             "bgpu_read_colour_batches": (S, [P, U32P, U32P, U32, U32P]),
+            "bgpu_selftest_wait_timeout": (S, [U32, U32P, F]),
             "bgpu_get_stats": (S, [P, ctypes.POINTER(StepStats)]),
             "bgpu_enable_step_timing": (S, [P, ctypes.c_int]),
             "bgpu_broadphase_pairs": (S, [F, U32, U32P, ctypes.c_uint64, U64P]),
@@ -151,6 +152,14 @@ def f32(a):
 
 def device_count():
     return lib().bgpu_device_count()
+
+
+def selftest_wait_timeout(limit_ms):
+    """Runs a device wait that nothing completes; returns (device status bits, device ms)."""
+    st = ctypes.c_uint32()
+    ms = ctypes.c_float()
+    check(lib().bgpu_selftest_wait_timeout(int(limit_ms), ctypes.byref(st), ctypes.byref(ms)), "selftest_wait_timeout")
+    return st.value, ms.value
 
 
 def solver_info(**kw):

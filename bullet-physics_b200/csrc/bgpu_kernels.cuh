@@ -69,26 +69,44 @@ struct DevBuf {
 
 // ---------------------------------------------------------------- device helpers shared by the solver and its adjoint
 constexpr unsigned int BARRIER_SPIN_LIMIT = 1u << 26;
+constexpr unsigned long long BARRIER_TIMEOUT_NS = 2000000000ull;  // 2 s: phases take microseconds
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 // Barrier of a team of co-resident blocks (a cooperative launch) on a counter
 // that only grows during the launch: the k-th barrier (k from 1) of a team of
 // n blocks completes when the counter reaches k * n. One atomic per block,
-// then a tight spin. The spin is bounded: on timeout the status word records
-// it and every later barrier returns at once, so no launch can hang the device.
+// then a tight spin. The spin is bounded in time (limit_ns, measured from the
+// 64th poll on the global timer, with a poll count as a second bound): when it
+// gives up the status word records ST_BARRIER_TIMEOUT, and every block's spin
+// also gives up within 64 polls once the word shows it, so no launch can hang
+// the device and the host reads the error. The status word is not read before
+// the arrival: that read would put an L2 round trip in front of every barrier.
 // (Spinning on relaxed loads with one acquire fence at the end measured slower.)
-__device__ __forceinline__ void team_barrier(unsigned int* ctr, unsigned int target, uint32_t* status) {
+__device__ __forceinline__ void team_barrier(unsigned int* ctr, unsigned int target, uint32_t* status,
+                                             unsigned long long limit_ns = BARRIER_TIMEOUT_NS) {
     __syncthreads();
-    if (threadIdx.x == 0 && !(*(volatile uint32_t*)status & ST_BARRIER_TIMEOUT)) {
+    if (threadIdx.x == 0) {
         // The release add publishes the block's writes (ordered before it by the
         // bar.sync above); the acquire load makes the other blocks' writes visible.
         asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(ctr) : "memory");
         unsigned int v, spins = 0;
+        unsigned long long t0 = 0;
         for (;;) {
             asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(ctr) : "memory");
             if (v >= target) break;
-            if (++spins > BARRIER_SPIN_LIMIT) {
-                atomicOr(status, ST_BARRIER_TIMEOUT);
-                break;
+            if ((++spins & 63u) == 0u) {
+                const unsigned long long now = globaltimer_ns();
+                if (t0 == 0) t0 = now;
+                if ((*(volatile uint32_t*)status & ST_BARRIER_TIMEOUT) || now - t0 > limit_ns ||
+                    spins > BARRIER_SPIN_LIMIT) {
+                    atomicOr(status, ST_BARRIER_TIMEOUT);
+                    break;
+                }
             }
         }
     }
@@ -317,6 +335,9 @@ void launch_compute_iw(const BodyDev& b, uint32_t n, cudaStream_t s);
 // seed_colours: start the colouring from the colours the pairs' manifolds carry from last step.
 void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
                 uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark, bool seed_colours);
+// One team barrier that nothing completes (2 blocks): the wait gives up after limit_ns and
+// leaves ST_BARRIER_TIMEOUT in *status. ctr and status are device words the caller zeroes.
+void run_wait_selftest(unsigned long long limit_ns, unsigned int* ctr, uint32_t* status, cudaStream_t s);
 // Impulse writeback, then compaction of the surviving manifolds into `next`.
 // simulate / prev_simulate hold one flag per world, indexed through world_of (null: one world).
 void run_cache_update(const uint64_t* pairs, uint32_t npairs, const Manifolds& old_cache, PairData& pd,

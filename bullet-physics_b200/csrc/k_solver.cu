@@ -829,6 +829,11 @@ __global__ void k_merge(const uint64_t* __restrict__ pairs, const float4* __rest
     }
 }
 
+// A barrier whose target counts one block more than the grid has: nothing completes it.
+__global__ void k_wait_selftest(unsigned int* ctr, uint32_t* status, unsigned long long limit_ns) {
+    team_barrier(ctr, gridDim.x + 1u, status, limit_ns);
+}
+
 int coop_grid(const void* fn, int block, size_t smem) {
     static int sms = -1;
     if (sms < 0) {
@@ -843,6 +848,10 @@ int coop_grid(const void* fn, int block, size_t smem) {
 }
 
 }  // namespace
+
+void run_wait_selftest(unsigned long long limit_ns, unsigned int* ctr, uint32_t* status, cudaStream_t s) {
+    k_wait_selftest<<<2, 32, 0, s>>>(ctr, status, limit_ns);
+}
 
 void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
                 uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark, bool seed_colours) {

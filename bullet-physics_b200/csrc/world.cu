@@ -827,6 +827,38 @@ extern "C" {
 
 const char* bgpu_version(void) { return "bgpu 0.1 (sm_100a)"; }
 
+bgpu_status bgpu_selftest_wait_timeout(uint32_t limit_ms, uint32_t* device_status, float* waited_ms) {
+    if (limit_ms < 1 || limit_ms > 2000) {
+        bgpu::g_last_error = "bgpu_selftest_wait_timeout: limit_ms must lie in 1..2000";
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&]() -> bgpu_status {
+        bgpu::DevBuf<uint32_t> words;
+        words.reserve(2);
+        cudaStream_t s = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        bgpu::check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+        bgpu::check_cuda(cudaEventCreate(&e0), "event");
+        bgpu::check_cuda(cudaEventCreate(&e1), "event");
+        bgpu::check_cuda(cudaMemsetAsync(words.p, 0, 2 * sizeof(uint32_t), s), "memset");
+        bgpu::check_cuda(cudaEventRecord(e0, s), "event");
+        bgpu::run_wait_selftest(uint64_t(limit_ms) * 1000000ull, reinterpret_cast<unsigned int*>(words.p), words.p + 1, s);
+        bgpu::check_cuda(cudaGetLastError(), "selftest launch");
+        bgpu::check_cuda(cudaEventRecord(e1, s), "event");
+        uint32_t st = 0;
+        bgpu::check_cuda(cudaMemcpyAsync(&st, words.p + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "d2h");
+        bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+        float ms = 0.0f;
+        bgpu::check_cuda(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaStreamDestroy(s);
+        if (device_status) *device_status = st;
+        if (waited_ms) *waited_ms = ms;
+        return BGPU_OK;
+    });
+}
+
 int bgpu_device_count(void) {
     int c = 0;
     if (cudaGetDeviceCount(&c) != cudaSuccess) {

@@ -231,6 +231,11 @@ bgpu_status bgpu_read_colour_batches(bgpu_world* w, uint32_t* groups, uint32_t* 
 bgpu_status bgpu_get_stats(bgpu_world* w, bgpu_step_stats* out);
 /* Turns per-stage timing on (resetting the sums) or off. */
 bgpu_status bgpu_enable_step_timing(bgpu_world* w, int on);
+/* Diagnostics: runs one solver team barrier that nothing completes, with a time limit of
+ * limit_ms (1..2000), and reports the device status bits it left (BGPU_DEVSTAT_BARRIER_TIMEOUT
+ * when the wait gave up, as it must) and the device time the launch took. Shows that the
+ * device-side waits of the step end with an error status instead of hanging the device. */
+bgpu_status bgpu_selftest_wait_timeout(uint32_t limit_ms, uint32_t* device_status, float* waited_ms);
 
 /* Stand-alone stages on caller data (parity harness entry points).
  * Broad phase: aabbs n x 6 (min3, max3) -> the closed-overlap pairs (i < j),

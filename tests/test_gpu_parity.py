@@ -374,3 +374,19 @@ def test_colour_batches_cover_every_row_group(gpu):
     assert int(groups.sum()) == st["num_contact_pairs"]
     assert int(split.sum()) == st["num_split_pairs"]
     assert np.all(groups > 0) and np.all(split <= groups)
+
+
+def test_device_wait_gives_up_with_an_error_status(gpu):
+    """A solver team barrier that nothing completes ends after its time limit with
+    BGPU_DEVSTAT_BARRIER_TIMEOUT (0x4) in the status word, and the context stays usable."""
+    import scenes
+
+    status, ms = gpu.selftest_wait_timeout(50)
+    assert status & 0x4, status
+    assert 45.0 <= ms < 2000.0, ms
+    s = scenes.falling_box_stack(2, 2, 2, seed=1, steps=5)
+    w = s.build_gpu(gpu)
+    w.step(s.dt, 5)
+    assert w.stats()["device_status"] == 0
+    with pytest.raises(gpu.BgpuError):
+        gpu.selftest_wait_timeout(0)
