@@ -229,6 +229,8 @@ struct PairDataDev {
 };
 
 constexpr uint32_t ROUTE_COUNT0 = 16;  // first per-route counter in PairData::scalars
+constexpr uint32_t CAPTURE_COUNT = ROUTE_COUNT0 + NP_CONVEX + 1;  // detections with points (capture list length)
+constexpr uint32_t CAPTURE_LIST = NP_CONVEX;  // the capture list is route_list region [7 P, 8 P)
 
 struct PairData {
     // Per pair (indexed like the sorted pair array).
@@ -238,12 +240,13 @@ struct PairData {
     DevBuf<uint32_t> detect_n;     // points per fresh detection
     DevBuf<uint32_t> row_count;    // solver rows per pair (0..4)
     DevBuf<float4> rows;           // ROW_F4 per contact slot, 4 slots per pair
-    DevBuf<uint32_t> route_list;   // pairs needing detection, one list per route r: [(r - 1) P, r P)
+    DevBuf<uint32_t> route_list;   // pairs needing detection, one list per route r: [(r - 1) P, r P);
+                                   // then [7 P, 8 P): the detections that found points
     DevBuf<uint32_t> old_owned;    // per old manifold: 1 when a current pair took it over
     DevBuf<uint32_t> scalars;      // [0] analytic count [1] convex count [2] contact pairs [3] contacts
                                    // [4] colours [5] split pairs [6] detect total [7] manifolds
                                    // [8] [9] cache compaction counts [10] split contacts [11] largest split batch
-                                   // [ROUTE_COUNT0 + r] pairs on narrow-phase route r
+                                   // [ROUTE_COUNT0 + r] pairs on narrow-phase route r [CAPTURE_COUNT]
     // Solver batches
     DevBuf<uint32_t> contact_pairs;  // pair ids with rows (ascending)
     DevBuf<uint32_t> colour;         // per contact pair
@@ -252,6 +255,7 @@ struct PairData {
     DevBuf<unsigned long long> body_dup;   // 2 words per body: colours seeded twice at the body
     DevBuf<uint32_t> colour_remap;         // colour -> dense colour (empty colours dropped)
     DevBuf<uint32_t> colour_work;          // two lists of uncoloured groups (Jones-Plassmann rounds)
+    DevBuf<uint32_t> colour_sub;           // groups per (colour, row count), then the scatter's cursors
     DevBuf<uint32_t> colour_count, colour_offset, colour_cursor;
     DevBuf<uint32_t> split_count, split_offset, split_cursor;
     DevBuf<uint4> batch_rec;         // contact pairs in colour order: body a, body b, pair | rows << 29, 0
@@ -269,9 +273,9 @@ struct PairData {
         detect_n.reserve(npairs);
         row_count.reserve(npairs);
         rows.reserve(npairs * 4 * ROW_F4);
-        route_list.reserve(size_t(NP_CONVEX) * npairs);
+        route_list.reserve(size_t(CAPTURE_LIST + 1) * npairs);
         old_owned.reserve(old_manifolds + 1);
-        scalars.reserve(ROUTE_COUNT0 + NP_CONVEX + 1);
+        scalars.reserve(CAPTURE_COUNT + 1);
         contact_pairs.reserve(npairs);
         colour.reserve(npairs);
         body_prio.reserve(nbodies);

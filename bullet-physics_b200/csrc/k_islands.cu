@@ -77,7 +77,7 @@ __global__ void k_island_need(const uint4* __restrict__ info, uint32_t n, uint32
         uint4 in = info[i];
         c = participates(in.y) && (in.z == ACT_ISLAND_SLEEPING || in.z == ACT_WANTS_DEACTIVATION);
     }
-    if (__ballot_sync(0xffffffffu, c) && (threadIdx.x & 31u) == 0u) atomicOr(need, 1u);
+    if (__ballot_sync(0xffffffffu, c) && (threadIdx.x & 31u) == 0u && *(volatile uint32_t*)need == 0u) atomicOr(need, 1u);
 }
 
 __global__ void k_uf_init(uint32_t n, uint32_t* parent, uint32_t* awake) {
@@ -173,7 +173,12 @@ __global__ void k_uf_apply(uint4* info, float4* lv, float4* av, float4* sleep, u
         if (rec_flags) rec_flags[i] |= RF_ZEROED;
     }
     bool active = in.z == ACT_ACTIVE || in.z == ACT_WANTS_DEACTIVATION || in.z == ACT_DISABLE_DEACTIVATION;
-    if (active) atomicOr(&simulate[world_of ? world_of[i] : 0u], 1u);
+    if (active) {
+        // The flag only goes from 0 to 1 here: skip the atomic once it reads as raised
+        // (one word shared by every body of a world would otherwise serialise them all).
+        uint32_t* f = &simulate[world_of ? world_of[i] : 0u];
+        if (*f == 0u) atomicOr(f, 1u);
+    }
 }
 
 }  // namespace

@@ -7,6 +7,7 @@
 // compacted list so EPA's scratch only costs where it runs), and
 // capture+refresh+rows for the pairs that were re-detected.
 #include <cub/cub.cuh>
+#include <cooperative_groups.h>
 #include "bgpu_kernels.cuh"
 
 namespace bgpu {
@@ -393,13 +394,25 @@ __device__ __noinline__ void collide_convex(const Shape& sa, V3 pa, Q qa, const 
     mf_push(m, point_a - n * depth, n, depth);
 }
 
-__device__ __forceinline__ void store_detection(PairDataDev& pd, uint32_t p, const Manifold& m) {
+// A detection with points goes to the capture list; one without drops the pair's manifold
+// here (step.rs:800-853: an empty detection removes it), so the capture pass only runs
+// where there is something to merge.
+__device__ __forceinline__ void store_detection(PairDataDev& pd, uint32_t p, uint32_t npairs, const Manifold& m) {
     float4* d = pd.detect + size_t(p) * 8;
     for (int k = 0; k < m.n; ++k) {
         d[2 * k] = to4(m.pos[k], m.pen[k]);
         d[2 * k + 1] = to4(m.nrm[k], 0.0f);
     }
     pd.detect_n[p] = uint32_t(m.n);
+    if (m.n == 0) {
+        store_meta_only(pd.entries + size_t(p) * ENTRY_F4, 0u);
+        return;
+    }
+    cooperative_groups::coalesced_group g = cooperative_groups::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(&pd.scalars[CAPTURE_COUNT], g.size());
+    base = g.shfl(base, 0);
+    pd.route_list[size_t(CAPTURE_LIST) * npairs + base + g.thread_rank()] = p;
 }
 
 __device__ __forceinline__ bool entry_seed(const float4* __restrict__ e, V3& s) {
@@ -431,7 +444,7 @@ __global__ void k_narrow_analytic(BodyDev b, const Shape* __restrict__ shapes, c
         Manifold m;
         collide_analytic(pd.status[p] >> 8, sa, from4(b.pred[i]), q4(b.quat[i]), sb, from4(b.pred[j]), q4(b.quat[j]),
                          hull, m);
-        store_detection(pd, p, m);
+        store_detection(pd, p, npairs, m);
     }
 }
 
@@ -451,7 +464,7 @@ __global__ void k_narrow_convex(BodyDev b, const Shape* __restrict__ shapes, con
         Manifold m;
         collide_convex(sa, from4(b.pred[i]), q4(b.quat[i]), sb, from4(b.pred[j]), q4(b.quat[j]), has_seed, seed, hull,
                        scratch, m, status);
-        store_detection(pd, p, m);
+        store_detection(pd, p, npairs, m);
     }
 }
 
@@ -461,11 +474,7 @@ __device__ __forceinline__ void capture_one(const BodyDev& b, const Shape* __res
     uint64_t key = pairs[p];
     uint32_t i = key_lo(key), j = key_hi(key);
     float4* ne = pd.entries + size_t(p) * ENTRY_F4;
-    uint32_t n = pd.detect_n[p];
-    if (n == 0) {
-        store_meta_only(ne, 0u);
-        return;
-    }
+    const uint32_t n = pd.detect_n[p];  // > 0: the capture list holds detections with points
     Manifold m;
     m.n = int(n);
     const float4* d = pd.detect + size_t(p) * 8;
@@ -499,16 +508,10 @@ __device__ __forceinline__ void capture_one(const BodyDev& b, const Shape* __res
 
 __global__ void k_capture(BodyDev b, const Shape* __restrict__ shapes, const uint64_t* __restrict__ pairs,
                           uint32_t npairs, StepParams sp, PairDataDev pd) {
-    uint32_t counts[NP_CONVEX + 1];
-    uint32_t cnt = 0;
-#pragma unroll
-    for (uint32_t r = 0; r <= NP_CONVEX; ++r) {
-        counts[r] = pd.scalars[ROUTE_COUNT0 + r];
-        if (r >= NP_PLANE_A) cnt += counts[r];
-    }
+    const uint32_t cnt = pd.scalars[CAPTURE_COUNT];
+    const uint32_t* list = pd.route_list + size_t(CAPTURE_LIST) * npairs;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
-        const uint32_t p = detect_list_pair(pd.route_list, counts, npairs, t, NP_CONVEX);
-        capture_one(b, shapes, pairs, sp, pd, p);
+        capture_one(b, shapes, pairs, sp, pd, list[t]);
     }
 }
 
@@ -582,7 +585,8 @@ void run_pair_pass(const WorldView& w, const uint64_t* pairs, uint32_t npairs, c
     if (npairs == 0) return;
     PairDataDev d = pd.dev();
     check_cuda(cudaMemsetAsync(pd.scalars.p, 0, 8 * sizeof(uint32_t), s), "memset scalars");
-    check_cuda(cudaMemsetAsync(pd.scalars.p + ROUTE_COUNT0, 0, (NP_CONVEX + 1) * sizeof(uint32_t), s), "memset scalars");
+    check_cuda(cudaMemsetAsync(pd.scalars.p + ROUTE_COUNT0, 0, (CAPTURE_COUNT + 1 - ROUTE_COUNT0) * sizeof(uint32_t), s),
+               "memset scalars");
     const int TB = 128;
     k_classify<<<(npairs + TB - 1) / TB, TB, 0, s>>>(w.b, w.shapes, pairs, npairs, old_cache.keys.p,
                                                      old_cache.entries.p, old_cache.count_dev, sp, d);

@@ -285,11 +285,14 @@ __global__ void k_colour(ColourArgs a, JpList wl) {
 // plus the row and split-row totals.
 __global__ void k_colour_hist(const uint32_t* __restrict__ count, const uint32_t* __restrict__ contact_pairs,
                               const uint32_t* __restrict__ colour, const uint32_t* __restrict__ row_count,
-                              const float4* __restrict__ rows, uint32_t* hist, uint32_t* split_hist, uint32_t* split_flag) {
-    // Block-local histograms; [MAX_COLOURS] rows, [MAX_COLOURS + 1] split-active rows.
-    __shared__ uint32_t sh[MAX_COLOURS + 2], ssh[MAX_COLOURS];
+                              const float4* __restrict__ rows, uint32_t* hist, uint32_t* split_hist, uint32_t* split_flag,
+                              uint32_t* sub_hist) {
+    // Block-local histograms; [MAX_COLOURS] rows, [MAX_COLOURS + 1] split-active rows;
+    // shc: groups per (colour, row count - 1).
+    __shared__ uint32_t sh[MAX_COLOURS + 2], ssh[MAX_COLOURS], shc[MAX_COLOURS * 4];
     for (uint32_t i = threadIdx.x; i < MAX_COLOURS + 2; i += blockDim.x) sh[i] = 0;
     for (uint32_t i = threadIdx.x; i < MAX_COLOURS; i += blockDim.x) ssh[i] = 0;
+    for (uint32_t i = threadIdx.x; i < MAX_COLOURS * 4; i += blockDim.x) shc[i] = 0;
     __syncthreads();
     uint32_t K = *count;
     uint32_t nrows = 0, nsplit_rows = 0;
@@ -302,6 +305,7 @@ __global__ void k_colour_hist(const uint32_t* __restrict__ count, const uint32_t
         atomicAdd(&sh[c], 1u);
         uint32_t p = contact_pairs[k];
         uint32_t n = row_count[p];
+        atomicAdd(&shc[c * 4 + (n - 1)], 1u);
         nrows += n;
         uint32_t nsr = 0;  // split-active rows
         for (uint32_t r = 0; r < n; ++r) nsr += rows[(size_t(p) * 4 + r) * ROW_F4 + 5].z != 0.0f ? 1u : 0u;
@@ -322,6 +326,8 @@ __global__ void k_colour_hist(const uint32_t* __restrict__ count, const uint32_t
         if (sh[i]) atomicAdd(&hist[i], sh[i]);
         if (ssh[i]) atomicAdd(&split_hist[i], ssh[i]);
     }
+    for (uint32_t i = threadIdx.x; i < MAX_COLOURS * 4; i += blockDim.x)
+        if (shc[i]) atomicAdd(&sub_hist[i], shc[i]);
     if (threadIdx.x == 0) {
         if (sh[MAX_COLOURS]) atomicAdd(&hist[MAX_COLOURS + 1], sh[MAX_COLOURS]);
         if (sh[MAX_COLOURS + 1]) atomicAdd(&hist[MAX_COLOURS + 2], sh[MAX_COLOURS + 1]);
@@ -332,20 +338,28 @@ __global__ void k_colour_hist(const uint32_t* __restrict__ count, const uint32_t
 // [10] split rows [11] largest split batch.
 __global__ void k_colour_scan(uint32_t* hist, uint32_t* offset, uint32_t* cursor, uint32_t* split_hist,
                               uint32_t* split_offset, uint32_t* split_cursor, const unsigned int* bar, uint32_t* scalars,
-                              uint32_t* remap) {
+                              uint32_t* remap, const uint32_t* sub_hist, uint32_t* sub_cursor) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const uint32_t nraw = bar[5];
     uint32_t acc = 0, sacc = 0, smax = 0, split_groups = 0, d = 0;
     // Colours without groups are dropped (remap: colour -> dense colour), batches start on
-    // multiples of 32 (one warp's slots never straddle two batches); after the scatter the
-    // cursors hold the batch ends.
+    // multiples of 32 (one warp's slots never straddle two batches). Inside a batch the
+    // groups with 4 rows come first, then 3, 2, 1 (sub_cursor: the scatter's cursor of each
+    // part), so most warps hold groups of one size: their lanes run the same number of
+    // contacts and read the table's contact planes without gaps. The split batches keep
+    // their cursors; after the scatter they hold the split batch ends.
     for (uint32_t c = 0; c < nraw; ++c) {
         if (hist[c] == 0) continue;
         remap[c] = d;
         acc = (acc + 31u) & ~31u;
         offset[d] = acc;
-        cursor[d] = acc;
+        uint32_t part = acc;
+        for (uint32_t n = 4; n >= 1; --n) {
+            sub_cursor[d * 4 + (n - 1)] = part;
+            part += sub_hist[c * 4 + (n - 1)];
+        }
         acc += hist[c];
+        cursor[d] = acc;  // the batch end
         sacc = (sacc + 31u) & ~31u;
         split_offset[d] = sacc;
         split_cursor[d] = sacc;
@@ -381,7 +395,7 @@ __device__ __forceinline__ uint32_t claim_slot(uint32_t* cursor, uint32_t c) {
 __global__ void k_colour_scatter(const uint32_t* __restrict__ count, const uint32_t* __restrict__ contact_pairs,
                                  const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ row_count,
                                  const uint32_t* __restrict__ colour, const uint32_t* __restrict__ split_flag,
-                                 uint32_t* cursor, uint32_t* split_cursor, uint4* batch_rec, uint4* split_rec,
+                                 uint32_t* sub_cursor, uint32_t* split_cursor, uint4* batch_rec, uint4* split_rec,
                                  float4* entries, const uint32_t* __restrict__ remap) {
     uint32_t K = *count;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
@@ -393,7 +407,7 @@ __global__ void k_colour_scatter(const uint32_t* __restrict__ count, const uint3
         // The colour rides in the manifold's meta bits to seed next step's colouring.
         float* mw = &entries[size_t(p) * ENTRY_F4 + 2].w;
         *mw = __uint_as_float((__float_as_uint(*mw) & ~(0xffu << META_COLOUR_SHIFT)) | ((c + 1u) << META_COLOUR_SHIFT));
-        batch_rec[claim_slot(cursor, c)] = rec;
+        batch_rec[claim_slot(sub_cursor, c * 4 + (row_count[p] - 1))] = rec;
         if (split_flag[k]) split_rec[claim_slot(split_cursor, c)] = rec;
     }
 }
@@ -887,13 +901,18 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
     // Batches.
     check_cuda(cudaMemsetAsync(pd.colour_count.p, 0, (MAX_COLOURS + 3) * sizeof(uint32_t), s), "memset");
     check_cuda(cudaMemsetAsync(pd.split_count.p, 0, (MAX_COLOURS + 3) * sizeof(uint32_t), s), "memset");
+    pd.colour_sub.reserve(2 * 4 * MAX_COLOURS);
+    uint32_t* sub_hist = pd.colour_sub.p;
+    uint32_t* sub_cursor = pd.colour_sub.p + 4 * MAX_COLOURS;
+    check_cuda(cudaMemsetAsync(sub_hist, 0, 4 * MAX_COLOURS * sizeof(uint32_t), s), "memset");
     uint32_t g = std::min<uint32_t>((npairs + TB - 1) / TB, 148u * 8u);
     k_colour_hist<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pd.colour.p, pd.row_count.p, pd.rows.p,
-                                   pd.colour_count.p, pd.split_count.p, pd.flags.p);
+                                   pd.colour_count.p, pd.split_count.p, pd.flags.p, sub_hist);
     k_colour_scan<<<1, 32, 0, s>>>(pd.colour_count.p, pd.colour_offset.p, pd.colour_cursor.p, pd.split_count.p,
-                                   pd.split_offset.p, pd.split_cursor.p, pd.barrier.p, pd.scalars.p, pd.colour_remap.p);
+                                   pd.split_offset.p, pd.split_cursor.p, pd.barrier.p, pd.scalars.p, pd.colour_remap.p,
+                                   sub_hist, sub_cursor);
     k_colour_scatter<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pairs, pd.row_count.p, pd.colour.p,
-                                      pd.flags.p, pd.colour_cursor.p, pd.split_cursor.p, pd.batch_rec.p,
+                                      pd.flags.p, sub_cursor, pd.split_cursor.p, pd.batch_rec.p,
                                       pd.split_rec.p, pd.entries.p, pd.colour_remap.p);
     // PGS (cooperative launch: the teams' barriers need every block resident).
     check_cuda(cudaMemsetAsync(pd.barrier.p, 0, 2 * sizeof(unsigned int), s), "memset barrier");
