@@ -174,10 +174,13 @@ __global__ void k_uf_apply(uint4* info, float4* lv, float4* av, float4* sleep, u
     }
     bool active = in.z == ACT_ACTIVE || in.z == ACT_WANTS_DEACTIVATION || in.z == ACT_DISABLE_DEACTIVATION;
     if (active) {
-        // The flag only goes from 0 to 1 here: skip the atomic once it reads as raised
-        // (one word shared by every body of a world would otherwise serialise them all).
-        uint32_t* f = &simulate[world_of ? world_of[i] : 0u];
-        if (*f == 0u) atomicOr(f, 1u);
+        // One lane per world among the warp's active bodies raises the flag, and only while
+        // it reads as 0 (the flag only goes from 0 to 1): a word shared by every body of a
+        // world would otherwise take one atomic per body.
+        const uint32_t w = world_of ? world_of[i] : 0u;
+        const uint32_t peers = __match_any_sync(__activemask(), w);
+        uint32_t* f = &simulate[w];
+        if ((threadIdx.x & 31u) == uint32_t(__ffs(int(peers)) - 1) && *f == 0u) atomicOr(f, 1u);
     }
 }
 

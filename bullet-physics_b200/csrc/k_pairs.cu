@@ -245,16 +245,43 @@ __device__ __forceinline__ uint32_t route_of(uint32_t ta, uint32_t tb) {
     return NP_CONVEX;
 }
 
-__device__ __forceinline__ int64_t find_key(const uint64_t* __restrict__ keys, uint32_t n, uint64_t k) {
-    uint32_t lo = 0, hi = n;
+// Position of k in the sorted keys[0, n), or -1. The search starts with a galloping
+// probe around `guess` (from step to step a pair keeps nearly the same rank among the
+// sorted pairs, so the key is usually a few places away) and ends with a binary search
+// of the bracket it found: a few dependent loads instead of log2(n).
+__device__ __forceinline__ int64_t find_key(const uint64_t* __restrict__ keys, uint32_t n, uint64_t k, uint32_t guess) {
+    if (n == 0) return -1;
+    uint32_t lo, hi;  // the answer (first index with keys[i] >= k) lies in [lo, hi]
+    const uint32_t g = guess < n ? guess : n - 1;
+    if (keys[g] < k) {
+        lo = g + 1;
+        uint32_t step = 1;
+        hi = n;
+        while (lo + step - 1 < n) {
+            const uint32_t probe = lo + step - 1;
+            if (keys[probe] >= k) { hi = probe; break; }
+            lo = probe + 1;
+            step <<= 1;
+        }
+    } else {
+        hi = g;
+        uint32_t step = 1;
+        lo = 0;
+        while (hi >= step) {
+            const uint32_t probe = hi - step;
+            if (keys[probe] < k) { lo = probe + 1; break; }
+            hi = probe;
+            step <<= 1;
+        }
+    }
     while (lo < hi) {
         uint32_t mid = (lo + hi) >> 1;
-        uint64_t v = keys[mid];
-        if (v < k) lo = mid + 1;
+        if (keys[mid] < k) lo = mid + 1;
         else hi = mid;
     }
     return (lo < n && keys[lo] == k) ? int64_t(lo) : -1;
 }
+
 
 __device__ __forceinline__ bool active_state(uint32_t a) {
     return a == ACT_ACTIVE || a == ACT_WANTS_DEACTIVATION || a == ACT_DISABLE_DEACTIVATION;
@@ -302,7 +329,8 @@ __global__ void k_classify(BodyDev b, const Shape* __restrict__ shapes, const ui
         return;
     }
     uint32_t old_count = *old_count_ptr;
-    int64_t old = old_count ? find_key(old_keys, old_count, key) : -1;
+    const uint32_t guess = uint32_t((uint64_t(p) * old_count) / npairs);
+    int64_t old = old_count ? find_key(old_keys, old_count, key, guess) : -1;
     if (old >= 0) pd.old_owned[old] = 1u;
     bool act_a = active_state(ia.z), act_b = active_state(ib.z);
     bool sk_a = (ia.y & (BF_STATIC | BF_KINEMATIC)) != 0, sk_b = (ib.y & (BF_STATIC | BF_KINEMATIC)) != 0;
