@@ -172,6 +172,8 @@ struct Broadphase {
     DevBuf<uint32_t> leaf_body, parent, left, right, counts, offsets, refit_flag, flags, scan_out, unbounded;
     DevBuf<uint32_t> stash, overflow;  // partners of proxies with few of them; proxies with many
     DevBuf<float4> node_min, node_max;
+    DevBuf<uint32_t> node_maxid;       // largest body index below each node
+    DevBuf<float4> node_rec;           // per internal node: both children's boxes and references
     DevBuf<unsigned char> cub_tmp;
     DevBuf<int> bounds;          // 6 ordered ints: scene min/max of leaf centres
     DevBuf<uint32_t> scalars;    // [0] total pairs, [1] proxies with more partners than the stash holds

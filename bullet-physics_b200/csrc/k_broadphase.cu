@@ -73,31 +73,42 @@ __device__ __forceinline__ uint32_t quantize(float c, float lo, float hi) {
     return uint32_t(t * 1023.0f);
 }
 
+// Morton code of each proxy's AABB centre (unbounded proxies: all ones, so they sort last),
+// and the proxy index as the sort's value. A stable radix sort of the 32-bit codes with the
+// indices as values orders the proxies exactly as sorting (code << 32 | index) would, in
+// four 8-bit passes instead of eight.
 __global__ void k_keys(const float4* __restrict__ mn, const float4* __restrict__ mx, const uint32_t* __restrict__ is_unb,
-                       uint32_t n, const int* __restrict__ bounds, uint64_t* keys) {
+                       uint32_t n, const int* __restrict__ bounds, uint32_t* codes, uint32_t* index) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    if (is_unb[i]) { keys[i] = ~0ull; return; }
+    index[i] = i;
+    if (is_unb[i]) { codes[i] = 0xffffffffu; return; }
     float4 a = mn[i], b = mx[i];
     float lo0 = ordered_to_float(bounds[0]), lo1 = ordered_to_float(bounds[1]), lo2 = ordered_to_float(bounds[2]);
     float hi0 = ordered_to_float(bounds[3]), hi1 = ordered_to_float(bounds[4]), hi2 = ordered_to_float(bounds[5]);
     uint32_t x = quantize(0.5f * (a.x + b.x), lo0, hi0);
     uint32_t y = quantize(0.5f * (a.y + b.y), lo1, hi1);
     uint32_t z = quantize(0.5f * (a.z + b.z), lo2, hi2);
-    uint32_t code = (expand_bits(x) << 2) | (expand_bits(y) << 1) | expand_bits(z);
-    keys[i] = (uint64_t(code) << 32) | i;
+    codes[i] = (expand_bits(x) << 2) | (expand_bits(y) << 1) | expand_bits(z);
 }
 
-__device__ __forceinline__ int delta(const uint64_t* __restrict__ k, int m, int i, int j) {
+// Sorted leaves as unique 64-bit keys: code << 32 | proxy index.
+struct LeafKeys {
+    const uint32_t* __restrict__ code;
+    const uint32_t* __restrict__ index;
+    __device__ __forceinline__ uint64_t operator[](int i) const { return (uint64_t(code[i]) << 32) | index[i]; }
+};
+
+__device__ __forceinline__ int delta(const LeafKeys& k, int m, int i, int j) {
     if (j < 0 || j >= m) return -1;
     return __clzll(k[i] ^ k[j]);
 }
 
 // Karras 2012: internal node i spans a key range split at its highest differing bit.
-__global__ void k_build(const uint64_t* __restrict__ k, int m, uint32_t* left, uint32_t* right, uint32_t* parent,
+__global__ void k_build(LeafKeys k, int m, uint32_t* left, uint32_t* right, uint32_t* parent,
                         uint32_t* leaf_body, uint32_t* refit_flag) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < m) leaf_body[i] = uint32_t(k[i] & 0xffffffffu);
+    if (i < m) leaf_body[i] = k.index[i];
     if (i >= m - 1) return;
     refit_flag[i] = 0;
     int d = (delta(k, m, i, i + 1) - delta(k, m, i, i - 1)) >= 0 ? 1 : -1;
@@ -125,15 +136,24 @@ __global__ void k_build(const uint64_t* __restrict__ k, int m, uint32_t* left, u
     parent[rc] = uint32_t(i);
 }
 
+// Leaf children are referenced as LEAF_REF | body index in the node records.
+constexpr uint32_t LEAF_REF = 0x80000000u;
+
+// Bottom-up refit: node boxes and the largest body index below each node; each internal
+// node's record (4 float4: left child min | ref, left max | ref of right, right min | largest
+// body index under left, right max | largest under right) is written by the thread that
+// completes it, so a query reads one 64-byte record per node it visits.
 __global__ void k_refit(int m, const uint32_t* __restrict__ leaf_body, const uint32_t* __restrict__ parent,
                         const uint32_t* __restrict__ left, const uint32_t* __restrict__ right, uint32_t* refit_flag,
-                        const float4* __restrict__ bmin, const float4* __restrict__ bmax, float4* nmin, float4* nmax) {
+                        const float4* __restrict__ bmin, const float4* __restrict__ bmax, float4* nmin, float4* nmax,
+                        uint32_t* nid, float4* rec) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= m) return;
     uint32_t node = uint32_t(m - 1 + t);
     uint32_t body = leaf_body[t];
     nmin[node] = bmin[body];
     nmax[node] = bmax[body];
+    nid[node] = body;
     if (m == 1) return;
     __threadfence();
     uint32_t cur = parent[node];
@@ -142,8 +162,17 @@ __global__ void k_refit(int m, const uint32_t* __restrict__ leaf_body, const uin
         __threadfence();
         uint32_t l = left[cur], r = right[cur];
         float4 a0 = __ldcg(&nmin[l]), a1 = __ldcg(&nmax[l]), b0 = __ldcg(&nmin[r]), b1 = __ldcg(&nmax[r]);
+        const uint32_t il = __ldcg(&nid[l]), ir = __ldcg(&nid[r]);
         nmin[cur] = make_float4(fminf(a0.x, b0.x), fminf(a0.y, b0.y), fminf(a0.z, b0.z), 0.f);
         nmax[cur] = make_float4(fmaxf(a1.x, b1.x), fmaxf(a1.y, b1.y), fmaxf(a1.z, b1.z), 0.f);
+        nid[cur] = il > ir ? il : ir;
+        const uint32_t lref = l >= uint32_t(m - 1) ? (LEAF_REF | il) : l;
+        const uint32_t rref = r >= uint32_t(m - 1) ? (LEAF_REF | ir) : r;
+        float4* rc = rec + size_t(cur) * 4;
+        rc[0] = make_float4(a0.x, a0.y, a0.z, __uint_as_float(lref));
+        rc[1] = make_float4(a1.x, a1.y, a1.z, __uint_as_float(rref));
+        rc[2] = make_float4(b0.x, b0.y, b0.z, __uint_as_float(il));
+        rc[3] = make_float4(b1.x, b1.y, b1.z, __uint_as_float(ir));
         __threadfence();
         if (cur == 0) return;
         cur = parent[cur];
@@ -163,8 +192,7 @@ constexpr uint32_t STASH_SLOTS = 32;
 
 template <int MODE>
 __global__ void k_query(int m, uint32_t n, const uint32_t* __restrict__ is_unb, const float4* __restrict__ bmin,
-                        const float4* __restrict__ bmax, const float4* __restrict__ nmin, const float4* __restrict__ nmax,
-                        const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                        const float4* __restrict__ bmax, const float4* __restrict__ rec,
                         const uint32_t* __restrict__ leaf_body, const uint32_t* __restrict__ unb, uint32_t nunb,
                         uint32_t* counts, const uint32_t* __restrict__ offsets, uint64_t* out, uint32_t* status,
                         uint32_t* list, uint32_t* list_len, uint32_t* stash) {
@@ -202,28 +230,27 @@ __global__ void k_query(int m, uint32_t n, const uint32_t* __restrict__ is_unb, 
         }
         ++cnt;
     };
-    if (m > 0) {
+    if (m == 1) {  // the root is the single leaf
+        const uint32_t j = leaf_body[0];
+        if (j > i && overlaps(qmin, qmax, bmin[j], bmax[j])) emit(j);
+    } else if (m > 1) {
+        // Subtrees whose largest body index is at most i hold no partner j > i and are skipped.
         uint32_t stack[STACK_DEPTH];
         int sp = 0;
         stack[sp++] = 0u;
-        if (m == 1) {
-            // The root is the single leaf.
-            sp = 0;
-            uint32_t j = leaf_body[0];
-            if (j > i && overlaps(qmin, qmax, bmin[j], bmax[j])) emit(j);
-        }
         while (sp > 0) {
-            uint32_t node = stack[--sp];
-            uint32_t ch[2] = {left[node], right[node]};
+            const float4* r = rec + size_t(stack[--sp]) * 4;
+            const float4 a = r[0], b = r[1], c = r[2], d = r[3];
+            const uint32_t ref[2] = {__float_as_uint(a.w), __float_as_uint(b.w)};
+            const bool hit[2] = {__float_as_uint(c.w) > i && overlaps(qmin, qmax, a, b),
+                                 __float_as_uint(d.w) > i && overlaps(qmin, qmax, c, d)};
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                uint32_t cn = ch[c];
-                if (!overlaps(qmin, qmax, nmin[cn], nmax[cn])) continue;
-                if (cn >= uint32_t(m - 1)) {
-                    uint32_t j = leaf_body[cn - (m - 1)];
-                    if (j > i) emit(j);
+            for (int k = 0; k < 2; ++k) {
+                if (!hit[k]) continue;
+                if (ref[k] & LEAF_REF) {
+                    emit(ref[k] & ~LEAF_REF);
                 } else if (sp < STACK_DEPTH) {
-                    stack[sp++] = cn;
+                    stack[sp++] = ref[k];
                 } else {
                     atomicOr(status, ST_TRAVERSAL_STACK);
                 }
@@ -409,6 +436,8 @@ uint64_t Broadphase::run(const float4* aabb_min, const float4* aabb_max, uint32_
     refit_flag.reserve(n);
     node_min.reserve(2 * size_t(n));
     node_max.reserve(2 * size_t(n));
+    node_maxid.reserve(2 * size_t(n));
+    node_rec.reserve(4 * size_t(n));
     counts.reserve(n);
     offsets.reserve(n);
     flags.reserve(n);
@@ -423,22 +452,24 @@ uint64_t Broadphase::run(const float4* aabb_min, const float4* aabb_max, uint32_
     if (nunb) k_set_unbounded<<<(nunb + TB - 1) / TB, TB, 0, s>>>(unbounded.p, nunb, flags.p);
     k_reset_bounds<<<1, 32, 0, s>>>(bounds.p);
     k_bounds<<<grid, TB, 0, s>>>(aabb_min, aabb_max, flags.p, n, bounds.p);
-    k_keys<<<grid, TB, 0, s>>>(aabb_min, aabb_max, flags.p, n, bounds.p, keys.p);
+    // keys / keys_alt (n x 8 bytes each) hold the codes and indices and their sort buffers.
+    uint32_t* codes = reinterpret_cast<uint32_t*>(keys.p);
+    uint32_t* codes_alt = reinterpret_cast<uint32_t*>(keys_alt.p);
+    k_keys<<<grid, TB, 0, s>>>(aabb_min, aabb_max, flags.p, n, bounds.p, codes, codes + n);
 
-    // Sort the Morton keys (unbounded proxies carry ~0 and sort last).
     size_t tmp_bytes = 0;
-    cub::DoubleBuffer<uint64_t> db(keys.p, keys_alt.p);
-    check_cuda(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, int(n), 0, 64, s), "sort size");
+    cub::DoubleBuffer<uint32_t> dk(codes, codes_alt), dv(codes + n, codes_alt + n);
+    check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, dk, dv, int(n), 0, 32, s), "sort size");
     size_t scan_bytes = 0;
     check_cuda(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, counts.p, offsets.p, int(n), s), "scan size");
     cub_tmp.reserve(std::max(tmp_bytes, scan_bytes));
-    check_cuda(cub::DeviceRadixSort::SortKeys(cub_tmp.p, tmp_bytes, db, int(n), 0, 64, s), "sort");
-    const uint64_t* sorted = db.Current();
+    check_cuda(cub::DeviceRadixSort::SortPairs(cub_tmp.p, tmp_bytes, dk, dv, int(n), 0, 32, s), "sort");
+    const LeafKeys sorted{dk.Current(), dv.Current()};
 
     if (m > 0) {
         k_build<<<(m + TB - 1) / TB, TB, 0, s>>>(sorted, m, left.p, right.p, parent.p, leaf_body.p, refit_flag.p);
         k_refit<<<(m + TB - 1) / TB, TB, 0, s>>>(m, leaf_body.p, parent.p, left.p, right.p, refit_flag.p, aabb_min,
-                                                 aabb_max, node_min.p, node_max.p);
+                                                 aabb_max, node_min.p, node_max.p, node_maxid.p, node_rec.p);
     }
     const uint32_t qgrid = m > 0 ? (uint32_t(m) + TB - 1) / TB : 1u;
     // One traversal per proxy: counts, plus the sorted partners of every proxy with at
@@ -446,9 +477,9 @@ uint64_t Broadphase::run(const float4* aabb_min, const float4* aabb_max, uint32_
     stash.reserve(size_t(STASH_SLOTS) * uint32_t(m > 0 ? m : 1));
     overflow.reserve(uint32_t(m > 0 ? m : 1));
     check_cuda(cudaMemsetAsync(scalars.p, 0, 2 * sizeof(uint32_t), s), "memset");
-    k_query<Q_STASH><<<qgrid, TB, 0, s>>>(m, n, flags.p, aabb_min, aabb_max, node_min.p, node_max.p, left.p, right.p,
-                                          leaf_body.p, unbounded.p, nunb, counts.p, nullptr, nullptr, status_dev,
-                                          overflow.p, scalars.p + 1, stash.p);
+    k_query<Q_STASH><<<qgrid, TB, 0, s>>>(m, n, flags.p, aabb_min, aabb_max, node_rec.p, leaf_body.p, unbounded.p,
+                                          nunb, counts.p, nullptr, nullptr, status_dev, overflow.p, scalars.p + 1,
+                                          stash.p);
     // Unbounded proxies: count their segments by flag + scan.
     for (uint32_t u = 0; u < nunb; ++u) {
         uint32_t h = unbounded_host[u];
@@ -468,8 +499,8 @@ uint64_t Broadphase::run(const float4* aabb_min, const float4* aabb_max, uint32_
         if (m > 0) k_stash_copy<<<qgrid, TB, 0, s>>>(m, leaf_body.p, counts.p, offsets.p, stash.p, out.p);
         if (n_overflow)
             k_query<Q_WRITE><<<(n_overflow + TB - 1) / TB, TB, 0, s>>>(
-                m, n, flags.p, aabb_min, aabb_max, node_min.p, node_max.p, left.p, right.p, leaf_body.p, unbounded.p,
-                nunb, counts.p, offsets.p, out.p, status_dev, overflow.p, scalars.p + 1, nullptr);
+                m, n, flags.p, aabb_min, aabb_max, node_rec.p, leaf_body.p, unbounded.p, nunb, counts.p, offsets.p,
+                out.p, status_dev, overflow.p, scalars.p + 1, nullptr);
         for (uint32_t u = 0; u < nunb; ++u) {
             uint32_t h = unbounded_host[u];
             k_unb_flags<<<grid, TB, 0, s>>>(h, n, aabb_min, aabb_max, scan_out.p);
@@ -605,11 +636,15 @@ extern "C" bgpu_status bgpu_broadphase_pairs_noalloc(const float* aabbs_dev, uin
         uint32_t* unb_list = sb.take<uint32_t>(BGPU_NOALLOC_MAX_UNBOUNDED + 1);
         float4* node_min = sb.take<float4>(2 * size_t(n));
         float4* node_max = sb.take<float4>(2 * size_t(n));
+        float4* node_rec = sb.take<float4>(4 * size_t(n));
+        uint32_t* node_maxid = sb.take<uint32_t>(2 * size_t(n));
         int* bounds = sb.take<int>(8);
         uint32_t* scalars = sb.take<uint32_t>(8);
         size_t sort_bytes = 0, scan_bytes = 0;
-        cub::DoubleBuffer<uint64_t> db(keys, keys_alt);
-        check_cuda(cub::DeviceRadixSort::SortKeys(nullptr, sort_bytes, db, int(n), 0, 64, s), "sort size");
+        uint32_t* codes = reinterpret_cast<uint32_t*>(keys);
+        uint32_t* codes_alt = reinterpret_cast<uint32_t*>(keys_alt);
+        cub::DoubleBuffer<uint32_t> dk(codes, codes_alt), dv(codes + n, codes_alt + n);
+        check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, dk, dv, int(n), 0, 32, s), "sort size");
         check_cuda(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, counts, offsets, int(n), s), "scan size");
         size_t tmp_bytes = std::max(sort_bytes, scan_bytes);
         unsigned char* tmp = sb.take<unsigned char>(tmp_bytes);
@@ -642,20 +677,19 @@ extern "C" bgpu_status bgpu_broadphase_pairs_noalloc(const float* aabbs_dev, uin
         const int m = int(n - nunb);
         k_reset_bounds<<<1, 32, 0, s>>>(bounds);
         k_bounds<<<grid, TB, 0, s>>>(mn, mx, is_unb, n, bounds);
-        k_keys<<<grid, TB, 0, s>>>(mn, mx, is_unb, n, bounds, keys);
-        check_cuda(cub::DeviceRadixSort::SortKeys(tmp, sort_bytes, db, int(n), 0, 64, s), "sort");
-        const uint64_t* sorted = db.Current();
+        k_keys<<<grid, TB, 0, s>>>(mn, mx, is_unb, n, bounds, codes, codes + n);
+        check_cuda(cub::DeviceRadixSort::SortPairs(tmp, sort_bytes, dk, dv, int(n), 0, 32, s), "sort");
+        const LeafKeys sorted{dk.Current(), dv.Current()};
         if (m > 0) {
             k_build<<<(m + TB - 1) / TB, TB, 0, s>>>(sorted, m, left, right, parent, leaf_body, refit_flag);
             k_refit<<<(m + TB - 1) / TB, TB, 0, s>>>(m, leaf_body, parent, left, right, refit_flag, mn, mx, node_min,
-                                                     node_max);
+                                                     node_max, node_maxid, node_rec);
         }
         uint32_t* status = scalars + 1;
         const uint32_t qgrid = m > 0 ? (uint32_t(m) + TB - 1) / TB : 1u;
-        k_query<Q_COUNT><<<qgrid, TB, 0, s>>>(m, n, is_unb, mn, mx, node_min, node_max, left, right, leaf_body,
-                                              unb_list, nunb, counts, nullptr, nullptr, status, nullptr, nullptr,
-                                              nullptr);
-        uint32_t* unb_scan = reinterpret_cast<uint32_t*>(db.Alternate());  // free after the build
+        k_query<Q_COUNT><<<qgrid, TB, 0, s>>>(m, n, is_unb, mn, mx, node_rec, leaf_body, unb_list, nunb, counts,
+                                              nullptr, nullptr, status, nullptr, nullptr, nullptr);
+        uint32_t* unb_scan = dk.Alternate();  // free after the build
         check_cuda(cudaStreamSynchronize(s), "sync");
         for (uint32_t u = 0; u < nunb; ++u) {
             uint32_t h = unb_host[u];
@@ -676,9 +710,8 @@ extern "C" bgpu_status bgpu_broadphase_pairs_noalloc(const float* aabbs_dev, uin
         }
         uint64_t* out = reinterpret_cast<uint64_t*>(pairs_dev);
         if (total) {
-            k_query<Q_WRITE><<<qgrid, TB, 0, s>>>(m, n, is_unb, mn, mx, node_min, node_max, left, right, leaf_body,
-                                                  unb_list, nunb, counts, offsets, out, status, nullptr, nullptr,
-                                                  nullptr);
+            k_query<Q_WRITE><<<qgrid, TB, 0, s>>>(m, n, is_unb, mn, mx, node_rec, leaf_body, unb_list, nunb, counts,
+                                                  offsets, out, status, nullptr, nullptr, nullptr);
             for (uint32_t u = 0; u < nunb; ++u) {
                 uint32_t h = unb_host[u];
                 k_unb_flags<<<grid, TB, 0, s>>>(h, n, mn, mx, flags);
