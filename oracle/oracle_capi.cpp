@@ -366,6 +366,99 @@ void orc_world_set_solve_order(void* p, const uint64_t* keys, uint32_t n) {
     DISPATCH(h, { w.solve_order.assign(keys, keys + n); });
 }
 
+// Joint descriptor layout (doubles), shared with tests/oracle_api.py and the GPU's
+// bgpu_joint_desc: 0 kind, 1 body_a, 2 body_b, 3 flags (1 disable collisions, 2 disabled,
+// 4 angular only, 8 limit, 16 motor, 32 ERP override), 4-15 frame A (origin, basis columns
+// x y z), 16-27 frame B, 28 erp, 29 impulse clamp, 30 limit low, 31 limit high,
+// 32 softness, 33 bias factor, 34 relaxation, 35 motor target velocity, 36 motor max impulse.
+constexpr int JDESC = 37;
+
+uint32_t orc_world_add_joint(void* p, const double* d) {
+    Handle* h = static_cast<Handle*>(p);
+    uint32_t r = 0;
+    DISPATCH(h, {
+        using R = std::remove_reference_t<decltype(w.gravity.x)>;
+        Joint<R> jt;
+        auto v3 = [&](int o) { return V3<R>(static_cast<R>(d[o]), static_cast<R>(d[o + 1]), static_cast<R>(d[o + 2])); };
+        jt.kind = uint32_t(d[0]);
+        jt.body_a = uint32_t(d[1]);
+        jt.body_b = uint32_t(d[2]);
+        uint32_t f = uint32_t(d[3]);
+        jt.disable_collisions = (f & 1u) != 0;
+        jt.enabled = (f & 2u) == 0;
+        jt.angular_only = (f & 4u) != 0;
+        jt.has_limit = (f & 8u) != 0;
+        jt.has_motor = (f & 16u) != 0;
+        jt.has_erp = (f & 32u) != 0;
+        jt.frame_a.origin = v3(4);
+        jt.frame_a.basis = M3<R>(v3(7), v3(10), v3(13));
+        jt.frame_b.origin = v3(16);
+        jt.frame_b.basis = M3<R>(v3(19), v3(22), v3(25));
+        jt.erp = static_cast<R>(d[28]);
+        jt.impulse_clamp = static_cast<R>(d[29]);
+        jt.limit.low = static_cast<R>(d[30]);
+        jt.limit.high = static_cast<R>(d[31]);
+        jt.limit.softness = static_cast<R>(d[32]);
+        jt.limit.bias_factor = static_cast<R>(d[33]);
+        jt.limit.relaxation = static_cast<R>(d[34]);
+        jt.motor_target = static_cast<R>(d[35]);
+        jt.motor_max = static_cast<R>(d[36]);
+        w.joints.push_back(jt);
+        r = uint32_t(w.joints.size() - 1);
+    });
+    return r;
+}
+
+void orc_world_set_joint_order(void* p, const uint32_t* ids, uint32_t n) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, { w.joint_order.assign(ids, ids + n); });
+}
+
+void orc_world_joint_angles(void* p, double* out) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, { for (size_t k = 0; k < w.joints.size(); ++k) out[k] = w.joints[k].hinge_angle; });
+}
+
+uint32_t orc_world_num_joint_rows(void* p) {
+    Handle* h = static_cast<Handle*>(p);
+    uint32_t r = 0;
+    DISPATCH(h, { r = uint32_t(w.last_joint_rows.size()); });
+    return r;
+}
+
+// Joint rows of the last step in solve order, 8 doubles each: joint, body_a, body_b, mass,
+// bias, limit kind, accumulated impulse, 0.
+void orc_world_joint_rows(void* p, double* out) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, {
+        for (size_t k = 0; k < w.last_joint_rows.size(); ++k) {
+            const auto& jr = w.last_joint_rows[k];
+            double* o = out + 8 * k;
+            o[0] = jr.joint; o[1] = jr.body_a; o[2] = jr.body_b; o[3] = jr.mass; o[4] = jr.bias;
+            o[5] = jr.lim; o[6] = jr.impulse; o[7] = 0;
+        }
+    });
+}
+
+// hinge.rs:60-100: frames (24 doubles: origin + basis columns, for A then B) from pivots and axes.
+void orc_hinge_frames(int f64, const double* pa, const double* axa, const double* pb, const double* axb, double* out) {
+    auto run = [&](auto tag) {
+        using R = decltype(tag);
+        JointFrame<R> fa, fb;
+        auto v3 = [](const double* x) { return V3<R>(static_cast<R>(x[0]), static_cast<R>(x[1]), static_cast<R>(x[2])); };
+        hinge_frames(v3(pa), v3(axa), v3(pb), v3(axb), fa, fb);
+        const JointFrame<R>* fr[2] = {&fa, &fb};
+        for (int f = 0; f < 2; ++f) {
+            const V3<R> cols[4] = {fr[f]->origin, fr[f]->basis.c0, fr[f]->basis.c1, fr[f]->basis.c2};
+            for (int c = 0; c < 4; ++c) {
+                out[12 * f + 3 * c] = cols[c].x; out[12 * f + 3 * c + 1] = cols[c].y; out[12 * f + 3 * c + 2] = cols[c].z;
+            }
+        }
+    };
+    if (f64) run(double(0));
+    else run(float(0));
+}
+
 void orc_world_stage_seconds(void* p, double* out7) {
     Handle* h = static_cast<Handle*>(p);
     DISPATCH(h, { for (int k = 0; k < 7; ++k) out7[k] = w.stage_s[k]; });

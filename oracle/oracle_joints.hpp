@@ -1,0 +1,331 @@
+// CPU oracle — TEST INFRASTRUCTURE ONLY: joint rows in the PGS solve.
+//
+// Restates, for the point-to-point, fixed and hinge joints:
+//   crates/bullet-dynamics/src/solver/sequential_impulse.rs:214-328 (ConstraintRow, prepare),
+//     :931-971 (solve_joint_row), :720-735 (joint rows after the contacts in each sweep);
+//   crates/bullet-dynamics/src/constraint.rs:755-842 (prepare_rows: point-to-point rows),
+//     :658-752 (JointFrame, AngularLimit::test);
+//   crates/bullet-dynamics/src/constraint/fixed.rs:33-90 (locked-6DOF rows);
+//   crates/bullet-dynamics/src/constraint/hinge.rs:60-100 (frames from pivot/axis), :130-267 (rows);
+//   crates/bullet-dynamics/src/constraint/shared.rs:6-155 (hinge angle, angle wrap, Euler XYZ,
+//     relative rotation axes, motor factor).
+// Frame construction uses glam 0.33.3's `Quat::from_rotation_arc` (not in the reference tree);
+// its published algorithm is restated in rotation_arc() below.
+#pragma once
+#include <cmath>
+#include <cstdint>
+#include <limits>
+#include <vector>
+#include "oracle_math.hpp"
+
+namespace oracle {
+
+enum : uint32_t { JOINT_POINT2POINT = 0, JOINT_FIXED = 1, JOINT_HINGE = 2 };
+// RowLimits (sequential_impulse.rs): which clamp the accumulated impulse takes.
+enum : uint32_t { LIM_UNBOUNDED = 0, LIM_BILATERAL = 1, LIM_LOWER = 2, LIM_UPPER = 3, LIM_WINDOW = 4 };
+
+template <class R>
+struct JointFrame {  // constraint.rs:658-682
+    V3<R> origin;
+    M3<R> basis;  // column 2 is the hinge axis
+};
+
+template <class R>
+struct AngularLimit {  // constraint.rs:684-752
+    R low = 0, high = 0, softness = R(0.9), bias_factor = R(0.3), relaxation = R(1);
+};
+
+template <class R>
+struct Joint {
+    uint32_t kind = JOINT_POINT2POINT, body_a = 0, body_b = 0;
+    bool enabled = true, disable_collisions = true;
+    JointFrame<R> frame_a, frame_b;  // point-to-point: the origins are the pivots
+    R impulse_clamp = 0;             // point-to-point (p2p.rs:11-17)
+    bool has_erp = false;
+    R erp = 0;
+    bool angular_only = false, has_limit = false, has_motor = false;  // hinge (hinge.rs:20-45)
+    AngularLimit<R> limit;
+    R motor_target = 0, motor_max = 0;
+    R hinge_angle = 0;  // per-step state (hinge.rs:37)
+};
+
+template <class R>
+struct JointRow {  // sequential_impulse.rs:214-258
+    uint32_t body_a = 0, body_b = 0, joint = 0;
+    V3<R> lin_a, ang_a, lin_b, ang_b;
+    R inv_mass_a = 0, inv_mass_b = 0;
+    M3<R> iia, iib;
+    R mass = 0, bias = 0, cfm = 0;
+    uint32_t lim = LIM_UNBOUNDED;
+    R lo = 0, hi = 0;
+    R impulse = 0;
+};
+
+// sequential_impulse.rs:260-299 (ConstraintRow::prepare)
+template <class R, class B>
+JointRow<R> prepare_joint_row(uint32_t ia, uint32_t ib, const V3<R>& lin_a, const V3<R>& ang_a, const V3<R>& lin_b,
+                              const V3<R>& ang_b, const B& a, const B& b, R bias, uint32_t lim, R lo, R hi) {
+    JointRow<R> r;
+    r.body_a = ia; r.body_b = ib;
+    r.lin_a = lin_a; r.ang_a = ang_a; r.lin_b = lin_b; r.ang_b = ang_b;
+    r.iia = a.inv_inertia_world();
+    r.iib = b.inv_inertia_world();
+    r.inv_mass_a = a.inv_mass;
+    r.inv_mass_b = b.inv_mass;
+    R k = r.inv_mass_a * lin_a.length_squared() + r.inv_mass_b * lin_b.length_squared() + ang_a.dot(r.iia * ang_a) +
+          ang_b.dot(r.iib * ang_b);
+    r.mass = k > R(0) ? R(1) / k : R(0);
+    r.bias = bias;
+    r.lim = lim; r.lo = lo; r.hi = hi;
+    return r;
+}
+
+// sequential_impulse.rs:931-971 (solve_joint_row)
+template <class R, class B>
+void solve_joint_row(std::vector<B>& bodies, JointRow<R>& c, R damping) {
+    B& a = bodies[c.body_a];
+    B& b = bodies[c.body_b];
+    R row_vel = (c.lin_b.dot(b.linear_velocity) + c.ang_b.dot(b.angular_velocity)) -
+                (c.lin_a.dot(a.linear_velocity) + c.ang_a.dot(a.angular_velocity));
+    R old = c.impulse;
+    R base = damping != R(1) ? c.mass * (c.bias - row_vel * damping) : c.mass * (c.bias - row_vel);
+    R lambda = c.cfm != R(0) ? base - c.cfm * old : base;
+    R nw = old + lambda;
+    switch (c.lim) {
+        case LIM_BILATERAL: nw = std::min(std::max(nw, -c.hi), c.hi); break;
+        case LIM_LOWER: nw = std::max(nw, c.lo); break;
+        case LIM_UPPER: nw = std::min(nw, c.hi); break;
+        case LIM_WINDOW: nw = std::min(std::max(nw, c.lo), c.hi); break;
+        default: break;
+    }
+    c.impulse = nw;
+    R j = nw - old;
+    if (j != R(0)) {
+        a.linear_velocity -= c.lin_a * (j * c.inv_mass_a);
+        b.linear_velocity += c.lin_b * (j * c.inv_mass_b);
+        a.angular_velocity -= c.iia * (c.ang_a * j);
+        b.angular_velocity += c.iib * (c.ang_b * j);
+    }
+}
+
+// shared.rs:9-14 (get_hinge_angle)
+template <class R>
+R hinge_angle_of(const M3<R>& tr_a, const M3<R>& tr_b) {
+    V3<R> swing = tr_b.c1;
+    return std::atan2(swing.dot(tr_a.c0), swing.dot(tr_a.c1));
+}
+
+// shared.rs:17-27 (normalize_angle; % truncates like fmod)
+template <class R>
+R normalize_angle(R angle) {
+    const R pi = R(3.14159265358979323846);
+    const R two_pi = R(2) * pi;
+    R a = std::fmod(angle, two_pi);
+    if (a < -pi) a += two_pi;
+    else if (a > pi) a -= two_pi;
+    return a;
+}
+
+// constraint.rs:735-751 (AngularLimit::test): correction, sign, active
+template <class R>
+void limit_test(const AngularLimit<R>& l, R angle, R& correction, R& sign, bool& active) {
+    R half_range = (l.high - l.low) / R(2);
+    correction = 0; sign = 0; active = false;
+    if (half_range >= R(0)) {
+        R center = normalize_angle(l.low + half_range);
+        R deviation = normalize_angle(angle - center);
+        if (deviation < -half_range) { correction = -(deviation + half_range); sign = 1; active = true; return; }
+        if (deviation > half_range) { correction = half_range - deviation; sign = -1; active = true; return; }
+    }
+}
+
+// shared.rs:123-155 (get_motor_factor)
+template <class R>
+R motor_factor(R pos, R low_lim, R upp_lim, R vel, R time_fact) {
+    if (low_lim > upp_lim) return R(1);
+    if (low_lim == upp_lim) return R(0);
+    R delta_max = vel / time_fact;
+    if (delta_max < R(0)) {
+        if (pos >= low_lim && pos < low_lim - delta_max) return (low_lim - pos) / delta_max;
+        if (pos < low_lim) return R(0);
+        return R(1);
+    }
+    if (delta_max > R(0)) {
+        if (pos <= upp_lim && pos > upp_lim - delta_max) return (upp_lim - pos) / delta_max;
+        if (pos > upp_lim) return R(0);
+        return R(1);
+    }
+    return R(0);
+}
+
+// shared.rs:85-101 (euler_xyz: Bullet's matrixToEulerXYZ on column-major storage)
+template <class R>
+V3<R> euler_xyz(const M3<R>& m) {
+    const R half_pi = R(1.57079632679489661923);
+    R r20 = m.c0.z, r21 = m.c1.z, r22 = m.c2.z, r10 = m.c0.y, r11 = m.c1.y, r01 = m.c1.x, r00 = m.c0.x;
+    if (r20 < R(1)) {
+        if (r20 > R(-1)) return V3<R>(std::atan2(-r21, r22), std::asin(r20), std::atan2(-r10, r00));
+        return V3<R>(-std::atan2(r01, r11), -half_pi, R(0));
+    }
+    return V3<R>(std::atan2(r01, r11), half_pi, R(0));
+}
+
+// shared.rs:108-123 (relative_rotation_info)
+template <class R>
+void relative_rotation_info(const M3<R>& tr_a, const M3<R>& tr_b, V3<R>& euler, V3<R> axes[3]) {
+    M3<R> relative = tr_a.transpose() * tr_b;
+    euler = euler_xyz(relative);
+    V3<R> axis0 = tr_b.c0, axis2 = tr_a.c2;
+    axes[1] = axis2.cross(axis0);
+    axes[0] = axes[1].cross(axis2);
+    axes[2] = axis0.cross(axes[1]);
+    for (int i = 0; i < 3; ++i) axes[i] = axes[i].normalize();
+}
+
+// glam Quat::from_rotation_arc (published algorithm): identity for parallel unit vectors, a half
+// turn about any orthonormal vector for opposite ones, else normalize(from x to, 1 + from . to).
+template <class R>
+Quat<R> rotation_arc(const V3<R>& from, const V3<R>& to) {
+    const R eps = std::numeric_limits<R>::epsilon();
+    const R one_minus_eps = R(1) - R(2) * eps;
+    R d = from.dot(to);
+    if (d > one_minus_eps) return Quat<R>::identity();
+    if (d < -one_minus_eps) {
+        // A half turn about a vector orthonormal to `from` (Duff et al. 2017 branchless basis).
+        // Which of the two basis vectors glam picks is not pinned here: hinge frames of exactly
+        // opposite axes are outside the parity cases.
+        R sign = std::signbit(from.z) ? R(-1) : R(1);
+        R aa = R(-1) / (sign + from.z);
+        R bb = from.x * from.y * aa;
+        V3<R> o(bb, sign + from.y * from.y * aa, -from.y);
+        R half = R(3.14159265358979323846) * R(0.5);
+        R s = std::sin(half);
+        return Quat<R>(o.x * s, o.y * s, o.z * s, std::cos(half));
+    }
+    V3<R> c = from.cross(to);
+    return Quat<R>(c.x, c.y, c.z, R(1) + d).normalize();
+}
+
+// hinge.rs:60-100 (HingeConstraint::new): frames from pivots and axes.
+template <class R>
+void hinge_frames(const V3<R>& pivot_a, const V3<R>& axis_a_in, const V3<R>& pivot_b, const V3<R>& axis_b_in,
+                  JointFrame<R>& fa, JointFrame<R>& fb) {
+    V3<R> axis_a = axis_a_in.normalize(), axis_b = axis_b_in.normalize();
+    V3<R> helper = std::fabs(axis_a.x) < R(0.9) ? V3<R>(1, 0, 0) : V3<R>(0, 1, 0);
+    V3<R> t1 = axis_a.cross(helper).normalize();
+    V3<R> t2 = axis_a.cross(t1);
+    fa.origin = pivot_a;
+    fa.basis = M3<R>(t1, t2, axis_a);
+    Quat<R> rot = rotation_arc(axis_a, axis_b);
+    V3<R> t1b = rot.rotate(t1);
+    V3<R> t2b = axis_b.cross(t1b);
+    fb.origin = pivot_b;
+    fb.basis = M3<R>(t1b, t2b, axis_b);
+}
+
+// constraint.rs:755-842 + fixed.rs:33-90 + hinge.rs:130-267: the joint's rows for this step.
+template <class R, class B>
+void prepare_joint_rows(Joint<R>& jt, uint32_t jid, const std::vector<B>& bodies, R inv_dt, R erp,
+                        std::vector<JointRow<R>>& out) {
+    if (!jt.enabled) return;
+    const uint32_t ia = jt.body_a, ib = jt.body_b;
+    const B& a = bodies[ia];
+    const B& b = bodies[ib];
+    const size_t first = out.size();
+    auto push = [&](const V3<R>& la, const V3<R>& aa, const V3<R>& lb, const V3<R>& ab, R bias, uint32_t lim, R lo, R hi) {
+        out.push_back(prepare_joint_row(ia, ib, la, aa, lb, ab, a, b, bias, lim, lo, hi));
+    };
+    const V3<R> zero;
+    if (jt.kind == JOINT_POINT2POINT) {
+        V3<R> pivot_a = a.position + a.orientation.rotate(jt.frame_a.origin);
+        V3<R> pivot_b = b.position + b.orientation.rotate(jt.frame_b.origin);
+        V3<R> r_a = pivot_a - a.position, r_b = pivot_b - b.position;
+        R k = inv_dt * (jt.has_erp ? jt.erp : erp);
+        uint32_t lim = jt.impulse_clamp > R(0) ? LIM_BILATERAL : LIM_UNBOUNDED;
+        for (int axis = 0; axis < 3; ++axis) {
+            V3<R> n;
+            n.at(axis) = R(1);
+            push(n, r_a.cross(n), n, r_b.cross(n), k * (pivot_a - pivot_b)[axis], lim, -jt.impulse_clamp, jt.impulse_clamp);
+        }
+    } else if (jt.kind == JOINT_FIXED) {
+        M3<R> tr_a = M3<R>::from_quat(a.orientation) * jt.frame_a.basis;
+        M3<R> tr_b = M3<R>::from_quat(b.orientation) * jt.frame_b.basis;
+        V3<R> pivot_a = a.position + a.orientation.rotate(jt.frame_a.origin);
+        V3<R> pivot_b = b.position + b.orientation.rotate(jt.frame_b.origin);
+        V3<R> r_a = pivot_a - a.position, r_b = pivot_b - b.position;
+        R k = inv_dt * erp;
+        for (int axis = 0; axis < 3; ++axis) {
+            V3<R> n;
+            n.at(axis) = R(1);
+            push(n, r_a.cross(n), n, r_b.cross(n), k * (pivot_a - pivot_b)[axis], LIM_UNBOUNDED, 0, 0);
+        }
+        V3<R> euler, axes[3];
+        relative_rotation_info(tr_a, tr_b, euler, axes);
+        for (int i = 0; i < 3; ++i) push(zero, axes[i], zero, axes[i], k * euler[i], LIM_UNBOUNDED, 0, 0);
+    } else {  // hinge
+        M3<R> tr_a = M3<R>::from_quat(a.orientation) * jt.frame_a.basis;
+        M3<R> tr_b = M3<R>::from_quat(b.orientation) * jt.frame_b.basis;
+        V3<R> pivot_a = a.position + a.orientation.rotate(jt.frame_a.origin);
+        V3<R> pivot_b = b.position + b.orientation.rotate(jt.frame_b.origin);
+        V3<R> r_a = pivot_a - a.position, r_b = pivot_b - b.position;
+        V3<R> ax1 = tr_a.c2, p = tr_a.c0, q = tr_a.c1, ax2 = tr_b.c2;
+        R k = inv_dt * erp;
+        if (!jt.angular_only) {
+            for (int axis = 0; axis < 3; ++axis) {
+                V3<R> n;
+                n.at(axis) = R(1);
+                push(n, r_a.cross(n), n, r_b.cross(n), k * (pivot_a - pivot_b)[axis], LIM_UNBOUNDED, 0, 0);
+            }
+        }
+        V3<R> u = ax1.cross(ax2);
+        push(zero, p, zero, p, -k * u.dot(p), LIM_UNBOUNDED, 0, 0);
+        push(zero, q, zero, q, -k * u.dot(q), LIM_UNBOUNDED, 0, 0);
+        jt.hinge_angle = hinge_angle_of(tr_a, tr_b);
+        R correction = 0, sign = 0;
+        bool solve = false;
+        if (jt.has_limit) limit_test(jt.limit, jt.hinge_angle, correction, sign, solve);
+        const bool powered = jt.has_motor;
+        if (solve || powered) {
+            R row_error = 0;
+            R lostop = jt.has_limit ? jt.limit.low : R(1);
+            R histop = jt.has_limit ? jt.limit.high : R(-1);
+            bool motor_ineffective = solve && lostop == histop;
+            if (powered && !motor_ineffective) {
+                R mf = motor_factor(jt.hinge_angle, lostop, histop, jt.motor_target, inv_dt * erp);
+                row_error += mf * jt.motor_target;
+            }
+            if (solve) {
+                row_error += k * correction;
+                R bounce = jt.has_limit ? jt.limit.relaxation : R(1);
+                if (bounce > R(0)) {
+                    R vel = a.angular_velocity.dot(ax1) - b.angular_velocity.dot(ax1);
+                    if (sign > R(0)) {
+                        if (vel < R(0)) {
+                            R newc = -bounce * vel;
+                            if (newc > row_error) row_error = newc;
+                        }
+                    } else if (vel > R(0)) {
+                        R newc = -bounce * vel;
+                        if (newc < row_error) row_error = newc;
+                    }
+                }
+                row_error *= jt.has_limit ? jt.limit.bias_factor : R(1);
+            }
+            uint32_t lim;
+            R lo = 0, hi = 0;
+            if (solve) {
+                if (lostop == histop) lim = LIM_UNBOUNDED;
+                else if (sign > R(0)) { lim = LIM_UPPER; hi = 0; }
+                else { lim = LIM_LOWER; lo = 0; }
+            } else {
+                lim = LIM_BILATERAL;
+                hi = jt.has_motor ? jt.motor_max : R(0);
+                lo = -hi;
+            }
+            push(zero, ax1, zero, ax1, -row_error, lim, lo, hi);
+        }
+    }
+    for (size_t r = first; r < out.size(); ++r) out[r].joint = jid;
+}
+
+}  // namespace oracle

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <map>
 #include <unordered_map>
+#include "oracle_joints.hpp"
 #include "oracle_narrow.hpp"
 
 namespace oracle {
@@ -411,9 +412,11 @@ void solve_contact(std::vector<Body<R>>& bodies, ContactConstraint<R>& c, R inv_
     }
 }
 
-// sequential_impulse.rs:692-802
+// sequential_impulse.rs:692-802; each velocity sweep solves the contacts, then the joint rows
+// (sequential_impulse.rs:720-735); joint rows take no warm start and no split pass.
 template <class R>
-void solve(std::vector<Body<R>>& bodies, std::vector<ContactConstraint<R>>& cs, R inv_dt, const SolverInfo<R>& info) {
+void solve(std::vector<Body<R>>& bodies, std::vector<ContactConstraint<R>>& cs, R inv_dt, const SolverInfo<R>& info,
+           std::vector<JointRow<R>>* joint_rows = nullptr) {
     for (auto& c : cs) {  // warm_start :710-717
         Body<R>& a = bodies[c.body_a];
         Body<R>& b = bodies[c.body_b];
@@ -421,8 +424,11 @@ void solve(std::vector<Body<R>>& bodies, std::vector<ContactConstraint<R>>& cs, 
         apply_impulse(a, b, c, c.tangent1, c.ang_t1_a, c.ang_t1_b, c.tangent1_impulse);
         apply_impulse(a, b, c, c.tangent2, c.ang_t2_a, c.ang_t2_b, c.tangent2_impulse);
     }
-    for (uint32_t it = 0; it < info.num_iterations; ++it)
+    for (uint32_t it = 0; it < info.num_iterations; ++it) {
         for (auto& c : cs) solve_contact(bodies, c, inv_dt, info);
+        if (joint_rows)
+            for (auto& jr : *joint_rows) solve_joint_row(bodies, jr, info.damping);
+    }
     for (auto& c : cs)
         if (c.split_active) c.rhs_penetration = c.penetration * c.erp * inv_dt * c.normal_mass;
     for (uint32_t it = 0; it < info.num_iterations; ++it) {
@@ -616,6 +622,11 @@ struct World {
     // Empty = the reference's pair order.
     std::vector<uint64_t> solve_order;
 
+    // Joints (constraint.rs) and the order their rows are solved in (empty: index order).
+    std::vector<Joint<R>> joints;
+    std::vector<uint32_t> joint_order;
+    std::vector<JointRow<R>> last_joint_rows;
+
     // Snapshots of the last step (for parity checks).
     std::vector<std::pair<uint32_t, uint32_t>> last_pairs;
     std::vector<ContactConstraint<R>> last_rows;     // after the solve, in solve order
@@ -676,6 +687,11 @@ struct World {
             if ((a.flags | b.flags) & CF_NO_CONTACT_RESPONSE) continue;
             if ((a.group & b.mask) == 0 || (b.group & a.mask) == 0) continue;
             if (a.participates_in_islands() && b.participates_in_islands()) uf.unite(p.first, p.second);
+        }
+        for (auto& jt : joints) {  // islands.rs:186-196: enabled joints between two dynamic bodies
+            if (!jt.enabled) continue;
+            if (bodies[jt.body_a].participates_in_islands() && bodies[jt.body_b].participates_in_islands())
+                uf.unite(jt.body_a, jt.body_b);
         }
         for (size_t i = 0; i < n; ++i)
             if (bodies[i].participates_in_islands() && bodies[i].is_island_awake()) island_awake[uf.find(i)] = 1;
@@ -759,6 +775,12 @@ struct World {
         std::vector<ContactConstraint<R>> rows;
         std::vector<ContactPoint<R>> refresh_out;
         const R REDETECT_SPEED_SQUARED = R(0.08) * R(0.08);  // world.rs:62
+        // world.rs:873-880 + step.rs:645-651: pairs linked by a joint with disable_collisions
+        // (enabled or not) are skipped like group/mask rejects.
+        std::vector<uint64_t> suppressed;
+        for (auto& jt : joints)
+            if (jt.disable_collisions) suppressed.push_back(pair_key(jt.body_a, jt.body_b));
+        std::sort(suppressed.begin(), suppressed.end());
         last_narrowphase_calls = 0;
         for (auto& pr : pairs) {
             uint32_t i = pr.first, j = pr.second;
@@ -766,6 +788,7 @@ struct World {
             Body<R>& b = bodies[j];
             if ((a.group & b.mask) == 0 || (b.group & a.mask) == 0) continue;
             uint64_t key = pair_key(i, j);
+            if (!suppressed.empty() && std::binary_search(suppressed.begin(), suppressed.end(), key)) continue;
             auto it = cache.find(key);
             if (simulate && it != cache.end()) it->second.touched = stamp;
             if (!a.is_active() && !b.is_active()) continue;
@@ -812,9 +835,19 @@ struct World {
             });
         }
         last_rows_pre = rows;
+        // 5a. joint rows from the current poses (step.rs:928-949): joints of a sleeping island
+        // (both bodies inactive) produce none.
+        std::vector<JointRow<R>> jrows;
+        for (size_t o = 0; o < joints.size(); ++o) {
+            uint32_t jid = joint_order.empty() ? uint32_t(o) : joint_order[o];
+            Joint<R>& jt = joints[jid];
+            if (!bodies[jt.body_a].is_active() && !bodies[jt.body_b].is_active()) continue;
+            prepare_joint_rows(jt, jid, bodies, inv_dt, info.erp, jrows);
+        }
         clk_mark(4);
         // 6. solve (step.rs:959-972)
-        solve(bodies, rows, inv_dt, info);
+        solve(bodies, rows, inv_dt, info, &jrows);
+        last_joint_rows = jrows;
         // 6b. impulse writeback + prune (step.rs:982-1010)
         for (auto& c : rows) {
             auto ci = cache.find(pair_key(c.body_a, c.body_b));

@@ -68,6 +68,12 @@ def lib():
             "orc_pm_set_impulse": (None, [P, U32, ctypes.c_double]),
             "orc_pm_points": (U32, [P, D]),
             "orc_interpolate_pose": (None, [ctypes.c_int, D, ctypes.c_double, D]),
+            "orc_world_add_joint": (U32, [P, D]),
+            "orc_world_set_joint_order": (None, [P, ctypes.POINTER(U32), U32]),
+            "orc_world_joint_angles": (None, [P, D]),
+            "orc_world_num_joint_rows": (U32, [P]),
+            "orc_world_joint_rows": (None, [P, D]),
+            "orc_hinge_frames": (None, [ctypes.c_int, D, D, D, D, D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -109,6 +115,39 @@ def body_desc(shape, pos, quat=(0, 0, 0, 1), linvel=(0, 0, 0), angvel=(0, 0, 0),
     d[22] = activation
     d[23] = kinematic
     return d
+
+
+JDESC = 37   # joint descriptor doubles (orc_world_add_joint)
+JOINT_POINT2POINT, JOINT_FIXED, JOINT_HINGE = 0, 1, 2
+JF_DISABLE_COLLISIONS, JF_DISABLED, JF_ANGULAR_ONLY, JF_LIMIT, JF_MOTOR, JF_ERP = 1, 2, 4, 8, 16, 32
+
+
+def joint_desc(kind, body_a, body_b, frame_a, frame_b, flags=JF_DISABLE_COLLISIONS, erp=0.0, impulse_clamp=0.0,
+               limit=(1.0, -1.0), softness=0.9, bias_factor=0.3, relaxation=1.0, motor=(0.0, 0.0)):
+    """frame_*: 12 numbers (origin xyz, basis columns x, y, z) in the body's frame."""
+    d = np.zeros(JDESC)
+    d[0], d[1], d[2], d[3] = kind, body_a, body_b, flags
+    d[4:16] = frame_a
+    d[16:28] = frame_b
+    d[28], d[29] = erp, impulse_clamp
+    d[30], d[31] = limit
+    d[32], d[33], d[34] = softness, bias_factor, relaxation
+    d[35], d[36] = motor
+    return d
+
+
+def frame(origin, basis=np.eye(3)):
+    """origin + basis (columns) as the 12 numbers of a joint descriptor frame."""
+    b = np.asarray(basis, dtype=np.float64)
+    return np.concatenate([np.asarray(origin, dtype=np.float64), b[:, 0], b[:, 1], b[:, 2]])
+
+
+def hinge_frames(pivot_a, axis_a, pivot_b, axis_b, precision="f32"):
+    """hinge.rs:60-100: the two hinge frames (12 numbers each) from pivots and axes."""
+    out = np.zeros(24)
+    lib().orc_hinge_frames(1 if precision == "f64" else 0, dptr(f64(pivot_a)), dptr(f64(axis_a)), dptr(f64(pivot_b)),
+                           dptr(f64(axis_b)), dptr(out))
+    return out[:12], out[12:]
 
 
 class OracleWorld:
@@ -226,6 +265,25 @@ class OracleWorld:
     def stage_seconds(self):
         out = np.zeros(7)
         self.L.orc_world_stage_seconds(self.h, dptr(out))
+        return out
+
+    def add_joint(self, desc):
+        return self.L.orc_world_add_joint(self.h, dptr(f64(desc)))
+
+    def set_joint_order(self, ids):
+        a = np.ascontiguousarray(ids, dtype=np.uint32)
+        self.L.orc_world_set_joint_order(self.h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(a))
+
+    def joint_angles(self, n):
+        out = np.zeros(n)
+        self.L.orc_world_joint_angles(self.h, dptr(out))
+        return out
+
+    def joint_rows(self):
+        n = self.L.orc_world_num_joint_rows(self.h)
+        out = np.zeros((n, 8))
+        if n:
+            self.L.orc_world_joint_rows(self.h, dptr(out))
         return out
 
     def set_solve_order(self, keys):

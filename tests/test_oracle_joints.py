@@ -1,0 +1,262 @@
+"""Oracle joints pinned by the reference's own joint tests.
+
+Each case restates the scene and the assertions of a test in
+crates/bullet-dynamics/src/constraint/tests.rs (point-to-point, hinge and fixed
+joints; the line of each test is cited), run through the oracle's full step in
+both precisions.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle_api as orc
+
+DT = 1.0 / 60.0
+PRECISIONS = ["f32", "f64"]
+
+
+def quat_z(a):  # Quaternion::from_rotation_z
+    return (0.0, 0.0, math.sin(a / 2), math.cos(a / 2))
+
+
+def rotate(q, v):
+    x, y, z, w = q
+    b = np.array([x, y, z])
+    v = np.asarray(v, dtype=np.float64)
+    return v * (w * w - b @ b) + b * (2 * (v @ b)) + np.cross(b, v) * (2 * w)
+
+
+def quat_angle(q):  # conetwist.rs:546-548
+    return 2.0 * math.acos(max(-1.0, min(1.0, q[3])))
+
+
+def qmul(a, b):
+    ax, ay, az, aw = a
+    bx, by, bz, bw = b
+    return (aw * bx + ax * bw + ay * bz - az * by, aw * by - ax * bz + ay * bw + az * bx,
+            aw * bz + ax * by - ay * bx + az * bw, aw * bw - ax * bx - ay * by - az * bz)
+
+
+def world(precision, gravity=(0.0, -9.81, 0.0)):
+    w = orc.OracleWorld(precision)
+    w.set_gravity(gravity)
+    return w
+
+
+def p2p(w, a, b, pivot_a, pivot_b, **kw):
+    return w.add_joint(orc.joint_desc(orc.JOINT_POINT2POINT, a, b, orc.frame(pivot_a), orc.frame(pivot_b), **kw))
+
+
+def pendulum(precision, bob_offset, anchor_offset):
+    w = world(precision)
+    anchor_shape = w.add_shape(orc.BOX, [0.2, 0.2, 0.2])
+    bob_shape = w.add_shape(orc.SPHERE, [0.1])
+    anchor = w.add_body(anchor_shape, (0, 0, 0), mass=0.0)
+    bob = w.add_body(bob_shape, tuple(np.subtract(anchor_offset, bob_offset)), mass=1.0)
+    p2p(w, bob, anchor, bob_offset, anchor_offset)
+    return w, bob
+
+
+def set_pose(w, i, pos=None, quat=None, linvel=None, angvel=None):
+    st = w.state()
+    if pos is not None:
+        st[i, 0:3] = pos
+    if quat is not None:
+        st[i, 3:7] = quat
+    if linvel is not None:
+        st[i, 7:10] = linvel
+    if angvel is not None:
+        st[i, 10:13] = angvel
+    w.set_state(st)
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_pendulum_swings_and_keeps_the_pivot(precision):  # tests.rs:46-91
+    w, bob = pendulum(precision, (-1.0, 0.0, 0.0), (0.0, 0.0, 0.0))
+    a45 = math.pi / 4
+    set_pose(w, bob, pos=(math.sin(a45), -math.cos(a45), 0.0), quat=quat_z(-a45))
+    max_err, min_x, max_speed, crossings = 0.0, math.inf, 0.0, 0
+    prev_x = w.state()[bob, 0]
+    for _ in range(600):
+        w.step(DT)
+        s = w.state()[bob]
+        max_err = max(max_err, float(np.linalg.norm(s[0:3] + rotate(s[3:7], (-1.0, 0.0, 0.0)))))
+        min_x = min(min_x, s[0])
+        max_speed = max(max_speed, float(np.linalg.norm(s[7:10])))
+        if prev_x > 0.0 and s[0] <= 0.0:
+            crossings += 1
+        prev_x = s[0]
+    assert max_err < 0.2 and crossings >= 3 and min_x < -0.5 and max_speed > 1.5
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_pendulum_hangs_at_equilibrium(precision):  # tests.rs:94-121
+    w, bob = pendulum(precision, (0.0, 1.0, 0.0), (0.0, 1.0, 0.0))
+    for _ in range(600):
+        w.step(DT)
+    s = w.state()[bob]
+    pivot = s[0:3] + rotate(s[3:7], (0.0, 1.0, 0.0))
+    assert np.linalg.norm(pivot - (0.0, 1.0, 0.0)) < 0.01
+    assert np.linalg.norm(s[0:3]) < 0.02
+    assert np.linalg.norm(s[7:10]) < 0.05
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_two_link_chain_keeps_its_lengths(precision):  # tests.rs:124-176
+    w = world(precision)
+    anchor = w.add_body(w.add_shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+    sph = w.add_shape(orc.SPHERE, [0.1])
+    upper = w.add_body(sph, (0.0, -1.0, 0.0), mass=1.0)
+    lower = w.add_body(sph, (0.0, -3.0, 0.0), mass=1.0)
+    p2p(w, upper, anchor, (0.0, 1.0, 0.0), (0.0, 0.0, 0.0))
+    p2p(w, lower, upper, (0.0, 1.0, 0.0), (0.0, -1.0, 0.0))
+    set_pose(w, lower, linvel=(2.0, 0.0, 0.0))
+    max_err = 0.0
+    for _ in range(300):
+        w.step(DT)
+        s = w.state()
+        u, l = s[upper], s[lower]
+        max_err = max(max_err, float(np.linalg.norm(u[0:3] + rotate(u[3:7], (0, 1, 0)))),
+                      float(np.linalg.norm(l[0:3] + rotate(l[3:7], (0, 1, 0)) - (u[0:3] + rotate(u[3:7], (0, -1, 0))))))
+    assert max_err < 0.2
+
+
+def door_world(precision, gravity=(0.0, -9.81, 0.0), door_pos=(0.0, 0.5, 0.0), open_45=True):
+    w = world(precision, gravity)
+    anchor = w.add_body(w.add_shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+    door = w.add_body(w.add_shape(orc.BOX, [0.5, 0.5, 0.2]), door_pos, mass=2.0)
+    if open_45:
+        a45 = math.pi / 4
+        set_pose(w, door, pos=(math.cos(a45) * 0.5, math.sin(a45) * 0.5, 0.0), quat=quat_z(a45))
+    fa, fb = orc.hinge_frames((-0.5, 0.0, 0.0), (0, 0, 1), (0, 0, 0), (0, 0, 1), precision)
+    return w, door, anchor, fa, fb
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_hinge_swings_and_keeps_axis_aligned(precision):  # tests.rs:180-235
+    w, door, anchor, fa, fb = door_world(precision)
+    w.add_joint(orc.joint_desc(orc.JOINT_HINGE, door, anchor, fa, fb))
+    max_pivot, min_align, max_angle, crossings, prev = 0.0, 1.0, 0.0, 0, 0.0
+    for step in range(600):
+        w.step(DT)
+        d = w.state()[door]
+        max_pivot = max(max_pivot, float(np.linalg.norm(d[0:3] + rotate(d[3:7], (-0.5, 0.0, 0.0)))))
+        min_align = min(min_align, abs(rotate(d[3:7], (0, 0, 1))[2]))
+        angle = w.joint_angles(1)[0]
+        max_angle = max(max_angle, abs(angle))
+        if step > 0 and prev > 0.0 and angle <= 0.0:
+            crossings += 1
+        prev = angle
+    assert max_pivot < 0.2 and min_align > 0.99 and max_angle > 0.5 and crossings >= 3
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_hinge_limit_stops_the_door(precision):  # tests.rs:238-281
+    w, door, anchor, fa, fb = door_world(precision, door_pos=(0.0, 0.0, 0.0))
+    w.add_joint(orc.joint_desc(orc.JOINT_HINGE, door, anchor, fa, fb,
+                               flags=orc.JF_DISABLE_COLLISIONS | orc.JF_LIMIT, limit=(-0.3, 0.3)))
+    min_angle = 0.0
+    for _ in range(600):
+        w.step(DT)
+        min_angle = min(min_angle, w.joint_angles(1)[0])
+    assert min_angle > -0.35
+    assert abs(w.joint_angles(1)[0] + 0.3) < 0.05
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_hinge_motor_rotates_the_door(precision):  # tests.rs:284-316
+    w, door, anchor, fa, fb = door_world(precision, gravity=(0.0, 0.0, 0.0), door_pos=(0.5, 0.0, 0.0), open_45=False)
+    w.add_joint(orc.joint_desc(orc.JOINT_HINGE, door, anchor, fa, fb,
+                               flags=orc.JF_DISABLE_COLLISIONS | orc.JF_MOTOR, motor=(1.0, 1000.0)))
+    for _ in range(180):
+        w.step(DT)
+    assert abs(w.joint_angles(1)[0] - 3.0) < 1.0
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_joint_suppresses_collisions_between_linked_bodies(precision):  # tests.rs:320-360
+    def run(with_joint):
+        w = world(precision, (0.0, 0.0, 0.0))
+        box = w.add_shape(orc.BOX, [0.5, 0.5, 0.5])
+        a = w.add_body(box, (0, 0, 0), mass=1.0)
+        b = w.add_body(box, (0, 0, 0), mass=1.0)
+        if with_joint:
+            p2p(w, a, b, (0, 0, 0), (0, 0, 0))
+        for _ in range(30):
+            w.step(DT)
+        s = w.state()
+        return s[b, 0:3] - s[a, 0:3]
+
+    assert np.linalg.norm(run(False)) > 0.05
+    assert np.linalg.norm(run(True)) < 0.02
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_impulse_clamp_limits_the_support_impulse(precision):  # tests.rs:363-400
+    def run(clamp):
+        w = world(precision)
+        anchor = w.add_body(w.add_shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+        bob = w.add_body(w.add_shape(orc.SPHERE, [0.1]), (0, 0, 0), mass=10.0)
+        p2p(w, bob, anchor, (0, 0, 0), (0, 0, 0), impulse_clamp=clamp)
+        for _ in range(300):
+            w.step(DT)
+        return w.state()[bob, 1]
+
+    assert run(0.1) < -1.0
+    assert abs(run(0.0)) < 0.05
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_fixed_joint_locks_a_rigid_assembly(precision):  # tests.rs:403-458
+    w = world(precision)
+    anchor = w.add_body(w.add_shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+    box = w.add_body(w.add_shape(orc.BOX, [0.3, 0.3, 0.3]), (0.0, 1.0, 0.0), mass=1.0)
+    w.add_joint(orc.joint_desc(orc.JOINT_FIXED, box, anchor, orc.frame((0.0, 0.5, 0.0)), orc.frame((0.0, 1.5, 0.0))))
+    set_pose(w, box, linvel=(2.0, 0.0, 0.0), angvel=(0.0, 0.0, 4.0))
+    max_rel = 0.0
+    for _ in range(600):
+        w.step(DT)
+        max_rel = max(max_rel, quat_angle(w.state()[box, 3:7]))
+    b = w.state()[box]
+    assert max_rel < 0.5
+    assert np.linalg.norm(b[0:3] - (0.0, 1.0, 0.0)) < 0.03
+    assert np.linalg.norm(b[10:13]) < 0.05
+    assert np.linalg.norm(b[0:3] + rotate(b[3:7], (0.0, 0.5, 0.0)) - (0.0, 1.5, 0.0)) < 0.03
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_fixed_joint_welds_two_dynamic_bodies(precision):  # tests.rs:461-515
+    w = world(precision)
+    w.add_body(w.add_shape(orc.PLANE, [0.0, 1.0, 0.0, 0.0]), (0, 0, 0), mass=0.0)
+    box = w.add_shape(orc.BOX, [0.4, 0.4, 0.4])
+    a = w.add_body(box, (0.0, 1.2, 0.0), mass=1.0)
+    b = w.add_body(box, (0.0, 1.6, 0.0), mass=1.0)
+    w.add_joint(orc.joint_desc(orc.JOINT_FIXED, a, b, orc.frame((0.0, 0.2, 0.0)), orc.frame((0.0, -0.2, 0.0))))
+    set_pose(w, a, angvel=(1.0, 2.0, 0.0))
+    set_pose(w, b, angvel=(1.0, 2.0, 0.0))
+    max_rel, max_pivot = 0.0, 0.0
+    for _ in range(300):
+        w.step(DT)
+        s = w.state()
+        qa, qb = s[a, 3:7], s[b, 3:7]
+        rel = qmul((-qb[0], -qb[1], -qb[2], qb[3]), tuple(qa))
+        max_rel = max(max_rel, quat_angle(rel))
+        pa = s[a, 0:3] + rotate(qa, (0.0, 0.2, 0.0))
+        pb = s[b, 0:3] + rotate(qb, (0.0, -0.2, 0.0))
+        max_pivot = max(max_pivot, float(np.linalg.norm(pb - pa)))
+    assert max_rel < 0.15 and max_pivot < 0.15
+
+
+def test_hinge_frames_follow_the_pivot_axis_recipe():  # hinge.rs:60-100
+    fa, fb = orc.hinge_frames((1.0, 2.0, 3.0), (0.0, 0.0, 2.0), (-1.0, 0.0, 0.5), (0.0, 1.0, 0.0), "f64")
+    ba = fa[3:].reshape(3, 3).T
+    bb = fb[3:].reshape(3, 3).T
+    np.testing.assert_allclose(fa[:3], (1.0, 2.0, 3.0))
+    np.testing.assert_allclose(ba[:, 2], (0.0, 0.0, 1.0), atol=1e-12)
+    np.testing.assert_allclose(bb[:, 2], (0.0, 1.0, 0.0), atol=1e-12)
+    for basis in (ba, bb):  # orthonormal, right-handed
+        np.testing.assert_allclose(basis.T @ basis, np.eye(3), atol=1e-12)
+        assert np.linalg.det(basis) == pytest.approx(1.0)
+    # t1 = axis x (X when |axis.x| < 0.9), normalized; frame B's X is t1 carried by the shortest arc
+    np.testing.assert_allclose(ba[:, 0], (0.0, 1.0, 0.0), atol=1e-12)
