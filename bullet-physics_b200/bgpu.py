@@ -13,6 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libbgpu.so")
 
 SPHERE, BOX, CAPSULE, HULL, PLANE = 0, 1, 2, 3, 4
+JOINT_POINT2POINT, JOINT_FIXED, JOINT_HINGE = 0, 1, 2
+JOINT_DISABLE_COLLISIONS, JOINT_DISABLED, JOINT_ANGULAR_ONLY, JOINT_LIMIT, JOINT_MOTOR, JOINT_ERP = 1, 2, 4, 8, 16, 32
 NO_CONTACT_RESPONSE, DISABLE_WORLD_GRAVITY, KINEMATIC, ADDITIONAL_DAMPING = 0x1, 0x2, 0x4, 0x10
 STATE = 15
 CONTACT = 18
@@ -23,7 +25,16 @@ class SolverInfo(ctypes.Structure):
                 ("restitution_velocity_threshold", ctypes.c_float), ("split_impulse", ctypes.c_uint32),
                 ("split_impulse_penetration_threshold", ctypes.c_float), ("split_impulse_turn_erp", ctypes.c_float),
                 ("warmstarting_factor", ctypes.c_float), ("global_cfm", ctypes.c_float), ("sor", ctypes.c_float),
-                ("num_iterations", ctypes.c_uint32)]
+                ("num_iterations", ctypes.c_uint32), ("erp", ctypes.c_float), ("damping", ctypes.c_float)]
+
+
+class JointDesc(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_uint32), ("body_a", ctypes.c_uint32), ("body_b", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32), ("frame_a", ctypes.c_float * 12), ("frame_b", ctypes.c_float * 12),
+                ("erp", ctypes.c_float), ("impulse_clamp", ctypes.c_float), ("limit_low", ctypes.c_float),
+                ("limit_high", ctypes.c_float), ("limit_softness", ctypes.c_float),
+                ("limit_bias_factor", ctypes.c_float), ("limit_relaxation", ctypes.c_float),
+                ("motor_target_velocity", ctypes.c_float), ("motor_max_impulse", ctypes.c_float)]
 
 
 class BodyDesc(ctypes.Structure):
@@ -93,6 +104,12 @@ def lib():
             "bgpu_read_solve_order": (S, [P, U64P, ctypes.c_uint64, U64P]),
             "bgpu_read_colour_batches": (S, [P, U32P, U32P, U32, U32P]),
             "bgpu_selftest_wait_timeout": (S, [U32, U32P, F]),
+            "bgpu_joint_desc_default": (None, [ctypes.POINTER(JointDesc)]),
+            "bgpu_add_joints": (S, [P, U32, ctypes.POINTER(JointDesc), U32P]),
+            "bgpu_num_joints": (U32, [P]),
+            "bgpu_read_joint_angles": (S, [P, F]),
+            "bgpu_read_joint_order": (S, [P, U32P, U32, U32P]),
+            "bgpu_read_joint_rows": (S, [P, F, U32, U32P]),
             "bgpu_get_stats": (S, [P, ctypes.POINTER(StepStats)]),
             "bgpu_enable_step_timing": (S, [P, ctypes.c_int]),
             "bgpu_broadphase_pairs": (S, [F, U32, U32P, ctypes.c_uint64, U64P]),
@@ -368,6 +385,50 @@ class World:
         out = np.zeros(n.value, dtype=np.uint64)
         if n.value:
             check(self.L.bgpu_read_solve_order(self.h, u64ptr(out), n.value, ctypes.byref(n)), "read_solve_order")
+        return out
+
+    def add_joint(self, kind, body_a, body_b, frame_a, frame_b, flags=JOINT_DISABLE_COLLISIONS, erp=0.0,
+                  impulse_clamp=0.0, limit=(1.0, -1.0), softness=0.9, bias_factor=0.3, relaxation=1.0,
+                  motor=(0.0, 0.0)):
+        """frame_*: 12 numbers (pivot xyz, basis columns x, y, z) in the body's frame."""
+        d = JointDesc()
+        self.L.bgpu_joint_desc_default(ctypes.byref(d))
+        d.kind, d.body_a, d.body_b, d.flags = kind, body_a, body_b, flags
+        d.frame_a[:] = [float(x) for x in frame_a]
+        d.frame_b[:] = [float(x) for x in frame_b]
+        d.erp, d.impulse_clamp = erp, impulse_clamp
+        d.limit_low, d.limit_high = limit
+        d.limit_softness, d.limit_bias_factor, d.limit_relaxation = softness, bias_factor, relaxation
+        d.motor_target_velocity, d.motor_max_impulse = motor
+        first = ctypes.c_uint32()
+        check(self.L.bgpu_add_joints(self.h, 1, ctypes.byref(d), ctypes.byref(first)), "add_joints")
+        return first.value
+
+    @property
+    def num_joints(self):
+        return self.L.bgpu_num_joints(self.h)
+
+    def joint_angles(self):
+        out = np.zeros(self.num_joints, dtype=np.float32)
+        if len(out):
+            check(self.L.bgpu_read_joint_angles(self.h, fptr(out)), "read_joint_angles")
+        return out
+
+    def joint_order(self):
+        n = ctypes.c_uint32()
+        check(self.L.bgpu_read_joint_order(self.h, None, 0, ctypes.byref(n)), "read_joint_order")
+        out = np.zeros(n.value, dtype=np.uint32)
+        if n.value:
+            check(self.L.bgpu_read_joint_order(self.h, u32ptr(out), n.value, ctypes.byref(n)), "read_joint_order")
+        return out
+
+    def joint_rows(self):
+        """Rows of the last step in solve order: joint, body_a, body_b, mass, bias, limit kind, impulse, 0."""
+        n = ctypes.c_uint32()
+        check(self.L.bgpu_read_joint_rows(self.h, None, 0, ctypes.byref(n)), "read_joint_rows")
+        out = np.zeros((n.value, 8), dtype=np.float32)
+        if n.value:
+            check(self.L.bgpu_read_joint_rows(self.h, fptr(out), n.value, ctypes.byref(n)), "read_joint_rows")
         return out
 
     def colour_batches(self):

@@ -13,7 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libbgpu.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["k_body.cu", "k_broadphase.cu", "k_islands.cu", "k_pairs.cu", "k_solver.cu", "k_adjoint.cu", "world.cu"]
+SOURCES = ["k_body.cu", "k_broadphase.cu", "k_islands.cu", "k_pairs.cu", "k_solver.cu", "k_adjoint.cu", "k_joints.cu",
+           "world.cu"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [

@@ -189,18 +189,94 @@ struct Broadphase {
 };
 
 // ---------------------------------------------------------------- islands (k_islands.cu)
+// ---------------------------------------------------------------- joints (k_joints.cu)
+// Joint descriptor on the device, JOINT_F4 float4 per joint id: [0] kind, body a, body b,
+// flags (as bits); [1] frame A origin; [2..4] frame A basis columns; [5] frame B origin;
+// [6..8] frame B basis columns; [9] erp, impulse clamp, limit low, limit high;
+// [10] softness, bias factor, relaxation, motor target velocity; [11] motor max impulse.
+constexpr uint32_t JOINT_F4 = 12;
+constexpr uint32_t JOINT_MAX_ROWS = 6;
+// Joint row, JROW_F4 float4: [0] lin_a | effective mass, [1] ang_a | bias, [2] lin_b | cfm,
+// [3] ang_b | limit kind (bits), [4] lower, upper, accumulated impulse, 0.
+constexpr uint32_t JROW_F4 = 5;
+enum : uint32_t { JK_POINT2POINT = 0, JK_FIXED = 1, JK_HINGE = 2 };
+enum : uint32_t { JF_DISABLE_COLLISIONS = 1u, JF_DISABLED = 2u, JF_ANGULAR_ONLY = 4u, JF_LIMIT = 8u, JF_MOTOR = 16u, JF_ERP = 32u };
+enum : uint32_t { JL_UNBOUNDED = 0, JL_BILATERAL = 1, JL_LOWER = 2, JL_UPPER = 3 };
+
+struct JointsDev {
+    const float4* desc = nullptr;    // JOINT_F4 per joint id
+    const uint32_t* order = nullptr; // solve slot -> joint id (joint colour by colour)
+    const uint32_t* coff = nullptr;  // joint colour c owns slots [coff[c], coff[c + 1])
+    uint32_t n = 0, ncol = 0;
+    float4* rows = nullptr;          // JOINT_MAX_ROWS rows of JROW_F4 per slot
+    uint32_t* count = nullptr;       // rows per slot this step
+    float* angle = nullptr;          // hinge angle per joint id
+};
+
+// Rows of every joint for this step, from the current poses (constraint.rs:755-842).
+void launch_joint_rows(const BodyDev& b, const JointsDev& j, float inv_dt, float erp, cudaStream_t s);
+
+// solve_joint_row (sequential_impulse.rs:931-971) over the rows of one joint slot; the
+// two bodies' velocities come from and go back to L2 (dynamic bodies only).
+__device__ __forceinline__ void solve_joint_slot(const JointsDev& jd, uint32_t t, float4* linvel, float4* angvel,
+                                                 const float4* __restrict__ iw, float damping) {
+    const uint32_t cnt = jd.count[t];
+    if (!cnt) return;
+    const uint32_t jid = jd.order[t];
+    const float4 h = jd.desc[size_t(jid) * JOINT_F4];
+    const uint32_t ia = __float_as_uint(h.y), ib = __float_as_uint(h.z);
+    auto load_iw_j = [&](uint32_t i, float& im) {
+        const float4 x = iw[3 * i], y = iw[3 * i + 1], z = iw[3 * i + 2];
+        im = z.y;
+        return M3{V3{x.x, x.y, x.z}, V3{x.w, y.x, y.y}, V3{y.z, y.w, z.x}};
+    };
+    float ima, imb;
+    const M3 iia = load_iw_j(ia, ima), iib = load_iw_j(ib, imb);
+    V3 la = from4(__ldcg(&linvel[ia])), wa = from4(__ldcg(&angvel[ia]));
+    V3 lb = from4(__ldcg(&linvel[ib])), wb = from4(__ldcg(&angvel[ib]));
+    float4* row = jd.rows + size_t(t) * JOINT_MAX_ROWS * JROW_F4;
+    for (uint32_t r = 0; r < cnt; ++r, row += JROW_F4) {
+        const float4 r0 = row[0], r1 = row[1], r2 = row[2], r3 = row[3], r4 = row[4];
+        const V3 lin_a = from4(r0), ang_a = from4(r1), lin_b = from4(r2), ang_b = from4(r3);
+        const float mass = r0.w, bias = r1.w, cfm = r2.w;
+        const uint32_t lim = __float_as_uint(r3.w);
+        const float row_vel = (dot(lin_b, lb) + dot(ang_b, wb)) - (dot(lin_a, la) + dot(ang_a, wa));
+        const float old = r4.z;
+        const float base = damping != 1.0f ? mass * (bias - row_vel * damping) : mass * (bias - row_vel);
+        const float lambda = cfm != 0.0f ? base - cfm * old : base;
+        float nw = old + lambda;
+        if (lim == JL_BILATERAL) nw = fminf(fmaxf(nw, -r4.y), r4.y);
+        else if (lim == JL_LOWER) nw = fmaxf(nw, r4.x);
+        else if (lim == JL_UPPER) nw = fminf(nw, r4.y);
+        row[4] = make_float4(r4.x, r4.y, nw, 0.0f);
+        const float j = nw - old;
+        if (j != 0.0f) {
+            la -= lin_a * (j * ima);
+            lb += lin_b * (j * imb);
+            wa -= mul(iia, ang_a * j);
+            wb += mul(iib, ang_b * j);
+        }
+    }
+    if (ima > 0.0f) { __stcg(&linvel[ia], to4(la, 0.0f)); __stcg(&angvel[ia], to4(wa, 0.0f)); }
+    if (imb > 0.0f) { __stcg(&linvel[ib], to4(lb, 0.0f)); __stcg(&angvel[ib], to4(wb, 0.0f)); }
+}
+
 struct Islands {
     DevBuf<uint32_t> parent, awake, need;
     // simulate_flag[world] is raised when the world has an active body; world_of
-    // (per body) is null for a single world.
+    // (per body) is null for a single world. Enabled joints between two dynamic bodies
+    // link their islands (islands.rs:186-196).
     void run(const BodyDev& b, uint32_t n, const uint64_t* pairs, uint32_t npairs, const uint32_t* world_of,
-             uint32_t* simulate_flag, uint32_t* status_dev, cudaStream_t s);
+             uint32_t* simulate_flag, uint32_t* status_dev, cudaStream_t s, const float4* joint_desc = nullptr,
+             uint32_t njoints = 0);
 };
 
 // ---------------------------------------------------------------- pair pass + solver (k_pairs.cu, k_solver.cu)
 struct StepParams {
     float dt, inv_dt;
     SolverParams info;
+    const uint64_t* suppressed = nullptr;  // sorted keys of pairs whose collisions a joint disables
+    uint32_t nsuppressed = 0;
 };
 
 constexpr uint32_t REC_NONE = 0xffffffffu;
@@ -340,7 +416,8 @@ void launch_compute_iw(const BodyDev& b, uint32_t n, cudaStream_t s);
 // `mark(5)` is called after the colouring and `mark(6)` after the PGS kernel (timing hooks).
 // seed_colours: start the colouring from the colours the pairs' manifolds carry from last step.
 void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
-                uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark, bool seed_colours);
+                uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark, bool seed_colours,
+                const JointsDev* joints = nullptr);
 // One team barrier that nothing completes (2 blocks): the wait gives up after limit_ns and
 // leaves ST_BARRIER_TIMEOUT in *status. ctr and status are device words the caller zeroes.
 void run_wait_selftest(unsigned long long limit_ns, unsigned int* ctr, uint32_t* status, cudaStream_t s);

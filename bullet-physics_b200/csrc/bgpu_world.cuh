@@ -53,6 +53,7 @@ struct SolverParams {  // solver/info.rs:24-86 (the contact subset)
     uint32_t split_impulse;
     float split_impulse_penetration_threshold, split_impulse_turn_erp, warmstarting_factor, global_cfm, sor;
     uint32_t num_iterations;
+    float erp, damping;  // joint rows
 };
 
 struct BodyDev {

@@ -87,6 +87,16 @@ __global__ void k_uf_init(uint32_t n, uint32_t* parent, uint32_t* awake) {
     awake[i] = 0;
 }
 
+__device__ __forceinline__ void link(uint32_t* parent, uint32_t a, uint32_t b, uint32_t* status) {
+    for (int g = 0; g < UF_LIMIT; ++g) {
+        uint32_t ra = find_halving(parent, a, status), rb = find_halving(parent, b, status);
+        if (ra == rb) return;
+        if (ra > rb) { uint32_t t = ra; ra = rb; rb = t; }
+        if (atomicCAS(&parent[rb], rb, ra) == rb) return;
+    }
+    atomicOr(status, ST_UNION_FIND_LIMIT);
+}
+
 __global__ void k_uf_link(const uint4* __restrict__ info, const uint64_t* __restrict__ pairs, uint32_t npairs,
                           uint32_t* parent, uint32_t* status, const uint32_t* __restrict__ need) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -96,13 +106,22 @@ __global__ void k_uf_link(const uint4* __restrict__ info, const uint64_t* __rest
     uint4 ia = info[a], ib = info[b];
     if (!eligible(ia, ib) || !participates(ia.y) || !participates(ib.y)) return;
     if (awake_member(ia) && awake_member(ib)) return;
-    for (int g = 0; g < UF_LIMIT; ++g) {
-        uint32_t ra = find_halving(parent, a, status), rb = find_halving(parent, b, status);
-        if (ra == rb) return;
-        if (ra > rb) { uint32_t t = ra; ra = rb; rb = t; }
-        if (atomicCAS(&parent[rb], rb, ra) == rb) return;
-    }
-    atomicOr(status, ST_UNION_FIND_LIMIT);
+    link(parent, a, b, status);
+}
+
+// islands.rs:186-196: an enabled joint between two dynamic bodies links their islands
+// (whatever its collision suppression).
+__global__ void k_uf_link_joints(const uint4* __restrict__ info, const float4* __restrict__ desc, uint32_t nj,
+                                 uint32_t* parent, uint32_t* status, const uint32_t* __restrict__ need) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nj || !*need) return;
+    const float4 h = desc[size_t(j) * JOINT_F4];
+    if (__float_as_uint(h.w) & JF_DISABLED) return;
+    const uint32_t a = __float_as_uint(h.y), b = __float_as_uint(h.z);
+    const uint4 ia = info[a], ib = info[b];
+    if (!participates(ia.y) || !participates(ib.y)) return;
+    if (awake_member(ia) && awake_member(ib)) return;
+    link(parent, a, b, status);
 }
 
 __global__ void k_uf_flatten_awake(const uint4* __restrict__ info, uint32_t n, uint32_t* parent, uint32_t* awake,
@@ -187,7 +206,8 @@ __global__ void k_uf_apply(uint4* info, float4* lv, float4* av, float4* sleep, u
 }  // namespace
 
 void Islands::run(const BodyDev& b, uint32_t n, const uint64_t* pairs, uint32_t npairs, const uint32_t* world_of,
-                  uint32_t* simulate_flag, uint32_t* status_dev, cudaStream_t s) {
+                  uint32_t* simulate_flag, uint32_t* status_dev, cudaStream_t s, const float4* joint_desc,
+                  uint32_t njoints) {
     if (n == 0) return;
     parent.reserve(n);
     awake.reserve(n);
@@ -197,6 +217,8 @@ void Islands::run(const BodyDev& b, uint32_t n, const uint64_t* pairs, uint32_t 
     k_island_need<<<(n + TB - 1) / TB, TB, 0, s>>>(b.info, n, need.p);
     k_uf_init<<<(n + TB - 1) / TB, TB, 0, s>>>(n, parent.p, awake.p);
     if (npairs) k_uf_link<<<(npairs + TB - 1) / TB, TB, 0, s>>>(b.info, pairs, npairs, parent.p, status_dev, need.p);
+    if (njoints)
+        k_uf_link_joints<<<(njoints + TB - 1) / TB, TB, 0, s>>>(b.info, joint_desc, njoints, parent.p, status_dev, need.p);
     k_uf_flatten_awake<<<(n + TB - 1) / TB, TB, 0, s>>>(b.info, n, parent.p, awake.p, status_dev, need.p);
     k_uf_store_roots<<<(n + TB - 1) / TB, TB, 0, s>>>(n, parent.p, status_dev, need.p);
     if (npairs)

@@ -323,7 +323,10 @@ __global__ void k_classify(BodyDev b, const Shape* __restrict__ shapes, const ui
     pd.row_count[p] = 0;
     pd.detect_n[p] = 0;
     uint32_t ga = ia.w & 0xffffu, mka = ia.w >> 16, gb = ib.w & 0xffffu, mkb = ib.w >> 16;
-    if ((ga & mkb) == 0 || (gb & mka) == 0) {
+    // step.rs:645-651: pairs linked by a joint with disable_collisions are skipped like
+    // group/mask rejects.
+    const bool suppressed = sp.nsuppressed && find_key(sp.suppressed, sp.nsuppressed, key, 0) >= 0;
+    if (suppressed || (ga & mkb) == 0 || (gb & mka) == 0) {
         pd.status[p] = PS_NONE;
         store_meta_only(ne, 0u);
         return;

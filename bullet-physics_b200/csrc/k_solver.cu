@@ -434,6 +434,8 @@ struct SolveArgs {
     float inv_dt;
     float restitution_threshold;
     uint32_t iterations;
+    JointsDev j;              // joint rows, solved after the contacts of each sweep (j.ncol == 0: none)
+    float damping;            // joint rows (info.rs damping)
 };
 
 __device__ __forceinline__ void apply(V3& la, V3& wa, V3& lb, V3& wb, bool appa, bool appb, float ima, float imb, V3 d,
@@ -685,7 +687,7 @@ template <bool VELOCITY>
 __device__ __forceinline__ void run_phases(const SolveArgs& a, const uint4* __restrict__ recs, const uint32_t* soff,
                                            const uint32_t* send, uint32_t ncol, uint32_t nphases, uint32_t last, uint32_t tid,
                                            uint32_t stride, unsigned int* ctr, uint32_t team_blocks, uint32_t team_block,
-                                           uint32_t& nbar) {
+                                           uint32_t& nbar, uint32_t sweep0 = 0) {
     if (ncol == 0 || nphases == 0) return;
     auto small = [&](uint32_t c) { return send[c] - soff[c] <= blockDim.x; };
     auto first_slot = [&](uint32_t c) -> uint32_t {
@@ -698,7 +700,7 @@ __device__ __forceinline__ void run_phases(const SolveArgs& a, const uint4* __re
     };
     uint4 rec = first_rec(0);  // rec.z == 0 (no rows): no slot for this thread
     for (uint32_t q = 0; q < nphases; ++q) {
-        const uint32_t c = q % ncol, sweep = q / ncol;
+        const uint32_t c = q % ncol, sweep = sweep0 + q / ncol;
         const uint4 next = q + 1 < nphases ? first_rec((q + 1) % ncol) : make_uint4(0u, 0u, 0u, 0u);
         if (rec.z) {
             const uint32_t t0 = first_slot(c);
@@ -720,10 +722,55 @@ __device__ __forceinline__ void run_phases(const SolveArgs& a, const uint4* __re
     }
 }
 
+// One joint colour: slots [first, end) with the given stride.
+__device__ __forceinline__ void joint_phase(JointsDev j, float4* linvel, float4* angvel, const float4* iw, float damping,
+                                         uint32_t first, uint32_t end, uint32_t stride) {
+    for (uint32_t t = first; t < end; t += stride) solve_joint_slot(j, t, linvel, angvel, iw, damping);
+}
+
+// The velocity team's sweeps in a world with joints: sweep by sweep, the contact phases,
+// then (velocity sweeps only) one phase per joint colour (sequential_impulse.rs:720-735).
+// Between two phases that block 0 runs alone (at most one block's worth of slots) the
+// block syncs locally; otherwise the team meets at its barrier. Only the k_solve built
+// for worlds with joints contains it.
+__device__ __forceinline__ void velocity_sweeps_with_joints(const SolveArgs& a, const uint32_t* s_off, const uint32_t* s_end,
+                                                         const uint32_t* s_joff, uint32_t ncol, uint32_t njcol,
+                                                         uint32_t iters, uint32_t tid, uint32_t stride,
+                                                         uint32_t team_blocks, uint32_t team_block, uint32_t& nbar) {
+    auto csmall = [&](uint32_t c) { return s_end[c] - s_off[c] <= blockDim.x; };
+    auto jsmall = [&](uint32_t c) { return s_joff[c + 1] - s_joff[c] <= blockDim.x; };
+    auto sync = [&](bool local) {
+        if (local) __syncthreads();
+        else team_barrier(a.bar, ++nbar * team_blocks, a.status);
+    };
+    for (uint32_t sw = 0; sw <= iters; ++sw) {
+        run_phases<true>(a, a.batch_rec, s_off, s_end, ncol, ncol, iters, tid, stride, a.bar, team_blocks, team_block,
+                         nbar, sw);
+        bool prev_small = ncol ? csmall(ncol - 1) : true;
+        if (sw >= 1) {
+            for (uint32_t jc = 0; jc < njcol; ++jc) {
+                const bool small = jsmall(jc);
+                sync(prev_small && small);
+                const uint32_t lo = s_joff[jc], hi = s_joff[jc + 1];
+                if (small) {
+                    if (team_block == 0 && lo + threadIdx.x < hi)
+                        joint_phase(a.j, a.linvel, a.angvel, a.iw, a.damping, lo + threadIdx.x, hi, blockDim.x);
+                } else {
+                    joint_phase(a.j, a.linvel, a.angvel, a.iw, a.damping, lo + tid, hi, stride);
+                }
+                prev_small = small;
+            }
+        }
+        if (sw < iters) sync(prev_small && (ncol ? csmall(0) : true));
+    }
+}
+
 // solve() (sequential_impulse.rs:692-705): warm start and velocity sweeps on
 // the velocity team; the split sweeps on the split team, which has enough
 // blocks for the largest split batch and at most a quarter of the grid (none
 // on a grid too small to split, where the velocity team runs them last).
+// JOINTS: the build for worlds with joints (the contact-only build carries none of their code).
+template <bool JOINTS>
 __global__ void __launch_bounds__(256, 2) k_solve(SolveArgs a) {
     const uint32_t ncol = a.scalars[4];
     const uint32_t nsplit = a.scalars[5];
@@ -746,15 +793,23 @@ __global__ void __launch_bounds__(256, 2) k_solve(SolveArgs a) {
         s_split_off[c] = a.split_offset[c];
         s_split_end[c] = a.split_end[c];
     }
-    __syncthreads();
+    const uint32_t njcol = JOINTS ? a.j.ncol : 0u;
+    __shared__ uint32_t s_joff[JOINTS ? MAX_COLOURS + 1 : 1];
+    if (JOINTS)
+        for (uint32_t c = threadIdx.x; c <= njcol && njcol; c += blockDim.x) s_joff[c] = a.j.coff[c];
+    __syncthreads();  // the batch ranges above are read by every thread of the block
     uint32_t nbar = 0;
     if (split_team) {
         run_phases<false>(a, a.split_rec, s_split_off, s_split_end, ncol, iters * ncol, iters - 1u, tid, stride, a.bar + 1,
                           team_blocks, team_block, nbar);
         return;
     }
-    run_phases<true>(a, a.batch_rec, s_off, s_end, ncol, (iters + 1) * ncol, iters, tid, stride, a.bar, team_blocks,
-                     team_block, nbar);
+    if (!JOINTS || njcol == 0) {
+        run_phases<true>(a, a.batch_rec, s_off, s_end, ncol, (iters + 1) * ncol, iters, tid, stride, a.bar, team_blocks,
+                         team_block, nbar);
+    } else {
+        velocity_sweeps_with_joints(a, s_off, s_end, s_joff, ncol, njcol, iters, tid, stride, team_blocks, team_block, nbar);
+    }
     if (nsplit && iters && split_blocks == 0) {
         team_barrier(a.bar, ++nbar * team_blocks, a.status);
         run_phases<false>(a, a.split_rec, s_split_off, s_split_end, ncol, iters * ncol, iters - 1u, tid, stride, a.bar, team_blocks,
@@ -863,16 +918,37 @@ int coop_grid(const void* fn, int block, size_t smem) {
 
 }  // namespace
 
+// PGS (cooperative launch: the teams' barriers need every block resident).
+static void launch_solve(const WorldView& w, PairData& pd, const StepParams& sp, uint32_t* status_dev, cudaStream_t s,
+                         const JointsDev* joints) {
+    const int TB = 256;
+    check_cuda(cudaMemsetAsync(pd.barrier.p, 0, 2 * sizeof(unsigned int), s), "memset barrier");
+    SolveArgs sa{pd.rows.p, pd.batch_rec.p, pd.colour_offset.p, pd.colour_cursor.p, pd.split_rec.p,
+                 pd.split_offset.p, pd.split_cursor.p, pd.scalars.p, w.b.linvel, w.b.angvel, w.b.push_lin,
+                 w.b.push_ang, w.b.iw, pd.vtab.p, pd.stab.p, pd.rec.sweeps,
+                 pd.barrier.p, status_dev, sp.inv_dt, sp.info.restitution_velocity_threshold,
+                 sp.info.num_iterations, joints ? *joints : JointsDev{}, sp.info.damping};
+    const void* fn = joints ? (const void*)k_solve<true> : (const void*)k_solve<false>;
+    static int solve_grid[2] = {0, 0};
+    int& grid = solve_grid[joints ? 1 : 0];
+    if (!grid) grid = coop_grid(fn, TB, 0);
+    void* sargs[] = {&sa};
+    check_cuda(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(TB), sargs, 0, s), "solve launch");
+}
+
 void run_wait_selftest(unsigned long long limit_ns, unsigned int* ctr, uint32_t* status, cudaStream_t s) {
     k_wait_selftest<<<2, 32, 0, s>>>(ctr, status, limit_ns);
 }
 
 void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
-                uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark, bool seed_colours) {
+                uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark, bool seed_colours,
+                const JointsDev* joints) {
+    const bool with_joints = joints && joints->n && joints->ncol;
     if (npairs == 0) {
         check_cuda(cudaMemsetAsync(pd.scalars.p + 2, 0, 4 * sizeof(uint32_t), s), "memset");
         check_cuda(cudaMemsetAsync(pd.scalars.p + 10, 0, 2 * sizeof(uint32_t), s), "memset");
         mark(5);
+        if (with_joints) launch_solve(w, pd, sp, status_dev, s, joints);
         mark(6);
         return;
     }
@@ -914,23 +990,12 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
     k_colour_scatter<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pairs, pd.row_count.p, pd.colour.p,
                                       pd.flags.p, sub_cursor, pd.split_cursor.p, pd.batch_rec.p,
                                       pd.split_rec.p, pd.entries.p, pd.colour_remap.p);
-    // PGS (cooperative launch: the teams' barriers need every block resident).
-    check_cuda(cudaMemsetAsync(pd.barrier.p, 0, 2 * sizeof(unsigned int), s), "memset barrier");
     mark(5);
     // Slot capacity: every group plus the 32-alignment padding of each batch.
     const size_t slots = (size_t(npairs) + 32u * (MAX_COLOURS + 1) + 31u) & ~size_t(31);
     pd.vtab.reserve(size_t(VT_PLANES) * 4 * slots);
     pd.stab.reserve(size_t(ST_PLANES) * 4 * slots);
-    SolveArgs sa{pd.rows.p, pd.batch_rec.p, pd.colour_offset.p, pd.colour_cursor.p, pd.split_rec.p,
-                 pd.split_offset.p, pd.split_cursor.p, pd.scalars.p, w.b.linvel, w.b.angvel, w.b.push_lin,
-                 w.b.push_ang, w.b.iw, pd.vtab.p, pd.stab.p, pd.rec.sweeps,
-                 pd.barrier.p, status_dev, sp.inv_dt, sp.info.restitution_velocity_threshold,
-                 sp.info.num_iterations};
-    static int solve_grid = 0;
-    if (!solve_grid) solve_grid = coop_grid((const void*)k_solve, TB, 0);
-    void* sargs[] = {&sa};
-    check_cuda(cudaLaunchCooperativeKernel((const void*)k_solve, dim3(solve_grid), dim3(TB), sargs, 0, s),
-               "solve launch");
+    launch_solve(w, pd, sp, status_dev, s, with_joints ? joints : nullptr);
     mark(6);
 }
 

@@ -3,6 +3,7 @@
 // phase, islands, pair pass, solve, manifold writeback/prune, integrate
 // positions), and the C ABI declared in include/bgpu.h.
 #include <algorithm>
+#include <unordered_map>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -112,6 +113,12 @@ struct StepRecord {
     }
 };
 
+inline float __uint_as_float_host(uint32_t u) {
+    float f;
+    std::memcpy(&f, &u, sizeof(f));
+    return f;
+}
+
 struct World {
     cudaStream_t stream = nullptr;
     SolverParams info{};
@@ -161,6 +168,14 @@ struct World {
     DevBuf<float> host_io;  // device staging for the caller-layout force / pose buffers
     DevBuf<uint8_t> rec_pt_src;
     DevBuf<uint32_t> rec_pair_old;
+    // joints: descriptors by id, solve order (joint colour by colour), per-step rows
+    std::vector<bgpu_joint_desc> joints_h;
+    std::vector<uint32_t> joint_order_h, joint_coff_h;
+    DevBuf<float4> joint_desc_d, joint_rows_d;
+    DevBuf<uint32_t> joint_order_d, joint_coff_d, joint_count_d;
+    DevBuf<float> joint_angle_d;
+    DevBuf<uint64_t> suppressed_d;  // sorted keys of the pairs a joint keeps from colliding
+    uint32_t nsuppressed = 0;
 
     World() {
         check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
@@ -391,6 +406,112 @@ struct World {
         return first_world;
     }
 
+    JointsDev joints_dev() {
+        JointsDev j;
+        j.desc = joint_desc_d.p;
+        j.order = joint_order_d.p;
+        j.coff = joint_coff_d.p;
+        j.n = uint32_t(joints_h.size());
+        j.ncol = joint_coff_h.empty() ? 0u : uint32_t(joint_coff_h.size() - 1);
+        j.rows = joint_rows_d.p;
+        j.count = joint_count_d.p;
+        j.angle = joint_angle_d.p;
+        return j;
+    }
+
+    // PhysicsWorld::add_constraint. The joint graph is coloured here, once per change:
+    // first fit in joint id order, with only dynamic bodies in conflict (static and
+    // kinematic bodies take no impulse), so a joint colour never holds a dynamic body twice.
+    uint32_t add_joints(uint32_t cnt, const bgpu_joint_desc* d) {
+        for (uint32_t k = 0; k < cnt; ++k) {
+            if (d[k].kind > BGPU_JOINT_HINGE) throw InvalidArg{"unknown joint kind"};
+            if (d[k].body_a >= n || d[k].body_b >= n || d[k].body_a == d[k].body_b)
+                throw InvalidArg{"joint bodies out of range or equal"};
+        }
+        const uint32_t first = uint32_t(joints_h.size());
+        joints_h.insert(joints_h.end(), d, d + cnt);
+        const uint32_t nj = uint32_t(joints_h.size());
+        std::vector<uint4> hinfo(n);
+        check_cuda(cudaMemcpyAsync(hinfo.data(), info_d.p, n * sizeof(uint4), cudaMemcpyDeviceToHost, stream), "d2h");
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+        auto dynamic = [&](uint32_t i) { return (hinfo[i].y & (BF_STATIC | BF_KINEMATIC)) == 0; };
+        std::unordered_map<uint32_t, std::vector<uint64_t>> used;  // body -> colour bits
+        std::vector<uint32_t> colour(nj);
+        uint32_t ncol = 0;
+        for (uint32_t j = 0; j < nj; ++j) {
+            uint64_t m[2] = {0, 0};
+            const uint32_t ends[2] = {joints_h[j].body_a, joints_h[j].body_b};
+            for (uint32_t e : ends) {
+                if (!dynamic(e)) continue;
+                auto it = used.find(e);
+                if (it != used.end()) { m[0] |= it->second[0]; m[1] |= it->second[1]; }
+            }
+            uint32_t c = 0;
+            while (c < 128 && ((m[c >> 6] >> (c & 63)) & 1ull)) ++c;
+            if (c >= uint32_t(MAX_COLOURS)) throw InvalidArg{"a body is linked by more than 127 joints"};
+            colour[j] = c;
+            ncol = std::max(ncol, c + 1);
+            for (uint32_t e : ends) {
+                if (!dynamic(e)) continue;
+                auto& v = used[e];
+                if (v.empty()) v.assign(2, 0ull);
+                v[c >> 6] |= 1ull << (c & 63);
+            }
+        }
+        joint_coff_h.assign(ncol + 1, 0u);
+        for (uint32_t j = 0; j < nj; ++j) joint_coff_h[colour[j] + 1] += 1;
+        for (uint32_t c = 0; c < ncol; ++c) joint_coff_h[c + 1] += joint_coff_h[c];
+        joint_order_h.assign(nj, 0u);
+        std::vector<uint32_t> fill(joint_coff_h.begin(), joint_coff_h.end() - 1);
+        for (uint32_t j = 0; j < nj; ++j) joint_order_h[fill[colour[j]]++] = j;
+        // device descriptors (JOINT_F4 float4 per joint id)
+        std::vector<float4> hd(size_t(nj) * JOINT_F4);
+        for (uint32_t j = 0; j < nj; ++j) {
+            const bgpu_joint_desc& x = joints_h[j];
+            float4* o = &hd[size_t(j) * JOINT_F4];
+            o[0] = make_float4(__uint_as_float_host(x.kind), __uint_as_float_host(x.body_a),
+                               __uint_as_float_host(x.body_b), __uint_as_float_host(x.flags));
+            for (int f = 0; f < 2; ++f) {
+                const float* fr = f ? x.frame_b : x.frame_a;
+                for (int c = 0; c < 4; ++c) o[1 + 4 * f + c] = make_float4(fr[3 * c], fr[3 * c + 1], fr[3 * c + 2], 0.0f);
+            }
+            o[9] = make_float4(x.erp, x.impulse_clamp, x.limit_low, x.limit_high);
+            o[10] = make_float4(x.limit_softness, x.limit_bias_factor, x.limit_relaxation, x.motor_target_velocity);
+            o[11] = make_float4(x.motor_max_impulse, 0.0f, 0.0f, 0.0f);
+        }
+        joint_desc_d.reserve(hd.size());
+        joint_order_d.reserve(nj);
+        joint_coff_d.reserve(ncol + 1);
+        joint_count_d.reserve(nj);
+        joint_rows_d.reserve(size_t(nj) * JOINT_MAX_ROWS * JROW_F4);
+        joint_angle_d.grow_keep(nj, first, stream);
+        check_cuda(cudaMemsetAsync(joint_angle_d.p + first, 0, cnt * sizeof(float), stream), "memset");
+        check_cuda(cudaMemsetAsync(joint_count_d.p, 0, nj * sizeof(uint32_t), stream), "memset");
+        check_cuda(cudaMemcpyAsync(joint_desc_d.p, hd.data(), hd.size() * sizeof(float4), cudaMemcpyHostToDevice, stream),
+                   "upload joints");
+        check_cuda(cudaMemcpyAsync(joint_order_d.p, joint_order_h.data(), nj * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                   stream), "upload joint order");
+        check_cuda(cudaMemcpyAsync(joint_coff_d.p, joint_coff_h.data(), (ncol + 1) * sizeof(uint32_t),
+                                   cudaMemcpyHostToDevice, stream), "upload joint colours");
+        // world.rs:873-880: suppressed pairs (independent of enabled)
+        std::vector<uint64_t> keys;
+        for (const auto& x : joints_h)
+            if (x.flags & BGPU_JOINT_DISABLE_COLLISIONS) {
+                const uint32_t lo = std::min(x.body_a, x.body_b), hi = std::max(x.body_a, x.body_b);
+                keys.push_back((uint64_t(lo) << 32) | hi);
+            }
+        std::sort(keys.begin(), keys.end());
+        keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+        nsuppressed = uint32_t(keys.size());
+        if (nsuppressed) {
+            suppressed_d.reserve(nsuppressed);
+            check_cuda(cudaMemcpyAsync(suppressed_d.p, keys.data(), nsuppressed * sizeof(uint64_t),
+                                       cudaMemcpyHostToDevice, stream), "upload suppressed pairs");
+        }
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+        return first;
+    }
+
     void set_gravity(const float* g) {
         gravity[0] = g[0]; gravity[1] = g[1]; gravity[2] = g[2];
         // world.rs:467-481: active bodies that did not opt out take the new gravity.
@@ -450,6 +571,9 @@ struct World {
         sp.dt = dt;
         sp.inv_dt = 1.0f / dt;
         sp.info = info;
+        sp.suppressed = nsuppressed ? suppressed_d.p : nullptr;
+        sp.nsuppressed = nsuppressed;
+        JointsDev jd = joints_dev();
         if (rec_step) {
             rec_step->flags.reserve(std::max<uint32_t>(n, 1));
             check_cuda(cudaMemsetAsync(rec_step->flags.p, 0, std::max<uint32_t>(n, 1), stream), "memset");
@@ -479,18 +603,20 @@ struct World {
         if (rec_step) prepare_record(old_cache.count_host);
         mark(2);
         // 4b: islands
-        islands.run(b, n, pairs.p, npairs, world_of, simulate, status, stream);
+        islands.run(b, n, pairs.p, npairs, world_of, simulate, status, stream, jd.desc, jd.n);
         mark(3);
         // 5: pair pass
         pd.reserve(std::max<uint32_t>(npairs, 1), n, old_cache.count_host);
         if (old_cache.count_host)
             check_cuda(cudaMemsetAsync(pd.old_owned.p, 0, old_cache.count_host * sizeof(uint32_t), stream), "memset");
         run_pair_pass(wv, pairs.p, npairs, old_cache, pd, sp, simulate, status, stream);
+        // 5a: joint rows from the current poses (step.rs:928-949)
+        launch_joint_rows(b, jd, sp.inv_dt, info.erp, stream);
         mark(4);
         // 6: solve (colouring, then the PGS kernel)
         // The colouring starts from last step's colours, except every RECOLOUR_PERIOD-th step.
         run_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); },
-                   step_count % RECOLOUR_PERIOD != 0);
+                   step_count % RECOLOUR_PERIOD != 0, &jd);
         ++step_count;
         // 6b: impulse writeback + prune
         run_cache_update(pairs.p, npairs, old_cache, pd, next, world_of, simulate, prev_simulate, stream);
@@ -890,6 +1016,21 @@ void bgpu_solver_info_default(bgpu_solver_info* o) {
     o->global_cfm = 0.0f;
     o->sor = 1.0f;
     o->num_iterations = 10;
+    o->erp = 0.2f;
+    o->damping = 1.0f;
+}
+
+void bgpu_joint_desc_default(bgpu_joint_desc* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->flags = BGPU_JOINT_DISABLE_COLLISIONS;
+    const float ident[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    for (int k = 0; k < 9; ++k) o->frame_a[3 + k] = o->frame_b[3 + k] = ident[k];
+    o->limit_low = 1.0f;
+    o->limit_high = -1.0f;
+    o->limit_softness = 0.9f;
+    o->limit_bias_factor = 0.3f;
+    o->limit_relaxation = 1.0f;
 }
 
 void bgpu_body_desc_default(bgpu_body_desc* o) {
@@ -913,6 +1054,8 @@ static void copy_info(bgpu::SolverParams& d, const bgpu_solver_info& s) {
     d.global_cfm = s.global_cfm;
     d.sor = s.sor;
     d.num_iterations = s.num_iterations;
+    d.erp = s.erp;
+    d.damping = s.damping;
 }
 
 bgpu_status bgpu_world_create(const bgpu_solver_info* info, const float* gravity, bgpu_world** out) {
@@ -1020,6 +1163,7 @@ bgpu_status bgpu_tape_create(bgpu_world* w, uint32_t checkpoint_every, bgpu_tape
     }
     *out = nullptr;
     return guarded([&]() -> bgpu_status {
+        if (!w->impl.joints_h.empty()) throw bgpu::InvalidArg{"the adjoint tape does not cover joints"};
         std::unique_ptr<bgpu_tape> t(new bgpu_tape());
         t->impl.reset(new bgpu::Tape(&w->impl, checkpoint_every));
         *out = t.release();
@@ -1342,6 +1486,71 @@ bgpu_status bgpu_read_solve_order(bgpu_world* w, uint64_t* out, uint64_t cap, ui
         if (out_n) *out_n = keys.size();
         uint64_t k = std::min<uint64_t>(cap, keys.size());
         if (out && k) std::memcpy(out, keys.data(), k * sizeof(uint64_t));
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_add_joints(bgpu_world* w, uint32_t n, const bgpu_joint_desc* d, uint32_t* first_id) {
+    if (!w || (n && !d)) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        uint32_t f = w->impl.add_joints(n, d);
+        if (first_id) *first_id = f;
+        return BGPU_OK;
+    });
+}
+
+uint32_t bgpu_num_joints(bgpu_world* w) { return w ? uint32_t(w->impl.joints_h.size()) : 0u; }
+
+bgpu_status bgpu_read_joint_angles(bgpu_world* w, float* angles) {
+    if (!w || !angles) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        const size_t nj = W.joints_h.size();
+        if (!nj) return BGPU_OK;
+        bgpu::check_cuda(cudaMemcpyAsync(angles, W.joint_angle_d.p, nj * sizeof(float), cudaMemcpyDeviceToHost, W.stream),
+                         "d2h");
+        bgpu::check_cuda(cudaStreamSynchronize(W.stream), "sync");
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_read_joint_order(bgpu_world* w, uint32_t* ids, uint32_t cap, uint32_t* out_n) {
+    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    const auto& o = w->impl.joint_order_h;
+    if (out_n) *out_n = uint32_t(o.size());
+    const uint32_t k = std::min<uint32_t>(cap, uint32_t(o.size()));
+    if (ids && k) std::memcpy(ids, o.data(), k * sizeof(uint32_t));
+    return BGPU_OK;
+}
+
+bgpu_status bgpu_read_joint_rows(bgpu_world* w, float* rows, uint32_t cap, uint32_t* out_n) {
+    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        W.finish_stats();
+        const uint32_t nj = uint32_t(W.joints_h.size());
+        std::vector<uint32_t> cnt(nj);
+        std::vector<float4> r(size_t(nj) * bgpu::JOINT_MAX_ROWS * bgpu::JROW_F4);
+        if (nj) {
+            bgpu::check_cuda(cudaMemcpyAsync(cnt.data(), W.joint_count_d.p, nj * 4, cudaMemcpyDeviceToHost, W.stream), "d2h");
+            bgpu::check_cuda(cudaMemcpyAsync(r.data(), W.joint_rows_d.p, r.size() * sizeof(float4), cudaMemcpyDeviceToHost,
+                                             W.stream), "d2h");
+            bgpu::check_cuda(cudaStreamSynchronize(W.stream), "sync");
+        }
+        uint32_t total = 0;
+        for (uint32_t t = 0; t < nj; ++t) {
+            const bgpu_joint_desc& jd = W.joints_h[W.joint_order_h[t]];
+            for (uint32_t k = 0; k < cnt[t]; ++k, ++total) {
+                if (!rows || total >= cap) continue;
+                const float4* x = &r[(size_t(t) * bgpu::JOINT_MAX_ROWS + k) * bgpu::JROW_F4];
+                float* o = rows + 8 * size_t(total);
+                uint32_t lim;
+                std::memcpy(&lim, &x[3].w, 4);
+                o[0] = float(W.joint_order_h[t]); o[1] = float(jd.body_a); o[2] = float(jd.body_b);
+                o[3] = x[0].w; o[4] = x[1].w; o[5] = float(lim); o[6] = x[4].z; o[7] = 0.0f;
+            }
+        }
+        if (out_n) *out_n = total;
         return BGPU_OK;
     });
 }

@@ -83,6 +83,8 @@ typedef struct bgpu_solver_info {
     float global_cfm;                          /* 0.0 */
     float sor;                                 /* 1.0 */
     uint32_t num_iterations;                   /* 10 */
+    float erp;                                 /* 0.2: joint position correction (info.rs erp) */
+    float damping;                             /* 1.0: joint row velocity scale (info.rs damping) */
 } bgpu_solver_info;
 
 /* RigidBody construction parameters (body.rs:388-499). mass == 0 builds a static
@@ -128,10 +130,38 @@ typedef struct bgpu_step_stats {
     uint32_t num_split_contacts; /* solver rows with an active split-impulse term */
 } bgpu_step_stats;
 
+/* Joints (constraint.rs:67-132: the point-to-point, fixed and hinge kinds). A frame is
+ * the pivot followed by the basis columns x, y, z, in the body's centre-of-mass frame
+ * (JointFrame, constraint.rs:658-682; the hinge axis is column z). Point-to-point joints
+ * use only the frame origins (the pivots). Rows are rebuilt every step from the current
+ * poses and solved after the contacts in each PGS sweep (sequential_impulse.rs:720-735);
+ * a joint of a sleeping island (both bodies inactive) produces no rows. */
+enum { BGPU_JOINT_POINT2POINT = 0, BGPU_JOINT_FIXED = 1, BGPU_JOINT_HINGE = 2 };
+#define BGPU_JOINT_DISABLE_COLLISIONS 0x01u /* no contacts between the two bodies (default on) */
+#define BGPU_JOINT_DISABLED 0x02u           /* set_enabled(false): no rows, no island link */
+#define BGPU_JOINT_ANGULAR_ONLY 0x04u       /* hinge: skip the three pivot rows */
+#define BGPU_JOINT_LIMIT 0x08u              /* hinge: angular limit [limit_low, limit_high] */
+#define BGPU_JOINT_MOTOR 0x10u              /* hinge: motor (target velocity, max impulse) */
+#define BGPU_JOINT_ERP 0x20u                /* point-to-point: own ERP instead of the solver's */
+typedef struct bgpu_joint_desc {
+    uint32_t kind;
+    uint32_t body_a, body_b;
+    uint32_t flags;
+    float frame_a[12];
+    float frame_b[12];
+    float erp;           /* point-to-point, with BGPU_JOINT_ERP */
+    float impulse_clamp; /* point-to-point: clamp of each row's impulse (0: none) */
+    float limit_low, limit_high, limit_softness, limit_bias_factor, limit_relaxation; /* hinge */
+    float motor_target_velocity, motor_max_impulse;                                    /* hinge */
+} bgpu_joint_desc;
+
 typedef struct bgpu_world bgpu_world;
 
 void bgpu_solver_info_default(bgpu_solver_info* out);
 void bgpu_body_desc_default(bgpu_body_desc* out);
+/* Identity frames, collisions between the two bodies disabled, limit off (low 1 > high -1),
+ * softness 0.9, bias factor 0.3, relaxation 1.0 (AngularLimit::new). */
+void bgpu_joint_desc_default(bgpu_joint_desc* out);
 
 /* Library and device probes. */
 const char* bgpu_version(void);
@@ -226,6 +256,18 @@ bgpu_status bgpu_read_solve_order(bgpu_world* w, uint64_t* keys, uint64_t cap, u
  * (row groups) in the batch, and those of them with split-impulse rows. Each solver
  * iteration runs one phase per colour, so these sizes set how the work spreads over
  * the device. Either array may be NULL; out_n receives the colour count. */
+/* Joints (PhysicsWorld::add_constraint, world.rs): ids are consecutive from *first_id.
+ * Rejects unknown kinds, out-of-range or equal bodies. */
+bgpu_status bgpu_add_joints(bgpu_world* w, uint32_t n, const bgpu_joint_desc* d, uint32_t* first_id);
+uint32_t bgpu_num_joints(bgpu_world* w);
+/* Per joint: the hinge angle of the last step that built its rows (HingeConstraint::hinge_angle;
+ * 0 for the other kinds). */
+bgpu_status bgpu_read_joint_angles(bgpu_world* w, float* angles);
+/* Joint ids in the order their rows are solved (joint colour by colour). */
+bgpu_status bgpu_read_joint_order(bgpu_world* w, uint32_t* ids, uint32_t cap, uint32_t* out_n);
+/* Joint rows of the last step in solve order, 8 floats each: joint id, body_a, body_b,
+ * effective mass, bias, limit kind, accumulated impulse, 0. */
+bgpu_status bgpu_read_joint_rows(bgpu_world* w, float* rows, uint32_t cap, uint32_t* out_n);
 bgpu_status bgpu_read_colour_batches(bgpu_world* w, uint32_t* groups, uint32_t* split_groups, uint32_t cap,
                                      uint32_t* out_n);
 bgpu_status bgpu_get_stats(bgpu_world* w, bgpu_step_stats* out);

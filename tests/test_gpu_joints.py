@@ -1,0 +1,294 @@
+"""GPU joint rows (point-to-point, fixed, hinge) against the oracle.
+
+Every scene is built twice from one description, stepped on the GPU and in the
+oracle (f32), and the oracle is given the GPU's solve order for the contact
+groups and for the joints. Joint rows use atan2/asin (hinge angle, fixed-joint
+Euler angles), whose last ulp may differ between CUDA and the host libm, so the
+states are compared in windows of 10 steps from a shared state (the oracle takes
+the GPU's body state at the start of each window) within 1e-4; activation states
+must be equal at every compared step. The reference's own assertions for the
+scenes (crates/bullet-dynamics/src/constraint/tests.rs) are also checked on the
+GPU trajectory.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle_api as orc
+
+pytestmark = pytest.mark.gpu
+
+DT = 1.0 / 60.0
+
+
+class JScene:
+    def __init__(self, gravity=(0.0, -9.81, 0.0)):
+        self.gravity = gravity
+        self.shapes, self.bodies, self.joints = [], [], []
+
+    def shape(self, kind, params):
+        self.shapes.append((kind, list(params)))
+        return len(self.shapes) - 1
+
+    def body(self, shape, pos, quat=(0, 0, 0, 1), mass=1.0, linvel=(0, 0, 0), angvel=(0, 0, 0), activation=0):
+        self.bodies.append(dict(shape=shape, pos=pos, quat=quat, mass=mass, linvel=linvel, angvel=angvel,
+                                activation=activation))
+        return len(self.bodies) - 1
+
+    def joint(self, kind, a, b, fa, fb, **kw):
+        self.joints.append((kind, a, b, np.asarray(fa, dtype=np.float64), np.asarray(fb, dtype=np.float64), kw))
+
+    def build(self, gpu):
+        w = gpu.World(gravity=self.gravity, num_iterations=10)
+        o = orc.OracleWorld("f32")
+        o.set_gravity(self.gravity)
+        o.set_solver(num_iterations=10)
+        for kind, params in self.shapes:
+            w.add_shape(kind, params)
+            o.add_shape(kind, params)
+        for b in self.bodies:
+            w.add_body(b["shape"], b["pos"], b["quat"], b["linvel"], b["angvel"], mass=b["mass"],
+                       activation=b["activation"])
+            o.add_body(b["shape"], b["pos"], quat=b["quat"], linvel=b["linvel"], angvel=b["angvel"], mass=b["mass"],
+                       activation=b["activation"])
+        for kind, a, b, fa, fb, kw in self.joints:
+            gkw = dict(kw)
+            w.add_joint(kind, a, b, fa, fb, **gkw)
+            o.add_joint(orc.joint_desc(kind, a, b, fa, fb, **kw))
+        o.set_joint_order(w.joint_order())
+        return w, o
+
+
+def run_pair(scene, gpu, steps, tol=1e-4, window=10, each=None):
+    """Steps both worlds; returns the GPU states per step. `each(step, gpu_world)` runs after every step."""
+    w, o = scene.build(gpu)
+    states = []
+    worst = 0.0
+    for step in range(steps):
+        if step % window == 0:
+            o.set_state(w.state().astype(np.float64))
+        w.step(DT)
+        o.set_solve_order(w.solve_order())
+        o.step(DT)
+        st = w.stats()
+        assert st["device_status"] == 0, st
+        g, r = w.state(), o.state()
+        np.testing.assert_array_equal(g[:, 13], r[:, 13], err_msg=f"activation, step {step}")
+        err = float(np.abs(g[:, :13] - r[:, :13]).max())
+        worst = max(worst, err)
+        assert err <= tol, f"step {step}: max abs state error {err}"
+        if len(scene.joints):
+            ga = w.joint_angles()
+            ra = o.joint_angles(len(scene.joints))
+            assert np.abs(ga - ra).max() <= 10 * tol, (step, ga, ra)
+        states.append(g)
+        if each:
+            each(step, w)
+    return w, o, np.array(states), worst
+
+
+def quat_z(a):
+    return (0.0, 0.0, math.sin(a / 2), math.cos(a / 2))
+
+
+def rotate(q, v):
+    x, y, z, w = q
+    b = np.array([x, y, z])
+    v = np.asarray(v, dtype=np.float64)
+    return v * (w * w - b @ b) + b * (2 * (v @ b)) + np.cross(b, v) * (2 * w)
+
+
+def test_pendulum_matches_the_oracle_and_keeps_its_pivot(gpu):  # constraint/tests.rs:46-91
+    s = JScene()
+    anchor = s.body(s.shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+    a45 = math.pi / 4
+    bob = s.body(s.shape(orc.SPHERE, [0.1]), (math.sin(a45), -math.cos(a45), 0.0), quat=quat_z(-a45))
+    s.joint(orc.JOINT_POINT2POINT, bob, anchor, orc.frame((-1.0, 0.0, 0.0)), orc.frame((0.0, 0.0, 0.0)))
+    _, _, st, _ = run_pair(s, gpu, 300)
+    err = [np.linalg.norm(x[bob, 0:3] + rotate(x[bob, 3:7], (-1.0, 0.0, 0.0))) for x in st]
+    assert max(err) < 0.2 and st[:, bob, 0].min() < -0.5
+
+
+def test_two_link_chain_matches_the_oracle(gpu):  # constraint/tests.rs:124-176
+    s = JScene()
+    anchor = s.body(s.shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+    sph = s.shape(orc.SPHERE, [0.1])
+    upper = s.body(sph, (0.0, -1.0, 0.0))
+    lower = s.body(sph, (0.0, -3.0, 0.0), linvel=(2.0, 0.0, 0.0))
+    s.joint(orc.JOINT_POINT2POINT, upper, anchor, orc.frame((0.0, 1.0, 0.0)), orc.frame((0.0, 0.0, 0.0)))
+    s.joint(orc.JOINT_POINT2POINT, lower, upper, orc.frame((0.0, 1.0, 0.0)), orc.frame((0.0, -1.0, 0.0)))
+    w, _, st, _ = run_pair(s, gpu, 200)
+    assert len(w.joint_order()) == 2
+
+
+def door(gravity=(0.0, -9.81, 0.0), door_pos=(0.0, 0.5, 0.0), open_45=True, **kw):
+    s = JScene(gravity)
+    anchor = s.body(s.shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+    pos, quat = door_pos, (0, 0, 0, 1)
+    if open_45:
+        a45 = math.pi / 4
+        pos, quat = (math.cos(a45) * 0.5, math.sin(a45) * 0.5, 0.0), quat_z(a45)
+    d = s.body(s.shape(orc.BOX, [0.5, 0.5, 0.2]), pos, quat=quat, mass=2.0)
+    fa, fb = orc.hinge_frames((-0.5, 0.0, 0.0), (0, 0, 1), (0, 0, 0), (0, 0, 1))
+    s.joint(orc.JOINT_HINGE, d, anchor, fa, fb, **kw)
+    return s
+
+
+def test_hinge_door_matches_the_oracle(gpu):  # constraint/tests.rs:180-235
+    w, _, st, _ = run_pair(door(), gpu, 300)
+    assert abs(w.joint_angles()[0]) <= math.pi
+
+
+def test_hinge_limit_matches_the_oracle(gpu):  # constraint/tests.rs:238-281
+    s = door(door_pos=(0.0, 0.0, 0.0), flags=orc.JF_DISABLE_COLLISIONS | orc.JF_LIMIT, limit=(-0.3, 0.3))
+    angles = []
+    run_pair(s, gpu, 300, each=lambda step, w: angles.append(float(w.joint_angles()[0])))
+    assert min(angles) > -0.35
+
+
+def test_hinge_motor_matches_the_oracle(gpu):  # constraint/tests.rs:284-316
+    s = door(gravity=(0.0, 0.0, 0.0), door_pos=(0.5, 0.0, 0.0), open_45=False,
+             flags=orc.JF_DISABLE_COLLISIONS | orc.JF_MOTOR, motor=(1.0, 1000.0))
+    w, _, _, _ = run_pair(s, gpu, 180)
+    assert abs(w.joint_angles()[0] - 3.0) < 1.0
+
+
+def test_joint_suppresses_collisions_between_linked_bodies(gpu):  # constraint/tests.rs:320-360
+    s = JScene((0.0, 0.0, 0.0))
+    box = s.shape(orc.BOX, [0.5, 0.5, 0.5])
+    a = s.body(box, (0, 0, 0))
+    b = s.body(box, (0, 0, 0))
+    s.joint(orc.JOINT_POINT2POINT, a, b, orc.frame((0, 0, 0)), orc.frame((0, 0, 0)))
+    w, o, st, _ = run_pair(s, gpu, 30)
+    assert w.stats()["num_contacts"] == 0
+    assert np.linalg.norm(st[-1, b, 0:3] - st[-1, a, 0:3]) < 0.02
+
+
+def test_impulse_clamp_matches_the_oracle(gpu):  # constraint/tests.rs:363-400
+    s = JScene()
+    anchor = s.body(s.shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+    bob = s.body(s.shape(orc.SPHERE, [0.1]), (0, 0, 0), mass=10.0)
+    s.joint(orc.JOINT_POINT2POINT, bob, anchor, orc.frame((0, 0, 0)), orc.frame((0, 0, 0)), impulse_clamp=0.1)
+    _, _, st, _ = run_pair(s, gpu, 120)
+    assert st[-1, bob, 1] < -0.5
+
+
+def test_fixed_joint_matches_the_oracle(gpu):  # constraint/tests.rs:403-458
+    s = JScene()
+    anchor = s.body(s.shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+    box = s.body(s.shape(orc.BOX, [0.3, 0.3, 0.3]), (0.0, 1.0, 0.0), linvel=(2.0, 0.0, 0.0), angvel=(0.0, 0.0, 4.0))
+    s.joint(orc.JOINT_FIXED, box, anchor, orc.frame((0.0, 0.5, 0.0)), orc.frame((0.0, 1.5, 0.0)))
+    _, _, st, _ = run_pair(s, gpu, 300)
+    assert np.linalg.norm(st[-1, box, 0:3] - (0.0, 1.0, 0.0)) < 0.03
+
+
+def test_welded_pair_lands_on_the_ground_like_the_oracle(gpu):  # constraint/tests.rs:461-515
+    """Contacts and joint rows in one solve: the welded boxes tumble onto a plane."""
+    s = JScene()
+    s.body(s.shape(orc.PLANE, [0.0, 1.0, 0.0, 0.0]), (0, 0, 0), mass=0.0)
+    box = s.shape(orc.BOX, [0.4, 0.4, 0.4])
+    a = s.body(box, (0.0, 1.2, 0.0), angvel=(1.0, 2.0, 0.0))
+    b = s.body(box, (0.0, 1.6, 0.0), angvel=(1.0, 2.0, 0.0))
+    s.joint(orc.JOINT_FIXED, a, b, orc.frame((0.0, 0.2, 0.0)), orc.frame((0.0, -0.2, 0.0)))
+    w, _, st, _ = run_pair(s, gpu, 150)
+    assert w.stats()["num_contacts"] > 0
+
+
+def chains(kinds, n_chains=400):
+    """n_chains eight-link chains of boxes dropped onto a plane; link k of chain c is a joint of
+    kind kinds[(c + k) % len(kinds)]."""
+    s = JScene()
+    s.body(s.shape(orc.PLANE, [0.0, 1.0, 0.0, 0.0]), (0, 0, 0), mass=0.0)
+    box = s.shape(orc.BOX, [0.2, 0.1, 0.1])
+    rng = np.random.default_rng(5)
+    hfa, hfb = orc.hinge_frames((0.25, 0.0, 0.0), (0, 0, 1), (-0.25, 0.0, 0.0), (0, 0, 1))
+    for c in range(n_chains):
+        x0, z0 = (c % 20) * 1.2 - 12.0, (c // 20) * 1.2 - 12.0
+        y0 = 0.5 + rng.uniform(0.0, 0.4)
+        ids = [s.body(box, (x0 + 0.5 * k, y0, z0)) for k in range(8)]
+        for k in range(7):
+            kind = kinds[(c + k) % len(kinds)]
+            if kind == orc.JOINT_HINGE:
+                s.joint(kind, ids[k], ids[k + 1], hfa, hfb)
+            else:
+                s.joint(kind, ids[k], ids[k + 1], orc.frame((0.25, 0.0, 0.0)), orc.frame((-0.25, 0.0, 0.0)))
+    return s
+
+
+def test_many_chains_on_the_ground_match_the_oracle(gpu):
+    """400 eight-link chains (point-to-point and hinge links, 2,800 joints, joint colours
+    larger than one block) fall onto a plane: grid-wide joint phases mixed with contacts.
+    The pose update's sin/cos may differ in the last ulp, and 3,200 colliding links amplify
+    that within a window, so the windows are 5 steps and the bound 1e-3 (the mixed convex
+    pile's); the rows themselves are compared one step from identical states below."""
+    w, _, _, _ = run_pair(chains((orc.JOINT_POINT2POINT, orc.JOINT_HINGE)), gpu, 40, tol=1e-3, window=5)
+    assert w.num_joints == 2800 and w.stats()["num_contacts"] > 0
+
+
+def test_many_chains_with_fixed_links_match_the_oracle(gpu):
+    """The same with a third of the links fixed joints, whose angular rows take their bias
+    from atan2/asin of the relative rotation (last-ulp differences between CUDA and the host
+    libm, amplified the same way): 5-step windows, 1e-3."""
+    w, _, _, _ = run_pair(chains((orc.JOINT_POINT2POINT, orc.JOINT_HINGE, orc.JOINT_FIXED)), gpu, 40, tol=1e-3,
+                          window=5)
+    assert w.num_joints == 2800
+
+
+def test_chain_joint_rows_match_the_oracle_after_one_step(gpu):
+    """One step of the 400 chains from identical states: every joint row (ids, bodies, limit
+    kind exact; effective mass, bias and accumulated impulse within 1e-5 relative)."""
+    w, o = chains((orc.JOINT_POINT2POINT, orc.JOINT_HINGE, orc.JOINT_FIXED)).build(gpu)
+    w.step(DT)
+    o.set_solve_order(w.solve_order())
+    o.step(DT)
+    g, r = w.joint_rows(), o.joint_rows()
+    rows_of = {orc.JOINT_POINT2POINT: 3, orc.JOINT_HINGE: 5, orc.JOINT_FIXED: 6}
+    kinds = (orc.JOINT_POINT2POINT, orc.JOINT_HINGE, orc.JOINT_FIXED)
+    expected = sum(rows_of[kinds[(c + k) % 3]] for c in range(400) for k in range(7))
+    assert g.shape == r.shape == (expected, 8)
+    np.testing.assert_array_equal(g[:, [0, 1, 2, 5]], r[:, [0, 1, 2, 5]])
+    np.testing.assert_allclose(g[:, [3, 4, 6]], r[:, [3, 4, 6]], rtol=1e-5, atol=1e-6)
+
+
+def test_joint_keeps_its_partner_awake_like_the_oracle(gpu):  # world/islands.rs:539-575
+    """Two bodies far apart joined by a point-to-point joint, one that never deactivates:
+    the joint links their islands, so the other one never sleeps; an unlinked copy sleeps."""
+    s = JScene((0.0, 0.0, 0.0))
+    sph = s.shape(orc.SPHERE, [0.5])
+    a = s.body(sph, (4.0, 0.0, 0.0), activation=4)  # DISABLE_DEACTIVATION
+    b = s.body(sph, (6.0, 0.0, 0.0))
+    c = s.body(sph, (20.0, 0.0, 0.0))  # no joint: falls asleep after 2 s
+    s.joint(orc.JOINT_POINT2POINT, a, b, orc.frame((1.0, 0.0, 0.0)), orc.frame((-1.0, 0.0, 0.0)))
+    _, _, st, _ = run_pair(s, gpu, 200)
+    assert st[-1, b, 13] != 2 and st[-1, c, 13] == 2
+
+
+def test_joint_rows_and_impulses_match_the_oracle(gpu):
+    """One step of the door with a motor: the GPU's rows (effective mass, bias, limit kind,
+    accumulated impulse) equal the oracle's in solve order."""
+    s = door(gravity=(0.0, -9.81, 0.0), flags=orc.JF_DISABLE_COLLISIONS | orc.JF_MOTOR, motor=(0.5, 2.0))
+    w, o = s.build(gpu)
+    w.step(DT)
+    o.set_solve_order(w.solve_order())
+    o.step(DT)
+    g, r = w.joint_rows(), o.joint_rows()
+    assert g.shape == r.shape == (6, 8)
+    np.testing.assert_array_equal(g[:, [0, 1, 2, 5]], r[:, [0, 1, 2, 5]])
+    np.testing.assert_allclose(g[:, [3, 4, 6]], r[:, [3, 4, 6]], rtol=1e-5, atol=1e-6)
+
+
+def test_joint_descriptors_are_checked(gpu):
+    w = gpu.World()
+    sph = w.sphere(0.5)
+    a = w.add_body(sph, (0, 0, 0))
+    with pytest.raises(gpu.BgpuError):
+        w.add_joint(0, a, a, orc.frame((0, 0, 0)), orc.frame((0, 0, 0)))
+    with pytest.raises(gpu.BgpuError):
+        w.add_joint(0, a, 7, orc.frame((0, 0, 0)), orc.frame((0, 0, 0)))
+    with pytest.raises(gpu.BgpuError):
+        w.add_joint(9, a, a, orc.frame((0, 0, 0)), orc.frame((0, 0, 0)))
+    b = w.add_body(sph, (2, 0, 0))
+    w.add_joint(0, a, b, orc.frame((1, 0, 0)), orc.frame((-1, 0, 0)))
+    with pytest.raises(gpu.BgpuError):
+        gpu.Tape(w, 10)
