@@ -13,8 +13,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libbgpu.so")
 
 SPHERE, BOX, CAPSULE, HULL, PLANE = 0, 1, 2, 3, 4
-JOINT_POINT2POINT, JOINT_FIXED, JOINT_HINGE = 0, 1, 2
+JOINT_POINT2POINT, JOINT_FIXED, JOINT_HINGE, JOINT_GEAR, JOINT_SLIDER = 0, 1, 2, 3, 4
 JOINT_DISABLE_COLLISIONS, JOINT_DISABLED, JOINT_ANGULAR_ONLY, JOINT_LIMIT, JOINT_MOTOR, JOINT_ERP = 1, 2, 4, 8, 16, 32
+JOINT_LIN_MOTOR, JOINT_ANG_MOTOR, JOINT_FRAME_B = 64, 128, 256
 NO_CONTACT_RESPONSE, DISABLE_WORLD_GRAVITY, KINEMATIC, ADDITIONAL_DAMPING = 0x1, 0x2, 0x4, 0x10
 STATE = 15
 CONTACT = 18
@@ -34,7 +35,14 @@ class JointDesc(ctypes.Structure):
                 ("erp", ctypes.c_float), ("impulse_clamp", ctypes.c_float), ("limit_low", ctypes.c_float),
                 ("limit_high", ctypes.c_float), ("limit_softness", ctypes.c_float),
                 ("limit_bias_factor", ctypes.c_float), ("limit_relaxation", ctypes.c_float),
-                ("motor_target_velocity", ctypes.c_float), ("motor_max_impulse", ctypes.c_float)]
+                ("motor_target_velocity", ctypes.c_float), ("motor_max_impulse", ctypes.c_float),
+                ("gear_ratio", ctypes.c_float), ("lin_limit_low", ctypes.c_float), ("lin_limit_high", ctypes.c_float),
+                ("ang_limit_low", ctypes.c_float), ("ang_limit_high", ctypes.c_float),
+                ("softness_lim_lin", ctypes.c_float), ("softness_lim_ang", ctypes.c_float),
+                ("damping_lim_lin", ctypes.c_float), ("damping_lim_ang", ctypes.c_float),
+                ("softness_ortho_lin", ctypes.c_float), ("softness_ortho_ang", ctypes.c_float),
+                ("lin_motor_target_velocity", ctypes.c_float), ("lin_motor_max_force", ctypes.c_float),
+                ("ang_motor_target_velocity", ctypes.c_float), ("ang_motor_max_force", ctypes.c_float)]
 
 
 class BodyDesc(ctypes.Structure):
@@ -108,6 +116,7 @@ def lib():
             "bgpu_add_joints": (S, [P, U32, ctypes.POINTER(JointDesc), U32P]),
             "bgpu_num_joints": (U32, [P]),
             "bgpu_read_joint_angles": (S, [P, F]),
+            "bgpu_read_joint_positions": (S, [P, F]),
             "bgpu_read_joint_order": (S, [P, U32P, U32, U32P]),
             "bgpu_read_joint_rows": (S, [P, F, U32, U32P]),
             "bgpu_get_stats": (S, [P, ctypes.POINTER(StepStats)]),
@@ -389,7 +398,8 @@ class World:
 
     def add_joint(self, kind, body_a, body_b, frame_a, frame_b, flags=JOINT_DISABLE_COLLISIONS, erp=0.0,
                   impulse_clamp=0.0, limit=(1.0, -1.0), softness=0.9, bias_factor=0.3, relaxation=1.0,
-                  motor=(0.0, 0.0)):
+                  motor=(0.0, 0.0), gear_ratio=1.0, lin_limits=(1.0, -1.0), ang_limits=(0.0, 0.0),
+                  slider_softness=(1.0, 1.0, 1.0, 1.0, 1.0, 1.0), lin_motor=(0.0, 0.0), ang_motor=(0.0, 0.0)):
         """frame_*: 12 numbers (pivot xyz, basis columns x, y, z) in the body's frame."""
         d = JointDesc()
         self.L.bgpu_joint_desc_default(ctypes.byref(d))
@@ -400,6 +410,13 @@ class World:
         d.limit_low, d.limit_high = limit
         d.limit_softness, d.limit_bias_factor, d.limit_relaxation = softness, bias_factor, relaxation
         d.motor_target_velocity, d.motor_max_impulse = motor
+        d.gear_ratio = gear_ratio
+        d.lin_limit_low, d.lin_limit_high = lin_limits
+        d.ang_limit_low, d.ang_limit_high = ang_limits
+        (d.softness_lim_lin, d.softness_lim_ang, d.damping_lim_lin, d.damping_lim_ang, d.softness_ortho_lin,
+         d.softness_ortho_ang) = slider_softness
+        d.lin_motor_target_velocity, d.lin_motor_max_force = lin_motor
+        d.ang_motor_target_velocity, d.ang_motor_max_force = ang_motor
         first = ctypes.c_uint32()
         check(self.L.bgpu_add_joints(self.h, 1, ctypes.byref(d), ctypes.byref(first)), "add_joints")
         return first.value
@@ -412,6 +429,12 @@ class World:
         out = np.zeros(self.num_joints, dtype=np.float32)
         if len(out):
             check(self.L.bgpu_read_joint_angles(self.h, fptr(out)), "read_joint_angles")
+        return out
+
+    def joint_positions(self):
+        out = np.zeros(self.num_joints, dtype=np.float32)
+        if len(out):
+            check(self.L.bgpu_read_joint_positions(self.h, fptr(out)), "read_joint_positions")
         return out
 
     def joint_order(self):

@@ -193,14 +193,17 @@ struct Broadphase {
 // Joint descriptor on the device, JOINT_F4 float4 per joint id: [0] kind, body a, body b,
 // flags (as bits); [1] frame A origin; [2..4] frame A basis columns; [5] frame B origin;
 // [6..8] frame B basis columns; [9] erp, impulse clamp, limit low, limit high;
-// [10] softness, bias factor, relaxation, motor target velocity; [11] motor max impulse.
-constexpr uint32_t JOINT_F4 = 12;
+// [10] softness, bias factor, relaxation, motor target velocity; [11] motor max impulse, gear ratio;
+// slider: [12] linear limits low/high, angular limits low/high; [13] softness lim lin/ang, damping
+// lim lin/ang; [14] softness ortho lin/ang, linear motor target/max force; [15] angular motor.
+constexpr uint32_t JOINT_F4 = 16;
 constexpr uint32_t JOINT_MAX_ROWS = 6;
 // Joint row, JROW_F4 float4: [0] lin_a | effective mass, [1] ang_a | bias, [2] lin_b | cfm,
 // [3] ang_b | limit kind (bits), [4] lower, upper, accumulated impulse, 0.
 constexpr uint32_t JROW_F4 = 5;
-enum : uint32_t { JK_POINT2POINT = 0, JK_FIXED = 1, JK_HINGE = 2 };
-enum : uint32_t { JF_DISABLE_COLLISIONS = 1u, JF_DISABLED = 2u, JF_ANGULAR_ONLY = 4u, JF_LIMIT = 8u, JF_MOTOR = 16u, JF_ERP = 32u };
+enum : uint32_t { JK_POINT2POINT = 0, JK_FIXED = 1, JK_HINGE = 2, JK_GEAR = 3, JK_SLIDER = 4 };
+enum : uint32_t { JF_DISABLE_COLLISIONS = 1u, JF_DISABLED = 2u, JF_ANGULAR_ONLY = 4u, JF_LIMIT = 8u, JF_MOTOR = 16u, JF_ERP = 32u,
+                  JF_LIN_MOTOR = 64u, JF_ANG_MOTOR = 128u, JF_FRAME_B = 256u };
 enum : uint32_t { JL_UNBOUNDED = 0, JL_BILATERAL = 1, JL_LOWER = 2, JL_UPPER = 3 };
 
 struct JointsDev {
@@ -210,7 +213,8 @@ struct JointsDev {
     uint32_t n = 0, ncol = 0;
     float4* rows = nullptr;          // JOINT_MAX_ROWS rows of JROW_F4 per slot
     uint32_t* count = nullptr;       // rows per slot this step
-    float* angle = nullptr;          // hinge angle per joint id
+    float* angle = nullptr;          // hinge angle / slider angular position per joint id
+    float* position = nullptr;       // slider linear position per joint id
 };
 
 // Rows of every joint for this step, from the current poses (constraint.rs:755-842).

@@ -1,4 +1,5 @@
-// Joint rows of one step (constraint.rs:755-842; fixed.rs:33-90; hinge.rs:130-267;
+// Joint rows of one step (constraint.rs:755-842; fixed.rs:33-90; hinge.rs:130-267; gear.rs:33-57;
+// slider.rs:159-475;
 // row preparation sequential_impulse.rs:260-299), one thread per joint slot in solve
 // order. Each joint of an awake island is flattened into its rows from the current
 // (pre-integration) poses, with the reference's arithmetic: the three pivot rows along
@@ -44,6 +45,36 @@ __device__ __forceinline__ float motor_factor(float pos, float low_lim, float up
         return 1.0f;
     }
     return 0.0f;
+}
+
+// shared.rs:30-55 (adjust_angle_to_limits)
+__device__ __forceinline__ float adjust_angle_to_limits(float angle, float lo, float hi) {
+    const float two_pi = 2.0f * PI_F;
+    if (lo >= hi) return angle;
+    if (angle < lo) {
+        const float diff_lo = fabsf(normalize_angle(lo - angle)), diff_hi = fabsf(normalize_angle(hi - angle));
+        return diff_lo < diff_hi ? angle : angle + two_pi;
+    }
+    if (angle > hi) {
+        const float diff_hi = fabsf(normalize_angle(angle - hi)), diff_lo = fabsf(normalize_angle(angle - lo));
+        return diff_lo < diff_hi ? angle - two_pi : angle;
+    }
+    return angle;
+}
+
+// shared.rs:126-145 (mirrored_row_limits): Bullet's window [lower, upper] in the row convention.
+__device__ __forceinline__ void mirrored_row_limits(float lower, float upper, uint32_t& lim, float& lo, float& hi) {
+    const bool lower_inf = isinf(lower) && lower < 0.0f, upper_inf = isinf(upper) && upper > 0.0f;
+    lo = 0.0f;
+    hi = 0.0f;
+    if (lower_inf && upper_inf) lim = JL_UNBOUNDED;
+    else if (lower_inf) lim = JL_LOWER;
+    else if (upper_inf) lim = JL_UPPER;
+    else {
+        lim = JL_BILATERAL;
+        hi = (upper - lower) / 2.0f;
+        lo = -hi;
+    }
 }
 
 // shared.rs:85-101 (euler_xyz)
@@ -117,6 +148,155 @@ __global__ void k_joint_rows(BodyDev b, JointsDev jd, float inv_dt, float erp) {
             const V3 nrm = axis_vec(axis);
             out.push(nrm, cross(r_a, nrm), nrm, cross(r_b, nrm), k * comp(dp, axis), lim, -clamp, clamp);
         }
+    } else if (kind == JK_SLIDER) {  // slider.rs:159-475
+        const float eps = 1.1920929e-7f;  // f32::EPSILON
+        const float inf = INFINITY;
+        const float4 p12 = d[12], p13 = d[13], p14 = d[14], p15 = d[15];
+        const float lower_lin = p12.x, upper_lin = p12.y, lower_ang = p12.z, upper_ang = p12.w;
+        const float softness_lim_lin = p13.x, softness_lim_ang = p13.y, damping_lim_lin = p13.z, damping_lim_ang = p13.w;
+        const float softness_ortho_lin = p14.x, softness_ortho_ang = p14.y;
+        const M3 tr_a = mul(from_quat(qa), M3{from4(d[2]), from4(d[3]), from4(d[4])});
+        const M3 tr_b = mul(from_quat(qb), M3{from4(d[6]), from4(d[7]), from4(d[8])});
+        const V3 delta = pivot_b - pivot_a;
+        const V3 ax1_a = tr_a.c0;
+        float depth0 = dot(delta, tr_a.c0);
+        const float lin_pos = depth0;
+        jd.position[jid] = lin_pos;
+        bool solve_lin_limit = false;
+        if (lower_lin <= upper_lin) {
+            if (depth0 > upper_lin) { depth0 -= upper_lin; solve_lin_limit = true; }
+            else if (depth0 < lower_lin) { depth0 -= lower_lin; solve_lin_limit = true; }
+            else depth0 = 0.0f;
+        } else {
+            depth0 = 0.0f;
+        }
+        const float lin_depth = depth0;
+        bool solve_ang_limit = false;
+        float ang_depth = 0.0f, ang_pos = 0.0f;
+        if (lower_ang <= upper_ang) {
+            const V3 axis_a0 = tr_a.c1, axis_a1 = tr_a.c2, axis_b0 = tr_b.c1;
+            const float rot = adjust_angle_to_limits(atan2f(dot(axis_b0, axis_a1), dot(axis_b0, axis_a0)), lower_ang, upper_ang);
+            ang_pos = rot;
+            jd.angle[jid] = rot;
+            if (rot < lower_ang) { ang_depth = rot - lower_ang; solve_ang_limit = true; }
+            else if (rot > upper_ang) { ang_depth = rot - upper_ang; solve_ang_limit = true; }
+        }
+        const float sign_fact = (flags & JF_FRAME_B) ? -1.0f : 1.0f;
+        const V3 ofs = pivot_b - pivot_a;
+        const bool has_static = out.ima < eps || out.imb < eps;
+        const float ims = out.ima + out.imb;
+        const float fact_a = ims > 0.0f ? out.imb / ims : 0.5f;
+        const float fact_b = 1.0f - fact_a;
+        const V3 ax1 = normalize(ax1_a * fact_a + tr_b.c0 * fact_b);
+        const float k = inv_dt * (softness_ortho_ang * erp);
+        const V3 u = cross(ax1_a, tr_b.c0);
+        const V3 rel_pa = pivot_a - pa, rel_pb = pivot_b - pb;
+        const V3 ortho_a = rel_pa - ax1 * dot(rel_pa, ax1);
+        const V3 ortho_b = rel_pb - ax1 * dot(rel_pb, ax1);
+        const float slider_offs = lin_pos - depth0;
+        const V3 total_dist = ax1 * (dot(ax1, pivot_a - pa) + slider_offs) - ax1 * dot(ax1, pivot_b - pb);
+        const V3 rel_a = ortho_a + total_dist * fact_a;
+        const V3 rel_b = ortho_b - total_dist * fact_b;
+        const V3 avg = ortho_b * fact_a + ortho_a * fact_b;
+        const V3 p = len2(avg) > eps ? normalize(avg) : tr_a.c1;
+        const V3 q = cross(ax1, p);
+        out.push(zero, p, zero, p, -k * dot(u, p), JL_UNBOUNDED, 0.0f, 0.0f);
+        out.push(zero, q, zero, q, -k * dot(u, q), JL_UNBOUNDED, 0.0f, 0.0f);
+        const float k_lin = inv_dt * (softness_ortho_lin * erp);
+        out.push(p, cross(rel_a, p), p, cross(rel_b, p), -k_lin * dot(p, ofs), JL_UNBOUNDED, 0.0f, 0.0f);
+        {
+            V3 tmp_a = cross(rel_a, q), tmp_b = cross(rel_b, q);
+            if (has_static && solve_ang_limit) { tmp_a = tmp_a * fact_a; tmp_b = tmp_b * fact_b; }
+            out.push(q, tmp_a, q, tmp_b, -k_lin * dot(q, ofs), JL_UNBOUNDED, 0.0f, 0.0f);
+        }
+        // linear limit / motor row
+        float limit_err = 0.0f;
+        int limit = 0;
+        if (solve_lin_limit) {
+            limit_err = lin_depth * sign_fact;
+            limit = limit_err > 0.0f ? 2 : 1;
+        }
+        bool powered = (flags & JF_LIN_MOTOR) != 0;
+        if (limit != 0 && lower_lin == upper_lin) powered = false;
+        if (limit != 0 || powered) {
+            const float curr_erp = erp;
+            float row_error = 0.0f, lower = 0.0f, upper = 0.0f;
+            if (powered) {
+                const float target = p14.z, max_force = p14.w;
+                const float mf = motor_factor(lin_pos, lower_lin, upper_lin, target, inv_dt * curr_erp);
+                row_error -= sign_fact * mf * target;
+                lower += -max_force / inv_dt;
+                upper += max_force / inv_dt;
+            }
+            if (limit != 0) {
+                row_error += inv_dt * curr_erp * limit_err;
+                if (lower_lin == upper_lin) { lower = -inf; upper = inf; }
+                else if (limit == 1) { lower = -inf; upper = 0.0f; }
+                else { lower = 0.0f; upper = inf; }
+                const float bounce = fabsf(1.0f - damping_lim_lin);
+                if (bounce > 0.0f) {
+                    float vel = dot(from4(b.linvel[ia]), ax1) - dot(from4(b.linvel[ib]), ax1);
+                    vel *= sign_fact;
+                    if (limit == 1) {
+                        if (vel < 0.0f) { const float newc = -bounce * vel; if (newc > row_error) row_error = newc; }
+                    } else if (vel > 0.0f) {
+                        const float newc = -bounce * vel;
+                        if (newc < row_error) row_error = newc;
+                    }
+                }
+                row_error *= softness_lim_lin;
+            }
+            uint32_t lim;
+            float lo, hi;
+            mirrored_row_limits(lower, upper, lim, lo, hi);
+            const V3 ang_a = has_static ? zero : cross(rel_a, ax1);
+            const V3 ang_b = has_static ? zero : cross(rel_b, ax1);
+            out.push(ax1, ang_a, ax1, ang_b, -row_error, lim, lo, hi);
+        }
+        // angular limit / motor row
+        limit_err = 0.0f;
+        limit = 0;
+        if (solve_ang_limit) {
+            limit_err = ang_depth;
+            limit = limit_err > 0.0f ? 1 : 2;
+        }
+        powered = (flags & JF_ANG_MOTOR) != 0;
+        if (limit != 0 && lower_ang == upper_ang) powered = false;
+        if (limit != 0 || powered) {
+            const float curr_erp = erp;
+            float row_error = 0.0f, lower = 0.0f, upper = 0.0f;
+            if (powered) {
+                const float target = p15.x, max_force = p15.y;
+                const float mf = motor_factor(ang_pos, lower_ang, upper_ang, target, inv_dt * curr_erp);
+                row_error = mf * target;
+                lower = -max_force / inv_dt;
+                upper = max_force / inv_dt;
+            }
+            if (limit != 0) {
+                row_error += inv_dt * curr_erp * limit_err;
+                if (lower_ang == upper_ang) { lower = -inf; upper = inf; }
+                else if (limit == 1) { lower = 0.0f; upper = inf; }
+                else { lower = -inf; upper = 0.0f; }
+                const float bounce = fabsf(1.0f - damping_lim_ang);
+                if (bounce > 0.0f) {
+                    const float vel = dot(from4(b.angvel[ia]), ax1) - dot(from4(b.angvel[ib]), ax1);
+                    if (limit == 1) {
+                        if (vel < 0.0f) { const float newc = -bounce * vel; if (newc > row_error) row_error = newc; }
+                    } else if (vel > 0.0f) {
+                        const float newc = -bounce * vel;
+                        if (newc < row_error) row_error = newc;
+                    }
+                }
+                row_error *= softness_lim_ang;
+            }
+            uint32_t lim;
+            float lo, hi;
+            mirrored_row_limits(lower, upper, lim, lo, hi);
+            out.push(zero, ax1, zero, ax1, -row_error, lim, lo, hi);
+        }
+    } else if (kind == JK_GEAR) {  // gear.rs:33-57: the spins about the frames' z columns, coupled
+        const V3 axis_a_world = rotate(qa, from4(d[4])), axis_b_world = rotate(qb, from4(d[8]));
+        out.push(zero, axis_a_world, zero, -(axis_b_world * p11.y), 0.0f, JL_UNBOUNDED, 0.0f, 0.0f);
     } else {
         const M3 basis_a = M3{from4(d[2]), from4(d[3]), from4(d[4])};
         const M3 basis_b = M3{from4(d[6]), from4(d[7]), from4(d[8])};

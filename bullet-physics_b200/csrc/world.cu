@@ -173,7 +173,7 @@ struct World {
     std::vector<uint32_t> joint_order_h, joint_coff_h;
     DevBuf<float4> joint_desc_d, joint_rows_d;
     DevBuf<uint32_t> joint_order_d, joint_coff_d, joint_count_d;
-    DevBuf<float> joint_angle_d;
+    DevBuf<float> joint_angle_d, joint_pos_d;
     DevBuf<uint64_t> suppressed_d;  // sorted keys of the pairs a joint keeps from colliding
     uint32_t nsuppressed = 0;
 
@@ -416,6 +416,7 @@ struct World {
         j.rows = joint_rows_d.p;
         j.count = joint_count_d.p;
         j.angle = joint_angle_d.p;
+        j.position = joint_pos_d.p;
         return j;
     }
 
@@ -424,7 +425,7 @@ struct World {
     // kinematic bodies take no impulse), so a joint colour never holds a dynamic body twice.
     uint32_t add_joints(uint32_t cnt, const bgpu_joint_desc* d) {
         for (uint32_t k = 0; k < cnt; ++k) {
-            if (d[k].kind > BGPU_JOINT_HINGE) throw InvalidArg{"unknown joint kind"};
+            if (d[k].kind > BGPU_JOINT_SLIDER) throw InvalidArg{"unknown joint kind"};
             if (d[k].body_a >= n || d[k].body_b >= n || d[k].body_a == d[k].body_b)
                 throw InvalidArg{"joint bodies out of range or equal"};
         }
@@ -477,7 +478,12 @@ struct World {
             }
             o[9] = make_float4(x.erp, x.impulse_clamp, x.limit_low, x.limit_high);
             o[10] = make_float4(x.limit_softness, x.limit_bias_factor, x.limit_relaxation, x.motor_target_velocity);
-            o[11] = make_float4(x.motor_max_impulse, 0.0f, 0.0f, 0.0f);
+            o[11] = make_float4(x.motor_max_impulse, x.gear_ratio, 0.0f, 0.0f);
+            o[12] = make_float4(x.lin_limit_low, x.lin_limit_high, x.ang_limit_low, x.ang_limit_high);
+            o[13] = make_float4(x.softness_lim_lin, x.softness_lim_ang, x.damping_lim_lin, x.damping_lim_ang);
+            o[14] = make_float4(x.softness_ortho_lin, x.softness_ortho_ang, x.lin_motor_target_velocity,
+                                x.lin_motor_max_force);
+            o[15] = make_float4(x.ang_motor_target_velocity, x.ang_motor_max_force, 0.0f, 0.0f);
         }
         joint_desc_d.reserve(hd.size());
         joint_order_d.reserve(nj);
@@ -486,6 +492,8 @@ struct World {
         joint_rows_d.reserve(size_t(nj) * JOINT_MAX_ROWS * JROW_F4);
         joint_angle_d.grow_keep(nj, first, stream);
         check_cuda(cudaMemsetAsync(joint_angle_d.p + first, 0, cnt * sizeof(float), stream), "memset");
+        joint_pos_d.grow_keep(nj, first, stream);
+        check_cuda(cudaMemsetAsync(joint_pos_d.p + first, 0, cnt * sizeof(float), stream), "memset");
         check_cuda(cudaMemsetAsync(joint_count_d.p, 0, nj * sizeof(uint32_t), stream), "memset");
         check_cuda(cudaMemcpyAsync(joint_desc_d.p, hd.data(), hd.size() * sizeof(float4), cudaMemcpyHostToDevice, stream),
                    "upload joints");
@@ -1031,6 +1039,13 @@ void bgpu_joint_desc_default(bgpu_joint_desc* o) {
     o->limit_softness = 0.9f;
     o->limit_bias_factor = 0.3f;
     o->limit_relaxation = 1.0f;
+    o->gear_ratio = 1.0f;
+    o->lin_limit_low = 1.0f;
+    o->lin_limit_high = -1.0f;
+    o->ang_limit_low = 0.0f;
+    o->ang_limit_high = 0.0f;
+    o->softness_lim_lin = o->softness_lim_ang = o->damping_lim_lin = o->damping_lim_ang = 1.0f;
+    o->softness_ortho_lin = o->softness_ortho_ang = 1.0f;
 }
 
 void bgpu_body_desc_default(bgpu_body_desc* o) {
@@ -1509,6 +1524,19 @@ bgpu_status bgpu_read_joint_angles(bgpu_world* w, float* angles) {
         if (!nj) return BGPU_OK;
         bgpu::check_cuda(cudaMemcpyAsync(angles, W.joint_angle_d.p, nj * sizeof(float), cudaMemcpyDeviceToHost, W.stream),
                          "d2h");
+        bgpu::check_cuda(cudaStreamSynchronize(W.stream), "sync");
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_read_joint_positions(bgpu_world* w, float* positions) {
+    if (!w || !positions) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        const size_t nj = W.joints_h.size();
+        if (!nj) return BGPU_OK;
+        bgpu::check_cuda(cudaMemcpyAsync(positions, W.joint_pos_d.p, nj * sizeof(float), cudaMemcpyDeviceToHost,
+                                         W.stream), "d2h");
         bgpu::check_cuda(cudaStreamSynchronize(W.stream), "sync");
         return BGPU_OK;
     });

@@ -130,19 +130,24 @@ typedef struct bgpu_step_stats {
     uint32_t num_split_contacts; /* solver rows with an active split-impulse term */
 } bgpu_step_stats;
 
-/* Joints (constraint.rs:67-132: the point-to-point, fixed and hinge kinds). A frame is
+/* Joints (constraint.rs:67-132: the point-to-point, fixed, hinge, gear and slider kinds). A frame is
  * the pivot followed by the basis columns x, y, z, in the body's centre-of-mass frame
  * (JointFrame, constraint.rs:658-682; the hinge axis is column z). Point-to-point joints
- * use only the frame origins (the pivots). Rows are rebuilt every step from the current
+ * use only the frame origins (the pivots); gear joints (gear.rs) couple the spins about the
+ * frames' z columns with gear_ratio; slider joints (slider.rs) slide along the frames' x
+ * columns. Rows are rebuilt every step from the current
  * poses and solved after the contacts in each PGS sweep (sequential_impulse.rs:720-735);
  * a joint of a sleeping island (both bodies inactive) produces no rows. */
-enum { BGPU_JOINT_POINT2POINT = 0, BGPU_JOINT_FIXED = 1, BGPU_JOINT_HINGE = 2 };
+enum { BGPU_JOINT_POINT2POINT = 0, BGPU_JOINT_FIXED = 1, BGPU_JOINT_HINGE = 2, BGPU_JOINT_GEAR = 3, BGPU_JOINT_SLIDER = 4 };
 #define BGPU_JOINT_DISABLE_COLLISIONS 0x01u /* no contacts between the two bodies (default on) */
 #define BGPU_JOINT_DISABLED 0x02u           /* set_enabled(false): no rows, no island link */
 #define BGPU_JOINT_ANGULAR_ONLY 0x04u       /* hinge: skip the three pivot rows */
 #define BGPU_JOINT_LIMIT 0x08u              /* hinge: angular limit [limit_low, limit_high] */
 #define BGPU_JOINT_MOTOR 0x10u              /* hinge: motor (target velocity, max impulse) */
 #define BGPU_JOINT_ERP 0x20u                /* point-to-point: own ERP instead of the solver's */
+#define BGPU_JOINT_LIN_MOTOR 0x40u          /* slider: linear motor */
+#define BGPU_JOINT_ANG_MOTOR 0x80u          /* slider: angular motor */
+#define BGPU_JOINT_FRAME_B 0x100u           /* slider: linear reference frame B (use_linear_reference_frame_a off) */
 typedef struct bgpu_joint_desc {
     uint32_t kind;
     uint32_t body_a, body_b;
@@ -153,6 +158,13 @@ typedef struct bgpu_joint_desc {
     float impulse_clamp; /* point-to-point: clamp of each row's impulse (0: none) */
     float limit_low, limit_high, limit_softness, limit_bias_factor, limit_relaxation; /* hinge */
     float motor_target_velocity, motor_max_impulse;                                    /* hinge */
+    float gear_ratio;                                                                  /* gear */
+    /* slider (SliderConstraint, slider.rs:8-60): limits (lower > upper frees the axis), */
+    float lin_limit_low, lin_limit_high, ang_limit_low, ang_limit_high;
+    /* softness / damping of the limits and of the orthogonal rows, */
+    float softness_lim_lin, softness_lim_ang, damping_lim_lin, damping_lim_ang, softness_ortho_lin, softness_ortho_ang;
+    /* motors (target velocity, max force) */
+    float lin_motor_target_velocity, lin_motor_max_force, ang_motor_target_velocity, ang_motor_max_force;
 } bgpu_joint_desc;
 
 typedef struct bgpu_world bgpu_world;
@@ -160,7 +172,8 @@ typedef struct bgpu_world bgpu_world;
 void bgpu_solver_info_default(bgpu_solver_info* out);
 void bgpu_body_desc_default(bgpu_body_desc* out);
 /* Identity frames, collisions between the two bodies disabled, limit off (low 1 > high -1),
- * softness 0.9, bias factor 0.3, relaxation 1.0 (AngularLimit::new). */
+ * softness 0.9, bias factor 0.3, relaxation 1.0 (AngularLimit::new), gear ratio 1; slider:
+ * linear axis free (1 > -1), rotation locked (0, 0), softness and damping 1 (SliderConstraint::new). */
 void bgpu_joint_desc_default(bgpu_joint_desc* out);
 
 /* Library and device probes. */
@@ -260,9 +273,11 @@ bgpu_status bgpu_read_solve_order(bgpu_world* w, uint64_t* keys, uint64_t cap, u
  * Rejects unknown kinds, out-of-range or equal bodies. */
 bgpu_status bgpu_add_joints(bgpu_world* w, uint32_t n, const bgpu_joint_desc* d, uint32_t* first_id);
 uint32_t bgpu_num_joints(bgpu_world* w);
-/* Per joint: the hinge angle of the last step that built its rows (HingeConstraint::hinge_angle;
- * 0 for the other kinds). */
+/* Per joint: the hinge angle (HingeConstraint::hinge_angle) or the slider's angular position
+ * (ang_pos) of the last step that built its rows; 0 for the other kinds. */
 bgpu_status bgpu_read_joint_angles(bgpu_world* w, float* angles);
+/* Per joint: the slider's linear position (SliderConstraint::lin_pos); 0 for the other kinds. */
+bgpu_status bgpu_read_joint_positions(bgpu_world* w, float* positions);
 /* Joint ids in the order their rows are solved (joint colour by colour). */
 bgpu_status bgpu_read_joint_order(bgpu_world* w, uint32_t* ids, uint32_t cap, uint32_t* out_n);
 /* Joint rows of the last step in solve order, 8 floats each: joint id, body_a, body_b,

@@ -370,8 +370,12 @@ void orc_world_set_solve_order(void* p, const uint64_t* keys, uint32_t n) {
 // bgpu_joint_desc: 0 kind, 1 body_a, 2 body_b, 3 flags (1 disable collisions, 2 disabled,
 // 4 angular only, 8 limit, 16 motor, 32 ERP override), 4-15 frame A (origin, basis columns
 // x y z), 16-27 frame B, 28 erp, 29 impulse clamp, 30 limit low, 31 limit high,
-// 32 softness, 33 bias factor, 34 relaxation, 35 motor target velocity, 36 motor max impulse.
-constexpr int JDESC = 37;
+// 32 softness, 33 bias factor, 34 relaxation, 35 motor target velocity, 36 motor max impulse,
+// 37 gear ratio; slider: 38 lower / 39 upper linear limit, 40 lower / 41 upper angular limit,
+// 42 softness lim lin, 43 softness lim ang, 44 damping lim lin, 45 damping lim ang, 46 softness
+// ortho lin, 47 softness ortho ang, 48 / 49 linear motor target velocity / max force, 50 / 51
+// angular motor (flags 64 linear motor, 128 angular motor, 256 linear reference frame B).
+constexpr int JDESC = 52;
 
 uint32_t orc_world_add_joint(void* p, const double* d) {
     Handle* h = static_cast<Handle*>(p);
@@ -403,6 +407,17 @@ uint32_t orc_world_add_joint(void* p, const double* d) {
         jt.limit.relaxation = static_cast<R>(d[34]);
         jt.motor_target = static_cast<R>(d[35]);
         jt.motor_max = static_cast<R>(d[36]);
+        jt.gear_ratio = static_cast<R>(d[37]);
+        jt.lower_lin = static_cast<R>(d[38]); jt.upper_lin = static_cast<R>(d[39]);
+        jt.lower_ang = static_cast<R>(d[40]); jt.upper_ang = static_cast<R>(d[41]);
+        jt.softness_lim_lin = static_cast<R>(d[42]); jt.softness_lim_ang = static_cast<R>(d[43]);
+        jt.damping_lim_lin = static_cast<R>(d[44]); jt.damping_lim_ang = static_cast<R>(d[45]);
+        jt.softness_ortho_lin = static_cast<R>(d[46]); jt.softness_ortho_ang = static_cast<R>(d[47]);
+        jt.lin_motor_target = static_cast<R>(d[48]); jt.lin_motor_max = static_cast<R>(d[49]);
+        jt.ang_motor_target = static_cast<R>(d[50]); jt.ang_motor_max = static_cast<R>(d[51]);
+        jt.has_lin_motor = (f & 64u) != 0;
+        jt.has_ang_motor = (f & 128u) != 0;
+        jt.use_frame_a = (f & 256u) == 0;
         w.joints.push_back(jt);
         r = uint32_t(w.joints.size() - 1);
     });
@@ -414,9 +429,19 @@ void orc_world_set_joint_order(void* p, const uint32_t* ids, uint32_t n) {
     DISPATCH(h, { w.joint_order.assign(ids, ids + n); });
 }
 
+// Per joint: the hinge angle (hinge) or the angular position (slider); 0 for other kinds.
 void orc_world_joint_angles(void* p, double* out) {
     Handle* h = static_cast<Handle*>(p);
-    DISPATCH(h, { for (size_t k = 0; k < w.joints.size(); ++k) out[k] = w.joints[k].hinge_angle; });
+    DISPATCH(h, {
+        for (size_t k = 0; k < w.joints.size(); ++k)
+            out[k] = w.joints[k].kind == JOINT_SLIDER ? w.joints[k].ang_pos : w.joints[k].hinge_angle;
+    });
+}
+
+// Per joint: the slider's linear position (0 for other kinds).
+void orc_world_joint_positions(void* p, double* out) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, { for (size_t k = 0; k < w.joints.size(); ++k) out[k] = w.joints[k].lin_pos; });
 }
 
 uint32_t orc_world_num_joint_rows(void* p) {

@@ -8,7 +8,12 @@
 //   crates/bullet-dynamics/src/constraint/fixed.rs:33-90 (locked-6DOF rows);
 //   crates/bullet-dynamics/src/constraint/hinge.rs:60-100 (frames from pivot/axis), :130-267 (rows);
 //   crates/bullet-dynamics/src/constraint/shared.rs:6-155 (hinge angle, angle wrap, Euler XYZ,
-//     relative rotation axes, motor factor).
+//     relative rotation axes, motor factor);
+//   crates/bullet-dynamics/src/constraint/gear.rs:33-57 (gear: one angular coupling row; the
+//     axes are the frames' z columns here);
+//   crates/bullet-dynamics/src/constraint/slider.rs:159-475 (slider: frame-offset rows, linear and
+//     angular limits and motors), shared.rs:30-55 (adjust_angle_to_limits), :126-145
+//     (mirrored_row_limits).
 // Frame construction uses glam 0.33.3's `Quat::from_rotation_arc` (not in the reference tree);
 // its published algorithm is restated in rotation_arc() below.
 #pragma once
@@ -20,7 +25,7 @@
 
 namespace oracle {
 
-enum : uint32_t { JOINT_POINT2POINT = 0, JOINT_FIXED = 1, JOINT_HINGE = 2 };
+enum : uint32_t { JOINT_POINT2POINT = 0, JOINT_FIXED = 1, JOINT_HINGE = 2, JOINT_GEAR = 3, JOINT_SLIDER = 4 };
 // RowLimits (sequential_impulse.rs): which clamp the accumulated impulse takes.
 enum : uint32_t { LIM_UNBOUNDED = 0, LIM_BILATERAL = 1, LIM_LOWER = 2, LIM_UPPER = 3, LIM_WINDOW = 4 };
 
@@ -46,7 +51,15 @@ struct Joint {
     bool angular_only = false, has_limit = false, has_motor = false;  // hinge (hinge.rs:20-45)
     AngularLimit<R> limit;
     R motor_target = 0, motor_max = 0;
+    R gear_ratio = 1;   // gear (gear.rs:9-13): axes are the frames' basis z columns
     R hinge_angle = 0;  // per-step state (hinge.rs:37)
+    // slider (slider.rs:8-60, defaults of SliderConstraint::new)
+    R lower_lin = 1, upper_lin = -1, lower_ang = 0, upper_ang = 0;
+    R softness_lim_lin = 1, softness_lim_ang = 1, damping_lim_lin = 1, damping_lim_ang = 1;
+    R softness_ortho_lin = 1, softness_ortho_ang = 1;
+    bool has_lin_motor = false, has_ang_motor = false, use_frame_a = true;
+    R lin_motor_target = 0, lin_motor_max = 0, ang_motor_target = 0, ang_motor_max = 0;
+    R lin_pos = 0, ang_pos = 0;  // per-step state
 };
 
 template <class R>
@@ -182,6 +195,36 @@ void relative_rotation_info(const M3<R>& tr_a, const M3<R>& tr_b, V3<R>& euler, 
     for (int i = 0; i < 3; ++i) axes[i] = axes[i].normalize();
 }
 
+// shared.rs:30-55 (adjust_angle_to_limits)
+template <class R>
+R adjust_angle_to_limits(R angle, R lo, R hi) {
+    const R two_pi = R(2) * R(3.14159265358979323846);
+    if (lo >= hi) return angle;
+    if (angle < lo) {
+        R diff_lo = std::fabs(normalize_angle(lo - angle));
+        R diff_hi = std::fabs(normalize_angle(hi - angle));
+        return diff_lo < diff_hi ? angle : angle + two_pi;
+    }
+    if (angle > hi) {
+        R diff_hi = std::fabs(normalize_angle(angle - hi));
+        R diff_lo = std::fabs(normalize_angle(angle - lo));
+        return diff_lo < diff_hi ? angle - two_pi : angle;
+    }
+    return angle;
+}
+
+// shared.rs:126-145 (mirrored_row_limits): Bullet's window [lower, upper] in the row convention.
+template <class R>
+void mirrored_row_limits(R lower, R upper, uint32_t& lim, R& lo, R& hi) {
+    const bool lower_inf = std::isinf(lower) && lower < R(0);
+    const bool upper_inf = std::isinf(upper) && upper > R(0);
+    lo = 0; hi = 0;
+    if (lower_inf && upper_inf) lim = LIM_UNBOUNDED;
+    else if (lower_inf) lim = LIM_LOWER;   // lower bound 0
+    else if (upper_inf) lim = LIM_UPPER;   // upper bound 0
+    else { lim = LIM_BILATERAL; hi = (upper - lower) / R(2); lo = -hi; }
+}
+
 // glam Quat::from_rotation_arc (published algorithm): identity for parallel unit vectors, a half
 // turn about any orthonormal vector for opposite ones, else normalize(from x to, 1 + from . to).
 template <class R>
@@ -246,6 +289,150 @@ void prepare_joint_rows(Joint<R>& jt, uint32_t jid, const std::vector<B>& bodies
             V3<R> n;
             n.at(axis) = R(1);
             push(n, r_a.cross(n), n, r_b.cross(n), k * (pivot_a - pivot_b)[axis], lim, -jt.impulse_clamp, jt.impulse_clamp);
+        }
+    } else if (jt.kind == JOINT_GEAR) {  // gear.rs:33-57
+        V3<R> axis_a_world = a.orientation.rotate(jt.frame_a.basis.c2);
+        V3<R> axis_b_world = b.orientation.rotate(jt.frame_b.basis.c2);
+        push(zero, axis_a_world, zero, -(axis_b_world * jt.gear_ratio), R(0), LIM_UNBOUNDED, 0, 0);
+    } else if (jt.kind == JOINT_SLIDER) {  // slider.rs:159-475
+        const R eps = std::numeric_limits<R>::epsilon();
+        const R inf = std::numeric_limits<R>::infinity();
+        M3<R> tr_a = M3<R>::from_quat(a.orientation) * jt.frame_a.basis;
+        M3<R> tr_b = M3<R>::from_quat(b.orientation) * jt.frame_b.basis;
+        V3<R> pivot_a = a.position + a.orientation.rotate(jt.frame_a.origin);
+        V3<R> pivot_b = b.position + b.orientation.rotate(jt.frame_b.origin);
+        V3<R> delta = pivot_b - pivot_a;
+        V3<R> ax1_a = tr_a.c0;
+        R depth0 = delta.dot(tr_a.c0);
+        jt.lin_pos = depth0;
+        bool solve_lin_limit = false;
+        if (jt.lower_lin <= jt.upper_lin) {
+            if (depth0 > jt.upper_lin) { depth0 -= jt.upper_lin; solve_lin_limit = true; }
+            else if (depth0 < jt.lower_lin) { depth0 -= jt.lower_lin; solve_lin_limit = true; }
+            else depth0 = 0;
+        } else {
+            depth0 = 0;
+        }
+        const R lin_depth = depth0;
+        bool solve_ang_limit = false;
+        R ang_depth = 0;
+        if (jt.lower_ang <= jt.upper_ang) {
+            V3<R> axis_a0 = tr_a.c1, axis_a1 = tr_a.c2, axis_b0 = tr_b.c1;
+            R rot = adjust_angle_to_limits(std::atan2(axis_b0.dot(axis_a1), axis_b0.dot(axis_a0)), jt.lower_ang,
+                                           jt.upper_ang);
+            jt.ang_pos = rot;
+            if (rot < jt.lower_ang) { ang_depth = rot - jt.lower_ang; solve_ang_limit = true; }
+            else if (rot > jt.upper_ang) { ang_depth = rot - jt.upper_ang; solve_ang_limit = true; }
+        }
+        const R sign_fact = jt.use_frame_a ? R(1) : R(-1);
+        V3<R> ofs = pivot_b - pivot_a;
+        const R ima = a.inv_mass, imb = b.inv_mass;
+        const bool has_static = ima < eps || imb < eps;
+        const R ims = ima + imb;
+        const R fact_a = ims > R(0) ? imb / ims : R(0.5);
+        const R fact_b = R(1) - fact_a;
+        V3<R> ax1 = (ax1_a * fact_a + tr_b.c0 * fact_b).normalize();
+        const R k = inv_dt * (jt.softness_ortho_ang * erp);
+        V3<R> u = ax1_a.cross(tr_b.c0);
+        V3<R> rel_pa = pivot_a - a.position, rel_pb = pivot_b - b.position;
+        V3<R> ortho_a = rel_pa - ax1 * rel_pa.dot(ax1);
+        V3<R> ortho_b = rel_pb - ax1 * rel_pb.dot(ax1);
+        const R slider_offs = jt.lin_pos - depth0;
+        V3<R> total_dist = ax1 * (ax1.dot(pivot_a - a.position) + slider_offs) - ax1 * ax1.dot(pivot_b - b.position);
+        V3<R> rel_a = ortho_a + total_dist * fact_a;
+        V3<R> rel_b = ortho_b - total_dist * fact_b;
+        V3<R> avg = ortho_b * fact_a + ortho_a * fact_b;
+        V3<R> p = avg.length_squared() > eps ? avg.normalize() : tr_a.c1;
+        V3<R> q = ax1.cross(p);
+        push(zero, p, zero, p, -k * u.dot(p), LIM_UNBOUNDED, 0, 0);
+        push(zero, q, zero, q, -k * u.dot(q), LIM_UNBOUNDED, 0, 0);
+        const R k_lin = inv_dt * (jt.softness_ortho_lin * erp);
+        push(p, rel_a.cross(p), p, rel_b.cross(p), -k_lin * p.dot(ofs), LIM_UNBOUNDED, 0, 0);
+        {
+            V3<R> tmp_a = rel_a.cross(q), tmp_b = rel_b.cross(q);
+            if (has_static && solve_ang_limit) { tmp_a *= fact_a; tmp_b *= fact_b; }
+            push(q, tmp_a, q, tmp_b, -k_lin * q.dot(ofs), LIM_UNBOUNDED, 0, 0);
+        }
+        // linear limit / motor row
+        R limit_err = 0;
+        int limit = 0;
+        if (solve_lin_limit) {
+            limit_err = lin_depth * sign_fact;
+            limit = limit_err > R(0) ? 2 : 1;
+        }
+        bool powered = jt.has_lin_motor;
+        if (limit != 0 && jt.lower_lin == jt.upper_lin) powered = false;
+        if (limit != 0 || powered) {
+            const R curr_erp = erp;
+            R row_error = 0, lower = 0, upper = 0;
+            if (powered) {
+                R mf = motor_factor(jt.lin_pos, jt.lower_lin, jt.upper_lin, jt.lin_motor_target, inv_dt * curr_erp);
+                row_error -= sign_fact * mf * jt.lin_motor_target;
+                lower += -jt.lin_motor_max / inv_dt;
+                upper += jt.lin_motor_max / inv_dt;
+            }
+            if (limit != 0) {
+                row_error += inv_dt * curr_erp * limit_err;
+                if (jt.lower_lin == jt.upper_lin) { lower = -inf; upper = inf; }
+                else if (limit == 1) { lower = -inf; upper = 0; }
+                else { lower = 0; upper = inf; }
+                R bounce = std::fabs(R(1) - jt.damping_lim_lin);
+                if (bounce > R(0)) {
+                    R vel = a.linear_velocity.dot(ax1) - b.linear_velocity.dot(ax1);
+                    vel *= sign_fact;
+                    if (limit == 1) {
+                        if (vel < R(0)) { R newc = -bounce * vel; if (newc > row_error) row_error = newc; }
+                    } else if (vel > R(0)) {
+                        R newc = -bounce * vel;
+                        if (newc < row_error) row_error = newc;
+                    }
+                }
+                row_error *= jt.softness_lim_lin;
+            }
+            uint32_t lim; R lo, hi;
+            mirrored_row_limits(lower, upper, lim, lo, hi);
+            V3<R> ang_a = has_static ? zero : rel_a.cross(ax1);
+            V3<R> ang_b = has_static ? zero : rel_b.cross(ax1);
+            push(ax1, ang_a, ax1, ang_b, -row_error, lim, lo, hi);
+        }
+        // angular limit / motor row
+        limit_err = 0;
+        limit = 0;
+        if (solve_ang_limit) {
+            limit_err = ang_depth;
+            limit = limit_err > R(0) ? 1 : 2;
+        }
+        powered = jt.has_ang_motor;
+        if (limit != 0 && jt.lower_ang == jt.upper_ang) powered = false;
+        if (limit != 0 || powered) {
+            const R curr_erp = erp;
+            R row_error = 0, lower = 0, upper = 0;
+            if (powered) {
+                R mf = motor_factor(jt.ang_pos, jt.lower_ang, jt.upper_ang, jt.ang_motor_target, inv_dt * curr_erp);
+                row_error = mf * jt.ang_motor_target;
+                lower = -jt.ang_motor_max / inv_dt;
+                upper = jt.ang_motor_max / inv_dt;
+            }
+            if (limit != 0) {
+                row_error += inv_dt * curr_erp * limit_err;
+                if (jt.lower_ang == jt.upper_ang) { lower = -inf; upper = inf; }
+                else if (limit == 1) { lower = 0; upper = inf; }
+                else { lower = -inf; upper = 0; }
+                R bounce = std::fabs(R(1) - jt.damping_lim_ang);
+                if (bounce > R(0)) {
+                    R vel = a.angular_velocity.dot(ax1) - b.angular_velocity.dot(ax1);
+                    if (limit == 1) {
+                        if (vel < R(0)) { R newc = -bounce * vel; if (newc > row_error) row_error = newc; }
+                    } else if (vel > R(0)) {
+                        R newc = -bounce * vel;
+                        if (newc < row_error) row_error = newc;
+                    }
+                }
+                row_error *= jt.softness_lim_ang;
+            }
+            uint32_t lim; R lo, hi;
+            mirrored_row_limits(lower, upper, lim, lo, hi);
+            push(zero, ax1, zero, ax1, -row_error, lim, lo, hi);
         }
     } else if (jt.kind == JOINT_FIXED) {
         M3<R> tr_a = M3<R>::from_quat(a.orientation) * jt.frame_a.basis;

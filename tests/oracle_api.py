@@ -71,6 +71,7 @@ def lib():
             "orc_world_add_joint": (U32, [P, D]),
             "orc_world_set_joint_order": (None, [P, ctypes.POINTER(U32), U32]),
             "orc_world_joint_angles": (None, [P, D]),
+            "orc_world_joint_positions": (None, [P, D]),
             "orc_world_num_joint_rows": (U32, [P]),
             "orc_world_joint_rows": (None, [P, D]),
             "orc_hinge_frames": (None, [ctypes.c_int, D, D, D, D, D]),
@@ -117,13 +118,16 @@ def body_desc(shape, pos, quat=(0, 0, 0, 1), linvel=(0, 0, 0), angvel=(0, 0, 0),
     return d
 
 
-JDESC = 37   # joint descriptor doubles (orc_world_add_joint)
-JOINT_POINT2POINT, JOINT_FIXED, JOINT_HINGE = 0, 1, 2
+JDESC = 52   # joint descriptor doubles (orc_world_add_joint)
+JOINT_POINT2POINT, JOINT_FIXED, JOINT_HINGE, JOINT_GEAR, JOINT_SLIDER = 0, 1, 2, 3, 4
 JF_DISABLE_COLLISIONS, JF_DISABLED, JF_ANGULAR_ONLY, JF_LIMIT, JF_MOTOR, JF_ERP = 1, 2, 4, 8, 16, 32
+JF_LIN_MOTOR, JF_ANG_MOTOR, JF_FRAME_B = 64, 128, 256
 
 
 def joint_desc(kind, body_a, body_b, frame_a, frame_b, flags=JF_DISABLE_COLLISIONS, erp=0.0, impulse_clamp=0.0,
-               limit=(1.0, -1.0), softness=0.9, bias_factor=0.3, relaxation=1.0, motor=(0.0, 0.0)):
+               limit=(1.0, -1.0), softness=0.9, bias_factor=0.3, relaxation=1.0, motor=(0.0, 0.0), gear_ratio=1.0,
+               lin_limits=(1.0, -1.0), ang_limits=(0.0, 0.0), slider_softness=(1.0, 1.0, 1.0, 1.0, 1.0, 1.0),
+               lin_motor=(0.0, 0.0), ang_motor=(0.0, 0.0)):
     """frame_*: 12 numbers (origin xyz, basis columns x, y, z) in the body's frame."""
     d = np.zeros(JDESC)
     d[0], d[1], d[2], d[3] = kind, body_a, body_b, flags
@@ -133,6 +137,12 @@ def joint_desc(kind, body_a, body_b, frame_a, frame_b, flags=JF_DISABLE_COLLISIO
     d[30], d[31] = limit
     d[32], d[33], d[34] = softness, bias_factor, relaxation
     d[35], d[36] = motor
+    d[37] = gear_ratio
+    d[38], d[39] = lin_limits
+    d[40], d[41] = ang_limits
+    d[42:48] = slider_softness  # softness lim lin, lim ang, damping lim lin, lim ang, ortho lin, ortho ang
+    d[48], d[49] = lin_motor
+    d[50], d[51] = ang_motor
     return d
 
 
@@ -277,6 +287,11 @@ class OracleWorld:
     def joint_angles(self, n):
         out = np.zeros(n)
         self.L.orc_world_joint_angles(self.h, dptr(out))
+        return out
+
+    def joint_positions(self, n):
+        out = np.zeros(n)
+        self.L.orc_world_joint_positions(self.h, dptr(out))
         return out
 
     def joint_rows(self):

@@ -195,16 +195,18 @@ def test_welded_pair_lands_on_the_ground_like_the_oracle(gpu):  # constraint/tes
     assert w.stats()["num_contacts"] > 0
 
 
-def chains(kinds, n_chains=400):
-    """n_chains eight-link chains of boxes dropped onto a plane; link k of chain c is a joint of
-    kind kinds[(c + k) % len(kinds)]."""
+def chains(kinds, n_chains=80):
+    """n_chains eight-link chains of boxes dropped onto a plane, five chains per row, rows 0.6 m
+    apart (no two chains touch at the start); link k of chain c is a joint of kind
+    kinds[(c + k) % len(kinds)]. 80 chains give two joint colours of 280 joints, more than
+    one block, so the grid-wide joint phases run."""
     s = JScene()
     s.body(s.shape(orc.PLANE, [0.0, 1.0, 0.0, 0.0]), (0, 0, 0), mass=0.0)
     box = s.shape(orc.BOX, [0.2, 0.1, 0.1])
     rng = np.random.default_rng(5)
     hfa, hfb = orc.hinge_frames((0.25, 0.0, 0.0), (0, 0, 1), (-0.25, 0.0, 0.0), (0, 0, 1))
     for c in range(n_chains):
-        x0, z0 = (c % 20) * 1.2 - 12.0, (c // 20) * 1.2 - 12.0
+        x0, z0 = (c % 5) * 4.5 - 11.0, (c // 5) * 0.6 - 5.0
         y0 = 0.5 + rng.uniform(0.0, 0.4)
         ids = [s.body(box, (x0 + 0.5 * k, y0, z0)) for k in range(8)]
         for k in range(7):
@@ -217,26 +219,25 @@ def chains(kinds, n_chains=400):
 
 
 def test_many_chains_on_the_ground_match_the_oracle(gpu):
-    """400 eight-link chains (point-to-point and hinge links, 2,800 joints, joint colours
-    larger than one block) fall onto a plane: grid-wide joint phases mixed with contacts.
-    The pose update's sin/cos may differ in the last ulp, and 3,200 colliding links amplify
-    that within a window, so the windows are 5 steps and the bound 1e-3 (the mixed convex
-    pile's); the rows themselves are compared one step from identical states below."""
-    w, _, _, _ = run_pair(chains((orc.JOINT_POINT2POINT, orc.JOINT_HINGE)), gpu, 40, tol=1e-3, window=5)
-    assert w.num_joints == 2800 and w.stats()["num_contacts"] > 0
+    """80 eight-link chains (point-to-point and hinge links, 560 joints, joint colours larger
+    than one block) fall onto a plane: grid-wide joint phases mixed with contacts. The pose
+    update's sin/cos and the redetect gate's acos may differ in the last ulp, so the windows
+    are 5 steps and the bound 1e-3 (the mixed convex pile's); the rows themselves are
+    compared one step from identical states below."""
+    w, _, _, _ = run_pair(chains((orc.JOINT_POINT2POINT, orc.JOINT_HINGE)), gpu, 30, tol=1e-3, window=5)
+    assert w.num_joints == 560 and w.stats()["num_contacts"] > 0
 
 
 def test_many_chains_with_fixed_links_match_the_oracle(gpu):
     """The same with a third of the links fixed joints, whose angular rows take their bias
-    from atan2/asin of the relative rotation (last-ulp differences between CUDA and the host
-    libm, amplified the same way): 5-step windows, 1e-3."""
-    w, _, _, _ = run_pair(chains((orc.JOINT_POINT2POINT, orc.JOINT_HINGE, orc.JOINT_FIXED)), gpu, 40, tol=1e-3,
+    from atan2/asin of the relative rotation: 5-step windows, 1e-3."""
+    w, _, _, _ = run_pair(chains((orc.JOINT_POINT2POINT, orc.JOINT_HINGE, orc.JOINT_FIXED)), gpu, 30, tol=1e-3,
                           window=5)
-    assert w.num_joints == 2800
+    assert w.num_joints == 560
 
 
 def test_chain_joint_rows_match_the_oracle_after_one_step(gpu):
-    """One step of the 400 chains from identical states: every joint row (ids, bodies, limit
+    """One step of the 80 chains from identical states: every joint row (ids, bodies, limit
     kind exact; effective mass, bias and accumulated impulse within 1e-5 relative)."""
     w, o = chains((orc.JOINT_POINT2POINT, orc.JOINT_HINGE, orc.JOINT_FIXED)).build(gpu)
     w.step(DT)
@@ -245,7 +246,7 @@ def test_chain_joint_rows_match_the_oracle_after_one_step(gpu):
     g, r = w.joint_rows(), o.joint_rows()
     rows_of = {orc.JOINT_POINT2POINT: 3, orc.JOINT_HINGE: 5, orc.JOINT_FIXED: 6}
     kinds = (orc.JOINT_POINT2POINT, orc.JOINT_HINGE, orc.JOINT_FIXED)
-    expected = sum(rows_of[kinds[(c + k) % 3]] for c in range(400) for k in range(7))
+    expected = sum(rows_of[kinds[(c + k) % 3]] for c in range(80) for k in range(7))
     assert g.shape == r.shape == (expected, 8)
     np.testing.assert_array_equal(g[:, [0, 1, 2, 5]], r[:, [0, 1, 2, 5]])
     np.testing.assert_allclose(g[:, [3, 4, 6]], r[:, [3, 4, 6]], rtol=1e-5, atol=1e-6)
@@ -292,3 +293,67 @@ def test_joint_descriptors_are_checked(gpu):
     w.add_joint(0, a, b, orc.frame((1, 0, 0)), orc.frame((-1, 0, 0)))
     with pytest.raises(gpu.BgpuError):
         gpu.Tape(w, 10)
+
+
+@pytest.mark.parametrize("ratio,pos_b,quat_a,spin", [
+    (2.0, (3.0, 0.0, 0.0), (0, 0, 0, 1), (0.0, 0.0, 6.0)),                                          # gear.rs:77-101
+    (1.0, (5.0, 1.0, -2.0), (0, 0, 0, 1), (0.0, 0.0, 6.0)),                                         # gear.rs:122-157
+    (1.0, (4.0, 0.0, 0.0), (math.sin(math.pi / 4), 0.0, 0.0, math.cos(math.pi / 4)), (0.0, -6.0, 0.0)),  # :159-187
+])
+def test_gear_matches_the_oracle(gpu, ratio, pos_b, quat_a, spin):
+    s = JScene((0.0, 0.0, 0.0))
+    sph = s.shape(orc.SPHERE, [0.5])
+    mass = 2.0 if ratio == 2.0 else 1.0
+    a = s.body(sph, (0.0, 0.0, 0.0), quat=quat_a, mass=mass, angvel=spin)
+    b = s.body(sph, pos_b, mass=mass)
+    s.joint(orc.JOINT_GEAR, a, b, orc.frame((0, 0, 0)), orc.frame((0, 0, 0)), gear_ratio=ratio)
+    _, _, st, _ = run_pair(s, gpu, 30)
+    if ratio == 2.0:
+        assert abs(st[9, b, 12] + st[9, a, 12] / 2.0) < 1e-3
+
+
+def slider_scene(box_pos, linvel=(0, 0, 0), angvel=(0, 0, 0), **kw):
+    s = JScene((0.0, 0.0, 0.0))
+    anchor = s.body(s.shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+    box = s.body(s.shape(orc.BOX, [0.3, 0.3, 0.3]), box_pos, linvel=linvel, angvel=angvel)
+    s.joint(orc.JOINT_SLIDER, anchor, box, orc.frame((0, 0, 0)), orc.frame((0, 0, 0)), **kw)
+    return s, box
+
+
+@pytest.mark.parametrize("case", ["slide", "limit", "motor", "angular_limit", "frame_b_motor"])
+def test_slider_matches_the_oracle(gpu, case):  # constraint/tests.rs:608-771
+    if case == "slide":
+        s, box = slider_scene((1.0, 0.0, 0.0), linvel=(1.5, 0.5, 0.2), angvel=(0.0, 0.0, 3.0))
+    elif case == "limit":
+        s, box = slider_scene((0.2, 0.0, 0.0), linvel=(4.0, 0.0, 0.0), lin_limits=(-0.3, 0.3))
+    elif case == "motor":
+        s, box = slider_scene((0.0, 0.0, 0.0), flags=orc.JF_DISABLE_COLLISIONS | orc.JF_LIN_MOTOR,
+                              lin_motor=(1.5, 100.0))
+    elif case == "angular_limit":
+        s, box = slider_scene((0.0, 0.0, 0.0), angvel=(3.0, 0.0, 0.0), ang_limits=(-0.4, 0.4))
+    else:
+        s, box = slider_scene((0.0, 0.0, 0.0), flags=orc.JF_DISABLE_COLLISIONS | orc.JF_LIN_MOTOR | orc.JF_FRAME_B,
+                              lin_motor=(-1.0, 50.0), lin_limits=(-1.0, 1.0))
+    positions = []
+
+    def each(step, w):
+        positions.append(float(w.joint_positions()[0]))
+
+    w, o, st, _ = run_pair(s, gpu, 150, each=each)
+    assert abs(positions[-1] - o.joint_positions(1)[0]) < 1e-3
+    if case == "limit":
+        assert st[:, box, 0].max() < 0.34
+    if case == "motor":
+        assert abs(st[-1, box, 0] - 3.75) < 0.3
+
+
+def test_slider_between_two_bodies_on_the_ground_matches_the_oracle(gpu):
+    """A slider between two dynamic boxes resting on a plane: contacts and the slider's
+    frame-offset rows (both bodies dynamic, so no static-body branch) in one solve."""
+    s = JScene()
+    s.body(s.shape(orc.PLANE, [0.0, 1.0, 0.0, 0.0]), (0, 0, 0), mass=0.0)
+    box = s.shape(orc.BOX, [0.3, 0.3, 0.3])
+    a = s.body(box, (0.0, 0.3, 0.0))
+    b = s.body(box, (1.0, 0.3, 0.0), linvel=(1.0, 0.0, 0.5))
+    s.joint(orc.JOINT_SLIDER, a, b, orc.frame((0.5, 0.0, 0.0)), orc.frame((-0.5, 0.0, 0.0)), lin_limits=(-0.2, 0.4))
+    run_pair(s, gpu, 120)

@@ -260,3 +260,102 @@ def test_hinge_frames_follow_the_pivot_axis_recipe():  # hinge.rs:60-100
         assert np.linalg.det(basis) == pytest.approx(1.0)
     # t1 = axis x (X when |axis.x| < 0.9), normalized; frame B's X is t1 carried by the shortest arc
     np.testing.assert_allclose(ba[:, 0], (0.0, 1.0, 0.0), atol=1e-12)
+
+
+def gear_world(precision, pos_b, ratio, quat_a=(0, 0, 0, 1)):
+    w = world(precision, (0.0, 0.0, 0.0))
+    sph = w.add_shape(orc.SPHERE, [0.5])
+    a = w.add_body(sph, (0, 0, 0), quat=quat_a, mass=2.0 if ratio == 2.0 else 1.0)
+    b = w.add_body(sph, pos_b, mass=2.0 if ratio == 2.0 else 1.0)
+    w.add_joint(orc.joint_desc(orc.JOINT_GEAR, a, b, orc.frame((0, 0, 0)), orc.frame((0, 0, 0)), gear_ratio=ratio))
+    return w, a, b
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_gears_couple_parallel_axes_to_opposite_spins(precision):  # gear.rs:77-101
+    w, a, b = gear_world(precision, (3.0, 0.0, 0.0), 2.0)
+    set_pose(w, a, angvel=(0.0, 0.0, 6.0))
+    for _ in range(10):
+        w.step(DT)
+    s = w.state()
+    wa, wb = s[a, 12], s[b, 12]
+    assert abs(wa - 4.8) < 1e-2 and abs(wb + 2.4) < 1e-2 and abs(wb + wa / 2.0) < 1e-3
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_gear_offset_bodies_feel_no_position_pull(precision):  # gear.rs:122-157
+    w, a, b = gear_world(precision, (5.0, 1.0, -2.0), 1.0)
+    set_pose(w, a, angvel=(0.0, 0.0, 6.0))
+    before = w.state()
+    for _ in range(30):
+        w.step(DT)
+    s = w.state()
+    assert abs(s[a, 0] - before[a, 0]) < 1e-5 and abs(s[a, 1] - before[a, 1]) < 1e-5
+    assert abs(s[b, 0] - before[b, 0]) < 1e-5 and abs(s[b, 2] - before[b, 2]) < 1e-5
+    assert abs(s[b, 12] + s[a, 12]) < 1e-3
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_gear_local_axes_follow_body_rotation(precision):  # gear.rs:159-187
+    q = (math.sin(math.pi / 4), 0.0, 0.0, math.cos(math.pi / 4))
+    w, a, b = gear_world(precision, (4.0, 0.0, 0.0), 1.0, quat_a=q)
+    set_pose(w, a, angvel=(0.0, -6.0, 0.0))
+    for _ in range(10):
+        w.step(DT)
+    s = w.state()
+    assert abs(s[a, 11] + 3.0) < 1e-2 and abs(s[b, 12] + 3.0) < 1e-2
+
+
+def slider_world(precision, box_pos, **kw):
+    w = world(precision, (0.0, 0.0, 0.0))
+    anchor = w.add_body(w.add_shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+    box = w.add_body(w.add_shape(orc.BOX, [0.3, 0.3, 0.3]), box_pos, mass=1.0)
+    w.add_joint(orc.joint_desc(orc.JOINT_SLIDER, anchor, box, orc.frame((0, 0, 0)), orc.frame((0, 0, 0)), **kw))
+    return w, box
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_slider_slides_along_its_axis(precision):  # tests.rs:608-646
+    w, box = slider_world(precision, (1.0, 0.0, 0.0))
+    set_pose(w, box, linvel=(1.5, 0.5, 0.2), angvel=(0.0, 0.0, 3.0))
+    max_off, max_rel = 0.0, 0.0
+    for _ in range(180):
+        w.step(DT)
+        s = w.state()[box]
+        max_off = max(max_off, abs(s[1]), abs(s[2]))
+        max_rel = max(max_rel, quat_angle(s[3:7]))
+    assert w.state()[box, 0] > 1.1 and max_off < 0.05 and max_rel < 0.15
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_slider_limit_stops_the_slide(precision):  # tests.rs:651-692
+    w, box = slider_world(precision, (0.2, 0.0, 0.0), lin_limits=(-0.3, 0.3))
+    set_pose(w, box, linvel=(4.0, 0.0, 0.0))
+    max_x, fired = 0.0, False
+    for _ in range(180):
+        w.step(DT)
+        rows = w.joint_rows()
+        fired |= bool(np.any((rows[:, 5] == 2) | (rows[:, 5] == 3)))  # a one-sided limit row
+        max_x = max(max_x, w.state()[box, 0])
+    assert max_x < 0.34 and fired and w.state()[box, 0] < 0.3
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_slider_motor_drives_along_the_axis(precision):  # tests.rs:697-735
+    w, box = slider_world(precision, (0.0, 0.0, 0.0), flags=orc.JF_DISABLE_COLLISIONS | orc.JF_LIN_MOTOR,
+                          lin_motor=(1.5, 100.0))
+    for _ in range(150):
+        w.step(DT)
+    s = w.state()[box]
+    assert abs(s[0] - 3.75) < 0.3 and abs(s[7]) < 1.8
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_slider_angular_limit_stops_the_twist(precision):  # tests.rs:738-771
+    w, box = slider_world(precision, (0.0, 0.0, 0.0), ang_limits=(-0.4, 0.4))
+    set_pose(w, box, angvel=(3.0, 0.0, 0.0))
+    max_ang = 0.0
+    for _ in range(180):
+        w.step(DT)
+        max_ang = max(max_ang, abs(w.joint_angles(1)[0]))
+    assert max_ang < 0.5
