@@ -16,6 +16,10 @@ SPHERE, BOX, CAPSULE, HULL, PLANE = 0, 1, 2, 3, 4
 JOINT_POINT2POINT, JOINT_FIXED, JOINT_HINGE, JOINT_GEAR, JOINT_SLIDER = 0, 1, 2, 3, 4
 JOINT_DISABLE_COLLISIONS, JOINT_DISABLED, JOINT_ANGULAR_ONLY, JOINT_LIMIT, JOINT_MOTOR, JOINT_ERP = 1, 2, 4, 8, 16, 32
 JOINT_LIN_MOTOR, JOINT_ANG_MOTOR, JOINT_FRAME_B = 64, 128, 256
+JOINT_SPRING2 = 5
+ROTATE_XYZ, ROTATE_XZY, ROTATE_YXZ, ROTATE_YZX, ROTATE_ZXY, ROTATE_ZYX = range(6)
+(S2_MOTOR, S2_SERVO, S2_SPRING, S2_STIFFNESS_LIMITED, S2_DAMPING_LIMITED, S2_STOP_ERP, S2_STOP_CFM, S2_MOTOR_ERP,
+ S2_MOTOR_CFM) = (1, 2, 4, 8, 16, 32, 64, 128, 256)
 NO_CONTACT_RESPONSE, DISABLE_WORLD_GRAVITY, KINEMATIC, ADDITIONAL_DAMPING = 0x1, 0x2, 0x4, 0x10
 STATE = 15
 CONTACT = 18
@@ -43,6 +47,156 @@ class JointDesc(ctypes.Structure):
                 ("softness_ortho_lin", ctypes.c_float), ("softness_ortho_ang", ctypes.c_float),
                 ("lin_motor_target_velocity", ctypes.c_float), ("lin_motor_max_force", ctypes.c_float),
                 ("ang_motor_target_velocity", ctypes.c_float), ("ang_motor_max_force", ctypes.c_float)]
+
+
+class Spring2Axis(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_float) for n in ("lower_limit", "upper_limit", "bounce", "stop_erp", "stop_cfm",
+                                              "motor_erp", "motor_cfm", "target_velocity", "max_motor_force",
+                                              "servo_target", "stiffness", "damping", "equilibrium_point")] + \
+        [("flags", ctypes.c_uint32)]
+
+
+class Spring2Desc(ctypes.Structure):
+    _fields_ = [("body_a", ctypes.c_uint32), ("body_b", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+                ("rotate_order", ctypes.c_uint32), ("frame_a", ctypes.c_float * 12), ("frame_b", ctypes.c_float * 12),
+                ("axis", Spring2Axis * 6)]
+
+
+_PI = np.float32(np.pi)
+_TWO_PI = np.float32(2.0) * _PI
+
+
+def _normalize_angle(angle):
+    """shared.rs:17-27 (normalize_angle) in f32."""
+    a = np.fmod(np.float32(angle), _TWO_PI)
+    if a < -_PI:
+        a = np.float32(a + _TWO_PI)
+    elif a > _PI:
+        a = np.float32(a - _TWO_PI)
+    return float(a)
+
+
+class Spring2:
+    """One generic 6DOF spring-2 joint (Generic6DofSpring2Constraint, generic6dof_spring2.rs:259-650)
+    with the reference's setters: axes 0-2 linear, 3-5 angular. Starts from Bullet's defaults
+    (linear locked, angular free), so a fresh joint is a ball joint."""
+
+    def __init__(self, body_a, body_b, frame_a=None, frame_b=None, rotate_order=ROTATE_XYZ,
+                 flags=JOINT_DISABLE_COLLISIONS):
+        self.desc = Spring2Desc()
+        lib().bgpu_spring2_desc_default(ctypes.byref(self.desc))
+        d = self.desc
+        d.body_a, d.body_b, d.flags, d.rotate_order = body_a, body_b, flags, rotate_order
+        if frame_a is not None:
+            d.frame_a[:] = [float(x) for x in frame_a]
+        if frame_b is not None:
+            d.frame_b[:] = [float(x) for x in frame_b]
+
+    @classmethod
+    def hinge2(cls, body_a, body_b, pos_a, quat_a, pos_b, quat_b, anchor, axis1, axis2):
+        """Generic6DofSpring2Constraint::hinge2 (PhysicsWorld::add_hinge2) from the bodies' poses."""
+        j = cls.__new__(cls)
+        j.desc = Spring2Desc()
+        args = [f32(v) for v in (pos_a, quat_a, pos_b, quat_b, anchor, axis1, axis2)]
+        check(lib().bgpu_spring2_hinge2(*[fptr(a) for a in args], body_a, body_b, ctypes.byref(j.desc)), "hinge2")
+        return j
+
+    def axis(self, i):
+        return self.desc.axis[i]
+
+    def set_linear_limits(self, lower, upper):
+        for i in range(3):
+            self.desc.axis[i].lower_limit, self.desc.axis[i].upper_limit = lower[i], upper[i]
+
+    def set_angular_limits(self, lower, upper):
+        for i in range(3):
+            a = self.desc.axis[3 + i]
+            a.lower_limit, a.upper_limit = _normalize_angle(lower[i]), _normalize_angle(upper[i])
+
+    def set_limit(self, axis, lo, hi):
+        a = self.desc.axis[axis]
+        if axis < 3:
+            a.lower_limit, a.upper_limit = lo, hi
+        else:
+            a.lower_limit, a.upper_limit = _normalize_angle(lo), _normalize_angle(hi)
+
+    def set_limit_reversed(self, axis, lo, hi):
+        a = self.desc.axis[axis]
+        if axis < 3:
+            a.lower_limit, a.upper_limit = lo, hi
+        else:
+            a.upper_limit, a.lower_limit = _normalize_angle(-lo), _normalize_angle(-hi)
+
+    def set_rotation_order(self, order):
+        self.desc.rotate_order = order
+
+    def set_bounce(self, axis, bounce):
+        self.desc.axis[axis].bounce = bounce
+
+    def _flag(self, axis, bit, on):
+        a = self.desc.axis[axis]
+        a.flags = (a.flags | bit) if on else (a.flags & ~bit)
+
+    def enable_motor(self, axis, on=True):
+        self._flag(axis, S2_MOTOR, on)
+
+    def set_servo(self, axis, on=True):
+        self._flag(axis, S2_SERVO, on)
+
+    def set_target_velocity(self, axis, velocity):
+        self.desc.axis[axis].target_velocity = velocity
+
+    def set_servo_target(self, axis, target):
+        """Angular targets wrap into [-pi, pi] (generic6dof_spring2.rs:489-514), in f32."""
+        if axis < 3:
+            self.desc.axis[axis].servo_target = target
+            return
+        t = np.float32(np.float32(target) + _PI)
+        m = np.fmod(t, _TWO_PI)
+        if m >= _TWO_PI:
+            t = np.float32(0.0)
+        elif m < 0:
+            t = np.float32(0.0) if np.float32(_TWO_PI + m) == _TWO_PI else np.float32(_TWO_PI + m)
+        else:
+            t = m
+        self.desc.axis[axis].servo_target = float(np.float32(t - _PI))
+
+    def set_max_motor_force(self, axis, force):
+        self.desc.axis[axis].max_motor_force = force
+
+    def enable_spring(self, axis, on=True):
+        self._flag(axis, S2_SPRING, on)
+
+    def set_stiffness(self, axis, stiffness, limit_needed=True):
+        self.desc.axis[axis].stiffness = stiffness
+        self._flag(axis, S2_STIFFNESS_LIMITED, limit_needed)
+
+    def set_damping(self, axis, damping, limit_needed=True):
+        self.desc.axis[axis].damping = damping
+        self._flag(axis, S2_DAMPING_LIMITED, limit_needed)
+
+    def set_equilibrium_point(self, axis, value):
+        self.desc.axis[axis].equilibrium_point = value
+
+    def set_stop_erp(self, axis, value):
+        self.desc.axis[axis].stop_erp = value
+        self._flag(axis, S2_STOP_ERP, True)
+
+    def set_stop_cfm(self, axis, value):
+        self.desc.axis[axis].stop_cfm = value
+        self._flag(axis, S2_STOP_CFM, True)
+
+    def set_motor_erp(self, axis, value):
+        self.desc.axis[axis].motor_erp = value
+        self._flag(axis, S2_MOTOR_ERP, True)
+
+    def set_motor_cfm(self, axis, value):
+        self.desc.axis[axis].motor_cfm = value
+        self._flag(axis, S2_MOTOR_CFM, True)
+
+    def axis_table(self):
+        """(6, 14) array: per axis the 13 parameters in field order, then the flags."""
+        return np.array([[getattr(a, f) for f, _ in Spring2Axis._fields_] for a in self.desc.axis], dtype=np.float64)
 
 
 class BodyDesc(ctypes.Structure):
@@ -114,6 +268,10 @@ def lib():
             "bgpu_selftest_wait_timeout": (S, [U32, U32P, F]),
             "bgpu_joint_desc_default": (None, [ctypes.POINTER(JointDesc)]),
             "bgpu_add_joints": (S, [P, U32, ctypes.POINTER(JointDesc), U32P]),
+            "bgpu_spring2_desc_default": (None, [ctypes.POINTER(Spring2Desc)]),
+            "bgpu_spring2_hinge2": (S, [F, F, F, F, F, F, F, U32, U32, ctypes.POINTER(Spring2Desc)]),
+            "bgpu_add_spring2_joints": (S, [P, U32, ctypes.POINTER(Spring2Desc), U32P]),
+            "bgpu_read_joint_spring2_state": (S, [P, F]),
             "bgpu_num_joints": (U32, [P]),
             "bgpu_read_joint_angles": (S, [P, F]),
             "bgpu_read_joint_positions": (S, [P, F]),
@@ -421,9 +579,23 @@ class World:
         check(self.L.bgpu_add_joints(self.h, 1, ctypes.byref(d), ctypes.byref(first)), "add_joints")
         return first.value
 
+    def add_spring2(self, joint):
+        """Adds a Spring2 joint (Constraint::generic_6dof_spring2); returns its joint id."""
+        first = ctypes.c_uint32()
+        check(self.L.bgpu_add_spring2_joints(self.h, 1, ctypes.byref(joint.desc), ctypes.byref(first)),
+              "add_spring2_joints")
+        return first.value
+
     @property
     def num_joints(self):
         return self.L.bgpu_num_joints(self.h)
+
+    def spring2_state(self):
+        """Per joint: Euler angles (3), pivot offset in frame A (3), fact_a, has_static_body."""
+        out = np.zeros((self.num_joints, 8), dtype=np.float32)
+        if len(out):
+            check(self.L.bgpu_read_joint_spring2_state(self.h, fptr(out)), "read_joint_spring2_state")
+        return out
 
     def joint_angles(self):
         out = np.zeros(self.num_joints, dtype=np.float32)
@@ -446,7 +618,7 @@ class World:
         return out
 
     def joint_rows(self):
-        """Rows of the last step in solve order: joint, body_a, body_b, mass, bias, limit kind, impulse, 0."""
+        """Rows of the last step in solve order: joint, body_a, body_b, mass, bias, limit kind, impulse, cfm."""
         n = ctypes.c_uint32()
         check(self.L.bgpu_read_joint_rows(self.h, None, 0, ctypes.byref(n)), "read_joint_rows")
         out = np.zeros((n.value, 8), dtype=np.float32)

@@ -195,26 +195,39 @@ struct Broadphase {
 // [6..8] frame B basis columns; [9] erp, impulse clamp, limit low, limit high;
 // [10] softness, bias factor, relaxation, motor target velocity; [11] motor max impulse, gear ratio;
 // slider: [12] linear limits low/high, angular limits low/high; [13] softness lim lin/ang, damping
-// lim lin/ang; [14] softness ortho lin/ang, linear motor target/max force; [15] angular motor.
+// lim lin/ang; [14] softness ortho lin/ang, linear motor target/max force; [15] angular motor;
+// spring 2: [9].x first float4 of the joint's axis table in JointsDev::aux, [9].y rotate order.
 constexpr uint32_t JOINT_F4 = 16;
+// Row capacity of a joint of every kind but spring 2, whose capacity follows its axis settings.
 constexpr uint32_t JOINT_MAX_ROWS = 6;
+// Spring-2 axis table (generic6dof_spring2.rs:47-232), S2_AXIS_F4 float4 per axis, axes 0-2
+// linear and 3-5 angular: [0] lower, upper, bounce, stop erp; [1] stop cfm, motor erp, motor cfm,
+// target velocity; [2] max motor force, servo target, stiffness, damping; [3] equilibrium point,
+// axis flags (S2_*), 0, 0.
+constexpr uint32_t S2_AXIS_F4 = 4;
+enum : uint32_t { S2_MOTOR = 1u, S2_SERVO = 2u, S2_SPRING = 4u, S2_STIFFNESS_LIMITED = 8u, S2_DAMPING_LIMITED = 16u,
+                  S2_STOP_ERP = 32u, S2_STOP_CFM = 64u, S2_MOTOR_ERP = 128u, S2_MOTOR_CFM = 256u };
 // Joint row, JROW_F4 float4: [0] lin_a | effective mass, [1] ang_a | bias, [2] lin_b | cfm,
 // [3] ang_b | limit kind (bits), [4] lower, upper, accumulated impulse, 0.
 constexpr uint32_t JROW_F4 = 5;
-enum : uint32_t { JK_POINT2POINT = 0, JK_FIXED = 1, JK_HINGE = 2, JK_GEAR = 3, JK_SLIDER = 4 };
+enum : uint32_t { JK_POINT2POINT = 0, JK_FIXED = 1, JK_HINGE = 2, JK_GEAR = 3, JK_SLIDER = 4, JK_SPRING2 = 5 };
 enum : uint32_t { JF_DISABLE_COLLISIONS = 1u, JF_DISABLED = 2u, JF_ANGULAR_ONLY = 4u, JF_LIMIT = 8u, JF_MOTOR = 16u, JF_ERP = 32u,
                   JF_LIN_MOTOR = 64u, JF_ANG_MOTOR = 128u, JF_FRAME_B = 256u };
-enum : uint32_t { JL_UNBOUNDED = 0, JL_BILATERAL = 1, JL_LOWER = 2, JL_UPPER = 3 };
+enum : uint32_t { JL_UNBOUNDED = 0, JL_BILATERAL = 1, JL_LOWER = 2, JL_UPPER = 3, JL_WINDOW = 4 };
 
 struct JointsDev {
     const float4* desc = nullptr;    // JOINT_F4 per joint id
     const uint32_t* order = nullptr; // solve slot -> joint id (joint colour by colour)
     const uint32_t* coff = nullptr;  // joint colour c owns slots [coff[c], coff[c + 1])
     uint32_t n = 0, ncol = 0;
-    float4* rows = nullptr;          // JOINT_MAX_ROWS rows of JROW_F4 per slot
+    float4* rows = nullptr;          // JROW_F4 per row; slot t's rows start at row row_off[t]
+    const uint32_t* row_off = nullptr;  // first row of each slot (its capacity ends at row_off[t + 1])
     uint32_t* count = nullptr;       // rows per slot this step
     float* angle = nullptr;          // hinge angle / slider angular position per joint id
     float* position = nullptr;       // slider linear position per joint id
+    const float4* aux = nullptr;     // spring-2 axis tables (S2_AXIS_F4 per axis, 6 axes per joint)
+    float4* s2_state = nullptr;      // spring 2, 8 floats per joint id: Euler angles, pivot offset, fact_a, static
+    float global_cfm = 0.0f;         // SolverInfo::global_cfm, the spring-2 rows' default compliance
 };
 
 // Rows of every joint for this step, from the current poses (constraint.rs:755-842).
@@ -238,7 +251,7 @@ __device__ __forceinline__ void solve_joint_slot(const JointsDev& jd, uint32_t t
     const M3 iia = load_iw_j(ia, ima), iib = load_iw_j(ib, imb);
     V3 la = from4(__ldcg(&linvel[ia])), wa = from4(__ldcg(&angvel[ia]));
     V3 lb = from4(__ldcg(&linvel[ib])), wb = from4(__ldcg(&angvel[ib]));
-    float4* row = jd.rows + size_t(t) * JOINT_MAX_ROWS * JROW_F4;
+    float4* row = jd.rows + size_t(jd.row_off[t]) * JROW_F4;
     for (uint32_t r = 0; r < cnt; ++r, row += JROW_F4) {
         const float4 r0 = row[0], r1 = row[1], r2 = row[2], r3 = row[3], r4 = row[4];
         const V3 lin_a = from4(r0), ang_a = from4(r1), lin_b = from4(r2), ang_b = from4(r3);
@@ -252,6 +265,7 @@ __device__ __forceinline__ void solve_joint_slot(const JointsDev& jd, uint32_t t
         if (lim == JL_BILATERAL) nw = fminf(fmaxf(nw, -r4.y), r4.y);
         else if (lim == JL_LOWER) nw = fmaxf(nw, r4.x);
         else if (lim == JL_UPPER) nw = fminf(nw, r4.y);
+        else if (lim == JL_WINDOW) nw = fminf(fmaxf(nw, r4.x), r4.y);
         row[4] = make_float4(r4.x, r4.y, nw, 0.0f);
         const float j = nw - old;
         if (j != 0.0f) {

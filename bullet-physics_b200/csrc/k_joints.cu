@@ -1,5 +1,5 @@
 // Joint rows of one step (constraint.rs:755-842; fixed.rs:33-90; hinge.rs:130-267; gear.rs:33-57;
-// slider.rs:159-475;
+// slider.rs:159-475; generic6dof_spring2.rs:650-1383;
 // row preparation sequential_impulse.rs:260-299), one thread per joint slot in solve
 // order. Each joint of an awake island is flattened into its rows from the current
 // (pre-integration) poses, with the reference's arithmetic: the three pivot rows along
@@ -95,13 +95,13 @@ struct RowOut {
     M3 iia, iib;
     // ConstraintRow::prepare (sequential_impulse.rs:260-299)
     __device__ __forceinline__ void push(V3 lin_a, V3 ang_a, V3 lin_b, V3 ang_b, float bias, uint32_t lim, float lo,
-                                         float hi) {
+                                         float hi, float cfm = 0.0f) {
         const float k = ima * len2(lin_a) + imb * len2(lin_b) + dot(ang_a, mul(iia, ang_a)) + dot(ang_b, mul(iib, ang_b));
         const float mass = k > 0.0f ? 1.0f / k : 0.0f;
         float4* r = row + size_t(n) * JROW_F4;
         r[0] = to4(lin_a, mass);
         r[1] = to4(ang_a, bias);
-        r[2] = to4(lin_b, 0.0f);
+        r[2] = to4(lin_b, cfm);
         r[3] = to4(ang_b, __uint_as_float(lim));
         r[4] = make_float4(lo, hi, 0.0f, 0.0f);
         ++n;
@@ -110,6 +110,299 @@ struct RowOut {
 
 __device__ __forceinline__ V3 axis_vec(int axis) {
     return V3{axis == 0 ? 1.0f : 0.0f, axis == 1 ? 1.0f : 0.0f, axis == 2 ? 1.0f : 0.0f};
+}
+
+// generic6dof_spring2.rs:1236-1241 (btGetMatrixElem): row index % 3 of column index / 3.
+__device__ __forceinline__ float mat_elem(const M3& m, int index) {
+    const V3& c = index < 3 ? m.c0 : (index < 6 ? m.c1 : m.c2);
+    return comp(c, index % 3);
+}
+
+// generic6dof_spring2.rs:1243-1373 (matrixToEuler* for the five orders other than XYZ)
+__device__ V3 matrix_to_euler(const M3& m, uint32_t order) {
+    const float half_pi = 1.57079632679489661923f;
+    auto e = [&](int i) { return mat_elem(m, i); };
+    switch (order) {
+        case 1: {  // XZY
+            const float fi = e(1);
+            if (fi < 1.0f) {
+                if (fi > -1.0f) return V3{atan2f(e(7), e(4)), atan2f(e(2), e(0)), asinf(-e(1))};
+                return V3{-atan2f(-e(6), e(8)), 0.0f, half_pi};
+            }
+            return V3{atan2f(-e(6), e(8)), 0.0f, -half_pi};
+        }
+        case 2: {  // YXZ
+            const float fi = e(5);
+            if (fi < 1.0f) {
+                if (fi > -1.0f) return V3{asinf(-e(5)), atan2f(e(2), e(8)), atan2f(e(3), e(4))};
+                return V3{half_pi, -atan2f(-e(1), e(0)), 0.0f};
+            }
+            return V3{-half_pi, atan2f(-e(1), e(0)), 0.0f};
+        }
+        case 3: {  // YZX
+            const float fi = e(3);
+            if (fi < 1.0f) {
+                if (fi > -1.0f) return V3{atan2f(-e(5), e(4)), atan2f(-e(6), e(0)), asinf(e(3))};
+                return V3{0.0f, -atan2f(e(7), e(8)), -half_pi};
+            }
+            return V3{0.0f, atan2f(e(7), e(8)), half_pi};
+        }
+        case 4: {  // ZXY
+            const float fi = e(7);
+            if (fi < 1.0f) {
+                if (fi > -1.0f) return V3{asinf(e(7)), atan2f(-e(6), e(8)), atan2f(-e(1), e(4))};
+                return V3{-half_pi, 0.0f, -atan2f(e(2), e(0))};
+            }
+            return V3{half_pi, 0.0f, atan2f(e(2), e(0))};
+        }
+        case 5: {  // ZYX
+            const float fi = e(6);
+            if (fi < 1.0f) {
+                if (fi > -1.0f) return V3{atan2f(e(7), e(8)), asinf(-e(6)), atan2f(e(3), e(0))};
+                return V3{0.0f, half_pi, -atan2f(-e(1), -e(2))};
+            }
+            return V3{0.0f, -half_pi, atan2f(-e(1), -e(2))};
+        }
+        default: return euler_xyz(m);
+    }
+}
+
+// generic6dof_spring2.rs:1375-1383 (mirrored_window)
+__device__ __forceinline__ void mirrored_window(float lower, float upper, uint32_t& lim, float& lo, float& hi) {
+    const bool lf = isfinite(lower), uf = isfinite(upper);
+    lo = 0.0f;
+    hi = 0.0f;
+    if (lf && uf) {
+        if (lower == -upper) { lim = JL_BILATERAL; hi = upper; lo = -upper; }
+        else { lim = JL_WINDOW; lo = -upper; hi = -lower; }
+    } else if (!lf && uf) { lim = JL_LOWER; lo = -upper; }
+    else if (lf && !uf) { lim = JL_UPPER; hi = -lower; }
+    else lim = JL_UNBOUNDED;
+}
+
+// One axis of a spring-2 joint, with its step state (testLimitValue: 0 free, 3 locked, 4 limited).
+struct S2Axis {
+    float lower, upper, bounce, stop_erp, stop_cfm, motor_erp, motor_cfm, target_velocity, max_motor_force,
+        servo_target, stiffness, damping, equilibrium;
+    uint32_t flags;
+    int current_limit;
+    float error, error_hi;
+};
+
+__device__ __forceinline__ S2Axis load_s2_axis(const float4* a, float erp, float global_cfm) {
+    const float4 x = a[0], y = a[1], z = a[2], w = a[3];
+    S2Axis m;
+    m.lower = x.x; m.upper = x.y; m.bounce = x.z;
+    m.flags = __float_as_uint(w.y);
+    // generic6dof_spring2.rs:690-709, :736-760: without its override flag an axis takes the
+    // global ERP / CFM
+    m.stop_erp = (m.flags & S2_STOP_ERP) ? x.w : erp;
+    m.stop_cfm = (m.flags & S2_STOP_CFM) ? y.x : global_cfm;
+    m.motor_erp = (m.flags & S2_MOTOR_ERP) ? y.y : erp;
+    m.motor_cfm = (m.flags & S2_MOTOR_CFM) ? y.z : global_cfm;
+    m.target_velocity = y.w; m.max_motor_force = z.x; m.servo_target = z.y; m.stiffness = z.z; m.damping = z.w;
+    m.equilibrium = w.x;
+    m.current_limit = 0; m.error = 0.0f; m.error_hi = 0.0f;
+    return m;
+}
+
+// generic6dof_spring2.rs:135-151, :237-256 (testLimitValue)
+__device__ __forceinline__ void s2_test_limit(S2Axis& m, float value) {
+    if (m.lower > m.upper) { m.current_limit = 0; m.error = 0.0f; }
+    else if (m.lower == m.upper) { m.error = value - m.lower; m.current_limit = 3; }
+    else { m.error = value - m.lower; m.error_hi = value - m.upper; m.current_limit = 4; }
+}
+
+// generic6dof_spring2.rs:1154-1162 (angular_axis_violated)
+__device__ __forceinline__ bool s2_violated(const S2Axis& m) {
+    const float t = 1.0e-3f;
+    return (m.current_limit == 3 && (m.error < -t || m.error > t)) ||
+           (m.current_limit == 4 && (m.error < -t || m.error_hi > t));
+}
+
+struct S2Ctx {
+    V3 r_a, r_b, va, vb, wa, wb;
+    M3 iia, iib;
+    float ima, imb, inv_dt, fact_a, fact_b;
+    bool has_static;
+};
+
+// generic6dof_spring2.rs:1113-1152 (push_row)
+__device__ __forceinline__ void s2_push(RowOut& out, const S2Ctx& c, V3 ax1, bool rotational, bool rot_allowed,
+                                        float bullet_error, float cfm, float lower, float upper) {
+    const V3 zero = V3{0.0f, 0.0f, 0.0f};
+    V3 lin_a = zero, lin_b = zero, ang_a = ax1, ang_b = ax1;
+    if (!rotational) {
+        lin_a = ax1;
+        lin_b = ax1;
+        ang_a = cross(c.r_a, ax1);
+        ang_b = cross(c.r_b, ax1);
+        if (c.has_static && !rot_allowed) { ang_a = ang_a * c.fact_a; ang_b = ang_b * c.fact_b; }
+    }
+    uint32_t lim;
+    float lo, hi;
+    mirrored_window(lower, upper, lim, lo, hi);
+    out.push(lin_a, ang_a, lin_b, ang_b, -bullet_error, lim, lo, hi, cfm);
+}
+
+// generic6dof_spring2.rs:846-1111 (push_limit_motor_rows): the limit pair or lock row, the
+// motor or servo row and the spring row of one axis, in that order.
+__device__ __noinline__ void s2_axis_rows(RowOut& out, const S2Ctx& c, const S2Axis& m, float position, V3 ax1,
+                                          bool rotational, bool rot_allowed) {
+    const float inf = INFINITY;
+    const float sign = rotational ? -1.0f : 1.0f;
+    const bool motor = (m.flags & S2_MOTOR) != 0, servo = (m.flags & S2_SERVO) != 0;
+    const float inv_dt = c.inv_dt;
+    if (m.current_limit == 4) {
+        const float vel = rotational ? dot(c.wa, ax1) - dot(c.wb, ax1) : dot(c.va, ax1) - dot(c.vb, ax1);
+        float row_error = inv_dt * m.stop_erp * m.error * sign;
+        if (rotational) {
+            if (row_error - vel * m.stop_erp > 0.0f) {
+                const float bounce_error = -m.bounce * vel;
+                if (bounce_error > row_error) row_error = bounce_error;
+            }
+        } else if (row_error - vel * m.stop_erp < 0.0f) {
+            const float bounce_error = -m.bounce * vel;
+            if (bounce_error < row_error) row_error = bounce_error;
+        }
+        if (rotational) s2_push(out, c, ax1, true, rot_allowed, row_error, m.stop_cfm, 0.0f, inf);
+        else s2_push(out, c, ax1, false, rot_allowed, row_error, m.stop_cfm, -inf, 0.0f);
+        row_error = inv_dt * m.stop_erp * m.error_hi * sign;
+        if (rotational) {
+            if (row_error - vel * m.stop_erp < 0.0f) {
+                const float bounce_error = -m.bounce * vel;
+                if (bounce_error < row_error) row_error = bounce_error;
+            }
+        } else if (row_error - vel * m.stop_erp > 0.0f) {
+            const float bounce_error = -m.bounce * vel;
+            if (bounce_error > row_error) row_error = bounce_error;
+        }
+        if (rotational) s2_push(out, c, ax1, true, rot_allowed, row_error, m.stop_cfm, -inf, 0.0f);
+        else s2_push(out, c, ax1, false, rot_allowed, row_error, m.stop_cfm, 0.0f, inf);
+    }
+    if (m.current_limit == 3) {
+        const float row_error = inv_dt * m.stop_erp * m.error * sign;
+        s2_push(out, c, ax1, rotational, rot_allowed, row_error, m.stop_cfm, -inf, inf);
+    }
+    if (motor && !servo) {
+        const float tag_vel = rotational ? m.target_velocity : -m.target_velocity;
+        const float mot_fact = motor_factor(position, m.lower, m.upper, tag_vel, inv_dt * m.motor_erp);
+        const float row_error = mot_fact * m.target_velocity;
+        const float f = m.max_motor_force / inv_dt;
+        s2_push(out, c, ax1, rotational, rot_allowed, row_error, m.motor_cfm, -f, f);
+    }
+    if (motor && servo) {
+        float error = position - m.servo_target;
+        float cur_servo_target = m.servo_target;
+        if (rotational) {
+            if (error > PI_F) { error -= 2.0f * PI_F; cur_servo_target += 2.0f * PI_F; }
+            if (error < -PI_F) { error += 2.0f * PI_F; cur_servo_target -= 2.0f * PI_F; }
+        }
+        const float targetvelocity = error < 0.0f ? -m.target_velocity : m.target_velocity;
+        const float tag_vel = -targetvelocity;
+        float mot_fact = 0.0f;
+        if (error != 0.0f) {
+            float low_limit, hi_limit;
+            if (m.lower > m.upper) {
+                low_limit = error > 0.0f ? cur_servo_target : -inf;
+                hi_limit = error < 0.0f ? cur_servo_target : inf;
+            } else {
+                low_limit = error > 0.0f && cur_servo_target > m.lower ? cur_servo_target : m.lower;
+                hi_limit = error < 0.0f && cur_servo_target < m.upper ? cur_servo_target : m.upper;
+            }
+            mot_fact = motor_factor(position, low_limit, hi_limit, tag_vel, inv_dt * m.motor_erp);
+        }
+        const float row_error = mot_fact * targetvelocity * sign;
+        const float f = m.max_motor_force / inv_dt;
+        s2_push(out, c, ax1, rotational, rot_allowed, row_error, m.motor_cfm, -f, f);
+    }
+    if (m.flags & S2_SPRING) {
+        const float error = position - m.equilibrium;
+        float vel;
+        if (rotational) vel = dot(c.wa, ax1) - dot(c.wb, ax1);
+        else vel = dot(c.va + cross(c.wa, c.r_a), ax1) - dot(c.vb + cross(c.wb, c.r_b), ax1);
+        float m_a = 1.0f / c.ima, m_b = 1.0f / c.imb;
+        if (rotational) {
+            if (c.ima != 0.0f) m_a = m_a * len2(c.r_a) + 1.0f / len(mul(c.iia, ax1));
+            if (c.imb != 0.0f) m_b = m_b * len2(c.r_b) + 1.0f / len(mul(c.iib, ax1));
+        }
+        const float mm = c.ima == 0.0f ? m_b : (c.imb == 0.0f ? m_a : m_a * m_b / (m_a + m_b));
+        const float dt = 1.0f / inv_dt;
+        float kd = m.damping, ks = m.stiffness;
+        const float angularfreq = sqrtf(ks / mm);
+        if ((m.flags & S2_STIFFNESS_LIMITED) && 0.25f < angularfreq * dt) ks = 1.0f / dt / dt / 16.0f * mm;
+        if ((m.flags & S2_DAMPING_LIMITED) && kd * dt > mm) kd = mm / dt;
+        const float fs = ks * error * dt;
+        const float fd = -kd * vel * sign * dt;
+        const float f = fs + fd;
+        const float row_error = vel + f / mm * sign;
+        const float minf = f < fd ? f : fd, maxf = f < fd ? fd : f;
+        float lo, hi;
+        if (!rotational) { lo = minf > 0.0f ? 0.0f : minf; hi = maxf < 0.0f ? 0.0f : maxf; }
+        else { lo = -maxf > 0.0f ? 0.0f : -maxf; hi = -minf < 0.0f ? 0.0f : -minf; }
+        s2_push(out, c, ax1, rotational, rot_allowed, row_error, 0.0f, lo, hi);
+    }
+}
+
+// generic6dof_spring2.rs:650-820 (prepare_rows) with calculate_angle_info (:1164-1233)
+__device__ __noinline__ void spring2_rows(RowOut& out, const BodyDev& b, const JointsDev& jd, uint32_t jid,
+                                          const float4* d, uint32_t ia, uint32_t ib, V3 pa, V3 pb, Q qa, Q qb,
+                                          V3 pivot_a, V3 pivot_b, float inv_dt, float erp) {
+    const uint32_t aux0 = __float_as_uint(d[9].x), order = __float_as_uint(d[9].y);
+    const float4* aux = jd.aux + aux0;
+    const M3 tr_a = mul(from_quat(qa), M3{from4(d[2]), from4(d[3]), from4(d[4])});
+    const M3 tr_b = mul(from_quat(qb), M3{from4(d[6]), from4(d[7]), from4(d[8])});
+    S2Ctx c;
+    c.r_a = pivot_a - pa;
+    c.r_b = pivot_b - pb;
+    c.va = from4(b.linvel[ia]); c.vb = from4(b.linvel[ib]);
+    c.wa = from4(b.angvel[ia]); c.wb = from4(b.angvel[ib]);
+    c.iia = out.iia; c.iib = out.iib; c.ima = out.ima; c.imb = out.imb;
+    c.inv_dt = inv_dt;
+    const V3 diff = mul(transpose(tr_a), pivot_b - pivot_a);
+    const V3 euler = matrix_to_euler(mul(transpose(tr_a), tr_b), order);
+    V3 axes[3];
+    switch (order) {
+        case 1: { const V3 axis0 = tr_b.c0, axis1 = tr_a.c1;
+                  axes[2] = cross(axis0, axis1); axes[0] = cross(axis1, axes[2]); axes[1] = cross(axes[2], axis0); break; }
+        case 2: { const V3 axis1 = tr_b.c1, axis2 = tr_a.c2;
+                  axes[0] = cross(axis1, axis2); axes[1] = cross(axis2, axes[0]); axes[2] = cross(axes[0], axis1); break; }
+        case 3: { const V3 axis0 = tr_a.c0, axis1 = tr_b.c1;
+                  axes[2] = cross(axis0, axis1); axes[0] = cross(axis1, axes[2]); axes[1] = cross(axes[2], axis0); break; }
+        case 4: { const V3 axis1 = tr_a.c1, axis2 = tr_b.c2;
+                  axes[0] = cross(axis1, axis2); axes[1] = cross(axis2, axes[0]); axes[2] = cross(axes[0], axis1); break; }
+        case 5: { const V3 axis0 = tr_a.c0, axis2 = tr_b.c2;
+                  axes[1] = cross(axis2, axis0); axes[0] = cross(axes[1], axis2); axes[2] = cross(axis0, axes[1]); break; }
+        default: { const V3 axis0 = tr_b.c0, axis2 = tr_a.c2;
+                   axes[1] = cross(axis2, axis0); axes[0] = cross(axes[1], axis2); axes[2] = cross(axis0, axes[1]); break; }
+    }
+    for (int i = 0; i < 3; ++i) axes[i] = normalize(axes[i]);
+    const float eps = 1.1920929e-7f;  // f32::EPSILON
+    c.has_static = c.ima < eps || c.imb < eps;
+    const float ims = c.ima + c.imb;
+    c.fact_a = ims > 0.0f ? c.imb / ims : 0.5f;
+    c.fact_b = 1.0f - c.fact_a;
+    jd.s2_state[2 * size_t(jid)] = to4(euler, diff.x);
+    jd.s2_state[2 * size_t(jid) + 1] = make_float4(diff.y, diff.z, c.fact_a, c.has_static ? 1.0f : 0.0f);
+    // the angular axes first (their limit states gate the linear rows' rot_allowed)
+    S2Axis ang[3];
+    float ang_pos[3];
+    for (int i = 0; i < 3; ++i) {
+        ang[i] = load_s2_axis(aux + (3 + i) * S2_AXIS_F4, erp, jd.global_cfm);
+        ang_pos[i] = adjust_angle_to_limits(comp(euler, i), ang[i].lower, ang[i].upper);
+        s2_test_limit(ang[i], ang_pos[i]);
+    }
+    for (int i = 0; i < 3; ++i)
+        if (ang[i].current_limit != 0 || (ang[i].flags & (S2_MOTOR | S2_SPRING)))
+            s2_axis_rows(out, c, ang[i], ang_pos[i], axes[i], true, true);
+    for (int i = 0; i < 3; ++i) {
+        S2Axis lin = load_s2_axis(aux + i * S2_AXIS_F4, erp, jd.global_cfm);
+        const float pos = comp(diff, i);
+        s2_test_limit(lin, pos);
+        if (lin.current_limit == 0 && !(lin.flags & (S2_MOTOR | S2_SPRING))) continue;
+        const bool rot_allowed = !(s2_violated(ang[(i + 1) % 3]) && s2_violated(ang[(i + 2) % 3]));
+        s2_axis_rows(out, c, lin, pos, i == 0 ? tr_a.c0 : (i == 1 ? tr_a.c1 : tr_a.c2), false, rot_allowed);
+    }
 }
 
 __global__ void k_joint_rows(BodyDev b, JointsDev jd, float inv_dt, float erp) {
@@ -128,7 +421,7 @@ __global__ void k_joint_rows(BodyDev b, JointsDev jd, float inv_dt, float erp) {
         return;
     }
     RowOut out;
-    out.row = jd.rows + size_t(t) * JOINT_MAX_ROWS * JROW_F4;
+    out.row = jd.rows + size_t(jd.row_off[t]) * JROW_F4;
     out.n = 0;
     out.iia = load_iw_body(b.iw, ia, out.ima);
     out.iib = load_iw_body(b.iw, ib, out.imb);
@@ -294,6 +587,8 @@ __global__ void k_joint_rows(BodyDev b, JointsDev jd, float inv_dt, float erp) {
             mirrored_row_limits(lower, upper, lim, lo, hi);
             out.push(zero, ax1, zero, ax1, -row_error, lim, lo, hi);
         }
+    } else if (kind == JK_SPRING2) {
+        spring2_rows(out, b, jd, jid, d, ia, ib, pa, pb, qa, qb, pivot_a, pivot_b, inv_dt, erp);
     } else if (kind == JK_GEAR) {  // gear.rs:33-57: the spins about the frames' z columns, coupled
         const V3 axis_a_world = rotate(qa, from4(d[4])), axis_b_world = rotate(qb, from4(d[8]));
         out.push(zero, axis_a_world, zero, -(axis_b_world * p11.y), 0.0f, JL_UNBOUNDED, 0.0f, 0.0f);

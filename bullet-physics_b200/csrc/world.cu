@@ -174,6 +174,13 @@ struct World {
     DevBuf<float4> joint_desc_d, joint_rows_d;
     DevBuf<uint32_t> joint_order_d, joint_coff_d, joint_count_d;
     DevBuf<float> joint_angle_d, joint_pos_d;
+    // spring-2 joints: descriptors by spring-2 index, the index of each joint id (-1: other
+    // kinds), axis tables and step state on the device; every slot's first row (slot order)
+    std::vector<bgpu_spring2_desc> s2_h;
+    std::vector<int32_t> joint_s2_h;
+    std::vector<uint32_t> joint_row_off_h;
+    DevBuf<float4> joint_aux_d, joint_s2_state_d;
+    DevBuf<uint32_t> joint_row_off_d;
     DevBuf<uint64_t> suppressed_d;  // sorted keys of the pairs a joint keeps from colliding
     uint32_t nsuppressed = 0;
 
@@ -417,20 +424,62 @@ struct World {
         j.count = joint_count_d.p;
         j.angle = joint_angle_d.p;
         j.position = joint_pos_d.p;
+        j.row_off = joint_row_off_d.p;
+        j.aux = joint_aux_d.p;
+        j.s2_state = joint_s2_state_d.p;
+        j.global_cfm = info.global_cfm;
         return j;
+    }
+
+    // Row capacity of joint j: JOINT_MAX_ROWS, or for a spring-2 joint its exact row count
+    // (generic6dof_spring2.rs:846-1111): per axis 2 limit rows (lower < upper) or 1 lock row
+    // (lower == upper), plus 1 for a motor or servo and 1 for a spring.
+    uint32_t joint_row_capacity(uint32_t j) const {
+        if (joint_s2_h[j] < 0) return JOINT_MAX_ROWS;
+        uint32_t r = 0;
+        for (const bgpu_spring2_axis& a : s2_h[size_t(joint_s2_h[j])].axis) {
+            r += a.lower_limit < a.upper_limit ? 2u : (a.lower_limit == a.upper_limit ? 1u : 0u);
+            r += (a.flags & BGPU_S2_MOTOR) ? 1u : 0u;
+            r += (a.flags & BGPU_S2_SPRING) ? 1u : 0u;
+        }
+        return r;
+    }
+
+    // Constraint::generic_6dof_spring2: validated, then added as joints of kind SPRING2 whose axis
+    // tables live beside the descriptors.
+    uint32_t add_spring2_joints(uint32_t cnt, const bgpu_spring2_desc* d) {
+        std::vector<bgpu_joint_desc> base(cnt);
+        for (uint32_t k = 0; k < cnt; ++k) {
+            if (d[k].rotate_order > BGPU_ROTATE_ZYX) throw InvalidArg{"unknown rotate order"};
+            for (const bgpu_spring2_axis& a : d[k].axis)
+                if (std::isnan(a.lower_limit) || std::isnan(a.upper_limit)) throw InvalidArg{"NaN axis limit"};
+            bgpu_joint_desc_default(&base[k]);
+            base[k].kind = BGPU_JOINT_SPRING2;
+            base[k].body_a = d[k].body_a;
+            base[k].body_b = d[k].body_b;
+            base[k].flags = d[k].flags & (BGPU_JOINT_DISABLE_COLLISIONS | BGPU_JOINT_DISABLED);
+            std::memcpy(base[k].frame_a, d[k].frame_a, sizeof(base[k].frame_a));
+            std::memcpy(base[k].frame_b, d[k].frame_b, sizeof(base[k].frame_b));
+        }
+        return add_joints(cnt, base.data(), d);
     }
 
     // PhysicsWorld::add_constraint. The joint graph is coloured here, once per change:
     // first fit in joint id order, with only dynamic bodies in conflict (static and
     // kinematic bodies take no impulse), so a joint colour never holds a dynamic body twice.
-    uint32_t add_joints(uint32_t cnt, const bgpu_joint_desc* d) {
+    uint32_t add_joints(uint32_t cnt, const bgpu_joint_desc* d, const bgpu_spring2_desc* s2 = nullptr) {
         for (uint32_t k = 0; k < cnt; ++k) {
-            if (d[k].kind > BGPU_JOINT_SLIDER) throw InvalidArg{"unknown joint kind"};
+            if (s2 ? d[k].kind != BGPU_JOINT_SPRING2 : d[k].kind > BGPU_JOINT_SLIDER)
+                throw InvalidArg{"unknown joint kind (spring-2 joints go through bgpu_add_spring2_joints)"};
             if (d[k].body_a >= n || d[k].body_b >= n || d[k].body_a == d[k].body_b)
                 throw InvalidArg{"joint bodies out of range or equal"};
         }
         const uint32_t first = uint32_t(joints_h.size());
         joints_h.insert(joints_h.end(), d, d + cnt);
+        for (uint32_t k = 0; k < cnt; ++k) {
+            joint_s2_h.push_back(s2 ? int32_t(s2_h.size()) : -1);
+            if (s2) s2_h.push_back(s2[k]);
+        }
         const uint32_t nj = uint32_t(joints_h.size());
         std::vector<uint4> hinfo(n);
         check_cuda(cudaMemcpyAsync(hinfo.data(), info_d.p, n * sizeof(uint4), cudaMemcpyDeviceToHost, stream), "d2h");
@@ -484,12 +533,40 @@ struct World {
             o[14] = make_float4(x.softness_ortho_lin, x.softness_ortho_ang, x.lin_motor_target_velocity,
                                 x.lin_motor_max_force);
             o[15] = make_float4(x.ang_motor_target_velocity, x.ang_motor_max_force, 0.0f, 0.0f);
+            if (joint_s2_h[j] >= 0) {
+                const uint32_t aux0 = uint32_t(joint_s2_h[j]) * 6u * S2_AXIS_F4;
+                o[9] = make_float4(__uint_as_float_host(aux0), __uint_as_float_host(s2_h[size_t(joint_s2_h[j])].rotate_order),
+                                   0.0f, 0.0f);
+            }
         }
+        // spring-2 axis tables (S2_AXIS_F4 per axis)
+        std::vector<float4> aux(std::max<size_t>(s2_h.size(), 1) * 6 * S2_AXIS_F4, make_float4(0, 0, 0, 0));
+        for (size_t k = 0; k < s2_h.size(); ++k)
+            for (int i = 0; i < 6; ++i) {
+                const bgpu_spring2_axis& a = s2_h[k].axis[i];
+                float4* o = &aux[(k * 6 + i) * S2_AXIS_F4];
+                o[0] = make_float4(a.lower_limit, a.upper_limit, a.bounce, a.stop_erp);
+                o[1] = make_float4(a.stop_cfm, a.motor_erp, a.motor_cfm, a.target_velocity);
+                o[2] = make_float4(a.max_motor_force, a.servo_target, a.stiffness, a.damping);
+                o[3] = make_float4(a.equilibrium_point, __uint_as_float_host(a.flags), 0.0f, 0.0f);
+            }
+        // every slot's first row, slot by slot in solve order
+        joint_row_off_h.assign(nj + 1, 0u);
+        for (uint32_t t = 0; t < nj; ++t) joint_row_off_h[t + 1] = joint_row_off_h[t] + joint_row_capacity(joint_order_h[t]);
         joint_desc_d.reserve(hd.size());
         joint_order_d.reserve(nj);
         joint_coff_d.reserve(ncol + 1);
         joint_count_d.reserve(nj);
-        joint_rows_d.reserve(size_t(nj) * JOINT_MAX_ROWS * JROW_F4);
+        joint_rows_d.reserve(std::max<size_t>(joint_row_off_h[nj], 1) * JROW_F4);
+        joint_row_off_d.reserve(nj + 1);
+        joint_aux_d.reserve(aux.size());
+        joint_s2_state_d.grow_keep(2 * size_t(nj), 2 * size_t(first), stream);
+        check_cuda(cudaMemsetAsync(joint_s2_state_d.p + 2 * size_t(first), 0, 2 * size_t(cnt) * sizeof(float4), stream),
+                   "memset");
+        check_cuda(cudaMemcpyAsync(joint_row_off_d.p, joint_row_off_h.data(), (nj + 1) * sizeof(uint32_t),
+                                   cudaMemcpyHostToDevice, stream), "upload joint row offsets");
+        check_cuda(cudaMemcpyAsync(joint_aux_d.p, aux.data(), aux.size() * sizeof(float4), cudaMemcpyHostToDevice, stream),
+                   "upload spring-2 axes");
         joint_angle_d.grow_keep(nj, first, stream);
         check_cuda(cudaMemsetAsync(joint_angle_d.p + first, 0, cnt * sizeof(float), stream), "memset");
         joint_pos_d.grow_keep(nj, first, stream);
@@ -1505,6 +1582,118 @@ bgpu_status bgpu_read_solve_order(bgpu_world* w, uint64_t* out, uint64_t cap, ui
     });
 }
 
+void bgpu_spring2_desc_default(bgpu_spring2_desc* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->flags = BGPU_JOINT_DISABLE_COLLISIONS;
+    o->rotate_order = BGPU_ROTATE_XYZ;
+    const float ident[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    for (int k = 0; k < 9; ++k) o->frame_a[3 + k] = o->frame_b[3 + k] = ident[k];
+    for (int i = 0; i < 6; ++i) {
+        bgpu_spring2_axis& a = o->axis[i];
+        const bool angular = i >= 3;
+        a.lower_limit = angular ? 1.0f : 0.0f;
+        a.upper_limit = angular ? -1.0f : 0.0f;
+        a.stop_erp = 0.2f;
+        a.motor_erp = 0.9f;
+        a.max_motor_force = angular ? 6.0f : 0.0f;
+    }
+}
+
+namespace {
+// shared.rs:17-27 (normalize_angle) on the host
+float normalize_angle_host(float angle) {
+    const float pi = 3.14159265358979323846f, two_pi = 2.0f * pi;
+    float a = std::fmod(angle, two_pi);
+    if (a < -pi) a += two_pi;
+    else if (a > pi) a -= two_pi;
+    return a;
+}
+// shared.rs:85-101 (euler_xyz) on the host
+bgpu::V3 euler_xyz_host(const bgpu::M3& m) {
+    const float half_pi = 1.57079632679489661923f;
+    const float r20 = m.c0.z, r21 = m.c1.z, r22 = m.c2.z, r10 = m.c0.y, r11 = m.c1.y, r01 = m.c1.x, r00 = m.c0.x;
+    if (r20 < 1.0f) {
+        if (r20 > -1.0f) return bgpu::V3{std::atan2(-r21, r22), std::asin(r20), std::atan2(-r10, r00)};
+        return bgpu::V3{-std::atan2(r01, r11), -half_pi, 0.0f};
+    }
+    return bgpu::V3{std::atan2(r01, r11), half_pi, 0.0f};
+}
+}  // namespace
+
+bgpu_status bgpu_spring2_hinge2(const float* pos_a, const float* quat_a, const float* pos_b, const float* quat_b,
+                                const float* anchor, const float* axis1, const float* axis2, uint32_t body_a,
+                                uint32_t body_b, bgpu_spring2_desc* out) {
+    if (!pos_a || !quat_a || !pos_b || !quat_b || !anchor || !axis1 || !axis2 || !out) return BGPU_ERR_INVALID_ARGUMENT;
+    using bgpu::V3;
+    using bgpu::M3;
+    const V3 pa{pos_a[0], pos_a[1], pos_a[2]}, pb{pos_b[0], pos_b[1], pos_b[2]}, an{anchor[0], anchor[1], anchor[2]};
+    const bgpu::Q qa{quat_a[0], quat_a[1], quat_a[2], quat_a[3]}, qb{quat_b[0], quat_b[1], quat_b[2], quat_b[3]};
+    // generic6dof_spring2.rs:338-350: axis1 is the frame z, axis2 the frame x, y = z x x
+    const V3 z_axis = bgpu::normalize(V3{axis1[0], axis1[1], axis1[2]});
+    const V3 x_axis = bgpu::normalize(V3{axis2[0], axis2[1], axis2[2]});
+    const V3 y_axis = bgpu::cross(z_axis, x_axis);
+    const M3 basis{x_axis, y_axis, z_axis};
+    const M3 rot_a = bgpu::from_quat(qa), rot_b = bgpu::from_quat(qb);
+    const M3 ba = bgpu::mul(bgpu::transpose(rot_a), basis), bb = bgpu::mul(bgpu::transpose(rot_b), basis);
+    const V3 oa = bgpu::mul(bgpu::transpose(rot_a), an - pa), ob = bgpu::mul(bgpu::transpose(rot_b), an - pb);
+    bgpu_spring2_desc_default(out);
+    out->body_a = body_a;
+    out->body_b = body_b;
+    auto put = [](float* f, const V3& o, const M3& m) {
+        const V3 c[4] = {o, m.c0, m.c1, m.c2};
+        for (int k = 0; k < 4; ++k) { f[3 * k] = c[k].x; f[3 * k + 1] = c[k].y; f[3 * k + 2] = c[k].z; }
+    };
+    put(out->frame_a, oa, ba);
+    put(out->frame_b, ob, bb);
+    // :352-362: linear x/y locked, z over [-1, 1]; angular x free, y locked, z +-pi/4
+    out->axis[2].lower_limit = -1.0f;
+    out->axis[2].upper_limit = 1.0f;
+    const float steer = 1.57079632679489661923f * 0.5f;
+    const float lo[3] = {1.0f, 0.0f, -steer}, hi[3] = {-1.0f, 0.0f, steer};
+    for (int i = 0; i < 3; ++i) {
+        out->axis[3 + i].lower_limit = normalize_angle_host(lo[i]);
+        out->axis[3 + i].upper_limit = normalize_angle_host(hi[i]);
+    }
+    // :363-367: the suspension spring on linear z
+    const float pi = 3.14159265358979323846f;
+    out->axis[2].flags |= BGPU_S2_SPRING | BGPU_S2_STIFFNESS_LIMITED | BGPU_S2_DAMPING_LIMITED;
+    out->axis[2].stiffness = pi * pi * 4.0f;
+    out->axis[2].damping = 0.01f;
+    // :368-376: the equilibrium is the construction pose (pivot offset and XYZ Euler angles)
+    const M3 tr_a = bgpu::mul(rot_a, ba), tr_b = bgpu::mul(rot_b, bb);
+    const V3 pivot_a = pa + bgpu::rotate(qa, oa), pivot_b = pb + bgpu::rotate(qb, ob);
+    const V3 diff = bgpu::mul(bgpu::transpose(tr_a), pivot_b - pivot_a);
+    const V3 euler = euler_xyz_host(bgpu::mul(bgpu::transpose(tr_a), tr_b));
+    for (int i = 0; i < 3; ++i) {
+        out->axis[i].equilibrium_point = bgpu::comp(diff, i);
+        out->axis[3 + i].equilibrium_point = bgpu::comp(euler, i);
+    }
+    return BGPU_OK;
+}
+
+bgpu_status bgpu_add_spring2_joints(bgpu_world* w, uint32_t n, const bgpu_spring2_desc* d, uint32_t* first_id) {
+    if (!w || (n && !d)) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        uint32_t f = w->impl.add_spring2_joints(n, d);
+        if (first_id) *first_id = f;
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_read_joint_spring2_state(bgpu_world* w, float* state) {
+    if (!w || !state) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        const size_t nj = W.joints_h.size();
+        if (!nj) return BGPU_OK;
+        bgpu::check_cuda(cudaMemcpyAsync(state, W.joint_s2_state_d.p, 2 * nj * sizeof(float4), cudaMemcpyDeviceToHost,
+                                         W.stream), "d2h");
+        bgpu::check_cuda(cudaStreamSynchronize(W.stream), "sync");
+        return BGPU_OK;
+    });
+}
+
 bgpu_status bgpu_add_joints(bgpu_world* w, uint32_t n, const bgpu_joint_desc* d, uint32_t* first_id) {
     if (!w || (n && !d)) return BGPU_ERR_INVALID_ARGUMENT;
     return guarded([&]() -> bgpu_status {
@@ -1558,7 +1747,7 @@ bgpu_status bgpu_read_joint_rows(bgpu_world* w, float* rows, uint32_t cap, uint3
         W.finish_stats();
         const uint32_t nj = uint32_t(W.joints_h.size());
         std::vector<uint32_t> cnt(nj);
-        std::vector<float4> r(size_t(nj) * bgpu::JOINT_MAX_ROWS * bgpu::JROW_F4);
+        std::vector<float4> r(size_t(nj ? W.joint_row_off_h[nj] : 0) * bgpu::JROW_F4);
         if (nj) {
             bgpu::check_cuda(cudaMemcpyAsync(cnt.data(), W.joint_count_d.p, nj * 4, cudaMemcpyDeviceToHost, W.stream), "d2h");
             bgpu::check_cuda(cudaMemcpyAsync(r.data(), W.joint_rows_d.p, r.size() * sizeof(float4), cudaMemcpyDeviceToHost,
@@ -1570,12 +1759,12 @@ bgpu_status bgpu_read_joint_rows(bgpu_world* w, float* rows, uint32_t cap, uint3
             const bgpu_joint_desc& jd = W.joints_h[W.joint_order_h[t]];
             for (uint32_t k = 0; k < cnt[t]; ++k, ++total) {
                 if (!rows || total >= cap) continue;
-                const float4* x = &r[(size_t(t) * bgpu::JOINT_MAX_ROWS + k) * bgpu::JROW_F4];
+                const float4* x = &r[(size_t(W.joint_row_off_h[t]) + k) * bgpu::JROW_F4];
                 float* o = rows + 8 * size_t(total);
                 uint32_t lim;
                 std::memcpy(&lim, &x[3].w, 4);
                 o[0] = float(W.joint_order_h[t]); o[1] = float(jd.body_a); o[2] = float(jd.body_b);
-                o[3] = x[0].w; o[4] = x[1].w; o[5] = float(lim); o[6] = x[4].z; o[7] = 0.0f;
+                o[3] = x[0].w; o[4] = x[1].w; o[5] = float(lim); o[6] = x[4].z; o[7] = x[2].w;
             }
         }
         if (out_n) *out_n = total;

@@ -138,7 +138,8 @@ typedef struct bgpu_step_stats {
  * columns. Rows are rebuilt every step from the current
  * poses and solved after the contacts in each PGS sweep (sequential_impulse.rs:720-735);
  * a joint of a sleeping island (both bodies inactive) produces no rows. */
-enum { BGPU_JOINT_POINT2POINT = 0, BGPU_JOINT_FIXED = 1, BGPU_JOINT_HINGE = 2, BGPU_JOINT_GEAR = 3, BGPU_JOINT_SLIDER = 4 };
+enum { BGPU_JOINT_POINT2POINT = 0, BGPU_JOINT_FIXED = 1, BGPU_JOINT_HINGE = 2, BGPU_JOINT_GEAR = 3, BGPU_JOINT_SLIDER = 4,
+       BGPU_JOINT_SPRING2 = 5 /* added through bgpu_add_spring2_joints only */ };
 #define BGPU_JOINT_DISABLE_COLLISIONS 0x01u /* no contacts between the two bodies (default on) */
 #define BGPU_JOINT_DISABLED 0x02u           /* set_enabled(false): no rows, no island link */
 #define BGPU_JOINT_ANGULAR_ONLY 0x04u       /* hinge: skip the three pivot rows */
@@ -167,6 +168,41 @@ typedef struct bgpu_joint_desc {
     float lin_motor_target_velocity, lin_motor_max_force, ang_motor_target_velocity, ang_motor_max_force;
 } bgpu_joint_desc;
 
+/* Generic 6DOF spring-2 joints (Generic6DofSpring2Constraint, generic6dof_spring2.rs; Bullet's
+ * btGeneric6DofSpring2Constraint). Axes 0-2 are linear along frame A's columns, 3-5 angular
+ * about the relative-rotation axes of rotate_order (BGPU_ROTATE_*). Per axis: lower > upper
+ * frees it, lower == upper locks it, lower < upper limits it with two one-sided elastic rows;
+ * a motor (or position servo), and a damped spring toward equilibrium_point, may be added.
+ * Axis fields mirror RotationalLimitMotor2 (:47-128) and TranslationalLimitMotor2 (:155-232).
+ * stop_erp / stop_cfm / motor_erp / motor_cfm apply only with their BGPU_S2_* override flag
+ * (setParam); without it the axis takes the solver's erp and global_cfm. Angular limits and
+ * servo targets are taken as given (set_limit / set_servo_target normalise them on the
+ * caller's side). */
+enum { BGPU_ROTATE_XYZ = 0, BGPU_ROTATE_XZY = 1, BGPU_ROTATE_YXZ = 2, BGPU_ROTATE_YZX = 3, BGPU_ROTATE_ZXY = 4,
+       BGPU_ROTATE_ZYX = 5 };
+#define BGPU_S2_MOTOR 0x01u              /* enable_motor */
+#define BGPU_S2_SERVO 0x02u              /* set_servo (with the motor) */
+#define BGPU_S2_SPRING 0x04u             /* enable_spring */
+#define BGPU_S2_STIFFNESS_LIMITED 0x08u  /* set_stiffness(.., limit_needed = true) */
+#define BGPU_S2_DAMPING_LIMITED 0x10u    /* set_damping(.., limit_needed = true) */
+#define BGPU_S2_STOP_ERP 0x20u           /* set_stop_erp override */
+#define BGPU_S2_STOP_CFM 0x40u           /* set_stop_cfm override */
+#define BGPU_S2_MOTOR_ERP 0x80u          /* set_motor_erp override */
+#define BGPU_S2_MOTOR_CFM 0x100u         /* set_motor_cfm override */
+typedef struct bgpu_spring2_axis {
+    float lower_limit, upper_limit, bounce, stop_erp, stop_cfm, motor_erp, motor_cfm;
+    float target_velocity, max_motor_force, servo_target, stiffness, damping, equilibrium_point;
+    uint32_t flags; /* BGPU_S2_* */
+} bgpu_spring2_axis;
+typedef struct bgpu_spring2_desc {
+    uint32_t body_a, body_b;
+    uint32_t flags;        /* BGPU_JOINT_DISABLE_COLLISIONS, BGPU_JOINT_DISABLED */
+    uint32_t rotate_order; /* BGPU_ROTATE_* */
+    float frame_a[12];
+    float frame_b[12];
+    bgpu_spring2_axis axis[6];
+} bgpu_spring2_desc;
+
 typedef struct bgpu_world bgpu_world;
 
 void bgpu_solver_info_default(bgpu_solver_info* out);
@@ -175,6 +211,18 @@ void bgpu_body_desc_default(bgpu_body_desc* out);
  * softness 0.9, bias factor 0.3, relaxation 1.0 (AngularLimit::new), gear ratio 1; slider:
  * linear axis free (1 > -1), rotation locked (0, 0), softness and damping 1 (SliderConstraint::new). */
 void bgpu_joint_desc_default(bgpu_joint_desc* out);
+/* Generic6DofSpring2Constraint::new: identity frames, collisions disabled, XYZ order, linear axes
+ * locked at 0 (max motor force 0), angular axes free (1 > -1, max motor force 6); stop ERP 0.2,
+ * motor ERP 0.9, everything else 0. */
+void bgpu_spring2_desc_default(bgpu_spring2_desc* out);
+/* Generic6DofSpring2Constraint::hinge2 (generic6dof_spring2.rs:329-377, Bullet's
+ * btHinge2Constraint): the wheel joint from the two bodies' poses, a world anchor, the steering
+ * axis axis1 and the spin axis axis2 (orthogonal): linear x/y locked, z a suspension spring
+ * (stiffness 4 pi^2, damping 0.01, both auto-clamped) over [-1, 1], angular x free, y locked, z
+ * limited to +-pi/4, equilibrium at the construction pose. Host arithmetic only. */
+bgpu_status bgpu_spring2_hinge2(const float* pos_a, const float* quat_a, const float* pos_b, const float* quat_b,
+                                const float* anchor, const float* axis1, const float* axis2, uint32_t body_a,
+                                uint32_t body_b, bgpu_spring2_desc* out);
 
 /* Library and device probes. */
 const char* bgpu_version(void);
@@ -272,7 +320,13 @@ bgpu_status bgpu_read_solve_order(bgpu_world* w, uint64_t* keys, uint64_t cap, u
 /* Joints (PhysicsWorld::add_constraint, world.rs): ids are consecutive from *first_id.
  * Rejects unknown kinds, out-of-range or equal bodies. */
 bgpu_status bgpu_add_joints(bgpu_world* w, uint32_t n, const bgpu_joint_desc* d, uint32_t* first_id);
+/* Spring-2 joints (Constraint::generic_6dof_spring2), in the same id space as bgpu_add_joints. */
+bgpu_status bgpu_add_spring2_joints(bgpu_world* w, uint32_t n, const bgpu_spring2_desc* d, uint32_t* first_id);
 uint32_t bgpu_num_joints(bgpu_world* w);
+/* Per joint, 8 floats of the last step that built its rows (spring-2 joints; 0 for the other
+ * kinds): the relative Euler angles (get_angle 0-2), the pivot offset in frame A
+ * (get_relative_pivot_position 0-2), fact_a and has_static_body (0 or 1). */
+bgpu_status bgpu_read_joint_spring2_state(bgpu_world* w, float* state);
 /* Per joint: the hinge angle (HingeConstraint::hinge_angle) or the slider's angular position
  * (ang_pos) of the last step that built its rows; 0 for the other kinds. */
 bgpu_status bgpu_read_joint_angles(bgpu_world* w, float* angles);
@@ -281,7 +335,7 @@ bgpu_status bgpu_read_joint_positions(bgpu_world* w, float* positions);
 /* Joint ids in the order their rows are solved (joint colour by colour). */
 bgpu_status bgpu_read_joint_order(bgpu_world* w, uint32_t* ids, uint32_t cap, uint32_t* out_n);
 /* Joint rows of the last step in solve order, 8 floats each: joint id, body_a, body_b,
- * effective mass, bias, limit kind, accumulated impulse, 0. */
+ * effective mass, bias, limit kind, accumulated impulse, cfm. */
 bgpu_status bgpu_read_joint_rows(bgpu_world* w, float* rows, uint32_t cap, uint32_t* out_n);
 bgpu_status bgpu_read_colour_batches(bgpu_world* w, uint32_t* groups, uint32_t* split_groups, uint32_t cap,
                                      uint32_t* out_n);

@@ -230,7 +230,7 @@ void orc_world_set_gravity(void* p, double gx, double gy, double gz) {
 }
 
 // params: erp2, linear_slop, restitution_threshold, split_impulse, split_threshold,
-// split_turn_erp, warmstarting_factor, global_cfm, sor, num_iterations
+// split_turn_erp, warmstarting_factor, global_cfm, sor, num_iterations, erp (joints), damping (joints)
 void orc_world_set_solver(void* p, const double* s) {
     Handle* h = static_cast<Handle*>(p);
     DISPATCH(h, {
@@ -239,6 +239,7 @@ void orc_world_set_solver(void* p, const double* s) {
         w.info.split_impulse = s[3] != 0; w.info.split_impulse_penetration_threshold = static_cast<R>(s[4]);
         w.info.split_impulse_turn_erp = static_cast<R>(s[5]); w.info.warmstarting_factor = static_cast<R>(s[6]); w.info.global_cfm = static_cast<R>(s[7]);
         w.info.sor = static_cast<R>(s[8]); w.info.num_iterations = uint32_t(s[9]);
+        w.info.erp = static_cast<R>(s[10]); w.info.damping = static_cast<R>(s[11]);
     });
 }
 
@@ -361,6 +362,22 @@ uint32_t orc_world_num_manifolds(void* p) {
     return r;
 }
 
+// RigidBody::ccd (body.rs:680-692): motion threshold and swept-sphere radius of body i.
+void orc_world_set_ccd(void* p, uint32_t i, double threshold, double radius) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, {
+        using R = std::remove_reference_t<decltype(w.gravity.x)>;
+        w.bodies[i].ccd_threshold = static_cast<R>(threshold);
+        w.bodies[i].ccd_radius = static_cast<R>(radius);
+    });
+}
+
+// CCD clamp fraction per body of the last step (1: not clamped).
+void orc_world_ccd_clamps(void* p, double* out) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, { for (size_t k = 0; k < w.last_ccd_clamps.size(); ++k) out[k] = w.last_ccd_clamps[k]; });
+}
+
 void orc_world_set_solve_order(void* p, const uint64_t* keys, uint32_t n) {
     Handle* h = static_cast<Handle*>(p);
     DISPATCH(h, { w.solve_order.assign(keys, keys + n); });
@@ -374,8 +391,11 @@ void orc_world_set_solve_order(void* p, const uint64_t* keys, uint32_t n) {
 // 37 gear ratio; slider: 38 lower / 39 upper linear limit, 40 lower / 41 upper angular limit,
 // 42 softness lim lin, 43 softness lim ang, 44 damping lim lin, 45 damping lim ang, 46 softness
 // ortho lin, 47 softness ortho ang, 48 / 49 linear motor target velocity / max force, 50 / 51
-// angular motor (flags 64 linear motor, 128 angular motor, 256 linear reference frame B).
-constexpr int JDESC = 52;
+// angular motor (flags 64 linear motor, 128 angular motor, 256 linear reference frame B);
+// spring 2: 52 rotate order, then per axis (0-2 linear, 3-5 angular) 14 values from 53 + 14 i:
+// lower, upper, bounce, stop erp, stop cfm, motor erp, motor cfm, target velocity, max motor
+// force, servo target, stiffness, damping, equilibrium point, axis flags (S2_*).
+constexpr int JDESC = 137;
 
 uint32_t orc_world_add_joint(void* p, const double* d) {
     Handle* h = static_cast<Handle*>(p);
@@ -418,6 +438,18 @@ uint32_t orc_world_add_joint(void* p, const double* d) {
         jt.has_lin_motor = (f & 64u) != 0;
         jt.has_ang_motor = (f & 128u) != 0;
         jt.use_frame_a = (f & 256u) == 0;
+        jt.rotate_order = uint32_t(d[52]);
+        for (int i = 0; i < 6; ++i) {
+            const double* x = d + 53 + 14 * i;
+            Spring2Axis<R>& m = jt.s2[i];
+            m.lower = static_cast<R>(x[0]); m.upper = static_cast<R>(x[1]); m.bounce = static_cast<R>(x[2]);
+            m.stop_erp = static_cast<R>(x[3]); m.stop_cfm = static_cast<R>(x[4]);
+            m.motor_erp = static_cast<R>(x[5]); m.motor_cfm = static_cast<R>(x[6]);
+            m.target_velocity = static_cast<R>(x[7]); m.max_motor_force = static_cast<R>(x[8]);
+            m.servo_target = static_cast<R>(x[9]); m.stiffness = static_cast<R>(x[10]);
+            m.damping = static_cast<R>(x[11]); m.equilibrium = static_cast<R>(x[12]);
+            m.flags = uint32_t(x[13]);
+        }
         w.joints.push_back(jt);
         r = uint32_t(w.joints.size() - 1);
     });
@@ -444,6 +476,37 @@ void orc_world_joint_positions(void* p, double* out) {
     DISPATCH(h, { for (size_t k = 0; k < w.joints.size(); ++k) out[k] = w.joints[k].lin_pos; });
 }
 
+// Per joint, 8 doubles of the spring-2 step state: Euler angles (3), pivot offset in A's frame
+// (3), fact_a, has_static_body.
+void orc_world_joint_spring2_state(void* p, double* out) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, {
+        for (size_t k = 0; k < w.joints.size(); ++k) {
+            const auto& jt = w.joints[k];
+            double* o = out + 8 * k;
+            for (int i = 0; i < 3; ++i) { o[i] = jt.s2_euler[i]; o[3 + i] = jt.s2_diff[i]; }
+            o[6] = jt.fact_a; o[7] = jt.has_static_body ? 1.0 : 0.0;
+        }
+    });
+}
+
+// generic6dof_spring2.rs:1164-1233 on two frames: Euler angles (3) then the three axes (9).
+void orc_spring2_angle_info(int f64, const double* tr_a, const double* tr_b, uint32_t order, double* out) {
+    auto run = [&](auto tag) {
+        using R = decltype(tag);
+        auto m3 = [](const double* c) {
+            return M3<R>(V3<R>(R(c[0]), R(c[1]), R(c[2])), V3<R>(R(c[3]), R(c[4]), R(c[5])),
+                         V3<R>(R(c[6]), R(c[7]), R(c[8])));
+        };
+        V3<R> euler, axes[3];
+        spring2_angle_info(m3(tr_a), m3(tr_b), order, euler, axes);
+        for (int i = 0; i < 3; ++i) out[i] = euler[i];
+        for (int a = 0; a < 3; ++a)
+            for (int i = 0; i < 3; ++i) out[3 + 3 * a + i] = axes[a][i];
+    };
+    if (f64) run(double(0)); else run(float(0));
+}
+
 uint32_t orc_world_num_joint_rows(void* p) {
     Handle* h = static_cast<Handle*>(p);
     uint32_t r = 0;
@@ -452,7 +515,7 @@ uint32_t orc_world_num_joint_rows(void* p) {
 }
 
 // Joint rows of the last step in solve order, 8 doubles each: joint, body_a, body_b, mass,
-// bias, limit kind, accumulated impulse, 0.
+// bias, limit kind, accumulated impulse, cfm.
 void orc_world_joint_rows(void* p, double* out) {
     Handle* h = static_cast<Handle*>(p);
     DISPATCH(h, {
@@ -460,7 +523,7 @@ void orc_world_joint_rows(void* p, double* out) {
             const auto& jr = w.last_joint_rows[k];
             double* o = out + 8 * k;
             o[0] = jr.joint; o[1] = jr.body_a; o[2] = jr.body_b; o[3] = jr.mass; o[4] = jr.bias;
-            o[5] = jr.lim; o[6] = jr.impulse; o[7] = 0;
+            o[5] = jr.lim; o[6] = jr.impulse; o[7] = jr.cfm;
         }
     });
 }

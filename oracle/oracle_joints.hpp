@@ -13,7 +13,10 @@
 //     axes are the frames' z columns here);
 //   crates/bullet-dynamics/src/constraint/slider.rs:159-475 (slider: frame-offset rows, linear and
 //     angular limits and motors), shared.rs:30-55 (adjust_angle_to_limits), :126-145
-//     (mirrored_row_limits).
+//     (mirrored_row_limits);
+//   crates/bullet-dynamics/src/constraint/generic6dof_spring2.rs:650-1383 (spring 2: per-axis
+//     limit pairs, lock rows, motors, servos, clamped springs, six Euler orders, static-body
+//     mass split), with the global ERP / CFM fallback of prepare_rows (constraint.rs:755-829).
 // Frame construction uses glam 0.33.3's `Quat::from_rotation_arc` (not in the reference tree);
 // its published algorithm is restated in rotation_arc() below.
 #pragma once
@@ -25,7 +28,7 @@
 
 namespace oracle {
 
-enum : uint32_t { JOINT_POINT2POINT = 0, JOINT_FIXED = 1, JOINT_HINGE = 2, JOINT_GEAR = 3, JOINT_SLIDER = 4 };
+enum : uint32_t { JOINT_POINT2POINT = 0, JOINT_FIXED = 1, JOINT_HINGE = 2, JOINT_GEAR = 3, JOINT_SLIDER = 4, JOINT_SPRING2 = 5 };
 // RowLimits (sequential_impulse.rs): which clamp the accumulated impulse takes.
 enum : uint32_t { LIM_UNBOUNDED = 0, LIM_BILATERAL = 1, LIM_LOWER = 2, LIM_UPPER = 3, LIM_WINDOW = 4 };
 
@@ -39,6 +42,25 @@ template <class R>
 struct AngularLimit {  // constraint.rs:684-752
     R low = 0, high = 0, softness = R(0.9), bias_factor = R(0.3), relaxation = R(1);
 };
+
+// Generic6DofSpring2 per-axis parameters: RotationalLimitMotor2 (generic6dof_spring2.rs:47-128)
+// for the angular axes 3-5, and one column of TranslationalLimitMotor2 (:155-232) for the linear
+// axes 0-2. lower > upper frees the axis, == locks it, < limits it (two one-sided rows).
+enum : uint32_t {
+    S2_MOTOR = 1, S2_SERVO = 2, S2_SPRING = 4, S2_STIFFNESS_LIMITED = 8, S2_DAMPING_LIMITED = 16,
+    // per-axis ERP/CFM overrides (Bullet's BT_6DOF_FLAGS_*2): without them the global values apply
+    S2_STOP_ERP = 32, S2_STOP_CFM = 64, S2_MOTOR_ERP = 128, S2_MOTOR_CFM = 256
+};
+template <class R>
+struct Spring2Axis {
+    R lower = 1, upper = -1, bounce = 0, stop_erp = R(0.2), stop_cfm = 0, motor_erp = R(0.9), motor_cfm = 0;
+    R target_velocity = 0, max_motor_force = R(6), servo_target = 0, stiffness = 0, damping = 0, equilibrium = 0;
+    uint32_t flags = 0;
+    // per-step state (testLimitValue): 0 free, 3 locked, 4 limited
+    int current_limit = 0;
+    R error = 0, error_hi = 0, position = 0;
+};
+enum : uint32_t { ORDER_XYZ = 0, ORDER_XZY = 1, ORDER_YXZ = 2, ORDER_YZX = 3, ORDER_ZXY = 4, ORDER_ZYX = 5 };
 
 template <class R>
 struct Joint {
@@ -60,6 +82,15 @@ struct Joint {
     bool has_lin_motor = false, has_ang_motor = false, use_frame_a = true;
     R lin_motor_target = 0, lin_motor_max = 0, ang_motor_target = 0, ang_motor_max = 0;
     R lin_pos = 0, ang_pos = 0;  // per-step state
+    // generic 6DOF spring 2 (Generic6DofSpring2Constraint::new: linear axes locked, angular free)
+    uint32_t rotate_order = ORDER_XYZ;
+    Spring2Axis<R> s2[6];
+    V3<R> s2_diff, s2_euler;  // per-step state: pivot offset in A's frame, relative Euler angles
+    R fact_a = R(0.5), fact_b = R(0.5);
+    bool has_static_body = false;
+    Joint() {
+        for (int i = 0; i < 3; ++i) { s2[i].lower = 0; s2[i].upper = 0; s2[i].max_motor_force = 0; }
+    }
 };
 
 template <class R>
@@ -266,10 +297,305 @@ void hinge_frames(const V3<R>& pivot_a, const V3<R>& axis_a_in, const V3<R>& piv
     fb.basis = M3<R>(t1b, t2b, axis_b);
 }
 
+// generic6dof_spring2.rs:1236-1241 (btGetMatrixElem): row index % 3 of column index / 3.
+template <class R>
+R mat_elem(const M3<R>& m, int index) {
+    return m.col(index / 3)[index % 3];
+}
+
+// generic6dof_spring2.rs:1243-1373 (matrixToEuler{XZY,YXZ,YZX,ZXY,ZYX}); XYZ is euler_xyz above.
+// The gimbal fallback angles feed the state (the "exact" flag is ignored upstream).
+template <class R>
+V3<R> matrix_to_euler(const M3<R>& m, uint32_t order) {
+    const R half_pi = R(1.57079632679489661923);
+    auto e = [&](int i) { return mat_elem(m, i); };
+    switch (order) {
+        case ORDER_XZY: {
+            R fi = e(1);
+            if (fi < R(1)) {
+                if (fi > R(-1)) return V3<R>(std::atan2(e(7), e(4)), std::atan2(e(2), e(0)), std::asin(-e(1)));
+                return V3<R>(-std::atan2(-e(6), e(8)), R(0), half_pi);
+            }
+            return V3<R>(std::atan2(-e(6), e(8)), R(0), -half_pi);
+        }
+        case ORDER_YXZ: {
+            R fi = e(5);
+            if (fi < R(1)) {
+                if (fi > R(-1)) return V3<R>(std::asin(-e(5)), std::atan2(e(2), e(8)), std::atan2(e(3), e(4)));
+                return V3<R>(half_pi, -std::atan2(-e(1), e(0)), R(0));
+            }
+            return V3<R>(-half_pi, std::atan2(-e(1), e(0)), R(0));
+        }
+        case ORDER_YZX: {
+            R fi = e(3);
+            if (fi < R(1)) {
+                if (fi > R(-1)) return V3<R>(std::atan2(-e(5), e(4)), std::atan2(-e(6), e(0)), std::asin(e(3)));
+                return V3<R>(R(0), -std::atan2(e(7), e(8)), -half_pi);
+            }
+            return V3<R>(R(0), std::atan2(e(7), e(8)), half_pi);
+        }
+        case ORDER_ZXY: {
+            R fi = e(7);
+            if (fi < R(1)) {
+                if (fi > R(-1)) return V3<R>(std::asin(e(7)), std::atan2(-e(6), e(8)), std::atan2(-e(1), e(4)));
+                return V3<R>(-half_pi, R(0), -std::atan2(e(2), e(0)));
+            }
+            return V3<R>(half_pi, R(0), std::atan2(e(2), e(0)));
+        }
+        case ORDER_ZYX: {
+            R fi = e(6);
+            if (fi < R(1)) {
+                if (fi > R(-1)) return V3<R>(std::atan2(e(7), e(8)), std::asin(-e(6)), std::atan2(e(3), e(0)));
+                return V3<R>(R(0), half_pi, -std::atan2(-e(1), -e(2)));
+            }
+            return V3<R>(R(0), -half_pi, std::atan2(-e(1), -e(2)));
+        }
+        default: return euler_xyz(m);
+    }
+}
+
+// generic6dof_spring2.rs:1164-1233 (calculate_angle_info): Euler angles of trA^-1 trB in the
+// configured order and the three normalized world axes built from per-order cross products.
+template <class R>
+void spring2_angle_info(const M3<R>& tr_a, const M3<R>& tr_b, uint32_t order, V3<R>& euler, V3<R> axes[3]) {
+    euler = matrix_to_euler(tr_a.transpose() * tr_b, order);
+    switch (order) {
+        case ORDER_XZY: {
+            V3<R> axis0 = tr_b.c0, axis1 = tr_a.c1;
+            axes[2] = axis0.cross(axis1); axes[0] = axis1.cross(axes[2]); axes[1] = axes[2].cross(axis0);
+            break;
+        }
+        case ORDER_YXZ: {
+            V3<R> axis1 = tr_b.c1, axis2 = tr_a.c2;
+            axes[0] = axis1.cross(axis2); axes[1] = axis2.cross(axes[0]); axes[2] = axes[0].cross(axis1);
+            break;
+        }
+        case ORDER_YZX: {
+            V3<R> axis0 = tr_a.c0, axis1 = tr_b.c1;
+            axes[2] = axis0.cross(axis1); axes[0] = axis1.cross(axes[2]); axes[1] = axes[2].cross(axis0);
+            break;
+        }
+        case ORDER_ZXY: {
+            V3<R> axis1 = tr_a.c1, axis2 = tr_b.c2;
+            axes[0] = axis1.cross(axis2); axes[1] = axis2.cross(axes[0]); axes[2] = axes[0].cross(axis1);
+            break;
+        }
+        case ORDER_ZYX: {
+            V3<R> axis0 = tr_a.c0, axis2 = tr_b.c2;
+            axes[1] = axis2.cross(axis0); axes[0] = axes[1].cross(axis2); axes[2] = axis0.cross(axes[1]);
+            break;
+        }
+        default: {
+            V3<R> axis0 = tr_b.c0, axis2 = tr_a.c2;
+            axes[1] = axis2.cross(axis0); axes[0] = axes[1].cross(axis2); axes[2] = axis0.cross(axes[1]);
+            break;
+        }
+    }
+    for (int i = 0; i < 3; ++i) axes[i] = axes[i].normalize();
+}
+
+// generic6dof_spring2.rs:1375-1383 (mirrored_window): Bullet's window [lower, upper] in the row
+// convention (lambda_ours = -lambda_bullet).
+template <class R>
+void mirrored_window(R lower, R upper, uint32_t& lim, R& lo, R& hi) {
+    const bool lf = std::isfinite(lower), uf = std::isfinite(upper);
+    lo = 0; hi = 0;
+    if (lf && uf) {
+        if (lower == -upper) { lim = LIM_BILATERAL; hi = upper; lo = -upper; }
+        else { lim = LIM_WINDOW; lo = -upper; hi = -lower; }
+    } else if (!lf && uf) { lim = LIM_LOWER; lo = -upper; }
+    else if (lf && !uf) { lim = LIM_UPPER; hi = -lower; }
+    else lim = LIM_UNBOUNDED;
+}
+
+// generic6dof_spring2.rs:135-151 and :237-256 (testLimitValue)
+template <class R>
+void spring2_test_limit(Spring2Axis<R>& m, R value) {
+    if (m.lower > m.upper) { m.current_limit = 0; m.error = 0; }
+    else if (m.lower == m.upper) { m.error = value - m.lower; m.current_limit = 3; }
+    else { m.error = value - m.lower; m.error_hi = value - m.upper; m.current_limit = 4; }
+}
+
+// generic6dof_spring2.rs:1154-1162 (angular_axis_violated)
+template <class R>
+bool spring2_axis_violated(const Spring2Axis<R>& m) {
+    const R t = R(1.0e-3);
+    return (m.current_limit == 3 && (m.error < -t || m.error > t)) ||
+           (m.current_limit == 4 && (m.error < -t || m.error_hi > t));
+}
+
+// generic6dof_spring2.rs:650-820 (prepare_rows), :846-1111 (push_limit_motor_rows),
+// :1113-1152 (push_row): the rows of one spring-2 joint.
+template <class R, class B>
+void prepare_spring2_rows(Joint<R>& jt, uint32_t ia, uint32_t ib, const B& a, const B& b, R inv_dt, R erp,
+                          R global_cfm, std::vector<JointRow<R>>& out) {
+    const R pi = R(3.14159265358979323846);
+    const R inf = std::numeric_limits<R>::infinity();
+    M3<R> tr_a = M3<R>::from_quat(a.orientation) * jt.frame_a.basis;
+    M3<R> tr_b = M3<R>::from_quat(b.orientation) * jt.frame_b.basis;
+    V3<R> pivot_a = a.position + a.orientation.rotate(jt.frame_a.origin);
+    V3<R> pivot_b = b.position + b.orientation.rotate(jt.frame_b.origin);
+    V3<R> r_a = pivot_a - a.position, r_b = pivot_b - b.position;
+    V3<R> diff = tr_a.transpose() * (pivot_b - pivot_a);
+    jt.s2_diff = diff;
+    for (int i = 0; i < 3; ++i) spring2_test_limit(jt.s2[i], diff[i]);
+    V3<R> euler, axes[3];
+    spring2_angle_info(tr_a, tr_b, jt.rotate_order, euler, axes);
+    jt.s2_euler = euler;
+    for (int i = 0; i < 3; ++i) {
+        Spring2Axis<R>& m = jt.s2[3 + i];
+        m.position = adjust_angle_to_limits(euler[i], m.lower, m.upper);
+        spring2_test_limit(m, m.position);
+    }
+    const R mi_a = a.inv_mass, mi_b = b.inv_mass;
+    const R eps = std::numeric_limits<R>::epsilon();
+    jt.has_static_body = mi_a < eps || mi_b < eps;
+    const R mi_s = mi_a + mi_b;
+    jt.fact_a = mi_s > R(0) ? mi_b / mi_s : R(0.5);
+    jt.fact_b = R(1) - jt.fact_a;
+
+    auto push_row = [&](const V3<R>& ax1, bool rotational, bool rot_allowed, R bullet_error, R cfm, R lower,
+                        R upper) {
+        V3<R> lin_a, ang_a, lin_b, ang_b;
+        if (rotational) { ang_a = ax1; ang_b = ax1; }
+        else {
+            lin_a = ax1; lin_b = ax1;
+            ang_a = r_a.cross(ax1); ang_b = r_b.cross(ax1);
+            if (jt.has_static_body && !rot_allowed) { ang_a = ang_a * jt.fact_a; ang_b = ang_b * jt.fact_b; }
+        }
+        uint32_t lim; R lo, hi;
+        mirrored_window(lower, upper, lim, lo, hi);
+        out.push_back(prepare_joint_row(ia, ib, lin_a, ang_a, lin_b, ang_b, a, b, -bullet_error, lim, lo, hi));
+        out.back().cfm = cfm;
+    };
+    // stop/motor ERP and CFM of an axis: the override when its flag is set, else the global value
+    auto stop_erp = [&](const Spring2Axis<R>& m) { return (m.flags & S2_STOP_ERP) ? m.stop_erp : erp; };
+    auto stop_cfm = [&](const Spring2Axis<R>& m) { return (m.flags & S2_STOP_CFM) ? m.stop_cfm : global_cfm; };
+    auto motor_erp = [&](const Spring2Axis<R>& m) { return (m.flags & S2_MOTOR_ERP) ? m.motor_erp : erp; };
+    auto motor_cfm = [&](const Spring2Axis<R>& m) { return (m.flags & S2_MOTOR_CFM) ? m.motor_cfm : global_cfm; };
+
+    auto axis_rows = [&](const Spring2Axis<R>& m, R position, const V3<R>& ax1, bool rotational, bool rot_allowed) {
+        const R sign = rotational ? R(-1) : R(1);
+        const bool motor = (m.flags & S2_MOTOR) != 0, servo = (m.flags & S2_SERVO) != 0;
+        if (m.current_limit == 4) {
+            const R vel = rotational ? a.angular_velocity.dot(ax1) - b.angular_velocity.dot(ax1)
+                                     : a.linear_velocity.dot(ax1) - b.linear_velocity.dot(ax1);
+            const R serp = stop_erp(m);
+            R row_error = inv_dt * serp * m.error * sign;
+            if (rotational) {
+                if (row_error - vel * serp > R(0)) {
+                    R bounce_error = -m.bounce * vel;
+                    if (bounce_error > row_error) row_error = bounce_error;
+                }
+            } else if (row_error - vel * serp < R(0)) {
+                R bounce_error = -m.bounce * vel;
+                if (bounce_error < row_error) row_error = bounce_error;
+            }
+            if (rotational) push_row(ax1, rotational, rot_allowed, row_error, stop_cfm(m), R(0), inf);
+            else push_row(ax1, rotational, rot_allowed, row_error, stop_cfm(m), -inf, R(0));
+            row_error = inv_dt * serp * m.error_hi * sign;
+            if (rotational) {
+                if (row_error - vel * serp < R(0)) {
+                    R bounce_error = -m.bounce * vel;
+                    if (bounce_error < row_error) row_error = bounce_error;
+                }
+            } else if (row_error - vel * serp > R(0)) {
+                R bounce_error = -m.bounce * vel;
+                if (bounce_error > row_error) row_error = bounce_error;
+            }
+            if (rotational) push_row(ax1, rotational, rot_allowed, row_error, stop_cfm(m), -inf, R(0));
+            else push_row(ax1, rotational, rot_allowed, row_error, stop_cfm(m), R(0), inf);
+        }
+        if (m.current_limit == 3) {
+            R row_error = inv_dt * stop_erp(m) * m.error * sign;
+            push_row(ax1, rotational, rot_allowed, row_error, stop_cfm(m), -inf, inf);
+        }
+        if (motor && !servo) {
+            R tag_vel = rotational ? m.target_velocity : -m.target_velocity;
+            R mot_fact = motor_factor(position, m.lower, m.upper, tag_vel, inv_dt * motor_erp(m));
+            R row_error = mot_fact * m.target_velocity;
+            R f = m.max_motor_force / inv_dt;
+            push_row(ax1, rotational, rot_allowed, row_error, motor_cfm(m), -f, f);
+        }
+        if (motor && servo) {
+            R error = position - m.servo_target;
+            R cur_servo_target = m.servo_target;
+            if (rotational) {
+                if (error > pi) { error -= R(2) * pi; cur_servo_target += R(2) * pi; }
+                if (error < -pi) { error += R(2) * pi; cur_servo_target -= R(2) * pi; }
+            }
+            R targetvelocity = error < R(0) ? -m.target_velocity : m.target_velocity;
+            R tag_vel = -targetvelocity;
+            R mot_fact = R(0);
+            if (error != R(0)) {
+                R low_limit, hi_limit;
+                if (m.lower > m.upper) {
+                    low_limit = error > R(0) ? cur_servo_target : -inf;
+                    hi_limit = error < R(0) ? cur_servo_target : inf;
+                } else {
+                    low_limit = error > R(0) && cur_servo_target > m.lower ? cur_servo_target : m.lower;
+                    hi_limit = error < R(0) && cur_servo_target < m.upper ? cur_servo_target : m.upper;
+                }
+                mot_fact = motor_factor(position, low_limit, hi_limit, tag_vel, inv_dt * motor_erp(m));
+            }
+            R row_error = mot_fact * targetvelocity * sign;
+            R f = m.max_motor_force / inv_dt;
+            push_row(ax1, rotational, rot_allowed, row_error, motor_cfm(m), -f, f);
+        }
+        if (m.flags & S2_SPRING) {
+            R error = position - m.equilibrium;
+            R vel;
+            if (rotational) vel = a.angular_velocity.dot(ax1) - b.angular_velocity.dot(ax1);
+            else {
+                V3<R> tan_vel_a = a.angular_velocity.cross(r_a), tan_vel_b = b.angular_velocity.cross(r_b);
+                vel = (a.linear_velocity + tan_vel_a).dot(ax1) - (b.linear_velocity + tan_vel_b).dot(ax1);
+            }
+            R m_a = R(1) / mi_a, m_b = R(1) / mi_b;
+            if (rotational) {
+                if (mi_a != R(0)) {
+                    R rr_a = r_a.length_squared();
+                    m_a = m_a * rr_a + R(1) / (a.inv_inertia_world() * ax1).length();
+                }
+                if (mi_b != R(0)) {
+                    R rr_b = r_b.length_squared();
+                    m_b = m_b * rr_b + R(1) / (b.inv_inertia_world() * ax1).length();
+                }
+            }
+            R mm = mi_a == R(0) ? m_b : (mi_b == R(0) ? m_a : m_a * m_b / (m_a + m_b));
+            R dt = R(1) / inv_dt;
+            R kd = m.damping, ks = m.stiffness;
+            R angularfreq = std::sqrt(ks / mm);
+            if ((m.flags & S2_STIFFNESS_LIMITED) && R(0.25) < angularfreq * dt) ks = R(1) / dt / dt / R(16) * mm;
+            if ((m.flags & S2_DAMPING_LIMITED) && kd * dt > mm) kd = mm / dt;
+            R fs = ks * error * dt;
+            R fd = -kd * vel * sign * dt;
+            R f = fs + fd;
+            R row_error = vel + f / mm * sign;
+            R minf = f < fd ? f : fd;
+            R maxf = f < fd ? fd : f;
+            R lo, hi;
+            if (!rotational) { lo = minf > R(0) ? R(0) : minf; hi = maxf < R(0) ? R(0) : maxf; }
+            else { lo = -maxf > R(0) ? R(0) : -maxf; hi = -minf < R(0) ? R(0) : -minf; }
+            push_row(ax1, rotational, rot_allowed, row_error, R(0), lo, hi);
+        }
+    };
+    auto produces_rows = [](const Spring2Axis<R>& m) {
+        return m.current_limit != 0 || (m.flags & (S2_MOTOR | S2_SPRING)) != 0;
+    };
+    for (int i = 0; i < 3; ++i)
+        if (produces_rows(jt.s2[3 + i])) axis_rows(jt.s2[3 + i], jt.s2[3 + i].position, axes[i], true, true);
+    for (int i = 0; i < 3; ++i) {
+        if (!produces_rows(jt.s2[i])) continue;
+        const bool rot_allowed = !(spring2_axis_violated(jt.s2[3 + (i + 1) % 3]) &&
+                                   spring2_axis_violated(jt.s2[3 + (i + 2) % 3]));
+        axis_rows(jt.s2[i], diff[i], tr_a.col(i), false, rot_allowed);
+    }
+}
+
 // constraint.rs:755-842 + fixed.rs:33-90 + hinge.rs:130-267: the joint's rows for this step.
 template <class R, class B>
 void prepare_joint_rows(Joint<R>& jt, uint32_t jid, const std::vector<B>& bodies, R inv_dt, R erp,
-                        std::vector<JointRow<R>>& out) {
+                        std::vector<JointRow<R>>& out, R global_cfm = R(0)) {
     if (!jt.enabled) return;
     const uint32_t ia = jt.body_a, ib = jt.body_b;
     const B& a = bodies[ia];
@@ -290,6 +616,8 @@ void prepare_joint_rows(Joint<R>& jt, uint32_t jid, const std::vector<B>& bodies
             n.at(axis) = R(1);
             push(n, r_a.cross(n), n, r_b.cross(n), k * (pivot_a - pivot_b)[axis], lim, -jt.impulse_clamp, jt.impulse_clamp);
         }
+    } else if (jt.kind == JOINT_SPRING2) {
+        prepare_spring2_rows(jt, ia, ib, a, b, inv_dt, erp, global_cfm, out);
     } else if (jt.kind == JOINT_GEAR) {  // gear.rs:33-57
         V3<R> axis_a_world = a.orientation.rotate(jt.frame_a.basis.c2);
         V3<R> axis_b_world = b.orientation.rotate(jt.frame_b.basis.c2);

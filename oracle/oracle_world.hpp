@@ -10,6 +10,7 @@
 #include <map>
 #include <unordered_map>
 #include "oracle_joints.hpp"
+#include "oracle_ccd.hpp"
 #include "oracle_narrow.hpp"
 
 namespace oracle {
@@ -160,6 +161,7 @@ struct Body {  // body.rs:270-384 (rigid, shape by index)
     R deactivation_time = 0;
     R lin_sleep = R(0.8), ang_sleep = R(1.0);
     V3<R> push_linear, push_angular;
+    R ccd_threshold = 0, ccd_radius = 0;  // body.rs:365-367, 680-692 (RigidBody::ccd); 0 = off
 
     bool is_kinematic() const { return (flags & CF_KINEMATIC) != 0; }
     bool is_static_or_kinematic() const { return is_static || is_kinematic(); }
@@ -611,6 +613,7 @@ struct World {
     std::vector<Shape<R>> shapes;
     std::vector<Body<R>> bodies;
     std::vector<Aabb<R>> proxy_aabbs;  // broad-phase proxies (index = body index)
+    std::vector<R> last_ccd_clamps;    // CCD clamp fraction per body of the last step (1: none)
     V3<R> gravity = V3<R>(0, R(-9.81), 0);
     SolverInfo<R> info;
     std::unordered_map<uint64_t, PersistentManifold<R>> cache;
@@ -842,7 +845,7 @@ struct World {
             uint32_t jid = joint_order.empty() ? uint32_t(o) : joint_order[o];
             Joint<R>& jt = joints[jid];
             if (!bodies[jt.body_a].is_active() && !bodies[jt.body_b].is_active()) continue;
-            prepare_joint_rows(jt, jid, bodies, inv_dt, info.erp, jrows);
+            prepare_joint_rows(jt, jid, bodies, inv_dt, info.erp, jrows, info.global_cfm);
         }
         clk_mark(4);
         // 6. solve (step.rs:959-972)
@@ -863,8 +866,41 @@ struct World {
         clk_mark(5);
         // 6c. deactivation (step.rs:1059-1061)
         for (auto& b : bodies) b.update_deactivation(dt);
+        // 7a. CCD clamp fractions (step.rs:1068-1155): a fast CCD body is swept as a sphere from its
+        // position along v dt against every other body that passes the collision filters and whose
+        // broad-phase proxy AABB touches the swept box; the first hit fraction is kept.
+        std::vector<R> ccd_clamps(n, R(1));
+        for (size_t i = 0; i < n; ++i) {
+            const Body<R>& body = bodies[i];
+            const R threshold = body.ccd_threshold;
+            if (!body.is_active() || body.is_static_or_kinematic() || threshold <= R(0)) continue;
+            const R radius = body.ccd_radius;
+            if (radius <= R(0) || !shapes[body.shape].is_convex()) continue;
+            const V3<R> from = body.position;
+            const V3<R> to = from + body.linear_velocity * dt;
+            if ((to - from).length_squared() <= threshold * threshold) continue;
+            R best = R(1);
+            const Aabb<R> swept = Aabb<R>(from.min(to), from.max(to)).expanded(radius);
+            for (size_t j = 0; j < n; ++j) {
+                if (i == j) continue;
+                const Body<R>& other = bodies[j];
+                if (other.flags & CF_NO_CONTACT_RESPONSE) continue;
+                if (!suppressed.empty() &&
+                    std::binary_search(suppressed.begin(), suppressed.end(), pair_key(uint32_t(i), uint32_t(j))))
+                    continue;
+                if ((body.group & other.mask) == 0 || (other.group & body.mask) == 0) continue;
+                if (!proxy_aabbs[j].overlaps(swept)) continue;
+                SweepHit<R> hit;
+                if (swept_sphere_cast(from, to, radius, shapes[other.shape], other.position, other.orientation, hit) &&
+                    hit.fraction < best)
+                    best = hit.fraction;
+            }
+            ccd_clamps[i] = best;
+        }
+        last_ccd_clamps = ccd_clamps;
         // 7. integrate positions + split-impulse push (step.rs:1171-1215)
-        for (auto& b : bodies) {
+        for (size_t bi = 0; bi < n; ++bi) {
+            Body<R>& b = bodies[bi];
             if (!(b.is_static || !b.is_active())) {
                 V3<R> np; Quat<R> nq;
                 interpolate_pose(b.position, b.orientation, b.linear_velocity, b.angular_velocity, dt, np, nq);
@@ -881,6 +917,10 @@ struct World {
             }
             b.push_linear = V3<R>();
             b.push_angular = V3<R>();
+            if (ccd_clamps[bi] < R(1)) {  // step.rs:1210-1214
+                V3<R> from = b.position - b.linear_velocity * dt;
+                b.position = from + (b.position - from) * ccd_clamps[bi];
+            }
         }
         // 8. clear forces (step.rs:1272-1274)
         for (auto& b : bodies) { b.force = V3<R>(); b.torque = V3<R>(); }

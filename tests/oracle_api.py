@@ -75,6 +75,10 @@ def lib():
             "orc_world_num_joint_rows": (U32, [P]),
             "orc_world_joint_rows": (None, [P, D]),
             "orc_hinge_frames": (None, [ctypes.c_int, D, D, D, D, D]),
+            "orc_world_joint_spring2_state": (None, [P, D]),
+            "orc_world_set_ccd": (None, [P, U32, ctypes.c_double, ctypes.c_double]),
+            "orc_world_ccd_clamps": (None, [P, D]),
+            "orc_spring2_angle_info": (None, [ctypes.c_int, D, D, U32, D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -118,7 +122,7 @@ def body_desc(shape, pos, quat=(0, 0, 0, 1), linvel=(0, 0, 0), angvel=(0, 0, 0),
     return d
 
 
-JDESC = 52   # joint descriptor doubles (orc_world_add_joint)
+JDESC = 137   # joint descriptor doubles (orc_world_add_joint)
 JOINT_POINT2POINT, JOINT_FIXED, JOINT_HINGE, JOINT_GEAR, JOINT_SLIDER = 0, 1, 2, 3, 4
 JF_DISABLE_COLLISIONS, JF_DISABLED, JF_ANGULAR_ONLY, JF_LIMIT, JF_MOTOR, JF_ERP = 1, 2, 4, 8, 16, 32
 JF_LIN_MOTOR, JF_ANG_MOTOR, JF_FRAME_B = 64, 128, 256
@@ -127,8 +131,9 @@ JF_LIN_MOTOR, JF_ANG_MOTOR, JF_FRAME_B = 64, 128, 256
 def joint_desc(kind, body_a, body_b, frame_a, frame_b, flags=JF_DISABLE_COLLISIONS, erp=0.0, impulse_clamp=0.0,
                limit=(1.0, -1.0), softness=0.9, bias_factor=0.3, relaxation=1.0, motor=(0.0, 0.0), gear_ratio=1.0,
                lin_limits=(1.0, -1.0), ang_limits=(0.0, 0.0), slider_softness=(1.0, 1.0, 1.0, 1.0, 1.0, 1.0),
-               lin_motor=(0.0, 0.0), ang_motor=(0.0, 0.0)):
-    """frame_*: 12 numbers (origin xyz, basis columns x, y, z) in the body's frame."""
+               lin_motor=(0.0, 0.0), ang_motor=(0.0, 0.0), rotate_order=0, s2_axes=None):
+    """frame_*: 12 numbers (origin xyz, basis columns x, y, z) in the body's frame; s2_axes: the
+    (6, 14) spring-2 axis table (parameters in bgpu_spring2_axis field order, then the flags)."""
     d = np.zeros(JDESC)
     d[0], d[1], d[2], d[3] = kind, body_a, body_b, flags
     d[4:16] = frame_a
@@ -143,7 +148,26 @@ def joint_desc(kind, body_a, body_b, frame_a, frame_b, flags=JF_DISABLE_COLLISIO
     d[42:48] = slider_softness  # softness lim lin, lim ang, damping lim lin, lim ang, ortho lin, ortho ang
     d[48], d[49] = lin_motor
     d[50], d[51] = ang_motor
+    d[52] = rotate_order
+    if s2_axes is not None:
+        d[53:53 + 84] = np.asarray(s2_axes, dtype=np.float64).reshape(84)
     return d
+
+
+def spring2_joint_desc(joint):
+    """The oracle descriptor of a bgpu.Spring2 joint (same bodies, frames, order and axes)."""
+    d = joint.desc
+    return joint_desc(5, d.body_a, d.body_b, list(d.frame_a), list(d.frame_b), flags=d.flags,
+                      rotate_order=d.rotate_order, s2_axes=joint.axis_table())
+
+
+def spring2_angle_info(tr_a, tr_b, order, precision="f32"):
+    """generic6dof_spring2.rs:1164-1233: (Euler angles, 3 axes) of two 3x3 frames (numpy, row-major)."""
+    out = np.zeros(12)
+    a = np.ascontiguousarray(np.asarray(tr_a, dtype=np.float64).T.reshape(9))
+    b = np.ascontiguousarray(np.asarray(tr_b, dtype=np.float64).T.reshape(9))
+    lib().orc_spring2_angle_info(1 if precision == "f64" else 0, dptr(a), dptr(b), order, dptr(out))
+    return out[:3], out[3:].reshape(3, 3)
 
 
 def frame(origin, basis=np.eye(3)):
@@ -181,9 +205,9 @@ class OracleWorld:
 
     def set_solver(self, erp2=0.2, linear_slop=0.005, restitution_threshold=1.0, split_impulse=True,
                    split_threshold=-0.04, split_turn_erp=0.1, warmstarting_factor=0.85, global_cfm=0.0, sor=1.0,
-                   num_iterations=10):
+                   num_iterations=10, erp=0.2, damping=1.0):
         s = f64([erp2, linear_slop, restitution_threshold, 1.0 if split_impulse else 0.0, split_threshold,
-                 split_turn_erp, warmstarting_factor, global_cfm, sor, num_iterations])
+                 split_turn_erp, warmstarting_factor, global_cfm, sor, num_iterations, erp, damping])
         self.L.orc_world_set_solver(self.h, dptr(s))
 
     def set_brute_force(self, on=True):
@@ -292,6 +316,20 @@ class OracleWorld:
     def joint_positions(self, n):
         out = np.zeros(n)
         self.L.orc_world_joint_positions(self.h, dptr(out))
+        return out
+
+    def set_ccd(self, i, threshold, radius):
+        self.L.orc_world_set_ccd(self.h, i, threshold, radius)
+
+    def ccd_clamps(self):
+        out = np.ones(self.num_bodies)
+        self.L.orc_world_ccd_clamps(self.h, dptr(out))
+        return out
+
+    def spring2_state(self, n):
+        out = np.zeros((n, 8))
+        if n:
+            self.L.orc_world_joint_spring2_state(self.h, dptr(out))
         return out
 
     def joint_rows(self):

@@ -26,6 +26,7 @@ class JScene:
     def __init__(self, gravity=(0.0, -9.81, 0.0)):
         self.gravity = gravity
         self.shapes, self.bodies, self.joints = [], [], []
+        self.solver = {}
 
     def shape(self, kind, params):
         self.shapes.append((kind, list(params)))
@@ -39,11 +40,15 @@ class JScene:
     def joint(self, kind, a, b, fa, fb, **kw):
         self.joints.append((kind, a, b, np.asarray(fa, dtype=np.float64), np.asarray(fb, dtype=np.float64), kw))
 
+    def spring2(self, joint):
+        """A bgpu.Spring2 joint (its descriptor drives both worlds)."""
+        self.joints.append(("spring2", joint))
+
     def build(self, gpu):
-        w = gpu.World(gravity=self.gravity, num_iterations=10)
+        w = gpu.World(gravity=self.gravity, num_iterations=10, **self.solver)
         o = orc.OracleWorld("f32")
         o.set_gravity(self.gravity)
-        o.set_solver(num_iterations=10)
+        o.set_solver(num_iterations=10, **self.solver)
         for kind, params in self.shapes:
             w.add_shape(kind, params)
             o.add_shape(kind, params)
@@ -52,9 +57,13 @@ class JScene:
                        activation=b["activation"])
             o.add_body(b["shape"], b["pos"], quat=b["quat"], linvel=b["linvel"], angvel=b["angvel"], mass=b["mass"],
                        activation=b["activation"])
-        for kind, a, b, fa, fb, kw in self.joints:
-            gkw = dict(kw)
-            w.add_joint(kind, a, b, fa, fb, **gkw)
+        for jt in self.joints:
+            if jt[0] == "spring2":
+                w.add_spring2(jt[1])
+                o.add_joint(orc.spring2_joint_desc(jt[1]))
+                continue
+            kind, a, b, fa, fb, kw = jt
+            w.add_joint(kind, a, b, fa, fb, **kw)
             o.add_joint(orc.joint_desc(kind, a, b, fa, fb, **kw))
         o.set_joint_order(w.joint_order())
         return w, o
@@ -82,6 +91,9 @@ def run_pair(scene, gpu, steps, tol=1e-4, window=10, each=None):
             ga = w.joint_angles()
             ra = o.joint_angles(len(scene.joints))
             assert np.abs(ga - ra).max() <= 10 * tol, (step, ga, ra)
+            if any(jt[0] == "spring2" for jt in scene.joints):
+                gs, rs = w.spring2_state(), o.spring2_state(len(scene.joints))
+                assert np.abs(gs - rs).max() <= 10 * tol, (step, gs, rs)
         states.append(g)
         if each:
             each(step, w)
@@ -357,3 +369,214 @@ def test_slider_between_two_bodies_on_the_ground_matches_the_oracle(gpu):
     b = s.body(box, (1.0, 0.3, 0.0), linvel=(1.0, 0.0, 0.5))
     s.joint(orc.JOINT_SLIDER, a, b, orc.frame((0.5, 0.0, 0.0)), orc.frame((-0.5, 0.0, 0.0)), lin_limits=(-0.2, 0.4))
     run_pair(s, gpu, 120)
+
+
+def spring2_pair(b_quat=(0.0, 0.0, 0.0, 1.0), order=0, setup=None, gravity=(0.0, 0.0, 0.0), linvel_b=(0, 0, 0),
+                 angvel_b=(0, 0, 0)):
+    """generic6dof_spring2.rs:1590-1630: two never-sleeping 1 kg spheres at x = -1 and +1 joined at
+    the origin, B pre-rotated by b_quat with its pivot counter-rotated."""
+    import bgpu
+    s = JScene(gravity)
+    sph = s.shape(orc.SPHERE, [0.5])
+    a = s.body(sph, (-1.0, 0.0, 0.0), activation=orc.DISABLE_DEACTIVATION)
+    b = s.body(sph, (1.0, 0.0, 0.0), quat=b_quat, linvel=linvel_b, angvel=angvel_b,
+               activation=orc.DISABLE_DEACTIVATION)
+    inv = (-b_quat[0], -b_quat[1], -b_quat[2], b_quat[3])
+    j = bgpu.Spring2(a, b, orc.frame((1.0, 0.0, 0.0)), orc.frame(rotate(inv, (-1.0, 0.0, 0.0))), rotate_order=order)
+    if setup:
+        setup(j)
+    s.spring2(j)
+    return s, a, b
+
+
+def quat_axis(axis, a):
+    v = [0.0, 0.0, 0.0]
+    v[axis] = math.sin(a / 2)
+    return (v[0], v[1], v[2], math.cos(a / 2))
+
+
+def _s2_case(case):
+    """The reference's spring-2 world tests (generic6dof_spring2.rs:1644-1903) as scenes."""
+    if case == "ball":  # :1644-1664
+        return spring2_pair(linvel_b=(0.0, 2.0, 0.0), angvel_b=(0.0, 0.0, 3.0)), 120
+    if case == "limit_inside":  # :1668-1706
+        return spring2_pair(quat_axis(0, 0.2), setup=lambda j: j.set_limit(3, -1.0, 1.0)), 120
+    if case == "limit_outside":
+        return spring2_pair(quat_axis(0, 1.5), setup=lambda j: j.set_limit(3, -1.0, 1.0)), 60
+    if case == "locked":  # :1709-1727
+        return spring2_pair(quat_axis(0, -0.5), setup=lambda j: j.set_limit(3, 0.3, 0.3)), 180
+
+    def spring_y(k, d=None):
+        def f(j):
+            j.enable_spring(4)
+            j.set_stiffness(4, k, True)
+            if d is not None:
+                j.set_damping(4, d, True)
+        return f
+    if case == "spring":  # :1730-1770
+        return spring2_pair(quat_axis(1, 0.3), setup=spring_y(40.0, 0.5)), 300
+    if case == "stiffness_clamp":  # :1773-1795
+        return spring2_pair(quat_axis(1, 0.3), setup=spring_y(1.0e6)), 240
+    if case == "damping_clamp":  # :1798-1822
+        return spring2_pair(quat_axis(1, 0.3), setup=spring_y(40.0, 100.0)), 300
+    if case == "linear_spring":  # :1825-1847
+        def f(j):
+            j.set_linear_limits((1.0, 1.0, 1.0), (-1.0, -1.0, -1.0))
+            j.enable_spring(0)
+            j.set_stiffness(0, 5.0, True)
+            j.set_damping(0, 0.5, True)
+            j.set_equilibrium_point(0, 0.5)
+        return spring2_pair(setup=f), 360
+    if case == "servo":  # :1850-1871
+        def f(j):
+            j.enable_motor(3)
+            j.set_servo(3)
+            j.set_servo_target(3, 0.5)
+            j.set_target_velocity(3, 2.0)
+            j.set_max_motor_force(3, 10.0)
+        return spring2_pair(setup=f), 300
+    if case == "overrides":  # :1874-1903, plus every override and a bounce
+        def f(j):
+            j.set_limit(3, -1.0, 1.0)
+            j.set_stop_erp(3, 0.3)
+            j.set_stop_cfm(3, 0.01)
+            j.set_bounce(3, 0.5)
+            j.set_limit(4, -0.2, 0.2)
+            j.enable_motor(5)
+            j.set_target_velocity(5, 1.0)
+            j.set_max_motor_force(5, 4.0)
+            j.set_motor_erp(5, 0.5)
+            j.set_motor_cfm(5, 0.02)
+        s = spring2_pair(quat_axis(0, 1.5), setup=f)
+        s[0].solver = dict(erp=0.5)
+        return s, 120
+    raise KeyError(case)
+
+
+@pytest.mark.parametrize("case", ["ball", "limit_inside", "limit_outside", "locked", "spring", "stiffness_clamp",
+                                  "damping_clamp", "linear_spring", "servo", "overrides"])
+def test_spring2_matches_the_oracle(gpu, case):
+    (s, a, b), steps = _s2_case(case)
+    angles = []
+    _, _, st, _ = run_pair(s, gpu, steps, each=lambda step, w: angles.append(w.spring2_state()[0].copy()))
+    angles = np.array(angles)
+    # the reference's own assertions on the GPU trajectory
+    if case == "limit_inside":
+        assert abs(angles[-1, 0] + 0.2) < 0.02
+    if case == "limit_outside":
+        assert angles[-1, 0] > -1.3
+    if case == "locked":
+        assert abs(angles[-1, 0] - 0.3) < 0.02
+    if case == "spring":
+        assert np.count_nonzero(np.diff(np.sign(angles[:, 1]))) >= 2 and np.abs(angles[:, 1]).max() < 0.35
+    if case == "damping_clamp":
+        assert angles[:, 1].max() <= 0.0
+    if case == "linear_spring":
+        assert abs(angles[-1, 3] - 0.5) < 0.05
+    if case == "servo":
+        assert abs(angles[-1, 0] - 0.5) < 0.05
+
+
+@pytest.mark.parametrize("order", [0, 1, 2, 3, 4, 5])
+def test_spring2_rotate_orders_match_the_oracle(gpu, order):
+    """Every Euler order, with a limited, a locked and a sprung angular axis and a linear spring."""
+    def f(j):
+        j.set_limit(3, -0.3, 0.4)
+        j.set_limit(4, 0.1, 0.1)
+        j.enable_spring(5)
+        j.set_stiffness(5, 20.0, True)
+        j.set_damping(5, 0.2, True)
+        j.set_limit(2, -0.1, 0.1)
+        j.enable_spring(2)
+        j.set_stiffness(2, 30.0, True)
+    q = (0.1, -0.2, 0.15, math.sqrt(1.0 - 0.01 - 0.04 - 0.0225))
+    (s, a, b) = spring2_pair(q, order=order, setup=f, gravity=(0.0, -9.81, 0.0), angvel_b=(1.0, -2.0, 0.5))
+    s.bodies[a]["mass"] = 0.0
+    s.bodies[a]["activation"] = 0
+    run_pair(s, gpu, 90)
+
+
+def test_spring2_rows_match_the_oracle(gpu):
+    """One step's rows (mass, bias, limit kind, impulse, cfm) of a joint with every row shape."""
+    def f(j):
+        j.set_limit(3, -1.0, 1.0)
+        j.set_stop_cfm(3, 0.01)
+        j.set_limit(4, 0.2, 0.2)
+        j.enable_motor(4)
+        j.set_target_velocity(4, 1.0)
+        j.enable_motor(5)
+        j.set_servo(5)
+        j.set_servo_target(5, 0.4)
+        j.set_target_velocity(5, 2.0)
+        j.enable_spring(5)
+        j.set_stiffness(5, 10.0, True)
+        j.set_linear_limits((0.0, -0.1, 1.0), (0.0, 0.1, -1.0))
+        j.enable_spring(2)
+        j.set_stiffness(2, 5.0, False)
+        j.set_damping(2, 0.5, False)
+    (s, a, b) = spring2_pair(quat_axis(0, 1.5), setup=f, angvel_b=(0.5, 0.2, -0.3))
+    w, o = s.build(gpu)
+    o.set_state(w.state().astype(np.float64))
+    w.step(DT)
+    o.step(DT)
+    g, r = w.joint_rows(), o.joint_rows()
+    assert g.shape == r.shape and len(g) == 2 + 2 + 2 + 1 + 2 + 1, (g.shape, r.shape)
+    np.testing.assert_array_equal(g[:, [0, 1, 2, 5]], r[:, [0, 1, 2, 5]])
+    np.testing.assert_allclose(g[:, [3, 4, 6, 7]], r[:, [3, 4, 6, 7]], rtol=1e-4, atol=1e-5)
+
+
+@pytest.mark.parametrize("case", ["suspension", "axle_spin", "steering"])
+def test_hinge2_matches_the_oracle(gpu, case):  # generic6dof_spring2.rs:2027-2111
+    import bgpu
+    gravity, radius, pos, angvel, steps = {
+        "suspension": ((0.0, 0.0, -9.8), 0.2, (0.0, 0.0, -0.3), (0.0, 0.0, 0.0), 240),
+        "axle_spin": ((0.0, 0.0, 0.0), 0.2, (0.0, 0.0, 0.0), (8.0, 0.0, 0.0), 60),
+        "steering": ((0.0, 0.0, 0.0), 0.15, (0.9, 0.0, 0.0), (0.0, 0.0, 6.0), 120),
+    }[case]
+    s = JScene(gravity)
+    chassis = s.body(s.shape(orc.SPHERE, [0.5]), (0.0, 0.0, 0.0), mass=0.0)
+    wheel = s.body(s.shape(orc.SPHERE, [radius]), pos, angvel=angvel)
+    s.spring2(bgpu.Spring2.hinge2(chassis, wheel, (0, 0, 0), (0, 0, 0, 1), pos, (0, 0, 0, 1), (0, 0, 0), (0, 0, 1),
+                                  (1, 0, 0)))
+    steer = []
+    _, _, st, _ = run_pair(s, gpu, steps, each=lambda step, w: steer.append(float(w.spring2_state()[0, 2])))
+    if case == "suspension":
+        assert -0.45 < st[-1, wheel, 2] < -0.10 and abs(st[-1, wheel, 9]) < 1.0
+    if case == "axle_spin":
+        assert st[-1, wheel, 10] > 7.5 and abs(st[-1, wheel, 2]) < 1e-4
+    if case == "steering":
+        assert max(abs(x) for x in steer) < math.pi / 4 + 0.15
+
+
+def spring2_chains(count=150, cols=15, links=3, spacing=4.0, base_height=4.0, pitch=0.55, half=0.2, mass=1.0,
+                   stiffness=5.0, damping=0.3):
+    """The reference's spring2_chains perf scene (tools/perf_scenes.json "spring2_chains";
+    examples/perf_scenes.rs add_spring2): static anchors with horizontal chains of boxes joined by
+    spring-2 joints whose three angular springs are on, never sleeping."""
+    import bgpu
+    s = JScene()
+    box = s.shape(orc.BOX, [half, half, half])
+    rows = -(-count // cols)
+    for k in range(count):
+        col, row = k % cols, k // cols
+        x = (col - (cols - 1) / 2.0) * spacing
+        z = (row - (rows - 1) / 2.0) * spacing
+        prev = s.body(box, (x, base_height, z), mass=0.0)
+        for i in range(1, links + 1):
+            body = s.body(box, (x + i * pitch, base_height, z), mass=mass, activation=orc.DISABLE_DEACTIVATION)
+            j = bgpu.Spring2(prev, body, orc.frame((pitch / 2.0, 0.0, 0.0)), orc.frame((-pitch / 2.0, 0.0, 0.0)))
+            for ax in range(3, 6):
+                j.enable_spring(ax)
+                j.set_stiffness(ax, stiffness, True)
+                j.set_damping(ax, damping, True)
+            s.spring2(j)
+            prev = body
+    return s
+
+
+def test_spring2_chains_match_the_oracle(gpu):
+    """The spring2_chains scene (150 chains, 450 joints of 6 rows): hanging under gravity."""
+    s = spring2_chains()
+    w, _, st, _ = run_pair(s, gpu, 120, tol=1e-3, window=5)
+    assert w.joint_rows().shape[0] == 450 * 6
+    assert st[-1, :, 1].min() < 3.9  # the chains sag
