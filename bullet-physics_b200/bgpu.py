@@ -272,6 +272,8 @@ def lib():
             "bgpu_spring2_hinge2": (S, [F, F, F, F, F, F, F, U32, U32, ctypes.POINTER(Spring2Desc)]),
             "bgpu_add_spring2_joints": (S, [P, U32, ctypes.POINTER(Spring2Desc), U32P]),
             "bgpu_read_joint_spring2_state": (S, [P, F]),
+            "bgpu_set_ccd": (S, [P, U32, U32, F, F]),
+            "bgpu_read_ccd_clamps": (S, [P, F]),
             "bgpu_num_joints": (U32, [P]),
             "bgpu_read_joint_angles": (S, [P, F]),
             "bgpu_read_joint_positions": (S, [P, F]),
@@ -578,6 +580,18 @@ class World:
         first = ctypes.c_uint32()
         check(self.L.bgpu_add_joints(self.h, 1, ctypes.byref(d), ctypes.byref(first)), "add_joints")
         return first.value
+
+    def set_ccd(self, first, motion_threshold, swept_sphere_radius):
+        """RigidBody::ccd for bodies first, first + 1, ... (arrays or scalars for one body)."""
+        thr = np.atleast_1d(f32(motion_threshold))
+        rad = np.atleast_1d(f32(swept_sphere_radius))
+        check(self.L.bgpu_set_ccd(self.h, first, len(thr), fptr(thr), fptr(rad)), "set_ccd")
+
+    def ccd_clamps(self):
+        out = np.ones(self.num_bodies, dtype=np.float32)
+        if len(out):
+            check(self.L.bgpu_read_ccd_clamps(self.h, fptr(out)), "read_ccd_clamps")
+        return out
 
     def add_spring2(self, joint):
         """Adds a Spring2 joint (Constraint::generic_6dof_spring2); returns its joint id."""

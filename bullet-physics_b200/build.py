@@ -14,7 +14,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libbgpu.so")
 BUILD = os.path.join(HERE, "_build")
 SOURCES = ["k_body.cu", "k_broadphase.cu", "k_islands.cu", "k_pairs.cu", "k_solver.cu", "k_adjoint.cu", "k_joints.cu",
-           "world.cu"]
+           "k_ccd.cu", "world.cu"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [

@@ -159,6 +159,13 @@ void launch_integrate_velocities(const BodyDev& b, const Shape* shapes, const fl
 void launch_initial_aabbs(const BodyDev& b, const Shape* shapes, const float4* hull, uint32_t first, uint32_t n,
                           cudaStream_t s);
 void launch_integrate_positions(const BodyDev& b, uint32_t n, float dt, float turn_erp, cudaStream_t s);
+// CCD swept-sphere clamp (step.rs:1068-1155): clamp[k] for the bodies ids[0..m) (par: motion
+// threshold, swept-sphere radius), scanning the bodies of each one's world (all n when world_of is
+// null); then, after the position integration, the clamp applied (step.rs:1210-1214).
+void launch_ccd_sweep(const BodyDev& b, const Shape* shapes, const float4* hull, const uint32_t* ids, const float2* par,
+                      uint32_t m, uint32_t n, const uint32_t* world_off, const uint32_t* world_of,
+                      const uint64_t* suppressed, uint32_t nsuppressed, float dt, float* clamp, cudaStream_t s);
+void launch_ccd_apply(const BodyDev& b, const uint32_t* ids, const float* clamp, uint32_t m, float dt, cudaStream_t s);
 // Host-facing layouts: n x 3 floats -> float4 lanes, and poses -> n x 7 floats.
 void launch_unpack3(uint32_t n, const float* src, float4* dst, cudaStream_t s);
 void launch_pack_poses(uint32_t n, const float4* pos, const float4* quat, float* out, cudaStream_t s);

@@ -1,0 +1,318 @@
+// CCD swept-sphere clamp (step.rs:1068-1155, :1210-1214; convex_sweep.rs:37-214, :263-295;
+// gjk.rs:864-1044). One block per body that has CCD settings: the block's threads stride over
+// the bodies of its world, keep those that pass the collision filters (no-contact-response
+// targets, joint-suppressed pairs, group/mask) and whose broad-phase proxy touches the swept box,
+// and cast a sphere against each; the block's smallest hit fraction is the clamp. A second
+// kernel, after the position integration, pulls each clamped body back along its step motion.
+// The reference scans every body for every CCD body as well; the cast itself (a ternary search
+// for the closest approach, then bisection, each probe a GJK point distance) matches its
+// arithmetic step for step.
+#include "bgpu_kernels.cuh"
+
+namespace bgpu {
+
+namespace {
+
+// A GJK simplex of up to four points, in the order the closest-feature tests keep them.
+struct Simplex {
+    V3 p[4];
+    int n;
+};
+
+__device__ __forceinline__ void keep1(Simplex& s, V3 a) { s.p[0] = a; s.n = 1; }
+__device__ __forceinline__ void keep2(Simplex& s, V3 a, V3 b) { s.p[0] = a; s.p[1] = b; s.n = 2; }
+__device__ __forceinline__ void keep3(Simplex& s, V3 a, V3 b, V3 c) { s.p[0] = a; s.p[1] = b; s.p[2] = c; s.n = 3; }
+
+// gjk.rs:889-906
+__device__ V3 closest_segment(V3 a, V3 b, Simplex& keep) {
+    const V3 ab = b - a;
+    if (len2(ab) == 0.0f) { keep1(keep, a); return a; }
+    const float t = -dot(a, ab) / len2(ab);
+    if (t <= 0.0f) { keep1(keep, a); return a; }
+    if (t >= 1.0f) { keep1(keep, b); return b; }
+    keep2(keep, b, a);
+    return a + ab * t;
+}
+
+// gjk.rs:911-989
+__device__ V3 closest_triangle(V3 a, V3 b, V3 c, Simplex& keep) {
+    const V3 ab = b - a, ac = c - a, ap = -a;
+    const float d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0.0f && d2 <= 0.0f) { keep1(keep, a); return a; }
+    const V3 bp = -b;
+    const float d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0.0f && d4 <= d3) { keep1(keep, b); return b; }
+    const float vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+        if (d1 == d3) { keep1(keep, a); return a; }
+        const float v = d1 / (d1 - d3);
+        keep2(keep, b, a);
+        return a + ab * v;
+    }
+    const V3 cp = -c;
+    const float d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0.0f && d5 <= d6) { keep1(keep, c); return c; }
+    const float vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+        if (d2 == d6) { keep1(keep, a); return a; }
+        const float w = d2 / (d2 - d6);
+        keep2(keep, c, a);
+        return a + ac * w;
+    }
+    const float va = d3 * d6 - d5 * d4;
+    if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+        if ((d4 - d3) + (d5 - d6) == 0.0f) { keep1(keep, b); return b; }
+        const float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        keep2(keep, c, b);
+        return b + (c - b) * w;
+    }
+    const float sum = va + vb + vc;
+    if (sum <= 0.0f || isnan(sum)) {
+        Simplex kab, kbc, kca;
+        const V3 qab = closest_segment(a, b, kab), qbc = closest_segment(b, c, kbc), qca = closest_segment(c, a, kca);
+        if (len2(qab) <= len2(qbc) && len2(qab) <= len2(qca)) { keep = kab; return qab; }
+        if (len2(qbc) <= len2(qca)) { keep = kbc; return qbc; }
+        keep = kca;
+        return qca;
+    }
+    const float denom = 1.0f / sum;
+    const float v = vb * denom, w = vc * denom;
+    keep3(keep, c, b, a);
+    return a + ab * v + ac * w;
+}
+
+// gjk.rs:994-1044
+__device__ V3 closest_tetrahedron(V3 a, V3 b, V3 c, V3 d, Simplex& keep) {
+    const V3 ao = -a, ab = b - a, ac = c - a, ad = d - a;
+    if (fabsf(dot(cross(ab, ac), ad)) < 1e-12f) {
+        // coplanar: the closest of the four faces, the first of equal ones
+        const V3 f[4][3] = {{a, b, c}, {a, b, d}, {a, c, d}, {b, c, d}};
+        V3 best = V3{0.0f, 0.0f, 0.0f};
+        Simplex best_keep;
+        best_keep.n = 0;
+        for (int k = 0; k < 4; ++k) {
+            Simplex kk;
+            const V3 q = closest_triangle(f[k][0], f[k][1], f[k][2], kk);
+            if (k == 0 || len2(q) < len2(best)) { best = q; best_keep = kk; }
+        }
+        keep = best_keep;
+        return best;
+    }
+    const V3 abc = cross(ab, ac), acd = cross(ac, ad), adb = cross(ad, ab);
+    const V3 bo = -b;
+    const V3 bcd = cross(c - b, d - b);
+    if (dot(abc, ao) * dot(abc, ad) < 0.0f) return closest_triangle(a, b, c, keep);
+    if (dot(acd, ao) * dot(acd, ab) < 0.0f) return closest_triangle(a, c, d, keep);
+    if (dot(adb, ao) * dot(adb, ac) < 0.0f) return closest_triangle(a, d, b, keep);
+    if (dot(bcd, bo) * dot(bcd, a - b) < 0.0f) return closest_triangle(b, c, d, keep);
+    keep.p[0] = a; keep.p[1] = b; keep.p[2] = c; keep.p[3] = d; keep.n = 4;
+    return V3{0.0f, 0.0f, 0.0f};
+}
+
+// gjk.rs:864-885
+__device__ V3 closest_origin(Simplex& s) {
+    Simplex keep;
+    V3 v;
+    switch (s.n) {
+        case 0: return V3{0.0f, 0.0f, 0.0f};
+        case 1: return s.p[0];
+        case 2: v = closest_segment(s.p[0], s.p[1], keep); break;
+        case 3: v = closest_triangle(s.p[0], s.p[1], s.p[2], keep); break;
+        default: v = closest_tetrahedron(s.p[0], s.p[1], s.p[2], s.p[3], keep); break;
+    }
+    s = keep;
+    return v;
+}
+
+// The target inflated by the swept sphere (convex_sweep.rs:107-125): its support point along d.
+struct Inflated {
+    Shape s;
+    V3 pos;
+    Q ori;
+    float radius;
+    const float4* hull;
+    __device__ __forceinline__ V3 support(V3 d) const {
+        const V3 sphere = len2(d) > 1e-12f ? d / len(d) * radius : V3{0.0f, 0.0f, 0.0f};
+        return support_world(s, pos, ori, d, hull) + sphere;
+    }
+};
+
+// convex_sweep.rs:72-103: squared distance from `point` to the inflated target and the unit
+// direction from the target toward the point (zero when inside or touching).
+__device__ float point_distance(const Inflated& t, V3 point, V3& dir) {
+    auto mink = [&](V3 v) { return point - t.support(-v); };
+    V3 v = point;
+    if (len2(v) < 1e-12f) v = V3{1.0f, 0.0f, 0.0f};
+    Simplex s;
+    s.p[0] = mink(v);
+    s.n = 1;
+    v = s.p[0];
+    for (int it = 0; it < 64; ++it) {
+        if (len2(v) < 1e-10f) { dir = V3{0.0f, 0.0f, 0.0f}; return 0.0f; }
+        const V3 w = mink(-v);
+        for (int k = 0; k < s.n; ++k)
+            if (len2(s.p[k] - w) < 1e-12f) { dir = v / len(v); return len2(v); }
+        if (s.n >= 4) break;  // unreachable: a kept tetrahedron means v == 0, which returned above
+        s.p[s.n++] = w;
+        v = closest_origin(s);
+    }
+    if (len2(v) < 1e-10f) { dir = V3{0.0f, 0.0f, 0.0f}; return 0.0f; }
+    dir = v / len(v);
+    return len2(v);
+}
+
+__device__ __forceinline__ float point_distance2(const Inflated& t, V3 p) {
+    V3 d;
+    return point_distance(t, p, d);
+}
+
+// convex_sweep.rs:155-214 (sweep_with_dist), the fraction only
+__device__ bool sweep_convex(V3 from, V3 dir, float length, const Inflated& t, float& fraction) {
+    float lo = 0.0f, hi = 1.0f;
+    for (int it = 0; it < 40; ++it) {
+        const float m1 = lo + (hi - lo) / 3.0f;
+        const float m2 = hi - (hi - lo) / 3.0f;
+        if (point_distance2(t, from + dir * (m1 * length)) < point_distance2(t, from + dir * (m2 * length))) hi = m2;
+        else lo = m1;
+    }
+    const float s_min = (lo + hi) * 0.5f;
+    if (point_distance2(t, from + dir * (s_min * length)) > 1e-8f) return false;
+    float low = 0.0f, high = s_min;
+    for (int it = 0; it < 60; ++it) {
+        const float mid = (low + high) * 0.5f;
+        if (point_distance2(t, from + dir * (mid * length)) <= 1e-8f) high = mid;
+        else low = mid;
+    }
+    fraction = (low + high) * 0.5f;
+    return true;
+}
+
+// convex_sweep.rs:263-295 (sweep_plane), the fraction only
+__device__ bool sweep_plane(V3 from, V3 dir, float length, float radius, const Shape& s, Q ori, float& fraction) {
+    const V3 n = rotate(ori, V3{s.p0, s.p1, s.p2});
+    const float dn0 = dot(n, from) - s.p3;
+    if (fabsf(dn0) <= radius) { fraction = 0.0f; return true; }
+    const float dd = dot(n, dir * length);
+    if (dd >= 0.0f) return false;
+    const float sign = dn0 > 0.0f ? 1.0f : -1.0f;
+    const float f = (sign * radius - dn0) / dd;
+    if (!(f >= 0.0f && f <= 1.0f)) return false;
+    fraction = f;
+    return true;
+}
+
+__device__ bool key_suppressed(const uint64_t* keys, uint32_t n, uint64_t k) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (keys[mid] < k) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < n && keys[lo] == k;
+}
+
+__device__ __forceinline__ bool body_active(uint32_t act) {
+    return act == ACT_ACTIVE || act == ACT_WANTS_DEACTIVATION || act == ACT_DISABLE_DEACTIVATION;
+}
+
+constexpr int CCD_THREADS = 128;
+
+// step.rs:1068-1155: the clamp fraction of CCD list entry blockIdx.x (1 when not clamped).
+__global__ void __launch_bounds__(CCD_THREADS) k_ccd_sweep(BodyDev b, const Shape* __restrict__ shapes,
+                                                           const float4* __restrict__ hull, const uint32_t* __restrict__ ids,
+                                                           const float2* __restrict__ par, uint32_t n,
+                                                           const uint32_t* __restrict__ world_off,
+                                                           const uint32_t* __restrict__ world_of,
+                                                           const uint64_t* __restrict__ suppressed, uint32_t nsuppressed,
+                                                           float dt, float* clamp) {
+    const uint32_t k = blockIdx.x;
+    const uint32_t i = ids[k];
+    const float threshold = par[k].x, radius = par[k].y;
+    const uint4 info = b.info[i];
+    const Shape& si = shapes[info.x];
+    const V3 from = from4(b.pos[i]);
+    const V3 to = from + from4(b.linvel[i]) * dt;
+    bool eligible = body_active(info.z) && !(info.y & (BF_STATIC | BF_KINEMATIC)) && threshold > 0.0f && radius > 0.0f &&
+                    si.type != SHAPE_PLANE;
+    eligible = eligible && !(len2(to - from) <= threshold * threshold);
+    if (!eligible) {
+        if (threadIdx.x == 0) clamp[k] = 1.0f;
+        return;
+    }
+    const V3 smin = vmin(from, to) - V3{radius, radius, radius}, smax = vmax(from, to) + V3{radius, radius, radius};
+    const V3 delta = to - from;
+    const float length = len(delta);
+    const V3 dir = delta / length;
+    const uint32_t gi = info.w & 0xFFFFu, mi = info.w >> 16;
+    uint32_t lo = 0, hi = n;
+    if (world_of) { lo = world_off[world_of[i]]; hi = world_off[world_of[i] + 1]; }
+    float best = 1.0f;
+    for (uint32_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+        if (j == i) continue;
+        const uint4 oj = b.info[j];
+        if (oj.y & BF_NO_RESPONSE) continue;
+        const uint32_t gj = oj.w & 0xFFFFu, mj = oj.w >> 16;
+        if ((gi & mj) == 0 || (gj & mi) == 0) continue;
+        const float4 amin = b.aabb_min[j], amax = b.aabb_max[j];
+        // Aabb::overlaps (util.rs:28-38), closed on every axis
+        if (!(amin.x <= smax.x && amin.y <= smax.y && amin.z <= smax.z && smin.x <= amax.x && smin.y <= amax.y &&
+              smin.z <= amax.z))
+            continue;
+        if (nsuppressed) {
+            const uint64_t key = (uint64_t(min(i, j)) << 32) | max(i, j);
+            if (key_suppressed(suppressed, nsuppressed, key)) continue;
+        }
+        // convex_sweep.rs:45-50: no cast for a vanishing motion
+        if (length <= 1.1920929e-7f) continue;
+        const Shape& sj = shapes[oj.x];
+        float f;
+        bool hit;
+        if (sj.type == SHAPE_PLANE) {
+            hit = sweep_plane(from, dir, length, radius, sj, q4(b.quat[j]), f);
+        } else {
+            Inflated t{sj, from4(b.pos[j]), q4(b.quat[j]), radius, hull};
+            hit = sweep_convex(from, dir, length, t, f);
+        }
+        if (hit && f < best) best = f;
+    }
+    // block minimum
+    for (int o = 16; o > 0; o >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, o));
+    __shared__ float wmin[CCD_THREADS / 32];
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float m = wmin[0];
+        for (int w = 1; w < CCD_THREADS / 32; ++w) m = fminf(m, wmin[w]);
+        clamp[k] = m;
+    }
+}
+
+// step.rs:1210-1214, after the position integration (which leaves the velocities unchanged).
+__global__ void k_ccd_apply(BodyDev b, const uint32_t* __restrict__ ids, const float* __restrict__ clamp, uint32_t m,
+                            float dt) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    const float c = clamp[k];
+    if (!(c < 1.0f)) return;
+    const uint32_t i = ids[k];
+    const V3 p = from4(b.pos[i]);
+    const V3 from = p - from4(b.linvel[i]) * dt;
+    b.pos[i] = to4(from + (p - from) * c, 0.0f);
+}
+
+}  // namespace
+
+void launch_ccd_sweep(const BodyDev& b, const Shape* shapes, const float4* hull, const uint32_t* ids, const float2* par,
+                      uint32_t m, uint32_t n, const uint32_t* world_off, const uint32_t* world_of,
+                      const uint64_t* suppressed, uint32_t nsuppressed, float dt, float* clamp, cudaStream_t s) {
+    if (m == 0) return;
+    k_ccd_sweep<<<m, CCD_THREADS, 0, s>>>(b, shapes, hull, ids, par, n, world_off, world_of, suppressed, nsuppressed,
+                                          dt, clamp);
+}
+
+void launch_ccd_apply(const BodyDev& b, const uint32_t* ids, const float* clamp, uint32_t m, float dt, cudaStream_t s) {
+    if (m == 0) return;
+    k_ccd_apply<<<(m + 127) / 128, 128, 0, s>>>(b, ids, clamp, m, dt);
+}
+
+}  // namespace bgpu

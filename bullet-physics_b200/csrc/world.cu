@@ -181,6 +181,14 @@ struct World {
     std::vector<uint32_t> joint_row_off_h;
     DevBuf<float4> joint_aux_d, joint_s2_state_d;
     DevBuf<uint32_t> joint_row_off_d;
+    // CCD (RigidBody::ccd): per-body motion threshold and swept-sphere radius; the bodies with both
+    // positive form the list the clamp kernels walk, with one clamp fraction per entry
+    std::vector<float> ccd_thr_h, ccd_rad_h;
+    std::vector<uint32_t> ccd_ids_h;
+    DevBuf<uint32_t> ccd_ids_d;
+    DevBuf<float2> ccd_par_d;
+    DevBuf<float> ccd_clamp_d;
+    uint32_t nccd = 0;
     DevBuf<uint64_t> suppressed_d;  // sorted keys of the pairs a joint keeps from colliding
     uint32_t nsuppressed = 0;
 
@@ -429,6 +437,39 @@ struct World {
         j.s2_state = joint_s2_state_d.p;
         j.global_cfm = info.global_cfm;
         return j;
+    }
+
+    // RigidBody::ccd for bodies [first, first + cnt): the list holds the bodies whose threshold
+    // and radius are both positive (the others are never swept, step.rs:1072-1079).
+    void set_ccd(uint32_t first, uint32_t cnt, const float* thr, const float* rad) {
+        if (uint64_t(first) + cnt > n) throw InvalidArg{"CCD body range out of bounds"};
+        ccd_thr_h.resize(n, 0.0f);
+        ccd_rad_h.resize(n, 0.0f);
+        for (uint32_t k = 0; k < cnt; ++k) {
+            if (std::isnan(thr[k]) || std::isnan(rad[k])) throw InvalidArg{"NaN CCD setting"};
+            ccd_thr_h[first + k] = thr[k];
+            ccd_rad_h[first + k] = rad[k];
+        }
+        ccd_ids_h.clear();
+        std::vector<float2> par;
+        for (uint32_t i = 0; i < uint32_t(ccd_thr_h.size()); ++i)
+            if (ccd_thr_h[i] > 0.0f && ccd_rad_h[i] > 0.0f) {
+                ccd_ids_h.push_back(i);
+                par.push_back(make_float2(ccd_thr_h[i], ccd_rad_h[i]));
+            }
+        nccd = uint32_t(ccd_ids_h.size());
+        if (!nccd) return;
+        ccd_ids_d.reserve(nccd);
+        ccd_par_d.reserve(nccd);
+        ccd_clamp_d.reserve(nccd);
+        check_cuda(cudaMemcpyAsync(ccd_ids_d.p, ccd_ids_h.data(), nccd * sizeof(uint32_t), cudaMemcpyHostToDevice, stream),
+                   "upload CCD ids");
+        check_cuda(cudaMemcpyAsync(ccd_par_d.p, par.data(), nccd * sizeof(float2), cudaMemcpyHostToDevice, stream),
+                   "upload CCD settings");
+        std::vector<float> ones(nccd, 1.0f);
+        check_cuda(cudaMemcpyAsync(ccd_clamp_d.p, ones.data(), nccd * sizeof(float), cudaMemcpyHostToDevice, stream),
+                   "reset CCD clamps");
+        check_cuda(cudaStreamSynchronize(stream), "sync");
     }
 
     // Row capacity of joint j: JOINT_MAX_ROWS, or for a spring-2 joint its exact row count
@@ -708,8 +749,12 @@ struct World {
         check_cuda(cudaMemcpyAsync(prev_simulate, simulate, nw * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream),
                    "flag");
         mark(7);
+        // 7a: CCD clamp fractions, from the solved velocities and the pre-integration poses
+        launch_ccd_sweep(b, shapes_d.p, hull_d.p, ccd_ids_d.p, ccd_par_d.p, nccd, n, batch ? world_off_d.p : nullptr,
+                         world_of, sp.suppressed, sp.nsuppressed, dt, ccd_clamp_d.p, stream);
         // 6c + 7 + 8: deactivation, pose integration with the split push, force clear.
         launch_integrate_positions(b, n, dt, info.split_impulse_turn_erp, stream);
+        launch_ccd_apply(b, ccd_ids_d.p, ccd_clamp_d.p, nccd, dt, stream);
         mark(8);
         if (timing) {
             ev_pending[ev_cur] = true;
@@ -1256,6 +1301,7 @@ bgpu_status bgpu_tape_create(bgpu_world* w, uint32_t checkpoint_every, bgpu_tape
     *out = nullptr;
     return guarded([&]() -> bgpu_status {
         if (!w->impl.joints_h.empty()) throw bgpu::InvalidArg{"the adjoint tape does not cover joints"};
+        if (w->impl.nccd) throw bgpu::InvalidArg{"the adjoint tape does not cover the CCD clamp"};
         std::unique_ptr<bgpu_tape> t(new bgpu_tape());
         t->impl.reset(new bgpu::Tape(&w->impl, checkpoint_every));
         *out = t.release();
@@ -1690,6 +1736,30 @@ bgpu_status bgpu_read_joint_spring2_state(bgpu_world* w, float* state) {
         bgpu::check_cuda(cudaMemcpyAsync(state, W.joint_s2_state_d.p, 2 * nj * sizeof(float4), cudaMemcpyDeviceToHost,
                                          W.stream), "d2h");
         bgpu::check_cuda(cudaStreamSynchronize(W.stream), "sync");
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_set_ccd(bgpu_world* w, uint32_t first, uint32_t n, const float* motion_threshold,
+                         const float* swept_sphere_radius) {
+    if (!w || (n && (!motion_threshold || !swept_sphere_radius))) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        w->impl.set_ccd(first, n, motion_threshold, swept_sphere_radius);
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_read_ccd_clamps(bgpu_world* w, float* clamps) {
+    if (!w || !clamps) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        for (uint32_t i = 0; i < W.n; ++i) clamps[i] = 1.0f;
+        if (!W.nccd) return BGPU_OK;
+        std::vector<float> c(W.nccd);
+        bgpu::check_cuda(cudaMemcpyAsync(c.data(), W.ccd_clamp_d.p, W.nccd * sizeof(float), cudaMemcpyDeviceToHost,
+                                         W.stream), "d2h");
+        bgpu::check_cuda(cudaStreamSynchronize(W.stream), "sync");
+        for (uint32_t k = 0; k < W.nccd; ++k) clamps[W.ccd_ids_h[k]] = c[k];
         return BGPU_OK;
     });
 }

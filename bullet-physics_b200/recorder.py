@@ -6,7 +6,8 @@ protocol"; tools/scenes.json): a JSON object {"scenes": {name: scene}} where a s
 "name", "shape" {"type": box | sphere | capsule | plane, ...}, "position", "mass" (0 =
 static), optional "friction", "restitution", "velocity", "angular_velocity",
 "linear_damping", "angular_damping", "additional_damping", "no_contact_response",
-"group", "mask" (-1 = all)), "record" (body names) and optional "substeps"
+"group", "mask" (-1 = all), "ccd" {"motion_threshold", "swept_sphere_radius"}), "record" (body
+names) and optional "substeps"
 {"max_sub_steps", "fixed_dt"}.
 
 Output format (docs/parity-harness.md, "Output format"; tools/bullet_record.cpp:352-383):
@@ -14,7 +15,7 @@ one file <scene>_<body>_<suffix>.csv per recorded body, one line per frame
 "t px py pz qx qy qz qw" with %.6f, t = frame * dt in f32.
 
 Shape types the GPU step has no narrow phase for (cylinder, cone, mesh, mesh_parts),
-per-body gravity vectors, CCD settings and ray probes are rejected with ValueError.
+per-body gravity vectors and ray probes are rejected with ValueError.
 """
 import json
 import os
@@ -63,8 +64,8 @@ def build_world(scene, lib=bgpu):
     shape_ids = {}
     index = {}
     for body in scene["bodies"]:
-        if "gravity" in body or "ccd" in body:
-            raise ValueError(f"body '{body['name']}': per-body gravity and CCD are not supported by the GPU step")
+        if "gravity" in body:
+            raise ValueError(f"body '{body['name']}': per-body gravity is not supported by the GPU step")
         kind, params = shape_params(body["shape"])
         key = (kind, tuple(params))
         if key not in shape_ids:
@@ -83,6 +84,9 @@ def build_world(scene, lib=bgpu):
             friction=float(body.get("friction", 0.5)), restitution=float(body.get("restitution", 0.0)), flags=flags,
             group=0xFFFF if group == -1 else group, mask=0xFFFF if mask == -1 else mask,
             lin_damping=float(body.get("linear_damping", 0.0)), ang_damping=float(body.get("angular_damping", 0.0)))
+        if "ccd" in body:
+            w.set_ccd(index[body["name"]], float(body["ccd"]["motion_threshold"]),
+                      float(body["ccd"]["swept_sphere_radius"]))
     return w, index
 
 

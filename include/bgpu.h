@@ -320,6 +320,16 @@ bgpu_status bgpu_read_solve_order(bgpu_world* w, uint64_t* keys, uint64_t cap, u
 /* Joints (PhysicsWorld::add_constraint, world.rs): ids are consecutive from *first_id.
  * Rejects unknown kinds, out-of-range or equal bodies. */
 bgpu_status bgpu_add_joints(bgpu_world* w, uint32_t n, const bgpu_joint_desc* d, uint32_t* first_id);
+/* Continuous collision detection (RigidBody::ccd, body.rs:680-692) for bodies [first, first + n):
+ * a dynamic, active body whose step motion |v dt| exceeds its motion threshold is swept as a
+ * sphere of its swept-sphere radius against the other bodies of its world (those with contact
+ * response, not joint-suppressed, passing group/mask, whose broad-phase box touches the swept
+ * box) and its position is pulled back to the first hit after the integration
+ * (step.rs:1068-1155, :1210-1214). A threshold or radius of 0 turns it off for that body. */
+bgpu_status bgpu_set_ccd(bgpu_world* w, uint32_t first, uint32_t n, const float* motion_threshold,
+                         const float* swept_sphere_radius);
+/* Per body: the CCD clamp fraction of the last step (1 where no clamp happened). */
+bgpu_status bgpu_read_ccd_clamps(bgpu_world* w, float* clamps);
 /* Spring-2 joints (Constraint::generic_6dof_spring2), in the same id space as bgpu_add_joints. */
 bgpu_status bgpu_add_spring2_joints(bgpu_world* w, uint32_t n, const bgpu_spring2_desc* d, uint32_t* first_id);
 uint32_t bgpu_num_joints(bgpu_world* w);

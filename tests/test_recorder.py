@@ -38,6 +38,8 @@ def oracle_record(scene, out_path_of):
                                       angvel=b.get("angular_velocity", (0, 0, 0)), mass=b["mass"],
                                       friction=b.get("friction", 0.5), restitution=b.get("restitution", 0.0),
                                       lin_damping=b.get("linear_damping", 0.0))
+        if "ccd" in b:
+            o.set_ccd(index[b["name"]], b["ccd"]["motion_threshold"], b["ccd"]["swept_sphere_radius"])
     dt = recorder.scene_dt(scene)
     out = {n: [] for n in scene["record"]}
     for frame in range(1, scene["frames"] + 1):
@@ -49,7 +51,7 @@ def oracle_record(scene, out_path_of):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["dropped_cube", "capsule_and_ball"])
+@pytest.mark.parametrize("name", ["dropped_cube", "capsule_and_ball", "ccd_wall"])
 def test_recorded_trajectories_match_the_oracle(gpu, tmp_path, name):
     import recorder
 
