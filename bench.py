@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--batch-worlds", type=int, default=4096, help="batched-worlds leg: number of worlds (0: skip)")
     p.add_argument("--batch-steps", type=int, default=30)
     p.add_argument("--adjoint-worlds", type=int, default=1024, help="adjoint leg: number of worlds (0: skip)")
+    p.add_argument("--spring2-counts", default="150,15000",
+                   help="joint leg: chain counts of the spring2_chains scene, comma separated (empty: skip)")
     return p.parse_args()
 
 
@@ -268,6 +270,29 @@ def bench_adjoint(bgpu, scenes, n_worlds, steps=120, every=20):
             "grad_norms": {k: float(np.linalg.norm(v)) for k, v in g.items()}}
 
 
+def bench_spring2(bgpu, scenes, count, frames=300, warmup=5):
+    """Joint leg: the spring2_chains perf scene (spring-2 joint rows in the PGS) at `count`
+    chains of 3 boxes (150 is the reference's scene: 600 bodies, 450 joints), `frames` steps at
+    dt 1/60 after `warmup`, device time. The reference publishes its own CPU times for the
+    150-chain scene (docs/perf/speed.md, spring2_chains); they are quoted beside ours."""
+    w = scenes.spring2_chains_world(bgpu, count=count)
+    dt = 1.0 / 60.0
+    w.step_timed(dt, warmup)
+    ms = w.step_timed(dt, frames)
+    rows = int(w.joint_rows().shape[0])
+    n = int(w.num_bodies)
+    status = int(w.stats()["device_status"])
+    w.close()
+    out = {"workload": f"spring2_chains_{count}: {n} bodies, {3 * count} spring-2 joints, {rows} joint rows per "
+                       f"step, 10 iterations, dt 1/60, {frames} steps",
+           "value": n * frames / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms / frames,
+           "joint_rows_per_step": rows, "device_status": status}
+    if count == 150:
+        out["reference_published_ms_per_frame"] = {"rust": 0.709, "bullet": 1.318,
+                                                   "source": "docs/perf/speed.md spring2_chains, f32, their CPU"}
+    return out
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -390,6 +415,8 @@ def main():
             line["batched_worlds"] = bench_batched(bgpu, scenes, args.batch_worlds, args.batch_steps, args.warmup)
         if args.adjoint_worlds > 0:
             line["adjoint"] = bench_adjoint(bgpu, scenes, args.adjoint_worlds)
+        if args.spring2_counts:
+            line["spring2_chains"] = [bench_spring2(bgpu, scenes, int(c)) for c in args.spring2_counts.split(",")]
         if world_size == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(grid_of(args.cpu_sample_grid), min(args.preroll, 240), 30)
         print(json.dumps(line), flush=True)

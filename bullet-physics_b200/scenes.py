@@ -33,6 +33,9 @@ import numpy as np
 SPHERE, BOX, CAPSULE, HULL, PLANE = 0, 1, 2, 3, 4
 
 
+ACT_DISABLE_DEACTIVATION = 4  # ActivationState::DisableDeactivation (body.rs:140-153)
+
+
 class Scene:
     def __init__(self, name, dt, iterations, steps):
         self.name = name
@@ -409,3 +412,45 @@ def com_loss(positions, masses, offsets, targets):
         loss += float(d @ d)
         g[lo:hi] = 2.0 * d[None, :] * (mk / M)[:, None]
     return loss, g
+
+
+def spring2_chains_world(bgpu, count=150, cols=15, links=3, spacing=4.0, base_height=4.0, pitch=0.55, half=0.2,
+                         mass=1.0, stiffness=5.0, damping=0.3, iterations=10):
+    """The spring2_chains perf scene (tools/perf_scenes.json "spring2_chains",
+    examples/perf_scenes.rs add_spring2): `count` static anchor boxes in a grid of `cols` columns,
+    each with a horizontal chain of `links` 1 kg boxes joined by spring-2 joints whose three angular
+    springs are on (linear axes locked), never sleeping. The reference's scene is count=150 (600
+    bodies, 450 joints); larger counts extend the grid. Returns the GPU world."""
+    w = bgpu.World(gravity=(0.0, -9.81, 0.0), num_iterations=iterations)
+    box = w.add_shape(bgpu.BOX, [half, half, half])
+    rows = -(-count // cols)
+    k = np.arange(count)
+    x = (k % cols - (cols - 1) / 2.0) * spacing
+    z = (k // cols - (rows - 1) / 2.0) * spacing
+    per = links + 1
+    n = count * per
+    pos = np.zeros((n, 3), dtype=np.float32)
+    pos[:, 0] = np.repeat(x, per) + np.tile(np.arange(per), count) * pitch
+    pos[:, 1] = base_height
+    pos[:, 2] = np.repeat(z, per)
+    quat = np.tile(np.array([0.0, 0.0, 0.0, 1.0], dtype=np.float32), (n, 1))
+    m = np.tile(np.array([0.0] + [mass] * links, dtype=np.float32), count)
+    d = bgpu.desc_array(np.full(n, box), pos, quat, mass=m)
+    d["activation"] = np.where(m > 0, ACT_DISABLE_DEACTIVATION, 0).astype(np.uint32)
+    first = bgpu.ctypes.c_uint32()
+    bgpu.check(w.L.bgpu_add_bodies(w.h, n, d.ctypes.data_as(bgpu.ctypes.POINTER(bgpu.BodyDesc)),
+                                   bgpu.ctypes.byref(first)), "add_bodies")
+    frame = lambda ox: [ox, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0]
+    descs = (bgpu.Spring2Desc * (count * links))()
+    t = 0
+    for c in range(count):
+        for i in range(1, links + 1):
+            j = bgpu.Spring2(c * per + i - 1, c * per + i, frame(pitch / 2.0), frame(-pitch / 2.0))
+            for ax in range(3, 6):
+                j.enable_spring(ax)
+                j.set_stiffness(ax, stiffness, True)
+                j.set_damping(ax, damping, True)
+            descs[t] = j.desc
+            t += 1
+    bgpu.check(w.L.bgpu_add_spring2_joints(w.h, t, descs, bgpu.ctypes.byref(first)), "add_spring2_joints")
+    return w
