@@ -16,7 +16,7 @@ SPHERE, BOX, CAPSULE, HULL, PLANE = 0, 1, 2, 3, 4
 JOINT_POINT2POINT, JOINT_FIXED, JOINT_HINGE, JOINT_GEAR, JOINT_SLIDER = 0, 1, 2, 3, 4
 JOINT_DISABLE_COLLISIONS, JOINT_DISABLED, JOINT_ANGULAR_ONLY, JOINT_LIMIT, JOINT_MOTOR, JOINT_ERP = 1, 2, 4, 8, 16, 32
 JOINT_LIN_MOTOR, JOINT_ANG_MOTOR, JOINT_FRAME_B = 64, 128, 256
-JOINT_SPRING2 = 5
+JOINT_SPRING2, JOINT_CONETWIST, JOINT_CONE_MOTOR = 5, 6, 512
 ROTATE_XYZ, ROTATE_XZY, ROTATE_YXZ, ROTATE_YZX, ROTATE_ZXY, ROTATE_ZYX = range(6)
 (S2_MOTOR, S2_SERVO, S2_SPRING, S2_STIFFNESS_LIMITED, S2_DAMPING_LIMITED, S2_STOP_ERP, S2_STOP_CFM, S2_MOTOR_ERP,
  S2_MOTOR_CFM) = (1, 2, 4, 8, 16, 32, 64, 128, 256)
@@ -46,7 +46,11 @@ class JointDesc(ctypes.Structure):
                 ("damping_lim_lin", ctypes.c_float), ("damping_lim_ang", ctypes.c_float),
                 ("softness_ortho_lin", ctypes.c_float), ("softness_ortho_ang", ctypes.c_float),
                 ("lin_motor_target_velocity", ctypes.c_float), ("lin_motor_max_force", ctypes.c_float),
-                ("ang_motor_target_velocity", ctypes.c_float), ("ang_motor_max_force", ctypes.c_float)]
+                ("ang_motor_target_velocity", ctypes.c_float), ("ang_motor_max_force", ctypes.c_float),
+                ("swing_span1", ctypes.c_float), ("swing_span2", ctypes.c_float), ("twist_span", ctypes.c_float),
+                ("cone_softness", ctypes.c_float), ("cone_bias_factor", ctypes.c_float),
+                ("cone_relaxation", ctypes.c_float), ("cone_motor_target", ctypes.c_float * 4),
+                ("cone_motor_max_impulse", ctypes.c_float)]
 
 
 class Spring2Axis(ctypes.Structure):
@@ -559,7 +563,8 @@ class World:
     def add_joint(self, kind, body_a, body_b, frame_a, frame_b, flags=JOINT_DISABLE_COLLISIONS, erp=0.0,
                   impulse_clamp=0.0, limit=(1.0, -1.0), softness=0.9, bias_factor=0.3, relaxation=1.0,
                   motor=(0.0, 0.0), gear_ratio=1.0, lin_limits=(1.0, -1.0), ang_limits=(0.0, 0.0),
-                  slider_softness=(1.0, 1.0, 1.0, 1.0, 1.0, 1.0), lin_motor=(0.0, 0.0), ang_motor=(0.0, 0.0)):
+                  slider_softness=(1.0, 1.0, 1.0, 1.0, 1.0, 1.0), lin_motor=(0.0, 0.0), ang_motor=(0.0, 0.0),
+                  cone=None, cone_motor=None):
         """frame_*: 12 numbers (pivot xyz, basis columns x, y, z) in the body's frame."""
         d = JointDesc()
         self.L.bgpu_joint_desc_default(ctypes.byref(d))
@@ -577,6 +582,12 @@ class World:
          d.softness_ortho_ang) = slider_softness
         d.lin_motor_target_velocity, d.lin_motor_max_force = lin_motor
         d.ang_motor_target_velocity, d.ang_motor_max_force = ang_motor
+        if cone is not None:  # swing span 1, swing span 2, twist span, softness, bias factor, relaxation
+            (d.swing_span1, d.swing_span2, d.twist_span, d.cone_softness, d.cone_bias_factor,
+             d.cone_relaxation) = cone
+        if cone_motor is not None:  # (target quaternion in constraint space, max impulse)
+            d.cone_motor_target[:] = [float(x) for x in cone_motor[0]]
+            d.cone_motor_max_impulse = cone_motor[1]
         first = ctypes.c_uint32()
         check(self.L.bgpu_add_joints(self.h, 1, ctypes.byref(d), ctypes.byref(first)), "add_joints")
         return first.value

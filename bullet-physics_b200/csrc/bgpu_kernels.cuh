@@ -203,6 +203,8 @@ struct Broadphase {
 // [10] softness, bias factor, relaxation, motor target velocity; [11] motor max impulse, gear ratio;
 // slider: [12] linear limits low/high, angular limits low/high; [13] softness lim lin/ang, damping
 // lim lin/ang; [14] softness ortho lin/ang, linear motor target/max force; [15] angular motor;
+// cone twist: [12] swing spans 1 and 2, twist span, softness; [13] bias, relaxation, motor max
+// impulse; [14] motor target quaternion;
 // spring 2: [9].x first float4 of the joint's axis table in JointsDev::aux, [9].y rotate order.
 constexpr uint32_t JOINT_F4 = 16;
 // Row capacity of a joint of every kind but spring 2, whose capacity follows its axis settings.
@@ -217,9 +219,10 @@ enum : uint32_t { S2_MOTOR = 1u, S2_SERVO = 2u, S2_SPRING = 4u, S2_STIFFNESS_LIM
 // Joint row, JROW_F4 float4: [0] lin_a | effective mass, [1] ang_a | bias, [2] lin_b | cfm,
 // [3] ang_b | limit kind (bits), [4] lower, upper, accumulated impulse, 0.
 constexpr uint32_t JROW_F4 = 5;
-enum : uint32_t { JK_POINT2POINT = 0, JK_FIXED = 1, JK_HINGE = 2, JK_GEAR = 3, JK_SLIDER = 4, JK_SPRING2 = 5 };
+enum : uint32_t { JK_POINT2POINT = 0, JK_FIXED = 1, JK_HINGE = 2, JK_GEAR = 3, JK_SLIDER = 4, JK_SPRING2 = 5, JK_CONETWIST = 6 };
 enum : uint32_t { JF_DISABLE_COLLISIONS = 1u, JF_DISABLED = 2u, JF_ANGULAR_ONLY = 4u, JF_LIMIT = 8u, JF_MOTOR = 16u, JF_ERP = 32u,
-                  JF_LIN_MOTOR = 64u, JF_ANG_MOTOR = 128u, JF_FRAME_B = 256u };
+                  JF_LIN_MOTOR = 64u, JF_ANG_MOTOR = 128u, JF_FRAME_B = 256u,
+                  JF_CONE_MOTOR = 512u };
 enum : uint32_t { JL_UNBOUNDED = 0, JL_BILATERAL = 1, JL_LOWER = 2, JL_UPPER = 3, JL_WINDOW = 4 };
 
 struct JointsDev {

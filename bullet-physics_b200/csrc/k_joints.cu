@@ -112,6 +112,196 @@ __device__ __forceinline__ V3 axis_vec(int axis) {
     return V3{axis == 0 ? 1.0f : 0.0f, axis == 1 ? 1.0f : 0.0f, axis == 2 ? 1.0f : 0.0f};
 }
 
+__device__ __forceinline__ Q qnormalize(Q q) {
+    const float l = sqrtf(qlen2(q));
+    return Q{q.x / l, q.y / l, q.z / l, q.w / l};
+}
+
+// glam 0.33.3 Quat::from_mat3 (the published branch on the diagonal; mRC is column R, row C)
+__device__ Q quat_from_mat3(const M3& m) {
+    const float m00 = m.c0.x, m01 = m.c0.y, m02 = m.c0.z, m10 = m.c1.x, m11 = m.c1.y, m12 = m.c1.z;
+    const float m20 = m.c2.x, m21 = m.c2.y, m22 = m.c2.z;
+    if (m22 <= 0.0f) {
+        const float dif10 = m11 - m00, omm22 = 1.0f - m22;
+        if (dif10 <= 0.0f) {
+            const float f = omm22 - dif10, inv = 0.5f / sqrtf(f);
+            return Q{f * inv, (m01 + m10) * inv, (m02 + m20) * inv, (m12 - m21) * inv};
+        }
+        const float f = omm22 + dif10, inv = 0.5f / sqrtf(f);
+        return Q{(m01 + m10) * inv, f * inv, (m12 + m21) * inv, (m20 - m02) * inv};
+    }
+    const float sum10 = m11 + m00, opm22 = 1.0f + m22;
+    if (sum10 <= 0.0f) {
+        const float f = opm22 - sum10, inv = 0.5f / sqrtf(f);
+        return Q{(m02 + m20) * inv, (m12 + m21) * inv, f * inv, (m01 - m10) * inv};
+    }
+    const float f = opm22 + sum10, inv = 0.5f / sqrtf(f);
+    return Q{(m12 - m21) * inv, (m20 - m02) * inv, (m01 - m10) * inv, f * inv};
+}
+
+// glam Quat::from_rotation_arc (published algorithm), as the host frames use it
+__device__ Q rotation_arc(V3 from, V3 to) {
+    const float eps = 1.1920929e-7f;
+    const float one_minus_eps = 1.0f - 2.0f * eps;
+    const float d = dot(from, to);
+    if (d > one_minus_eps) return Q{0.0f, 0.0f, 0.0f, 1.0f};
+    if (d < -one_minus_eps) {
+        const float sign = signbit(from.z) ? -1.0f : 1.0f;
+        const float aa = -1.0f / (sign + from.z);
+        const float bb = from.x * from.y * aa;
+        const V3 o = V3{bb, sign + from.y * from.y * aa, -from.y};
+        const float half = PI_F * 0.5f;
+        const float sn = sinf(half);
+        return Q{o.x * sn, o.y * sn, o.z * sn, cosf(half)};
+    }
+    const V3 c = cross(from, to);
+    return qnormalize(Q{c.x, c.y, c.z, 1.0f + d});
+}
+
+// conetwist.rs:546-548
+__device__ __forceinline__ float quaternion_angle(Q q) { return 2.0f * acosf(fminf(fmaxf(q.w, -1.0f), 1.0f)); }
+
+// conetwist.rs:222-342 (prepare_rows) with calc_angle_info (:344-479), compute_cone_limit_info
+// (:481-502), compute_twist_limit_info (:504-519) and the ellipse-normal swing axis (:521-539).
+__device__ __noinline__ void conetwist_rows(RowOut& out, const BodyDev& b, const JointsDev& jd, uint32_t jid,
+                                            const float4* d, uint32_t flags, Q qa, Q qb, V3 r_a, V3 r_b, V3 pivot_a,
+                                            V3 pivot_b, float inv_dt, float erp) {
+    const float eps = 1.1920929e-7f, fix = 0.05f;
+    const V3 zero = V3{0.0f, 0.0f, 0.0f}, X = V3{1.0f, 0.0f, 0.0f};
+    const float4 p12 = d[12], p13 = d[13], p14 = d[14];
+    const float s1 = p12.x, s2 = p12.y, twist_span = p12.z, softness = p12.w;
+    const float bias = p13.x, relax = p13.y, max_impulse = p13.z;
+    const bool has_motor = (flags & JF_CONE_MOTOR) != 0;
+    const M3 tr_a = mul(from_quat(qa), M3{from4(d[2]), from4(d[3]), from4(d[4])});
+    const M3 tr_b = mul(from_quat(qb), M3{from4(d[6]), from4(d[7]), from4(d[8])});
+    const float k = inv_dt * erp;
+    const V3 dp = pivot_a - pivot_b;
+    for (int axis = 0; axis < 3; ++axis) {
+        const V3 nrm = axis_vec(axis);
+        out.push(nrm, cross(r_a, nrm), nrm, cross(r_b, nrm), k * comp(dp, axis), JL_UNBOUNDED, 0.0f, 0.0f);
+    }
+    float swing_corr = 0.0f, twist_corr = 0.0f;
+    V3 swing_axis = zero, twist_axis = zero;
+    bool solve_swing = false, solve_twist = false;
+    if (has_motor) {
+        const M3 r_delta = mul(mul(tr_b, from_quat(Q{p14.x, p14.y, p14.z, p14.w})), transpose(tr_a));
+        const Q q_delta = qnormalize(quat_from_mat3(r_delta));
+        const V3 sa = V3{q_delta.x, q_delta.y, q_delta.z};
+        const float l2 = len2(sa);
+        if (l2 > eps) {
+            swing_axis = sa / sqrtf(l2);
+            swing_corr = quaternion_angle(q_delta);
+            if (fabsf(swing_corr) > eps) solve_swing = true;
+        }
+    } else {
+        const Q q_a = quat_from_mat3(tr_a), q_b = quat_from_mat3(tr_b);
+        const Q q_ab = qnormalize(qmul(qinv(q_b), q_a));
+        const V3 v_cone = normalize(rotate(q_ab, X));
+        const Q q_cone = qnormalize(rotation_arc(X, v_cone));
+        const Q q_twist = qnormalize(qmul(qinv(q_cone), q_ab));
+        if (s1 >= fix && s2 >= fix) {
+            const float angle = quaternion_angle(q_cone);
+            V3 axis = zero;
+            float limit = s1;
+            if (angle > eps) {
+                axis = normalize(V3{q_cone.x, q_cone.y, q_cone.z});
+                const float xe = axis.y, ye = -axis.z;
+                if (fabsf(xe) > eps) {
+                    const float slope2 = (ye * ye) / (xe * xe);
+                    float norm = 1.0f / (s2 * s2);
+                    norm += slope2 / (s1 * s1);
+                    limit = sqrtf((1.0f + slope2) / norm);
+                }
+            }
+            if (angle > limit * softness) {
+                solve_swing = true;
+                swing_corr = angle - limit * softness;
+                float y = -axis.z;
+                const float z = axis.y;
+                if (fabsf(z) > eps) {
+                    float grad = y / z;
+                    grad *= s2 / s1;
+                    y = y > 0.0f ? fabsf(grad * z) : -fabsf(grad * z);
+                    axis.z = -y;
+                    axis.y = z;
+                    axis = normalize(axis);
+                }
+                swing_axis = rotate(q_b, -axis);
+            }
+        } else {
+            const V3 iv_a = tr_a.c0, jv_a = tr_a.c1, kv_a = tr_a.c2, iv_b = tr_b.c0;
+            float x = dot(iv_b, iv_a), y = dot(iv_b, jv_a), z = dot(iv_b, kv_a);
+            if (s1 < fix && s2 < fix) {
+                if (fabsf(y) > eps || fabsf(z) > eps) {
+                    solve_swing = true;
+                    swing_axis = -cross(iv_b, iv_a);
+                }
+            } else {
+                if (s1 < fix) {
+                    if (fabsf(x) > eps || fabsf(z) > eps) {
+                        solve_swing = true;
+                        if (s2 >= fix) {
+                            y = 0.0f;
+                            const float span2 = atan2f(z, x);
+                            if (span2 > s2) { x = cosf(s2); z = sinf(s2); }
+                            else if (span2 < -s2) { x = cosf(s2); z = -sinf(s2); }
+                        }
+                    }
+                } else {
+                    if (fabsf(x) > eps || fabsf(y) > eps) {
+                        solve_swing = true;
+                        if (s1 >= fix) {
+                            z = 0.0f;
+                            const float span1 = atan2f(y, x);
+                            if (span1 > s1) { x = cosf(s1); y = sinf(s1); }
+                            else if (span1 < -s1) { x = cosf(s1); y = -sinf(s1); }
+                        }
+                    }
+                }
+                const V3 target = normalize(iv_a * x + jv_a * y + kv_a * z);
+                swing_axis = -cross(iv_b, target);
+                swing_corr = len(swing_axis);
+                if (fabsf(swing_corr) > eps) swing_axis = normalize(swing_axis);
+            }
+        }
+        float twist_angle = 0.0f;
+        if (twist_span >= 0.0f) {
+            Q qm = q_twist;
+            twist_angle = quaternion_angle(q_twist);
+            if (twist_angle > PI_F) {
+                qm = Q{-q_twist.x, -q_twist.y, -q_twist.z, -q_twist.w};
+                twist_angle = quaternion_angle(qm);
+            }
+            V3 axis = V3{qm.x, qm.y, qm.z};
+            if (twist_angle > eps) axis = normalize(axis);
+            if (twist_angle > twist_span * softness) {
+                solve_twist = true;
+                twist_corr = twist_angle - twist_span * softness;
+                twist_axis = rotate(q_b, -axis);
+            }
+        }
+        jd.angle[jid] = twist_angle;
+    }
+    if (solve_swing) {
+        if (s1 < fix && s2 < fix) {
+            const float fact = inv_dt * relax;
+            out.push(zero, tr_a.c1, zero, tr_a.c1, -fact * dot(swing_axis, tr_a.c1), JL_UNBOUNDED, 0.0f, 0.0f);
+            out.push(zero, tr_a.c2, zero, tr_a.c2, -fact * dot(swing_axis, tr_a.c2), JL_UNBOUNDED, 0.0f, 0.0f);
+        } else {
+            const V3 ax1 = swing_axis * (relax * relax);
+            if (has_motor && max_impulse >= 0.0f)
+                out.push(zero, ax1, zero, ax1, -inv_dt * bias * swing_corr, JL_WINDOW, -max_impulse, 0.0f);
+            else
+                out.push(zero, ax1, zero, ax1, -inv_dt * bias * swing_corr, JL_UPPER, 0.0f, 0.0f);
+        }
+    }
+    if (solve_twist) {
+        const V3 ax1 = twist_axis * (relax * relax);
+        const uint32_t lim = twist_span > 0.0f ? (twist_corr > 0.0f ? JL_UPPER : JL_LOWER) : JL_UNBOUNDED;
+        out.push(zero, ax1, zero, ax1, -inv_dt * bias * twist_corr, lim, 0.0f, 0.0f);
+    }
+}
+
 // generic6dof_spring2.rs:1236-1241 (btGetMatrixElem): row index % 3 of column index / 3.
 __device__ __forceinline__ float mat_elem(const M3& m, int index) {
     const V3& c = index < 3 ? m.c0 : (index < 6 ? m.c1 : m.c2);
@@ -589,6 +779,8 @@ __global__ void k_joint_rows(BodyDev b, JointsDev jd, float inv_dt, float erp) {
         }
     } else if (kind == JK_SPRING2) {
         spring2_rows(out, b, jd, jid, d, ia, ib, pa, pb, qa, qb, pivot_a, pivot_b, inv_dt, erp);
+    } else if (kind == JK_CONETWIST) {
+        conetwist_rows(out, b, jd, jid, d, flags, qa, qb, r_a, r_b, pivot_a, pivot_b, inv_dt, erp);
     } else if (kind == JK_GEAR) {  // gear.rs:33-57: the spins about the frames' z columns, coupled
         const V3 axis_a_world = rotate(qa, from4(d[4])), axis_b_world = rotate(qb, from4(d[8]));
         out.push(zero, axis_a_world, zero, -(axis_b_world * p11.y), 0.0f, JL_UNBOUNDED, 0.0f, 0.0f);

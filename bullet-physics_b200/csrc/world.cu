@@ -510,7 +510,8 @@ struct World {
     // kinematic bodies take no impulse), so a joint colour never holds a dynamic body twice.
     uint32_t add_joints(uint32_t cnt, const bgpu_joint_desc* d, const bgpu_spring2_desc* s2 = nullptr) {
         for (uint32_t k = 0; k < cnt; ++k) {
-            if (s2 ? d[k].kind != BGPU_JOINT_SPRING2 : d[k].kind > BGPU_JOINT_SLIDER)
+            if (s2 ? d[k].kind != BGPU_JOINT_SPRING2
+                   : (d[k].kind > BGPU_JOINT_CONETWIST || d[k].kind == BGPU_JOINT_SPRING2))
                 throw InvalidArg{"unknown joint kind (spring-2 joints go through bgpu_add_spring2_joints)"};
             if (d[k].body_a >= n || d[k].body_b >= n || d[k].body_a == d[k].body_b)
                 throw InvalidArg{"joint bodies out of range or equal"};
@@ -574,6 +575,12 @@ struct World {
             o[14] = make_float4(x.softness_ortho_lin, x.softness_ortho_ang, x.lin_motor_target_velocity,
                                 x.lin_motor_max_force);
             o[15] = make_float4(x.ang_motor_target_velocity, x.ang_motor_max_force, 0.0f, 0.0f);
+            if (x.kind == BGPU_JOINT_CONETWIST) {  // kind-specific slots [12..14]
+                o[12] = make_float4(x.swing_span1, x.swing_span2, x.twist_span, x.cone_softness);
+                o[13] = make_float4(x.cone_bias_factor, x.cone_relaxation, x.cone_motor_max_impulse, 0.0f);
+                o[14] = make_float4(x.cone_motor_target[0], x.cone_motor_target[1], x.cone_motor_target[2],
+                                    x.cone_motor_target[3]);
+            }
             if (joint_s2_h[j] >= 0) {
                 const uint32_t aux0 = uint32_t(joint_s2_h[j]) * 6u * S2_AXIS_F4;
                 o[9] = make_float4(__uint_as_float_host(aux0), __uint_as_float_host(s2_h[size_t(joint_s2_h[j])].rotate_order),
@@ -1162,6 +1169,12 @@ void bgpu_joint_desc_default(bgpu_joint_desc* o) {
     o->limit_bias_factor = 0.3f;
     o->limit_relaxation = 1.0f;
     o->gear_ratio = 1.0f;
+    o->swing_span1 = o->swing_span2 = o->twist_span = 1e30f;
+    o->cone_softness = 1.0f;
+    o->cone_bias_factor = 0.3f;
+    o->cone_relaxation = 1.0f;
+    o->cone_motor_target[3] = 1.0f;
+    o->cone_motor_max_impulse = -1.0f;
     o->lin_limit_low = 1.0f;
     o->lin_limit_high = -1.0f;
     o->ang_limit_low = 0.0f;

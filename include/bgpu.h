@@ -130,7 +130,7 @@ typedef struct bgpu_step_stats {
     uint32_t num_split_contacts; /* solver rows with an active split-impulse term */
 } bgpu_step_stats;
 
-/* Joints (constraint.rs:67-132: the point-to-point, fixed, hinge, gear and slider kinds). A frame is
+/* Joints (constraint.rs:67-132: the point-to-point, fixed, hinge, gear, slider and cone-twist kinds). A frame is
  * the pivot followed by the basis columns x, y, z, in the body's centre-of-mass frame
  * (JointFrame, constraint.rs:658-682; the hinge axis is column z). Point-to-point joints
  * use only the frame origins (the pivots); gear joints (gear.rs) couple the spins about the
@@ -139,7 +139,8 @@ typedef struct bgpu_step_stats {
  * poses and solved after the contacts in each PGS sweep (sequential_impulse.rs:720-735);
  * a joint of a sleeping island (both bodies inactive) produces no rows. */
 enum { BGPU_JOINT_POINT2POINT = 0, BGPU_JOINT_FIXED = 1, BGPU_JOINT_HINGE = 2, BGPU_JOINT_GEAR = 3, BGPU_JOINT_SLIDER = 4,
-       BGPU_JOINT_SPRING2 = 5 /* added through bgpu_add_spring2_joints only */ };
+       BGPU_JOINT_SPRING2 = 5 /* added through bgpu_add_spring2_joints only */,
+       BGPU_JOINT_CONETWIST = 6 /* ConeTwistConstraint, conetwist.rs: cone axis is the frames' x column */ };
 #define BGPU_JOINT_DISABLE_COLLISIONS 0x01u /* no contacts between the two bodies (default on) */
 #define BGPU_JOINT_DISABLED 0x02u           /* set_enabled(false): no rows, no island link */
 #define BGPU_JOINT_ANGULAR_ONLY 0x04u       /* hinge: skip the three pivot rows */
@@ -149,6 +150,7 @@ enum { BGPU_JOINT_POINT2POINT = 0, BGPU_JOINT_FIXED = 1, BGPU_JOINT_HINGE = 2, B
 #define BGPU_JOINT_LIN_MOTOR 0x40u          /* slider: linear motor */
 #define BGPU_JOINT_ANG_MOTOR 0x80u          /* slider: angular motor */
 #define BGPU_JOINT_FRAME_B 0x100u           /* slider: linear reference frame B (use_linear_reference_frame_a off) */
+#define BGPU_JOINT_CONE_MOTOR 0x200u        /* cone twist: motor toward cone_motor_target */
 typedef struct bgpu_joint_desc {
     uint32_t kind;
     uint32_t body_a, body_b;
@@ -166,6 +168,14 @@ typedef struct bgpu_joint_desc {
     float softness_lim_lin, softness_lim_ang, damping_lim_lin, damping_lim_ang, softness_ortho_lin, softness_ortho_ang;
     /* motors (target velocity, max force) */
     float lin_motor_target_velocity, lin_motor_max_force, ang_motor_target_velocity, ang_motor_max_force;
+    /* cone twist (conetwist.rs:86-135): swing spans about the frame's y and z axes and the twist
+     * span about x (a span below 0.05 is a fixed or hinge configuration, a negative twist span
+     * frees the twist), limit softness, bias and relaxation factors; */
+    float swing_span1, swing_span2, twist_span, cone_softness, cone_bias_factor, cone_relaxation;
+    /* the motor target in constraint space (x y z w, as set_motor_target_in_constraint_space stores
+     * it) and its max impulse (negative: the swing row keeps its one-sided window) */
+    float cone_motor_target[4];
+    float cone_motor_max_impulse;
 } bgpu_joint_desc;
 
 /* Generic 6DOF spring-2 joints (Generic6DofSpring2Constraint, generic6dof_spring2.rs; Bullet's
@@ -207,7 +217,9 @@ typedef struct bgpu_world bgpu_world;
 
 void bgpu_solver_info_default(bgpu_solver_info* out);
 void bgpu_body_desc_default(bgpu_body_desc* out);
-/* Identity frames, collisions between the two bodies disabled, limit off (low 1 > high -1),
+/* Cone twist: spans 1e30 (unlimited), softness 1, bias factor 0.3, relaxation 1, no motor
+ * (identity target, max impulse -1).
+ * Identity frames, collisions between the two bodies disabled, limit off (low 1 > high -1),
  * softness 0.9, bias factor 0.3, relaxation 1.0 (AngularLimit::new), gear ratio 1; slider:
  * linear axis free (1 > -1), rotation locked (0, 0), softness and damping 1 (SliderConstraint::new). */
 void bgpu_joint_desc_default(bgpu_joint_desc* out);

@@ -394,8 +394,11 @@ void orc_world_set_solve_order(void* p, const uint64_t* keys, uint32_t n) {
 // angular motor (flags 64 linear motor, 128 angular motor, 256 linear reference frame B);
 // spring 2: 52 rotate order, then per axis (0-2 linear, 3-5 angular) 14 values from 53 + 14 i:
 // lower, upper, bounce, stop erp, stop cfm, motor erp, motor cfm, target velocity, max motor
-// force, servo target, stiffness, damping, equilibrium point, axis flags (S2_*).
-constexpr int JDESC = 137;
+// force, servo target, stiffness, damping, equilibrium point, axis flags (S2_*);
+// cone twist: 137 swing span 1, 138 swing span 2, 139 twist span, 140 limit softness, 141 bias
+// factor, 142 relaxation factor, 143-146 motor target (x y z w, constraint space), 147 motor max
+// impulse (flag 512: motor on).
+constexpr int JDESC = 148;
 
 uint32_t orc_world_add_joint(void* p, const double* d) {
     Handle* h = static_cast<Handle*>(p);
@@ -439,6 +442,11 @@ uint32_t orc_world_add_joint(void* p, const double* d) {
         jt.has_ang_motor = (f & 128u) != 0;
         jt.use_frame_a = (f & 256u) == 0;
         jt.rotate_order = uint32_t(d[52]);
+        jt.ct_span1 = static_cast<R>(d[137]); jt.ct_span2 = static_cast<R>(d[138]); jt.ct_twist = static_cast<R>(d[139]);
+        jt.ct_softness = static_cast<R>(d[140]); jt.ct_bias = static_cast<R>(d[141]); jt.ct_relax = static_cast<R>(d[142]);
+        jt.ct_target = Quat<R>(static_cast<R>(d[143]), static_cast<R>(d[144]), static_cast<R>(d[145]), static_cast<R>(d[146]));
+        jt.ct_max_impulse = static_cast<R>(d[147]);
+        jt.ct_has_motor = (f & 512u) != 0;
         for (int i = 0; i < 6; ++i) {
             const double* x = d + 53 + 14 * i;
             Spring2Axis<R>& m = jt.s2[i];
@@ -466,7 +474,9 @@ void orc_world_joint_angles(void* p, double* out) {
     Handle* h = static_cast<Handle*>(p);
     DISPATCH(h, {
         for (size_t k = 0; k < w.joints.size(); ++k)
-            out[k] = w.joints[k].kind == JOINT_SLIDER ? w.joints[k].ang_pos : w.joints[k].hinge_angle;
+            out[k] = w.joints[k].kind == JOINT_SLIDER      ? w.joints[k].ang_pos
+                     : w.joints[k].kind == JOINT_CONETWIST ? w.joints[k].ct_twist_angle
+                                                           : w.joints[k].hinge_angle;
     });
 }
 

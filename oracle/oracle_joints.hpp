@@ -14,6 +14,8 @@
 //   crates/bullet-dynamics/src/constraint/slider.rs:159-475 (slider: frame-offset rows, linear and
 //     angular limits and motors), shared.rs:30-55 (adjust_angle_to_limits), :126-145
 //     (mirrored_row_limits);
+//   crates/bullet-dynamics/src/constraint/conetwist.rs:222-548 (cone twist: pivot rows, elliptical
+//     swing limit, fixed and hinge configurations, twist limit, motor target);
 //   crates/bullet-dynamics/src/constraint/generic6dof_spring2.rs:650-1383 (spring 2: per-axis
 //     limit pairs, lock rows, motors, servos, clamped springs, six Euler orders, static-body
 //     mass split), with the global ERP / CFM fallback of prepare_rows (constraint.rs:755-829).
@@ -28,7 +30,8 @@
 
 namespace oracle {
 
-enum : uint32_t { JOINT_POINT2POINT = 0, JOINT_FIXED = 1, JOINT_HINGE = 2, JOINT_GEAR = 3, JOINT_SLIDER = 4, JOINT_SPRING2 = 5 };
+enum : uint32_t { JOINT_POINT2POINT = 0, JOINT_FIXED = 1, JOINT_HINGE = 2, JOINT_GEAR = 3, JOINT_SLIDER = 4, JOINT_SPRING2 = 5,
+                  JOINT_CONETWIST = 6 };
 // RowLimits (sequential_impulse.rs): which clamp the accumulated impulse takes.
 enum : uint32_t { LIM_UNBOUNDED = 0, LIM_BILATERAL = 1, LIM_LOWER = 2, LIM_UPPER = 3, LIM_WINDOW = 4 };
 
@@ -88,6 +91,13 @@ struct Joint {
     V3<R> s2_diff, s2_euler;  // per-step state: pivot offset in A's frame, relative Euler angles
     R fact_a = R(0.5), fact_b = R(0.5);
     bool has_static_body = false;
+    // cone twist (ConeTwistConstraint, conetwist.rs:5-116): spans, limit softness, bias and
+    // relaxation; an optional motor target in constraint space with its max impulse (< 0: none)
+    R ct_span1 = R(1e30), ct_span2 = R(1e30), ct_twist = R(1e30), ct_softness = 1, ct_bias = R(0.3), ct_relax = 1;
+    bool ct_has_motor = false;
+    Quat<R> ct_target;
+    R ct_max_impulse = -1;
+    R ct_twist_angle = 0;  // per-step state
     Joint() {
         for (int i = 0; i < 3; ++i) { s2[i].lower = 0; s2[i].upper = 0; s2[i].max_motor_force = 0; }
     }
@@ -295,6 +305,203 @@ void hinge_frames(const V3<R>& pivot_a, const V3<R>& axis_a_in, const V3<R>& piv
     V3<R> t2b = axis_b.cross(t1b);
     fb.origin = pivot_b;
     fb.basis = M3<R>(t1b, t2b, axis_b);
+}
+
+// glam 0.33.3 Quat::from_mat3 (not in the reference tree; used through compat.rs:52-62): the
+// published branch on the diagonal (m22, then m11 -/+ m00) choosing the largest of x, y, z, w to
+// divide by. mRC below is column R, row C.
+template <class R>
+Quat<R> quat_from_mat3(const M3<R>& m) {
+    const R m00 = m.c0.x, m01 = m.c0.y, m02 = m.c0.z, m10 = m.c1.x, m11 = m.c1.y, m12 = m.c1.z;
+    const R m20 = m.c2.x, m21 = m.c2.y, m22 = m.c2.z;
+    if (m22 <= R(0)) {
+        const R dif10 = m11 - m00, omm22 = R(1) - m22;
+        if (dif10 <= R(0)) {
+            const R f = omm22 - dif10, inv = R(0.5) / std::sqrt(f);
+            return Quat<R>(f * inv, (m01 + m10) * inv, (m02 + m20) * inv, (m12 - m21) * inv);
+        }
+        const R f = omm22 + dif10, inv = R(0.5) / std::sqrt(f);
+        return Quat<R>((m01 + m10) * inv, f * inv, (m12 + m21) * inv, (m20 - m02) * inv);
+    }
+    const R sum10 = m11 + m00, opm22 = R(1) + m22;
+    if (sum10 <= R(0)) {
+        const R f = opm22 - sum10, inv = R(0.5) / std::sqrt(f);
+        return Quat<R>((m02 + m20) * inv, (m12 + m21) * inv, f * inv, (m01 - m10) * inv);
+    }
+    const R f = opm22 + sum10, inv = R(0.5) / std::sqrt(f);
+    return Quat<R>((m12 - m21) * inv, (m20 - m02) * inv, (m01 - m10) * inv, f * inv);
+}
+
+// conetwist.rs:546-548
+template <class R>
+R quaternion_angle(const Quat<R>& q) {
+    return R(2) * std::acos(std::min(std::max(q.w, R(-1)), R(1)));
+}
+
+// conetwist.rs:481-502 (compute_cone_limit_info): swing angle, axis, elliptical limit
+template <class R>
+void ct_cone_limit_info(const Joint<R>& jt, const Quat<R>& q, R& angle, V3<R>& axis, R& limit) {
+    const R eps = std::numeric_limits<R>::epsilon();
+    angle = quaternion_angle(q);
+    axis = V3<R>();
+    limit = jt.ct_span1;
+    if (angle > eps) {
+        axis = q.xyz().normalize();
+        const R xe = axis.y, ye = -axis.z;
+        if (std::fabs(xe) > eps) {
+            const R slope2 = (ye * ye) / (xe * xe);
+            R norm = R(1) / (jt.ct_span2 * jt.ct_span2);
+            norm += slope2 / (jt.ct_span1 * jt.ct_span1);
+            limit = std::sqrt((R(1) + slope2) / norm);
+        }
+    }
+}
+
+// conetwist.rs:504-519 (compute_twist_limit_info)
+template <class R>
+void ct_twist_limit_info(const Quat<R>& q, R& angle, V3<R>& axis) {
+    Quat<R> qm = q;
+    angle = quaternion_angle(q);
+    if (angle > R(3.14159265358979323846)) {
+        qm = Quat<R>(-q.x, -q.y, -q.z, -q.w);
+        angle = quaternion_angle(qm);
+    }
+    axis = qm.xyz();
+    if (angle > std::numeric_limits<R>::epsilon()) axis = axis.normalize();
+}
+
+// conetwist.rs:222-342 (prepare_rows) with calc_angle_info (:344-479) and
+// adjust_swing_axis_to_use_ellipse_normal (:521-539).
+template <class R, class B>
+void prepare_conetwist_rows(Joint<R>& jt, uint32_t ia, uint32_t ib, const B& a, const B& b, R inv_dt, R erp,
+                            std::vector<JointRow<R>>& out) {
+    const R eps = std::numeric_limits<R>::epsilon(), fix = R(0.05);
+    const R inf = std::numeric_limits<R>::infinity();
+    M3<R> tr_a = M3<R>::from_quat(a.orientation) * jt.frame_a.basis;
+    M3<R> tr_b = M3<R>::from_quat(b.orientation) * jt.frame_b.basis;
+    V3<R> pivot_a = a.position + a.orientation.rotate(jt.frame_a.origin);
+    V3<R> pivot_b = b.position + b.orientation.rotate(jt.frame_b.origin);
+    V3<R> r_a = pivot_a - a.position, r_b = pivot_b - b.position;
+    const R k = inv_dt * erp;
+    auto push = [&](const V3<R>& la, const V3<R>& aa, const V3<R>& lb, const V3<R>& ab, R bias, uint32_t lim, R lo,
+                    R hi) { out.push_back(prepare_joint_row(ia, ib, la, aa, lb, ab, a, b, bias, lim, lo, hi)); };
+    const V3<R> zero;
+    for (int axis = 0; axis < 3; ++axis) {
+        V3<R> n;
+        n.at(axis) = R(1);
+        push(n, r_a.cross(n), n, r_b.cross(n), k * (pivot_a - pivot_b)[axis], LIM_UNBOUNDED, 0, 0);
+    }
+    // calc_angle_info
+    R swing_corr = 0, twist_corr = 0;
+    V3<R> swing_axis, twist_axis;
+    bool solve_swing = false, solve_twist = false;
+    const V3<R> X(1, 0, 0);
+    if (jt.ct_has_motor) {
+        M3<R> r_delta = tr_b * M3<R>::from_quat(jt.ct_target) * tr_a.transpose();
+        Quat<R> q_delta = quat_from_mat3(r_delta).normalize();
+        V3<R> sa = q_delta.xyz();
+        R l2 = sa.length_squared();
+        if (l2 > eps) {
+            swing_axis = sa / std::sqrt(l2);
+            swing_corr = quaternion_angle(q_delta);
+            if (std::fabs(swing_corr) > eps) solve_swing = true;
+        }
+    } else {
+        Quat<R> q_a = quat_from_mat3(tr_a), q_b = quat_from_mat3(tr_b);
+        Quat<R> q_ab = (q_b.inverse() * q_a).normalize();
+        V3<R> v_cone = q_ab.rotate(X).normalize();
+        Quat<R> q_cone = rotation_arc(X, v_cone).normalize();
+        Quat<R> q_twist = (q_cone.inverse() * q_ab).normalize();
+        const R s1 = jt.ct_span1, s2 = jt.ct_span2;
+        if (s1 >= fix && s2 >= fix) {
+            R angle, limit;
+            V3<R> axis;
+            ct_cone_limit_info(jt, q_cone, angle, axis, limit);
+            if (angle > limit * jt.ct_softness) {
+                solve_swing = true;
+                swing_corr = angle - limit * jt.ct_softness;
+                // adjust_swing_axis_to_use_ellipse_normal
+                R y = -axis.z, z = axis.y;
+                if (std::fabs(z) > eps) {
+                    R grad = y / z;
+                    grad *= s2 / s1;
+                    y = y > R(0) ? std::fabs(grad * z) : -std::fabs(grad * z);
+                    axis.z = -y;
+                    axis.y = z;
+                    axis = axis.normalize();
+                }
+                swing_axis = q_b.rotate(-axis);
+            }
+        } else {
+            const V3<R> iv_a = tr_a.c0, jv_a = tr_a.c1, kv_a = tr_a.c2, iv_b = tr_b.c0;
+            R x = iv_b.dot(iv_a), y = iv_b.dot(jv_a), z = iv_b.dot(kv_a);
+            if (s1 < fix && s2 < fix) {
+                if (std::fabs(y) > eps || std::fabs(z) > eps) {
+                    solve_swing = true;
+                    swing_axis = -iv_b.cross(iv_a);
+                }
+            } else {
+                if (s1 < fix) {
+                    if (std::fabs(x) > eps || std::fabs(z) > eps) {
+                        solve_swing = true;
+                        if (s2 >= fix) {
+                            y = 0;
+                            R span2 = std::atan2(z, x);
+                            if (span2 > s2) { x = std::cos(s2); z = std::sin(s2); }
+                            else if (span2 < -s2) { x = std::cos(s2); z = -std::sin(s2); }
+                        }
+                    }
+                } else {
+                    if (std::fabs(x) > eps || std::fabs(y) > eps) {
+                        solve_swing = true;
+                        if (s1 >= fix) {
+                            z = 0;
+                            R span1 = std::atan2(y, x);
+                            if (span1 > s1) { x = std::cos(s1); y = std::sin(s1); }
+                            else if (span1 < -s1) { x = std::cos(s1); y = -std::sin(s1); }
+                        }
+                    }
+                }
+                V3<R> target = (iv_a * x + jv_a * y + kv_a * z).normalize();
+                swing_axis = -iv_b.cross(target);
+                swing_corr = swing_axis.length();
+                if (std::fabs(swing_corr) > eps) swing_axis = swing_axis.normalize();
+            }
+        }
+        if (jt.ct_twist >= R(0)) {
+            R angle;
+            V3<R> axis;
+            ct_twist_limit_info(q_twist, angle, axis);
+            jt.ct_twist_angle = angle;
+            if (angle > jt.ct_twist * jt.ct_softness) {
+                solve_twist = true;
+                twist_corr = angle - jt.ct_twist * jt.ct_softness;
+                twist_axis = q_b.rotate(-axis);
+            }
+        } else {
+            jt.ct_twist_angle = 0;
+        }
+    }
+    const R relax = jt.ct_relax;
+    if (solve_swing) {
+        if (jt.ct_span1 < fix && jt.ct_span2 < fix) {
+            const R fact = inv_dt * relax;
+            const V3<R> dirs[2] = {tr_a.c1, tr_a.c2};
+            for (const V3<R>& dir : dirs) push(zero, dir, zero, dir, -fact * swing_axis.dot(dir), LIM_UNBOUNDED, 0, 0);
+        } else {
+            V3<R> ax1 = swing_axis * (relax * relax);
+            if (jt.ct_has_motor && jt.ct_max_impulse >= R(0))
+                push(zero, ax1, zero, ax1, -inv_dt * jt.ct_bias * swing_corr, LIM_WINDOW, -jt.ct_max_impulse, R(0));
+            else
+                push(zero, ax1, zero, ax1, -inv_dt * jt.ct_bias * swing_corr, LIM_UPPER, R(0), R(0));
+        }
+    }
+    if (solve_twist) {
+        V3<R> ax1 = twist_axis * (relax * relax);
+        uint32_t lim = jt.ct_twist > R(0) ? (twist_corr > R(0) ? LIM_UPPER : LIM_LOWER) : LIM_UNBOUNDED;
+        push(zero, ax1, zero, ax1, -inv_dt * jt.ct_bias * twist_corr, lim, R(0), R(0));
+    }
+    (void)inf;
 }
 
 // generic6dof_spring2.rs:1236-1241 (btGetMatrixElem): row index % 3 of column index / 3.
@@ -618,6 +825,8 @@ void prepare_joint_rows(Joint<R>& jt, uint32_t jid, const std::vector<B>& bodies
         }
     } else if (jt.kind == JOINT_SPRING2) {
         prepare_spring2_rows(jt, ia, ib, a, b, inv_dt, erp, global_cfm, out);
+    } else if (jt.kind == JOINT_CONETWIST) {
+        prepare_conetwist_rows(jt, ia, ib, a, b, inv_dt, erp, out);
     } else if (jt.kind == JOINT_GEAR) {  // gear.rs:33-57
         V3<R> axis_a_world = a.orientation.rotate(jt.frame_a.basis.c2);
         V3<R> axis_b_world = b.orientation.rotate(jt.frame_b.basis.c2);

@@ -122,8 +122,8 @@ def body_desc(shape, pos, quat=(0, 0, 0, 1), linvel=(0, 0, 0), angvel=(0, 0, 0),
     return d
 
 
-JDESC = 137   # joint descriptor doubles (orc_world_add_joint)
-JOINT_POINT2POINT, JOINT_FIXED, JOINT_HINGE, JOINT_GEAR, JOINT_SLIDER = 0, 1, 2, 3, 4
+JDESC = 148   # joint descriptor doubles (orc_world_add_joint)
+JOINT_POINT2POINT, JOINT_FIXED, JOINT_HINGE, JOINT_GEAR, JOINT_SLIDER, JOINT_CONETWIST = 0, 1, 2, 3, 4, 6
 JF_DISABLE_COLLISIONS, JF_DISABLED, JF_ANGULAR_ONLY, JF_LIMIT, JF_MOTOR, JF_ERP = 1, 2, 4, 8, 16, 32
 JF_LIN_MOTOR, JF_ANG_MOTOR, JF_FRAME_B = 64, 128, 256
 
@@ -131,7 +131,8 @@ JF_LIN_MOTOR, JF_ANG_MOTOR, JF_FRAME_B = 64, 128, 256
 def joint_desc(kind, body_a, body_b, frame_a, frame_b, flags=JF_DISABLE_COLLISIONS, erp=0.0, impulse_clamp=0.0,
                limit=(1.0, -1.0), softness=0.9, bias_factor=0.3, relaxation=1.0, motor=(0.0, 0.0), gear_ratio=1.0,
                lin_limits=(1.0, -1.0), ang_limits=(0.0, 0.0), slider_softness=(1.0, 1.0, 1.0, 1.0, 1.0, 1.0),
-               lin_motor=(0.0, 0.0), ang_motor=(0.0, 0.0), rotate_order=0, s2_axes=None):
+               lin_motor=(0.0, 0.0), ang_motor=(0.0, 0.0), rotate_order=0, s2_axes=None,
+               cone=(1e30, 1e30, 1e30, 1.0, 0.3, 1.0), cone_motor=((0.0, 0.0, 0.0, 1.0), -1.0)):
     """frame_*: 12 numbers (origin xyz, basis columns x, y, z) in the body's frame; s2_axes: the
     (6, 14) spring-2 axis table (parameters in bgpu_spring2_axis field order, then the flags)."""
     d = np.zeros(JDESC)
@@ -149,6 +150,9 @@ def joint_desc(kind, body_a, body_b, frame_a, frame_b, flags=JF_DISABLE_COLLISIO
     d[48], d[49] = lin_motor
     d[50], d[51] = ang_motor
     d[52] = rotate_order
+    d[137:143] = cone  # swing span 1, swing span 2, twist span, softness, bias factor, relaxation
+    d[143:147] = cone_motor[0]
+    d[147] = cone_motor[1]
     if s2_axes is not None:
         d[53:53 + 84] = np.asarray(s2_axes, dtype=np.float64).reshape(84)
     return d

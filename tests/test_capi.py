@@ -59,5 +59,5 @@ def test_struct_layouts_match_the_header(bgpu_mod):
     # bgpu_body_desc: 4 + 12 + 16 + 12 + 12 + 5*4 + 4 + 2 + 2 + 4 + 8 = 96 bytes
     assert ctypes.sizeof(bgpu_mod.BodyDesc) == 96
     assert ctypes.sizeof(bgpu_mod.SolverInfo) == 48
-    assert ctypes.sizeof(bgpu_mod.JointDesc) == 4 * 4 + 24 * 4 + 24 * 4
+    assert ctypes.sizeof(bgpu_mod.JointDesc) == 4 * 4 + 24 * 4 + 35 * 4
     assert ctypes.sizeof(bgpu_mod.StepStats) == 10 * 4 + 7 * 4 + 2 * 4 + 4

@@ -580,3 +580,35 @@ def test_spring2_chains_match_the_oracle(gpu):
     w, _, st, _ = run_pair(s, gpu, 120, tol=1e-3, window=5)
     assert w.joint_rows().shape[0] == 450 * 6
     assert st[-1, :, 1].min() < 3.9  # the chains sag
+
+
+@pytest.mark.parametrize("case", ["swing_limit", "twist_lock", "fixed", "hinge_y", "hinge_z", "motor"])
+def test_cone_twist_matches_the_oracle(gpu, case):  # constraint/tests.rs:518-600; conetwist.rs:222-539
+    """A bob pinned at a static anchor by a cone twist (cone axis X on both bodies): the reference's
+    two cone-twist tests, the fixed and both hinge configurations, and a motor target."""
+    spans, angvel, gravity, steps = {
+        "swing_limit": ((0.44, 0.44, -1.0), (0.0, 0.0, 4.0), (0.0, -9.81, 0.0), 300),
+        "twist_lock": ((0.9, 0.9, 0.0), (6.0, 0.0, 0.0), (0.0, -9.81, 0.0), 300),
+        "fixed": ((0.0, 0.0, 1e30), (0.0, 3.0, 3.0), (0.0, -9.81, 0.0), 120),
+        "hinge_y": ((0.0, 0.5, 1e30), (0.0, 3.0, 3.0), (0.0, -9.81, 0.0), 120),
+        "hinge_z": ((0.5, 0.0, 1e30), (0.0, 3.0, 3.0), (0.0, -9.81, 0.0), 120),
+        "motor": ((1.0, 1.0, 1.0), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), 200),
+    }[case]
+    s = JScene(gravity)
+    anchor = s.body(s.shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+    bob = s.body(s.shape(orc.SPHERE, [0.1]), (0, 0, 0), angvel=angvel)
+    kw = dict(cone=tuple(spans) + (1.0, 0.3, 1.0))
+    flags = orc.JF_DISABLE_COLLISIONS
+    if case == "motor":
+        kw["cone_motor"] = ((0.0, 0.0, math.sin(0.15), math.cos(0.15)), 5.0)
+        flags |= 512
+    s.joint(orc.JOINT_CONETWIST, bob, anchor, orc.frame((0, 0, 0)), orc.frame((0, 0, 0)), flags=flags, **kw)
+    _, _, st, _ = run_pair(s, gpu, steps)
+    ax = lambda x, i: rotate(x[i, 3:7], (1.0, 0.0, 0.0))
+    swing = [math.acos(max(-1.0, min(1.0, float(ax(x, anchor) @ ax(x, bob))))) for x in st]
+    if case == "swing_limit":
+        assert 0.3 < max(swing) < 0.55
+    if case == "twist_lock":
+        assert abs(st[-1, bob, 10]) < 0.1
+    if case == "motor":
+        assert abs(swing[-1] - 0.3) < 0.05

@@ -359,3 +359,73 @@ def test_slider_angular_limit_stops_the_twist(precision):  # tests.rs:738-771
         w.step(DT)
         max_ang = max(max_ang, abs(w.joint_angles(1)[0]))
     assert max_ang < 0.5
+
+
+def cone_world(precision, spans, angvel, gravity=(0.0, -9.81, 0.0), motor=None):
+    """tests.rs:518-600: a 0.1 m bob pinned at a static anchor by a cone twist whose cone axis is X
+    on both bodies (identity frames at the origin)."""
+    w = world(precision, gravity)
+    anchor = w.add_body(w.add_shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+    bob = w.add_body(w.add_shape(orc.SPHERE, [0.1]), (0, 0, 0), angvel=angvel, mass=1.0)
+    kw = dict(cone=tuple(spans) + (1.0, 0.3, 1.0))
+    flags = orc.JF_DISABLE_COLLISIONS
+    if motor is not None:
+        kw["cone_motor"] = motor
+        flags |= JF_CONE_MOTOR
+    w.add_joint(orc.joint_desc(orc.JOINT_CONETWIST, bob, anchor, orc.frame((0, 0, 0)), orc.frame((0, 0, 0)),
+                               flags=flags, **kw))
+    return w, anchor, bob
+
+
+JF_CONE_MOTOR = 512
+
+
+def axis_angle_between(st, a, b):
+    ax_a, ax_b = rotate(st[a, 3:7], (1, 0, 0)), rotate(st[b, 3:7], (1, 0, 0))
+    return math.acos(max(-1.0, min(1.0, float(ax_a @ ax_b))))
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_cone_twist_limits_the_swing(precision):  # tests.rs:518-560
+    w, anchor, bob = cone_world(precision, (0.44, 0.44, -1.0), (0.0, 0.0, 4.0))
+    max_swing = 0.0
+    for _ in range(600):
+        w.step(DT)
+        max_swing = max(max_swing, axis_angle_between(w.state(), anchor, bob))
+    assert 0.3 < max_swing < 0.55
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_cone_twist_locks_the_twist(precision):  # tests.rs:563-600
+    w, anchor, bob = cone_world(precision, (0.9, 0.9, 0.0), (6.0, 0.0, 0.0))
+    max_twist = 0.0
+    for _ in range(300):
+        w.step(DT)
+        max_twist = max(max_twist, w.joint_angles(1)[0])
+    assert max_twist < 0.1
+    assert abs(w.state()[bob, 10]) < 0.1
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+@pytest.mark.parametrize("spans, limit", [((0.0, 0.0, 1e30), 0.1), ((0.0, 0.5, 1e30), 0.62), ((0.5, 0.0, 1e30), 0.62)])
+def test_cone_twist_fixed_and_hinge_configurations(precision, spans, limit):
+    """conetwist.rs:406-461: a span below the fix threshold (0.05) turns the cone into a hinge
+    about the other axis (limited by the other span) or, both below, locks the X axes together."""
+    w, anchor, bob = cone_world(precision, spans, (0.0, 3.0, 3.0))
+    max_swing = 0.0
+    for _ in range(240):
+        w.step(DT)
+        st = w.state()
+        assert np.all(np.isfinite(st[:, :13]))
+        max_swing = max(max_swing, axis_angle_between(st, anchor, bob))
+    assert max_swing < limit
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_cone_twist_motor_drives_to_the_target(precision):  # conetwist.rs:138-187, :351-369
+    target = (0.0, 0.0, math.sin(0.15), math.cos(0.15))  # 0.3 rad about Z, in constraint space
+    w, anchor, bob = cone_world(precision, (1.0, 1.0, 1.0), (0.0, 0.0, 0.0), gravity=(0.0, 0.0, 0.0),
+                                motor=(target, 5.0))
+    for _ in range(300):
+        w.step(DT)
+    assert abs(axis_angle_between(w.state(), anchor, bob) - 0.3) < 0.05
