@@ -16,7 +16,7 @@ SPHERE, BOX, CAPSULE, HULL, PLANE = 0, 1, 2, 3, 4
 JOINT_POINT2POINT, JOINT_FIXED, JOINT_HINGE, JOINT_GEAR, JOINT_SLIDER = 0, 1, 2, 3, 4
 JOINT_DISABLE_COLLISIONS, JOINT_DISABLED, JOINT_ANGULAR_ONLY, JOINT_LIMIT, JOINT_MOTOR, JOINT_ERP = 1, 2, 4, 8, 16, 32
 JOINT_LIN_MOTOR, JOINT_ANG_MOTOR, JOINT_FRAME_B = 64, 128, 256
-JOINT_SPRING2, JOINT_CONETWIST, JOINT_CONE_MOTOR = 5, 6, 512
+JOINT_SPRING2, JOINT_CONETWIST, JOINT_CONE_MOTOR, JOINT_GENERIC6DOF = 5, 6, 512, 7
 ROTATE_XYZ, ROTATE_XZY, ROTATE_YXZ, ROTATE_YZX, ROTATE_ZXY, ROTATE_ZYX = range(6)
 (S2_MOTOR, S2_SERVO, S2_SPRING, S2_STIFFNESS_LIMITED, S2_DAMPING_LIMITED, S2_STOP_ERP, S2_STOP_CFM, S2_MOTOR_ERP,
  S2_MOTOR_CFM) = (1, 2, 4, 8, 16, 32, 64, 128, 256)
@@ -203,6 +203,33 @@ class Spring2:
         return np.array([[getattr(a, f) for f, _ in Spring2Axis._fields_] for a in self.desc.axis], dtype=np.float64)
 
 
+class Generic6Dof(Spring2):
+    """One classic generic 6DOF joint (Generic6DofConstraint, generic6dof.rs:131-262) with the
+    reference's setters; defaults are Bullet's (linear locked at 0, angular free)."""
+    KIND = JOINT_GENERIC6DOF
+
+    def __init__(self, body_a, body_b, frame_a=None, frame_b=None, flags=JOINT_DISABLE_COLLISIONS):
+        super().__init__(body_a, body_b, frame_a, frame_b, ROTATE_XYZ, flags)
+
+    @classmethod
+    def universal(cls, body_a, body_b, pos_a, quat_a, pos_b, quat_b, anchor, axis1, axis2):
+        """Generic6DofConstraint::universal (PhysicsWorld::add_universal) from the bodies' poses."""
+        j = cls.__new__(cls)
+        j.desc = Spring2Desc()
+        args = [f32(v) for v in (pos_a, quat_a, pos_b, quat_b, anchor, axis1, axis2)]
+        check(lib().bgpu_generic6dof_universal(*[fptr(a) for a in args], body_a, body_b, ctypes.byref(j.desc)),
+              "universal")
+        return j
+
+    def enable_motor(self, axis, target_velocity, max_force):
+        a = self.desc.axis[axis]
+        a.target_velocity, a.max_motor_force = target_velocity, max_force
+        self._flag(axis, S2_MOTOR, True)
+
+    def disable_motor(self, axis):
+        self._flag(axis, S2_MOTOR, False)
+
+
 class BodyDesc(ctypes.Structure):
     _fields_ = [("shape", ctypes.c_uint32), ("position", ctypes.c_float * 3), ("orientation", ctypes.c_float * 4),
                 ("linear_velocity", ctypes.c_float * 3), ("angular_velocity", ctypes.c_float * 3),
@@ -276,6 +303,8 @@ def lib():
             "bgpu_spring2_hinge2": (S, [F, F, F, F, F, F, F, U32, U32, ctypes.POINTER(Spring2Desc)]),
             "bgpu_add_spring2_joints": (S, [P, U32, ctypes.POINTER(Spring2Desc), U32P]),
             "bgpu_read_joint_spring2_state": (S, [P, F]),
+            "bgpu_add_generic6dof_joints": (S, [P, U32, ctypes.POINTER(Spring2Desc), U32P]),
+            "bgpu_generic6dof_universal": (S, [F, F, F, F, F, F, F, U32, U32, ctypes.POINTER(Spring2Desc)]),
             "bgpu_set_ccd": (S, [P, U32, U32, F, F]),
             "bgpu_read_ccd_clamps": (S, [P, F]),
             "bgpu_num_joints": (U32, [P]),
@@ -605,10 +634,12 @@ class World:
         return out
 
     def add_spring2(self, joint):
-        """Adds a Spring2 joint (Constraint::generic_6dof_spring2); returns its joint id."""
+        """Adds a Spring2 joint (Constraint::generic_6dof_spring2) or a Generic6Dof joint
+        (Constraint::generic_6dof); returns its joint id."""
         first = ctypes.c_uint32()
-        check(self.L.bgpu_add_spring2_joints(self.h, 1, ctypes.byref(joint.desc), ctypes.byref(first)),
-              "add_spring2_joints")
+        add = self.L.bgpu_add_generic6dof_joints if getattr(joint, "KIND", 5) == JOINT_GENERIC6DOF \
+            else self.L.bgpu_add_spring2_joints
+        check(add(self.h, 1, ctypes.byref(joint.desc), ctypes.byref(first)), "add_joints")
         return first.value
 
     @property

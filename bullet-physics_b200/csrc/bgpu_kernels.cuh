@@ -219,7 +219,8 @@ enum : uint32_t { S2_MOTOR = 1u, S2_SERVO = 2u, S2_SPRING = 4u, S2_STIFFNESS_LIM
 // Joint row, JROW_F4 float4: [0] lin_a | effective mass, [1] ang_a | bias, [2] lin_b | cfm,
 // [3] ang_b | limit kind (bits), [4] lower, upper, accumulated impulse, 0.
 constexpr uint32_t JROW_F4 = 5;
-enum : uint32_t { JK_POINT2POINT = 0, JK_FIXED = 1, JK_HINGE = 2, JK_GEAR = 3, JK_SLIDER = 4, JK_SPRING2 = 5, JK_CONETWIST = 6 };
+enum : uint32_t { JK_POINT2POINT = 0, JK_FIXED = 1, JK_HINGE = 2, JK_GEAR = 3, JK_SLIDER = 4, JK_SPRING2 = 5, JK_CONETWIST = 6,
+                  JK_GENERIC6DOF = 7 };
 enum : uint32_t { JF_DISABLE_COLLISIONS = 1u, JF_DISABLED = 2u, JF_ANGULAR_ONLY = 4u, JF_LIMIT = 8u, JF_MOTOR = 16u, JF_ERP = 32u,
                   JF_LIN_MOTOR = 64u, JF_ANG_MOTOR = 128u, JF_FRAME_B = 256u,
                   JF_CONE_MOTOR = 512u };

@@ -302,6 +302,96 @@ __device__ __noinline__ void conetwist_rows(RowOut& out, const BodyDev& b, const
     }
 }
 
+// generic6dof.rs:264-546 (classic 6DOF rows): per axis one limit-or-motor row, angular axes
+// first; the parameters come from the spring-2 axis table (lower, upper, bounce, stop erp,
+// target velocity, max motor force, S2_MOTOR).
+__device__ __noinline__ void generic6dof_rows(RowOut& out, const BodyDev& b, const JointsDev& jd, uint32_t jid,
+                                              const float4* d, uint32_t ia, uint32_t ib, Q qa, Q qb, V3 r_a, V3 r_b,
+                                              V3 pivot_a, V3 pivot_b, float inv_dt) {
+    const float inf = INFINITY;
+    const V3 zero = V3{0.0f, 0.0f, 0.0f};
+    const float4* aux = jd.aux + __float_as_uint(d[9].x);
+    const M3 tr_a = mul(from_quat(qa), M3{from4(d[2]), from4(d[3]), from4(d[4])});
+    const M3 tr_b = mul(from_quat(qb), M3{from4(d[6]), from4(d[7]), from4(d[8])});
+    const V3 diff = mul(transpose(tr_a), pivot_b - pivot_a);
+    // shared.rs:108-123 (relative_rotation_info)
+    const V3 euler = euler_xyz(mul(transpose(tr_a), tr_b));
+    const V3 axis0 = tr_b.c0, axis2 = tr_a.c2;
+    V3 axes[3];
+    axes[1] = cross(axis2, axis0);
+    axes[0] = cross(axes[1], axis2);
+    axes[2] = cross(axis0, axes[1]);
+    for (int i = 0; i < 3; ++i) axes[i] = normalize(axes[i]);
+    jd.s2_state[2 * size_t(jid)] = to4(euler, diff.x);
+    jd.s2_state[2 * size_t(jid) + 1] = make_float4(diff.y, diff.z, 0.5f, 0.0f);  // no static-body split here
+    const V3 va = from4(b.linvel[ia]), vb = from4(b.linvel[ib]), wa = from4(b.angvel[ia]), wb = from4(b.angvel[ib]);
+    auto push_row = [&](V3 ax1, bool linear, int limit, float limit_err, float lo, float hi, float stop_erp, bool powered,
+                        float target_velocity, float max_motor_force, float current_pos, float bounce, float row_vel) {
+        if (limit != 0 && lo == hi) powered = false;
+        float row_error = 0.0f;
+        if (powered && limit == 0) {
+            const float tag_vel = linear ? -target_velocity : target_velocity;
+            row_error += motor_factor(current_pos, lo, hi, tag_vel, inv_dt * stop_erp) * target_velocity;
+        }
+        if (limit != 0) {
+            const float k = inv_dt * stop_erp;
+            row_error += linear ? k * limit_err : -k * limit_err;
+            if (bounce > 0.0f) {
+                if (limit == 1) {
+                    if (row_vel < 0.0f) { const float newc = -bounce * row_vel; if (newc > row_error) row_error = newc; }
+                } else if (row_vel > 0.0f) {
+                    const float newc = -bounce * row_vel;
+                    if (newc < row_error) row_error = newc;
+                }
+            }
+        }
+        float lower = 0.0f, upper = 0.0f;
+        if (powered && limit == 0) { lower = -max_motor_force / inv_dt; upper = max_motor_force / inv_dt; }
+        else if (limit != 0) {
+            if (lo == hi) { lower = -inf; upper = inf; }
+            else if (limit == 1) { lower = 0.0f; upper = inf; }
+            else { lower = -inf; upper = 0.0f; }
+        }
+        uint32_t lim;
+        float rlo, rhi;
+        mirrored_row_limits(lower, upper, lim, rlo, rhi);
+        if (linear) out.push(ax1, cross(r_a, ax1), ax1, cross(r_b, ax1), -row_error, lim, rlo, rhi);
+        else out.push(zero, ax1, zero, ax1, -row_error, lim, rlo, rhi);
+    };
+    for (int i = 0; i < 3; ++i) {
+        const float4 x = aux[(3 + i) * S2_AXIS_F4], y = aux[(3 + i) * S2_AXIS_F4 + 1], z = aux[(3 + i) * S2_AXIS_F4 + 2];
+        const bool motor = (__float_as_uint(aux[(3 + i) * S2_AXIS_F4 + 3].y) & S2_MOTOR) != 0;
+        const float lo = x.x, hi = x.y;
+        const float angle = adjust_angle_to_limits(comp(euler, i), lo, hi);
+        int limit = 0;
+        float err = 0.0f;
+        if (!(lo > hi) && (angle < lo || angle > hi)) {
+            limit = angle < lo ? 1 : 2;
+            err = angle - (angle < lo ? lo : hi);
+            if (err > PI_F) err -= 2.0f * PI_F;
+            else if (err < -PI_F) err += 2.0f * PI_F;
+        }
+        if (limit != 0 || motor)
+            push_row(axes[i], false, limit, err, lo, hi, x.w, motor, y.w, z.x, angle, x.z,
+                     dot(wa, axes[i]) - dot(wb, axes[i]));
+    }
+    for (int i = 0; i < 3; ++i) {
+        const float4 x = aux[i * S2_AXIS_F4], y = aux[i * S2_AXIS_F4 + 1], z = aux[i * S2_AXIS_F4 + 2];
+        const bool motor = (__float_as_uint(aux[i * S2_AXIS_F4 + 3].y) & S2_MOTOR) != 0;
+        const float lo = x.x, hi = x.y, v = comp(diff, i);
+        int limit = 0;
+        float err = 0.0f;
+        if (!(lo > hi)) {
+            if (v < lo) { limit = 2; err = v - lo; }
+            else if (v > hi) { limit = 1; err = v - hi; }
+        }
+        if (limit != 0 || motor) {
+            const V3 ax1 = i == 0 ? tr_a.c0 : (i == 1 ? tr_a.c1 : tr_a.c2);
+            push_row(ax1, true, limit, err, lo, hi, x.w, motor, y.w, z.x, v, 0.0f, dot(va, ax1) - dot(vb, ax1));
+        }
+    }
+}
+
 // generic6dof_spring2.rs:1236-1241 (btGetMatrixElem): row index % 3 of column index / 3.
 __device__ __forceinline__ float mat_elem(const M3& m, int index) {
     const V3& c = index < 3 ? m.c0 : (index < 6 ? m.c1 : m.c2);
@@ -779,6 +869,8 @@ __global__ void k_joint_rows(BodyDev b, JointsDev jd, float inv_dt, float erp) {
         }
     } else if (kind == JK_SPRING2) {
         spring2_rows(out, b, jd, jid, d, ia, ib, pa, pb, qa, qb, pivot_a, pivot_b, inv_dt, erp);
+    } else if (kind == JK_GENERIC6DOF) {
+        generic6dof_rows(out, b, jd, jid, d, ia, ib, qa, qb, r_a, r_b, pivot_a, pivot_b, inv_dt);
     } else if (kind == JK_CONETWIST) {
         conetwist_rows(out, b, jd, jid, d, flags, qa, qb, r_a, r_b, pivot_a, pivot_b, inv_dt, erp);
     } else if (kind == JK_GEAR) {  // gear.rs:33-57: the spins about the frames' z columns, coupled

@@ -476,7 +476,7 @@ struct World {
     // (generic6dof_spring2.rs:846-1111): per axis 2 limit rows (lower < upper) or 1 lock row
     // (lower == upper), plus 1 for a motor or servo and 1 for a spring.
     uint32_t joint_row_capacity(uint32_t j) const {
-        if (joint_s2_h[j] < 0) return JOINT_MAX_ROWS;
+        if (joint_s2_h[j] < 0 || joints_h[j].kind == BGPU_JOINT_GENERIC6DOF) return JOINT_MAX_ROWS;
         uint32_t r = 0;
         for (const bgpu_spring2_axis& a : s2_h[size_t(joint_s2_h[j])].axis) {
             r += a.lower_limit < a.upper_limit ? 2u : (a.lower_limit == a.upper_limit ? 1u : 0u);
@@ -488,14 +488,14 @@ struct World {
 
     // Constraint::generic_6dof_spring2: validated, then added as joints of kind SPRING2 whose axis
     // tables live beside the descriptors.
-    uint32_t add_spring2_joints(uint32_t cnt, const bgpu_spring2_desc* d) {
+    uint32_t add_spring2_joints(uint32_t cnt, const bgpu_spring2_desc* d, uint32_t kind = BGPU_JOINT_SPRING2) {
         std::vector<bgpu_joint_desc> base(cnt);
         for (uint32_t k = 0; k < cnt; ++k) {
             if (d[k].rotate_order > BGPU_ROTATE_ZYX) throw InvalidArg{"unknown rotate order"};
             for (const bgpu_spring2_axis& a : d[k].axis)
                 if (std::isnan(a.lower_limit) || std::isnan(a.upper_limit)) throw InvalidArg{"NaN axis limit"};
             bgpu_joint_desc_default(&base[k]);
-            base[k].kind = BGPU_JOINT_SPRING2;
+            base[k].kind = kind;
             base[k].body_a = d[k].body_a;
             base[k].body_b = d[k].body_b;
             base[k].flags = d[k].flags & (BGPU_JOINT_DISABLE_COLLISIONS | BGPU_JOINT_DISABLED);
@@ -510,7 +510,7 @@ struct World {
     // kinematic bodies take no impulse), so a joint colour never holds a dynamic body twice.
     uint32_t add_joints(uint32_t cnt, const bgpu_joint_desc* d, const bgpu_spring2_desc* s2 = nullptr) {
         for (uint32_t k = 0; k < cnt; ++k) {
-            if (s2 ? d[k].kind != BGPU_JOINT_SPRING2
+            if (s2 ? (d[k].kind != BGPU_JOINT_SPRING2 && d[k].kind != BGPU_JOINT_GENERIC6DOF)
                    : (d[k].kind > BGPU_JOINT_CONETWIST || d[k].kind == BGPU_JOINT_SPRING2))
                 throw InvalidArg{"unknown joint kind (spring-2 joints go through bgpu_add_spring2_joints)"};
             if (d[k].body_a >= n || d[k].body_b >= n || d[k].body_a == d[k].body_b)
@@ -1738,6 +1738,52 @@ bgpu_status bgpu_add_spring2_joints(bgpu_world* w, uint32_t n, const bgpu_spring
         if (first_id) *first_id = f;
         return BGPU_OK;
     });
+}
+
+bgpu_status bgpu_add_generic6dof_joints(bgpu_world* w, uint32_t n, const bgpu_spring2_desc* d, uint32_t* first_id) {
+    if (!w || (n && !d)) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        uint32_t f = w->impl.add_spring2_joints(n, d, BGPU_JOINT_GENERIC6DOF);
+        if (first_id) *first_id = f;
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_generic6dof_universal(const float* pos_a, const float* quat_a, const float* pos_b, const float* quat_b,
+                                       const float* anchor, const float* axis1, const float* axis2, uint32_t body_a,
+                                       uint32_t body_b, bgpu_spring2_desc* out) {
+    if (!pos_a || !quat_a || !pos_b || !quat_b || !anchor || !axis1 || !axis2 || !out) return BGPU_ERR_INVALID_ARGUMENT;
+    using bgpu::V3;
+    using bgpu::M3;
+    const V3 pa{pos_a[0], pos_a[1], pos_a[2]}, pb{pos_b[0], pos_b[1], pos_b[2]}, an{anchor[0], anchor[1], anchor[2]};
+    const bgpu::Q qa{quat_a[0], quat_a[1], quat_a[2], quat_a[3]}, qb{quat_b[0], quat_b[1], quat_b[2], quat_b[3]};
+    // generic6dof.rs:168-176: axis1 is the frame z, axis2 the frame y, x = y x z
+    const V3 z_axis = bgpu::normalize(V3{axis1[0], axis1[1], axis1[2]});
+    const V3 y_axis = bgpu::normalize(V3{axis2[0], axis2[1], axis2[2]});
+    const V3 x_axis = bgpu::cross(y_axis, z_axis);
+    const M3 basis{x_axis, y_axis, z_axis};
+    const M3 rot_a = bgpu::from_quat(qa), rot_b = bgpu::from_quat(qb);
+    const M3 ba = bgpu::mul(bgpu::transpose(rot_a), basis), bb = bgpu::mul(bgpu::transpose(rot_b), basis);
+    const V3 oa = bgpu::mul(bgpu::transpose(rot_a), an - pa), ob = bgpu::mul(bgpu::transpose(rot_b), an - pb);
+    bgpu_spring2_desc_default(out);
+    out->body_a = body_a;
+    out->body_b = body_b;
+    auto put = [](float* f, const V3& o, const M3& m) {
+        const V3 c[4] = {o, m.c0, m.c1, m.c2};
+        for (int k = 0; k < 4; ++k) { f[3 * k] = c[k].x; f[3 * k + 1] = c[k].y; f[3 * k + 2] = c[k].z; }
+    };
+    put(out->frame_a, oa, ba);
+    put(out->frame_b, ob, bb);
+    // :181-188: linear locked; angular x locked, y within +-(pi/2 - 0.01), z within +-(pi - 0.01)
+    const float half_pi = 1.57079632679489661923f, pi = 3.14159265358979323846f;
+    const float lo[3] = {0.0f, -half_pi + 0.01f, -pi + 0.01f}, hi[3] = {0.0f, half_pi - 0.01f, pi - 0.01f};
+    for (int i = 0; i < 3; ++i) {
+        out->axis[i].lower_limit = 0.0f;
+        out->axis[i].upper_limit = 0.0f;
+        out->axis[3 + i].lower_limit = normalize_angle_host(lo[i]);
+        out->axis[3 + i].upper_limit = normalize_angle_host(hi[i]);
+    }
+    return BGPU_OK;
 }
 
 bgpu_status bgpu_read_joint_spring2_state(bgpu_world* w, float* state) {

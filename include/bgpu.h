@@ -140,7 +140,8 @@ typedef struct bgpu_step_stats {
  * a joint of a sleeping island (both bodies inactive) produces no rows. */
 enum { BGPU_JOINT_POINT2POINT = 0, BGPU_JOINT_FIXED = 1, BGPU_JOINT_HINGE = 2, BGPU_JOINT_GEAR = 3, BGPU_JOINT_SLIDER = 4,
        BGPU_JOINT_SPRING2 = 5 /* added through bgpu_add_spring2_joints only */,
-       BGPU_JOINT_CONETWIST = 6 /* ConeTwistConstraint, conetwist.rs: cone axis is the frames' x column */ };
+       BGPU_JOINT_CONETWIST = 6 /* ConeTwistConstraint, conetwist.rs: cone axis is the frames' x column */,
+       BGPU_JOINT_GENERIC6DOF = 7 /* added through bgpu_add_generic6dof_joints only */ };
 #define BGPU_JOINT_DISABLE_COLLISIONS 0x01u /* no contacts between the two bodies (default on) */
 #define BGPU_JOINT_DISABLED 0x02u           /* set_enabled(false): no rows, no island link */
 #define BGPU_JOINT_ANGULAR_ONLY 0x04u       /* hinge: skip the three pivot rows */
@@ -342,6 +343,21 @@ bgpu_status bgpu_set_ccd(bgpu_world* w, uint32_t first, uint32_t n, const float*
                          const float* swept_sphere_radius);
 /* Per body: the CCD clamp fraction of the last step (1 where no clamp happened). */
 bgpu_status bgpu_read_ccd_clamps(bgpu_world* w, float* clamps);
+/* Classic generic 6DOF joints (Constraint::generic_6dof, generic6dof.rs; Bullet's
+ * btGeneric6DofConstraint), described by the spring-2 record, of which they read per axis the
+ * limits (lower > upper free, else limited; angular ones normalised by the caller), the angular
+ * bounce, stop_erp (always, no global fallback), and with BGPU_S2_MOTOR the motor's
+ * target_velocity and max_motor_force; one limit-or-motor row per axis. Same id space as
+ * bgpu_add_joints. bgpu_read_joint_spring2_state gives their Euler angles and pivot offset (with
+ * fact_a 0.5 and has_static_body 0: this kind has no static-body split). */
+bgpu_status bgpu_add_generic6dof_joints(bgpu_world* w, uint32_t n, const bgpu_spring2_desc* d, uint32_t* first_id);
+/* Generic6DofConstraint::universal (generic6dof.rs:159-194, Bullet's btUniversalConstraint;
+ * PhysicsWorld::add_universal): pivots at the world anchor, axis1 the frame z and axis2 the frame y
+ * (orthogonal), linear and angular x locked, y within +-(pi/2 - 0.01), z within +-(pi - 0.01).
+ * Host arithmetic only; add the result with bgpu_add_generic6dof_joints. */
+bgpu_status bgpu_generic6dof_universal(const float* pos_a, const float* quat_a, const float* pos_b, const float* quat_b,
+                                       const float* anchor, const float* axis1, const float* axis2, uint32_t body_a,
+                                       uint32_t body_b, bgpu_spring2_desc* out);
 /* Spring-2 joints (Constraint::generic_6dof_spring2), in the same id space as bgpu_add_joints. */
 bgpu_status bgpu_add_spring2_joints(bgpu_world* w, uint32_t n, const bgpu_spring2_desc* d, uint32_t* first_id);
 uint32_t bgpu_num_joints(bgpu_world* w);

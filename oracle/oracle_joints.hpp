@@ -14,6 +14,8 @@
 //   crates/bullet-dynamics/src/constraint/slider.rs:159-475 (slider: frame-offset rows, linear and
 //     angular limits and motors), shared.rs:30-55 (adjust_angle_to_limits), :126-145
 //     (mirrored_row_limits);
+//   crates/bullet-dynamics/src/constraint/generic6dof.rs:159-546 (classic 6DOF: per-axis limit or
+//     motor rows, the universal frames);
 //   crates/bullet-dynamics/src/constraint/conetwist.rs:222-548 (cone twist: pivot rows, elliptical
 //     swing limit, fixed and hinge configurations, twist limit, motor target);
 //   crates/bullet-dynamics/src/constraint/generic6dof_spring2.rs:650-1383 (spring 2: per-axis
@@ -31,7 +33,7 @@
 namespace oracle {
 
 enum : uint32_t { JOINT_POINT2POINT = 0, JOINT_FIXED = 1, JOINT_HINGE = 2, JOINT_GEAR = 3, JOINT_SLIDER = 4, JOINT_SPRING2 = 5,
-                  JOINT_CONETWIST = 6 };
+                  JOINT_CONETWIST = 6, JOINT_GENERIC6DOF = 7 };
 // RowLimits (sequential_impulse.rs): which clamp the accumulated impulse takes.
 enum : uint32_t { LIM_UNBOUNDED = 0, LIM_BILATERAL = 1, LIM_LOWER = 2, LIM_UPPER = 3, LIM_WINDOW = 4 };
 
@@ -799,6 +801,105 @@ void prepare_spring2_rows(Joint<R>& jt, uint32_t ia, uint32_t ib, const B& a, co
     }
 }
 
+// generic6dof.rs:264-326, 328-546 (Generic6DofConstraint: test_linear_limit,
+// test_angular_limit_motor, prepare_rows, push_limit_motor_row). The per-axis parameters sit in
+// the spring-2 axis table: lower, upper, bounce (angular), stop_erp, target_velocity,
+// max_motor_force and S2_MOTOR; the per-step state in s2_diff / s2_euler.
+template <class R, class B>
+void prepare_generic6dof_rows(Joint<R>& jt, uint32_t ia, uint32_t ib, const B& a, const B& b, R inv_dt,
+                              std::vector<JointRow<R>>& out) {
+    const R pi = R(3.14159265358979323846);
+    const R inf = std::numeric_limits<R>::infinity();
+    M3<R> tr_a = M3<R>::from_quat(a.orientation) * jt.frame_a.basis;
+    M3<R> tr_b = M3<R>::from_quat(b.orientation) * jt.frame_b.basis;
+    V3<R> pivot_a = a.position + a.orientation.rotate(jt.frame_a.origin);
+    V3<R> pivot_b = b.position + b.orientation.rotate(jt.frame_b.origin);
+    V3<R> r_a = pivot_a - a.position, r_b = pivot_b - b.position;
+    V3<R> diff = tr_a.transpose() * (pivot_b - pivot_a);
+    jt.s2_diff = diff;
+    int lin_limit[3];
+    R lin_err[3];
+    for (int i = 0; i < 3; ++i) {
+        const Spring2Axis<R>& m = jt.s2[i];
+        const R v = diff[i];
+        if (m.lower > m.upper) { lin_limit[i] = 0; lin_err[i] = 0; }
+        else if (v < m.lower) { lin_limit[i] = 2; lin_err[i] = v - m.lower; }
+        else if (v > m.upper) { lin_limit[i] = 1; lin_err[i] = v - m.upper; }
+        else { lin_limit[i] = 0; lin_err[i] = 0; }
+    }
+    V3<R> euler, axes[3];
+    relative_rotation_info(tr_a, tr_b, euler, axes);
+    jt.s2_euler = euler;
+    auto push_row = [&](const V3<R>& ax1, bool linear, int limit, R limit_err, R lo, R hi, R stop_erp, bool powered,
+                        R target_velocity, R max_motor_force, R current_pos, R bounce, R row_vel) {
+        if (limit != 0 && lo == hi) powered = false;
+        R row_error = 0;
+        if (powered && limit == 0) {
+            R tag_vel = linear ? -target_velocity : target_velocity;
+            R mot_fact = motor_factor(current_pos, lo, hi, tag_vel, inv_dt * stop_erp);
+            row_error += mot_fact * target_velocity;
+        }
+        if (limit != 0) {
+            R k = inv_dt * stop_erp;
+            row_error += linear ? k * limit_err : -k * limit_err;
+            if (bounce > R(0)) {
+                if (limit == 1) {
+                    if (row_vel < R(0)) { R newc = -bounce * row_vel; if (newc > row_error) row_error = newc; }
+                } else if (row_vel > R(0)) {
+                    R newc = -bounce * row_vel;
+                    if (newc < row_error) row_error = newc;
+                }
+            }
+        }
+        R lower = 0, upper = 0;
+        if (powered && limit == 0) { lower = -max_motor_force / inv_dt; upper = max_motor_force / inv_dt; }
+        else if (limit != 0) {
+            if (lo == hi) { lower = -inf; upper = inf; }
+            else if (limit == 1) { lower = 0; upper = inf; }
+            else { lower = -inf; upper = 0; }
+        }
+        uint32_t lim;
+        R rlo, rhi;
+        mirrored_row_limits(lower, upper, lim, rlo, rhi);
+        const V3<R> zero;
+        if (linear)
+            out.push_back(prepare_joint_row(ia, ib, ax1, r_a.cross(ax1), ax1, r_b.cross(ax1), a, b, -row_error, lim, rlo, rhi));
+        else
+            out.push_back(prepare_joint_row(ia, ib, zero, ax1, zero, ax1, a, b, -row_error, lim, rlo, rhi));
+    };
+    for (int i = 0; i < 3; ++i) {
+        Spring2Axis<R>& m = jt.s2[3 + i];
+        const bool motor = (m.flags & S2_MOTOR) != 0;
+        const R angle = adjust_angle_to_limits(euler[i], m.lower, m.upper);
+        m.position = angle;
+        int limit = 0;
+        R err = m.error;
+        if (m.lower > m.upper) limit = 0;
+        else if (angle < m.lower || angle > m.upper) {
+            limit = angle < m.lower ? 1 : 2;
+            err = angle - (angle < m.lower ? m.lower : m.upper);
+            if (err > pi) err -= R(2) * pi;
+            else if (err < -pi) err += R(2) * pi;
+        }
+        m.error = err;
+        if (limit != 0 || motor) {
+            R row_vel = a.angular_velocity.dot(axes[i]) - b.angular_velocity.dot(axes[i]);
+            push_row(axes[i], false, limit, err, m.lower, m.upper, m.stop_erp, motor, m.target_velocity,
+                     m.max_motor_force, angle, m.bounce, row_vel);
+        }
+    }
+    for (int i = 0; i < 3; ++i) {
+        const Spring2Axis<R>& m = jt.s2[i];
+        const bool motor = (m.flags & S2_MOTOR) != 0;
+        if (lin_limit[i] != 0 || motor) {
+            V3<R> ax1 = tr_a.col(i);
+            R row_vel = a.linear_velocity.dot(ax1) - b.linear_velocity.dot(ax1);
+            push_row(ax1, true, lin_limit[i], lin_err[i], m.lower, m.upper, m.stop_erp, motor, m.target_velocity,
+                     m.max_motor_force, diff[i], R(0), row_vel);
+        }
+    }
+}
+
 // constraint.rs:755-842 + fixed.rs:33-90 + hinge.rs:130-267: the joint's rows for this step.
 template <class R, class B>
 void prepare_joint_rows(Joint<R>& jt, uint32_t jid, const std::vector<B>& bodies, R inv_dt, R erp,
@@ -825,6 +926,8 @@ void prepare_joint_rows(Joint<R>& jt, uint32_t jid, const std::vector<B>& bodies
         }
     } else if (jt.kind == JOINT_SPRING2) {
         prepare_spring2_rows(jt, ia, ib, a, b, inv_dt, erp, global_cfm, out);
+    } else if (jt.kind == JOINT_GENERIC6DOF) {
+        prepare_generic6dof_rows(jt, ia, ib, a, b, inv_dt, out);
     } else if (jt.kind == JOINT_CONETWIST) {
         prepare_conetwist_rows(jt, ia, ib, a, b, inv_dt, erp, out);
     } else if (jt.kind == JOINT_GEAR) {  // gear.rs:33-57

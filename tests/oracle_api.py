@@ -159,9 +159,10 @@ def joint_desc(kind, body_a, body_b, frame_a, frame_b, flags=JF_DISABLE_COLLISIO
 
 
 def spring2_joint_desc(joint):
-    """The oracle descriptor of a bgpu.Spring2 joint (same bodies, frames, order and axes)."""
+    """The oracle descriptor of a bgpu.Spring2 (kind 5) or bgpu.Generic6Dof (kind 7) joint: same
+    bodies, frames, order and axes."""
     d = joint.desc
-    return joint_desc(5, d.body_a, d.body_b, list(d.frame_a), list(d.frame_b), flags=d.flags,
+    return joint_desc(getattr(joint, "KIND", 5), d.body_a, d.body_b, list(d.frame_a), list(d.frame_b), flags=d.flags,
                       rotate_order=d.rotate_order, s2_axes=joint.axis_table())
 
 

@@ -612,3 +612,47 @@ def test_cone_twist_matches_the_oracle(gpu, case):  # constraint/tests.rs:518-60
         assert abs(st[-1, bob, 10]) < 0.1
     if case == "motor":
         assert abs(swing[-1] - 0.3) < 0.05
+
+
+@pytest.mark.parametrize("case", ["locked", "angular_limit", "motor", "linear_limit", "universal_free",
+                                  "universal_locked"])
+def test_generic_6dof_matches_the_oracle(gpu, case):  # constraint/tests.rs:773-930; generic6dof.rs:614-676
+    import bgpu
+    if case.startswith("universal"):
+        s = JScene((0.0, 0.0, 0.0))
+        sph = s.shape(orc.SPHERE, [0.3])
+        a = s.body(sph, (0, 0, 0), mass=0.0)
+        b = s.body(sph, (1, 0, 0), angvel=(0.0, 0.0, 5.0) if case == "universal_free" else (0.0, 5.0, 0.0))
+        s.spring2(bgpu.Generic6Dof.universal(a, b, (0, 0, 0), (0, 0, 0, 1), (1, 0, 0), (0, 0, 0, 1), (1, 0, 0),
+                                             (0, 0, 1), (1, 0, 0)))
+        _, _, st, _ = run_pair(s, gpu, 60)
+        if case == "universal_free":
+            assert st[-1, b, 12] > 4.0
+        else:
+            assert abs(st[-1, b, 11]) < 0.05
+        return
+    box_pos, frames, gravity, setup, linvel, angvel, steps = {
+        "locked": ((0, 1, 0), ((0, 0.5, 0), (0, 1.5, 0)), (0, -9.81, 0),
+                   lambda j: j.set_angular_limits((0, 0, 0), (0, 0, 0)), (2, 0, 0), (0, 0, 4), 300),
+        "angular_limit": ((0, 0, 0), ((0, 0, 0), (0, 0, 0)), (0, 0, 0),
+                          lambda j: j.set_angular_limits((-0.4, -1.0, -1.0), (0.4, 1.0, 1.0)), (0, 0, 0), (4, 0, 0), 300),
+        "motor": ((0, 0, 0), ((0, 0, 0), (0, 0, 0)), (0, 0, 0), lambda j: j.enable_motor(5, 1.0, 100.0), (0, 0, 0),
+                  (0, 0, 0), 180),
+        "linear_limit": ((0.2, 0, 0), ((0, 0, 0), (0, 0, 0)), (0, 0, 0),
+                         lambda j: j.set_linear_limits((-0.3, 0, 0), (0.3, 0, 0)), (4, 0, 0), (0, 0, 0), 180),
+    }[case]
+    s = JScene(gravity)
+    anchor = s.body(s.shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+    box = s.body(s.shape(orc.BOX, [0.3, 0.3, 0.3]), box_pos, linvel=linvel, angvel=angvel)
+    j = bgpu.Generic6Dof(box, anchor, orc.frame(frames[0]), orc.frame(frames[1]))
+    setup(j)
+    s.spring2(j)
+    angles = []
+    _, _, st, _ = run_pair(s, gpu, steps, each=lambda step, w: angles.append(w.spring2_state()[0].copy()))
+    angles = np.array(angles)
+    if case == "angular_limit":
+        assert 0.3 < np.abs(angles[:, 0]).max() < 0.5
+    if case == "motor":
+        assert abs(abs(angles[-1, 2]) - 3.0) < 1.0
+    if case == "linear_limit":
+        assert st[:, box, 0].max() < 0.34 and st[-1, box, 0] < 0.3

@@ -429,3 +429,92 @@ def test_cone_twist_motor_drives_to_the_target(precision):  # conetwist.rs:138-1
     for _ in range(300):
         w.step(DT)
     assert abs(axis_angle_between(w.state(), anchor, bob) - 0.3) < 0.05
+
+
+def g6dof_world(precision, box_pos, frames, gravity, setup, linvel=(0, 0, 0), angvel=(0, 0, 0)):
+    """constraint/tests.rs:770-930: a 0.3 m box tied to a static 0.2 m anchor by a classic 6DOF."""
+    import bgpu
+    w = world(precision, gravity)
+    anchor = w.add_body(w.add_shape(orc.BOX, [0.2, 0.2, 0.2]), (0, 0, 0), mass=0.0)
+    box = w.add_body(w.add_shape(orc.BOX, [0.3, 0.3, 0.3]), box_pos, linvel=linvel, angvel=angvel, mass=1.0)
+    j = bgpu.Generic6Dof(box, anchor, orc.frame(frames[0]), orc.frame(frames[1]))
+    setup(j)
+    w.add_joint(orc.spring2_joint_desc(j))
+    return w, box
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_generic_6dof_locked_is_rigid(precision):  # tests.rs:773-817
+    w, box = g6dof_world(precision, (0, 1, 0), ((0, 0.5, 0), (0, 1.5, 0)), (0, -9.81, 0),
+                         lambda j: j.set_angular_limits((0, 0, 0), (0, 0, 0)), linvel=(2, 0, 0), angvel=(0, 0, 4))
+    max_rel = 0.0
+    for _ in range(600):
+        w.step(DT)
+        max_rel = max(max_rel, quat_angle(w.state()[box, 3:7]))
+    assert max_rel < 0.5
+    assert np.linalg.norm(w.state()[box, 0:3] - (0, 1, 0)) < 0.03
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_generic_6dof_angular_limit_stops_the_spin(precision):  # tests.rs:820-855
+    w, box = g6dof_world(precision, (0, 0, 0), ((0, 0, 0), (0, 0, 0)), (0, 0, 0),
+                         lambda j: j.set_angular_limits((-0.4, -1.0, -1.0), (0.4, 1.0, 1.0)), angvel=(4, 0, 0))
+    max_angle = 0.0
+    for _ in range(300):
+        w.step(DT)
+        max_angle = max(max_angle, abs(w.spring2_state(1)[0, 0]))
+    assert 0.3 < max_angle < 0.5
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_generic_6dof_motor_rotates_an_axis(precision):  # tests.rs:858-890
+    w, box = g6dof_world(precision, (0, 0, 0), ((0, 0, 0), (0, 0, 0)), (0, 0, 0),
+                         lambda j: j.enable_motor(5, 1.0, 100.0))
+    for _ in range(180):
+        w.step(DT)
+    assert abs(abs(w.spring2_state(1)[0, 2]) - 3.0) < 1.0
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_generic_6dof_linear_limit_stops_the_slide(precision):  # tests.rs:893-930
+    w, box = g6dof_world(precision, (0.2, 0, 0), ((0, 0, 0), (0, 0, 0)), (0, 0, 0),
+                         lambda j: j.set_linear_limits((-0.3, 0, 0), (0.3, 0, 0)), linvel=(4, 0, 0))
+    max_x = 0.0
+    for _ in range(180):
+        w.step(DT)
+        max_x = max(max_x, w.state()[box, 0])
+    assert max_x < 0.34 and w.state()[box, 0] < 0.3
+
+
+def test_universal_frames_and_limits():  # generic6dof.rs:560-611
+    import bgpu
+    j = bgpu.Generic6Dof.universal(0, 1, (0, 0, 0), (0, 0, 0, 1), (0, 0, 0), (0, 0, 0, 1), (1.0, 2.0, 3.0), (0, 0, 1),
+                                   (1, 0, 0))
+    fa = np.array(j.desc.frame_a)
+    assert np.array_equal(fa[3:], [0.0, -1.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 1.0])
+    assert np.allclose(fa[:3], (1.0, 2.0, 3.0), atol=1e-6)
+    for i in range(3):
+        assert (j.axis(i).lower_limit, j.axis(i).upper_limit) == (0.0, 0.0)
+    assert (j.axis(3).lower_limit, j.axis(3).upper_limit) == (0.0, 0.0)
+    assert abs(j.axis(4).lower_limit - (-math.pi / 2 + 0.01)) < 1e-6 and abs(j.axis(4).upper_limit - (math.pi / 2 - 0.01)) < 1e-6
+    assert abs(j.axis(5).lower_limit - (-math.pi + 0.01)) < 1e-6 and abs(j.axis(5).upper_limit - (math.pi - 0.01)) < 1e-6
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+@pytest.mark.parametrize("spin, free", [((0.0, 0.0, 5.0), True), ((0.0, 5.0, 0.0), False)])
+def test_universal_bends_only_about_the_joint_axes(precision, spin, free):  # generic6dof.rs:614-676
+    import bgpu
+    w = world(precision, (0, 0, 0))
+    s = w.add_shape(orc.SPHERE, [0.3])
+    a = w.add_body(s, (0, 0, 0), mass=0.0)
+    b = w.add_body(s, (1, 0, 0), angvel=spin, mass=1.0)
+    j = bgpu.Generic6Dof.universal(a, b, (0, 0, 0), (0, 0, 0, 1), (1, 0, 0), (0, 0, 0, 1), (1, 0, 0), (0, 0, 1),
+                                   (1, 0, 0))
+    w.add_joint(orc.spring2_joint_desc(j))
+    for _ in range(60):
+        w.step(DT)
+    st = w.state()[b]
+    if free:
+        assert st[12] > 4.0
+    else:
+        assert abs(st[11]) < 0.05
