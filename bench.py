@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--batch-worlds", type=int, default=4096, help="batched-worlds leg: number of worlds (0: skip)")
     p.add_argument("--batch-steps", type=int, default=30)
     p.add_argument("--adjoint-worlds", type=int, default=1024, help="adjoint leg: number of worlds (0: skip)")
+    p.add_argument("--ccd-spheres", type=int, default=2048, help="CCD leg: fast CCD spheres (0: skip)")
     p.add_argument("--spring2-counts", default="150,15000",
                    help="joint leg: chain counts of the spring2_chains scene, comma separated (empty: skip)")
     return p.parse_args()
@@ -293,6 +294,24 @@ def bench_spring2(bgpu, scenes, count, frames=300, warmup=5):
     return out
 
 
+def bench_ccd(bgpu, scenes, n_ccd, steps=60, warmup=5):
+    """CCD leg: `n_ccd` fast CCD spheres and half as many boxes raining onto thin plates
+    (scenes.ccd_rain_world); device time of `steps` steps after `warmup`, and the clamps of the
+    last step."""
+    w, ids = scenes.ccd_rain_world(bgpu, n_ccd=n_ccd, n_boxes=n_ccd // 2)
+    dt = 1.0 / 60.0
+    w.step_timed(dt, warmup)
+    ms = w.step_timed(dt, steps)
+    clamped = int(np.count_nonzero(w.ccd_clamps()[ids] < 1.0))
+    n = int(w.num_bodies)
+    status = int(w.stats()["device_status"])
+    w.close()
+    return {"workload": f"ccd_rain_{n_ccd}: {n} bodies, {n_ccd} CCD spheres (60-400 m/s) and {n_ccd // 2} boxes "
+                        f"over 256 thin plates, 10 iterations, dt 1/60, {steps} steps",
+            "value": n * steps / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms / steps,
+            "ccd_bodies_clamped_last_step": clamped, "device_status": status}
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -415,6 +434,8 @@ def main():
             line["batched_worlds"] = bench_batched(bgpu, scenes, args.batch_worlds, args.batch_steps, args.warmup)
         if args.adjoint_worlds > 0:
             line["adjoint"] = bench_adjoint(bgpu, scenes, args.adjoint_worlds)
+        if args.ccd_spheres > 0:
+            line["ccd_rain"] = bench_ccd(bgpu, scenes, args.ccd_spheres)
         if args.spring2_counts:
             line["spring2_chains"] = [bench_spring2(bgpu, scenes, int(c)) for c in args.spring2_counts.split(",")]
         if world_size == 1 and not args.no_cpu_baseline:

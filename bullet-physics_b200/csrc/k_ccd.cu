@@ -215,7 +215,40 @@ __device__ __forceinline__ bool body_active(uint32_t act) {
     return act == ACT_ACTIVE || act == ACT_WANTS_DEACTIVATION || act == ACT_DISABLE_DEACTIVATION;
 }
 
-constexpr int CCD_THREADS = 128;
+// One warp per CCD body. Candidates that pass the filters and the proxy-box pretest are kept in
+// shared memory with a lower bound on their hit fraction; casts then run a warp-wide wave at a
+// time in that order, and stop once the next bound is not below the best hit. Two facts keep the
+// result equal to casting every candidate: the inflated target lies inside the ball of radius
+// bound + swept radius about its position, so a segment that misses that ball (by more than the
+// 1e-4 distance the cast accepts as touching, plus rounding) is a miss; and a hit's fraction is at
+// least where the segment enters that ball. Overflowing the candidate buffer falls back to casting
+// every candidate.
+constexpr int CCD_THREADS = 32;
+constexpr int CCD_CAP = 256;
+
+struct CcdCtx {
+    V3 from, dir;
+    float length, radius;
+};
+
+__device__ __forceinline__ float cast_one(const BodyDev& b, const Shape* __restrict__ shapes, const float4* __restrict__ hull,
+                                          const CcdCtx& c, uint32_t j) {
+    const Shape& sj = shapes[b.info[j].x];
+    float f;
+    bool hit;
+    if (sj.type == SHAPE_PLANE) {
+        hit = sweep_plane(c.from, c.dir, c.length, c.radius, sj, q4(b.quat[j]), f);
+    } else {
+        Inflated t{sj, from4(b.pos[j]), q4(b.quat[j]), c.radius, hull};
+        hit = sweep_convex(c.from, c.dir, c.length, t, f);
+    }
+    return hit ? f : 1.0f;
+}
+
+__device__ __forceinline__ float warp_min(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
 
 // step.rs:1068-1155: the clamp fraction of CCD list entry blockIdx.x (1 when not clamped).
 __global__ void __launch_bounds__(CCD_THREADS) k_ccd_sweep(BodyDev b, const Shape* __restrict__ shapes,
@@ -225,7 +258,10 @@ __global__ void __launch_bounds__(CCD_THREADS) k_ccd_sweep(BodyDev b, const Shap
                                                            const uint32_t* __restrict__ world_of,
                                                            const uint64_t* __restrict__ suppressed, uint32_t nsuppressed,
                                                            float dt, float* clamp) {
-    const uint32_t k = blockIdx.x;
+    __shared__ uint32_t cand[CCD_CAP], sorted[CCD_CAP];
+    __shared__ float lb[CCD_CAP], slb[CCD_CAP];
+    __shared__ uint32_t ncand;
+    const uint32_t k = blockIdx.x, lane = threadIdx.x;
     const uint32_t i = ids[k];
     const float threshold = par[k].x, radius = par[k].y;
     const uint4 info = b.info[i];
@@ -236,18 +272,28 @@ __global__ void __launch_bounds__(CCD_THREADS) k_ccd_sweep(BodyDev b, const Shap
                     si.type != SHAPE_PLANE;
     eligible = eligible && !(len2(to - from) <= threshold * threshold);
     if (!eligible) {
-        if (threadIdx.x == 0) clamp[k] = 1.0f;
+        if (lane == 0) clamp[k] = 1.0f;
         return;
     }
     const V3 smin = vmin(from, to) - V3{radius, radius, radius}, smax = vmax(from, to) + V3{radius, radius, radius};
     const V3 delta = to - from;
-    const float length = len(delta);
-    const V3 dir = delta / length;
+    CcdCtx c;
+    c.length = len(delta);
+    c.dir = delta / c.length;
+    c.from = from;
+    c.radius = radius;
+    // convex_sweep.rs:45-50: a vanishing motion casts nothing
+    if (c.length <= 1.1920929e-7f) {
+        if (lane == 0) clamp[k] = 1.0f;
+        return;
+    }
     const uint32_t gi = info.w & 0xFFFFu, mi = info.w >> 16;
     uint32_t lo = 0, hi = n;
     if (world_of) { lo = world_off[world_of[i]]; hi = world_off[world_of[i] + 1]; }
+    if (lane == 0) ncand = 0;
+    __syncthreads();
     float best = 1.0f;
-    for (uint32_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+    for (uint32_t j = lo + lane; j < hi; j += CCD_THREADS) {
         if (j == i) continue;
         const uint4 oj = b.info[j];
         if (oj.y & BF_NO_RESPONSE) continue;
@@ -262,29 +308,71 @@ __global__ void __launch_bounds__(CCD_THREADS) k_ccd_sweep(BodyDev b, const Shap
             const uint64_t key = (uint64_t(min(i, j)) << 32) | max(i, j);
             if (key_suppressed(suppressed, nsuppressed, key)) continue;
         }
-        // convex_sweep.rs:45-50: no cast for a vanishing motion
-        if (length <= 1.1920929e-7f) continue;
         const Shape& sj = shapes[oj.x];
-        float f;
-        bool hit;
-        if (sj.type == SHAPE_PLANE) {
-            hit = sweep_plane(from, dir, length, radius, sj, q4(b.quat[j]), f);
-        } else {
-            Inflated t{sj, from4(b.pos[j]), q4(b.quat[j]), radius, hull};
-            hit = sweep_convex(from, dir, length, t, f);
+        if (sj.type == SHAPE_PLANE) {  // analytic and cheap: cast now
+            best = fminf(best, cast_one(b, shapes, hull, c, j));
+            continue;
         }
-        if (hit && f < best) best = f;
+        // bounding ball of the inflated target, widened by the touch distance and rounding
+        const V3 cj = from4(b.pos[j]);
+        const float bound = len(vmax(vabs(V3{sj.lmin[0], sj.lmin[1], sj.lmin[2]}), vabs(V3{sj.lmax[0], sj.lmax[1], sj.lmax[2]})));
+        const float slack = 1e-3f + 1e-5f * (len(cj) + len(from) + c.length);
+        const float rr = bound + radius + slack;
+        const V3 m = from - cj;
+        const float bb = dot(m, c.dir);
+        const float tca = fminf(fmaxf(-bb, 0.0f), c.length);
+        if (len2(m + c.dir * tca) > rr * rr) continue;  // the segment misses the ball: no hit
+        const float cc = len2(m) - rr * rr;
+        float lower = 0.0f;
+        if (cc > 0.0f) {
+            const float disc = fmaxf(bb * bb - cc, 0.0f);
+            lower = fmaxf((-bb - sqrtf(disc)) / c.length - 1e-6f - slack / c.length, 0.0f);
+        }
+        const uint32_t slot = atomicAdd(&ncand, 1u);
+        if (slot < CCD_CAP) {
+            cand[slot] = j;
+            lb[slot] = lower;
+        }
     }
-    // block minimum
-    for (int o = 16; o > 0; o >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, o));
-    __shared__ float wmin[CCD_THREADS / 32];
-    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = best;
+    best = warp_min(best);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        float m = wmin[0];
-        for (int w = 1; w < CCD_THREADS / 32; ++w) m = fminf(m, wmin[w]);
-        clamp[k] = m;
+    const uint32_t nc = ncand;
+    if (nc > CCD_CAP) {
+        // too many candidates for the buffer: cast every candidate that passes the same tests
+        float mine = best;
+        for (uint32_t j = lo + lane; j < hi; j += CCD_THREADS) {
+            if (j == i) continue;
+            const uint4 oj = b.info[j];
+            if ((oj.y & BF_NO_RESPONSE) || shapes[oj.x].type == SHAPE_PLANE) continue;
+            const uint32_t gj = oj.w & 0xFFFFu, mj = oj.w >> 16;
+            if ((gi & mj) == 0 || (gj & mi) == 0) continue;
+            const float4 amin = b.aabb_min[j], amax = b.aabb_max[j];
+            if (!(amin.x <= smax.x && amin.y <= smax.y && amin.z <= smax.z && smin.x <= amax.x && smin.y <= amax.y &&
+                  smin.z <= amax.z))
+                continue;
+            if (nsuppressed && key_suppressed(suppressed, nsuppressed, (uint64_t(min(i, j)) << 32) | max(i, j))) continue;
+            mine = fminf(mine, cast_one(b, shapes, hull, c, j));
+        }
+        best = warp_min(mine);
+    } else {
+        // order the candidates by their lower bound (rank by counting; ties by slot)
+        for (uint32_t s = lane; s < nc; s += CCD_THREADS) {
+            uint32_t r = 0;
+            const float v = lb[s];
+            for (uint32_t t = 0; t < nc; ++t) r += (lb[t] < v || (lb[t] == v && t < s)) ? 1u : 0u;
+            sorted[r] = cand[s];
+            slb[r] = v;
+        }
+        __syncthreads();
+        for (uint32_t w0 = 0; w0 < nc; w0 += CCD_THREADS) {
+            if (!(slb[w0] < best)) break;  // every later candidate hits no sooner than best
+            const uint32_t s = w0 + lane;
+            float f = 1.0f;
+            if (s < nc && slb[s] < best) f = cast_one(b, shapes, hull, c, sorted[s]);
+            best = fminf(best, warp_min(f));
+        }
     }
+    if (lane == 0) clamp[k] = best;
 }
 
 // step.rs:1210-1214, after the position integration (which leaves the velocities unchanged).

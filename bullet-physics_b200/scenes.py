@@ -454,3 +454,38 @@ def spring2_chains_world(bgpu, count=150, cols=15, links=3, spacing=4.0, base_he
             t += 1
     bgpu.check(w.L.bgpu_add_spring2_joints(w.h, t, descs, bgpu.ctypes.byref(first)), "add_spring2_joints")
     return w
+
+
+def ccd_rain_world(bgpu, n_ccd=2048, n_boxes=1024, plates=16, seed=7, iterations=10):
+    """Fast CCD spheres (r 0.2, falling at 60-400 m/s, motion threshold 0.05, swept radius 0.2)
+    and plain boxes raining onto a `plates` x `plates` grid of thin static plates (0.1 m thick) over
+    a ground plane: each step sweeps every CCD sphere against the bodies of the world, as the
+    reference's CCD stage does (world/step.rs:1068-1155). Returns (world, CCD body ids)."""
+    rng = np.random.default_rng(seed)
+    w = bgpu.World(gravity=(0.0, -9.81, 0.0), num_iterations=iterations)
+    w.add_body(w.add_shape(bgpu.PLANE, [0.0, 1.0, 0.0, 0.0]), (0.0, 0.0, 0.0), mass=0.0)
+    plate = w.add_shape(bgpu.BOX, [1.5, 0.05, 1.5])
+    ext = plates * 3.2 / 2.0
+    for px in range(plates):
+        for pz in range(plates):
+            w.add_body(plate, (px * 3.2 - ext + 1.6, 2.0 + 0.3 * ((px + pz) % 3), pz * 3.2 - ext + 1.6), mass=0.0)
+    sph = w.add_shape(bgpu.SPHERE, [0.2])
+    box = w.add_shape(bgpu.BOX, [0.2, 0.2, 0.2])
+    n = n_ccd + n_boxes
+    kind = np.zeros(n, dtype=bool)
+    kind[rng.permutation(n)[:n_ccd]] = True
+    pos = np.stack([rng.uniform(-ext, ext, n), rng.uniform(4.0, 12.0, n), rng.uniform(-ext, ext, n)], axis=1)
+    vel = np.zeros((n, 3))
+    vel[:, 0] = np.where(kind, rng.uniform(-5.0, 5.0, n), 0.0)
+    vel[:, 1] = np.where(kind, rng.uniform(-400.0, -60.0, n), -5.0)
+    quat = np.tile(np.array([0.0, 0.0, 0.0, 1.0]), (n, 1))
+    d = bgpu.desc_array(np.where(kind, sph, box), pos, quat, linvel=vel, mass=np.ones(n))
+    first = bgpu.ctypes.c_uint32()
+    bgpu.check(w.L.bgpu_add_bodies(w.h, n, d.ctypes.data_as(bgpu.ctypes.POINTER(bgpu.BodyDesc)),
+                                   bgpu.ctypes.byref(first)), "add_bodies")
+    ids = first.value + np.flatnonzero(kind)
+    thr = np.zeros(n, dtype=np.float32)
+    rad = np.zeros(n, dtype=np.float32)
+    thr[kind], rad[kind] = 0.05, 0.2
+    w.set_ccd(first.value, thr, rad)
+    return w, ids
