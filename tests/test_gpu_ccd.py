@@ -193,3 +193,24 @@ def test_ccd_rain_of_fast_spheres_matches_the_oracle(gpu):
         t.step(tol=1e-3)
         clamped += int(np.count_nonzero(t.g.ccd_clamps() < 1.0))
     assert clamped > 50
+
+
+def test_ccd_in_batched_worlds_sweeps_only_its_own_world(gpu):
+    """Batched worlds: a CCD ball sweeps only the bodies of its own world. Two worlds hold a ball
+    at the same coordinates falling at 120 m/s; only world 0 has a wall under it (world 1's wall is
+    50 m aside), so world 0's ball is clamped on its wall and world 1's ball passes through the
+    place where world 0's wall is."""
+    w = gpu.World(gravity=(0.0, 0.0, 0.0), batch=True)
+    wall = w.add_shape(orc.BOX, [1.0, 0.1, 1.0])
+    ball = w.add_shape(orc.SPHERE, [0.3])
+    shape = np.array([wall, ball, wall, ball], dtype=np.uint32)
+    pos = np.array([[0.0, 0.5, 0.0], [0.0, 1.0, 0.0], [50.0, 0.5, 0.0], [0.0, 1.0, 0.0]])
+    quat = np.tile([0.0, 0.0, 0.0, 1.0], (4, 1))
+    vel = np.array([[0.0, 0.0, 0.0], [0.0, -120.0, 0.0], [0.0, 0.0, 0.0], [0.0, -120.0, 0.0]])
+    w.add_worlds_array([2, 2], shape, pos, quat, linvel=vel, mass=np.array([0.0, 1.0, 0.0, 1.0]))
+    w.set_ccd(0, np.array([0.0, 0.1, 0.0, 0.1]), np.array([0.0, 0.3, 0.0, 0.3]))
+    w.step(DT)
+    st, clamps = w.state(), w.ccd_clamps()
+    assert abs(st[1, 1] - 0.9) <= 0.05 and clamps[1] < 1.0
+    assert st[3, 1] < -0.5 and clamps[3] == 1.0
+    assert w.stats()["device_status"] == 0
