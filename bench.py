@@ -3,9 +3,10 @@
 
 Workload (config 3 of the benchmark set): 65,536 unit boxes (half 0.5) and
 65,536 spheres (r 0.5) on a jittered 64x64x32 grid with 1.05 m spacing over a
-ground plane; f32; dt 1/60; 20 PGS iterations. The pile first settles for
---preroll steps (untimed, 4 s simulated by default) so the timed steps run on
-a dense contact state; then --warmup untimed steps, then --steps timed steps.
+ground plane; f32; dt 1/60; 20 PGS iterations; 600 steps. The pile first
+settles for --preroll untimed steps, then --warmup untimed steps, then --steps
+timed steps; by default the preroll is 600 - warmup - steps, so the timed
+window is the last steps of the configuration's 600 (the settled pile).
 
 Arms:
   default            the sm_100a library through its C ABI; `value` is device
@@ -42,7 +43,8 @@ def parse():
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=60)
     p.add_argument("--warmup", type=int, default=5)
-    p.add_argument("--preroll", type=int, default=240)
+    p.add_argument("--preroll", type=int, default=None,
+                   help="untimed settle steps (default: 600 - warmup - steps, so the window ends at step 600)")
     p.add_argument("--impl", default="bgpu", choices=["bgpu", "reference"])
     p.add_argument("--grid", default="64,64,32", help="pile grid nx,nz,ny (default: the full 131,072-body pile)")
     p.add_argument("--cpu-sample-grid", default="16,16,32")
@@ -53,7 +55,13 @@ def parse():
     p.add_argument("--ccd-spheres", type=int, default=2048, help="CCD leg: fast CCD spheres (0: skip)")
     p.add_argument("--spring2-counts", default="150,15000",
                    help="joint leg: chain counts of the spring2_chains scene, comma separated (empty: skip)")
-    return p.parse_args()
+    p.add_argument("--stack-steps", type=int, default=300, help="1,000-box stack leg: steps (0: skip)")
+    p.add_argument("--mixed-steps", type=int, default=300, help="16,384-body mixed convex leg: steps (0: skip)")
+    p.add_argument("--drift-steps", type=int, default=300, help="f64 drift report: steps (0: skip)")
+    a = p.parse_args()
+    if a.preroll is None:
+        a.preroll = max(0, 600 - a.warmup - a.steps)
+    return a
 
 
 class ClockSampler:
@@ -124,8 +132,9 @@ def cpu_baseline(grid, preroll, steps):
     dt = time.perf_counter() - t0
     n = sc.num_dynamic
     return {"value": n * steps / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"large-pile recipe {nx}x{nz}x{ny} ({n} bodies), {preroll}-step settle, {steps} timed steps, "
-                      f"single thread, {dt:.2f} s"}
+            "sample": f"large-pile recipe {nx}x{nz}x{ny} ({n} bodies), {preroll} untimed steps, then steps "
+                      f"{preroll + 1}-{preroll + steps} timed, single thread, {dt:.2f} s",
+            "contacts_per_body": len(w.rows()) / n}
 
 
 def algorithmic_pgs_bytes(st, iters):
@@ -261,9 +270,13 @@ def bench_adjoint(bgpu, scenes, n_worlds, steps=120, every=20):
     tape.close()
     w.close()
     n_dyn = sc.num_dynamic
+    grad_ms = fwd_ms + bwd_ms
     return {"workload": f"adjoint_worlds_{n_worlds} (config 5): {n_dyn} boxes, {steps} steps, dt 1/120, "
                         f"10 iterations, checkpoint every {every} steps",
-            "value": steps / (bwd_ms / 1000.0), "unit": "adjoint steps/s",
+            "value": steps / (grad_ms / 1000.0), "unit": "adjoint steps/s",
+            "value_basis": "rollout steps / (taped forward + backward) device time",
+            "adjoint_over_forward": grad_ms / plain_ms if plain_ms > 0 else None,
+            "adjoint_over_forward_target": 3.0,
             "plain_forward_ms": plain_ms, "taped_forward_ms": fwd_ms, "backward_ms": bwd_ms,
             "backward_first_call_ms": cold_bwd_ms,
             "backward_over_plain_forward": bwd_ms / plain_ms if plain_ms > 0 else None,
@@ -312,6 +325,62 @@ def bench_ccd(bgpu, scenes, n_ccd, steps=60, warmup=5):
             "ccd_bodies_clamped_last_step": clamped, "device_status": status}
 
 
+def bench_scene(bgpu, sc, name, steps, warmup=5):
+    """Device time of `steps` steps of a plain-world scene from its initial state (the
+    configuration's own step window), with the per-stage split of the step."""
+    w = sc.build_gpu(bgpu)
+    w.step_timed(sc.dt, 1)  # sizes the world's buffers; the window below starts at step 2
+    w.enable_timing(True)
+    ms = w.step_timed(sc.dt, steps)
+    st = w.stats()
+    w.enable_timing(False)
+    w.close()
+    n = sc.num_dynamic
+    return {"workload": name, "value": n * steps / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms / steps,
+            "steps": steps, "last_step": {"pairs": st["num_pairs"], "contacts": st["num_contacts"],
+                                          "narrow_phase_detections": st["num_detect"], "colours": st["num_colours"]},
+            "stage_ms_per_step": [x / max(st["timed_steps"], 1) for x in st["stage_ms"]],
+            "device_status": st["device_status"]}
+
+
+def bench_stack(bgpu, scenes, steps):
+    """Config 1: the 1,000-box stack, steps 2..steps+1 of the recipe. The reference publishes
+    its own single-thread CPU frame time for its closest scene (stack_1000: 1,000 boxes on a box
+    ground, 10 iterations, 600 frames)."""
+    sc = scenes.falling_box_stack(10, 10, 10, seed=1, steps=steps)
+    out = bench_scene(bgpu, sc, f"falling_box_stack_1000 (config 1): 10x10x10 boxes, 10 iterations, dt 1/60, "
+                                f"{steps} steps", steps)
+    out["reference_published_ms_per_frame"] = {"rust": 1.211, "bullet": 1.208, "scene": "stack_1000",
+                                               "source": "docs/perf/speed.md stack_1000 per-frame median, f32, "
+                                                         "their CPU, 1 thread"}
+    return out
+
+
+def bench_mixed(bgpu, scenes, steps):
+    """Config 2: 16,384 mixed convex bodies (boxes, spheres, capsules, 24-point hulls; the
+    GJK/EPA path) dropped in a 40 m cube, steps 2..steps+1 of the recipe."""
+    sc = scenes.mixed_convex_pile(n=16384, seed=2, steps=steps)
+    return bench_scene(bgpu, sc, f"mixed_convex_pile_16384 (config 2): 40% boxes, 30% spheres, 15% capsules, "
+                                 f"15% hulls, 10 iterations, dt 1/60, {steps} steps", steps)
+
+
+def drift_report(bgpu, scenes, steps):
+    """Drift of the f32 device trajectory against the oracle's f64 build (the reference's
+    `--features f64` restated), on the 1,000-box stack and a 1,024-body slice of the mixed
+    convex recipe; the oracle runs as the checker, the device step is what is measured."""
+    import drift_f64
+    import oracle_api
+
+    out = {"tolerance": {"pos_m": drift_f64.LEDGER_TOL_POS, "ang_rad": drift_f64.LEDGER_TOL_ANG,
+                         "source": "docs/parity-harness.md Tolerance; tools/compare.py quat_angle"},
+           "solve_order": "the f64 oracle is fed the device's colour order every step"}
+    for key, sc in (("stack_1000", scenes.falling_box_stack(10, 10, 10, seed=1, steps=steps)),
+                    ("mixed_convex_1024", scenes.mixed_convex_pile(n=1024, seed=2, steps=steps, extent=13.0))):
+        d = drift_f64.drift_run(bgpu, oracle_api, sc, steps)
+        out[key] = drift_f64.summary(sc.name, sc, d)
+    return out
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -337,11 +406,14 @@ def main():
         dist = tdist
     if args.impl == "reference":
         if rank == 0:
-            base = cpu_baseline(grid_of(args.cpu_sample_grid), min(args.preroll, 240), max(1, min(args.steps, 30)))
+            base = cpu_baseline(grid_of(args.cpu_sample_grid), args.preroll + args.warmup, args.steps)
             line = {"metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
                     "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
                     "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
                     "config": {"workload": "large_pile_131072 (config 3): CPU sample of the same recipe",
+                               "sample_grid": args.cpu_sample_grid, "sample_bodies": int(np.prod(grid_of(args.cpu_sample_grid))),
+                               "timed_window": f"steps {args.preroll + args.warmup + 1}-"
+                                               f"{args.preroll + args.warmup + args.steps} of 600",
                                "iterations": 20, "dt": 1 / 60},
                     "cpu_baseline": base,
                     "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -372,6 +444,9 @@ def main():
         ms = w.step_timed(sc.dt, args.steps)
     st = w.stats()
     w.enable_timing(False)
+    act = w.state()[:, 13]
+    dyn = np.asarray(sc.mass) > 0
+    awake_fraction = float(np.count_nonzero(act[dyn] != 2)) / max(n_dyn, 1)  # 2 = island sleeping
     region_ms = max_over_ranks(dist, ms)
     if dist:
         dist.barrier()
@@ -412,6 +487,9 @@ def main():
             "config": {"workload": f"large_pile_{n_dyn} (config 3): {nx}x{nz}x{ny} grid, 50% unit boxes / 50% r0.5 "
                                    f"spheres, 1.05 m spacing, ground plane",
                        "iterations": sc.iterations, "dt": sc.dt, "preroll_steps": args.preroll,
+                       "timed_window": f"steps {args.preroll + args.warmup + 1}-{args.preroll + args.warmup + args.steps}"
+                                       f" of the recipe's 600",
+                       "awake_fraction": awake_fraction, "contacts_per_body": st["num_contacts"] / max(n_dyn, 1),
                        "parallelism": f"replicas x{world_size}",
                        "l2": "inputs larger than L2 (rows + manifolds + bodies > 126 MB)",
                        "pairs": st["num_pairs"], "contacts": st["num_contacts"],
@@ -423,6 +501,8 @@ def main():
                          "traffic_source": traffic_src, "peak_kind": peak_kind,
                          "kernel_ms_per_launch": solve_ms, "algorithmic_bytes_per_launch": alg,
                          "split_contacts": st["num_split_contacts"]},
+            "contacts_per_s": st["num_contacts"] * args.steps / (region_ms / 1000.0) * world_size,
+            "contacts_per_s_note": "contacts of the last timed step x timed steps / device time",
             "clocks": clocks.summary(),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(forces.nbytes),
                     "d2h_bytes_per_step": int(poses.nbytes)},
@@ -438,8 +518,15 @@ def main():
             line["ccd_rain"] = bench_ccd(bgpu, scenes, args.ccd_spheres)
         if args.spring2_counts:
             line["spring2_chains"] = [bench_spring2(bgpu, scenes, int(c)) for c in args.spring2_counts.split(",")]
+        if args.stack_steps > 0:
+            line["stack_1000"] = bench_stack(bgpu, scenes, args.stack_steps)
+        if args.mixed_steps > 0:
+            line["mixed_convex_16384"] = bench_mixed(bgpu, scenes, args.mixed_steps)
         if world_size == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(grid_of(args.cpu_sample_grid), min(args.preroll, 240), 30)
+            # CPU leg: the oracle timed on the host (the baseline) and run as the f64 checker.
+            line["cpu_baseline"] = cpu_baseline(grid_of(args.cpu_sample_grid), args.preroll + args.warmup, args.steps)
+            if args.drift_steps > 0:
+                line["drift_f64"] = drift_report(bgpu, scenes, args.drift_steps)
         print(json.dumps(line), flush=True)
     w.close()
     if dist:

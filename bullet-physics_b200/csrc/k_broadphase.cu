@@ -535,6 +535,13 @@ namespace bgpu {
 namespace {
 
 constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(24) << 20;
+// Bytes per proxy of the arrays taken below (AABBs 32, sort keys 16, flags / scans / counts /
+// offsets / tree links 36, parents 8, node boxes 64, node records 64, node index bounds 8),
+// plus 256 B of alignment per array and room for CUB's sort / scan scratch (a few hundred KB
+// at 65,536 keys; 4 MiB allowed). Each take() is also checked when the call runs.
+constexpr size_t NOALLOC_PER_PROXY_BYTES = 228;
+static_assert(NOALLOC_PER_PROXY_BYTES * BGPU_NOALLOC_MAX_PROXIES + 32 * 256 + (size_t(4) << 20) <= NOALLOC_SCRATCH_BYTES,
+              "the allocation-free broad phase's scratch array is too small for its proxy limit");
 static __device__ __align__(256) unsigned char g_bp_scratch[NOALLOC_SCRATCH_BYTES];
 
 std::mutex g_bp_scratch_mutex;
@@ -640,6 +647,13 @@ extern "C" bgpu_status bgpu_broadphase_pairs_noalloc(const float* aabbs_dev, uin
         uint32_t* node_maxid = sb.take<uint32_t>(2 * size_t(n));
         int* bounds = sb.take<int>(8);
         uint32_t* scalars = sb.take<uint32_t>(8);
+        const void* taken[] = {mn, mx, keys, keys_alt, is_unb, leaf_body, parent, left, right, refit_flag, counts,
+                               offsets, flags, scan, unb_list, node_min, node_max, node_rec, node_maxid, bounds, scalars};
+        for (const void* t : taken)
+            if (!t) {
+                set_last_error("allocation-free broad phase: scratch array too small");
+                return BGPU_ERR_CAPACITY;
+            }
         size_t sort_bytes = 0, scan_bytes = 0;
         uint32_t* codes = reinterpret_cast<uint32_t*>(keys);
         uint32_t* codes_alt = reinterpret_cast<uint32_t*>(keys_alt);
@@ -702,6 +716,10 @@ extern "C" bgpu_status bgpu_broadphase_pairs_noalloc(const float* aabbs_dev, uin
         uint32_t host_scalars[2] = {0, 0};
         check_cuda(cudaMemcpyAsync(host_scalars, scalars, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "d2h");
         check_cuda(cudaStreamSynchronize(s), "sync");
+        if (host_scalars[1]) {  // the count walk overflowed its stack: the total is not a pair count
+            set_last_error("allocation-free broad phase: traversal stack overflow");
+            return BGPU_ERR_DEVICE_STATUS;
+        }
         uint64_t total = host_scalars[0];
         if (out_n) *out_n = total;
         if (total > cap) {

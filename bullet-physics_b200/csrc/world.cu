@@ -865,7 +865,7 @@ static float4* body_array(World& W, int k) {
 }
 
 static void save_snapshot(World& W, Snapshot& S) {
-    check_cuda(cudaStreamSynchronize(W.stream), "sync");
+    check_cuda(cudaStreamSynchronize(W.stream), "sync");  // the cache's entry count is read on the host
     S.n = W.n;
     S.cur = W.cur;
     S.step_count = W.step_count;
@@ -887,7 +887,7 @@ static void save_snapshot(World& W, Snapshot& S) {
     d2d(S.entries.p, c.entries.p, size_t(S.count) * ENTRY_F4 * sizeof(float4));
     S.sim.reserve(S.nsim);
     d2d(S.sim.p, W.world_sim.p, S.nsim * sizeof(uint32_t));
-    check_cuda(cudaStreamSynchronize(W.stream), "sync");
+    // No wait here: the copies are ordered before the next step on the same stream.
 }
 
 static void restore_snapshot(World& W, const Snapshot& S) {
@@ -921,7 +921,8 @@ struct Tape {
     uint32_t every;
     float dt = 0.0f;
     uint32_t nsteps = 0;
-    std::vector<std::unique_ptr<Snapshot>> cps;
+    std::vector<std::unique_ptr<Snapshot>> cps;  // checkpoints; the first ncps belong to the last forward pass
+    uint32_t ncps = 0;
     Snapshot final_state;
     std::vector<std::unique_ptr<StepRecord>> recs;
     DevBuf<float4> xbar, vbar, wbar, lbar;
@@ -942,13 +943,13 @@ struct Tape {
         W->finish_stats();
         dt = step_dt;
         nsteps = steps;
-        cps.clear();
+        // The checkpoints of an earlier pass are reused: their device buffers only grow, so a
+        // repeated forward pass allocates (and frees) nothing.
+        ncps = (steps + every - 1) / every;
+        while (cps.size() < ncps) cps.emplace_back(new Snapshot);
         check_cuda(cudaEventRecord(ev[0], W->stream), "event");
         for (uint32_t s = 0; s < steps; ++s) {
-            if (s % every == 0) {
-                cps.emplace_back(new Snapshot);
-                save_snapshot(*W, *cps.back());
-            }
+            if (s % every == 0) save_snapshot(*W, *cps[s / every]);
             W->step_once(dt);
         }
         save_snapshot(*W, final_state);
@@ -959,13 +960,13 @@ struct Tape {
 
     // Back to the state at the start of the last forward pass (its first checkpoint).
     void rewind() {
-        if (cps.empty()) throw InvalidArg{"the tape has no forward pass"};
+        if (!ncps) throw InvalidArg{"the tape has no forward pass"};
         restore_snapshot(*W, *cps[0]);
     }
 
     // grad_state: n x 9 floats (dL/dx, dL/dv, dL/dw of the final state). Outputs may be null.
     void backward(const float* grad_state, float* gv0, float* gw0, float* gmu, float* ge) {
-        if (cps.empty()) throw InvalidArg{"the tape has no forward pass"};
+        if (!ncps) throw InvalidArg{"the tape has no forward pass"};
         const uint32_t n = W->n;
         cudaStream_t s = W->stream;
         std::vector<float4> hx(n), hv(n), hw(n);
@@ -989,7 +990,7 @@ struct Tape {
         while (recs.size() < every) recs.emplace_back(new StepRecord);
         const float* carry_in = nullptr;
         int o = 0;
-        for (size_t seg = cps.size(); seg-- > 0;) {
+        for (size_t seg = ncps; seg-- > 0;) {
             const uint32_t s0 = uint32_t(seg) * every, s1 = std::min(s0 + every, nsteps);
             restore_snapshot(*W, *cps[seg]);
             for (uint32_t st = s0; st < s1; ++st) {
@@ -1100,6 +1101,15 @@ bgpu_status bgpu_selftest_wait_timeout(uint32_t limit_ms, uint32_t* device_statu
         words.reserve(2);
         cudaStream_t s = nullptr;
         cudaEvent_t e0 = nullptr, e1 = nullptr;
+        struct Release {  // the stream and events go on every exit, a failed CUDA call included
+            cudaStream_t& s;
+            cudaEvent_t &e0, &e1;
+            ~Release() {
+                if (e0) cudaEventDestroy(e0);
+                if (e1) cudaEventDestroy(e1);
+                if (s) cudaStreamDestroy(s);
+            }
+        } release{s, e0, e1};
         bgpu::check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
         bgpu::check_cuda(cudaEventCreate(&e0), "event");
         bgpu::check_cuda(cudaEventCreate(&e1), "event");
@@ -1113,9 +1123,6 @@ bgpu_status bgpu_selftest_wait_timeout(uint32_t limit_ms, uint32_t* device_statu
         bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
         float ms = 0.0f;
         bgpu::check_cuda(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        cudaStreamDestroy(s);
         if (device_status) *device_status = st;
         if (waited_ms) *waited_ms = ms;
         return BGPU_OK;

@@ -421,8 +421,9 @@ bgpu_status bgpu_read_push(bgpu_world* w, float* push);
  * The first call on a device looks up the array's device address: make it
  * before any stream capture. Every call shares the array, so calls that overlap
  * on the GPU race and must be serialised by the caller. stream is a
- * cudaStream_t (NULL = the default stream); the call returns after its work on
- * that stream has finished. */
+ * cudaStream_t (NULL = the default stream). Every call, not only the first,
+ * copies the pair count to host memory and synchronises that stream before it
+ * sizes the output, and it returns after its work on the stream has finished. */
 #define BGPU_NOALLOC_MAX_PROXIES 65536u
 #define BGPU_NOALLOC_MAX_UNBOUNDED 16u
 bgpu_status bgpu_broadphase_pairs_noalloc(const float* aabbs_dev, uint32_t n, uint32_t* pairs_dev, uint64_t cap,

@@ -5,8 +5,9 @@ Tolerances (f32 compute):
   narrow phase  identical point counts; positions / normals / depths within 1e-5
   solver        the oracle solves the same rows in the GPU's colour order; body
                 velocities within 1e-5 relative (atol 1e-6)
-  world step    one step from identical states within 1e-5; short rollouts
-                within 1e-4 (transcendental ulps accumulate through sin/cos/acos)
+  world step    rollouts from a shared start within 1e-4 .. 2e-3 (last-ulp
+                differences of sin/cos/acos compound over many steps); the
+                per-step 1e-5 contract is in test_gpu_lockstep.py
 """
 import math
 
@@ -266,29 +267,6 @@ def test_world_small_stack_matches_oracle(gpu):
 
     s = scenes.falling_box_stack(3, 3, 3, seed=5, steps=90)
     _run_pair(s, 90, 2e-3, check_every=10)
-
-
-def test_world_single_step_from_identical_state(gpu):
-    """One step of a settled 4x4x4 pile from the same state: within 1e-5."""
-    import bgpu
-    import scenes
-
-    s = scenes.large_pile_fast(4, 4, 4, seed=9, steps=1)
-    w = s.build_gpu(bgpu)
-    o = s.build_oracle(orc)
-    for _ in range(40):  # settle both from identical inputs, re-synchronising the state each step
-        w.step(s.dt)
-        o.set_solve_order(w.solve_order())
-        o.step(s.dt)
-    g = w.state()
-    r = o.state()
-    err = np.abs(g[:, :13] - r[:, :13]).max()
-    assert err <= 1e-3, err
-    w.step(s.dt)
-    o.set_solve_order(w.solve_order())
-    o.step(s.dt)
-    np.testing.assert_array_equal(w.pairs(), o.pairs())
-    assert w.stats()["device_status"] == 0
 
 
 def test_world_mixed_convex_pile_matches_oracle(gpu):
