@@ -8,7 +8,7 @@ device's colour order every step (the rows of a pair missing from that order,
 once the two trajectories hold different pairs, go last in pair order), so
 the figure is the precision drift of the same algorithm, not an order effect.
 Per step and over the dynamic bodies: the position distance and the
-orientation angle 2 acos(|q1 . q2|) (double-cover aware), the two measures of
+orientation angle 2 acos(|q1 . q2|) (double-cover aware, in a stable form), the two measures of
 the reference's parity harness (tools/compare.py:43-47, tolerances 1e-2 m and
 1e-2 rad from docs/parity-harness.md "Tolerance").
 """
@@ -19,9 +19,17 @@ LEDGER_TOL_ANG = 1e-2
 
 
 def quat_angle(qa, qb):
-    """Row-wise angle between two quaternion arrays (x y z w), as tools/compare.py:43-47."""
-    d = np.abs(np.sum(np.asarray(qa, np.float64) * np.asarray(qb, np.float64), axis=1))
-    return 2.0 * np.arccos(np.minimum(1.0, d))
+    """Row-wise angle between two quaternion arrays (x y z w): tools/compare.py:43-47's
+    2 acos(|qa . qb|) for unit quaternions, computed as 2 atan2(|v|, |w|) of the relative
+    rotation conj(qa) qb after normalising both in f64. (acos near 1 turns the ~1e-7 norm
+    error of an f32 quaternion into a ~5e-4 rad floor; the atan2 form has none.)"""
+    a = np.asarray(qa, np.float64)
+    b = np.asarray(qb, np.float64)
+    a = a / np.linalg.norm(a, axis=1, keepdims=True)
+    b = b / np.linalg.norm(b, axis=1, keepdims=True)
+    w = np.sum(a * b, axis=1)
+    v = a[:, 3:4] * b[:, 0:3] - b[:, 3:4] * a[:, 0:3] - np.cross(a[:, 0:3], b[:, 0:3])
+    return 2.0 * np.arctan2(np.linalg.norm(v, axis=1), np.abs(w))
 
 
 def drift_run(bgpu, orc, scene, steps=None):

@@ -19,6 +19,16 @@ def test_quat_angle_double_cover():
     assert drift_f64.quat_angle(q, -q)[0] == 0.0
     h = np.array([[0.0, np.sin(0.05), 0.0, np.cos(0.05)]])
     assert drift_f64.quat_angle(q, h)[0] == pytest.approx(0.1, rel=1e-9)
+    assert drift_f64.quat_angle(h, q)[0] == pytest.approx(0.1, rel=1e-9)
+    rng = np.random.default_rng(3)
+    a = rng.normal(size=(50, 4))
+    b = rng.normal(size=(50, 4))
+    a /= np.linalg.norm(a, axis=1, keepdims=True)
+    b /= np.linalg.norm(b, axis=1, keepdims=True)
+    ref = 2.0 * np.arccos(np.minimum(1.0, np.abs(np.sum(a * b, axis=1))))  # tools/compare.py's form
+    np.testing.assert_allclose(drift_f64.quat_angle(a, b), ref, atol=1e-9)
+    # an f32-rounded copy of the same rotation: no acos floor
+    assert drift_f64.quat_angle(a, a.astype(np.float32)).max() < 1e-6
     assert drift_f64.first_over([0.0, 0.005, 0.02, 0.0], 1e-2) == 3
     assert drift_f64.first_over([0.0, 0.005], 1e-2) is None
 
