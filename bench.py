@@ -219,6 +219,7 @@ def bench_batched(bgpu, scenes, n_worlds, steps, warmup, sample_worlds=32, sampl
     w = sc.build_gpu(bgpu)
     n_dyn = sc.num_dynamic
     w.step_timed(sc.dt, 60)  # settle
+    tuning = w.autotune(sc.dt, 3)  # the solver's launch shape, timed from this state
     w.step_timed(sc.dt, warmup)
     w.enable_timing(True)
     ms = w.step_timed(sc.dt, steps)
@@ -246,6 +247,12 @@ def bench_batched(bgpu, scenes, n_worlds, steps, warmup, sample_worlds=32, sampl
                                      "sample": f"{len(idx)} of the worlds as plain worlds, {sample_steps} steps each, "
                                                f"device time summed"},
             "speedup_vs_one_world_per_launch": batched / per_world if per_world else None,
+            "autotune": {"threads_per_cta": tuning["threads_per_cta"],
+                         "warp_world_max_bodies": tuning["warp_world_max_bodies"], "ctas": tuning["ctas"],
+                         "candidates": tuning["candidates"], "ms_per_step": tuning["ms_per_step"],
+                         "global_solver_ms_per_step": tuning["global_ms_per_step"],
+                         "note": "threads_per_cta 0 = the global solver; worlds of at most warp_world_max_bodies "
+                                 "bodies are solved one per warp, larger ones one per CTA"},
             "device_status": st["device_status"]}
 
 
@@ -255,6 +262,7 @@ def bench_adjoint(bgpu, scenes, n_worlds, steps=120, every=20):
     every segment with recording, then the reverse sweeps), all device time."""
     sc = scenes.adjoint_worlds(n_worlds=n_worlds, seed=5, steps=steps)
     w = sc.build_gpu(bgpu)
+    tuning = w.autotune(sc.dt, 3)  # from the initial state, which it restores
     tape = bgpu.Tape(w, every)
     tape.forward(sc.dt, steps)  # first pass: grows the world's buffers
     tape.rewind()
@@ -281,6 +289,7 @@ def bench_adjoint(bgpu, scenes, n_worlds, steps=120, every=20):
             "backward_first_call_ms": cold_bwd_ms,
             "backward_over_plain_forward": bwd_ms / plain_ms if plain_ms > 0 else None,
             "plain_steps_per_s": steps / (plain_ms / 1000.0), "loss": loss,
+            "solver_launch_shape": {k: tuning[k] for k in ("threads_per_cta", "warp_world_max_bodies", "ctas")},
             "grad_norms": {k: float(np.linalg.norm(v)) for k, v in g.items()}}
 
 

@@ -248,6 +248,15 @@ class StepStats(ctypes.Structure):
                 ("step_ms", ctypes.c_float), ("num_split_contacts", ctypes.c_uint32)]
 
 
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("threads_per_cta", ctypes.c_uint32), ("warp_world_max_bodies", ctypes.c_uint32),
+                ("ctas", ctypes.c_uint32), ("candidates", ctypes.c_uint32), ("ms_per_step", ctypes.c_float),
+                ("global_ms_per_step", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 # numpy view of bgpu_body_desc (96 bytes), for building many descriptors at once
 DESC_DTYPE = np.dtype([("shape", "<u4"), ("position", "<f4", 3), ("orientation", "<f4", 4),
                        ("linear_velocity", "<f4", 3), ("angular_velocity", "<f4", 3), ("mass", "<f4"),
@@ -323,6 +332,9 @@ def lib():
             "bgpu_batch_num_worlds": (U32, [P]),
             "bgpu_batch_world_offsets": (S, [P, U32P]),
             "bgpu_batch_step": (S, [P, ctypes.c_float, U32]),
+            "bgpu_batch_autotune": (S, [P, ctypes.c_float, U32, ctypes.POINTER(BatchTuning)]),
+            "bgpu_batch_set_tuning": (S, [P, U32, U32]),
+            "bgpu_batch_get_tuning": (S, [P, ctypes.POINTER(BatchTuning)]),
             "bgpu_tape_create": (S, [P, U32, ctypes.POINTER(P)]),
             "bgpu_tape_destroy": (None, [P]),
             "bgpu_tape_forward": (S, [P, ctypes.c_float, U32]),
@@ -519,6 +531,20 @@ class World:
         return out.value
 
     @property
+    def autotune(self, dt, steps_per_candidate=3):
+        """Batched worlds: time the solver's launch shapes from the current state, keep the fastest."""
+        t = BatchTuning()
+        check(self.L.bgpu_batch_autotune(self.h, dt, steps_per_candidate, ctypes.byref(t)), "batch_autotune")
+        return t.as_dict()
+
+    def set_tuning(self, threads_per_cta, warp_world_max_bodies=64):
+        check(self.L.bgpu_batch_set_tuning(self.h, threads_per_cta, warp_world_max_bodies), "batch_set_tuning")
+
+    def tuning(self):
+        t = BatchTuning()
+        check(self.L.bgpu_batch_get_tuning(self.h, ctypes.byref(t)), "batch_get_tuning")
+        return t.as_dict()
+
     def num_worlds(self):
         return self.L.bgpu_batch_num_worlds(self.h)
 

@@ -447,6 +447,38 @@ void launch_compute_iw(const BodyDev& b, uint32_t n, cudaStream_t s);
 void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
                 uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark, bool seed_colours,
                 const JointsDev* joints = nullptr);
+// Batched worlds: the per-world PGS (k_solver.cu). A launch plan deals the worlds to CTAs:
+// a CTA either solves one world with all its threads (block mode: __syncthreads between
+// phases) or one world per warp (warp mode: __syncwarp between phases). Worlds are listed
+// largest first, so the longest solves start in the first wave.
+constexpr uint32_t WS_MAX_COLOURS = 64;              // colours per world (one 64-bit mask per body)
+constexpr uint32_t WS_STRIDE = WS_MAX_COLOURS + 3;   // per-world record: g0, ncol, offsets[ncol + 1]
+constexpr uint32_t WS_SMEM_PER_BODY = 64;            // velocities + push velocities (4 float4 per body)
+constexpr uint32_t WS_MAX_WARPS = 8;                 // block size <= 256
+struct WorldPlanDev {
+    const uint2* cta;        // per CTA: first list index, count | 1 << 31 in block mode
+    const uint32_t* list;    // world ids, largest first
+    uint32_t ncta, block;    // CTAs, threads per CTA
+    size_t smem;             // dynamic shared memory per CTA
+};
+struct WorldPlan {
+    DevBuf<uint2> cta;
+    DevBuf<uint32_t> list;
+    uint32_t ncta = 0, block = 0, tau = 0;  // tau: worlds of at most tau bodies run one per warp
+    size_t smem = 0;
+    bool valid = false;
+    WorldPlanDev dev() const { return WorldPlanDev{cta.p, list.p, ncta, block, smem}; }
+};
+// Builds the plan on the host from the world offsets (world k owns bodies [off[k], off[k + 1])).
+// Returns false when some world cannot be held in one CTA's shared memory.
+bool build_world_plan(const std::vector<uint32_t>& world_off, uint32_t block, uint32_t tau, WorldPlan& plan,
+                      cudaStream_t s);
+// The PGS of every world of a batch (no joints): world-local colouring, batches and solve.
+// Writes pd.colour (world-local colours), pd.batch_rec (slots grouped per world, then colour),
+// the per-world records `wcol` (WS_STRIDE words per world) and the step's counts in pd.scalars.
+void run_world_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
+                      uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark,
+                      const uint32_t* world_off, uint32_t nworlds, const WorldPlan& plan, uint32_t* wcol);
 // One team barrier that nothing completes (2 blocks): the wait gives up after limit_ns and
 // leaves ST_BARRIER_TIMEOUT in *status. ctr and status are device words the caller zeroes.
 void run_wait_selftest(unsigned long long limit_ns, unsigned int* ctr, uint32_t* status, cudaStream_t s);
@@ -475,5 +507,10 @@ void launch_adj_velocities(uint32_t n, float dt, const uint8_t* flags, const flo
 void run_adj_solve(const AdjStep& st, float4* lbar, float4* vbar, float4* wbar, float* mubar, float* ebar,
                    const float4* material, const float* carry_in, float* carry_out, float restitution_threshold,
                    float warm_factor, unsigned int* bar, uint32_t* status_dev, cudaStream_t s);
+// The same for a step the per-world solver ran: st.off holds its per-world records (WS_STRIDE
+// words per world); each world's phases run in reverse inside its CTA or warp.
+void run_adj_solve_worlds(const AdjStep& st, const WorldPlan& plan, float4* lbar, float4* vbar, float4* wbar,
+                          float* mubar, float* ebar, const float4* material, const float* carry_in, float* carry_out,
+                          float restitution_threshold, float warm_factor, uint32_t* status_dev, cudaStream_t s);
 
 }  // namespace bgpu

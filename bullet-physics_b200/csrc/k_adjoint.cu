@@ -209,6 +209,37 @@ __global__ void __launch_bounds__(256, 2) k_adj_solve(AdjArgs a) {
     }
 }
 
+// A step of the per-world solver in reverse: each world's phases (sweep, colour) run backwards
+// inside the CTA or warp the plan gives it (the same deal as the forward kernel, k_solver.cu),
+// with a block or warp sync between phases. Worlds share no body, so no barrier spans them.
+// wrec: per world g0, ncol, offsets[ncol + 1] (WS_STRIDE words).
+template <bool WARP>
+__device__ void reverse_world(const AdjArgs& a, const uint32_t* __restrict__ wrec, uint32_t w, uint32_t lane,
+                              uint32_t nt) {
+    const uint32_t* r = wrec + size_t(w) * WS_STRIDE;
+    const uint32_t g0 = r[0], ncol = min(r[1], WS_MAX_COLOURS);
+    for (uint32_t sweep = a.iters + 1; sweep-- > 0;) {
+        for (uint32_t c = ncol; c-- > 0;) {
+            const uint32_t hi = g0 + r[3 + c];
+            for (uint32_t t = g0 + r[2 + c] + lane; t < hi; t += nt) reverse_group(a, t, sweep);
+            if (WARP) __syncwarp();
+            else __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_adj_solve_worlds(AdjArgs a, WorldPlanDev plan, const uint32_t* wrec) {
+    const uint2 c = plan.cta[blockIdx.x];
+    const bool block_mode = (c.y >> 31) != 0u;
+    const uint32_t count = c.y & 0x7fffffffu;
+    if (block_mode) {
+        reverse_world<false>(a, wrec, plan.list[c.x], threadIdx.x, blockDim.x);
+        return;
+    }
+    const uint32_t wi = threadIdx.x >> 5;
+    if (wi < count) reverse_world<true>(a, wrec, plan.list[c.x + wi], threadIdx.x & 31u, 32u);
+}
+
 int adj_grid() {
     static int grid = 0;
     if (!grid) {
@@ -242,6 +273,18 @@ void run_adj_solve(const AdjStep& st, float4* lbar, float4* vbar, float4* wbar, 
     void* args[] = {&a};
     check_cuda(cudaLaunchCooperativeKernel((const void*)k_adj_solve, dim3(adj_grid()), dim3(256), args, 0, s),
                "adjoint solve launch");
+}
+
+void run_adj_solve_worlds(const AdjStep& st, const WorldPlan& plan, float4* lbar, float4* vbar, float4* wbar,
+                          float* mubar, float* ebar, const float4* material, const float* carry_in, float* carry_out,
+                          float restitution_threshold, float warm_factor, uint32_t* status_dev, cudaStream_t s) {
+    if (st.ncol == 0) return;
+    if (!plan.valid || plan.ncta == 0)
+        throw CudaError{cudaErrorInvalidValue, "the batch's solver launch shape changed between forward and backward"};
+    AdjArgs a{st.recs, st.off, st.end, st.ncol, st.iters, st.tab, st.sweeps, lbar, vbar, wbar, mubar, ebar, material,
+              st.merge_pos, carry_in, st.row_src, carry_out, restitution_threshold, warm_factor, nullptr, status_dev};
+    k_adj_solve_worlds<<<plan.ncta, plan.block, 0, s>>>(a, plan.dev(), st.off);
+    check_cuda(cudaGetLastError(), "adjoint world solve launch");
 }
 
 }  // namespace bgpu

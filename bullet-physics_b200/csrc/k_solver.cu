@@ -24,6 +24,7 @@
 // angular components Iw^-1 (r x d) and the velocity couplings are recomputed
 // from the per-body world inverse inertia with the reference's arithmetic, so
 // they equal the values the reference precomputes in prepare().
+#include <algorithm>
 #include <cooperative_groups.h>
 #include <cub/cub.cuh>
 #include "bgpu_kernels.cuh"
@@ -817,6 +818,265 @@ __global__ void __launch_bounds__(256, 2) k_solve(SolveArgs a) {
     }
 }
 
+// ---------------------------------------------------------------- per-world PGS (batched worlds)
+// Every world of a batch is solved on its own by one CTA or one warp: its row groups are
+// coloured in shared memory (Jones-Plassmann with the world's own priorities, colours from
+// one 64-bit mask per body), sorted into colour batches, and solved phase by phase with only
+// a block (or warp) sync between phases; its bodies' velocities and push velocities stay in
+// shared memory for the whole solve. No barrier spans worlds. Within a world the order is the
+// same (colour, pair) Gauss-Seidel order the global solver uses, so each world equals the
+// reference's sequential solve over its rows in that order. The split sweeps touch only push
+// velocities, so split sweep s runs in the phases of velocity sweep s + 1.
+struct WorldSolveArgs {
+    SolveArgs a;                       // rows, tables, adjoint sweep records, iw, constants
+    const uint32_t* contact_pairs;     // pair ids with rows, ascending (so grouped by world)
+    const uint32_t* ngroups;           // device count of contact_pairs
+    const uint64_t* pairs;
+    const uint32_t* row_count;
+    const uint32_t* world_off;
+    uint32_t* colour;                  // out: world-local colour per contact pair
+    uint4* recs;                       // out: slot records, world by world, colour by colour
+    uint32_t* wcol;                    // out: per world g0, ncol, offsets[ncol + 1]
+    uint32_t* colour_count;            // out: groups per colour summed over worlds (stats)
+    uint32_t* split_count;
+    uint32_t* scalars;                 // out: [3] rows [4] colours (max) [5] split groups [10] split rows
+    float4* linvel;
+    float4* angvel;
+    float4* push_lin;
+    float4* push_ang;
+    uint32_t* status;
+    WorldPlanDev plan;
+};
+
+struct WorldCtx {  // per world being solved by a CTA or a warp
+    uint32_t g0, g1, ncol, left, rows, split_groups, split_rows;
+    uint32_t hist[WS_MAX_COLOURS], off[WS_MAX_COLOURS + 1], cur[WS_MAX_COLOURS], split_hist[WS_MAX_COLOURS];
+};
+
+template <bool WARP>
+__device__ __forceinline__ void ws_sync() {
+    if (WARP) __syncwarp();
+    else __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t lower_bound_lo(const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ cp,
+                                                   uint32_t n, uint32_t body) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (key_lo(pairs[cp[mid]]) < body) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// One group of a world: velocities from the world's shared-memory arrays (body i at i - b0).
+template <int KIND>
+__device__ __forceinline__ void run_group_shared(const SolveArgs& a, uint32_t t, uint4 rec, uint32_t sweep,
+                                                 uint32_t last, float4* lin, float4* ang, uint32_t b0) {
+    const uint32_t ia = rec.x, ib = rec.y, p = rec.z & 0x1fffffffu, cnt = rec.z >> 29;
+    const uint32_t la_i = ia - b0, lb_i = ib - b0;
+    V3 la = from4(lin[la_i]), wa = from4(ang[la_i]);
+    V3 lb = from4(lin[lb_i]), wb = from4(ang[lb_i]);
+    bool appa, appb;
+    if (KIND == WARM) warm_group(a, t, p, cnt, ia, ib, la, wa, lb, wb, appa, appb);
+    else if (KIND == ITER) iter_group(a, t, p, cnt, sweep, sweep == last, la, wa, lb, wb, appa, appb);
+    else split_group(a, t, p, cnt, ia, ib, sweep == 0, sweep == last, la, wa, lb, wb, appa, appb);
+    if (appa) { lin[la_i] = to4(la, 0.0f); ang[la_i] = to4(wa, 0.0f); }
+    if (appb) { lin[lb_i] = to4(lb, 0.0f); ang[lb_i] = to4(wb, 0.0f); }
+}
+
+// The whole PGS of world w by `nt` threads (lane = 0 .. nt - 1), `sm` its 4 * nb float4 of
+// shared memory, `C` its context. Every thread of the CTA (block mode) or of the warp (warp
+// mode) calls it; every early return is taken by all of them together, so every sync is
+// reached by all of them.
+template <bool WARP>
+__device__ void solve_world(const WorldSolveArgs& A, uint32_t w, uint32_t lane, uint32_t nt, float4* sm, WorldCtx& C) {
+    const SolveArgs& a = A.a;
+    const uint32_t b0 = A.world_off[w], nb = A.world_off[w + 1] - b0;
+    float4* lin = sm;
+    float4* ang = sm + nb;
+    float4* plin = sm + 2 * nb;
+    float4* pang = sm + 3 * nb;
+    // Colouring scratch over the push-velocity region (24 of its 32 bytes per body).
+    unsigned long long* mask = reinterpret_cast<unsigned long long*>(plin);
+    unsigned long long* best0 = mask + nb;
+    unsigned long long* best1 = best0 + nb;
+    for (uint32_t i = lane; i < nb; i += nt) {
+        lin[i] = __ldcg(&A.linvel[b0 + i]);
+        ang[i] = __ldcg(&A.angvel[b0 + i]);
+        mask[i] = 0ull;
+        best0[i] = 0ull;
+        best1[i] = 0ull;
+    }
+    if (lane == 0) {
+        const uint32_t K = *A.ngroups;
+        C.g0 = lower_bound_lo(A.pairs, A.contact_pairs, K, b0);
+        C.g1 = lower_bound_lo(A.pairs, A.contact_pairs, K, b0 + nb);
+        C.left = C.g1 - C.g0;
+        C.ncol = 0;
+        C.rows = C.split_groups = C.split_rows = 0;
+    }
+    for (uint32_t c = lane; c < WS_MAX_COLOURS; c += nt) {
+        C.hist[c] = 0;
+        C.split_hist[c] = 0;
+    }
+    ws_sync<WARP>();
+    const uint32_t g0 = C.g0, g1 = C.g1;
+    if (g0 == g1) return;  // no rows in this world: its velocities stay as they are
+    auto dyn = [&](uint32_t i) { return inv_mass_of(a.iw, i) > 0.0f; };
+    // 1. Jones-Plassmann rounds: an uncoloured group wins when its priority is the largest
+    //    among the uncoloured groups at each of its dynamic bodies; a winner takes the lowest
+    //    colour free at both bodies (winners of one round share no dynamic body).
+    for (uint32_t g = g0 + lane; g < g1; g += nt) A.colour[g] = NO_COLOUR;
+    ws_sync<WARP>();
+    for (uint32_t r = 0; C.left != 0; ++r) {
+        if (r >= MAX_ROUNDS) {
+            if (lane == 0) atomicOr(A.status, ST_COLOUR_ROUNDS);
+            break;
+        }
+        unsigned long long* best = (r & 1) ? best1 : best0;
+        unsigned long long* other = (r & 1) ? best0 : best1;
+        for (uint32_t g = g0 + lane; g < g1; g += nt) {
+            if (A.colour[g] != NO_COLOUR) continue;
+            const uint64_t key = A.pairs[A.contact_pairs[g]];
+            const unsigned long long v = (static_cast<unsigned long long>(mix32(key)) << 32) | (g - g0 + 1u);
+            const uint32_t ia = key_lo(key), ib = key_hi(key);
+            if (dyn(ia)) atomicMax(&best[ia - b0], v);
+            if (dyn(ib)) atomicMax(&best[ib - b0], v);
+        }
+        ws_sync<WARP>();
+        uint32_t won = 0;
+        for (uint32_t g = g0 + lane; g < g1; g += nt) {
+            if (A.colour[g] != NO_COLOUR) continue;
+            const uint64_t key = A.pairs[A.contact_pairs[g]];
+            const unsigned long long v = (static_cast<unsigned long long>(mix32(key)) << 32) | (g - g0 + 1u);
+            const uint32_t ia = key_lo(key), ib = key_hi(key);
+            const bool da = dyn(ia), db = dyn(ib);
+            if ((da && best[ia - b0] != v) || (db && best[ib - b0] != v)) continue;
+            const unsigned long long m = (da ? mask[ia - b0] : 0ull) | (db ? mask[ib - b0] : 0ull);
+            int c = __ffsll(static_cast<long long>(~m)) - 1;
+            if (c < 0) {  // 64 colours taken at one body
+                atomicOr(A.status, ST_COLOUR_OVERFLOW);
+                c = int(WS_MAX_COLOURS) - 1;
+            }
+            A.colour[g] = uint32_t(c);
+            if (da) mask[ia - b0] |= 1ull << c;
+            if (db) mask[ib - b0] |= 1ull << c;
+            ++won;
+        }
+        for (uint32_t i = lane; i < nb; i += nt) other[i] = 0ull;
+        if (won) atomicSub(&C.left, won);
+        ws_sync<WARP>();
+    }
+    // 2. Colour batches: histogram, offsets, scatter of the slot records.
+    for (uint32_t g = g0 + lane; g < g1; g += nt) {
+        const uint32_t c = A.colour[g];
+        if (c >= WS_MAX_COLOURS) continue;  // left uncoloured (round limit; the status word says so)
+        atomicAdd(&C.hist[c], 1u);
+        atomicMax(&C.ncol, c + 1u);
+    }
+    ws_sync<WARP>();
+    const uint32_t ncol = C.ncol;
+    if (lane == 0) {
+        uint32_t acc = 0;
+        uint32_t* rec = A.wcol + size_t(w) * WS_STRIDE;
+        rec[0] = g0;
+        rec[1] = ncol;
+        for (uint32_t c = 0; c < ncol; ++c) {
+            C.off[c] = acc;
+            C.cur[c] = acc;
+            rec[2 + c] = acc;
+            acc += C.hist[c];
+        }
+        C.off[ncol] = acc;
+        rec[2 + ncol] = acc;
+        if (ncol) atomicMax(&A.scalars[4], ncol);
+    }
+    ws_sync<WARP>();
+    uint32_t my_rows = 0, my_split_groups = 0, my_split_rows = 0;
+    for (uint32_t g = g0 + lane; g < g1; g += nt) {
+        const uint32_t c = A.colour[g];
+        if (c >= WS_MAX_COLOURS) continue;
+        const uint32_t slot = g0 + atomicAdd(&C.cur[c], 1u);
+        const uint32_t p = A.contact_pairs[g];
+        const uint64_t key = A.pairs[p];
+        const uint32_t cnt = A.row_count[p];
+        uint32_t nsplit = 0;
+        for (uint32_t k = 0; k < cnt; ++k) nsplit += a.rows[(size_t(p) * 4 + k) * ROW_F4 + 5].z != 0.0f ? 1u : 0u;
+        A.recs[slot] = make_uint4(key_lo(key), key_hi(key), p | (cnt << 29), nsplit ? 1u : 0u);
+        my_rows += cnt;
+        if (nsplit) {
+            ++my_split_groups;
+            my_split_rows += nsplit;
+            atomicAdd(&C.split_hist[c], 1u);
+        }
+    }
+    if (my_rows) atomicAdd(&C.rows, my_rows);
+    if (my_split_groups) {
+        atomicAdd(&C.split_groups, my_split_groups);
+        atomicAdd(&C.split_rows, my_split_rows);
+    }
+    ws_sync<WARP>();  // the colouring scratch is free from here on
+    for (uint32_t i = lane; i < nb; i += nt) {
+        plin[i] = __ldcg(&A.push_lin[b0 + i]);
+        pang[i] = __ldcg(&A.push_ang[b0 + i]);
+    }
+    if (lane == 0) {
+        atomicAdd(&A.scalars[3], C.rows);
+        if (C.split_groups) {
+            atomicAdd(&A.scalars[5], C.split_groups);
+            atomicAdd(&A.scalars[10], C.split_rows);
+        }
+    }
+    for (uint32_t c = lane; c < ncol; c += nt) {
+        atomicAdd(&A.colour_count[c], C.hist[c]);
+        if (C.split_hist[c]) atomicAdd(&A.split_count[c], C.split_hist[c]);
+    }
+    ws_sync<WARP>();
+    // 3. Warm start and velocity sweeps; split sweep s rides along velocity sweep s + 1.
+    const uint32_t iters = a.iterations;
+    for (uint32_t sweep = 0; sweep <= iters; ++sweep) {
+        for (uint32_t c = 0; c < ncol; ++c) {
+            const uint32_t hi = g0 + C.off[c + 1];
+            for (uint32_t t = g0 + C.off[c] + lane; t < hi; t += nt) {
+                const uint4 rec = A.recs[t];
+                if (sweep == 0) run_group_shared<WARM>(a, t, rec, 0, iters, lin, ang, b0);
+                else run_group_shared<ITER>(a, t, rec, sweep, iters, lin, ang, b0);
+                if (sweep >= 1 && rec.w) run_group_shared<SPLIT>(a, t, rec, sweep - 1, iters - 1, plin, pang, b0);
+            }
+            ws_sync<WARP>();
+        }
+    }
+    // 4. The world's velocities and push velocities back to global memory.
+    for (uint32_t i = lane; i < nb; i += nt) {
+        __stcg(&A.linvel[b0 + i], lin[i]);
+        __stcg(&A.angvel[b0 + i], ang[i]);
+        __stcg(&A.push_lin[b0 + i], plin[i]);
+        __stcg(&A.push_ang[b0 + i], pang[i]);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_world_solve(WorldSolveArgs A) {
+    extern __shared__ float4 ws_dyn[];
+    __shared__ WorldCtx ctx[WS_MAX_WARPS];
+    const uint2 c = A.plan.cta[blockIdx.x];
+    const bool block_mode = (c.y >> 31) != 0u;
+    const uint32_t count = c.y & 0x7fffffffu;
+    if (block_mode) {
+        solve_world<false>(A, A.plan.list[c.x], threadIdx.x, blockDim.x, ws_dyn, ctx[0]);
+        return;
+    }
+    const uint32_t wi = threadIdx.x >> 5;
+    if (wi >= count) return;  // warp mode: warps never sync with each other
+    uint32_t off = 0;
+    for (uint32_t j = 0; j < wi; ++j) {
+        const uint32_t wj = A.plan.list[c.x + j];
+        off += A.world_off[wj + 1] - A.world_off[wj];
+    }
+    solve_world<true>(A, A.plan.list[c.x + wi], threadIdx.x & 31u, 32u, ws_dyn + 4 * size_t(off), ctx[wi]);
+}
+
 // ---------------------------------------------------------------- cache update
 // step.rs:982-1005: the solved normal impulse goes back to its manifold point.
 __global__ void k_writeback(uint32_t npairs, const uint32_t* __restrict__ row_count, const float4* __restrict__ rows,
@@ -996,6 +1256,111 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
     pd.vtab.reserve(size_t(VT_PLANES) * 4 * slots);
     pd.stab.reserve(size_t(ST_PLANES) * 4 * slots);
     launch_solve(w, pd, sp, status_dev, s, with_joints ? joints : nullptr);
+    mark(6);
+}
+
+bool build_world_plan(const std::vector<uint32_t>& world_off, uint32_t block, uint32_t tau, WorldPlan& plan,
+                      cudaStream_t s) {
+    plan.valid = false;
+    if (block < 32 || block > 32 * WS_MAX_WARPS || block % 32) return false;
+    const uint32_t nw = world_off.empty() ? 0u : uint32_t(world_off.size() - 1);
+    std::vector<uint32_t> order(nw);
+    for (uint32_t k = 0; k < nw; ++k) order[k] = k;
+    auto size = [&](uint32_t k) { return world_off[k + 1] - world_off[k]; };
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return size(x) > size(y); });
+    const size_t smem_cap = 200u * 1024u;  // leaves room for the static contexts and L1
+    std::vector<uint2> cta;
+    size_t smem = 0;
+    const uint32_t per_cta = block / 32;
+    uint32_t k = 0;
+    while (k < nw) {
+        const uint32_t nb = size(order[k]);
+        if (nb > tau) {  // block mode: one world per CTA
+            if (size_t(nb) * WS_SMEM_PER_BODY > smem_cap) return false;
+            cta.push_back(make_uint2(k, 1u | (1u << 31)));
+            smem = std::max(smem, size_t(nb) * WS_SMEM_PER_BODY);
+            ++k;
+            continue;
+        }
+        uint32_t cnt = 0;
+        size_t bodies = 0;
+        while (k + cnt < nw && cnt < per_cta && (bodies + size(order[k + cnt])) * WS_SMEM_PER_BODY <= smem_cap) {
+            bodies += size(order[k + cnt]);
+            ++cnt;
+        }
+        if (cnt == 0) return false;
+        cta.push_back(make_uint2(k, cnt));
+        smem = std::max(smem, bodies * WS_SMEM_PER_BODY);
+        k += cnt;
+    }
+    plan.cta.reserve(std::max<size_t>(cta.size(), 1));
+    plan.list.reserve(std::max<uint32_t>(nw, 1));
+    if (!cta.empty())
+        check_cuda(cudaMemcpyAsync(plan.cta.p, cta.data(), cta.size() * sizeof(uint2), cudaMemcpyHostToDevice, s), "h2d");
+    if (nw) check_cuda(cudaMemcpyAsync(plan.list.p, order.data(), nw * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "h2d");
+    check_cuda(cudaStreamSynchronize(s), "sync");  // the host vectors go out of scope
+    if (smem > 48u * 1024u)
+        check_cuda(cudaFuncSetAttribute((const void*)k_world_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(smem)), "smem attribute");
+    plan.ncta = uint32_t(cta.size());
+    plan.block = block;
+    plan.tau = tau;
+    plan.smem = smem;
+    plan.valid = true;
+    return true;
+}
+
+void run_world_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
+                      uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark,
+                      const uint32_t* world_off, uint32_t nworlds, const WorldPlan& plan, uint32_t* wcol) {
+    check_cuda(cudaMemsetAsync(pd.scalars.p + 2, 0, 4 * sizeof(uint32_t), s), "memset");
+    check_cuda(cudaMemsetAsync(pd.scalars.p + 10, 0, 2 * sizeof(uint32_t), s), "memset");
+    check_cuda(cudaMemsetAsync(pd.colour_count.p, 0, (MAX_COLOURS + 3) * sizeof(uint32_t), s), "memset");
+    check_cuda(cudaMemsetAsync(pd.split_count.p, 0, (MAX_COLOURS + 3) * sizeof(uint32_t), s), "memset");
+    if (npairs == 0 || nworlds == 0) {
+        mark(5);
+        mark(6);
+        return;
+    }
+    const int TB = 256;
+    if (npairs >= (1u << 29)) throw CudaError{cudaErrorInvalidValue, "more than 2^29 pairs for the solver's slot records"};
+    k_flag_contact_pairs<<<(npairs + TB - 1) / TB, TB, 0, s>>>(npairs, pd.row_count.p, pd.flags.p);
+    size_t bytes = 0;
+    cub::CountingInputIterator<uint32_t> it(0);
+    check_cuda(cub::DeviceSelect::Flagged(nullptr, bytes, it, pd.flags.p, pd.contact_pairs.p, pd.scalars.p + 2,
+                                          int(npairs), s), "select size");
+    pd.cub_tmp.reserve(bytes);
+    check_cuda(cub::DeviceSelect::Flagged(pd.cub_tmp.p, bytes, it, pd.flags.p, pd.contact_pairs.p, pd.scalars.p + 2,
+                                          int(npairs), s), "select");
+    mark(5);
+    const size_t slots = (size_t(npairs) + 32u * (MAX_COLOURS + 1) + 31u) & ~size_t(31);
+    pd.vtab.reserve(size_t(VT_PLANES) * 4 * slots);
+    pd.stab.reserve(size_t(ST_PLANES) * 4 * slots);
+    WorldSolveArgs A;
+    A.a = SolveArgs{pd.rows.p, pd.batch_rec.p, pd.colour_offset.p, pd.colour_cursor.p, pd.split_rec.p,
+                    pd.split_offset.p, pd.split_cursor.p, pd.scalars.p, w.b.linvel, w.b.angvel, w.b.push_lin,
+                    w.b.push_ang, w.b.iw, pd.vtab.p, pd.stab.p, pd.rec.sweeps,
+                    pd.barrier.p, status_dev, sp.inv_dt, sp.info.restitution_velocity_threshold,
+                    sp.info.num_iterations, JointsDev{}, sp.info.damping};
+    A.contact_pairs = pd.contact_pairs.p;
+    A.ngroups = pd.scalars.p + 2;
+    A.pairs = pairs;
+    A.row_count = pd.row_count.p;
+    A.world_off = world_off;
+    A.colour = pd.colour.p;
+    A.recs = pd.batch_rec.p;
+    A.wcol = wcol;
+    A.colour_count = pd.colour_count.p;
+    A.split_count = pd.split_count.p;
+    A.scalars = pd.scalars.p;
+    A.linvel = w.b.linvel;
+    A.angvel = w.b.angvel;
+    A.push_lin = w.b.push_lin;
+    A.push_ang = w.b.push_ang;
+    A.status = status_dev;
+    A.plan = plan.dev();
+    k_world_solve<<<plan.ncta, plan.block, plan.smem, s>>>(A);
+    check_cuda(cudaGetLastError(), "world solve launch");
     mark(6);
 }
 

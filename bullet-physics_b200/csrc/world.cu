@@ -106,8 +106,9 @@ struct StepRecord {
     DevBuf<uint4> recs;                  // batch slot records (colour order)
     DevBuf<float4> tab, sweeps;          // velocity contact table, per-sweep records
     DevBuf<uint32_t> row_src, merge_pos; // warm-start sources, merged cache positions
-    DevBuf<uint32_t> off, end;           // colour batch starts / ends
+    DevBuf<uint32_t> off, end;           // colour batch starts / ends (per-world solver: its world records)
     DevBuf<uint8_t> flags;               // RF_* per body
+    bool per_world = false;              // recorded from the per-world solver
     AdjStep view() const {
         return AdjStep{recs.p, off.p, end.p, ncol, iters, tab.p, sweeps.p, merge_pos.p, row_src.p};
     }
@@ -141,6 +142,14 @@ struct World {
     std::vector<uint32_t> world_off_h{0u};
     DevBuf<uint32_t> world_off_d, world_of_d;
     DevBuf<uint32_t> world_sim;  // [0, W) simulate, [W, 2W) prev_simulate, per world
+    // per-world solver of a batch (k_solver.cu): its launch plan, chosen by bgpu_batch_autotune
+    // (threads per CTA, largest world solved by one warp), and the per-world batch records
+    WorldPlan wplan;
+    uint32_t wplan_block = 128, wplan_tau = 64;  // 0 threads: the global (all-worlds) solver
+    DevBuf<uint32_t> wcol;
+    bool last_world_solver = false;  // the last step ran the per-world solver
+    float tuned_ms = 0.0f, tuned_global_ms = 0.0f;
+    uint32_t tuned_candidates = 0;
     // step machinery
     Broadphase bp;
     Islands islands;
@@ -418,8 +427,20 @@ struct World {
         check_cuda(cudaStreamSynchronize(stream), "sync");
         std::swap(world_sim.p, fresh.p);
         std::swap(world_sim.cap, fresh.cap);
+        rebuild_world_plan();
         return first_world;
     }
+
+    // The per-world solver's plan for the current worlds (an invalid plan, or a world with
+    // joints, falls back to the global solver).
+    void rebuild_world_plan() {
+        wplan.valid = false;
+        if (!batch || wplan_block == 0) return;
+        wcol.reserve(size_t(num_worlds()) * WS_STRIDE + 1);
+        build_world_plan(world_off_h, wplan_block, wplan_tau, wplan, stream);
+    }
+
+    bool use_world_solver() const { return batch && wplan.valid && joints_h.empty(); }
 
     JointsDev joints_dev() {
         JointsDev j;
@@ -748,8 +769,13 @@ struct World {
         mark(4);
         // 6: solve (colouring, then the PGS kernel)
         // The colouring starts from last step's colours, except every RECOLOUR_PERIOD-th step.
-        run_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); },
-                   step_count % RECOLOUR_PERIOD != 0, &jd);
+        last_world_solver = use_world_solver();
+        if (last_world_solver)
+            run_world_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); }, world_off_d.p,
+                             nw, wplan, wcol.p);
+        else
+            run_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); },
+                       step_count % RECOLOUR_PERIOD != 0, &jd);
         ++step_count;
         // 6b: impulse writeback + prune
         run_cache_update(pairs.p, npairs, old_cache, pd, next, world_of, simulate, prev_simulate, stream);
@@ -801,8 +827,24 @@ struct World {
         check_cuda(cudaStreamSynchronize(stream), "sync");
         R.ncol = hs->scalars[4];
         R.slots = 0;
+        R.per_world = last_world_solver;
         if (npairs == 0 || R.ncol == 0) {
             R.ncol = 0;
+            return;
+        }
+        if (R.per_world) {  // slots are the contact pairs, world by world; the world records say where
+            const uint32_t words = num_worlds() * WS_STRIDE;
+            R.slots = (hs->scalars[2] + 31u) & ~31u;
+            R.off.reserve(words);
+            R.recs.reserve(R.slots);
+            R.tab.reserve(size_t(R.slots) * VT_PLANES * 4);
+            check_cuda(cudaMemcpyAsync(R.off.p, wcol.p, words * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream),
+                       "record copy");
+            check_cuda(cudaMemcpyAsync(R.recs.p, pd.batch_rec.p, size_t(R.slots) * sizeof(uint4),
+                                       cudaMemcpyDeviceToDevice, stream), "record copy");
+            check_cuda(cudaMemcpyAsync(R.tab.p, pd.vtab.p, size_t(R.slots) * VT_PLANES * 4 * sizeof(float4),
+                                       cudaMemcpyDeviceToDevice, stream), "record copy");
+            check_cuda(cudaStreamSynchronize(stream), "sync");
             return;
         }
         std::vector<uint32_t> off(R.ncol + 1);
@@ -912,6 +954,65 @@ static void restore_snapshot(World& W, const Snapshot& S) {
     W.stats_pending = false;
 }
 
+// Autotuner of a batch's solver launch shape: every candidate steps the batch from the same
+// checkpoint for `steps` timed steps (after one untimed step); the fastest is kept and the
+// batch goes back to the checkpoint.
+static void autotune_batch(World& W, float dt, uint32_t steps) {
+    if (!W.batch) throw InvalidArg{"bgpu_batch_autotune needs a batched world"};
+    if (steps == 0 || steps > 1000) throw InvalidArg{"steps_per_candidate must lie in 1..1000"};
+    W.finish_stats();
+    Snapshot start;
+    save_snapshot(W, start);
+    struct Cand {
+        uint32_t block, tau;
+    };
+    std::vector<Cand> cands{{0u, 0u}};
+    for (uint32_t block : {32u, 64u, 128u, 256u})
+        for (uint32_t tau : {0u, 32u, 64u, 128u, 0x7fffffffu}) cands.push_back({block, tau});
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    struct Release {
+        cudaEvent_t &a, &b;
+        ~Release() {
+            if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
+        }
+    } release{e0, e1};
+    check_cuda(cudaEventCreate(&e0), "event");
+    check_cuda(cudaEventCreate(&e1), "event");
+    Cand best{W.wplan_block, W.wplan_tau};
+    float best_ms = 0.0f, global_ms = 0.0f;
+    uint32_t timed = 0;
+    for (const Cand& c : cands) {
+        W.wplan_block = c.block;
+        W.wplan_tau = c.tau;
+        W.rebuild_world_plan();
+        if (c.block && !W.wplan.valid) continue;
+        restore_snapshot(W, start);
+        W.step_once(dt);
+        W.finish_stats();
+        check_cuda(cudaEventRecord(e0, W.stream), "event");
+        for (uint32_t k = 0; k < steps; ++k) W.step_once(dt);
+        check_cuda(cudaEventRecord(e1, W.stream), "event");
+        W.finish_stats();
+        float ms = 0.0f;
+        check_cuda(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+        if (W.last.device_status) continue;  // e.g. a world needing more colours than one mask holds
+        ++timed;
+        if (c.block == 0) global_ms = ms;
+        if (best_ms == 0.0f || ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    restore_snapshot(W, start);
+    W.wplan_block = best.block;
+    W.wplan_tau = best.tau;
+    W.rebuild_world_plan();
+    W.tuned_ms = best_ms / float(steps);
+    W.tuned_global_ms = global_ms / float(steps);
+    W.tuned_candidates = timed;
+}
+
 // Tape::backward of the rigid-body step: a forward pass that keeps a
 // checkpoint every `every` steps, and a backward pass that replays each
 // segment from its checkpoint with recording on, then runs the segment's
@@ -1015,9 +1116,14 @@ struct Tape {
                 }
                 if (R.ncol) {
                     lbar.reserve(size_t(R.slots) * 4);
-                    run_adj_solve(R.view(), lbar.p, vbar.p, wbar.p, mubar.p, ebar.p, W->material.p, carry_in, cout,
-                                  W->info.restitution_velocity_threshold, W->info.warmstarting_factor, bar.p, status.p,
-                                  s);
+                    if (R.per_world)
+                        run_adj_solve_worlds(R.view(), W->wplan, lbar.p, vbar.p, wbar.p, mubar.p, ebar.p,
+                                             W->material.p, carry_in, cout, W->info.restitution_velocity_threshold,
+                                             W->info.warmstarting_factor, status.p, s);
+                    else
+                        run_adj_solve(R.view(), lbar.p, vbar.p, wbar.p, mubar.p, ebar.p, W->material.p, carry_in,
+                                      cout, W->info.restitution_velocity_threshold, W->info.warmstarting_factor, bar.p,
+                                      status.p, s);
                 }
                 launch_adj_velocities(n, dt, R.flags.p, W->material.p, vbar.p, wbar.p, s);
                 check_cuda(cudaGetLastError(), "adjoint launch");
@@ -1373,6 +1479,43 @@ bgpu_status bgpu_tape_timing(const bgpu_tape* t, float* forward_ms, float* backw
 }
 
 uint32_t bgpu_batch_num_worlds(const bgpu_world* w) { return (w && w->impl.batch) ? w->impl.num_worlds() : 0u; }
+
+bgpu_status bgpu_batch_autotune(bgpu_world* w, float dt, uint32_t steps_per_candidate, bgpu_batch_tuning* out) {
+    if (!w || !(dt > 0.0f)) return BGPU_ERR_INVALID_ARGUMENT;
+    bgpu_status st = guarded([&]() -> bgpu_status {
+        bgpu::autotune_batch(w->impl, dt, steps_per_candidate);
+        return BGPU_OK;
+    });
+    if (st == BGPU_OK && out) st = bgpu_batch_get_tuning(w, out);
+    return st;
+}
+
+bgpu_status bgpu_batch_set_tuning(bgpu_world* w, uint32_t threads_per_cta, uint32_t warp_world_max_bodies) {
+    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        World& W = w->impl;
+        if (!W.batch) throw bgpu::InvalidArg{"bgpu_batch_set_tuning needs a batched world"};
+        if (threads_per_cta && (threads_per_cta < 32 || threads_per_cta > 256 || threads_per_cta % 32))
+            throw bgpu::InvalidArg{"threads_per_cta must be 0 or a multiple of 32 in 32..256"};
+        W.finish_stats();
+        W.wplan_block = threads_per_cta;
+        W.wplan_tau = warp_world_max_bodies;
+        W.rebuild_world_plan();
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_batch_get_tuning(bgpu_world* w, bgpu_batch_tuning* out) {
+    if (!w || !out) return BGPU_ERR_INVALID_ARGUMENT;
+    World& W = w->impl;
+    out->threads_per_cta = W.wplan_block;
+    out->warp_world_max_bodies = W.wplan_tau;
+    out->ctas = W.use_world_solver() ? W.wplan.ncta : 0u;
+    out->candidates = W.tuned_candidates;
+    out->ms_per_step = W.tuned_ms;
+    out->global_ms_per_step = W.tuned_global_ms;
+    return BGPU_OK;
+}
 
 bgpu_status bgpu_batch_world_offsets(bgpu_world* w, uint32_t* offsets) {
     if (!w || !offsets || !w->impl.batch) {
@@ -1927,6 +2070,16 @@ bgpu_status bgpu_read_colour_batches(bgpu_world* w, uint32_t* groups, uint32_t* 
         const uint32_t k = std::min(cap, ncol);
         if (!k) return BGPU_OK;
         std::vector<uint32_t> off(k), end(k), soff(k), send(k);
+        if (W.last_world_solver) {  // per-world solver: groups per colour summed over the worlds
+            bgpu::check_cuda(cudaMemcpyAsync(end.data(), pd.colour_count.p, k * 4, cudaMemcpyDeviceToHost, s), "d2h");
+            bgpu::check_cuda(cudaMemcpyAsync(send.data(), pd.split_count.p, k * 4, cudaMemcpyDeviceToHost, s), "d2h");
+            bgpu::check_cuda(cudaStreamSynchronize(s), "sync");
+            for (uint32_t c = 0; c < k; ++c) {
+                if (groups) groups[c] = end[c];
+                if (split_groups) split_groups[c] = send[c];
+            }
+            return BGPU_OK;
+        }
         bgpu::check_cuda(cudaMemcpyAsync(off.data(), pd.colour_offset.p, k * 4, cudaMemcpyDeviceToHost, s), "d2h");
         bgpu::check_cuda(cudaMemcpyAsync(end.data(), pd.colour_cursor.p, k * 4, cudaMemcpyDeviceToHost, s), "d2h");
         bgpu::check_cuda(cudaMemcpyAsync(soff.data(), pd.split_offset.p, k * 4, cudaMemcpyDeviceToHost, s), "d2h");

@@ -273,6 +273,33 @@ bgpu_status bgpu_batch_world_offsets(bgpu_world* w, uint32_t* offsets);
 /* Steps every world of the batch nsteps times (the same as bgpu_step). */
 bgpu_status bgpu_batch_step(bgpu_world* w, float dt, uint32_t nsteps);
 
+/* Launch shape of a batch's solver (no counterpart in the reference, which steps
+ * one PhysicsWorld at a time: world/step.rs:100). Each world's PGS runs inside
+ * one CTA, or one warp for worlds of at most warp_world_max_bodies bodies (the
+ * world's row groups coloured and solved with the bodies' velocities in shared
+ * memory, only block- or warp-local syncs between colour phases), with
+ * threads_per_cta threads per CTA (32..256). threads_per_cta 0 selects the
+ * global solver (one colouring and one cooperative PGS launch over all worlds).
+ * A batch with joints, or a world too large for one CTA's shared memory, uses the
+ * global solver. Either way each world equals its own sequential solve in the
+ * order bgpu_read_solve_order reports. The launch shape must not change between
+ * a tape's forward and backward passes. */
+typedef struct bgpu_batch_tuning {
+    uint32_t threads_per_cta;        /* 0: the global solver */
+    uint32_t warp_world_max_bodies;  /* worlds with at most this many bodies: one per warp */
+    uint32_t ctas;                   /* CTAs of the per-world launch (0: global solver in use) */
+    uint32_t candidates;             /* configurations timed by the last bgpu_batch_autotune (0: none) */
+    float ms_per_step;               /* the chosen configuration's device time per step then */
+    float global_ms_per_step;        /* the global solver's device time per step in the same run */
+} bgpu_batch_tuning;
+/* Autotuner: from the batch's current state, times steps_per_candidate steps of
+ * every candidate launch shape (threads per CTA 32 / 64 / 128 / 256 x warp-world
+ * limits 0 / 32 / 64 / 128 / all, and the global solver), keeps the fastest, and
+ * puts the batch back in the state it started from. out may be NULL. */
+bgpu_status bgpu_batch_autotune(bgpu_world* w, float dt, uint32_t steps_per_candidate, bgpu_batch_tuning* out);
+bgpu_status bgpu_batch_set_tuning(bgpu_world* w, uint32_t threads_per_cta, uint32_t warp_world_max_bodies);
+bgpu_status bgpu_batch_get_tuning(bgpu_world* w, bgpu_batch_tuning* out);
+
 /* Adjoint (no counterpart in the reference, whose world is not differentiable).
  * A tape steps its world forward, keeping a checkpoint of the world state every
  * checkpoint_every steps, then returns gradients of a loss of the final state with

@@ -124,3 +124,79 @@ def test_batched_worlds_recipe():
     assert b.num_dynamic == int(n.sum())
     s = b.world_scene(7)
     assert s.num_bodies == int(b.bodies_per_world[7])
+
+
+def _lockstep_batch(w, b, steps):
+    """Per-step parity of every world against its own oracle (state copied in before each step)."""
+    off = w.world_offsets().astype(np.int64)
+    oracles = [b.world_scene(k).build_oracle(orc) for k in range(len(b.worlds))]
+    for step in range(steps):
+        g0 = w.state()
+        for k, o in enumerate(oracles):
+            o.set_state(g0[off[k]:off[k + 1]].astype(np.float64))
+        w.step(b.dt)
+        st = w.stats()
+        assert st["device_status"] == 0, st
+        order = w.solve_order()
+        g = w.state()
+        pairs = w.pairs().astype(np.int64)
+        for k, o in enumerate(oracles):
+            lo, hi = int(off[k]), int(off[k + 1])
+            o.set_solve_order(_world_order(order, lo, hi))
+            o.step(b.dt)
+            r = o.state()
+            np.testing.assert_array_equal(g[lo:hi, 13], r[:, 13])
+            np.testing.assert_allclose(g[lo:hi, :13], r[:, :13], rtol=1e-5, atol=1e-6,
+                                       err_msg=f"step {step} world {k}")
+            sel = (pairs[:, 0] >= lo) & (pairs[:, 0] < hi)
+            np.testing.assert_array_equal(pairs[sel] - lo, o.pairs())
+
+
+@gpu_only
+@pytest.mark.parametrize("threads,warp_max", [(0, 0), (32, 1 << 30), (64, 32), (128, 64), (256, 0)])
+def test_batch_solver_launch_shapes_match_the_oracle(gpu, threads, warp_max):
+    """Every launch shape of the batch solver (the global solver; one world per warp; worlds
+    split between warps and whole CTAs; one world per CTA) solves each world in an order the
+    oracle replays to 1e-5 after every step."""
+    import scenes
+
+    b = scenes.batched_worlds(n_worlds=24, seed=13, steps=40, min_bodies=8, max_bodies=160)
+    w = b.build_gpu(gpu)
+    w.set_tuning(threads, warp_max)
+    t = w.tuning()
+    assert t["threads_per_cta"] == threads
+    assert (t["ctas"] > 0) == (threads > 0)
+    _lockstep_batch(w, b, 40)
+
+
+@gpu_only
+def test_batch_autotune_keeps_the_state_and_the_parity(gpu):
+    """The autotuner times every launch shape from one checkpoint and puts the batch back:
+    the state after tuning equals the state before, and stepping goes on in parity."""
+    import scenes
+
+    b = scenes.batched_worlds(n_worlds=48, seed=17, steps=30, min_bodies=8, max_bodies=200)
+    w = b.build_gpu(gpu)
+    w.step(b.dt, 20)
+    before = w.state()
+    t = w.autotune(b.dt, 2)
+    np.testing.assert_array_equal(w.state(), before)
+    assert t["candidates"] >= 2 and t["ms_per_step"] > 0.0 and t["global_ms_per_step"] > 0.0
+    assert t["threads_per_cta"] in (0, 32, 64, 128, 256)
+    assert t["ms_per_step"] <= t["global_ms_per_step"] * 1.0001
+    _lockstep_batch(w, b, 10)
+
+
+@gpu_only
+def test_batch_set_tuning_rejects_bad_shapes(gpu):
+    import bgpu
+    import scenes
+
+    b = scenes.batched_worlds(n_worlds=4, seed=1, steps=1)
+    w = b.build_gpu(gpu)
+    for bad in (16, 48, 512):
+        with pytest.raises(bgpu.BgpuError):
+            w.set_tuning(bad, 64)
+    plain = bgpu.World()
+    with pytest.raises(bgpu.BgpuError):
+        plain.set_tuning(128, 64)
