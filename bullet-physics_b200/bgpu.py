@@ -530,7 +530,6 @@ class World:
               "batch_add_worlds")
         return out.value
 
-    @property
     def autotune(self, dt, steps_per_candidate=3):
         """Batched worlds: time the solver's launch shapes from the current state, keep the fastest."""
         t = BatchTuning()
@@ -545,6 +544,7 @@ class World:
         check(self.L.bgpu_batch_get_tuning(self.h, ctypes.byref(t)), "batch_get_tuning")
         return t.as_dict()
 
+    @property
     def num_worlds(self):
         return self.L.bgpu_batch_num_worlds(self.h)
 

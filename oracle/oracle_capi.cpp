@@ -248,6 +248,82 @@ void orc_world_set_brute_force(void* p, int on) {
     DISPATCH(h, { w.brute_force_broadphase = on != 0; });
 }
 
+using Tri3 = std::array<uint32_t, 3>;  // (a typedef: the dispatch macro splits on template commas)
+
+// Static triangle mesh: nv vertices (xyz) and nt triangles (3 vertex indices each).
+uint32_t orc_world_add_mesh(void* p, const double* v, uint32_t nv, const uint32_t* idx, uint32_t nt) {
+    Handle* h = static_cast<Handle*>(p);
+    uint32_t r = 0;
+    DISPATCH(h, {
+        using R = std::remove_reference_t<decltype(w.gravity.x)>;
+        std::vector<V3<R>> verts;
+        for (uint32_t i = 0; i < nv; ++i)
+            verts.push_back(V3<R>(static_cast<R>(v[3 * i]), static_cast<R>(v[3 * i + 1]), static_cast<R>(v[3 * i + 2])));
+        std::vector<Tri3> tris(nt);
+        for (uint32_t t = 0; t < nt; ++t)
+            for (int k = 0; k < 3; ++k) tris[t][k] = idx[3 * t + k];
+        w.shapes.push_back(Shape<R>::triangle_mesh(verts, tris));
+        r = uint32_t(w.shapes.size() - 1);
+    });
+    return r;
+}
+
+// Heightfield (heightfield.rs:84-140): width x depth heights, cell size xyz, option bits.
+uint32_t orc_world_add_heightfield(void* p, const double* heights, uint32_t width, uint32_t depth, const double* cell,
+                                   uint32_t options) {
+    Handle* h = static_cast<Handle*>(p);
+    uint32_t r = 0;
+    DISPATCH(h, {
+        using R = std::remove_reference_t<decltype(w.gravity.x)>;
+        std::vector<R> hv(size_t(width) * depth);
+        for (size_t i = 0; i < hv.size(); ++i) hv[i] = static_cast<R>(heights[i]);
+        V3<R> c(static_cast<R>(cell[0]), static_cast<R>(cell[1]), static_cast<R>(cell[2]));
+        w.shapes.push_back(Shape<R>::heightfield(hv, width, depth, c, options));
+        r = uint32_t(w.shapes.size() - 1);
+    });
+    return r;
+}
+
+// The triangles of a mesh shape (after any heightfield construction): vertices and indices.
+uint32_t orc_mesh_counts(void* p, uint32_t s, uint32_t* nv) {
+    Handle* h = static_cast<Handle*>(p);
+    uint32_t nt = 0;
+    DISPATCH(h, {
+        const auto& m = *w.shapes[s].mesh;
+        *nv = uint32_t(m.vertices.size());
+        nt = uint32_t(m.indices.size());
+    });
+    return nt;
+}
+
+void orc_mesh_data(void* p, uint32_t s, double* v, uint32_t* idx) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, {
+        const auto& m = *w.shapes[s].mesh;
+        for (size_t i = 0; i < m.vertices.size(); ++i) {
+            v[3 * i] = m.vertices[i].x; v[3 * i + 1] = m.vertices[i].y; v[3 * i + 2] = m.vertices[i].z;
+        }
+        for (size_t t = 0; t < m.indices.size(); ++t)
+            for (int k = 0; k < 3; ++k) idx[3 * t + k] = m.indices[t][k];
+    });
+}
+
+// BVH query of a mesh shape (bvh.rs:45-66): candidate triangles in walk order; returns the count.
+uint32_t orc_mesh_query(void* p, uint32_t s, const double* box6, uint32_t* out, uint32_t cap) {
+    Handle* h = static_cast<Handle*>(p);
+    uint32_t n = 0;
+    DISPATCH(h, {
+        using R = std::remove_reference_t<decltype(w.gravity.x)>;
+        Aabb<R> q(V3<R>(static_cast<R>(box6[0]), static_cast<R>(box6[1]), static_cast<R>(box6[2])),
+                  V3<R>(static_cast<R>(box6[3]), static_cast<R>(box6[4]), static_cast<R>(box6[5])));
+        std::vector<uint32_t> c;
+        w.shapes[s].mesh->triangles_in_aabb(q, c);
+        n = uint32_t(c.size());
+        for (uint32_t i = 0; i < n && i < cap; ++i) out[i] = c[i];
+    });
+    return n;
+}
+
 uint32_t orc_world_add_shape(void* p, uint32_t type, const double* params, const double* pts, uint32_t npts) {
     Handle* h = static_cast<Handle*>(p);
     uint32_t r = 0;

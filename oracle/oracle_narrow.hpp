@@ -844,13 +844,166 @@ bool convex_convex(const Shape<R>& sa, const V3<R>& pa, const Quat<R>& qa, const
     return true;
 }
 
-// narrowphase/mod.rs:63-286 (rigid convex/plane subset: no compounds/meshes).
+// manifold.rs:80-108 (ContactManifold::reduce): the deepest point first (stable sort by
+// penetration, deepest first), then greedily the candidate farthest from the kept points.
+template <class R>
+void reduce_manifold(Manifold<R>& m, size_t max) {
+    if (m.points.size() <= max) return;
+    std::vector<ContactPoint<R>> cand = m.points;
+    std::stable_sort(cand.begin(), cand.end(),
+                     [](const ContactPoint<R>& a, const ContactPoint<R>& b) { return a.penetration > b.penetration; });
+    std::vector<ContactPoint<R>> kept{cand[0]};
+    std::vector<char> used(cand.size(), 0);
+    used[0] = 1;
+    while (kept.size() < max) {
+        size_t best = 0;
+        R best_sep = -std::numeric_limits<R>::infinity();
+        for (size_t i = 0; i < cand.size(); ++i) {
+            if (used[i]) continue;
+            R sep = std::numeric_limits<R>::infinity();
+            for (auto& q : kept) sep = std::min(sep, (cand[i].position - q.position).length_squared());
+            if (sep > best_sep) { best_sep = sep; best = i; }
+        }
+        kept.push_back(cand[best]);
+        used[best] = 1;
+    }
+    m.points = kept;
+}
+
+// convex_mesh.rs:236-253 (segment_closest_point_sq)
+template <class R>
+R segment_closest_point_sq(const V3<R>& from, const V3<R>& to, const V3<R>& p, V3<R>& nearest) {
+    V3<R> v = to - from;
+    R t = v.dot(p - from);
+    if (t > R(0)) {
+        R dvv = v.dot(v);
+        if (t < dvv) t /= dvv;
+        else t = R(1);
+    } else {
+        t = R(0);
+    }
+    nearest = from + v * t;
+    return (p - nearest).length_squared();
+}
+
+// convex_mesh.rs:257-268 (point_in_triangle)
+template <class R>
+bool point_in_triangle(const V3<R>& p, const V3<R>& v1, const V3<R>& v2, const V3<R>& v3, const V3<R>& n) {
+    V3<R> e1 = v2 - v1, e2 = v3 - v2, e3 = v1 - v3;
+    R r1 = e1.cross(n).dot(p - v1), r2 = e2.cross(n).dot(p - v2), r3 = e3.cross(n).dot(p - v3);
+    return (r1 > R(0) && r2 > R(0) && r3 > R(0)) || (r1 <= R(0) && r2 <= R(0) && r3 <= R(0));
+}
+
+// convex_mesh.rs:160-232 (sphere_triangle_contact): point on the triangle, normal toward the
+// sphere centre, penetration radius - distance.
+template <class R>
+bool sphere_triangle_contact(const V3<R>& center, R radius, R threshold, const V3<R>& a, const V3<R>& b,
+                             const V3<R>& c, V3<R>& point, V3<R>& normal_out, R& pen) {
+    const R rwt = radius + threshold;
+    V3<R> normal = (b - a).cross(c - a);
+    R l2 = normal.length_squared();
+    if (l2 < Consts<R>::EPS * Consts<R>::EPS) return false;
+    normal = normal * (R(1) / std::sqrt(l2));
+    R dist = normal.dot(center - a);
+    if (dist < R(0)) {
+        dist = -dist;
+        normal = -normal;
+    }
+    if (dist >= rwt) return false;
+    V3<R> cp;
+    if (point_in_triangle(center, a, b, c, normal)) {
+        cp = center - normal * dist;
+    } else {
+        R min_d = rwt * rwt;
+        bool found = false;
+        const V3<R>* ends[3][2] = {{&a, &b}, {&b, &c}, {&c, &a}};
+        for (auto& e : ends) {
+            V3<R> on;
+            R d = segment_closest_point_sq(*e[0], *e[1], center, on);
+            if (d < min_d) { min_d = d; cp = on; found = true; }
+        }
+        if (!found) return false;
+    }
+    V3<R> to_c = center - cp;
+    R d2 = to_c.length_squared();
+    if (d2 >= rwt * rwt) return false;
+    point = cp;
+    if (d2 > Consts<R>::EPS) {
+        R d = std::sqrt(d2);
+        normal_out = to_c * (R(1) / d);
+        pen = radius - d;
+    } else {
+        normal_out = normal;
+        pen = radius;
+    }
+    return true;
+}
+
+// convex_mesh.rs:26-153: the convex's world AABB swept into the mesh frame picks candidate
+// triangles from the BVH; each candidate whose own AABB overlaps goes through the sphere
+// detector or convex_convex against the triangle as a three-vertex hull; at most four points
+// survive (reduce). Normals point from the convex to the mesh. (The internal-edge fix runs
+// only for meshes whose edge info was generated, which nothing here does.)
+template <class R>
+bool convex_mesh(const Shape<R>& cv, const V3<R>& pc, const Quat<R>& qc, const Shape<R>& ms, const V3<R>& pm,
+                 const Quat<R>& qm, bool has_seed, const V3<R>& seed, R threshold, Manifold<R>& out) {
+    Aabb<R> cw = cv.world_aabb(pc, qc);
+    Quat<R> inv_m = qm.inverse();
+    V3<R> lmin = V3<R>::splat(std::numeric_limits<R>::infinity());
+    V3<R> lmax = V3<R>::splat(-std::numeric_limits<R>::infinity());
+    V3<R> c = cw.center(), e = cw.extents();
+    for (int i = 0; i < 8; ++i) {
+        V3<R> corner((i & 1) == 0 ? c.x + e.x : c.x - e.x, (i & 2) == 0 ? c.y + e.y : c.y - e.y,
+                     (i & 4) == 0 ? c.z + e.z : c.z - e.z);
+        V3<R> p = inv_m.rotate(corner - pm);
+        lmin = lmin.min(p);
+        lmax = lmax.max(p);
+    }
+    Aabb<R> query(lmin, lmax);
+    const MeshData<R>& md = *ms.mesh;
+    std::vector<uint32_t> cand;
+    md.triangles_in_aabb(query, cand);
+    out.points.clear();
+    if (cv.type == SHAPE_SPHERE) {
+        V3<R> center = inv_m.rotate(pc - pm);
+        for (uint32_t t : cand) {
+            if (!md.tri_aabbs[t].overlaps(query)) continue;
+            V3<R> pt, nl;
+            R pen;
+            if (sphere_triangle_contact(center, cv.radius, threshold, md.tri_vertex(t, 0), md.tri_vertex(t, 1),
+                                        md.tri_vertex(t, 2), pt, nl, pen))
+                out.points.push_back(ContactPoint<R>(pm + qm.rotate(pt), qm.rotate(-nl), pen));
+        }
+    } else {
+        for (uint32_t t : cand) {
+            if (!md.tri_aabbs[t].overlaps(query)) continue;
+            Manifold<R> m;
+            if (convex_convex(cv, pc, qc, (*ms.tri_hulls)[t], pm, qm, has_seed, seed, threshold, m))
+                for (auto& pt : m.points) out.points.push_back(pt);
+        }
+    }
+    if (out.points.empty()) return false;
+    reduce_manifold(out, 4);
+    return true;
+}
+
+// narrowphase/mod.rs:63-286 (rigid convex/plane subset plus convex-vs-static-mesh: no compounds;
+// mesh-mesh and plane-mesh pairs are two static bodies here, which the pair pass never collides).
 template <class R>
 bool collide(const Shape<R>& sa, const V3<R>& pa, const Quat<R>& qa, const Shape<R>& sb, const V3<R>& pb,
              const Quat<R>& qb, bool has_seed, const V3<R>& seed, Manifold<R>& out) {
     R thr = pair_threshold(sa, sb);
     out.points.clear();
     if (sa.type == SHAPE_PLANE && sb.type == SHAPE_PLANE) return false;
+    if (sa.type == SHAPE_MESH || sb.type == SHAPE_MESH) {  // mod.rs:102-243
+        if (sa.type == SHAPE_MESH && sb.is_convex()) {
+            bool r = convex_mesh(sb, pb, qb, sa, pa, qa, has_seed, seed, thr, out);
+            if (r) out.flip();
+            return r;
+        }
+        if (sb.type == SHAPE_MESH && sa.is_convex()) return convex_mesh(sa, pa, qa, sb, pb, qb, has_seed, seed, thr, out);
+        return false;
+    }
     if (sa.type == SHAPE_PLANE) return plane_convex(sa, pa, qa, sb, pb, qb, thr, out);
     if (sb.type == SHAPE_PLANE) {
         bool r = plane_convex(sb, pb, qb, sa, pa, qa, thr, out);

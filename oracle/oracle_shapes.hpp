@@ -1,12 +1,126 @@
 // CPU oracle — TEST INFRASTRUCTURE ONLY (see oracle_math.hpp).
 // Shapes restated from crates/bullet-collision/src/shapes/{mod,box_shape,
-// sphere,capsule,convex_hull,plane}.rs.
+// sphere,capsule,convex_hull,plane,triangle_mesh,bvh,heightfield}.rs.
 #pragma once
+#include <algorithm>
+#include <array>
+#include <memory>
 #include "oracle_math.hpp"
 
 namespace oracle {
 
-enum ShapeType : uint32_t { SHAPE_SPHERE = 0, SHAPE_BOX = 1, SHAPE_CAPSULE = 2, SHAPE_HULL = 3, SHAPE_PLANE = 4 };
+enum ShapeType : uint32_t { SHAPE_SPHERE = 0, SHAPE_BOX = 1, SHAPE_CAPSULE = 2, SHAPE_HULL = 3, SHAPE_PLANE = 4,
+                            SHAPE_MESH = 5 };
+
+// util.rs:106-126 (Aabb::transformed): the eight corners of centre +- extents, rotated and moved.
+template <class R>
+Aabb<R> aabb_transformed(const Aabb<R>& a, const V3<R>& p, const Quat<R>& q) {
+    V3<R> c = a.center(), e = a.extents();
+    V3<R> mn = V3<R>::splat(std::numeric_limits<R>::infinity());
+    V3<R> mx = V3<R>::splat(-std::numeric_limits<R>::infinity());
+    for (int i = 0; i < 8; ++i) {
+        V3<R> corner((i & 1) == 0 ? c.x + e.x : c.x - e.x, (i & 2) == 0 ? c.y + e.y : c.y - e.y,
+                     (i & 4) == 0 ? c.z + e.z : c.z - e.z);
+        V3<R> w = q.rotate(corner) + p;
+        mn = mn.min(w);
+        mx = mx.max(w);
+    }
+    return Aabb<R>(mn, mx);
+}
+
+// Static triangle mesh (triangle_mesh.rs:34-123) with its BVH (bvh.rs:16-206): nodes in
+// pre-order, internal nodes with a child pair, leaves with a range of the triangle
+// permutation; longest-axis median split of the triangle centres, at most 4 per leaf.
+template <class R>
+struct MeshData {
+    struct Node {
+        Aabb<R> aabb;
+        bool leaf = true;
+        uint32_t a = 0, b = 0;  // leaf: start, count; internal: left, right
+    };
+    std::vector<V3<R>> vertices;
+    std::vector<std::array<uint32_t, 3>> indices;
+    std::vector<Node> nodes;
+    std::vector<uint32_t> tri_order;
+    std::vector<Aabb<R>> tri_aabbs;
+    Aabb<R> local_bounds;
+
+    V3<R> tri_vertex(uint32_t t, int k) const { return vertices[indices[t][k]]; }
+    V3<R> center(uint32_t t) const {  // bvh.rs:248-251
+        return (tri_vertex(t, 0) + tri_vertex(t, 1) + tri_vertex(t, 2)) * (R(1) / R(3));
+    }
+    // bvh.rs:210-225
+    Aabb<R> slice_aabb(uint32_t start, uint32_t count) const {
+        bool have = false;
+        Aabb<R> a{V3<R>(), V3<R>()};
+        for (uint32_t k = start; k < start + count; ++k)
+            for (int v = 0; v < 3; ++v) {
+                V3<R> p = tri_vertex(tri_order[k], v);
+                if (!have) { a = Aabb<R>(p, p); have = true; }
+                else a = Aabb<R>(a.min.min(p), a.max.max(p));
+            }
+        return a;
+    }
+    // bvh.rs:171-203
+    uint32_t build_node(uint32_t start, uint32_t count) {
+        Aabb<R> aabb = slice_aabb(start, count);
+        uint32_t index = uint32_t(nodes.size());
+        Node nd;
+        nd.aabb = aabb;
+        nd.leaf = true;
+        nd.a = start;
+        nd.b = count;
+        nodes.push_back(nd);
+        if (count <= 4) return index;
+        V3<R> e = aabb.extents();  // bvh.rs:255-268 longest_axis: first strict maximum
+        int axis = 0;
+        R mx = e.x;
+        if (e.y > mx) { axis = 1; mx = e.y; }
+        if (e.z > mx) axis = 2;
+        auto comp = [&](uint32_t t) { V3<R> c = center(t); return axis == 0 ? c.x : (axis == 1 ? c.y : c.z); };
+        std::stable_sort(tri_order.begin() + start, tri_order.begin() + start + count,
+                         [&](uint32_t x, uint32_t y) { return comp(x) < comp(y); });
+        uint32_t mid = count / 2;
+        uint32_t left = build_node(start, mid);
+        uint32_t right = build_node(start + mid, count - mid);
+        nodes[index].leaf = false;
+        nodes[index].a = left;
+        nodes[index].b = right;
+        return index;
+    }
+    void build() {
+        tri_order.resize(indices.size());
+        for (uint32_t t = 0; t < tri_order.size(); ++t) tri_order[t] = t;
+        nodes.clear();
+        build_node(0, uint32_t(indices.size()));
+        tri_aabbs.clear();
+        for (uint32_t t = 0; t < indices.size(); ++t) {  // triangle_mesh.rs:98-112
+            V3<R> a = tri_vertex(t, 0), b = tri_vertex(t, 1), c = tri_vertex(t, 2);
+            tri_aabbs.push_back(Aabb<R>(a.min(b.min(c)), a.max(b.max(c))));
+            local_bounds = t == 0 ? tri_aabbs[0] : Aabb<R>(local_bounds.min.min(tri_aabbs[t].min),
+                                                           local_bounds.max.max(tri_aabbs[t].max));
+        }
+        if (indices.empty()) local_bounds = Aabb<R>(V3<R>(), V3<R>());
+    }
+    // bvh.rs:45-66: stack walk (left pushed first, so the right child pops first).
+    void triangles_in_aabb(const Aabb<R>& q, std::vector<uint32_t>& out) const {
+        out.clear();
+        if (nodes.empty()) return;
+        std::vector<uint32_t> stack{0u};
+        while (!stack.empty()) {
+            uint32_t k = stack.back();
+            stack.pop_back();
+            const Node& n = nodes[k];
+            if (!n.aabb.overlaps(q)) continue;
+            if (!n.leaf) {
+                stack.push_back(n.a);
+                stack.push_back(n.b);
+            } else {
+                for (uint32_t i = n.a; i < n.a + n.b; ++i) out.push_back(tri_order[i]);
+            }
+        }
+    }
+};
 
 // manifold.rs:8
 template <class R> constexpr R CONTACT_BREAKING_THRESHOLD = R(0.02);
@@ -21,6 +135,8 @@ struct Shape {
     R constant = 0;        // plane
     std::vector<V3<R>> points;  // hull
     Aabb<R> hull_bounds;        // convex_hull.rs:22-34
+    std::shared_ptr<MeshData<R>> mesh;            // triangle mesh / heightfield (static only)
+    std::shared_ptr<std::vector<Shape>> tri_hulls;  // triangle_mesh.rs:94-104: 3-vertex hulls
 
     static Shape sphere(R r) { Shape s; s.type = SHAPE_SPHERE; s.radius = r; return s; }
     static Shape box(const V3<R>& h) { Shape s; s.type = SHAPE_BOX; s.half = h; return s; }
@@ -37,7 +153,58 @@ struct Shape {
         return s;
     }
 
-    bool is_convex() const { return type != SHAPE_PLANE; }
+    // triangle_mesh.rs:85-123 (one part): vertices, triangles, BVH, per-triangle hulls and boxes.
+    static Shape triangle_mesh(const std::vector<V3<R>>& v, const std::vector<std::array<uint32_t, 3>>& idx) {
+        Shape s;
+        s.type = SHAPE_MESH;
+        s.mesh = std::make_shared<MeshData<R>>();
+        s.mesh->vertices = v;
+        s.mesh->indices = idx;
+        s.mesh->build();
+        s.tri_hulls = std::make_shared<std::vector<Shape>>();
+        for (uint32_t t = 0; t < idx.size(); ++t)
+            s.tri_hulls->push_back(hull({s.mesh->tri_vertex(t, 0), s.mesh->tri_vertex(t, 1), s.mesh->tri_vertex(t, 2)}));
+        return s;
+    }
+    // heightfield.rs:84-140: a width x depth row-major grid centred on the origin, heights
+    // offset by the min/max midpoint, two triangles per cell. options: bit 0 flip quad edges,
+    // bit 1 diamond subdivision, bit 2 zigzag subdivision, bit 3 flip winding; up axis in bits 4-5
+    // (0 X, 1 Y, 2 Z).
+    static Shape heightfield(const std::vector<R>& h, uint32_t width, uint32_t depth, const V3<R>& cell,
+                             uint32_t options) {
+        R mn = std::numeric_limits<R>::infinity(), mx = -std::numeric_limits<R>::infinity();
+        for (R x : h) { mn = std::min(mn, x); mx = std::max(mx, x); }
+        R mid = (mn + mx) * R(0.5);
+        const uint32_t up = (options >> 4) & 3u;
+        std::vector<V3<R>> v;
+        for (uint32_t y = 0; y < depth; ++y)
+            for (uint32_t x = 0; x < width; ++x) {
+                R hh = h[size_t(y) * width + x] - mid;
+                R u = (R(x) - R(width - 1) * R(0.5)) * cell.x;
+                R w = (R(y) - R(depth - 1) * R(0.5)) * cell.z;
+                v.push_back(up == 0 ? V3<R>(hh, u, w) : (up == 1 ? V3<R>(u, hh, w) : V3<R>(u, w, hh)));
+            }
+        const bool flip_edges = options & 1u, diamond = options & 2u, zigzag = options & 4u, flip_wind = options & 8u;
+        auto wind = [&](std::array<uint32_t, 3> t) {
+            return flip_wind ? std::array<uint32_t, 3>{t[2], t[1], t[0]} : t;
+        };
+        std::vector<std::array<uint32_t, 3>> idx;
+        for (uint32_t y = 0; y + 1 < depth; ++y)
+            for (uint32_t x = 0; x + 1 < width; ++x) {
+                uint32_t v00 = y * width + x, v10 = v00 + 1, v01 = v00 + width, v11 = v01 + 1;
+                bool flipped = flip_edges || (diamond && ((y + x) & 1u) == 0) || (zigzag && (y & 1u) == 0);
+                if (flipped) {
+                    idx.push_back(wind({v00, v01, v11}));
+                    idx.push_back(wind({v00, v11, v10}));
+                } else {
+                    idx.push_back(wind({v00, v01, v10}));
+                    idx.push_back(wind({v10, v01, v11}));
+                }
+            }
+        return triangle_mesh(v, idx);
+    }
+
+    bool is_convex() const { return type != SHAPE_PLANE && type != SHAPE_MESH; }
 
     // shapes/mod.rs:236-251; box_shape.rs:20-22 (0.04); sphere.rs:18-20 (r);
     // capsule.rs:27-29 (r); convex_hull.rs:43-45 (0); plane.rs:26-28 (0).
@@ -60,6 +227,7 @@ struct Shape {
                 return Aabb<R>(-r, r);
             }
             case SHAPE_HULL: return hull_bounds;
+            case SHAPE_MESH: return mesh->local_bounds;  // triangle_mesh.rs:209-211
             default: return Aabb<R>(V3<R>::splat(R(-1e30)), V3<R>::splat(R(1e30)));
         }
     }
@@ -155,6 +323,7 @@ struct Shape {
                          p.z + support_local(uz).dot(uz));
                 return Aabb<R>(mn, mx);
             }
+            case SHAPE_MESH: return aabb_transformed(mesh->local_bounds, p, q);  // triangle_mesh.rs:213-216
             default: return local_aabb();  // plane.rs:38-40
         }
     }

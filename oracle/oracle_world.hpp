@@ -520,7 +520,8 @@ void sweep_pairs(const std::vector<Aabb<R>>& aabbs, std::vector<std::pair<uint32
 // larger than 1e15 (planes) are tested against everything. Exact 3-axis closed
 // overlap filter, lexicographic output.
 template <class R>
-void grid_pairs(const std::vector<Aabb<R>>& aabbs, std::vector<std::pair<uint32_t, uint32_t>>& out) {
+void grid_pairs(const std::vector<Aabb<R>>& aabbs, std::vector<std::pair<uint32_t, uint32_t>>& out,
+                const std::vector<char>* force_big = nullptr) {
     out.clear();
     const size_t n = aabbs.size();
     std::vector<uint32_t> big, small;
@@ -529,7 +530,8 @@ void grid_pairs(const std::vector<Aabb<R>>& aabbs, std::vector<std::pair<uint32_
     for (size_t i = 0; i < n; ++i) {
         const Aabb<R>& a = aabbs[i];
         R ex = std::max(std::max(a.max.x - a.min.x, a.max.y - a.min.y), a.max.z - a.min.z);
-        if (!(ex < R(1e15))) { big.push_back(uint32_t(i)); continue; }
+        // unbounded proxies, and the caller's large ones (static meshes), are tested against all
+        if (!(ex < R(1e15)) || (force_big && (*force_big)[i])) { big.push_back(uint32_t(i)); continue; }
         small.push_back(uint32_t(i));
         cell = std::max(cell, ex);
         lo = lo.min(a.min);
@@ -763,7 +765,11 @@ struct World {
         // 4. broad phase (step.rs:413-415)
         std::vector<std::pair<uint32_t, uint32_t>> pairs;
         if (brute_force_broadphase) brute_force_pairs(proxy_aabbs, pairs);
-        else grid_pairs(proxy_aabbs, pairs);
+        else {
+            std::vector<char> mesh_proxy(bodies.size(), 0);
+            for (size_t i = 0; i < bodies.size(); ++i) mesh_proxy[i] = shapes[bodies[i].shape].type == SHAPE_MESH;
+            grid_pairs(proxy_aabbs, pairs, &mesh_proxy);
+        }
         clk_mark(2);
         // 4b. islands (step.rs:423)
         step_islands(pairs);
