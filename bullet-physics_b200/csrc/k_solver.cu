@@ -1299,9 +1299,9 @@ bool build_world_plan(const std::vector<uint32_t>& world_off, uint32_t block, ui
         check_cuda(cudaMemcpyAsync(plan.cta.p, cta.data(), cta.size() * sizeof(uint2), cudaMemcpyHostToDevice, s), "h2d");
     if (nw) check_cuda(cudaMemcpyAsync(plan.list.p, order.data(), nw * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "h2d");
     check_cuda(cudaStreamSynchronize(s), "sync");  // the host vectors go out of scope
-    if (smem > 48u * 1024u)
-        check_cuda(cudaFuncSetAttribute((const void*)k_world_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        int(smem)), "smem attribute");
+    // Without this opt-in, dynamic shared memory is limited to 48 KB minus the kernel's static part.
+    check_cuda(cudaFuncSetAttribute((const void*)k_world_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(smem)), "smem attribute");
     plan.ncta = uint32_t(cta.size());
     plan.block = block;
     plan.tau = tau;
