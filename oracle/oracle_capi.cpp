@@ -654,6 +654,25 @@ int orc_convex_convex(void* p, uint32_t sa, const double* pose_a, uint32_t sb, c
     return r;
 }
 
+// convex_mesh.rs:160-232 on its own: out = point3, normal3 (toward the centre), penetration.
+int orc_sphere_triangle(int f64, const double* center, double radius, double threshold, const double* tri9,
+                        double* out7) {
+    auto run = [&](auto zero) -> int {
+        using R = decltype(zero);
+        auto v = [&](const double* d) { return V3<R>(static_cast<R>(d[0]), static_cast<R>(d[1]), static_cast<R>(d[2])); };
+        V3<R> pt, n;
+        R pen;
+        if (!sphere_triangle_contact(v(center), static_cast<R>(radius), static_cast<R>(threshold), v(tri9), v(tri9 + 3),
+                                     v(tri9 + 6), pt, n, pen))
+            return 0;
+        out7[0] = pt.x; out7[1] = pt.y; out7[2] = pt.z;
+        out7[3] = n.x; out7[4] = n.y; out7[5] = n.z;
+        out7[6] = pen;
+        return 1;
+    };
+    return f64 ? run(0.0) : run(0.0f);
+}
+
 int orc_gjk_kind(void* p, uint32_t sa, const double* pose_a, uint32_t sb, const double* pose_b) {
     Handle* h = static_cast<Handle*>(p);
     int r = 0;

@@ -169,7 +169,7 @@ struct Shape {
     // heightfield.rs:84-140: a width x depth row-major grid centred on the origin, heights
     // offset by the min/max midpoint, two triangles per cell. options: bit 0 flip quad edges,
     // bit 1 diamond subdivision, bit 2 zigzag subdivision, bit 3 flip winding; up axis in bits 4-5
-    // (0 X, 1 Y, 2 Z).
+    // (0 Y, the default; 1 X; 2 Z).
     static Shape heightfield(const std::vector<R>& h, uint32_t width, uint32_t depth, const V3<R>& cell,
                              uint32_t options) {
         R mn = std::numeric_limits<R>::infinity(), mx = -std::numeric_limits<R>::infinity();
@@ -182,7 +182,7 @@ struct Shape {
                 R hh = h[size_t(y) * width + x] - mid;
                 R u = (R(x) - R(width - 1) * R(0.5)) * cell.x;
                 R w = (R(y) - R(depth - 1) * R(0.5)) * cell.z;
-                v.push_back(up == 0 ? V3<R>(hh, u, w) : (up == 1 ? V3<R>(u, hh, w) : V3<R>(u, w, hh)));
+                v.push_back(up == 1 ? V3<R>(hh, u, w) : (up == 2 ? V3<R>(u, w, hh) : V3<R>(u, hh, w)));
             }
         const bool flip_edges = options & 1u, diamond = options & 2u, zigzag = options & 4u, flip_wind = options & 8u;
         auto wind = [&](std::array<uint32_t, 3> t) {

@@ -11,7 +11,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(ROOT, "oracle", "liboracle.so")
 
-SPHERE, BOX, CAPSULE, HULL, PLANE = 0, 1, 2, 3, 4
+SPHERE, BOX, CAPSULE, HULL, PLANE, MESH = 0, 1, 2, 3, 4, 5
 ACTIVE, ISLAND_SLEEPING, WANTS_DEACTIVATION, DISABLE_DEACTIVATION, DISABLE_SIMULATION = 1, 2, 3, 4, 5
 NO_CONTACT_RESPONSE, DISABLE_WORLD_GRAVITY, KINEMATIC = 0x1, 0x2, 0x4
 
@@ -79,6 +79,12 @@ def lib():
             "orc_world_set_ccd": (None, [P, U32, ctypes.c_double, ctypes.c_double]),
             "orc_world_ccd_clamps": (None, [P, D]),
             "orc_spring2_angle_info": (None, [ctypes.c_int, D, D, U32, D]),
+            "orc_world_add_mesh": (U32, [P, D, U32, ctypes.POINTER(U32), U32]),
+            "orc_world_add_heightfield": (U32, [P, D, U32, U32, D, U32]),
+            "orc_mesh_counts": (U32, [P, U32, ctypes.POINTER(U32)]),
+            "orc_mesh_data": (None, [P, U32, D, ctypes.POINTER(U32)]),
+            "orc_mesh_query": (U32, [P, U32, D, ctypes.POINTER(U32), U32]),
+            "orc_sphere_triangle": (ctypes.c_int, [ctypes.c_int, D, ctypes.c_double, ctypes.c_double, D, D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -239,6 +245,33 @@ class OracleWorld:
 
     def hull(self, pts):
         return self.add_shape(HULL, [], pts)
+
+    def mesh(self, vertices, indices):
+        """Static triangle mesh (triangle_mesh.rs:59-123): vertices n x 3, triangles m x 3."""
+        v = f64(np.asarray(vertices).reshape(-1, 3))
+        i = np.ascontiguousarray(np.asarray(indices).reshape(-1, 3), dtype=np.uint32)
+        return self.L.orc_world_add_mesh(self.h, dptr(v), len(v), i.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                         len(i))
+
+    def heightfield(self, heights, width, depth, cell=(1.0, 1.0, 1.0), options=0):
+        """Heightfield (heightfield.rs:84-140); options: 1 flip quad edges, 2 diamond, 4 zigzag,
+        8 flip winding, up axis << 4 (0 Y, the default; 1 X; 2 Z)."""
+        h = f64(np.asarray(heights).reshape(-1))
+        return self.L.orc_world_add_heightfield(self.h, dptr(h), width, depth, dptr(f64(cell)), options)
+
+    def mesh_data(self, s):
+        nv = ctypes.c_uint32(0)
+        nt = self.L.orc_mesh_counts(self.h, s, ctypes.byref(nv))
+        v = np.zeros((nv.value, 3))
+        i = np.zeros((nt, 3), dtype=np.uint32)
+        self.L.orc_mesh_data(self.h, s, dptr(v), i.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+        return v, i
+
+    def mesh_query(self, s, box6):
+        out = np.zeros(4096, dtype=np.uint32)
+        n = self.L.orc_mesh_query(self.h, s, dptr(f64(box6)), out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                  len(out))
+        return out[:n]
 
     def threshold(self, s):
         return self.L.orc_shape_threshold(self.h, s)
@@ -420,3 +453,12 @@ def interpolate_pose(pos, quat, linvel, angvel, dt, precision="f32"):
     out = np.zeros(7)
     lib().orc_interpolate_pose(1 if precision == "f64" else 0, dptr(inp), dt, dptr(out))
     return out
+
+
+def sphere_triangle(center, radius, threshold, a, b, c, precision="f32"):
+    """convex_mesh.rs:160-232: (point, normal toward the centre, penetration) or None."""
+    out = np.zeros(7)
+    tri = f64(np.concatenate([a, b, c]))
+    n = lib().orc_sphere_triangle(1 if precision == "f64" else 0, dptr(f64(center)), radius, threshold, dptr(tri),
+                                  dptr(out))
+    return (out[0:3], out[3:6], out[6]) if n else None

@@ -126,10 +126,13 @@ def test_batched_worlds_recipe():
     assert s.num_bodies == int(b.bodies_per_world[7])
 
 
-def _lockstep_batch(w, b, steps):
-    """Per-step parity of every world against its own oracle (state copied in before each step)."""
+def _lockstep_batch(w, b, steps, oracles=None):
+    """Per-step parity of every world against its own oracle (state copied in before each step;
+    the oracles must have stepped alongside the device world from the start, so that both hold
+    the same manifold caches). Returns the oracles."""
     off = w.world_offsets().astype(np.int64)
-    oracles = [b.world_scene(k).build_oracle(orc) for k in range(len(b.worlds))]
+    if oracles is None:
+        oracles = [b.world_scene(k).build_oracle(orc) for k in range(len(b.worlds))]
     for step in range(steps):
         g0 = w.state()
         for k, o in enumerate(oracles):
@@ -150,6 +153,7 @@ def _lockstep_batch(w, b, steps):
                                        err_msg=f"step {step} world {k}")
             sel = (pairs[:, 0] >= lo) & (pairs[:, 0] < hi)
             np.testing.assert_array_equal(pairs[sel] - lo, o.pairs())
+    return oracles
 
 
 @gpu_only
@@ -177,14 +181,14 @@ def test_batch_autotune_keeps_the_state_and_the_parity(gpu):
 
     b = scenes.batched_worlds(n_worlds=48, seed=17, steps=30, min_bodies=8, max_bodies=200)
     w = b.build_gpu(gpu)
-    w.step(b.dt, 20)
+    oracles = _lockstep_batch(w, b, 20)
     before = w.state()
     t = w.autotune(b.dt, 2)
     np.testing.assert_array_equal(w.state(), before)
     assert t["candidates"] >= 2 and t["ms_per_step"] > 0.0 and t["global_ms_per_step"] > 0.0
     assert t["threads_per_cta"] in (0, 32, 64, 128, 256)
     assert t["ms_per_step"] <= t["global_ms_per_step"] * 1.0001
-    _lockstep_batch(w, b, 10)
+    _lockstep_batch(w, b, 10, oracles)  # the manifold caches came back with the state
 
 
 @gpu_only
