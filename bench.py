@@ -58,6 +58,7 @@ def parse():
     p.add_argument("--stack-steps", type=int, default=300, help="1,000-box stack leg: steps (0: skip)")
     p.add_argument("--mixed-steps", type=int, default=300, help="16,384-body mixed convex leg: steps (0: skip)")
     p.add_argument("--drift-steps", type=int, default=300, help="f64 drift report: steps (0: skip)")
+    p.add_argument("--mesh-frames", type=int, default=300, help="terrain-mesh legs: frames (0: skip)")
     a = p.parse_args()
     if a.preroll is None:
         a.preroll = max(0, 600 - a.warmup - a.steps)
@@ -373,6 +374,22 @@ def bench_mixed(bgpu, scenes, steps):
                                  f"15% hulls, 10 iterations, dt 1/60, {steps} steps", steps)
 
 
+def bench_mesh_rain(bgpu, scenes, frames=300):
+    """Triangle-mesh legs: the reference's rain_500 and dbvt_rain_2000 perf scenes (mixed convex
+    raining onto a wavy terrain mesh, tools/perf_scenes.json), all `frames` frames from the
+    start, device time; the reference's own published CPU frame times quoted beside."""
+    out = []
+    for nx, grid, name, rust, bullet in ((10, 20, "rain_500", 1.253, 3.470), (20, 40, "dbvt_rain_2000", 5.988, 17.893)):
+        sc = scenes.mesh_rain(nx=nx, nz=nx, layers=5, grid=grid, steps=frames)
+        r = bench_scene(bgpu, sc, f"{name}: {sc.num_dynamic} boxes / spheres / capsules onto a {grid}x{grid} terrain "
+                                  f"mesh, 10 iterations, dt 1/60, {frames} frames", frames)
+        r["reference_published_ms_per_frame"] = {"rust": rust, "bullet": bullet,
+                                                 "source": f"docs/perf/speed.md {name} per-frame median, f32, their "
+                                                           f"CPU, 1 thread"}
+        out.append(r)
+    return out
+
+
 def drift_report(bgpu, scenes, steps):
     """Drift of the f32 device trajectory against the oracle's f64 build (the reference's
     `--features f64` restated), on the 1,000-box stack and a 1,024-body slice of the mixed
@@ -531,6 +548,8 @@ def main():
             line["stack_1000"] = bench_stack(bgpu, scenes, args.stack_steps)
         if args.mixed_steps > 0:
             line["mixed_convex_16384"] = bench_mixed(bgpu, scenes, args.mixed_steps)
+        if args.mesh_frames > 0:
+            line["mesh_rain"] = bench_mesh_rain(bgpu, scenes, args.mesh_frames)
         if world_size == 1 and not args.no_cpu_baseline:
             # CPU leg: the oracle timed on the host (the baseline) and run as the f64 checker.
             line["cpu_baseline"] = cpu_baseline(grid_of(args.cpu_sample_grid), args.preroll + args.warmup, args.steps)

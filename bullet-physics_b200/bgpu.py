@@ -12,7 +12,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libbgpu.so")
 
-SPHERE, BOX, CAPSULE, HULL, PLANE = 0, 1, 2, 3, 4
+SPHERE, BOX, CAPSULE, HULL, PLANE, MESH = 0, 1, 2, 3, 4, 5
+HF_FLIP_QUAD_EDGES, HF_DIAMOND, HF_ZIGZAG, HF_FLIP_WINDING = 1, 2, 4, 8
+HF_UP_Y, HF_UP_X, HF_UP_Z = 0, 16, 32
 JOINT_POINT2POINT, JOINT_FIXED, JOINT_HINGE, JOINT_GEAR, JOINT_SLIDER = 0, 1, 2, 3, 4
 JOINT_DISABLE_COLLISIONS, JOINT_DISABLED, JOINT_ANGULAR_ONLY, JOINT_LIMIT, JOINT_MOTOR, JOINT_ERP = 1, 2, 4, 8, 16, 32
 JOINT_LIN_MOTOR, JOINT_ANG_MOTOR, JOINT_FRAME_B = 64, 128, 256
@@ -293,6 +295,8 @@ def lib():
             "bgpu_world_set_solver_info": (S, [P, ctypes.POINTER(SolverInfo)]),
             "bgpu_add_shape": (S, [P, U32, F, F, U32, U32P]),
             "bgpu_add_bodies": (S, [P, U32, ctypes.POINTER(BodyDesc), U32P]),
+            "bgpu_add_mesh_shape": (S, [P, F, U32, U32P, U32, U32P]),
+            "bgpu_add_heightfield_shape": (S, [P, F, U32, U32, F, U32, U32P]),
             "bgpu_num_bodies": (U32, [P]),
             "bgpu_step": (S, [P, ctypes.c_float, U32]),
             "bgpu_step_simulation_fixed": (S, [P, ctypes.c_float, U32, ctypes.c_float, U32P]),
@@ -467,6 +471,22 @@ class World:
             check(self.L.bgpu_add_shape(self.h, kind, fptr(p), fptr(pts), len(pts), ctypes.byref(out)), "add_shape")
         else:
             check(self.L.bgpu_add_shape(self.h, kind, fptr(p), None, 0, ctypes.byref(out)), "add_shape")
+        return out.value
+
+    def mesh(self, vertices, indices):
+        """Static triangle mesh: vertices n x 3, triangles m x 3 vertex indices."""
+        v = f32(np.asarray(vertices).reshape(-1, 3))
+        i = np.ascontiguousarray(np.asarray(indices).reshape(-1, 3), dtype=np.uint32)
+        out = ctypes.c_uint32()
+        check(self.L.bgpu_add_mesh_shape(self.h, fptr(v), len(v), u32ptr(i), len(i), ctypes.byref(out)), "add_mesh")
+        return out.value
+
+    def heightfield(self, heights, width, depth, cell=(1.0, 1.0, 1.0), options=0):
+        """Static heightfield (width x depth row-major heights) built into a triangle mesh."""
+        h = f32(np.asarray(heights).reshape(-1))
+        out = ctypes.c_uint32()
+        check(self.L.bgpu_add_heightfield_shape(self.h, fptr(h), width, depth, fptr(f32(cell)), options,
+                                                ctypes.byref(out)), "add_heightfield")
         return out.value
 
     def sphere(self, r):

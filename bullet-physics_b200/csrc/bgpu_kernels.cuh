@@ -164,7 +164,8 @@ void launch_integrate_positions(const BodyDev& b, uint32_t n, float dt, float tu
 // null); then, after the position integration, the clamp applied (step.rs:1210-1214).
 void launch_ccd_sweep(const BodyDev& b, const Shape* shapes, const float4* hull, const uint32_t* ids, const float2* par,
                       uint32_t m, uint32_t n, const uint32_t* world_off, const uint32_t* world_of,
-                      const uint64_t* suppressed, uint32_t nsuppressed, float dt, float* clamp, cudaStream_t s);
+                      const uint64_t* suppressed, uint32_t nsuppressed, float dt, float* clamp, uint32_t* status,
+                      cudaStream_t s);
 void launch_ccd_apply(const BodyDev& b, const uint32_t* ids, const float* clamp, uint32_t m, float dt, cudaStream_t s);
 // Host-facing layouts: n x 3 floats -> float4 lanes, and poses -> n x 7 floats.
 void launch_unpack3(uint32_t n, const float* src, float4* dst, cudaStream_t s);
@@ -336,8 +337,8 @@ struct PairDataDev {
 };
 
 constexpr uint32_t ROUTE_COUNT0 = 16;  // first per-route counter in PairData::scalars
-constexpr uint32_t CAPTURE_COUNT = ROUTE_COUNT0 + NP_CONVEX + 1;  // detections with points (capture list length)
-constexpr uint32_t CAPTURE_LIST = NP_CONVEX;  // the capture list is route_list region [7 P, 8 P)
+constexpr uint32_t CAPTURE_COUNT = ROUTE_COUNT0 + NP_MESH + 1;  // detections with points (capture list length)
+constexpr uint32_t CAPTURE_LIST = NP_MESH;  // the capture list is route_list region [8 P, 9 P)
 
 struct PairData {
     // Per pair (indexed like the sorted pair array).
@@ -425,6 +426,7 @@ struct WorldView {
     const Shape* shapes;
     const float4* hull;
     uint32_t nbodies;
+    bool has_mesh = false;  // some shape is a triangle mesh (the mesh narrow-phase launch runs)
 };
 
 // Pair pass: classify + refresh, narrow phase, capture. Fills PairData for `npairs`.

@@ -10,7 +10,17 @@
 
 namespace bgpu {
 
-enum ShapeType : uint32_t { SHAPE_SPHERE = 0, SHAPE_BOX = 1, SHAPE_CAPSULE = 2, SHAPE_HULL = 3, SHAPE_PLANE = 4 };
+enum ShapeType : uint32_t { SHAPE_SPHERE = 0, SHAPE_BOX = 1, SHAPE_CAPSULE = 2, SHAPE_HULL = 3, SHAPE_PLANE = 4,
+                            SHAPE_MESH = 5 };
+
+// Static triangle mesh (triangle_mesh.rs, with its BVH from bvh.rs; heightfields are built into
+// one). The record keeps the BVH in the hull array: node k at float4 hull_off + 2k as
+// (min.xyz, a) and (max.xyz, b), with a = start | 1 << 31, b = count for a leaf and a = left,
+// b = right for an internal node (a, b as uint bits), hull_cnt nodes in the reference's
+// pre-order. The triangles follow in the BVH's permutation order: slot k holds three float4
+// vertices at tri_base + 3k (p0's bits), the triangle's own index in the first one's w bits;
+// p1's bits hold the triangle count. Local bounds in lmin / lmax; margin 0.
+constexpr uint32_t MESH_LEAF = 1u << 31;
 
 // 64-byte shape record.
 struct Shape {
@@ -23,6 +33,33 @@ struct Shape {
     float pad;
 };
 static_assert(sizeof(Shape) == 64, "Shape record is 64 bytes");
+
+__host__ __device__ __forceinline__ uint32_t mesh_tri_base(const Shape& s) {
+    uint32_t u;
+    memcpy(&u, &s.p0, 4);
+    return u;
+}
+__host__ __device__ __forceinline__ uint32_t mesh_ntris(const Shape& s) {
+    uint32_t u;
+    memcpy(&u, &s.p1, 4);
+    return u;
+}
+
+// util.rs:106-126 (Aabb::transformed): the eight corners of a box's centre +- extents, rotated
+// and moved, wrapped in an axis-aligned box.
+__device__ __forceinline__ void aabb_transformed(V3 lmin, V3 lmax, V3 p, Q q, V3& mn, V3& mx) {
+    const V3 c = (lmin + lmax) * 0.5f, e = (lmax - lmin) * 0.5f;
+    mn = splat(INFINITY);
+    mx = splat(-INFINITY);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const V3 corner = V3{(i & 1) == 0 ? c.x + e.x : c.x - e.x, (i & 2) == 0 ? c.y + e.y : c.y - e.y,
+                             (i & 4) == 0 ? c.z + e.z : c.z - e.z};
+        const V3 w = rotate(q, corner) + p;
+        mn = vmin(mn, w);
+        mx = vmax(mx, w);
+    }
+}
 
 // shapes/mod.rs:275-291 and the per-shape support_local.
 __device__ __forceinline__ V3 support_local(const Shape& s, V3 d, const float4* __restrict__ hull) {
@@ -117,6 +154,9 @@ __device__ __forceinline__ void world_aabb(const Shape& s, V3 p, Q q, const floa
                     p.z + dot(support_local(s, uz, hull), uz)};
             return;
         }
+        case SHAPE_MESH:  // triangle_mesh.rs:213-216
+            aabb_transformed(V3{s.lmin[0], s.lmin[1], s.lmin[2]}, V3{s.lmax[0], s.lmax[1], s.lmax[2]}, p, q, mn, mx);
+            return;
         default:
             mn = splat(-1e30f);
             mx = splat(1e30f);

@@ -34,6 +34,7 @@ enum : uint32_t {
     ST_NONFINITE = 1u << 5,
     ST_TRAVERSAL_STACK = 1u << 6,
     ST_COLOUR_ROUNDS = 1u << 7,
+    ST_MESH_CANDIDATES = 1u << 8,  // a convex-vs-mesh pair found more candidate points than it keeps
 };
 
 // Pair status codes written by the classify pass.
@@ -46,7 +47,7 @@ enum : uint32_t {
 
 // Narrow-phase routes (narrowphase/mod.rs:103-285).
 enum : uint32_t { NP_NONE = 0, NP_PLANE_A = 1, NP_PLANE_B = 2, NP_SPHERE_SPHERE = 3, NP_SPHERE_BOX = 4, NP_BOX_SPHERE = 5,
-                  NP_BOX_BOX = 6, NP_CONVEX = 7 };
+                  NP_BOX_BOX = 6, NP_CONVEX = 7, NP_MESH = 8 };
 
 struct SolverParams {  // solver/info.rs:24-86 (the contact subset)
     float erp2, linear_slop, restitution_velocity_threshold;

@@ -187,6 +187,123 @@ __device__ bool sweep_convex(V3 from, V3 dir, float length, const Inflated& t, f
     return true;
 }
 
+// convex_sweep.rs:217-262 (point_triangle_distance): squared distance to the triangle and the
+// vector from its closest point to `p`.
+__device__ float point_triangle_distance(V3 p, V3 a, V3 b, V3 c, V3& dv) {
+    const V3 ab = b - a, ac = c - a, ap = p - a;
+    const float d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0.0f && d2 <= 0.0f) { dv = p - a; return len2(dv); }
+    const V3 bp = p - b;
+    const float d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0.0f && d4 <= d3) { dv = p - b; return len2(dv); }
+    const float vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+        const float v = d1 / (d1 - d3);
+        dv = p - (a + ab * v);
+        return len2(dv);
+    }
+    const V3 cp = p - c;
+    const float d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0.0f && d5 <= d6) { dv = p - c; return len2(dv); }
+    const float vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+        const float w = d2 / (d2 - d6);
+        dv = p - (a + ac * w);
+        return len2(dv);
+    }
+    const float va = d3 * d6 - d5 * d4;
+    if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+        const float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        dv = p - (b + (c - b) * w);
+        return len2(dv);
+    }
+    const float denom = 1.0f / (va + vb + vc);
+    const float v = vb * denom, w = vc * denom;
+    dv = p - (a + ab * v + ac * w);
+    return len2(dv);
+}
+
+// convex_sweep.rs:131-151 (sweep_triangle) distance: zero inside the inflated triangle.
+__device__ __forceinline__ float tri_inflated_distance2(V3 p, V3 a, V3 b, V3 c, float radius) {
+    V3 dv;
+    const float q = point_triangle_distance(p, a, b, c, dv);
+    if (q <= radius * radius) return 0.0f;
+    const float d = sqrtf(q);
+    return (d - radius) * (d - radius);
+}
+
+// convex_sweep.rs:155-214 (sweep_with_dist) against one triangle, the fraction only.
+__device__ bool sweep_triangle(V3 from, V3 dir, float length, float radius, V3 a, V3 b, V3 c, float& fraction) {
+    float lo = 0.0f, hi = 1.0f;
+    for (int it = 0; it < 40; ++it) {
+        const float m1 = lo + (hi - lo) / 3.0f;
+        const float m2 = hi - (hi - lo) / 3.0f;
+        if (tri_inflated_distance2(from + dir * (m1 * length), a, b, c, radius) <
+            tri_inflated_distance2(from + dir * (m2 * length), a, b, c, radius))
+            hi = m2;
+        else
+            lo = m1;
+    }
+    const float s_min = (lo + hi) * 0.5f;
+    if (tri_inflated_distance2(from + dir * (s_min * length), a, b, c, radius) > 1e-8f) return false;
+    float low = 0.0f, high = s_min;
+    for (int it = 0; it < 60; ++it) {
+        const float mid = (low + high) * 0.5f;
+        if (tri_inflated_distance2(from + dir * (mid * length), a, b, c, radius) <= 1e-8f) high = mid;
+        else low = mid;
+    }
+    fraction = (low + high) * 0.5f;
+    return true;
+}
+
+// convex_sweep.rs:305-345 (sweep_mesh): the segment in the mesh frame, the BVH candidates of its
+// swept box (bgpu_shapes.cuh's mesh layout), the smallest per-triangle fraction.
+__device__ bool sweep_mesh(V3 from, V3 to, float radius, const Shape& ms, V3 pos, Q ori,
+                           const float4* __restrict__ hull, uint32_t* status, float& fraction) {
+    const Q inv = qinv(ori);
+    const V3 lf = rotate(inv, from - pos), lt = rotate(inv, to - pos);
+    const V3 delta = lt - lf;
+    const float length = len(delta);
+    if (length <= 1.1920929e-7f) return false;
+    const V3 dir = delta / length;
+    const V3 r = V3{radius, radius, radius};
+    const V3 bmin = vmin(lf, lt) - r, bmax = vmax(lf, lt) + r;
+    const uint32_t tri_base = mesh_tri_base(ms);
+    bool any = false;
+    float best = 1.0f;
+    uint32_t stack[64];
+    int sp = 0;
+    if (ms.hull_cnt) stack[sp++] = 0;
+    while (sp > 0) {
+        const uint32_t k = stack[--sp];
+        const float4 n0 = hull[ms.hull_off + 2 * k], n1 = hull[ms.hull_off + 2 * k + 1];
+        if (!(n0.x <= bmax.x && n0.y <= bmax.y && n0.z <= bmax.z && bmin.x <= n1.x && bmin.y <= n1.y && bmin.z <= n1.z))
+            continue;
+        const uint32_t na = __float_as_uint(n0.w), nb = __float_as_uint(n1.w);
+        if (!(na & MESH_LEAF)) {
+            if (sp + 2 > 64) {
+                atomicOr(status, ST_TRAVERSAL_STACK);
+                continue;
+            }
+            stack[sp++] = na;
+            stack[sp++] = nb;
+            continue;
+        }
+        const uint32_t start = na & ~MESH_LEAF;
+        for (uint32_t slot = start; slot < start + nb; ++slot) {
+            const uint32_t o = tri_base + 3 * slot;
+            float f;
+            if (sweep_triangle(lf, dir, length, radius, from4(hull[o]), from4(hull[o + 1]), from4(hull[o + 2]), f) &&
+                (!any || f < best)) {
+                best = f;
+                any = true;
+            }
+        }
+    }
+    if (any) fraction = best;
+    return any;
+}
+
 // convex_sweep.rs:263-295 (sweep_plane), the fraction only
 __device__ bool sweep_plane(V3 from, V3 dir, float length, float radius, const Shape& s, Q ori, float& fraction) {
     const V3 n = rotate(ori, V3{s.p0, s.p1, s.p2});
@@ -227,8 +344,9 @@ constexpr int CCD_THREADS = 32;
 constexpr int CCD_CAP = 256;
 
 struct CcdCtx {
-    V3 from, dir;
+    V3 from, to, dir;
     float length, radius;
+    uint32_t* status;
 };
 
 __device__ __forceinline__ float cast_one(const BodyDev& b, const Shape* __restrict__ shapes, const float4* __restrict__ hull,
@@ -238,6 +356,8 @@ __device__ __forceinline__ float cast_one(const BodyDev& b, const Shape* __restr
     bool hit;
     if (sj.type == SHAPE_PLANE) {
         hit = sweep_plane(c.from, c.dir, c.length, c.radius, sj, q4(b.quat[j]), f);
+    } else if (sj.type == SHAPE_MESH) {
+        hit = sweep_mesh(c.from, c.to, c.radius, sj, from4(b.pos[j]), q4(b.quat[j]), hull, c.status, f);
     } else {
         Inflated t{sj, from4(b.pos[j]), q4(b.quat[j]), c.radius, hull};
         hit = sweep_convex(c.from, c.dir, c.length, t, f);
@@ -257,7 +377,7 @@ __global__ void __launch_bounds__(CCD_THREADS) k_ccd_sweep(BodyDev b, const Shap
                                                            const uint32_t* __restrict__ world_off,
                                                            const uint32_t* __restrict__ world_of,
                                                            const uint64_t* __restrict__ suppressed, uint32_t nsuppressed,
-                                                           float dt, float* clamp) {
+                                                           float dt, float* clamp, uint32_t* status) {
     __shared__ uint32_t cand[CCD_CAP], sorted[CCD_CAP];
     __shared__ float lb[CCD_CAP], slb[CCD_CAP];
     __shared__ uint32_t ncand;
@@ -281,7 +401,9 @@ __global__ void __launch_bounds__(CCD_THREADS) k_ccd_sweep(BodyDev b, const Shap
     c.length = len(delta);
     c.dir = delta / c.length;
     c.from = from;
+    c.to = to;
     c.radius = radius;
+    c.status = status;
     // convex_sweep.rs:45-50: a vanishing motion casts nothing
     if (c.length <= 1.1920929e-7f) {
         if (lane == 0) clamp[k] = 1.0f;
@@ -392,10 +514,11 @@ __global__ void k_ccd_apply(BodyDev b, const uint32_t* __restrict__ ids, const f
 
 void launch_ccd_sweep(const BodyDev& b, const Shape* shapes, const float4* hull, const uint32_t* ids, const float2* par,
                       uint32_t m, uint32_t n, const uint32_t* world_off, const uint32_t* world_of,
-                      const uint64_t* suppressed, uint32_t nsuppressed, float dt, float* clamp, cudaStream_t s) {
+                      const uint64_t* suppressed, uint32_t nsuppressed, float dt, float* clamp, uint32_t* status,
+                      cudaStream_t s) {
     if (m == 0) return;
     k_ccd_sweep<<<m, CCD_THREADS, 0, s>>>(b, shapes, hull, ids, par, n, world_off, world_of, suppressed, nsuppressed,
-                                          dt, clamp);
+                                          dt, clamp, status);
 }
 
 void launch_ccd_apply(const BodyDev& b, const uint32_t* ids, const float* clamp, uint32_t m, float dt, cudaStream_t s) {

@@ -236,6 +236,10 @@ __device__ __forceinline__ void emit_rows(const BodyDev& b, uint32_t i, uint32_t
 
 __device__ __forceinline__ uint32_t route_of(uint32_t ta, uint32_t tb) {
     if (ta == SHAPE_PLANE && tb == SHAPE_PLANE) return NP_NONE;
+    if (ta == SHAPE_MESH || tb == SHAPE_MESH) {  // mod.rs:102-243: convex vs mesh only (meshes are static here)
+        const uint32_t other = ta == SHAPE_MESH ? tb : ta;
+        return (other == SHAPE_MESH || other == SHAPE_PLANE) ? NP_NONE : NP_MESH;
+    }
     if (ta == SHAPE_PLANE) return NP_PLANE_A;
     if (tb == SHAPE_PLANE) return NP_PLANE_B;
     if (ta == SHAPE_SPHERE && tb == SHAPE_SPHERE) return NP_SPHERE_SPHERE;
@@ -425,6 +429,219 @@ __device__ __noinline__ void collide_convex(const Shape& sa, V3 pa, Q qa, const 
     mf_push(m, point_a - n * depth, n, depth);
 }
 
+// ---------------------------------------------------------------- convex vs static mesh
+// narrowphase/convex_mesh.rs:26-153. The convex's world AABB, swept into the mesh frame, picks
+// candidate triangles from the mesh BVH (bvh.rs:45-66, the same stack walk: left pushed first,
+// so the right child is visited first); each candidate whose own AABB overlaps the query runs
+// the sphere detector (spheres) or convex_convex against the triangle as a three-vertex hull;
+// the points then reduce to four (manifold.rs:80-108). Normals point from the convex to the mesh.
+constexpr int MESH_MAX_CAND = 64;   // candidate points per pair (more: ST_MESH_CANDIDATES)
+constexpr int MESH_STACK = 64;      // BVH walk depth
+
+// convex_mesh.rs:236-253
+__device__ __forceinline__ float seg_closest_sq(V3 from, V3 to, V3 p, V3& nearest) {
+    const V3 v = to - from;
+    float t = dot(v, p - from);
+    if (t > 0.0f) {
+        const float dvv = dot(v, v);
+        if (t < dvv) t /= dvv;
+        else t = 1.0f;
+    } else {
+        t = 0.0f;
+    }
+    nearest = from + v * t;
+    return len2(p - nearest);
+}
+
+// convex_mesh.rs:160-232: point on the triangle, normal toward the centre, radius - distance.
+__device__ __forceinline__ bool sphere_triangle(V3 center, float radius, float threshold, V3 a, V3 b, V3 c, V3& point,
+                                                V3& normal_out, float& pen) {
+    const float rwt = radius + threshold;
+    V3 normal = cross(b - a, c - a);
+    const float l2 = len2(normal);
+    const float eps = 1.1920929e-7f;  // f32::EPSILON
+    if (l2 < eps * eps) return false;
+    normal = normal * (1.0f / sqrtf(l2));
+    float dist = dot(normal, center - a);
+    if (dist < 0.0f) {
+        dist = -dist;
+        normal = -normal;
+    }
+    if (dist >= rwt) return false;
+    V3 cp;
+    // convex_mesh.rs:257-268 point_in_triangle
+    const float r1 = dot(cross(b - a, normal), center - a), r2 = dot(cross(c - b, normal), center - b),
+                r3 = dot(cross(a - c, normal), center - c);
+    if ((r1 > 0.0f && r2 > 0.0f && r3 > 0.0f) || (r1 <= 0.0f && r2 <= 0.0f && r3 <= 0.0f)) {
+        cp = center - normal * dist;
+    } else {
+        float min_d = rwt * rwt;
+        bool found = false;
+        V3 on;
+        float d = seg_closest_sq(a, b, center, on);
+        if (d < min_d) { min_d = d; cp = on; found = true; }
+        d = seg_closest_sq(b, c, center, on);
+        if (d < min_d) { min_d = d; cp = on; found = true; }
+        d = seg_closest_sq(c, a, center, on);
+        if (d < min_d) { min_d = d; cp = on; found = true; }
+        if (!found) return false;
+    }
+    const V3 to_c = center - cp;
+    const float d2 = len2(to_c);
+    if (d2 >= rwt * rwt) return false;
+    point = cp;
+    if (d2 > eps) {
+        const float d = sqrtf(d2);
+        normal_out = to_c * (1.0f / d);
+        pen = radius - d;
+    } else {
+        normal_out = normal;
+        pen = radius;
+    }
+    return true;
+}
+
+struct MeshCandidates {
+    int n;
+    V3 pos[MESH_MAX_CAND];
+    V3 nrm[MESH_MAX_CAND];
+    float pen[MESH_MAX_CAND];
+};
+
+// manifold.rs:80-108: deepest first (stable), then greedily the farthest from the kept points.
+__device__ __forceinline__ void reduce_to_manifold(const MeshCandidates& c, Manifold& m) {
+    m.n = 0;
+    if (c.n <= 4) {
+        for (int i = 0; i < c.n; ++i) mf_push(m, c.pos[i], c.nrm[i], c.pen[i]);
+        return;
+    }
+    uint8_t ord[MESH_MAX_CAND];
+    for (int i = 0; i < c.n; ++i) {  // stable insertion sort by penetration, deepest first
+        int j = i;
+        while (j > 0 && c.pen[ord[j - 1]] < c.pen[i]) {
+            ord[j] = ord[j - 1];
+            --j;
+        }
+        ord[j] = uint8_t(i);
+    }
+    uint64_t used = 1ull;  // bit s: sorted position s taken
+    int kept[4] = {ord[0], 0, 0, 0};
+    int nk = 1;
+    while (nk < 4) {
+        int best = 0;
+        float best_sep = -INFINITY;
+        for (int s = 0; s < c.n; ++s) {
+            if (used & (1ull << s)) continue;
+            float sep = INFINITY;
+            for (int q = 0; q < nk; ++q) sep = fminf(sep, len2(c.pos[ord[s]] - c.pos[kept[q]]));
+            if (sep > best_sep) { best_sep = sep; best = s; }
+        }
+        kept[nk++] = ord[best];
+        used |= 1ull << best;
+    }
+    for (int q = 0; q < 4; ++q) mf_push(m, c.pos[kept[q]], c.nrm[kept[q]], c.pen[kept[q]]);
+}
+
+__device__ __noinline__ void collide_mesh(const Shape& cv, V3 pc, Q qc, const Shape& ms, V3 pm, Q qm, bool has_seed,
+                                          V3 seed, const float4* __restrict__ hull, EpaScratch& scratch, Manifold& m,
+                                          uint32_t* status) {
+    m.n = 0;
+    const float thr = fminf(cv.cbt, ms.cbt);
+    V3 wmn, wmx;
+    world_aabb(cv, pc, qc, hull, wmn, wmx);
+    const Q inv_m = qinv(qm);
+    const V3 c = (wmn + wmx) * 0.5f, e = (wmx - wmn) * 0.5f;
+    V3 lmin = splat(INFINITY), lmax = splat(-INFINITY);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const V3 corner = V3{(i & 1) == 0 ? c.x + e.x : c.x - e.x, (i & 2) == 0 ? c.y + e.y : c.y - e.y,
+                             (i & 4) == 0 ? c.z + e.z : c.z - e.z};
+        const V3 p = rotate(inv_m, corner - pm);
+        lmin = vmin(lmin, p);
+        lmax = vmax(lmax, p);
+    }
+    auto overlaps = [&](V3 a0, V3 a1) {  // util.rs:28-38, closed
+        return a0.x <= lmax.x && a0.y <= lmax.y && a0.z <= lmax.z && lmin.x <= a1.x && lmin.y <= a1.y && lmin.z <= a1.z;
+    };
+    const bool sphere = cv.type == SHAPE_SPHERE;
+    const V3 center = rotate(inv_m, pc - pm);
+    const uint32_t tri_base = mesh_tri_base(ms);
+    Shape tri;  // the candidate triangle as a three-vertex hull (margin 0)
+    tri.type = SHAPE_HULL;
+    tri.hull_cnt = 3;
+    tri.margin = 0.0f;
+    tri.cbt = thr;
+    MeshCandidates cand;
+    cand.n = 0;
+    uint32_t stack[MESH_STACK];
+    int sp = 0;
+    if (ms.hull_cnt) stack[sp++] = 0;
+    while (sp > 0) {
+        const uint32_t k = stack[--sp];
+        const float4 n0 = hull[ms.hull_off + 2 * k], n1 = hull[ms.hull_off + 2 * k + 1];
+        if (!overlaps(from4(n0), from4(n1))) continue;
+        const uint32_t na = __float_as_uint(n0.w), nb = __float_as_uint(n1.w);
+        if (!(na & MESH_LEAF)) {
+            if (sp + 2 > MESH_STACK) {
+                atomicOr(status, ST_TRAVERSAL_STACK);
+                continue;
+            }
+            stack[sp++] = na;
+            stack[sp++] = nb;
+            continue;
+        }
+        const uint32_t start = na & ~MESH_LEAF;
+        for (uint32_t slot = start; slot < start + nb; ++slot) {
+            const uint32_t o = tri_base + 3 * slot;
+            const V3 a = from4(hull[o]), b = from4(hull[o + 1]), cc = from4(hull[o + 2]);
+            if (!overlaps(vmin(a, vmin(b, cc)), vmax(a, vmax(b, cc)))) continue;  // triangle_mesh.rs:98-112 boxes
+            V3 pt, nl;
+            float pen;
+            bool hit = false;
+            if (sphere) {
+                if (sphere_triangle(center, cv.p0, thr, a, b, cc, pt, nl, pen)) {
+                    pt = pm + rotate(qm, pt);
+                    nl = rotate(qm, -nl);
+                    hit = true;
+                }
+            } else {
+                tri.hull_off = o;
+                Manifold one;
+                collide_convex(cv, pc, qc, tri, pm, qm, has_seed, seed, hull, scratch, one, status);
+                if (one.n) {
+                    pt = one.pos[0];
+                    nl = one.nrm[0];
+                    pen = one.pen[0];
+                    hit = true;
+                }
+            }
+            if (!hit) continue;
+            if (cand.n == MESH_MAX_CAND) {
+                atomicOr(status, ST_MESH_CANDIDATES);
+                continue;
+            }
+            cand.pos[cand.n] = pt;
+            cand.nrm[cand.n] = nl;
+            cand.pen[cand.n] = pen;
+            ++cand.n;
+        }
+    }
+    reduce_to_manifold(cand, m);
+}
+
+// One pair on the mesh route: the convex side against the mesh side (mod.rs:200-243); with the
+// mesh first the manifold is flipped.
+__device__ __forceinline__ void collide_mesh_pair(const Shape& sa, V3 pa, Q qa, const Shape& sb, V3 pb, Q qb,
+                                                  bool has_seed, V3 seed, const float4* __restrict__ hull,
+                                                  EpaScratch& scratch, Manifold& m, uint32_t* status) {
+    if (sa.type == SHAPE_MESH) {
+        collide_mesh(sb, pb, qb, sa, pa, qa, has_seed, seed, hull, scratch, m, status);
+        mf_flip(m);
+    } else {
+        collide_mesh(sa, pa, qa, sb, pb, qb, has_seed, seed, hull, scratch, m, status);
+    }
+}
+
 // A detection with points goes to the capture list; one without drops the pair's manifold
 // here (step.rs:800-853: an empty detection removes it), so the capture pass only runs
 // where there is something to merge.
@@ -499,6 +716,26 @@ __global__ void k_narrow_convex(BodyDev b, const Shape* __restrict__ shapes, con
     }
 }
 
+__global__ void k_narrow_mesh(BodyDev b, const Shape* __restrict__ shapes, const float4* __restrict__ hull,
+                              const uint64_t* __restrict__ pairs, uint32_t npairs, PairDataDev pd, uint32_t* status) {
+    const uint32_t cnt = pd.scalars[ROUTE_COUNT0 + NP_MESH];
+    if (blockIdx.x == 0 && threadIdx.x == 0) pd.scalars[1] += cnt;  // with the convex detections (statistics)
+    EpaScratch scratch;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+        const uint32_t p = pd.route_list[size_t(NP_MESH - 1) * npairs + t];
+        const uint64_t key = pairs[p];
+        const uint32_t i = key_lo(key), j = key_hi(key);
+        const uint4 ia = b.info[i], ib = b.info[j];
+        const Shape sa = shapes[ia.x], sb = shapes[ib.x];
+        V3 seed = V3{0.f, 0.f, 0.f};
+        const bool has_seed = entry_seed(pd.entries + size_t(p) * ENTRY_F4, seed);
+        Manifold m;
+        collide_mesh_pair(sa, from4(b.pred[i]), q4(b.quat[i]), sb, from4(b.pred[j]), q4(b.quat[j]), has_seed, seed,
+                          hull, scratch, m, status);
+        store_detection(pd, p, npairs, m);
+    }
+}
+
 // step.rs:800-853: merge the detection into the manifold, refresh, emit rows; or drop the manifold.
 __device__ __forceinline__ void capture_one(const BodyDev& b, const Shape* __restrict__ shapes, const uint64_t* __restrict__ pairs,
                                             const StepParams& sp, PairDataDev& pd, uint32_t p) {
@@ -566,12 +803,14 @@ __global__ void k_collide_queries(const Shape* __restrict__ shapes, const float4
     Q qa = q4(qa4[t]), qb = q4(qb4[t]);
     Manifold m;
     m.n = 0;
-    uint32_t route = force_convex ? NP_CONVEX : route_of(sa.type, sb.type);
-    if (route == NP_CONVEX) {
+    uint32_t route = route_of(sa.type, sb.type);
+    if (force_convex && route != NP_MESH && route != NP_NONE) route = NP_CONVEX;
+    if (route == NP_CONVEX || route == NP_MESH) {
         EpaScratch scratch;
         bool has_seed = seeds != nullptr;
         V3 seed = has_seed ? from4(seeds[t]) : V3{0.f, 0.f, 0.f};
-        collide_convex(sa, pa, qa, sb, pb, qb, has_seed, seed, hull, scratch, m, status);
+        if (route == NP_MESH) collide_mesh_pair(sa, pa, qa, sb, pb, qb, has_seed, seed, hull, scratch, m, status);
+        else collide_convex(sa, pa, qa, sb, pb, qb, has_seed, seed, hull, scratch, m, status);
     } else if (route != NP_NONE) {
         collide_analytic(route, sa, pa, qa, sb, pb, qb, hull, m);
     }
@@ -626,6 +865,7 @@ void run_pair_pass(const WorldView& w, const uint64_t* pairs, uint32_t npairs, c
     k_narrow_analytic<<<grid, TB, 0, s>>>(w.b, w.shapes, w.hull, pairs, npairs, d);
     uint32_t cgrid = std::min<uint32_t>((npairs + 63) / 64, 148u * 8u);
     k_narrow_convex<<<cgrid, 64, 0, s>>>(w.b, w.shapes, w.hull, pairs, npairs, d, status_dev);
+    if (w.has_mesh) k_narrow_mesh<<<cgrid, 64, 0, s>>>(w.b, w.shapes, w.hull, pairs, npairs, d, status_dev);
     k_capture<<<grid, TB, 0, s>>>(w.b, w.shapes, pairs, npairs, sp, d);
 }
 

@@ -923,7 +923,13 @@ __device__ void solve_world(const WorldSolveArgs& A, uint32_t w, uint32_t lane, 
     }
     ws_sync<WARP>();
     const uint32_t g0 = C.g0, g1 = C.g1;
-    if (g0 == g1) return;  // no rows in this world: its velocities stay as they are
+    if (g0 == g1) {  // no rows in this world: its velocities stay as they are
+        if (lane == 0) {  // an empty record (the adjoint's reverse pass reads every world's)
+            A.wcol[size_t(w) * WS_STRIDE] = g0;
+            A.wcol[size_t(w) * WS_STRIDE + 1] = 0;
+        }
+        return;
+    }
     auto dyn = [&](uint32_t i) { return inv_mass_of(a.iw, i) > 0.0f; };
     // 1. Jones-Plassmann rounds: an uncoloured group wins when its priority is the largest
     //    among the uncoloured groups at each of its dynamic bodies; a winner takes the lowest

@@ -230,7 +230,8 @@ struct World {
                        sleep.p, info_d.p, aabb_min.p, aabb_max.p, pred.p, settled.p, iw.p, push_lin.p, push_ang.p,
                        rec_step ? rec_step->flags.p : nullptr};
     }
-    WorldView view() { return WorldView{body_dev(), shapes_d.p, hull_d.p, n}; }
+    bool has_mesh = false;  // some shape is a triangle mesh
+    WorldView view() { return WorldView{body_dev(), shapes_d.p, hull_d.p, n, has_mesh}; }
 
     void sync_shapes() {
         if (!shapes_dirty) return;
@@ -306,6 +307,134 @@ struct World {
         return uint32_t(shapes_h.size() - 1);
     }
 
+    // A static triangle mesh (triangle_mesh.rs:59-123) with the BVH of bvh.rs:36-206: nodes in
+    // pre-order, longest-axis median split of the triangle centres (a stable sort on the
+    // centre coordinate), at most four triangles per leaf. Nodes and triangles go to the hull
+    // array in the layout bgpu_shapes.cuh describes.
+    uint32_t add_mesh(const float* v, uint32_t nv, const uint32_t* idx, uint32_t nt) {
+        if (!v || !idx || nv == 0 || nt == 0) throw InvalidArg{"a triangle mesh needs vertices and triangles"};
+        for (uint64_t k = 0; k < uint64_t(nt) * 3; ++k)
+            if (idx[k] >= nv) throw InvalidArg{"triangle index out of range"};
+        struct F3 { float x, y, z; };
+        auto vert = [&](uint32_t t, int c) { const float* p = v + 3 * size_t(idx[3 * size_t(t) + c]); return F3{p[0], p[1], p[2]}; };
+        std::vector<uint32_t> order(nt);
+        for (uint32_t t = 0; t < nt; ++t) order[t] = t;
+        struct Node { float mn[3], mx[3]; uint32_t a, b; };
+        std::vector<Node> nodes;
+        auto center = [&](uint32_t t, int axis) {  // bvh.rs:248-251: (a + b + c) * (1 / 3)
+            F3 a = vert(t, 0), b = vert(t, 1), c = vert(t, 2);
+            const float third = 1.0f / 3.0f;
+            float s3[3] = {(a.x + b.x + c.x) * third, (a.y + b.y + c.y) * third, (a.z + b.z + c.z) * third};
+            return s3[axis];
+        };
+        std::function<uint32_t(uint32_t, uint32_t)> build = [&](uint32_t start, uint32_t count) -> uint32_t {
+            Node nd;
+            bool have = false;
+            for (uint32_t k = start; k < start + count; ++k)  // bvh.rs:210-225
+                for (int c = 0; c < 3; ++c) {
+                    F3 p = vert(order[k], c);
+                    float q[3] = {p.x, p.y, p.z};
+                    for (int d = 0; d < 3; ++d) {
+                        nd.mn[d] = have ? std::min(nd.mn[d], q[d]) : q[d];
+                        nd.mx[d] = have ? std::max(nd.mx[d], q[d]) : q[d];
+                    }
+                    have = true;
+                }
+            nd.a = start | MESH_LEAF;
+            nd.b = count;
+            const uint32_t index = uint32_t(nodes.size());
+            nodes.push_back(nd);
+            if (count <= 4) return index;
+            float e[3];
+            for (int d = 0; d < 3; ++d) e[d] = (nd.mx[d] - nd.mn[d]) * 0.5f;
+            int axis = 0;  // bvh.rs:255-268: first strict maximum
+            float m = e[0];
+            if (e[1] > m) { axis = 1; m = e[1]; }
+            if (e[2] > m) axis = 2;
+            std::stable_sort(order.begin() + start, order.begin() + start + count,
+                             [&](uint32_t x, uint32_t y) { return center(x, axis) < center(y, axis); });
+            const uint32_t mid = count / 2;
+            const uint32_t left = build(start, mid);
+            const uint32_t right = build(start + mid, count - mid);
+            nodes[index].a = left;
+            nodes[index].b = right;
+            return index;
+        };
+        build(0, nt);
+        if (nodes.size() >= MESH_LEAF || nt >= MESH_LEAF) throw InvalidArg{"mesh too large"};
+        Shape s;
+        std::memset(&s, 0, sizeof(s));
+        s.type = SHAPE_MESH;
+        s.hull_off = uint32_t(hull_h.size());
+        s.hull_cnt = uint32_t(nodes.size());
+        for (const Node& nd : nodes) {
+            float fa, fb;
+            std::memcpy(&fa, &nd.a, 4);
+            std::memcpy(&fb, &nd.b, 4);
+            hull_h.push_back(make_float4(nd.mn[0], nd.mn[1], nd.mn[2], fa));
+            hull_h.push_back(make_float4(nd.mx[0], nd.mx[1], nd.mx[2], fb));
+        }
+        const uint32_t tri_base = uint32_t(hull_h.size());
+        for (uint32_t k = 0; k < nt; ++k) {
+            const uint32_t t = order[k];
+            float ft;
+            std::memcpy(&ft, &t, 4);
+            for (int c = 0; c < 3; ++c) {
+                F3 p = vert(t, c);
+                hull_h.push_back(make_float4(p.x, p.y, p.z, c == 0 ? ft : 0.0f));
+            }
+        }
+        std::memcpy(&s.p0, &tri_base, 4);
+        std::memcpy(&s.p1, &nt, 4);
+        s.margin = 0.0f;
+        for (int d = 0; d < 3; ++d) {  // triangle_mesh.rs:98-112 local bounds (the root box)
+            s.lmin[d] = nodes[0].mn[d];
+            s.lmax[d] = nodes[0].mx[d];
+        }
+        s.cbt = contact_breaking_threshold(s.lmin, s.lmax);
+        shapes_h.push_back(s);
+        shapes_dirty = true;
+        has_mesh = true;
+        return uint32_t(shapes_h.size() - 1);
+    }
+
+    // heightfield.rs:84-140: a width x depth row-major grid centred on the origin, heights offset
+    // by the min/max midpoint, two triangles per cell (diagonal and winding by the option bits:
+    // 1 flip quad edges, 2 diamond, 4 zigzag, 8 flip winding; up axis in bits 4-5: 0 Y, 1 X, 2 Z).
+    uint32_t add_heightfield(const float* h, uint32_t width, uint32_t depth, const float* cell, uint32_t options) {
+        if (!h || !cell || width < 2 || depth < 2) throw InvalidArg{"a heightfield needs at least 2 x 2 heights"};
+        if (uint64_t(width) * depth > (1ull << 26)) throw InvalidArg{"heightfield too large"};
+        float mn = INFINITY, mx = -INFINITY;
+        for (size_t i = 0; i < size_t(width) * depth; ++i) { mn = std::min(mn, h[i]); mx = std::max(mx, h[i]); }
+        const float mid = (mn + mx) * 0.5f;
+        const uint32_t up = (options >> 4) & 3u;
+        if (up == 3) throw InvalidArg{"heightfield up axis must be 0 (Y), 1 (X) or 2 (Z)"};
+        std::vector<float> v;
+        v.reserve(size_t(width) * depth * 3);
+        for (uint32_t y = 0; y < depth; ++y)
+            for (uint32_t x = 0; x < width; ++x) {
+                const float hh = h[size_t(y) * width + x] - mid;
+                const float u = (float(x) - float(width - 1) * 0.5f) * cell[0];
+                const float w = (float(y) - float(depth - 1) * 0.5f) * cell[2];
+                const float p[3] = {up == 1 ? hh : u, up == 1 ? u : (up == 2 ? w : hh), up == 2 ? hh : w};
+                v.insert(v.end(), p, p + 3);
+            }
+        const bool flip_edges = options & 1u, diamond = options & 2u, zigzag = options & 4u, flip_wind = options & 8u;
+        std::vector<uint32_t> idx;
+        auto tri = [&](uint32_t a, uint32_t b, uint32_t c) {
+            if (flip_wind) std::swap(a, c);
+            idx.push_back(a); idx.push_back(b); idx.push_back(c);
+        };
+        for (uint32_t y = 0; y + 1 < depth; ++y)
+            for (uint32_t x = 0; x + 1 < width; ++x) {
+                const uint32_t v00 = y * width + x, v10 = v00 + 1, v01 = v00 + width, v11 = v01 + 1;
+                const bool flipped = flip_edges || (diamond && ((y + x) & 1u) == 0) || (zigzag && (y & 1u) == 0);
+                if (flipped) { tri(v00, v01, v11); tri(v00, v11, v10); }
+                else { tri(v00, v01, v10); tri(v10, v01, v11); }
+            }
+        return add_mesh(v.data(), width * depth, idx.data(), uint32_t(idx.size() / 3));
+    }
+
     void grow_bodies(uint32_t need) {
         if (need <= cap) return;
         uint32_t c = std::max<uint32_t>(need, cap * 2);
@@ -329,6 +458,8 @@ struct World {
             if (d[k].shape >= shapes_h.size()) throw InvalidArg{"body shape id out of range"};
             if (shapes_h[d[k].shape].type == SHAPE_PLANE && d[k].mass != 0.0f)
                 throw InvalidArg{"a plane body must be static (mass 0)"};
+            if (shapes_h[d[k].shape].type == SHAPE_MESH && (d[k].mass != 0.0f || (d[k].flags & BGPU_BODY_KINEMATIC)))
+                throw InvalidArg{"a triangle mesh or heightfield body must be static (mass 0, not kinematic)"};
             if (!(d[k].mass >= 0.0f)) throw InvalidArg{"mass must be >= 0"};
         }
         sync_shapes();
@@ -784,7 +915,7 @@ struct World {
         mark(7);
         // 7a: CCD clamp fractions, from the solved velocities and the pre-integration poses
         launch_ccd_sweep(b, shapes_d.p, hull_d.p, ccd_ids_d.p, ccd_par_d.p, nccd, n, batch ? world_off_d.p : nullptr,
-                         world_of, sp.suppressed, sp.nsuppressed, dt, ccd_clamp_d.p, stream);
+                         world_of, sp.suppressed, sp.nsuppressed, dt, ccd_clamp_d.p, status, stream);
         // 6c + 7 + 8: deactivation, pose integration with the split push, force clear.
         launch_integrate_positions(b, n, dt, info.split_impulse_turn_erp, stream);
         launch_ccd_apply(b, ccd_ids_d.p, ccd_clamp_d.p, nccd, dt, stream);
@@ -1363,6 +1494,26 @@ bgpu_status bgpu_add_shape(bgpu_world* w, uint32_t type, const float* params, co
     if (!w) return BGPU_ERR_INVALID_ARGUMENT;
     return guarded([&]() -> bgpu_status {
         uint32_t id = w->impl.add_shape(type, params, pts, npts);
+        if (out) *out = id;
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_add_mesh_shape(bgpu_world* w, const float* vertices, uint32_t nverts, const uint32_t* indices,
+                                uint32_t ntris, uint32_t* out) {
+    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        uint32_t id = w->impl.add_mesh(vertices, nverts, indices, ntris);
+        if (out) *out = id;
+        return BGPU_OK;
+    });
+}
+
+bgpu_status bgpu_add_heightfield_shape(bgpu_world* w, const float* heights, uint32_t width, uint32_t depth,
+                                       const float* cell_size, uint32_t options, uint32_t* out) {
+    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    return guarded([&]() -> bgpu_status {
+        uint32_t id = w->impl.add_heightfield(heights, width, depth, cell_size, options);
         if (out) *out = id;
         return BGPU_OK;
     });

@@ -30,7 +30,7 @@ import math
 
 import numpy as np
 
-SPHERE, BOX, CAPSULE, HULL, PLANE = 0, 1, 2, 3, 4
+SPHERE, BOX, CAPSULE, HULL, PLANE, MESH = 0, 1, 2, 3, 4, 5
 
 
 ACT_DISABLE_DEACTIVATION = 4  # ActivationState::DisableDeactivation (body.rs:140-153)
@@ -55,6 +55,18 @@ class Scene:
 
     def add_shape(self, kind, params=(), points=None):
         self.shapes.append((kind, list(params), None if points is None else np.asarray(points, dtype=np.float32)))
+        return len(self.shapes) - 1
+
+    def add_mesh(self, vertices, indices):
+        """A static triangle mesh shape (vertices n x 3, triangles m x 3)."""
+        self.shapes.append((MESH, {"vertices": np.asarray(vertices, dtype=np.float32).reshape(-1, 3),
+                                   "indices": np.asarray(indices, dtype=np.uint32).reshape(-1, 3)}, None))
+        return len(self.shapes) - 1
+
+    def add_heightfield(self, heights, width, depth, cell=(1.0, 1.0, 1.0), options=0):
+        """A static heightfield shape (width x depth row-major heights)."""
+        self.shapes.append((MESH, {"heights": np.asarray(heights, dtype=np.float32).reshape(-1), "width": width,
+                                   "depth": depth, "cell": tuple(cell), "options": options}, None))
         return len(self.shapes) - 1
 
     def add(self, shape, pos, quat=(0, 0, 0, 1), mass=1.0, linvel=(0, 0, 0), angvel=(0, 0, 0), friction=0.5,
@@ -85,8 +97,7 @@ class Scene:
 
     def build_gpu(self, bgpu_module, **solver):
         w = bgpu_module.World(gravity=self.gravity, num_iterations=self.iterations, **solver)
-        for kind, params, pts in self.shapes:
-            w.add_shape(kind, params, pts)
+        add_shapes(w, self.shapes)
         a = self.arrays()
         w.add_bodies_array(a["shape"], a["pos"], a["quat"], a["linvel"], a["angvel"], a["mass"], a["friction"],
                            a["restitution"])
@@ -96,8 +107,7 @@ class Scene:
         w = oracle_module.OracleWorld(precision)
         w.set_gravity(self.gravity)
         w.set_solver(num_iterations=self.iterations, **solver)
-        for kind, params, pts in self.shapes:
-            w.add_shape(kind, params, pts)
+        add_shapes(w, self.shapes)
         a = self.arrays()
         for i in range(self.num_bodies):
             w.add_body(int(a["shape"][i]), a["pos"][i].astype(np.float64), quat=a["quat"][i].astype(np.float64),
@@ -105,6 +115,60 @@ class Scene:
                        mass=float(a["mass"][i]), friction=float(a["friction"][i]),
                        restitution=float(a["restitution"][i]))
         return w
+
+
+def add_shapes(w, shapes):
+    """Register a scene's shape list with a device world or an oracle world (same calls)."""
+    for kind, params, pts in shapes:
+        if kind == MESH and "heights" in params:
+            w.heightfield(params["heights"], params["width"], params["depth"], params["cell"], params["options"])
+        elif kind == MESH:
+            w.mesh(params["vertices"], params["indices"])
+        else:
+            w.add_shape(kind, params, pts)
+
+
+def wavy_grid_mesh(nx, nz, origin, cell, amp, ax, az):
+    """The perf scenes' terrain (tools/perf_scenes.json "mesh" shapes: heights
+    amp * sin(ax * x) * cos(az * z) on an nx x nz grid, vertices z-major at
+    origin + (x, z) * cell, two triangles per cell wound (v00, v11, v10),
+    (v00, v01, v11) for +Y faces)."""
+    z, x = np.meshgrid(np.arange(nz), np.arange(nx), indexing="ij")
+    h = amp * np.sin(x * ax) * np.cos(z * az)
+    v = np.stack([origin[0] + x * cell[0], h, origin[1] + z * cell[1]], axis=-1).reshape(-1, 3)
+    idx = []
+    for zz in range(nz - 1):
+        for xx in range(nx - 1):
+            v00 = zz * nx + xx
+            v10, v01 = v00 + 1, v00 + nx
+            v11 = v01 + 1
+            idx += [[v00, v11, v10], [v00, v01, v11]]
+    return v.astype(np.float32), np.asarray(idx, dtype=np.uint32)
+
+
+def mesh_rain(nx=10, nz=10, layers=5, grid=20, steps=300):
+    """The reference's rain_500 / dbvt_rain_2000 perf scenes (tools/perf_scenes.json): a lattice of
+    boxes (half 0.35), spheres (r 0.35) and capsules (r 0.3, half height 0.5), the kind cycling
+    with (i + nz j + layer) % 3, spaced 1.4 x 2.0 x 1.4 m from 4 m up, raining onto a wavy
+    grid x grid terrain mesh (amp 0.2, ax 0.7, az 0.6, 1 m cells, centred); mass 1, friction
+    0.6, restitution 0; dt 1/60, 10 iterations. nx = nz = 10, grid 20 is rain_500; 20 x 20 with
+    grid 40 is dbvt_rain_2000."""
+    s = Scene(f"mesh_rain_{nx * nz * layers}", 1.0 / 60.0, 10, steps)
+    half = (grid - 1) / 2.0
+    v, idx = wavy_grid_mesh(grid, grid, (-half, -half), (1.0, 1.0), 0.2, 0.7, 0.6)
+    terrain = s.add_mesh(v, idx)
+    box = s.add_shape(BOX, [0.35, 0.35, 0.35])
+    sph = s.add_shape(SPHERE, [0.35])
+    cap = s.add_shape(CAPSULE, [0.3, 0.5])
+    s.add(terrain, (0.0, 0.0, 0.0), mass=0.0, friction=0.6)
+    bx = -0.7 * (nx - 1)
+    bz = -0.7 * (nz - 1)
+    for layer in range(layers):
+        for j in range(nz):
+            for i in range(nx):
+                kind = (box, sph, cap)[(i + nz * j + layer) % 3]
+                s.add(kind, (bx + i * 1.4, 4.0 + layer * 2.0, bz + j * 1.4), mass=1.0, friction=0.6)
+    return s
 
 
 def random_quat_small(rng, max_deg):
@@ -294,8 +358,7 @@ class BatchScene:
 
     def build_gpu(self, bgpu_module, **solver):
         w = bgpu_module.World(gravity=self.gravity, batch=True, num_iterations=self.iterations, **solver)
-        for kind, params, pts in self.shapes:
-            w.add_shape(kind, params, pts)
+        add_shapes(w, self.shapes)
         a = self.arrays()
         w.add_worlds_array(self.bodies_per_world, a["shape"], a["pos"], a["quat"], a["linvel"], a["angvel"],
                            a["mass"], a["friction"], a["restitution"])

@@ -50,6 +50,7 @@ typedef int32_t bgpu_status;
 #define BGPU_DEVSTAT_EPA_CAPACITY 0x010u      /* EPA vertex/face budget */
 #define BGPU_DEVSTAT_TRAVERSAL_STACK 0x040u   /* BVH traversal stack */
 #define BGPU_DEVSTAT_COLOUR_ROUNDS 0x080u     /* colouring did not converge */
+#define BGPU_DEVSTAT_MESH_CANDIDATES 0x100u   /* a convex-vs-mesh pair found over 64 candidate points */
 
 /* Shape kinds (crates/bullet-collision/src/shapes/mod.rs:61-85, convex subset + plane). */
 #define BGPU_SHAPE_SPHERE 0  /* params: radius */
@@ -57,6 +58,7 @@ typedef int32_t bgpu_status;
 #define BGPU_SHAPE_CAPSULE 2 /* params: radius, half height (segment along local Y) */
 #define BGPU_SHAPE_HULL 3    /* hull_points: n x 3 floats (must be convex) */
 #define BGPU_SHAPE_PLANE 4   /* params: normal x, y, z, constant (static bodies only) */
+#define BGPU_SHAPE_MESH 5    /* made by bgpu_add_mesh_shape / bgpu_add_heightfield_shape (static bodies only) */
 
 /* Body flags (crates/bullet-dynamics/src/body.rs:204-252). */
 #define BGPU_BODY_NO_CONTACT_RESPONSE 0x1u
@@ -251,6 +253,26 @@ bgpu_status bgpu_world_set_solver_info(bgpu_world* w, const bgpu_solver_info* in
 /* Shapes and bodies (world.rs:524-563). */
 bgpu_status bgpu_add_shape(bgpu_world* w, uint32_t type, const float* params, const float* hull_points,
                            uint32_t num_hull_points, uint32_t* out_shape);
+/* Static triangle mesh (CollisionShape::triangle_mesh, shapes/triangle_mesh.rs:59-123):
+ * nverts vertices (xyz) and ntris triangles (three vertex indices each). The library
+ * builds the reference's BVH (shapes/bvh.rs:36-206) on the host. Meshes collide with
+ * convex shapes (narrowphase/convex_mesh.rs:26-153) and take CCD sweeps
+ * (convex_sweep.rs:305-345); a body with a mesh shape must be static. */
+bgpu_status bgpu_add_mesh_shape(bgpu_world* w, const float* vertices, uint32_t nverts, const uint32_t* indices,
+                                uint32_t ntris, uint32_t* out_id);
+/* Heightfield (Heightfield::with_options, shapes/heightfield.rs:84-140), built into a
+ * static triangle mesh: width x depth row-major heights, cell_size xyz (x and z used),
+ * options: BGPU_HF_FLIP_QUAD_EDGES, BGPU_HF_DIAMOND, BGPU_HF_ZIGZAG, BGPU_HF_FLIP_WINDING,
+ * and the up axis (BGPU_HF_UP_Y, the default, BGPU_HF_UP_X, BGPU_HF_UP_Z). */
+#define BGPU_HF_FLIP_QUAD_EDGES 1u
+#define BGPU_HF_DIAMOND 2u
+#define BGPU_HF_ZIGZAG 4u
+#define BGPU_HF_FLIP_WINDING 8u
+#define BGPU_HF_UP_Y 0u
+#define BGPU_HF_UP_X 16u
+#define BGPU_HF_UP_Z 32u
+bgpu_status bgpu_add_heightfield_shape(bgpu_world* w, const float* heights, uint32_t width, uint32_t depth,
+                                       const float* cell_size, uint32_t options, uint32_t* out_id);
 bgpu_status bgpu_add_bodies(bgpu_world* w, uint32_t n, const bgpu_body_desc* descs, uint32_t* out_first);
 uint32_t bgpu_num_bodies(const bgpu_world* w);
 

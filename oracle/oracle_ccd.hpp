@@ -17,6 +17,7 @@
 #include <limits>
 #include <vector>
 #include "oracle_math.hpp"
+#include "oracle_shapes.hpp"
 
 namespace oracle {
 
@@ -216,6 +217,94 @@ bool sweep_plane(const V3<R>& from, const V3<R>& dir, R length, R radius, const 
     return true;
 }
 
+// convex_sweep.rs:217-262 (point_triangle_distance): squared distance from `point` to the
+// triangle and the vector from its closest point to `point`.
+template <class R>
+R point_triangle_distance(const V3<R>& point, const V3<R>& a, const V3<R>& b, const V3<R>& c, V3<R>& dv) {
+    V3<R> ab = b - a, ac = c - a, ap = point - a;
+    R d1 = ab.dot(ap), d2 = ac.dot(ap);
+    if (d1 <= R(0) && d2 <= R(0)) { dv = point - a; return dv.length_squared(); }
+    V3<R> bp = point - b;
+    R d3 = ab.dot(bp), d4 = ac.dot(bp);
+    if (d3 >= R(0) && d4 <= d3) { dv = point - b; return dv.length_squared(); }
+    R vc = d1 * d4 - d3 * d2;
+    if (vc <= R(0) && d1 >= R(0) && d3 <= R(0)) {
+        R v = d1 / (d1 - d3);
+        V3<R> q = a + ab * v;
+        dv = point - q;
+        return dv.length_squared();
+    }
+    V3<R> cp = point - c;
+    R d5 = ab.dot(cp), d6 = ac.dot(cp);
+    if (d6 >= R(0) && d5 <= d6) { dv = point - c; return dv.length_squared(); }
+    R vb = d5 * d2 - d1 * d6;
+    if (vb <= R(0) && d2 >= R(0) && d6 <= R(0)) {
+        R w = d2 / (d2 - d6);
+        V3<R> q = a + ac * w;
+        dv = point - q;
+        return dv.length_squared();
+    }
+    R va = d3 * d6 - d5 * d4;
+    if (va <= R(0) && (d4 - d3) >= R(0) && (d5 - d6) >= R(0)) {
+        R w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        V3<R> q = b + (c - b) * w;
+        dv = point - q;
+        return dv.length_squared();
+    }
+    R denom = R(1) / (va + vb + vc);
+    R v = vb * denom, w = vc * denom;
+    V3<R> q = a + ab * v + ac * w;
+    dv = point - q;
+    return dv.length_squared();
+}
+
+// convex_sweep.rs:131-151 (sweep_triangle)
+template <class R>
+bool sweep_triangle(const V3<R>& from, const V3<R>& dir, R length, R radius, const V3<R>& a, const V3<R>& b,
+                    const V3<R>& c, SweepHit<R>& hit) {
+    auto dist = [&](const V3<R>& p, R& d2, V3<R>& v) {
+        V3<R> dv;
+        R q = point_triangle_distance(p, a, b, c, dv);
+        if (q <= radius * radius) { d2 = 0; v = V3<R>(); return; }
+        R d = std::sqrt(q);
+        d2 = (d - radius) * (d - radius);
+        v = dv / d;
+    };
+    return sweep_with_dist(from, dir, length, radius, dist, hit);
+}
+
+// convex_sweep.rs:305-345 (sweep_mesh): in the mesh frame, the BVH candidates of the swept box,
+// the closest per-triangle hit.
+template <class R>
+bool sweep_mesh(const V3<R>& from, const V3<R>& to, R radius, const MeshData<R>& mesh, const V3<R>& pos,
+                const Quat<R>& ori, SweepHit<R>& hit) {
+    Quat<R> inv = ori.inverse();
+    V3<R> lf = inv.rotate(from - pos), lt = inv.rotate(to - pos);
+    V3<R> delta = lt - lf;
+    R length = delta.length();
+    if (length <= std::numeric_limits<R>::epsilon()) return false;
+    V3<R> dir = delta / length;
+    V3<R> rr = V3<R>::splat(radius);
+    Aabb<R> box(lf.min(lt) - rr, lf.max(lt) + rr);
+    std::vector<uint32_t> cand;
+    mesh.triangles_in_aabb(box, cand);
+    bool any = false;
+    SweepHit<R> best;
+    for (uint32_t t : cand) {
+        SweepHit<R> h;
+        if (sweep_triangle(lf, dir, length, radius, mesh.tri_vertex(t, 0), mesh.tri_vertex(t, 1), mesh.tri_vertex(t, 2), h) &&
+            (!any || h.fraction < best.fraction)) {
+            best = h;
+            any = true;
+        }
+    }
+    if (!any) return false;
+    hit.fraction = best.fraction;
+    hit.normal = ori.rotate(best.normal);
+    hit.point = ori.rotate(best.point) + pos;
+    return true;
+}
+
 // convex_sweep.rs:37-59 + :107-125: a sphere of `radius` cast from `from` to `to` against a shape
 // at (pos, ori).
 template <class R, class S>
@@ -225,6 +314,7 @@ bool swept_sphere_cast(const V3<R>& from, const V3<R>& to, R radius, const S& sh
     R length = delta.length();
     if (length <= std::numeric_limits<R>::epsilon()) return false;
     V3<R> dir = delta / length;
+    if (shape.type == SHAPE_MESH) return sweep_mesh(from, to, radius, *shape.mesh, pos, ori, hit);
     if (!shape.is_convex()) return sweep_plane(from, dir, length, radius, shape.normal, shape.constant, ori, hit);
     auto support = [&](const V3<R>& d) {
         V3<R> sphere = d.length_squared() > R(1e-12) ? d / d.length() * radius : V3<R>();
