@@ -716,23 +716,146 @@ __global__ void k_narrow_convex(BodyDev b, const Shape* __restrict__ shapes, con
     }
 }
 
-__global__ void k_narrow_mesh(BodyDev b, const Shape* __restrict__ shapes, const float4* __restrict__ hull,
-                              const uint64_t* __restrict__ pairs, uint32_t npairs, PairDataDev pd, uint32_t* status) {
+// The mesh route of the pair pass: one warp per pair. Lane 0 walks the mesh BVH and lists the
+// candidate triangles (those whose own box overlaps the query) in walk order; the lanes run the
+// per-triangle detectors side by side; lane 0 then keeps the hits in candidate order and reduces
+// them (the same points, in the same order, as collide_mesh's single pass).
+constexpr int MESH_WARPS = 4;
+constexpr int MESH_MAX_TRIS = 128;  // candidate triangles per pair (more: ST_MESH_CANDIDATES)
+
+__global__ void __launch_bounds__(32 * MESH_WARPS) k_narrow_mesh(BodyDev b, const Shape* __restrict__ shapes,
+                                                                 const float4* __restrict__ hull,
+                                                                 const uint64_t* __restrict__ pairs, uint32_t npairs,
+                                                                 PairDataDev pd, uint32_t* status) {
+    __shared__ uint32_t s_slot[MESH_WARPS][MESH_MAX_TRIS];
+    __shared__ float4 s_pt[MESH_WARPS][MESH_MAX_TRIS], s_nr[MESH_WARPS][MESH_MAX_TRIS];
+    __shared__ uint32_t s_n[MESH_WARPS];
     const uint32_t cnt = pd.scalars[ROUTE_COUNT0 + NP_MESH];
     if (blockIdx.x == 0 && threadIdx.x == 0) pd.scalars[1] += cnt;  // with the convex detections (statistics)
+    const uint32_t wi = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     EpaScratch scratch;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+    for (uint32_t t = blockIdx.x * MESH_WARPS + wi; t < cnt; t += gridDim.x * MESH_WARPS) {
         const uint32_t p = pd.route_list[size_t(NP_MESH - 1) * npairs + t];
         const uint64_t key = pairs[p];
         const uint32_t i = key_lo(key), j = key_hi(key);
-        const uint4 ia = b.info[i], ib = b.info[j];
-        const Shape sa = shapes[ia.x], sb = shapes[ib.x];
+        const Shape sa = shapes[b.info[i].x], sb = shapes[b.info[j].x];
+        const bool mesh_a = sa.type == SHAPE_MESH;
+        const Shape& cv = mesh_a ? sb : sa;
+        const Shape& ms = mesh_a ? sa : sb;
+        const uint32_t ic = mesh_a ? j : i, im = mesh_a ? i : j;
+        const V3 pc = from4(b.pred[ic]), pm = from4(b.pred[im]);
+        const Q qc = q4(b.quat[ic]), qm = q4(b.quat[im]);
         V3 seed = V3{0.f, 0.f, 0.f};
         const bool has_seed = entry_seed(pd.entries + size_t(p) * ENTRY_F4, seed);
-        Manifold m;
-        collide_mesh_pair(sa, from4(b.pred[i]), q4(b.quat[i]), sb, from4(b.pred[j]), q4(b.quat[j]), has_seed, seed,
-                          hull, scratch, m, status);
-        store_detection(pd, p, npairs, m);
+        const float thr = fminf(cv.cbt, ms.cbt);
+        const uint32_t tri_base = mesh_tri_base(ms);
+        if (lane == 0) {  // convex_mesh.rs:37-60 query box, bvh.rs:45-66 walk, triangle box filter
+            V3 wmn, wmx;
+            world_aabb(cv, pc, qc, hull, wmn, wmx);
+            const Q inv_m = qinv(qm);
+            const V3 c = (wmn + wmx) * 0.5f, e = (wmx - wmn) * 0.5f;
+            V3 lmin = splat(INFINITY), lmax = splat(-INFINITY);
+            for (int k = 0; k < 8; ++k) {
+                const V3 corner = V3{(k & 1) == 0 ? c.x + e.x : c.x - e.x, (k & 2) == 0 ? c.y + e.y : c.y - e.y,
+                                     (k & 4) == 0 ? c.z + e.z : c.z - e.z};
+                const V3 q = rotate(inv_m, corner - pm);
+                lmin = vmin(lmin, q);
+                lmax = vmax(lmax, q);
+            }
+            auto overlaps = [&](V3 a0, V3 a1) {
+                return a0.x <= lmax.x && a0.y <= lmax.y && a0.z <= lmax.z && lmin.x <= a1.x && lmin.y <= a1.y &&
+                       lmin.z <= a1.z;
+            };
+            uint32_t nc = 0;
+            uint32_t stack[MESH_STACK];
+            int sp = 0;
+            if (ms.hull_cnt) stack[sp++] = 0;
+            while (sp > 0) {
+                const uint32_t k = stack[--sp];
+                const float4 n0 = hull[ms.hull_off + 2 * k], n1 = hull[ms.hull_off + 2 * k + 1];
+                if (!overlaps(from4(n0), from4(n1))) continue;
+                const uint32_t na = __float_as_uint(n0.w), nb = __float_as_uint(n1.w);
+                if (!(na & MESH_LEAF)) {
+                    if (sp + 2 > MESH_STACK) {
+                        atomicOr(status, ST_TRAVERSAL_STACK);
+                        continue;
+                    }
+                    stack[sp++] = na;
+                    stack[sp++] = nb;
+                    continue;
+                }
+                const uint32_t start = na & ~MESH_LEAF;
+                for (uint32_t slot = start; slot < start + nb; ++slot) {
+                    const uint32_t o = tri_base + 3 * slot;
+                    const V3 ta = from4(hull[o]), tb = from4(hull[o + 1]), tc = from4(hull[o + 2]);
+                    if (!overlaps(vmin(ta, vmin(tb, tc)), vmax(ta, vmax(tb, tc)))) continue;
+                    if (nc == MESH_MAX_TRIS) {
+                        atomicOr(status, ST_MESH_CANDIDATES);
+                        continue;
+                    }
+                    s_slot[wi][nc++] = slot;
+                }
+            }
+            s_n[wi] = nc;
+        }
+        __syncwarp();
+        const uint32_t nc = s_n[wi];
+        const bool sphere = cv.type == SHAPE_SPHERE;
+        const V3 center = rotate(qinv(qm), pc - pm);
+        Shape tri;
+        tri.type = SHAPE_HULL;
+        tri.hull_cnt = 3;
+        tri.margin = 0.0f;
+        tri.cbt = thr;
+        for (uint32_t k = lane; k < nc; k += 32) {
+            const uint32_t o = tri_base + 3 * s_slot[wi][k];
+            V3 pt = V3{0.f, 0.f, 0.f}, nl = V3{0.f, 0.f, 0.f};
+            float pen = 0.0f;
+            bool hit = false;
+            if (sphere) {
+                if (sphere_triangle(center, cv.p0, thr, from4(hull[o]), from4(hull[o + 1]), from4(hull[o + 2]), pt, nl,
+                                    pen)) {
+                    pt = pm + rotate(qm, pt);
+                    nl = rotate(qm, -nl);
+                    hit = true;
+                }
+            } else {
+                tri.hull_off = o;
+                Manifold one;
+                collide_convex(cv, pc, qc, tri, pm, qm, has_seed, seed, hull, scratch, one, status);
+                if (one.n) {
+                    pt = one.pos[0];
+                    nl = one.nrm[0];
+                    pen = one.pen[0];
+                    hit = true;
+                }
+            }
+            s_pt[wi][k] = to4(pt, pen);
+            s_nr[wi][k] = to4(nl, hit ? 1.0f : 0.0f);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            MeshCandidates cand;
+            cand.n = 0;
+            for (uint32_t k = 0; k < nc; ++k) {
+                const float4 nr = s_nr[wi][k];
+                if (nr.w == 0.0f) continue;
+                if (cand.n == MESH_MAX_CAND) {
+                    atomicOr(status, ST_MESH_CANDIDATES);
+                    break;
+                }
+                const float4 pt = s_pt[wi][k];
+                cand.pos[cand.n] = from4(pt);
+                cand.pen[cand.n] = pt.w;
+                cand.nrm[cand.n] = from4(nr);
+                ++cand.n;
+            }
+            Manifold m;
+            reduce_to_manifold(cand, m);
+            if (mesh_a) mf_flip(m);
+            store_detection(pd, p, npairs, m);
+        }
+        __syncwarp();  // the warp's shared lists are reused by its next pair
     }
 }
 
@@ -865,7 +988,10 @@ void run_pair_pass(const WorldView& w, const uint64_t* pairs, uint32_t npairs, c
     k_narrow_analytic<<<grid, TB, 0, s>>>(w.b, w.shapes, w.hull, pairs, npairs, d);
     uint32_t cgrid = std::min<uint32_t>((npairs + 63) / 64, 148u * 8u);
     k_narrow_convex<<<cgrid, 64, 0, s>>>(w.b, w.shapes, w.hull, pairs, npairs, d, status_dev);
-    if (w.has_mesh) k_narrow_mesh<<<cgrid, 64, 0, s>>>(w.b, w.shapes, w.hull, pairs, npairs, d, status_dev);
+    if (w.has_mesh) {
+        const uint32_t mgrid = std::min<uint32_t>((npairs + MESH_WARPS - 1) / MESH_WARPS, 148u * 8u);
+        k_narrow_mesh<<<mgrid, 32 * MESH_WARPS, 0, s>>>(w.b, w.shapes, w.hull, pairs, npairs, d, status_dev);
+    }
     k_capture<<<grid, TB, 0, s>>>(w.b, w.shapes, pairs, npairs, sp, d);
 }
 

@@ -136,7 +136,7 @@ struct World {
         pred, iw, push_lin, push_ang;
     DevBuf<uint4> info_d;
     DevBuf<float> settled;
-    std::vector<uint32_t> unbounded;  // plane bodies (kept out of the BVH)
+    std::vector<uint32_t> unbounded;  // plane and mesh bodies (kept out of the BVH)
     // batched worlds: world k owns bodies [world_off_h[k], world_off_h[k + 1])
     bool batch = false;
     std::vector<uint32_t> world_off_h{0u};
@@ -502,7 +502,9 @@ struct World {
             hsl[k] = make_float4(0.0f, lt, at, 0.0f);
             uint32_t group = b.group, mask = b.mask;
             hinfo[k] = make_uint4(b.shape, fl, act, group | (mask << 16));
-            if (s.type == SHAPE_PLANE) unbounded.push_back(first + k);
+            // Planes, and static meshes (a terrain's box overlaps most bodies, and a tree walk
+            // from it would list them one by one), go through the broad phase's all-bodies pass.
+            if (s.type == SHAPE_PLANE || s.type == SHAPE_MESH) unbounded.push_back(first + k);
         }
         auto up = [&](DevBuf<float4>& dst, const std::vector<float4>& src) {
             check_cuda(cudaMemcpyAsync(dst.p + first, src.data(), cnt * sizeof(float4), cudaMemcpyHostToDevice, stream),
