@@ -165,7 +165,8 @@ void launch_integrate_positions(const BodyDev& b, uint32_t n, float dt, float tu
 void launch_ccd_sweep(const BodyDev& b, const Shape* shapes, const float4* hull, const uint32_t* ids, const float2* par,
                       uint32_t m, uint32_t n, const uint32_t* world_off, const uint32_t* world_of,
                       const uint64_t* suppressed, uint32_t nsuppressed, float dt, float* clamp, uint32_t* status,
-                      cudaStream_t s);
+                      const float4* tree_rec, const uint32_t* tree_leaf, int tree_m, const uint32_t* unb,
+                      uint32_t nunb, cudaStream_t s);
 void launch_ccd_apply(const BodyDev& b, const uint32_t* ids, const float* clamp, uint32_t m, float dt, cudaStream_t s);
 // Host-facing layouts: n x 3 floats -> float4 lanes, and poses -> n x 7 floats.
 void launch_unpack3(uint32_t n, const float* src, float4* dst, cudaStream_t s);
@@ -186,6 +187,8 @@ struct Broadphase {
     DevBuf<int> bounds;          // 6 ordered ints: scene min/max of leaf centres
     DevBuf<uint32_t> scalars;    // [0] total pairs, [1] proxies with more partners than the stash holds
     uint32_t* host_scalars = nullptr;  // pinned
+    int tree_m = 0;                    // bounded proxies in the last run's tree (0: no tree)
+    uint32_t nunb = 0;                 // proxies of the last run kept out of the tree (device list `unbounded`)
     Broadphase();
     ~Broadphase();
     // Returns the pair count; pairs are written to `out` (grown as needed).

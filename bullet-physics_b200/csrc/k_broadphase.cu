@@ -425,6 +425,8 @@ uint64_t Broadphase::run(const float4* aabb_min, const float4* aabb_max, uint32_
     if (n == 0) return 0;
     const uint32_t nunb = uint32_t(unbounded_host.size());
     const int m = int(n - nunb);
+    tree_m = m;
+    this->nunb = nunb;
     const int TB = 256;
     const uint32_t grid = (n + TB - 1) / TB;
     keys.reserve(n);

@@ -342,6 +342,8 @@ __device__ __forceinline__ bool body_active(uint32_t act) {
 // every candidate.
 constexpr int CCD_THREADS = 32;
 constexpr int CCD_CAP = 256;
+constexpr uint32_t CCD_TREE_CAP = 1024;          // tree hits per CCD body before the world scan
+constexpr uint32_t TREE_LEAF_REF = 0x80000000u;  // leaf children in the broad-phase node records
 
 struct CcdCtx {
     V3 from, to, dir;
@@ -377,8 +379,13 @@ __global__ void __launch_bounds__(CCD_THREADS) k_ccd_sweep(BodyDev b, const Shap
                                                            const uint32_t* __restrict__ world_off,
                                                            const uint32_t* __restrict__ world_of,
                                                            const uint64_t* __restrict__ suppressed, uint32_t nsuppressed,
-                                                           float dt, float* clamp, uint32_t* status) {
+                                                           float dt, float* clamp, uint32_t* status,
+                                                           const float4* __restrict__ tree_rec,
+                                                           const uint32_t* __restrict__ tree_leaf, int tree_m,
+                                                           const uint32_t* __restrict__ unb, uint32_t nunb) {
     __shared__ uint32_t cand[CCD_CAP], sorted[CCD_CAP];
+    __shared__ uint32_t tlist[CCD_TREE_CAP];
+    __shared__ uint32_t ntl;
     __shared__ float lb[CCD_CAP], slb[CCD_CAP];
     __shared__ uint32_t ncand;
     const uint32_t k = blockIdx.x, lane = threadIdx.x;
@@ -412,10 +419,53 @@ __global__ void __launch_bounds__(CCD_THREADS) k_ccd_sweep(BodyDev b, const Shap
     const uint32_t gi = info.w & 0xFFFFu, mi = info.w >> 16;
     uint32_t lo = 0, hi = n;
     if (world_of) { lo = world_off[world_of[i]]; hi = world_off[world_of[i] + 1]; }
-    if (lane == 0) ncand = 0;
+    // The targets: in a plain world, the step's broad-phase tree gives the proxies whose boxes
+    // touch the swept box (the same closed test as the scan below, so the same set), plus the
+    // proxies kept out of the tree (planes, meshes); in a batch, or when the list overflows,
+    // every body of the world.
+    const bool use_tree = tree_rec && !world_of && tree_m >= 1;
+    if (lane == 0) {
+        ncand = 0;
+        ntl = 0;
+        if (use_tree) {
+            uint32_t cnt = 0;
+            auto push = [&](uint32_t j) {
+                if (cnt < CCD_TREE_CAP) tlist[cnt] = j;
+                ++cnt;
+            };
+            const float4 qmin = make_float4(smin.x, smin.y, smin.z, 0.0f), qmax = make_float4(smax.x, smax.y, smax.z, 0.0f);
+            auto touch = [&](float4 a, float4 b) {
+                return a.x <= qmax.x && a.y <= qmax.y && a.z <= qmax.z && qmin.x <= b.x && qmin.y <= b.y && qmin.z <= b.z;
+            };
+            if (tree_m == 1) {
+                push(tree_leaf[0]);
+            } else {
+                uint32_t stack[64];
+                int sp = 0;
+                stack[sp++] = 0u;
+                while (sp > 0 && cnt <= CCD_TREE_CAP) {
+                    const float4* r = tree_rec + size_t(stack[--sp]) * 4;
+                    const float4 a = r[0], bb = r[1], cc = r[2], d = r[3];
+                    const uint32_t ref[2] = {__float_as_uint(a.w), __float_as_uint(bb.w)};
+                    const bool hit[2] = {touch(a, bb), touch(cc, d)};
+                    for (int q = 0; q < 2; ++q) {
+                        if (!hit[q]) continue;
+                        if (ref[q] & TREE_LEAF_REF) push(ref[q] & ~TREE_LEAF_REF);
+                        else if (sp < 64) stack[sp++] = ref[q];
+                        else atomicOr(status, ST_TRAVERSAL_STACK);
+                    }
+                }
+            }
+            for (uint32_t u = 0; u < nunb; ++u) push(unb[u]);
+            ntl = cnt;
+        }
+    }
     __syncthreads();
+    const bool from_tree = use_tree && ntl <= CCD_TREE_CAP;
+    const uint32_t nsrc = from_tree ? ntl : hi - lo;
     float best = 1.0f;
-    for (uint32_t j = lo + lane; j < hi; j += CCD_THREADS) {
+    for (uint32_t s = lane; s < nsrc; s += CCD_THREADS) {
+        const uint32_t j = from_tree ? tlist[s] : lo + s;
         if (j == i) continue;
         const uint4 oj = b.info[j];
         if (oj.y & BF_NO_RESPONSE) continue;
@@ -462,7 +512,8 @@ __global__ void __launch_bounds__(CCD_THREADS) k_ccd_sweep(BodyDev b, const Shap
     if (nc > CCD_CAP) {
         // too many candidates for the buffer: cast every candidate that passes the same tests
         float mine = best;
-        for (uint32_t j = lo + lane; j < hi; j += CCD_THREADS) {
+        for (uint32_t s = lane; s < nsrc; s += CCD_THREADS) {
+            const uint32_t j = from_tree ? tlist[s] : lo + s;
             if (j == i) continue;
             const uint4 oj = b.info[j];
             if ((oj.y & BF_NO_RESPONSE) || shapes[oj.x].type == SHAPE_PLANE) continue;
@@ -515,10 +566,11 @@ __global__ void k_ccd_apply(BodyDev b, const uint32_t* __restrict__ ids, const f
 void launch_ccd_sweep(const BodyDev& b, const Shape* shapes, const float4* hull, const uint32_t* ids, const float2* par,
                       uint32_t m, uint32_t n, const uint32_t* world_off, const uint32_t* world_of,
                       const uint64_t* suppressed, uint32_t nsuppressed, float dt, float* clamp, uint32_t* status,
-                      cudaStream_t s) {
+                      const float4* tree_rec, const uint32_t* tree_leaf, int tree_m, const uint32_t* unb,
+                      uint32_t nunb, cudaStream_t s) {
     if (m == 0) return;
     k_ccd_sweep<<<m, CCD_THREADS, 0, s>>>(b, shapes, hull, ids, par, n, world_off, world_of, suppressed, nsuppressed,
-                                          dt, clamp, status);
+                                          dt, clamp, status, tree_rec, tree_leaf, tree_m, unb, nunb);
 }
 
 void launch_ccd_apply(const BodyDev& b, const uint32_t* ids, const float* clamp, uint32_t m, float dt, cudaStream_t s) {

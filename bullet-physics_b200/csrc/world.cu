@@ -917,7 +917,9 @@ struct World {
         mark(7);
         // 7a: CCD clamp fractions, from the solved velocities and the pre-integration poses
         launch_ccd_sweep(b, shapes_d.p, hull_d.p, ccd_ids_d.p, ccd_par_d.p, nccd, n, batch ? world_off_d.p : nullptr,
-                         world_of, sp.suppressed, sp.nsuppressed, dt, ccd_clamp_d.p, status, stream);
+                         world_of, sp.suppressed, sp.nsuppressed, dt, ccd_clamp_d.p, status,
+                         batch ? nullptr : bp.node_rec.p, bp.leaf_body.p, batch ? 0 : bp.tree_m, bp.unbounded.p,
+                         batch ? 0u : bp.nunb, stream);
         // 6c + 7 + 8: deactivation, pose integration with the split push, force clear.
         launch_integrate_positions(b, n, dt, info.split_impulse_turn_erp, stream);
         launch_ccd_apply(b, ccd_ids_d.p, ccd_clamp_d.p, nccd, dt, stream);
