@@ -147,6 +147,8 @@ struct World {
     WorldPlan wplan;
     uint32_t wplan_block = 128, wplan_tau = 64;  // 0 threads: the global (all-worlds) solver
     DevBuf<uint32_t> wcol;
+    DevBuf<uint32_t> plain_off_d;    // a plain world's {0, n}, for the per-world solver
+    static constexpr uint32_t PLAIN_WORLD_SOLVER_MAX_BODIES = 2048;
     bool last_world_solver = false;  // the last step ran the per-world solver
     float tuned_ms = 0.0f, tuned_global_ms = 0.0f;
     uint32_t tuned_candidates = 0;
@@ -450,7 +452,9 @@ struct World {
 
     uint32_t add_bodies(uint32_t cnt, const bgpu_body_desc* d) {
         if (batch) throw InvalidArg{"a batched world takes bodies through bgpu_batch_add_worlds"};
-        return add_bodies_impl(cnt, d);
+        const uint32_t first = add_bodies_impl(cnt, d);
+        rebuild_world_plan();
+        return first;
     }
 
     uint32_t add_bodies_impl(uint32_t cnt, const bgpu_body_desc* d) {
@@ -568,12 +572,25 @@ struct World {
     // joints, falls back to the global solver).
     void rebuild_world_plan() {
         wplan.valid = false;
-        if (!batch || wplan_block == 0) return;
+        if (!batch) {
+            // A plain world small enough for one CTA's shared memory is solved as a batch of one
+            // world (one CTA of 256 threads, velocities in shared memory, block-local syncs).
+            if (n == 0 || n > PLAIN_WORLD_SOLVER_MAX_BODIES) return;
+            const std::vector<uint32_t> off{0u, n};
+            plain_off_d.reserve(2);
+            check_cuda(cudaMemcpyAsync(plain_off_d.p, off.data(), 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, stream),
+                       "h2d");
+            wcol.reserve(WS_STRIDE + 1);
+            build_world_plan(off, 256u, 0u, wplan, stream);
+            return;
+        }
+        if (wplan_block == 0) return;
         wcol.reserve(size_t(num_worlds()) * WS_STRIDE + 1);
         build_world_plan(world_off_h, wplan_block, wplan_tau, wplan, stream);
     }
 
-    bool use_world_solver() const { return batch && wplan.valid && joints_h.empty(); }
+    bool use_world_solver() const { return wplan.valid && joints_h.empty(); }
+    const uint32_t* world_offsets_dev() const { return batch ? world_off_d.p : plain_off_d.p; }
 
     JointsDev joints_dev() {
         JointsDev j;
@@ -904,8 +921,8 @@ struct World {
         // The colouring starts from last step's colours, except every RECOLOUR_PERIOD-th step.
         last_world_solver = use_world_solver();
         if (last_world_solver)
-            run_world_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); }, world_off_d.p,
-                             nw, wplan, wcol.p);
+            run_world_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); },
+                             world_offsets_dev(), nw, wplan, wcol.p);
         else
             run_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); },
                        step_count % RECOLOUR_PERIOD != 0, &jd);
