@@ -131,12 +131,16 @@ constexpr int MAX_COLOURS = 128;
 // writes them.
 //
 // Velocity table planes: 0 n|friction 1 r_a|bias 2 r_b|bias 3 t1|1/m_a
-// 4 t2|1/m_b 5 Iw_a(r_a x n)|normal mass 6 Iw_b(r_b x n)|t1 mass
-// 7 Iw_a(r_a x t1)|t2 mass 8 Iw_b(r_b x t1)|cfm 9 Iw_a(r_a x t2)|restitution
-// 10 Iw_b(r_b x t2) 11 kn 12 kt1 13 kt2 14 accumulated impulses (row 3).
+// 4 Iw_a(r_a x n)|normal mass 5 Iw_b(r_b x n)|t1 mass 6 Iw_a(r_a x t1)|t2 mass
+// 7 Iw_b(r_b x t1)|cfm 8 Iw_a(r_a x t2)|restitution 9 Iw_b(r_b x t2)|1/m_b
+// 10 accumulated impulses (row 3). The second tangent t2 = n x t1 and the velocity couplings
+// kn / kt1 / kt2 are recomputed by each sweep with the same operations that first made them
+// (so their values are the same), which keeps a large pile's table (176 B per contact) inside L2.
 // Split table planes: 0 n|normal mass 1 r_a|cfm 2 r_b 3 Iw_a(r_a x n)|1/m_a
 // 4 Iw_b(r_b x n)|1/m_b 5 row 5 (rhs, push impulse, active, penetration).
-constexpr uint32_t VT_PLANES = 15;
+constexpr uint32_t VT_PLANES = 11;
+enum : uint32_t { VT_N = 0, VT_RA = 1, VT_RB = 2, VT_T1 = 3, VT_ANA = 4, VT_ANB = 5, VT_A1A = 6, VT_A1B = 7,
+                  VT_A2A = 8, VT_A2B = 9, VT_IMP = 10 };
 constexpr uint32_t ST_PLANES = 6;
 
 // Adjoint sweep record of (sweep >= 1, contact k, slot t), in 32-slot blocks like the tables.

@@ -90,7 +90,8 @@ __device__ __forceinline__ void reverse_group(const AdjArgs& a, uint32_t t, uint
     const uint4 rec = a.recs[t];
     const uint32_t ia = rec.x, ib = rec.y, p = rec.z & 0x1fffffffu, cnt = rec.z >> 29;
     const float4* e0 = a.tab + tix<VT_PLANES>(0, 0, t);
-    const float ima = e0[3 * PLANE_STRIDE].w, imb = e0[4 * PLANE_STRIDE].w;
+    const float ima = e0[VT_T1 * PLANE_STRIDE].w, imb = e0[VT_A2B * PLANE_STRIDE].w;
+    const float ims = ima + imb;
     const bool appa = ima > 0.0f, appb = imb > 0.0f;
     V3 La = from4(__ldcg(&a.vbar[ia])), Wa = from4(__ldcg(&a.wbar[ia]));
     V3 Lb = from4(__ldcg(&a.vbar[ib])), Wb = from4(__ldcg(&a.wbar[ib]));
@@ -112,8 +113,8 @@ __device__ __forceinline__ void reverse_group(const AdjArgs& a, uint32_t t, uint
     for (int kk = int(cnt) - 1; kk >= 0; --kk) {
         const uint32_t k = uint32_t(kk);
         const float4* e = a.tab + tix<VT_PLANES>(0, k, t);
-        const V3 n = from4(e[0 * PLANE_STRIDE]);
-        const V3 ana = from4(e[5 * PLANE_STRIDE]), anb = from4(e[6 * PLANE_STRIDE]);
+        const V3 n = from4(e[VT_N * PLANE_STRIDE]);
+        const V3 ana = from4(e[VT_ANA * PLANE_STRIDE]), anb = from4(e[VT_ANB * PLANE_STRIDE]);
         float4 lb = a.lbar[lix(k, t)];
         if (sweep == 0) {  // warm start: only the normal impulse is nonzero (step.rs:751)
             const float lin = lb.x + japp(n, ana, anb);
@@ -121,14 +122,15 @@ __device__ __forceinline__ void reverse_group(const AdjArgs& a, uint32_t t, uint
             if (src != REC_NONE && a.carry_out) atomicAdd(&a.carry_out[src], a.warm_factor * lin);
             continue;
         }
-        const float4 r0 = e[0 * PLANE_STRIDE], r1 = e[1 * PLANE_STRIDE], r2 = e[2 * PLANE_STRIDE];
-        const float4 q3 = e[3 * PLANE_STRIDE], q4 = e[4 * PLANE_STRIDE];
-        const float4 q5 = e[5 * PLANE_STRIDE], q6 = e[6 * PLANE_STRIDE];
-        const float4 q7 = e[7 * PLANE_STRIDE], q8 = e[8 * PLANE_STRIDE];
-        const float4 q9 = e[9 * PLANE_STRIDE], q10 = e[10 * PLANE_STRIDE];
-        const V3 ra = from4(r1), rb = from4(r2), t1 = from4(q3), t2 = from4(q4);
+        const float4 r0 = e[VT_N * PLANE_STRIDE], r1 = e[VT_RA * PLANE_STRIDE], r2 = e[VT_RB * PLANE_STRIDE];
+        const float4 q3 = e[VT_T1 * PLANE_STRIDE];
+        const float4 q5 = e[VT_ANA * PLANE_STRIDE], q6 = e[VT_ANB * PLANE_STRIDE];
+        const float4 q7 = e[VT_A1A * PLANE_STRIDE], q8 = e[VT_A1B * PLANE_STRIDE];
+        const float4 q9 = e[VT_A2A * PLANE_STRIDE], q10 = e[VT_A2B * PLANE_STRIDE];
+        const V3 ra = from4(r1), rb = from4(r2), t1 = from4(q3), t2 = cross(n, t1);
         const V3 a1a = from4(q7), a1b = from4(q8), a2a = from4(q9), a2b = from4(q10);
-        const V3 kn = from4(e[11 * PLANE_STRIDE]), kt1 = from4(e[12 * PLANE_STRIDE]);
+        const V3 kn = n * ims + cross(anb, rb) + cross(ana, ra);  // as the forward sweep makes them
+        const V3 kt1 = t1 * ims + cross(a1b, rb) + cross(a1a, ra);
         const float mn = q5.w, m1 = q6.w, m2 = q7.w, cfm = q8.w, e_ab = q9.w, mu_ab = r0.w;
         const float4 sr = a.sweeps[sweep_index(sweep, k, t, a.iters)];
         const float vn = sr.x, nimp = sr.y;

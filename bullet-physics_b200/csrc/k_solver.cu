@@ -471,29 +471,20 @@ __device__ __forceinline__ void warm_group(const SolveArgs& a, uint32_t t, uint3
         const V3 ana = mul(iwa, cross(ra, n)), anb = mul(iwb, cross(rb, n));
         const V3 a1a = mul(iwa, cross(ra, t1)), a1b = mul(iwb, cross(rb, t1));
         const V3 a2a = mul(iwa, cross(ra, t2)), a2b = mul(iwb, cross(rb, t2));
-        const float ims = ima + imb;
-        const V3 kn = n * ims + cross(anb, rb) + cross(ana, ra);
-        const V3 kt1 = t1 * ims + cross(a1b, rb) + cross(a1a, ra);
-        const V3 kt2 = t2 * ims + cross(a2b, rb) + cross(a2a, ra);
         apply(la, wa, lb, wb, appa, appb, ima, imb, n, ana, anb, r3.x);
         apply(la, wa, lb, wb, appa, appb, ima, imb, t1, a1a, a1b, r3.y);
         apply(la, wa, lb, wb, appa, appb, ima, imb, t2, a2a, a2b, r3.z);
-        float4* v = a.vtab;
-        e[0 * PLANE_STRIDE] = r0;
-        e[1 * PLANE_STRIDE] = r1;
-        e[2 * PLANE_STRIDE] = r2;
-        e[3 * PLANE_STRIDE] = f4(t1, ima);
-        e[4 * PLANE_STRIDE] = f4(t2, imb);
-        e[5 * PLANE_STRIDE] = f4(ana, r4.x);
-        e[6 * PLANE_STRIDE] = f4(anb, r4.y);
-        e[7 * PLANE_STRIDE] = f4(a1a, r4.z);
-        e[8 * PLANE_STRIDE] = f4(a1b, r4.w);
-        e[9 * PLANE_STRIDE] = f4(a2a, r3.w);
-        e[10 * PLANE_STRIDE] = f4(a2b, 0.0f);
-        e[11 * PLANE_STRIDE] = f4(kn, 0.0f);
-        e[12 * PLANE_STRIDE] = f4(kt1, 0.0f);
-        e[13 * PLANE_STRIDE] = f4(kt2, 0.0f);
-        e[14 * PLANE_STRIDE] = r3;
+        e[VT_N * PLANE_STRIDE] = r0;
+        e[VT_RA * PLANE_STRIDE] = r1;
+        e[VT_RB * PLANE_STRIDE] = r2;
+        e[VT_T1 * PLANE_STRIDE] = f4(t1, ima);
+        e[VT_ANA * PLANE_STRIDE] = f4(ana, r4.x);
+        e[VT_ANB * PLANE_STRIDE] = f4(anb, r4.y);
+        e[VT_A1A * PLANE_STRIDE] = f4(a1a, r4.z);
+        e[VT_A1B * PLANE_STRIDE] = f4(a1b, r4.w);
+        e[VT_A2A * PLANE_STRIDE] = f4(a2a, r3.w);
+        e[VT_A2B * PLANE_STRIDE] = f4(a2b, imb);
+        e[VT_IMP * PLANE_STRIDE] = r3;
     }
 }
 
@@ -504,23 +495,25 @@ __device__ __forceinline__ void warm_group(const SolveArgs& a, uint32_t t, uint3
 __device__ __forceinline__ void iter_group(const SolveArgs& a, uint32_t t, uint32_t p, uint32_t cnt, uint32_t sweep,
                                            bool last, V3& la, V3& wa, V3& lb, V3& wb, bool& appa, bool& appb) {
     const float4* e0 = a.vtab + tix<VT_PLANES>(0, 0, t);
-    const float ima = e0[3 * PLANE_STRIDE].w, imb = e0[4 * PLANE_STRIDE].w;
+    const float ima = e0[VT_T1 * PLANE_STRIDE].w, imb = e0[VT_A2B * PLANE_STRIDE].w;
+    const float ims = ima + imb;
     appa = ima > 0.0f;
     appb = imb > 0.0f;
     for (uint32_t k = 0; k < cnt; ++k) {
         float4* e = a.vtab + tix<VT_PLANES>(0, k, t);
-        const float4 r0 = e[0 * PLANE_STRIDE], r1 = e[1 * PLANE_STRIDE],
-                     r2 = e[2 * PLANE_STRIDE];
-        const float4 q3 = e[3 * PLANE_STRIDE], q4 = e[4 * PLANE_STRIDE];
-        const float4 q5 = e[5 * PLANE_STRIDE], q6 = e[6 * PLANE_STRIDE];
-        const float4 q7 = e[7 * PLANE_STRIDE], q8 = e[8 * PLANE_STRIDE];
-        const float4 q9 = e[9 * PLANE_STRIDE], q10 = e[10 * PLANE_STRIDE];
-        const float4 q11 = e[11 * PLANE_STRIDE], q12 = e[12 * PLANE_STRIDE];
-        const float4 q13 = e[13 * PLANE_STRIDE];
-        const float4 r3 = e[14 * PLANE_STRIDE];
-        const V3 n = from4(r0), ra = from4(r1), rb = from4(r2), t1 = from4(q3), t2 = from4(q4);
+        const float4 r0 = e[VT_N * PLANE_STRIDE], r1 = e[VT_RA * PLANE_STRIDE], r2 = e[VT_RB * PLANE_STRIDE];
+        const float4 q3 = e[VT_T1 * PLANE_STRIDE];
+        const float4 q5 = e[VT_ANA * PLANE_STRIDE], q6 = e[VT_ANB * PLANE_STRIDE];
+        const float4 q7 = e[VT_A1A * PLANE_STRIDE], q8 = e[VT_A1B * PLANE_STRIDE];
+        const float4 q9 = e[VT_A2A * PLANE_STRIDE], q10 = e[VT_A2B * PLANE_STRIDE];
+        const float4 r3 = e[VT_IMP * PLANE_STRIDE];
+        const V3 n = from4(r0), ra = from4(r1), rb = from4(r2), t1 = from4(q3);
+        const V3 t2 = cross(n, t1);  // tangent_basis (sequential_impulse.rs:620-629), as warm_group made it
         const V3 ana = from4(q5), anb = from4(q6), a1a = from4(q7), a1b = from4(q8), a2a = from4(q9), a2b = from4(q10);
-        const V3 kn = from4(q11), kt1 = from4(q12), kt2 = from4(q13);
+        // The velocity couplings of sequential_impulse.rs:352-520, in warm_group's operand order.
+        const V3 kn = n * ims + cross(anb, rb) + cross(ana, ra);
+        const V3 kt1 = t1 * ims + cross(a1b, rb) + cross(a1a, ra);
+        const V3 kt2 = t2 * ims + cross(a2b, rb) + cross(a2a, ra);
         const float4 r4 = make_float4(q5.w, q6.w, q7.w, q8.w);
         V3 va = la + cross(wa, ra);
         V3 vb = lb + cross(wb, rb);
@@ -558,7 +551,7 @@ __device__ __forceinline__ void iter_group(const SolveArgs& a, uint32_t t, uint3
             const uint32_t s2 = u2 > maxf ? 1u : (u2 < -maxf ? 2u : 0u);
             a.srec[sweep_index(sweep, k, t, a.iterations)] = make_float4(vn, nimp, __uint_as_float(s1 | (s2 << 2)), 0.0f);
         }
-        e[14 * PLANE_STRIDE] = nr3;
+        e[VT_IMP * PLANE_STRIDE] = nr3;
         if (last) a.rows[(size_t(p) * 4 + k) * ROW_F4 + 3] = nr3;
     }
 }
