@@ -254,6 +254,8 @@ void launch_joint_rows(const BodyDev& b, const JointsDev& j, float inv_dt, float
 
 // solve_joint_row (sequential_impulse.rs:931-971) over the rows of one joint slot; the
 // two bodies' velocities come from and go back to L2 (dynamic bodies only).
+// SHARED: linvel / angvel point into shared memory (the per-world solver), not global memory.
+template <bool SHARED = false>
 __device__ __forceinline__ void solve_joint_slot(const JointsDev& jd, uint32_t t, float4* linvel, float4* angvel,
                                                  const float4* __restrict__ iw, float damping) {
     const uint32_t cnt = jd.count[t];
@@ -268,8 +270,14 @@ __device__ __forceinline__ void solve_joint_slot(const JointsDev& jd, uint32_t t
     };
     float ima, imb;
     const M3 iia = load_iw_j(ia, ima), iib = load_iw_j(ib, imb);
-    V3 la = from4(__ldcg(&linvel[ia])), wa = from4(__ldcg(&angvel[ia]));
-    V3 lb = from4(__ldcg(&linvel[ib])), wb = from4(__ldcg(&angvel[ib]));
+    V3 la, wa, lb, wb;
+    if (SHARED) {
+        la = from4(linvel[ia]); wa = from4(angvel[ia]);
+        lb = from4(linvel[ib]); wb = from4(angvel[ib]);
+    } else {
+        la = from4(__ldcg(&linvel[ia])); wa = from4(__ldcg(&angvel[ia]));
+        lb = from4(__ldcg(&linvel[ib])); wb = from4(__ldcg(&angvel[ib]));
+    }
     float4* row = jd.rows + size_t(jd.row_off[t]) * JROW_F4;
     for (uint32_t r = 0; r < cnt; ++r, row += JROW_F4) {
         const float4 r0 = row[0], r1 = row[1], r2 = row[2], r3 = row[3], r4 = row[4];
@@ -294,8 +302,13 @@ __device__ __forceinline__ void solve_joint_slot(const JointsDev& jd, uint32_t t
             wb += mul(iib, ang_b * j);
         }
     }
-    if (ima > 0.0f) { __stcg(&linvel[ia], to4(la, 0.0f)); __stcg(&angvel[ia], to4(wa, 0.0f)); }
-    if (imb > 0.0f) { __stcg(&linvel[ib], to4(lb, 0.0f)); __stcg(&angvel[ib], to4(wb, 0.0f)); }
+    if (SHARED) {
+        if (ima > 0.0f) { linvel[ia] = to4(la, 0.0f); angvel[ia] = to4(wa, 0.0f); }
+        if (imb > 0.0f) { linvel[ib] = to4(lb, 0.0f); angvel[ib] = to4(wb, 0.0f); }
+    } else {
+        if (ima > 0.0f) { __stcg(&linvel[ia], to4(la, 0.0f)); __stcg(&angvel[ia], to4(wa, 0.0f)); }
+        if (imb > 0.0f) { __stcg(&linvel[ib], to4(lb, 0.0f)); __stcg(&angvel[ib], to4(wb, 0.0f)); }
+    }
 }
 
 struct Islands {
@@ -485,9 +498,12 @@ bool build_world_plan(const std::vector<uint32_t>& world_off, uint32_t block, ui
 // The PGS of every world of a batch (no joints): world-local colouring, batches and solve.
 // Writes pd.colour (world-local colours), pd.batch_rec (slots grouped per world, then colour),
 // the per-world records `wcol` (WS_STRIDE words per world) and the step's counts in pd.scalars.
+// joints (a plain world only, whose bodies start at index 0): joint rows solved after each
+// velocity sweep's contacts, joint colour by joint colour, as the global solver does.
 void run_world_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
                       uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark,
-                      const uint32_t* world_off, uint32_t nworlds, const WorldPlan& plan, uint32_t* wcol);
+                      const uint32_t* world_off, uint32_t nworlds, const WorldPlan& plan, uint32_t* wcol,
+                      const JointsDev* joints = nullptr);
 // One team barrier that nothing completes (2 blocks): the wait gives up after limit_ns and
 // leaves ST_BARRIER_TIMEOUT in *status. ctr and status are device words the caller zeroes.
 void run_wait_selftest(unsigned long long limit_ns, unsigned int* ctr, uint32_t* status, cudaStream_t s);

@@ -916,7 +916,7 @@ __device__ void solve_world(const WorldSolveArgs& A, uint32_t w, uint32_t lane, 
     }
     ws_sync<WARP>();
     const uint32_t g0 = C.g0, g1 = C.g1;
-    if (g0 == g1) {  // no rows in this world: its velocities stay as they are
+    if (g0 == g1 && !a.j.ncol) {  // no rows in this world: its velocities stay as they are
         if (lane == 0) {  // an empty record (the adjoint's reverse pass reads every world's)
             A.wcol[size_t(w) * WS_STRIDE] = g0;
             A.wcol[size_t(w) * WS_STRIDE + 1] = 0;
@@ -1045,6 +1045,16 @@ __device__ void solve_world(const WorldSolveArgs& A, uint32_t w, uint32_t lane, 
                 if (sweep >= 1 && rec.w) run_group_shared<SPLIT>(a, t, rec, sweep - 1, iters - 1, plin, pang, b0);
             }
             ws_sync<WARP>();
+        }
+        // sequential_impulse.rs:720-735: a velocity sweep's joint rows follow its contacts (the
+        // host allows joints here only for a plain world, whose bodies start at 0).
+        if (sweep >= 1 && a.j.ncol) {
+            for (uint32_t jc = 0; jc < a.j.ncol; ++jc) {
+                const uint32_t hi = a.j.coff[jc + 1];
+                for (uint32_t t = a.j.coff[jc] + lane; t < hi; t += nt)
+                    solve_joint_slot<true>(a.j, t, lin, ang, a.iw, a.damping);
+                ws_sync<WARP>();
+            }
         }
     }
     // 4. The world's velocities and push velocities back to global memory.
@@ -1311,26 +1321,31 @@ bool build_world_plan(const std::vector<uint32_t>& world_off, uint32_t block, ui
 
 void run_world_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
                       uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark,
-                      const uint32_t* world_off, uint32_t nworlds, const WorldPlan& plan, uint32_t* wcol) {
+                      const uint32_t* world_off, uint32_t nworlds, const WorldPlan& plan, uint32_t* wcol,
+                      const JointsDev* joints) {
+    const bool with_joints = joints && joints->n && joints->ncol;
     check_cuda(cudaMemsetAsync(pd.scalars.p + 2, 0, 4 * sizeof(uint32_t), s), "memset");
     check_cuda(cudaMemsetAsync(pd.scalars.p + 10, 0, 2 * sizeof(uint32_t), s), "memset");
     check_cuda(cudaMemsetAsync(pd.colour_count.p, 0, (MAX_COLOURS + 3) * sizeof(uint32_t), s), "memset");
     check_cuda(cudaMemsetAsync(pd.split_count.p, 0, (MAX_COLOURS + 3) * sizeof(uint32_t), s), "memset");
-    if (npairs == 0 || nworlds == 0) {
+    if (nworlds == 0 || (npairs == 0 && !with_joints)) {
         mark(5);
         mark(6);
         return;
     }
     const int TB = 256;
     if (npairs >= (1u << 29)) throw CudaError{cudaErrorInvalidValue, "more than 2^29 pairs for the solver's slot records"};
-    k_flag_contact_pairs<<<(npairs + TB - 1) / TB, TB, 0, s>>>(npairs, pd.row_count.p, pd.flags.p);
+    if (npairs)
+        k_flag_contact_pairs<<<(npairs + TB - 1) / TB, TB, 0, s>>>(npairs, pd.row_count.p, pd.flags.p);
     size_t bytes = 0;
     cub::CountingInputIterator<uint32_t> it(0);
-    check_cuda(cub::DeviceSelect::Flagged(nullptr, bytes, it, pd.flags.p, pd.contact_pairs.p, pd.scalars.p + 2,
-                                          int(npairs), s), "select size");
-    pd.cub_tmp.reserve(bytes);
-    check_cuda(cub::DeviceSelect::Flagged(pd.cub_tmp.p, bytes, it, pd.flags.p, pd.contact_pairs.p, pd.scalars.p + 2,
-                                          int(npairs), s), "select");
+    if (npairs) {
+        check_cuda(cub::DeviceSelect::Flagged(nullptr, bytes, it, pd.flags.p, pd.contact_pairs.p, pd.scalars.p + 2,
+                                              int(npairs), s), "select size");
+        pd.cub_tmp.reserve(bytes);
+        check_cuda(cub::DeviceSelect::Flagged(pd.cub_tmp.p, bytes, it, pd.flags.p, pd.contact_pairs.p,
+                                              pd.scalars.p + 2, int(npairs), s), "select");
+    }
     mark(5);
     const size_t slots = (size_t(npairs) + 32u * (MAX_COLOURS + 1) + 31u) & ~size_t(31);
     pd.vtab.reserve(size_t(VT_PLANES) * 4 * slots);
@@ -1340,7 +1355,7 @@ void run_world_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs
                     pd.split_offset.p, pd.split_cursor.p, pd.scalars.p, w.b.linvel, w.b.angvel, w.b.push_lin,
                     w.b.push_ang, w.b.iw, pd.vtab.p, pd.stab.p, pd.rec.sweeps,
                     pd.barrier.p, status_dev, sp.inv_dt, sp.info.restitution_velocity_threshold,
-                    sp.info.num_iterations, JointsDev{}, sp.info.damping};
+                    sp.info.num_iterations, with_joints ? *joints : JointsDev{}, sp.info.damping};
     A.contact_pairs = pd.contact_pairs.p;
     A.ngroups = pd.scalars.p + 2;
     A.pairs = pairs;

@@ -589,7 +589,7 @@ struct World {
         build_world_plan(world_off_h, wplan_block, wplan_tau, wplan, stream);
     }
 
-    bool use_world_solver() const { return wplan.valid && joints_h.empty(); }
+    bool use_world_solver() const { return wplan.valid && (joints_h.empty() || !batch); }
     const uint32_t* world_offsets_dev() const { return batch ? world_off_d.p : plain_off_d.p; }
 
     JointsDev joints_dev() {
@@ -922,7 +922,7 @@ struct World {
         last_world_solver = use_world_solver();
         if (last_world_solver)
             run_world_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); },
-                             world_offsets_dev(), nw, wplan, wcol.p);
+                             world_offsets_dev(), nw, wplan, wcol.p, batch ? nullptr : &jd);
         else
             run_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); },
                        step_count % RECOLOUR_PERIOD != 0, &jd);

@@ -271,7 +271,10 @@ def test_world_small_stack_matches_oracle(gpu):
 
 def test_world_mixed_convex_pile_matches_oracle(gpu):
     """Config 2 recipe at small scale (boxes, spheres, capsules, 24-point hulls): the world step
-    with GJK/EPA manifolds against the oracle, in windows of 10 steps from a shared state."""
+    with GJK/EPA manifolds against the oracle, the oracle taking the device state before every
+    step; state within 1e-5 relative and pairs bit-exact after every step. (Windows of several
+    steps without that copy are not comparable here: a last-ulp sin/cos difference can flip a
+    contact decision of a tumbling hull and the trajectories part.)"""
     import bgpu
     import scenes
 
@@ -280,21 +283,18 @@ def test_world_mixed_convex_pile_matches_oracle(gpu):
     o = s.build_oracle(orc)
     convex_pairs = 0
     for step in range(90):
-        if step % 10 == 0:
-            o.set_state(w.state().astype(np.float64))
+        o.set_state(w.state().astype(np.float64))
         w.step(s.dt)
         o.set_solve_order(w.solve_order())
         o.step(s.dt)
         st = w.stats()
         assert st["device_status"] == 0, st
         convex_pairs = max(convex_pairs, st["num_detect"])
-        if step % 10 == 9:
-            g = w.state()
-            r = o.state()
-            np.testing.assert_array_equal(g[:, 13], r[:, 13])
-            err = float(np.abs(g[:, :13] - r[:, :13]).max())
-            assert err <= 1e-3, f"step {step}: {err}"
-            _pairs_equal(w.pairs(), o.pairs())
+        g = w.state()
+        r = o.state()
+        np.testing.assert_array_equal(g[:, 13], r[:, 13])
+        np.testing.assert_allclose(g[:, :13], r[:, :13], rtol=1e-5, atol=1e-6, err_msg=f"step {step}")
+        _pairs_equal(w.pairs(), o.pairs())
     assert convex_pairs > 0
 
 
