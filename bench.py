@@ -212,7 +212,7 @@ def solve_traffic(contacts):
     return dram * contacts / cap_contacts, {"captured_bytes": dram, "captured_contacts": int(cap_contacts)}
 
 
-def bench_batched(bgpu, scenes, n_worlds, steps, warmup, sample_worlds=32, sample_steps=20):
+def bench_batched(bgpu, scenes, n_worlds, steps, warmup, sample_worlds=128, sample_steps=20):
     """Batched-worlds leg: body-steps/s of n_worlds independent worlds stepped as one batch,
     against the same worlds stepped one world at a time as plain worlds (a sample of the
     worlds, scaled to the whole batch by its body count)."""
