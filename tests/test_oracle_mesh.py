@@ -209,3 +209,29 @@ def test_box_falls_onto_a_heightfield_and_rests(prec):
     st = o.state()
     assert st[1, 1] == pytest.approx(0.5, abs=0.02)
     assert np.abs(st[1, 7:13]).max() < 1e-2
+
+
+def test_mesh_rain_recipe():
+    """rain_500 / dbvt_rain_2000 (tools/perf_scenes.json): lattice sizes, the kind cycling
+    (i + nz j + layer) % 3 (box, sphere, capsule), the terrain's grid and wave heights."""
+    import scenes
+
+    s = scenes.mesh_rain()
+    a = s.arrays()
+    assert s.num_bodies == 501 and s.num_dynamic == 500 and a["mass"][0] == 0.0
+    kind, params, _ = s.shapes[0]
+    assert kind == scenes.MESH
+    v, idx = params["vertices"], params["indices"]
+    assert v.shape == (400, 3) and idx.shape == (2 * 19 * 19, 3)
+    np.testing.assert_allclose(v[0], [-9.5, 0.0, -9.5])
+    np.testing.assert_allclose(v[21], [-8.5, 0.2 * np.sin(0.7) * np.cos(0.6), -8.5], rtol=1e-6)
+    assert list(idx[0]) == [0, 21, 1] and list(idx[1]) == [0, 20, 21]
+    # body 1 + (layer * 100 + j * 10 + i): kind (i + 10 j + layer) % 3 -> shape ids 1 (box), 2, 3
+    for layer, j, i in ((0, 0, 0), (0, 0, 1), (0, 1, 0), (4, 9, 9)):
+        b = 1 + layer * 100 + j * 10 + i
+        assert a["shape"][b] == 1 + (i + 10 * j + layer) % 3
+        np.testing.assert_allclose(a["pos"][b], [-6.3 + 1.4 * i, 4.0 + 2.0 * layer, -6.3 + 1.4 * j], rtol=1e-6)
+    big = scenes.mesh_rain(nx=20, nz=20, layers=5, grid=40)
+    assert big.num_dynamic == 2000
+    np.testing.assert_allclose(big.shapes[0][1]["vertices"][0], [-19.5, 0.0, -19.5])
+    np.testing.assert_allclose(big.arrays()["pos"][1], [-13.3, 4.0, -13.3], rtol=1e-6)
