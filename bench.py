@@ -66,7 +66,11 @@ def parse():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples during the timed region."""
+    """nvidia-smi clock / throttle samples during the timed region: the sampler is running
+    (its first sample seen, then dropped) before the region starts, samples every 20 ms, and
+    takes one more sample after the region ends."""
+
+    INTERVAL_MS = 20
 
     def __init__(self, index):
         self.index = index
@@ -79,10 +83,14 @@ class ClockSampler:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.INTERVAL_MS)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 5.0:
+                time.sleep(0.005)
+            self.samples.clear()
         except OSError:
             self.proc = None
         return self
@@ -95,6 +103,7 @@ class ClockSampler:
 
     def __exit__(self, *a):
         if self.proc:
+            time.sleep(1.5 * self.INTERVAL_MS / 1000.0)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -521,7 +530,7 @@ def main():
                        "pairs": st["num_pairs"], "contacts": st["num_contacts"],
                        "contact_pairs": st["num_contact_pairs"], "colours": st["num_colours"],
                        "stage_ms_per_step": [x / launches for x in st["stage_ms"]]},
-            "roofline": {"kernel": "k_solve (colour-batched PGS)", "bound": "hbm",
+            "roofline": {"kernel": "k_solve_chunks (chunked colour-batched PGS)", "bound": "hbm",
                          "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                          "traffic_source": traffic_src, "peak_kind": peak_kind,

@@ -389,6 +389,11 @@ struct PairData {
     DevBuf<uint4> batch_rec;         // contact pairs in colour order: body a, body b, pair | rows << 29, 0
     DevBuf<uint4> split_rec;         // the same for the pairs with split-active rows
     DevBuf<float4> vtab, stab;       // solver contact tables in batch-slot order (k_solver.cu)
+    // Chunked PGS (k_solver.cu): per body its chunk and the foreign chunks whose groups touch it;
+    // per (colour, chunk) the group counts / cursors and bin offsets; the chunk adjacency
+    // bit matrix and the per-chunk progress counters.
+    DevBuf<uint32_t> chunk_of, chunk_touch, chunk_hist, chunk_off, chunk_adj;
+    DevBuf<unsigned int> chunk_ctr;
     DevBuf<uint32_t> flags;          // selection flags
     DevBuf<uint32_t> sel_a, sel_b;   // cache compaction lists
     DevBuf<unsigned char> cub_tmp;
@@ -466,9 +471,13 @@ void launch_compute_iw(const BodyDev& b, uint32_t n, cudaStream_t s);
 // Colouring + PGS over the pairs with rows (counts stay on the device).
 // `mark(5)` is called after the colouring and `mark(6)` after the PGS kernel (timing hooks).
 // seed_colours: start the colouring from the colours the pairs' manifolds carry from last step.
+// morton_leaf / tree_m: the broad phase's tree leaves (bodies in Morton order), which the
+// chunked PGS cuts into its chunks (null: chunks are runs of body indices).
 void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
                 uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark, bool seed_colours,
-                const JointsDev* joints = nullptr);
+                const JointsDev* joints = nullptr, const uint32_t* morton_leaf = nullptr, uint32_t tree_m = 0);
+// Which PGS kernel the last run_solver launched: 0 none, 1 team barriers, 2 chunked.
+int last_solver_kind();
 // Batched worlds: the per-world PGS (k_solver.cu). A launch plan deals the worlds to CTAs:
 // a CTA either solves one world with all its threads (block mode: __syncthreads between
 // phases) or one world per warp (warp mode: __syncwarp between phases). Worlds are listed

@@ -992,6 +992,9 @@ void run_pair_pass(const WorldView& w, const uint64_t* pairs, uint32_t npairs, c
         const uint32_t mgrid = std::min<uint32_t>((npairs + MESH_WARPS - 1) / MESH_WARPS, 148u * 8u);
         k_narrow_mesh<<<mgrid, 32 * MESH_WARPS, 0, s>>>(w.b, w.shapes, w.hull, pairs, npairs, d, status_dev);
     }
+    // The GJK/EPA kernels keep their polytopes in local memory (12-15 KB a thread): a launch
+    // the device cannot back with local memory fails here rather than dropping detections.
+    check_cuda(cudaGetLastError(), "narrow phase launch");
     k_capture<<<grid, TB, 0, s>>>(w.b, w.shapes, pairs, npairs, sp, d);
 }
 

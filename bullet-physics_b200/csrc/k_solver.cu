@@ -10,14 +10,19 @@
 // is touched twice, so the result is bit-identical to the reference's
 // sequential solve over the same rows taken in (colour, pair) order.
 //
-// The PGS kernel is a persistent cooperative launch split into two teams of
-// blocks with their own grid barriers: the velocity team runs the warm start
-// and the velocity sweeps, the split team the split-impulse sweeps, which
-// touch only the push velocities and so run at the same time. The first
-// sweep of each team computes the per-contact terms that stay fixed during the
-// solve (tangent basis, Iw^-1 (r x d), the velocity couplings kn/kt1/kt2) once
-// and stores them in a contact table in batch-slot order, so the later sweeps
-// run only the impulse update, reading the table with coalesced loads.
+// Worlds without joints use the chunked PGS (k_solve_chunks): the bodies are cut into
+// Morton-ordered chunks, one per block of a cooperative launch, each block solves its own
+// chunk's groups colour by colour, and between two phases it waits only for the blocks whose
+// groups share a dynamic body with its own. A group's contacts are spread over lanes (one
+// contact per lane, the velocities handed from lane to lane in contact order), and the split
+// sweep s rides in the phases of velocity sweep s + 1. Worlds with joints use the team kernel
+// (k_solve): a persistent cooperative launch split into two teams of blocks with their own
+// grid barriers, the velocity team running the warm start, the velocity sweeps and the joint
+// rows, the split team the split-impulse sweeps, which touch only the push velocities and so
+// run at the same time. The warm start computes the per-contact terms that stay fixed during
+// the solve (tangent basis, Iw^-1 (r x d)) once and stores them in a contact table in
+// batch-slot order, so the later sweeps run only the impulse update, reading the table with
+// coalesced loads.
 //
 // Rows store only the contact frame (normal, lever arms), the bias terms, the
 // effective masses and the accumulated impulses; the tangent basis, the
@@ -25,6 +30,8 @@
 // from the per-body world inverse inertia with the reference's arithmetic, so
 // they equal the values the reference precomputes in prepare().
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 #include <cooperative_groups.h>
 #include <cub/cub.cuh>
 #include "bgpu_kernels.cuh"
@@ -339,7 +346,7 @@ __global__ void k_colour_hist(const uint32_t* __restrict__ count, const uint32_t
 // [10] split rows [11] largest split batch.
 __global__ void k_colour_scan(uint32_t* hist, uint32_t* offset, uint32_t* cursor, uint32_t* split_hist,
                               uint32_t* split_offset, uint32_t* split_cursor, const unsigned int* bar, uint32_t* scalars,
-                              uint32_t* remap, const uint32_t* sub_hist, uint32_t* sub_cursor) {
+                              uint32_t* remap, const uint32_t* sub_hist, uint32_t* sub_cursor, uint32_t chunked) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const uint32_t nraw = bar[5];
     uint32_t acc = 0, sacc = 0, smax = 0, split_groups = 0, d = 0;
@@ -348,7 +355,8 @@ __global__ void k_colour_scan(uint32_t* hist, uint32_t* offset, uint32_t* cursor
     // groups with 4 rows come first, then 3, 2, 1 (sub_cursor: the scatter's cursor of each
     // part), so most warps hold groups of one size: their lanes run the same number of
     // contacts and read the table's contact planes without gaps. The split batches keep
-    // their cursors; after the scatter they hold the split batch ends.
+    // their cursors; after the scatter they hold the split batch ends. (chunked: the scatter
+    // takes per-(colour, chunk) cursors, so the batch ends are written here.)
     for (uint32_t c = 0; c < nraw; ++c) {
         if (hist[c] == 0) continue;
         remap[c] = d;
@@ -363,7 +371,7 @@ __global__ void k_colour_scan(uint32_t* hist, uint32_t* offset, uint32_t* cursor
         cursor[d] = acc;  // the batch end
         sacc = (sacc + 31u) & ~31u;
         split_offset[d] = sacc;
-        split_cursor[d] = sacc;
+        split_cursor[d] = chunked ? sacc + split_hist[c] : sacc;
         sacc += split_hist[c];
         smax = max(smax, split_hist[c]);
         split_groups += split_hist[c];
@@ -391,25 +399,171 @@ __device__ __forceinline__ uint32_t claim_slot(uint32_t* cursor, uint32_t c) {
     return base + rank;
 }
 
+// ---------------------------------------------------------------- chunks (chunked PGS)
+// The chunked PGS deals each colour batch to the blocks of the launch by chunk: a chunk is a
+// run of bodies in Morton order (the broad phase's tree leaves), and a group belongs to the
+// chunk of its first dynamic body. Block b solves chunk b's groups of every colour; before
+// a phase it waits only for the blocks whose groups share a dynamic body with its own (its
+// neighbours), not for the whole grid. Two blocks share a body exactly when both appear in
+// the body's touch set, so the neighbour relation is built from the touch sets.
+constexpr uint32_t CHUNK_TOUCH = 8;          // foreign chunks recorded per body
+constexpr uint32_t CHUNK_EMPTY = 0xffffffffu;
+constexpr uint32_t CHUNK_MAX = 1024;         // blocks of a chunked launch
+constexpr uint32_t CHUNK_CTR_STRIDE = 8;     // progress counters 32 bytes apart
+
+__device__ __forceinline__ uint32_t group_owner(uint32_t ia, uint32_t ib, const float4* __restrict__ iw,
+                                                const uint32_t* __restrict__ chunk_of) {
+    return chunk_of[inv_mass_of(iw, ia) > 0.0f ? ia : ib];
+}
+
+// Bodies in Morton order cut into P equal runs (bodies outside the tree keep chunk 0); with no
+// tree, runs of body indices.
+__global__ void k_chunk_of(uint32_t n, uint32_t P, const uint32_t* __restrict__ leaf, uint32_t m, uint32_t* chunk_of) {
+    const uint32_t lim = leaf ? m : n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < lim; i += gridDim.x * blockDim.x) {
+        const uint32_t c = uint32_t(uint64_t(i) * P / lim);
+        chunk_of[leaf ? leaf[i] : i] = c;
+    }
+}
+
+// Records chunk B in the touch set of body x when B is not x's own chunk (slot values only
+// ever go from empty to a chunk id, so a stale read of a filled slot is still correct).
+__device__ __forceinline__ void chunk_touch(uint32_t* touch, uint32_t x, uint32_t B, uint32_t* all_flag) {
+    uint32_t* t = touch + size_t(x) * CHUNK_TOUCH;
+    for (uint32_t s = 0; s < CHUNK_TOUCH; ++s) {
+        uint32_t v = t[s];
+        if (v == B) return;
+        if (v == CHUNK_EMPTY) {
+            v = atomicCAS(&t[s], CHUNK_EMPTY, B);
+            if (v == CHUNK_EMPTY || v == B) return;
+        }
+    }
+    atomicOr(all_flag, 1u);  // more foreign chunks than slots: every block becomes every block's neighbour
+}
+
+// Groups per (colour, chunk, row count) and split groups per (colour, chunk), plus the
+// touch sets of the groups' dynamic bodies.
+__global__ void k_chunk_hist(const uint32_t* __restrict__ count, const uint32_t* __restrict__ contact_pairs,
+                             const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ row_count,
+                             const uint32_t* __restrict__ colour, const uint32_t* __restrict__ split_flag,
+                             const float4* __restrict__ iw, const uint32_t* __restrict__ chunk_of, uint32_t P,
+                             uint32_t* vhist, uint32_t* shist, uint32_t* touch, uint32_t* all_flag) {
+    const uint32_t K = *count;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        const uint32_t c = colour[k];
+        if (c >= MAX_COLOURS) continue;
+        const uint32_t p = contact_pairs[k];
+        const uint64_t key = pairs[p];
+        const uint32_t ia = key_lo(key), ib = key_hi(key);
+        const uint32_t B = group_owner(ia, ib, iw, chunk_of);
+        atomicAdd(&vhist[(size_t(c) * P + B) * 4 + (row_count[p] - 1)], 1u);
+        if (split_flag[k]) atomicAdd(&shist[size_t(c) * P + B], 1u);
+        if (inv_mass_of(iw, ia) > 0.0f && chunk_of[ia] != B) chunk_touch(touch, ia, B, all_flag);
+        if (inv_mass_of(iw, ib) > 0.0f && chunk_of[ib] != B) chunk_touch(touch, ib, B, all_flag);
+    }
+}
+
+// One block per raw colour: the colour's batch is laid out chunk by chunk (inside a chunk the
+// groups with 4 rows first, then 3, 2, 1), so the counts become the scatter's cursors and the
+// chunk bins [voff[d (P + 1) + b], voff[d (P + 1) + b + 1]) of dense colour d with the bin's
+// groups of 4, 3, 2 and 1 rows in vsec[(d P + b) 4 + 0..3]; the same for the split batch (one
+// part per chunk).
+template <int TB>
+__global__ void __launch_bounds__(TB) k_chunk_scan(uint32_t P, const uint32_t* __restrict__ hist,
+                                                   const uint32_t* __restrict__ remap,
+                                                   const uint32_t* __restrict__ offset,
+                                                   const uint32_t* __restrict__ split_offset,
+                                                   const unsigned int* __restrict__ bar, uint32_t* vhist,
+                                                   uint32_t* shist, uint32_t* voff, uint32_t* soff, uint32_t* vsec) {
+    using Scan = cub::BlockScan<uint32_t, TB>;
+    __shared__ typename Scan::TempStorage tmp;
+    const uint32_t c = blockIdx.x;
+    if (c >= bar[5] || hist[c] == 0) return;
+    const uint32_t d = remap[c];
+    const uint32_t per = (P + TB - 1) / TB;  // chunks per thread
+    const uint32_t b0 = min(P, threadIdx.x * per), b1 = min(P, b0 + per);
+    uint32_t* vh = vhist + size_t(c) * P * 4;
+    uint32_t* sh = shist + size_t(c) * P;
+    uint32_t vsum = 0, ssum = 0;
+    for (uint32_t b = b0; b < b1; ++b) {
+        for (uint32_t n = 0; n < 4; ++n) vsum += vh[b * 4 + n];
+        ssum += sh[b];
+    }
+    uint32_t vx, sx;
+    Scan(tmp).ExclusiveSum(vsum, vx);
+    __syncthreads();  // the scan's temporary storage is reused
+    Scan(tmp).ExclusiveSum(ssum, sx);
+    uint32_t vpos = offset[d] + vx, spos = split_offset[d] + sx;
+    for (uint32_t b = b0; b < b1; ++b) {
+        voff[size_t(d) * (P + 1) + b] = vpos;
+        for (int n = 3; n >= 0; --n) {  // 4 rows first
+            const uint32_t cnt = vh[b * 4 + n];
+            vsec[(size_t(d) * P + b) * 4 + (3 - n)] = cnt;
+            vh[b * 4 + n] = vpos;
+            vpos += cnt;
+        }
+        soff[size_t(d) * (P + 1) + b] = spos;
+        const uint32_t cnt = sh[b];
+        sh[b] = spos;
+        spos += cnt;
+    }
+    if (threadIdx.x == TB - 1) {
+        voff[size_t(d) * (P + 1) + P] = vpos;
+        soff[size_t(d) * (P + 1) + P] = spos;
+    }
+}
+
+// Neighbour bits: every two distinct chunks of a body's touch set (its own chunk included).
+__global__ void k_chunk_adjacency(uint32_t n, const uint32_t* __restrict__ chunk_of, const uint32_t* __restrict__ touch,
+                                  uint32_t W, uint32_t* adj) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t* t = touch + size_t(i) * CHUNK_TOUCH;
+        if (t[0] == CHUNK_EMPTY) continue;  // touched by its own chunk only
+        uint32_t v[CHUNK_TOUCH + 1];
+        uint32_t m = 0;
+        v[m++] = chunk_of[i];
+#pragma unroll
+        for (uint32_t s = 0; s < CHUNK_TOUCH; ++s)
+            if (t[s] != CHUNK_EMPTY) v[m++] = t[s];
+        for (uint32_t a = 0; a < m; ++a)
+            for (uint32_t b = 0; b < m; ++b) {
+                if (v[a] == v[b]) continue;
+                uint32_t* w = &adj[size_t(v[a]) * W + (v[b] >> 5)];
+                const uint32_t bit = 1u << (v[b] & 31u);
+                if (!(*w & bit)) atomicOr(w, bit);
+            }
+    }
+}
+
 // Slot record of a group: its two bodies and its pair index with the row count
-// in the top three bits.
+// in the top three bits. With chunk cursors (vcur / scur, by raw colour) the slot is taken
+// in the group's (colour, chunk, row count) part.
 __global__ void k_colour_scatter(const uint32_t* __restrict__ count, const uint32_t* __restrict__ contact_pairs,
                                  const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ row_count,
                                  const uint32_t* __restrict__ colour, const uint32_t* __restrict__ split_flag,
                                  uint32_t* sub_cursor, uint32_t* split_cursor, uint4* batch_rec, uint4* split_rec,
-                                 float4* entries, const uint32_t* __restrict__ remap) {
+                                 float4* entries, const uint32_t* __restrict__ remap,
+                                 const uint32_t* __restrict__ chunk_of, const float4* __restrict__ iw, uint32_t P,
+                                 uint32_t* vcur, uint32_t* scur) {
     uint32_t K = *count;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
         if (colour[k] >= MAX_COLOURS) continue;  // colouring gave up (its status bit is set)
-        uint32_t c = remap[colour[k]];
+        const uint32_t raw = colour[k];
+        uint32_t c = remap[raw];
         uint32_t p = contact_pairs[k];
         uint64_t key = pairs[p];
         uint4 rec = make_uint4(key_lo(key), key_hi(key), p | (row_count[p] << 29), 0u);
         // The colour rides in the manifold's meta bits to seed next step's colouring.
         float* mw = &entries[size_t(p) * ENTRY_F4 + 2].w;
         *mw = __uint_as_float((__float_as_uint(*mw) & ~(0xffu << META_COLOUR_SHIFT)) | ((c + 1u) << META_COLOUR_SHIFT));
-        batch_rec[claim_slot(sub_cursor, c * 4 + (row_count[p] - 1))] = rec;
-        if (split_flag[k]) split_rec[claim_slot(split_cursor, c)] = rec;
+        if (vcur) {
+            const uint32_t B = group_owner(rec.x, rec.y, iw, chunk_of);
+            batch_rec[claim_slot(vcur, (raw * P + B) * 4 + (row_count[p] - 1))] = rec;
+            if (split_flag[k]) split_rec[claim_slot(scur, raw * P + B)] = rec;
+        } else {
+            batch_rec[claim_slot(sub_cursor, c * 4 + (row_count[p] - 1))] = rec;
+            if (split_flag[k]) split_rec[claim_slot(split_cursor, c)] = rec;
+        }
     }
 }
 
@@ -451,9 +605,52 @@ __device__ __forceinline__ float4 f4(V3 v, float w) { return make_float4(v.x, v.
 
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
-// warm_start (sequential_impulse.rs:710-717) for group slot t, which also
-// fills the slot's velocity table with the prepared terms the sweeps use
-// (sequential_impulse.rs:352-520 computes the same values in prepare()).
+// The per-contact terms of warm_start (sequential_impulse.rs:710-717) for contact k of pair p,
+// written to the contact's velocity-table entries e (the terms sequential_impulse.rs:352-520
+// computes in prepare()); the warm-start impulses are applied by warm_apply.
+struct WarmTerms {
+    V3 n, t1, t2, ana, anb, a1a, a1b, a2a, a2b;
+    float4 r3;
+};
+
+__device__ __forceinline__ WarmTerms warm_terms(const SolveArgs& a, uint32_t p, uint32_t k, const M3& iwa,
+                                                const M3& iwb, float ima, float imb, float4* e) {
+    const float4* r = a.rows + (size_t(p) * 4 + k) * ROW_F4;
+    const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
+    WarmTerms w;
+    w.n = from4(r0);
+    const V3 ra = from4(r1), rb = from4(r2);
+    tangent_basis_dev(w.n, w.t1, w.t2);
+    w.ana = mul(iwa, cross(ra, w.n));
+    w.anb = mul(iwb, cross(rb, w.n));
+    w.a1a = mul(iwa, cross(ra, w.t1));
+    w.a1b = mul(iwb, cross(rb, w.t1));
+    w.a2a = mul(iwa, cross(ra, w.t2));
+    w.a2b = mul(iwb, cross(rb, w.t2));
+    w.r3 = r3;
+    e[VT_N * PLANE_STRIDE] = r0;
+    e[VT_RA * PLANE_STRIDE] = r1;
+    e[VT_RB * PLANE_STRIDE] = r2;
+    e[VT_T1 * PLANE_STRIDE] = f4(w.t1, ima);
+    e[VT_ANA * PLANE_STRIDE] = f4(w.ana, r4.x);
+    e[VT_ANB * PLANE_STRIDE] = f4(w.anb, r4.y);
+    e[VT_A1A * PLANE_STRIDE] = f4(w.a1a, r4.z);
+    e[VT_A1B * PLANE_STRIDE] = f4(w.a1b, r4.w);
+    e[VT_A2A * PLANE_STRIDE] = f4(w.a2a, r3.w);
+    e[VT_A2B * PLANE_STRIDE] = f4(w.a2b, imb);
+    e[VT_IMP * PLANE_STRIDE] = r3;
+    return w;
+}
+
+__device__ __forceinline__ void warm_apply(const WarmTerms& w, V3& la, V3& wa, V3& lb, V3& wb, bool appa, bool appb,
+                                           float ima, float imb) {
+    apply(la, wa, lb, wb, appa, appb, ima, imb, w.n, w.ana, w.anb, w.r3.x);
+    apply(la, wa, lb, wb, appa, appb, ima, imb, w.t1, w.a1a, w.a1b, w.r3.y);
+    apply(la, wa, lb, wb, appa, appb, ima, imb, w.t2, w.a2a, w.a2b, w.r3.z);
+}
+
+// warm_start for group slot t: every contact's terms into the slot's velocity table, its
+// warm-start impulses onto the velocities in contact order.
 __device__ __forceinline__ void warm_group(const SolveArgs& a, uint32_t t, uint32_t p, uint32_t cnt, uint32_t ia,
                                            uint32_t ib, V3& la, V3& wa, V3& lb, V3& wb, bool& appa, bool& appb) {
     float ima, imb;
@@ -462,33 +659,89 @@ __device__ __forceinline__ void warm_group(const SolveArgs& a, uint32_t t, uint3
     appa = ima > 0.0f;
     appb = imb > 0.0f;
     for (uint32_t k = 0; k < cnt; ++k) {
-        float4* e = a.vtab + tix<VT_PLANES>(0, k, t);
-        const float4* r = a.rows + (size_t(p) * 4 + k) * ROW_F4;
-        const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
-        const V3 n = from4(r0), ra = from4(r1), rb = from4(r2);
-        V3 t1, t2;
-        tangent_basis_dev(n, t1, t2);
-        const V3 ana = mul(iwa, cross(ra, n)), anb = mul(iwb, cross(rb, n));
-        const V3 a1a = mul(iwa, cross(ra, t1)), a1b = mul(iwb, cross(rb, t1));
-        const V3 a2a = mul(iwa, cross(ra, t2)), a2b = mul(iwb, cross(rb, t2));
-        apply(la, wa, lb, wb, appa, appb, ima, imb, n, ana, anb, r3.x);
-        apply(la, wa, lb, wb, appa, appb, ima, imb, t1, a1a, a1b, r3.y);
-        apply(la, wa, lb, wb, appa, appb, ima, imb, t2, a2a, a2b, r3.z);
-        e[VT_N * PLANE_STRIDE] = r0;
-        e[VT_RA * PLANE_STRIDE] = r1;
-        e[VT_RB * PLANE_STRIDE] = r2;
-        e[VT_T1 * PLANE_STRIDE] = f4(t1, ima);
-        e[VT_ANA * PLANE_STRIDE] = f4(ana, r4.x);
-        e[VT_ANB * PLANE_STRIDE] = f4(anb, r4.y);
-        e[VT_A1A * PLANE_STRIDE] = f4(a1a, r4.z);
-        e[VT_A1B * PLANE_STRIDE] = f4(a1b, r4.w);
-        e[VT_A2A * PLANE_STRIDE] = f4(a2a, r3.w);
-        e[VT_A2B * PLANE_STRIDE] = f4(a2b, imb);
-        e[VT_IMP * PLANE_STRIDE] = r3;
+        const WarmTerms w = warm_terms(a, p, k, iwa, iwb, ima, imb, a.vtab + tix<VT_PLANES>(0, k, t));
+        warm_apply(w, la, wa, lb, wb, appa, appb, ima, imb);
     }
 }
 
+// The velocity-table entries of one contact.
+struct VPlanes {
+    float4 r0, r1, r2, q3, q5, q6, q7, q8, q9, q10, r3;
+};
 
+__device__ __forceinline__ VPlanes load_vplanes(const float4* e) {
+    VPlanes v;
+    v.r0 = e[VT_N * PLANE_STRIDE];
+    v.r1 = e[VT_RA * PLANE_STRIDE];
+    v.r2 = e[VT_RB * PLANE_STRIDE];
+    v.q3 = e[VT_T1 * PLANE_STRIDE];
+    v.q5 = e[VT_ANA * PLANE_STRIDE];
+    v.q6 = e[VT_ANB * PLANE_STRIDE];
+    v.q7 = e[VT_A1A * PLANE_STRIDE];
+    v.q8 = e[VT_A1B * PLANE_STRIDE];
+    v.q9 = e[VT_A2A * PLANE_STRIDE];
+    v.q10 = e[VT_A2B * PLANE_STRIDE];
+    v.r3 = e[VT_IMP * PLANE_STRIDE];
+    return v;
+}
+
+// One solve_contact (sequential_impulse.rs:804-930) of contact k of slot t (pair p) from its
+// table entries (plane pl at src[pl * st]: the table itself or a shared-memory copy); the new
+// impulses go back to the table entry e (and, on the last sweep, to the pair's row).
+__device__ __forceinline__ void iter_contact(const SolveArgs& a, const float4* src, uint32_t st, float ima, float imb,
+                                             bool appa, bool appb, V3& la, V3& wa, V3& lb, V3& wb, float4* e,
+                                             uint32_t sweep, uint32_t k, uint32_t t, bool last, uint32_t p) {
+    const float ims = ima + imb;
+    const float4 r0 = src[VT_N * st], r1 = src[VT_RA * st], r2 = src[VT_RB * st], q3 = src[VT_T1 * st],
+                 q5 = src[VT_ANA * st], q6 = src[VT_ANB * st], q7 = src[VT_A1A * st], q8 = src[VT_A1B * st],
+                 q9 = src[VT_A2A * st], q10 = src[VT_A2B * st], r3 = src[VT_IMP * st];
+    const V3 n = from4(r0), ra = from4(r1), rb = from4(r2), t1 = from4(q3);
+    const V3 t2 = cross(n, t1);  // tangent_basis (sequential_impulse.rs:620-629), as warm_terms made it
+    const V3 ana = from4(q5), anb = from4(q6), a1a = from4(q7), a1b = from4(q8), a2a = from4(q9), a2b = from4(q10);
+    // The velocity couplings of sequential_impulse.rs:352-520, in warm_terms's operand order.
+    const V3 kn = n * ims + cross(anb, rb) + cross(ana, ra);
+    const V3 kt1 = t1 * ims + cross(a1b, rb) + cross(a1a, ra);
+    const V3 kt2 = t2 * ims + cross(a2b, rb) + cross(a2a, ra);
+    const float4 r4 = make_float4(q5.w, q6.w, q7.w, q8.w);
+    V3 va = la + cross(wa, ra);
+    V3 vb = lb + cross(wb, rb);
+    V3 rel = vb - va;
+    float vn = dot(rel, n);
+    float bias = 0.0f;
+    if (vn < -a.restitution_threshold) bias = -q9.w * vn;
+    if (r1.w != 0.0f) bias += r1.w;
+    if (r2.w != 0.0f) bias += r2.w;
+    float lambda = r4.w != 0.0f ? r4.x * (bias - vn) - r4.w * r3.x : r4.x * (bias - vn);
+    float old = r3.x;
+    float nimp = fmaxf(old + lambda, 0.0f);
+    float jn = nimp - old;
+    apply(la, wa, lb, wb, appa, appb, ima, imb, n, ana, anb, jn);
+    rel += kn * jn;
+    float maxf = r0.w * nimp;
+    float vt = dot(rel, t1);
+    float lam = -r4.y * (vt - 0.0f * a.inv_dt);
+    float o1 = r3.y;
+    const float u1 = o1 + lam;
+    float n1 = fminf(fmaxf(u1, -maxf), maxf);
+    float j1 = n1 - o1;
+    apply(la, wa, lb, wb, appa, appb, ima, imb, t1, a1a, a1b, j1);
+    rel += kt1 * j1;
+    vt = dot(rel, t2);
+    lam = -r4.z * (vt - 0.0f * a.inv_dt);
+    float o2 = r3.z;
+    const float u2 = o2 + lam;
+    float n2 = fminf(fmaxf(u2, -maxf), maxf);
+    float j2 = n2 - o2;
+    apply(la, wa, lb, wb, appa, appb, ima, imb, t2, a2a, a2b, j2);
+    const float4 nr3 = make_float4(nimp, n1, n2, r3.w);
+    if (a.srec) {  // the forward values the adjoint's frozen linearisation needs
+        const uint32_t s1 = u1 > maxf ? 1u : (u1 < -maxf ? 2u : 0u);
+        const uint32_t s2 = u2 > maxf ? 1u : (u2 < -maxf ? 2u : 0u);
+        a.srec[sweep_index(sweep, k, t, a.iterations)] = make_float4(vn, nimp, __uint_as_float(s1 | (s2 << 2)), 0.0f);
+    }
+    e[VT_IMP * PLANE_STRIDE] = nr3;
+    if (last) a.rows[(size_t(p) * 4 + k) * ROW_F4 + 3] = nr3;
+}
 
 // One solve_contact sweep (sequential_impulse.rs:804-930) over group slot t;
 // on the last sweep the impulses also go back to the pair's rows.
@@ -496,63 +749,11 @@ __device__ __forceinline__ void iter_group(const SolveArgs& a, uint32_t t, uint3
                                            bool last, V3& la, V3& wa, V3& lb, V3& wb, bool& appa, bool& appb) {
     const float4* e0 = a.vtab + tix<VT_PLANES>(0, 0, t);
     const float ima = e0[VT_T1 * PLANE_STRIDE].w, imb = e0[VT_A2B * PLANE_STRIDE].w;
-    const float ims = ima + imb;
     appa = ima > 0.0f;
     appb = imb > 0.0f;
     for (uint32_t k = 0; k < cnt; ++k) {
         float4* e = a.vtab + tix<VT_PLANES>(0, k, t);
-        const float4 r0 = e[VT_N * PLANE_STRIDE], r1 = e[VT_RA * PLANE_STRIDE], r2 = e[VT_RB * PLANE_STRIDE];
-        const float4 q3 = e[VT_T1 * PLANE_STRIDE];
-        const float4 q5 = e[VT_ANA * PLANE_STRIDE], q6 = e[VT_ANB * PLANE_STRIDE];
-        const float4 q7 = e[VT_A1A * PLANE_STRIDE], q8 = e[VT_A1B * PLANE_STRIDE];
-        const float4 q9 = e[VT_A2A * PLANE_STRIDE], q10 = e[VT_A2B * PLANE_STRIDE];
-        const float4 r3 = e[VT_IMP * PLANE_STRIDE];
-        const V3 n = from4(r0), ra = from4(r1), rb = from4(r2), t1 = from4(q3);
-        const V3 t2 = cross(n, t1);  // tangent_basis (sequential_impulse.rs:620-629), as warm_group made it
-        const V3 ana = from4(q5), anb = from4(q6), a1a = from4(q7), a1b = from4(q8), a2a = from4(q9), a2b = from4(q10);
-        // The velocity couplings of sequential_impulse.rs:352-520, in warm_group's operand order.
-        const V3 kn = n * ims + cross(anb, rb) + cross(ana, ra);
-        const V3 kt1 = t1 * ims + cross(a1b, rb) + cross(a1a, ra);
-        const V3 kt2 = t2 * ims + cross(a2b, rb) + cross(a2a, ra);
-        const float4 r4 = make_float4(q5.w, q6.w, q7.w, q8.w);
-        V3 va = la + cross(wa, ra);
-        V3 vb = lb + cross(wb, rb);
-        V3 rel = vb - va;
-        float vn = dot(rel, n);
-        float bias = 0.0f;
-        if (vn < -a.restitution_threshold) bias = -q9.w * vn;
-        if (r1.w != 0.0f) bias += r1.w;
-        if (r2.w != 0.0f) bias += r2.w;
-        float lambda = r4.w != 0.0f ? r4.x * (bias - vn) - r4.w * r3.x : r4.x * (bias - vn);
-        float old = r3.x;
-        float nimp = fmaxf(old + lambda, 0.0f);
-        float jn = nimp - old;
-        apply(la, wa, lb, wb, appa, appb, ima, imb, n, ana, anb, jn);
-        rel += kn * jn;
-        float maxf = r0.w * nimp;
-        float vt = dot(rel, t1);
-        float lam = -r4.y * (vt - 0.0f * a.inv_dt);
-        float o1 = r3.y;
-        const float u1 = o1 + lam;
-        float n1 = fminf(fmaxf(u1, -maxf), maxf);
-        float j1 = n1 - o1;
-        apply(la, wa, lb, wb, appa, appb, ima, imb, t1, a1a, a1b, j1);
-        rel += kt1 * j1;
-        vt = dot(rel, t2);
-        lam = -r4.z * (vt - 0.0f * a.inv_dt);
-        float o2 = r3.z;
-        const float u2 = o2 + lam;
-        float n2 = fminf(fmaxf(u2, -maxf), maxf);
-        float j2 = n2 - o2;
-        apply(la, wa, lb, wb, appa, appb, ima, imb, t2, a2a, a2b, j2);
-        const float4 nr3 = make_float4(nimp, n1, n2, r3.w);
-        if (a.srec) {  // the forward values the adjoint's frozen linearisation needs
-            const uint32_t s1 = u1 > maxf ? 1u : (u1 < -maxf ? 2u : 0u);
-            const uint32_t s2 = u2 > maxf ? 1u : (u2 < -maxf ? 2u : 0u);
-            a.srec[sweep_index(sweep, k, t, a.iterations)] = make_float4(vn, nimp, __uint_as_float(s1 | (s2 << 2)), 0.0f);
-        }
-        e[VT_IMP * PLANE_STRIDE] = nr3;
-        if (last) a.rows[(size_t(p) * 4 + k) * ROW_F4 + 3] = nr3;
+        iter_contact(a, e, PLANE_STRIDE, ima, imb, appa, appb, la, wa, lb, wb, e, sweep, k, t, last, p);
     }
 }
 
@@ -665,6 +866,83 @@ __device__ __forceinline__ void run_item(const SolveArgs& a, uint32_t sweep, uin
     if (!VELOCITY) run_group<SPLIT>(a, t, rec, sweep, last);
     else if (sweep == 0) run_group<WARM>(a, t, rec, sweep, last);
     else run_group<ITER>(a, t, rec, sweep, last);
+}
+
+__device__ __forceinline__ void shfl_v3(V3& v, int src) {
+    v.x = __shfl_sync(0xffffffffu, v.x, src);
+    v.y = __shfl_sync(0xffffffffu, v.y, src);
+    v.z = __shfl_sync(0xffffffffu, v.z, src);
+}
+
+// One group spread over a segment of lanes: lane k holds contact k of slot t (k < cnt; a
+// segment of 4 lanes holding a 3-contact group keeps its last lane idle). Every lane loads
+// its own contact's table entries (or, on the warm start, computes its contact's terms
+// from the rows) at once, in lane_prepare, which reads nothing another block writes during
+// the solve; lane_exec then loads the two bodies' velocities and solves the contacts in
+// order k = 0, 1, ..., the lane of contact k updating the velocities and handing them to
+// the segment by shuffles, so each contact sees exactly the velocities of the sequential
+// solve. All 32 lanes of the warp call lane_exec together (lanes without a group have
+// cnt = 0); seg0 is the lane of the segment's contact 0.
+template <bool WARM>
+struct LaneState {  // sweeps >= 1: the contact's table entries are in shared memory
+    uint4 rec;
+    float ima, imb;
+};
+template <>
+struct LaneState<true> {
+    uint4 rec;
+    float ima, imb;
+    WarmTerms W;  // the warm start
+};
+
+// Warm start: the slot record and the contact's terms (from the rows and the bodies' inverse
+// inertia), written to the velocity table.
+__device__ __forceinline__ void lane_prepare_warm(const SolveArgs& a, uint32_t t, uint32_t cnt, uint32_t k,
+                                                  LaneState<true>& S) {
+    S.rec = cnt ? __ldg(&a.batch_rec[t]) : make_uint4(0u, 0u, 0u, 0u);
+    S.ima = S.imb = 0.0f;
+    if (k >= cnt) return;
+    const M3 iwa = load_iw(a.iw, S.rec.x, S.ima);
+    const M3 iwb = load_iw(a.iw, S.rec.y, S.imb);
+    S.W = warm_terms(a, S.rec.z & 0x1fffffffu, k, iwa, iwb, S.ima, S.imb, a.vtab + tix<VT_PLANES>(0, k, t));
+}
+
+template <bool WARM>
+__device__ __forceinline__ void lane_exec(const SolveArgs& a, uint32_t t, uint32_t cnt, uint32_t k, uint32_t seg0,
+                                          uint32_t sweep, uint32_t last, const LaneState<WARM>& S, const float4* sp) {
+    const uint32_t jmax = __reduce_max_sync(0xffffffffu, cnt);
+    if (jmax == 0) return;
+    const uint32_t ia = S.rec.x, ib = S.rec.y, p = S.rec.z & 0x1fffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
+    V3 la{0.0f, 0.0f, 0.0f}, wa = la, lb = la, wb = la;
+    if (cnt) {
+        la = from4(__ldcg(&a.linvel[ia]));
+        wa = from4(__ldcg(&a.angvel[ia]));
+        lb = from4(__ldcg(&a.linvel[ib]));
+        wb = from4(__ldcg(&a.angvel[ib]));
+    }
+    const bool mine = k < cnt;
+    // Every lane of a segment holds the group's inverse masses except an idle fourth lane,
+    // which only forwards velocities; the store below is lane 0's.
+    const bool appa = S.ima > 0.0f, appb = S.imb > 0.0f;
+    float4* e = a.vtab + tix<VT_PLANES>(0, mine ? k : 0u, t);
+    for (uint32_t j = 0; j < jmax; ++j) {
+        if (mine && k == j) {
+            if constexpr (WARM) warm_apply(S.W, la, wa, lb, wb, appa, appb, S.ima, S.imb);
+            else iter_contact(a, sp, blockDim.x, S.ima, S.imb, appa, appb, la, wa, lb, wb, e, sweep, k, t, sweep == last, p);
+        }
+        if (jmax > 1) {  // else every segment is one lane
+            const int src = int(j < cnt ? seg0 + j : lane);
+            shfl_v3(la, src);
+            shfl_v3(wa, src);
+            shfl_v3(lb, src);
+            shfl_v3(wb, src);
+        }
+    }
+    if (cnt && k == 0) {
+        if (appa) { __stcg(&a.linvel[ia], to4(la, 0.0f)); __stcg(&a.angvel[ia], to4(wa, 0.0f)); }
+        if (appb) { __stcg(&a.linvel[ib], to4(lb, 0.0f)); __stcg(&a.angvel[ib], to4(wb, 0.0f)); }
+    }
 }
 
 // Phases 0 .. nphases-1 of a team: phase q is colour q % ncol of sweep q / ncol.
@@ -809,6 +1087,194 @@ __global__ void __launch_bounds__(256, 2) k_solve(SolveArgs a) {
         run_phases<false>(a, a.split_rec, s_split_off, s_split_end, ncol, iters * ncol, iters - 1u, tid, stride, a.bar, team_blocks,
                           team_block, nbar);
     }
+}
+
+// ---------------------------------------------------------------- chunked PGS
+struct ChunkArgs {
+    uint32_t P;                        // blocks of the launch = chunks
+    uint32_t W;                        // words per adjacency row
+    const uint32_t* voff;              // [d (P + 1) + b]: chunk b's part of colour batch d
+    const uint32_t* soff;              // the same for the split batches
+    const uint32_t* vsec;              // [(d P + b) 4 + i]: groups of 4 - i rows in chunk b's part of batch d
+    const uint32_t* adj;               // [b W + w]: neighbour bits of chunk b
+    const uint32_t* all_flag;          // nonzero: every chunk is every chunk's neighbour
+    unsigned int* ctr;                 // [b CHUNK_CTR_STRIDE]: phases chunk b has finished
+};
+
+// Publishes that this block finished every phase before q. The block's global writes are
+// ordered before the release store by the bar.sync.
+__device__ __forceinline__ void chunk_arrive(const ChunkArgs& ch, uint32_t q) {
+    __syncthreads();
+    if (threadIdx.x == 0)
+        asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(ch.ctr + blockIdx.x * CHUNK_CTR_STRIDE), "r"(q)
+                     : "memory");
+}
+
+// Waits until each neighbour has finished every phase before q: one warp polls the
+// neighbours' counters (acquire loads), and the closing bar.sync makes their writes visible
+// to the block. The wait is bounded like team_barrier's.
+__device__ __forceinline__ void chunk_poll(const ChunkArgs& ch, const uint16_t* nb, uint32_t nnb, uint32_t q,
+                                           uint32_t* status) {
+    if (threadIdx.x < 32u) {
+        uint32_t spins = 0;
+        unsigned long long t0 = 0;
+        bool gave_up = false;
+        for (uint32_t k = threadIdx.x; k < nnb && !gave_up; k += 32u) {
+            const unsigned int* c = ch.ctr + uint32_t(nb[k]) * CHUNK_CTR_STRIDE;
+            for (;;) {
+                unsigned int v;
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(c) : "memory");
+                if (v >= q) break;
+                if ((++spins & 63u) == 0u) {
+                    const unsigned long long now = globaltimer_ns();
+                    if (t0 == 0) t0 = now;
+                    if ((*(volatile uint32_t*)status & ST_BARRIER_TIMEOUT) || now - t0 > BARRIER_TIMEOUT_NS ||
+                        spins > BARRIER_SPIN_LIMIT) {
+                        atomicOr(status, ST_BARRIER_TIMEOUT);
+                        gave_up = true;
+                        break;
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned int d = static_cast<unsigned int>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
+}
+
+// One phase of a chunked block: velocity items are lanes (groups of 4 and 3 rows take 4 lanes,
+// of 2 rows 2, of 1 row one: parts L4, L3, L2, L), padded to a whole warp; split items (one
+// group per thread) follow from LV. Between publishing its progress and polling its
+// neighbours the block starts round 0's loads (item threadIdx.x), which read nothing another
+// block writes during the solve: its slot record and its contact's table entries (copied
+// into shared memory, s_pl[plane][thread]) or its warm-start terms, or its split group's
+// table entries (into L2). The loads come after the publishing bar.sync, which orders this
+// thread's earlier table writes before them. The item-to-thread deal depends only on the
+// bin's counts, so a contact's table entries are read by the thread that wrote them.
+template <bool WARM>
+__device__ __forceinline__ void chunk_phase(const SolveArgs& a, const ChunkArgs& ch, const uint16_t* nb, uint32_t nnb,
+                                            uint32_t q, uint32_t sw, uint32_t iters, uint32_t v0, uint32_t nv,
+                                            uint32_t n4, uint32_t n3, uint32_t n2, uint32_t s0, uint32_t ns,
+                                            float4* s_pl) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t L4 = 4u * n4, L3 = L4 + 4u * n3, L2 = L3 + 2u * n2, L = L2 + (nv - n4 - n3 - n2);
+    const uint32_t LV = (L + 31u) & ~31u;
+    auto lane_item = [&](uint32_t i, uint32_t& g, uint32_t& k, uint32_t& cnt, uint32_t& seg0) {
+        g = 0; k = 0; cnt = 0; seg0 = lane;
+        if (i < L4) { g = i >> 2; k = i & 3u; cnt = 4; seg0 = lane & ~3u; }
+        else if (i < L3) { g = n4 + ((i - L4) >> 2); k = i & 3u; cnt = 3; seg0 = lane & ~3u; }
+        else if (i < L2) { g = n4 + n3 + ((i - L3) >> 1); k = i & 1u; cnt = 2; seg0 = lane & ~1u; }
+        else if (i < L) { g = n4 + n3 + n2 + (i - L2); cnt = 1; }
+    };
+    const uint32_t first = threadIdx.x & ~31u;
+    // Round r's table entries of this thread's contact go to s_pl by cp.async.
+    auto stage = [&](uint32_t g, uint32_t k, uint32_t cnt) {
+        if (k < cnt) {
+            const float4* e = a.vtab + tix<VT_PLANES>(0, k, v0 + g);
+            for (uint32_t pl = 0; pl < VT_PLANES; ++pl)
+                cp_async16(&s_pl[pl * blockDim.x + threadIdx.x], e + pl * PLANE_STRIDE);
+        }
+    };
+    if (q) chunk_arrive(ch, q);
+    uint4 rec0 = make_uint4(0u, 0u, 0u, 0u);
+    LaneState<WARM> S0;
+    if (WARM && first < LV) {
+        uint32_t g, k, cnt, seg0;
+        lane_item(threadIdx.x, g, k, cnt, seg0);
+        if constexpr (WARM) lane_prepare_warm(a, v0 + g, cnt, k, S0);
+    } else if (!WARM && first < LV) {
+        uint32_t g, k, cnt, seg0;
+        lane_item(threadIdx.x, g, k, cnt, seg0);
+        stage(g, k, cnt);
+        if (cnt) rec0 = __ldg(&a.batch_rec[v0 + g]);
+    } else if (threadIdx.x >= LV && threadIdx.x - LV < ns && sw >= 2) {
+        prefetch_slot_l2<false>(a, s0 + threadIdx.x - LV, __ldg(&a.split_rec[s0 + threadIdx.x - LV]).z >> 29);
+    }
+    if (q) chunk_poll(ch, nb, nnb, q, a.status);
+    for (uint32_t base = first; base < LV + ns; base += blockDim.x) {
+        const uint32_t i = base + lane;
+        if (base < LV) {  // warp-uniform: the whole warp runs velocity lanes
+            uint32_t g, k, cnt, seg0;
+            lane_item(i, g, k, cnt, seg0);
+            LaneState<WARM> S;
+            const float4* sp = s_pl + threadIdx.x;
+            if constexpr (WARM) {
+                if (base != first) lane_prepare_warm(a, v0 + g, cnt, k, S);
+                else S = S0;
+            } else {
+                if (base != first) {
+                    stage(g, k, cnt);
+                    S.rec = cnt ? __ldg(&a.batch_rec[v0 + g]) : make_uint4(0u, 0u, 0u, 0u);
+                } else {
+                    S.rec = rec0;
+                }
+                asm volatile("cp.async.wait_all;" ::: "memory");
+                S.ima = k < cnt ? sp[VT_T1 * blockDim.x].w : 0.0f;
+                S.imb = k < cnt ? sp[VT_A2B * blockDim.x].w : 0.0f;
+            }
+            lane_exec<WARM>(a, v0 + g, cnt, k, seg0, sw, iters, S, sp);
+        } else if (i - LV < ns) {
+            run_item<false>(a, sw - 1u, iters - 1u, s0 + i - LV, __ldg(&a.split_rec[s0 + i - LV]));
+        }
+    }
+}
+
+// solve() (sequential_impulse.rs:692-705) for worlds without joints, one chunk per block:
+// phase (s, c) runs velocity sweep s (s = 0: warm start) over the block's groups of colour c
+// and split sweep s - 1 over its split groups of colour c (split sweeps touch only the push
+// velocities, so they share the phase). Each block runs its phases in the team kernel's order
+// and waits only on its neighbours, so every body sees the same sequence of updates as under
+// grid barriers: the result is the sequential solve in (colour, pair) order. A block skips
+// the phases it has no groups in. The warm start (phases 0 .. ncol - 1, WARM) and the sweeps
+// (the rest) are two launches of their own code (each keeps its registers); the counters run
+// on across the two, so the second launch starts with every neighbour past the warm start.
+template <bool WARM>
+__global__ void __launch_bounds__(256, 2) k_solve_chunks(SolveArgs a, ChunkArgs ch) {
+    const uint32_t ncol = a.scalars[4];
+    const uint32_t iters = a.iterations;
+    const uint32_t b = blockIdx.x;
+    extern __shared__ float4 s_pl[];  // [VT_PLANES][blockDim.x]: round 0's table entries
+    __shared__ uint32_t s_v[MAX_COLOURS][2], s_s[MAX_COLOURS][2], s_sec[MAX_COLOURS][3];
+    __shared__ uint16_t s_nb[CHUNK_MAX];
+    __shared__ unsigned int s_nnb;
+    if (threadIdx.x == 0) s_nnb = 0;
+    for (uint32_t c = threadIdx.x; c < ncol; c += blockDim.x) {
+        s_v[c][0] = ch.voff[size_t(c) * (ch.P + 1) + b];
+        s_v[c][1] = ch.voff[size_t(c) * (ch.P + 1) + b + 1];
+        s_s[c][0] = ch.soff[size_t(c) * (ch.P + 1) + b];
+        s_s[c][1] = ch.soff[size_t(c) * (ch.P + 1) + b + 1];
+        for (uint32_t i = 0; i < 3; ++i) s_sec[c][i] = ch.vsec[(size_t(c) * ch.P + b) * 4 + i];
+    }
+    __syncthreads();  // s_nnb
+    const bool all = *ch.all_flag != 0u;
+    for (uint32_t w = threadIdx.x; w < ch.W; w += blockDim.x) {
+        uint32_t bits = all ? 0xffffffffu : ch.adj[size_t(b) * ch.W + w];
+        while (bits) {
+            const uint32_t j = w * 32u + uint32_t(__ffs(int(bits)) - 1);
+            bits &= bits - 1u;
+            if (j < ch.P && j != b) s_nb[atomicAdd(&s_nnb, 1u)] = uint16_t(j);
+        }
+    }
+    __syncthreads();  // the neighbour list
+    const uint32_t nnb = s_nnb;
+    const uint32_t nphases = WARM ? ncol : (iters + 1) * ncol;
+    for (uint32_t q = WARM ? 0u : ncol; q < nphases; ++q) {
+        const uint32_t c = q % ncol, sw = q / ncol;
+        const uint32_t v0 = s_v[c][0], nv = s_v[c][1] - v0;
+        const uint32_t s0 = s_s[c][0], ns = sw >= 1 ? s_s[c][1] - s0 : 0u;
+        if (nv + ns == 0) continue;
+        const uint32_t n4 = s_sec[c][0], n3 = s_sec[c][1], n2 = s_sec[c][2];
+        chunk_phase<WARM>(a, ch, s_nb, nnb, q, sw, iters, v0, nv, n4, n3, n2, s0, ns, s_pl);
+    }
+    // Every later phase of this block is empty: publish the end.
+    __syncthreads();
+    if (threadIdx.x == 0)
+        asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(ch.ctr + b * CHUNK_CTR_STRIDE), "r"(nphases)
+                     : "memory");
 }
 
 // ---------------------------------------------------------------- per-world PGS (batched worlds)
@@ -1205,22 +1671,61 @@ static void launch_solve(const WorldView& w, PairData& pd, const StepParams& sp,
     check_cuda(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(TB), sargs, 0, s), "solve launch");
 }
 
+// The PGS kernel for worlds without joints is the chunked one; BGPU_PGS=team in the
+// environment keeps the team-barrier kernel (which worlds with joints always use), for
+// comparison.
+static int pgs_mode() {
+    static int mode = -1;
+    if (mode < 0) {
+        const char* e = std::getenv("BGPU_PGS");
+        mode = (e && std::strcmp(e, "team") == 0) ? 1 : 2;
+    }
+    return mode;
+}
+
+static int g_last_solver_kind = 0;
+int last_solver_kind() { return g_last_solver_kind; }
+
+constexpr size_t CHUNK_SMEM = size_t(VT_PLANES) * 256 * sizeof(float4);
+
+static int chunk_grid() {
+    static int grid = 0;
+    if (!grid) {
+        int g[2];
+        const void* fns[2] = {(const void*)k_solve_chunks<true>, (const void*)k_solve_chunks<false>};
+        for (int i = 0; i < 2; ++i) {
+            check_cuda(cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize, int(CHUNK_SMEM)),
+                       "smem attribute");
+            g[i] = coop_grid(fns[i], 256, CHUNK_SMEM);
+        }
+        grid = std::min(g[0], g[1]);  // both launches cut the bodies into the same chunks
+    }
+    if (grid > int(CHUNK_MAX)) throw CudaError{cudaErrorInvalidValue, "chunked PGS: more blocks than chunk slots"};
+    return grid;
+}
+
 void run_wait_selftest(unsigned long long limit_ns, unsigned int* ctr, uint32_t* status, cudaStream_t s) {
     k_wait_selftest<<<2, 32, 0, s>>>(ctr, status, limit_ns);
 }
 
 void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
                 uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark, bool seed_colours,
-                const JointsDev* joints) {
+                const JointsDev* joints, const uint32_t* morton_leaf, uint32_t tree_m) {
     const bool with_joints = joints && joints->n && joints->ncol;
+    g_last_solver_kind = 0;
     if (npairs == 0) {
         check_cuda(cudaMemsetAsync(pd.scalars.p + 2, 0, 4 * sizeof(uint32_t), s), "memset");
         check_cuda(cudaMemsetAsync(pd.scalars.p + 10, 0, 2 * sizeof(uint32_t), s), "memset");
         mark(5);
-        if (with_joints) launch_solve(w, pd, sp, status_dev, s, joints);
+        if (with_joints) {
+            launch_solve(w, pd, sp, status_dev, s, joints);
+            g_last_solver_kind = 1;
+        }
         mark(6);
         return;
     }
+    const int mode = with_joints ? 1 : pgs_mode();
+    const bool chunked = mode == 2;
     const int TB = 256;
     if (npairs >= (1u << 29)) throw CudaError{cudaErrorInvalidValue, "more than 2^29 pairs for the solver's slot records"};
     // Contact pairs (ascending pair order).
@@ -1253,18 +1758,75 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
     uint32_t g = std::min<uint32_t>((npairs + TB - 1) / TB, 148u * 8u);
     k_colour_hist<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pd.colour.p, pd.row_count.p, pd.rows.p,
                                    pd.colour_count.p, pd.split_count.p, pd.flags.p, sub_hist);
+    // Chunks: each body's chunk, the (colour, chunk) counts and the touch sets.
+    uint32_t P = 0, W = 0;
+    uint32_t *vhist = nullptr, *shist = nullptr, *all_flag = nullptr;
+    if (chunked) {
+        P = uint32_t(chunk_grid());
+        W = (P + 31u) / 32u;
+        const uint32_t n = w.nbodies;
+        pd.chunk_of.reserve(std::max<uint32_t>(n, 1));
+        pd.chunk_touch.reserve(size_t(std::max<uint32_t>(n, 1)) * CHUNK_TOUCH);
+        pd.chunk_hist.reserve(size_t(MAX_COLOURS) * P * 5);
+        pd.chunk_off.reserve(2 * size_t(MAX_COLOURS) * (P + 1) + size_t(MAX_COLOURS) * P * 4);
+        pd.chunk_adj.reserve(size_t(P) * W + 1);
+        pd.chunk_ctr.reserve(size_t(P) * CHUNK_CTR_STRIDE);
+        vhist = pd.chunk_hist.p;
+        shist = pd.chunk_hist.p + size_t(MAX_COLOURS) * P * 4;
+        all_flag = pd.chunk_adj.p + size_t(P) * W;
+        check_cuda(cudaMemsetAsync(pd.chunk_hist.p, 0, size_t(MAX_COLOURS) * P * 5 * sizeof(uint32_t), s), "memset");
+        check_cuda(cudaMemsetAsync(pd.chunk_touch.p, 0xff, size_t(n) * CHUNK_TOUCH * sizeof(uint32_t), s), "memset");
+        check_cuda(cudaMemsetAsync(pd.chunk_adj.p, 0, (size_t(P) * W + 1) * sizeof(uint32_t), s), "memset");
+        check_cuda(cudaMemsetAsync(pd.chunk_of.p, 0, size_t(n) * sizeof(uint32_t), s), "memset");
+        const uint32_t lim = (morton_leaf && tree_m) ? tree_m : n;
+        k_chunk_of<<<std::min<uint32_t>((lim + TB - 1) / TB, 148u * 8u), TB, 0, s>>>(
+            n, P, (morton_leaf && tree_m) ? morton_leaf : nullptr, tree_m, pd.chunk_of.p);
+        k_chunk_hist<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pairs, pd.row_count.p, pd.colour.p,
+                                      pd.flags.p, w.b.iw, pd.chunk_of.p, P, vhist, shist, pd.chunk_touch.p, all_flag);
+    }
     k_colour_scan<<<1, 32, 0, s>>>(pd.colour_count.p, pd.colour_offset.p, pd.colour_cursor.p, pd.split_count.p,
                                    pd.split_offset.p, pd.split_cursor.p, pd.barrier.p, pd.scalars.p, pd.colour_remap.p,
-                                   sub_hist, sub_cursor);
+                                   sub_hist, sub_cursor, chunked ? 1u : 0u);
+    uint32_t *voff = nullptr, *soff = nullptr, *vsec = nullptr;
+    if (chunked) {
+        voff = pd.chunk_off.p;
+        soff = pd.chunk_off.p + size_t(MAX_COLOURS) * (P + 1);
+        vsec = pd.chunk_off.p + 2 * size_t(MAX_COLOURS) * (P + 1);
+        k_chunk_scan<256><<<MAX_COLOURS, 256, 0, s>>>(P, pd.colour_count.p, pd.colour_remap.p, pd.colour_offset.p,
+                                                      pd.split_offset.p, pd.barrier.p, vhist, shist, voff, soff, vsec);
+    }
     k_colour_scatter<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pairs, pd.row_count.p, pd.colour.p,
                                       pd.flags.p, sub_cursor, pd.split_cursor.p, pd.batch_rec.p,
-                                      pd.split_rec.p, pd.entries.p, pd.colour_remap.p);
+                                      pd.split_rec.p, pd.entries.p, pd.colour_remap.p, pd.chunk_of.p, w.b.iw, P,
+                                      vhist, shist);
+    if (chunked)
+        k_chunk_adjacency<<<std::min<uint32_t>((w.nbodies + TB - 1) / TB, 148u * 8u), TB, 0, s>>>(
+            w.nbodies, pd.chunk_of.p, pd.chunk_touch.p, W, pd.chunk_adj.p);
     mark(5);
     // Slot capacity: every group plus the 32-alignment padding of each batch.
     const size_t slots = (size_t(npairs) + 32u * (MAX_COLOURS + 1) + 31u) & ~size_t(31);
     pd.vtab.reserve(size_t(VT_PLANES) * 4 * slots);
     pd.stab.reserve(size_t(ST_PLANES) * 4 * slots);
-    launch_solve(w, pd, sp, status_dev, s, with_joints ? joints : nullptr);
+    if (chunked) {
+        check_cuda(cudaMemsetAsync(pd.chunk_ctr.p, 0, size_t(P) * CHUNK_CTR_STRIDE * sizeof(unsigned int), s),
+                   "memset");
+        SolveArgs sa{pd.rows.p, pd.batch_rec.p, pd.colour_offset.p, pd.colour_cursor.p, pd.split_rec.p,
+                     pd.split_offset.p, pd.split_cursor.p, pd.scalars.p, w.b.linvel, w.b.angvel, w.b.push_lin,
+                     w.b.push_ang, w.b.iw, pd.vtab.p, pd.stab.p, pd.rec.sweeps,
+                     pd.barrier.p, status_dev, sp.inv_dt, sp.info.restitution_velocity_threshold,
+                     sp.info.num_iterations, JointsDev{}, sp.info.damping};
+        ChunkArgs ch{P, W, voff, soff, vsec, pd.chunk_adj.p, all_flag, pd.chunk_ctr.p};
+        void* args[] = {&sa, &ch};
+        check_cuda(cudaLaunchCooperativeKernel((const void*)k_solve_chunks<true>, dim3(P), dim3(256), args,
+                                               CHUNK_SMEM, s), "chunked warm-start launch");
+        if (sp.info.num_iterations)
+            check_cuda(cudaLaunchCooperativeKernel((const void*)k_solve_chunks<false>, dim3(P), dim3(256), args,
+                                                   CHUNK_SMEM, s), "chunked solve launch");
+        g_last_solver_kind = 2;
+    } else {
+        launch_solve(w, pd, sp, status_dev, s, with_joints ? joints : nullptr);
+        g_last_solver_kind = 1;
+    }
     mark(6);
 }
 

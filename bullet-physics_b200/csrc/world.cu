@@ -925,7 +925,8 @@ struct World {
                              world_offsets_dev(), nw, wplan, wcol.p, batch ? nullptr : &jd);
         else
             run_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); },
-                       step_count % RECOLOUR_PERIOD != 0, &jd);
+                       step_count % RECOLOUR_PERIOD != 0, &jd, batch ? nullptr : bp.leaf_body.p,
+                       batch ? 0u : uint32_t(bp.tree_m));
         ++step_count;
         // 6b: impulse writeback + prune
         run_cache_update(pairs.p, npairs, old_cache, pd, next, world_of, simulate, prev_simulate, stream);
