@@ -206,12 +206,12 @@ def count_launches(w, dt, nsteps=2):
 
 
 def solve_traffic(contacts):
-    """DRAM bytes per k_solve launch, from the committed ncu capture of the same kernel
-    (profiles/k_solve_large_pile_131072.md, a shorter-settled pile), scaled to this
-    launch by its contact count (the kernel's traffic grows with the rows it sweeps)."""
+    """DRAM bytes of the PGS launches of one step, from the committed ncu capture of the same
+    kernels (profiles/k_solve_chunks_large_pile_131072.md, a shorter-settled pile), scaled to
+    this step by its contact count (the kernels' traffic grows with the rows they sweep)."""
     import re
 
-    path = os.path.join(ROOT, "profiles", "k_solve_large_pile_131072.md")
+    path = os.path.join(ROOT, "profiles", "k_solve_chunks_large_pile_131072.md")
     try:
         text = open(path).read()
         dram = float(re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", text).group(1))
