@@ -410,6 +410,7 @@ constexpr uint32_t CHUNK_TOUCH = 8;          // foreign chunks recorded per body
 constexpr uint32_t CHUNK_EMPTY = 0xffffffffu;
 constexpr uint32_t CHUNK_MAX = 1024;         // blocks of a chunked launch
 constexpr uint32_t CHUNK_CTR_STRIDE = 8;     // progress counters 32 bytes apart
+constexpr uint32_t CHUNK_TB = 512;           // threads of a chunk block (one block per SM)
 
 __device__ __forceinline__ uint32_t group_owner(uint32_t ia, uint32_t ib, const float4* __restrict__ iw,
                                                 const uint32_t* __restrict__ chunk_of) {
@@ -1233,7 +1234,7 @@ __device__ __forceinline__ void chunk_phase(const SolveArgs& a, const ChunkArgs&
 // (the rest) are two launches of their own code (each keeps its registers); the counters run
 // on across the two, so the second launch starts with every neighbour past the warm start.
 template <bool WARM>
-__global__ void __launch_bounds__(256, 2) k_solve_chunks(SolveArgs a, ChunkArgs ch) {
+__global__ void __launch_bounds__(CHUNK_TB, 512 / CHUNK_TB) k_solve_chunks(SolveArgs a, ChunkArgs ch) {
     const uint32_t ncol = a.scalars[4];
     const uint32_t iters = a.iterations;
     const uint32_t b = blockIdx.x;
@@ -1686,7 +1687,7 @@ static int pgs_mode() {
 static int g_last_solver_kind = 0;
 int last_solver_kind() { return g_last_solver_kind; }
 
-constexpr size_t CHUNK_SMEM = size_t(VT_PLANES) * 256 * sizeof(float4);
+constexpr size_t CHUNK_SMEM = size_t(VT_PLANES) * CHUNK_TB * sizeof(float4);
 
 static int chunk_grid() {
     static int grid = 0;
@@ -1696,7 +1697,7 @@ static int chunk_grid() {
         for (int i = 0; i < 2; ++i) {
             check_cuda(cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize, int(CHUNK_SMEM)),
                        "smem attribute");
-            g[i] = coop_grid(fns[i], 256, CHUNK_SMEM);
+            g[i] = coop_grid(fns[i], CHUNK_TB, CHUNK_SMEM);
         }
         grid = std::min(g[0], g[1]);  // both launches cut the bodies into the same chunks
     }
@@ -1817,10 +1818,10 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
                      sp.info.num_iterations, JointsDev{}, sp.info.damping};
         ChunkArgs ch{P, W, voff, soff, vsec, pd.chunk_adj.p, all_flag, pd.chunk_ctr.p};
         void* args[] = {&sa, &ch};
-        check_cuda(cudaLaunchCooperativeKernel((const void*)k_solve_chunks<true>, dim3(P), dim3(256), args,
+        check_cuda(cudaLaunchCooperativeKernel((const void*)k_solve_chunks<true>, dim3(P), dim3(CHUNK_TB), args,
                                                CHUNK_SMEM, s), "chunked warm-start launch");
         if (sp.info.num_iterations)
-            check_cuda(cudaLaunchCooperativeKernel((const void*)k_solve_chunks<false>, dim3(P), dim3(256), args,
+            check_cuda(cudaLaunchCooperativeKernel((const void*)k_solve_chunks<false>, dim3(P), dim3(CHUNK_TB), args,
                                                    CHUNK_SMEM, s), "chunked solve launch");
         g_last_solver_kind = 2;
     } else {
