@@ -44,6 +44,7 @@ __device__ __forceinline__ Entry load_entry(const float4* __restrict__ e) {
     E.meta = __float_as_uint(c.w);
     E.dqb = q4(d);
     int n = E.count();
+#pragma unroll
     for (int k = 0; k < 4; ++k) {
         if (k >= n) break;
         float4 x = __ldg(&e[4 + 3 * k]), y = __ldg(&e[5 + 3 * k]), z = __ldg(&e[6 + 3 * k]);
@@ -55,13 +56,18 @@ __device__ __forceinline__ Entry load_entry(const float4* __restrict__ e) {
     return E;
 }
 
+// The point loops below run to a constant bound with a guard, so every E.p / Out index is a
+// compile-time constant after unrolling and the arrays stay in registers (a runtime index
+// would put them in local memory).
 __device__ __forceinline__ void store_entry(float4* e, const Entry& E) {
     e[0] = to4(E.dpa, E.thr);
     e[1] = to4(E.dqa);
     e[2] = to4(E.dpb, __uint_as_float(E.meta));
     e[3] = to4(E.dqb);
-    int n = E.count();
-    for (int k = 0; k < n; ++k) {
+    const int n = E.count();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (k >= n) break;
         e[4 + 3 * k] = to4(E.p[k].la, E.p[k].pen);
         e[5 + 3 * k] = to4(E.p[k].lb, E.p[k].imp);
         e[6 + 3 * k] = to4(E.p[k].n, __uint_as_float(E.p[k].life));
@@ -91,27 +97,59 @@ struct Out {
     uint32_t src[4];  // the loaded entry's index of the point each row comes from (0xff: new point)
 };
 
-// manifold.rs:246-282 — survivors keep their order, so out k addresses cache point k.
-__device__ __forceinline__ void refresh(Entry& E, V3 pa, Q qa, V3 pb, Q qb, Out& o) {
-    float thr = E.thr, thr_sq = thr * thr;
-    int kept = 0;
-    o.n = 0;
-    int n = E.count();
-    for (int k = 0; k < n; ++k) {
-        Pt p = E.p[k];
-        V3 wa = pa + rotate(qa, p.la);
-        V3 wb = pb + rotate(qb, p.lb);
-        V3 d = wa - wb;
-        float pen = dot(d, p.n);
-        if (pen < -thr) continue;
-        V3 lat = d - p.n * pen;
-        if (len2(lat) > thr_sq) continue;
-        p.pen = pen;
-        p.life += 1;
-        o.pos[o.n] = wb; o.nrm[o.n] = p.n; o.pen[o.n] = pen; o.imp[o.n] = p.imp; o.src[o.n] = p.src; o.n++;
-        E.p[kept++] = p;
+// manifold.rs:246-282: a point survives while its penetration stays above -thr and its lateral
+// drift below thr. The survivors keep their order (out k addresses surviving point k); they are
+// not moved here: K marks them, and store_entry_kept / emit_rows_kept write them compacted to
+// global memory, so no runtime index touches E.p and the entry stays in registers.
+struct Kept {
+    bool k[4];
+    V3 wb[4];  // the survivor's world point on B
+    int n;
+};
+
+__device__ __forceinline__ void refresh(Entry& E, V3 pa, Q qa, V3 pb, Q qb, Kept& K) {
+    const float thr = E.thr, thr_sq = thr * thr;
+    const int n = E.count();
+    K.n = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        K.k[k] = false;
+        K.wb[k] = V3{0.0f, 0.0f, 0.0f};
+        if (k < n) {
+            Pt& p = E.p[k];
+            const V3 wa = pa + rotate(qa, p.la);
+            const V3 wb = pb + rotate(qb, p.lb);
+            const V3 d = wa - wb;
+            const float pen = dot(d, p.n);
+            if (!(pen < -thr)) {
+                const V3 lat = d - p.n * pen;
+                if (!(len2(lat) > thr_sq)) {
+                    p.pen = pen;
+                    p.life += 1;
+                    K.wb[k] = wb;
+                    K.k[k] = true;
+                    ++K.n;
+                }
+            }
+        }
     }
-    E.meta = (E.meta & ~7u) | uint32_t(kept);
+}
+
+// The refreshed entry: header, count = survivors, survivors in order.
+__device__ __forceinline__ void store_entry_kept(float4* e, const Entry& E, const Kept& K) {
+    e[0] = to4(E.dpa, E.thr);
+    e[1] = to4(E.dqa);
+    e[2] = to4(E.dpb, __uint_as_float((E.meta & ~7u) | uint32_t(K.n)));
+    e[3] = to4(E.dqb);
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (!K.k[k]) continue;
+        e[4 + 3 * s] = to4(E.p[k].la, E.p[k].pen);
+        e[5 + 3 * s] = to4(E.p[k].lb, E.p[k].imp);
+        e[6 + 3 * s] = to4(E.p[k].n, __uint_as_float(E.p[k].life));
+        ++s;
+    }
 }
 
 __device__ __forceinline__ int32_t total_key(float v) {
@@ -119,15 +157,22 @@ __device__ __forceinline__ int32_t total_key(float v) {
     return b ^ int32_t(uint32_t(b >> 31) >> 1);
 }
 
-// manifold.rs:326-376
-__device__ __forceinline__ void capture(Entry& E, const Manifold& m, V3 pa, Q qa, V3 pb, Q qb, float thr) {
+// manifold.rs:326-376. pts holds the up to 8 candidate points of this thread (the cached ones,
+// then the new ones that match none), pts[k * stride]: k_capture keeps them in shared memory,
+// where a runtime index costs nothing.
+__device__ __forceinline__ void capture(Entry& E, const Manifold& m, V3 pa, Q qa, V3 pb, Q qb, float thr, Pt* pts,
+                                        uint32_t stride) {
     E.thr = thr;
     Q ia = qinv(qa), ib = qinv(qb);
     float thr_sq = thr * thr;
-    Pt pts[8];
+    auto P = [&](int k) -> Pt& { return pts[size_t(k) * stride]; };
     int n = E.count();
-    for (int k = 0; k < n; ++k) pts[k] = E.p[k];
-    for (int c = 0; c < m.n; ++c) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (k < n) P(k) = E.p[k];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        if (c >= m.n) break;
         V3 wb = m.pos[c];
         V3 wa = m.pos[c] + m.nrm[c] * m.pen[c];
         Pt pt;
@@ -140,27 +185,30 @@ __device__ __forceinline__ void capture(Entry& E, const Manifold& m, V3 pa, Q qa
         pt.src = 0xffu;
         bool matched = false;
         for (int k = 0; k < n; ++k) {
-            if (len2(pts[k].la - pt.la) < thr_sq && dot(pts[k].n, pt.n) >= 0.9f) {
-                pt.imp = pts[k].imp;
-                pt.src = pts[k].src;
-                pts[k] = pt;
+            Pt& q = P(k);
+            if (len2(q.la - pt.la) < thr_sq && dot(q.n, pt.n) >= 0.9f) {
+                pt.imp = q.imp;
+                pt.src = q.src;
+                q = pt;
                 matched = true;
                 break;
             }
         }
-        if (!matched) pts[n++] = pt;
+        if (!matched) P(n++) = pt;
     }
     if (n > 4) {  // stable descending sort by penetration (total order), keep four
         for (int a = 1; a < n; ++a) {
-            Pt v = pts[a];
+            Pt v = P(a);
             int32_t kv = total_key(v.pen);
             int b = a;
-            while (b > 0 && total_key(pts[b - 1].pen) < kv) { pts[b] = pts[b - 1]; --b; }
-            pts[b] = v;
+            while (b > 0 && total_key(P(b - 1).pen) < kv) { P(b) = P(b - 1); --b; }
+            P(b) = v;
         }
         n = 4;
     }
-    for (int k = 0; k < n; ++k) E.p[k] = pts[k];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (k < n) E.p[k] = P(k);
     E.dpa = pa; E.dqa = qa; E.dpb = pb; E.dqb = qb;
     E.meta = (E.meta & ~7u) | uint32_t(n) | META_INIT | META_VALID;
 }
@@ -180,58 +228,99 @@ __device__ __forceinline__ float effective_mass(float ima, float imb, V3 aa, V3 
 // step.rs:750-764 + sequential_impulse.rs:339-550: one prepared row per refreshed point.
 // rec_row_src (adjoint recording, else null) receives, per row, the old cache position * 4 + point
 // index that supplied its warm-start impulse (old: the pair's old cache position, or -1).
+struct RowCtx {
+    float ima, imb;
+    M3 iwa, iwb;
+    V3 posa, posb;
+    float4 ma, mb;
+};
+
+__device__ __forceinline__ RowCtx row_ctx(const BodyDev& b, uint32_t i, uint32_t j) {
+    RowCtx c;
+    c.iwa = load_iw(b.iw, i, c.ima);
+    c.iwb = load_iw(b.iw, j, c.imb);
+    c.posa = from4(b.pos[i]);
+    c.posb = from4(b.pos[j]);
+    c.ma = b.material[i];
+    c.mb = b.material[j];
+    return c;
+}
+
+__device__ __forceinline__ void emit_row(const RowCtx& c, const StepParams& sp, V3 pos, V3 n, float pen,
+                                         float imp_cached, float4* r) {
+    const SolverParams& info = sp.info;
+    const float inv_dt = sp.inv_dt;
+    const float ima = c.ima, imb = c.imb;
+    const M3& iwa = c.iwa;
+    const M3& iwb = c.iwb;
+    float imp = imp_cached * info.warmstarting_factor;
+    V3 t1, t2;
+    tangent_basis_dev(n, t1, t2);
+    V3 ra = pos - c.posa;
+    V3 rb = pos - c.posb;
+    V3 ana = mul(iwa, cross(ra, n)), anb = mul(iwb, cross(rb, n));
+    V3 a1a = mul(iwa, cross(ra, t1)), a1b = mul(iwb, cross(rb, t1));
+    V3 a2a = mul(iwa, cross(ra, t2)), a2b = mul(iwb, cross(rb, t2));
+    float nm = effective_mass(ima, imb, ana, anb, ra, rb, n);
+    float t1m = effective_mass(ima, imb, a1a, a1b, ra, rb, t1);
+    float t2m = effective_mass(ima, imb, a2a, a2b, ra, rb, t2);
+    float friction = c.ma.x * c.mb.x;
+    float restitution = c.ma.y * c.mb.y;
+    float erp = info.erp2;
+    float ncfm = 0.0f;
+    float cfm_global = info.global_cfm * inv_dt;
+    if (cfm_global != 0.0f || info.sor != 1.0f) {
+        float kk = nm > 0.0f ? 1.0f / nm : 0.0f;
+        nm = kk + cfm_global > 0.0f ? info.sor / (kk + cfm_global) : 0.0f;
+        ncfm = cfm_global * nm;
+    }
+    if (info.sor != 1.0f) { t1m *= info.sor; t2m *= info.sor; }
+    float span = fmaxf(pen - info.linear_slop, 0.0f);
+    float separation = fminf(pen, 0.0f);
+    bool split = info.split_impulse != 0 && pen > -info.split_impulse_penetration_threshold;
+    float baum = split ? 0.0f : erp * inv_dt * span;
+    float sepb = separation < 0.0f ? separation * inv_dt : 0.0f;
+    float rhs = split ? pen * erp * inv_dt * nm : 0.0f;
+    r[0] = to4(n, friction);
+    r[1] = to4(ra, baum);
+    r[2] = to4(rb, sepb);
+    r[3] = make_float4(imp, 0.0f, 0.0f, restitution);
+    r[4] = make_float4(nm, t1m, t2m, ncfm);
+    r[5] = make_float4(rhs, 0.0f, split ? 1.0f : 0.0f, pen);
+}
+
+// Rows of explicit contact points (the stand-alone row preparation).
 __device__ __forceinline__ void emit_rows(const BodyDev& b, uint32_t i, uint32_t j, const Out& o, const StepParams& sp,
                                           float4* __restrict__ rows, uint32_t* __restrict__ row_count, uint32_t p,
                                           uint32_t* rec_row_src, int64_t old) {
-    float ima, imb;
-    M3 iwa = load_iw(b.iw, i, ima);
-    M3 iwb = load_iw(b.iw, j, imb);
-    V3 posa = from4(b.pos[i]), posb = from4(b.pos[j]);
-    float4 ma = b.material[i], mb = b.material[j];
-    const SolverParams& info = sp.info;
-    float inv_dt = sp.inv_dt;
-    for (int k = 0; k < o.n; ++k) {
-        V3 n = o.nrm[k];
-        float imp = o.imp[k] * info.warmstarting_factor;
-        V3 t1, t2;
-        tangent_basis_dev(n, t1, t2);
-        V3 ra = o.pos[k] - posa;
-        V3 rb = o.pos[k] - posb;
-        V3 ana = mul(iwa, cross(ra, n)), anb = mul(iwb, cross(rb, n));
-        V3 a1a = mul(iwa, cross(ra, t1)), a1b = mul(iwb, cross(rb, t1));
-        V3 a2a = mul(iwa, cross(ra, t2)), a2b = mul(iwb, cross(rb, t2));
-        float nm = effective_mass(ima, imb, ana, anb, ra, rb, n);
-        float t1m = effective_mass(ima, imb, a1a, a1b, ra, rb, t1);
-        float t2m = effective_mass(ima, imb, a2a, a2b, ra, rb, t2);
-        float friction = ma.x * mb.x;
-        float restitution = ma.y * mb.y;
-        float erp = info.erp2;
-        float ncfm = 0.0f;
-        float cfm_global = info.global_cfm * inv_dt;
-        if (cfm_global != 0.0f || info.sor != 1.0f) {
-            float kk = nm > 0.0f ? 1.0f / nm : 0.0f;
-            nm = kk + cfm_global > 0.0f ? info.sor / (kk + cfm_global) : 0.0f;
-            ncfm = cfm_global * nm;
-        }
-        if (info.sor != 1.0f) { t1m *= info.sor; t2m *= info.sor; }
-        float pen = o.pen[k];
-        float span = fmaxf(pen - info.linear_slop, 0.0f);
-        float separation = fminf(pen, 0.0f);
-        bool split = info.split_impulse != 0 && pen > -info.split_impulse_penetration_threshold;
-        float baum = split ? 0.0f : erp * inv_dt * span;
-        float sepb = separation < 0.0f ? separation * inv_dt : 0.0f;
-        float rhs = split ? pen * erp * inv_dt * nm : 0.0f;
-        float4* r = rows + (size_t(p) * 4 + k) * ROW_F4;
-        r[0] = to4(n, friction);
-        r[1] = to4(ra, baum);
-        r[2] = to4(rb, sepb);
-        r[3] = make_float4(imp, 0.0f, 0.0f, restitution);
-        r[4] = make_float4(nm, t1m, t2m, ncfm);
-        r[5] = make_float4(rhs, 0.0f, split ? 1.0f : 0.0f, pen);
+    const RowCtx c = row_ctx(b, i, j);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (k >= o.n) break;
+        emit_row(c, sp, o.pos[k], o.nrm[k], o.pen[k], o.imp[k], rows + (size_t(p) * 4 + k) * ROW_F4);
         if (rec_row_src)
             rec_row_src[size_t(p) * 4 + k] = (old >= 0 && o.src[k] < 4u) ? uint32_t(old) * 4u + o.src[k] : REC_NONE;
     }
     row_count[p] = uint32_t(o.n);
+}
+
+// Rows of an entry's refreshed survivors, in order.
+__device__ __forceinline__ void emit_rows_kept(const BodyDev& b, uint32_t i, uint32_t j, const Entry& E, const Kept& K,
+                                               const StepParams& sp, float4* __restrict__ rows,
+                                               uint32_t* __restrict__ row_count, uint32_t p, uint32_t* rec_row_src,
+                                               int64_t old) {
+    const RowCtx c = row_ctx(b, i, j);
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (!K.k[k]) continue;
+        emit_row(c, sp, K.wb[k], E.p[k].n, E.p[k].pen, E.p[k].imp, rows + (size_t(p) * 4 + s) * ROW_F4);
+        if (rec_row_src)
+            rec_row_src[size_t(p) * 4 + s] =
+                (old >= 0 && E.p[k].src < 4u) ? uint32_t(old) * 4u + E.p[k].src : REC_NONE;
+        ++s;
+    }
+    row_count[p] = uint32_t(K.n);
 }
 
 __device__ __forceinline__ uint32_t route_of(uint32_t ta, uint32_t tb) {
@@ -359,23 +448,40 @@ __global__ void k_classify(BodyDev b, const Shape* __restrict__ shapes, const ui
     Entry E;
     E.meta = 0;
     if (old >= 0) E = load_entry(old_entries + size_t(old) * ENTRY_F4);
+    Kept K;
+    K.n = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) K.k[k] = k < E.count();  // no refresh: the loaded points as they are
     if (old >= 0 && !needs_redetect(E, pa, qa, pb, qb)) {
-        Out o;
-        refresh(E, pa, qa, pb, qb, o);
+        refresh(E, pa, qa, pb, qb, K);
         bool deep = false;
-        for (int k = 0; k < o.n; ++k) if (o.pen[k] > sp.info.linear_slop) deep = true;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (K.k[k] && E.p[k].pen > sp.info.linear_slop) deep = true;
         if (!fast || !deep) {
-            store_entry(ne, E);
-            if (!no_response) emit_rows(b, i, j, o, sp, pd.rows, pd.row_count, p, pd.rec.row_src, old);
+            store_entry_kept(ne, E, K);
+            if (!no_response) emit_rows_kept(b, i, j, E, K, sp, pd.rows, pd.row_count, p, pd.rec.row_src, old);
             pd.status[p] = PS_SERVED;
             return;
         }
+    } else {
+        K.n = E.count();
     }
-    if (old >= 0) store_entry(ne, E);
+    if (old >= 0) store_entry_kept(ne, E, K);
     else store_meta_only(ne, 0u);
     if (pd.rec.pt_src) {  // where the stored points came from, for the capture pass
         pd.rec.pair_old[p] = old >= 0 ? uint32_t(old) : REC_NONE;
-        for (int k = 0; k < 4; ++k) pd.rec.pt_src[size_t(p) * 4 + k] = (old >= 0 && k < E.count()) ? uint8_t(E.p[k].src) : uint8_t(0xff);
+        uint32_t packed = 0xffffffffu;  // byte s: the source of stored point s
+        int s = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (old >= 0 && K.k[k]) {
+                packed = (packed & ~(0xffu << (8 * s))) | ((E.p[k].src & 0xffu) << (8 * s));
+                ++s;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) pd.rec.pt_src[size_t(p) * 4 + k] = uint8_t(packed >> (8 * k));
     }
     uint32_t route = route_of(shapes[ia.x].type, shapes[ib.x].type);
     pd.status[p] = PS_DETECT | (route << 8);
@@ -861,7 +967,7 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_narrow_mesh(BodyDev b, cons
 
 // step.rs:800-853: merge the detection into the manifold, refresh, emit rows; or drop the manifold.
 __device__ __forceinline__ void capture_one(const BodyDev& b, const Shape* __restrict__ shapes, const uint64_t* __restrict__ pairs,
-                                            const StepParams& sp, PairDataDev& pd, uint32_t p) {
+                                            const StepParams& sp, PairDataDev& pd, uint32_t p, Pt* pts, uint32_t stride) {
     uint64_t key = pairs[p];
     uint32_t i = key_lo(key), j = key_hi(key);
     float4* ne = pd.entries + size_t(p) * ENTRY_F4;
@@ -869,7 +975,9 @@ __device__ __forceinline__ void capture_one(const BodyDev& b, const Shape* __res
     Manifold m;
     m.n = int(n);
     const float4* d = pd.detect + size_t(p) * 8;
-    for (uint32_t k = 0; k < n; ++k) {
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) {
+        if (k >= n) break;
         float4 a = d[2 * k], c = d[2 * k + 1];
         m.pos[k] = from4(a); m.pen[k] = a.w; m.nrm[k] = from4(c);
     }
@@ -887,22 +995,26 @@ __device__ __forceinline__ void capture_one(const BodyDev& b, const Shape* __res
     V3 pa = from4(b.pred[i]), pb = from4(b.pred[j]);
     Q qa = q4(b.quat[i]), qb = q4(b.quat[j]);
     float thr = fminf(shapes[ia.x].cbt, shapes[ib.x].cbt);
-    capture(E, m, pa, qa, pb, qb, thr);
-    Out o;
-    refresh(E, pa, qa, pb, qb, o);
-    store_entry(ne, E);
+    capture(E, m, pa, qa, pb, qb, thr, pts, stride);
+    Kept K;
+    refresh(E, pa, qa, pb, qb, K);
+    store_entry_kept(ne, E, K);
     if (((ia.y | ib.y) & BF_NO_RESPONSE) == 0) {
         const int64_t old = pd.rec.pair_old ? (pd.rec.pair_old[p] == REC_NONE ? -1 : int64_t(pd.rec.pair_old[p])) : -1;
-        emit_rows(b, i, j, o, sp, pd.rows, pd.row_count, p, pd.rec.row_src, old);
+        emit_rows_kept(b, i, j, E, K, sp, pd.rows, pd.row_count, p, pd.rec.row_src, old);
     }
 }
 
-__global__ void k_capture(BodyDev b, const Shape* __restrict__ shapes, const uint64_t* __restrict__ pairs,
-                          uint32_t npairs, StepParams sp, PairDataDev pd) {
+constexpr uint32_t CAPTURE_TB = 64;
+
+__global__ void __launch_bounds__(CAPTURE_TB) k_capture(BodyDev b, const Shape* __restrict__ shapes,
+                                                        const uint64_t* __restrict__ pairs, uint32_t npairs,
+                                                        StepParams sp, PairDataDev pd) {
+    __shared__ Pt s_pts[8][CAPTURE_TB];  // capture()'s candidate points, [k][thread]
     const uint32_t cnt = pd.scalars[CAPTURE_COUNT];
     const uint32_t* list = pd.route_list + size_t(CAPTURE_LIST) * npairs;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
-        capture_one(b, shapes, pairs, sp, pd, list[t]);
+        capture_one(b, shapes, pairs, sp, pd, list[t], &s_pts[0][threadIdx.x], CAPTURE_TB);
     }
 }
 
@@ -995,7 +1107,8 @@ void run_pair_pass(const WorldView& w, const uint64_t* pairs, uint32_t npairs, c
     // The GJK/EPA kernels keep their polytopes in local memory (12-15 KB a thread): a launch
     // the device cannot back with local memory fails here rather than dropping detections.
     check_cuda(cudaGetLastError(), "narrow phase launch");
-    k_capture<<<grid, TB, 0, s>>>(w.b, w.shapes, pairs, npairs, sp, d);
+    k_capture<<<(npairs + CAPTURE_TB - 1) / CAPTURE_TB < 148u * 16u ? (npairs + CAPTURE_TB - 1) / CAPTURE_TB : 148u * 16u,
+                CAPTURE_TB, 0, s>>>(w.b, w.shapes, pairs, npairs, sp, d);
 }
 
 void run_collide_queries(const Shape* shapes, const float4* hull, uint32_t n, const uint32_t* sa, const float4* pa,
