@@ -7,6 +7,8 @@
 // The reference scans every body for every CCD body as well; the cast itself (a ternary search
 // for the closest approach, then bisection, each probe a GJK point distance) matches its
 // arithmetic step for step.
+#include <cstdio>
+#include <cstdlib>
 #include "bgpu_kernels.cuh"
 
 namespace bgpu {
@@ -24,7 +26,7 @@ __device__ __forceinline__ void keep2(Simplex& s, V3 a, V3 b) { s.p[0] = a; s.p[
 __device__ __forceinline__ void keep3(Simplex& s, V3 a, V3 b, V3 c) { s.p[0] = a; s.p[1] = b; s.p[2] = c; s.n = 3; }
 
 // gjk.rs:889-906
-__device__ V3 closest_segment(V3 a, V3 b, Simplex& keep) {
+__device__ __forceinline__ V3 closest_segment(V3 a, V3 b, Simplex& keep) {
     const V3 ab = b - a;
     if (len2(ab) == 0.0f) { keep1(keep, a); return a; }
     const float t = -dot(a, ab) / len2(ab);
@@ -34,8 +36,19 @@ __device__ V3 closest_segment(V3 a, V3 b, Simplex& keep) {
     return a + ab * t;
 }
 
+// gjk.rs:911-989, a degenerate triangle: the closest of its three edges. A call of its own
+// (rarely taken), so the common path keeps the simplex in registers.
+__device__ __noinline__ V3 closest_triangle_edges(V3 a, V3 b, V3 c, Simplex& keep) {
+    Simplex kab, kbc, kca;
+    const V3 qab = closest_segment(a, b, kab), qbc = closest_segment(b, c, kbc), qca = closest_segment(c, a, kca);
+    if (len2(qab) <= len2(qbc) && len2(qab) <= len2(qca)) { keep = kab; return qab; }
+    if (len2(qbc) <= len2(qca)) { keep = kbc; return qbc; }
+    keep = kca;
+    return qca;
+}
+
 // gjk.rs:911-989
-__device__ V3 closest_triangle(V3 a, V3 b, V3 c, Simplex& keep) {
+__device__ __forceinline__ V3 closest_triangle(V3 a, V3 b, V3 c, Simplex& keep) {
     const V3 ab = b - a, ac = c - a, ap = -a;
     const float d1 = dot(ab, ap), d2 = dot(ac, ap);
     if (d1 <= 0.0f && d2 <= 0.0f) { keep1(keep, a); return a; }
@@ -67,37 +80,33 @@ __device__ V3 closest_triangle(V3 a, V3 b, V3 c, Simplex& keep) {
         return b + (c - b) * w;
     }
     const float sum = va + vb + vc;
-    if (sum <= 0.0f || isnan(sum)) {
-        Simplex kab, kbc, kca;
-        const V3 qab = closest_segment(a, b, kab), qbc = closest_segment(b, c, kbc), qca = closest_segment(c, a, kca);
-        if (len2(qab) <= len2(qbc) && len2(qab) <= len2(qca)) { keep = kab; return qab; }
-        if (len2(qbc) <= len2(qca)) { keep = kbc; return qbc; }
-        keep = kca;
-        return qca;
-    }
+    if (sum <= 0.0f || isnan(sum)) return closest_triangle_edges(a, b, c, keep);
     const float denom = 1.0f / sum;
     const float v = vb * denom, w = vc * denom;
     keep3(keep, c, b, a);
     return a + ab * v + ac * w;
 }
 
-// gjk.rs:994-1044
-__device__ V3 closest_tetrahedron(V3 a, V3 b, V3 c, V3 d, Simplex& keep) {
-    const V3 ao = -a, ab = b - a, ac = c - a, ad = d - a;
-    if (fabsf(dot(cross(ab, ac), ad)) < 1e-12f) {
-        // coplanar: the closest of the four faces, the first of equal ones
-        const V3 f[4][3] = {{a, b, c}, {a, b, d}, {a, c, d}, {b, c, d}};
-        V3 best = V3{0.0f, 0.0f, 0.0f};
-        Simplex best_keep;
-        best_keep.n = 0;
-        for (int k = 0; k < 4; ++k) {
-            Simplex kk;
-            const V3 q = closest_triangle(f[k][0], f[k][1], f[k][2], kk);
-            if (k == 0 || len2(q) < len2(best)) { best = q; best_keep = kk; }
-        }
-        keep = best_keep;
-        return best;
+// gjk.rs:994-1044, coplanar points: the closest of the four faces, the first of equal ones (a
+// call of its own, rarely taken).
+__device__ __noinline__ V3 closest_coplanar(V3 a, V3 b, V3 c, V3 d, Simplex& keep) {
+    const V3 f[4][3] = {{a, b, c}, {a, b, d}, {a, c, d}, {b, c, d}};
+    V3 best = V3{0.0f, 0.0f, 0.0f};
+    Simplex best_keep;
+    best_keep.n = 0;
+    for (int k = 0; k < 4; ++k) {
+        Simplex kk;
+        const V3 q = closest_triangle(f[k][0], f[k][1], f[k][2], kk);
+        if (k == 0 || len2(q) < len2(best)) { best = q; best_keep = kk; }
     }
+    keep = best_keep;
+    return best;
+}
+
+// gjk.rs:994-1044
+__device__ __forceinline__ V3 closest_tetrahedron(V3 a, V3 b, V3 c, V3 d, Simplex& keep) {
+    const V3 ao = -a, ab = b - a, ac = c - a, ad = d - a;
+    if (fabsf(dot(cross(ab, ac), ad)) < 1e-12f) return closest_coplanar(a, b, c, d, keep);
     const V3 abc = cross(ab, ac), acd = cross(ac, ad), adb = cross(ad, ab);
     const V3 bo = -b;
     const V3 bcd = cross(c - b, d - b);
@@ -110,7 +119,7 @@ __device__ V3 closest_tetrahedron(V3 a, V3 b, V3 c, V3 d, Simplex& keep) {
 }
 
 // gjk.rs:864-885
-__device__ V3 closest_origin(Simplex& s) {
+__device__ __forceinline__ V3 closest_origin(Simplex& s) {
     Simplex keep;
     V3 v;
     switch (s.n) {
@@ -139,7 +148,7 @@ struct Inflated {
 
 // convex_sweep.rs:72-103: squared distance from `point` to the inflated target and the unit
 // direction from the target toward the point (zero when inside or touching).
-__device__ float point_distance(const Inflated& t, V3 point, V3& dir) {
+__device__ __forceinline__ float point_distance(const Inflated& t, V3 point, V3& dir) {
     auto mink = [&](V3 v) { return point - t.support(-v); };
     V3 v = point;
     if (len2(v) < 1e-12f) v = V3{1.0f, 0.0f, 0.0f};
@@ -150,10 +159,18 @@ __device__ float point_distance(const Inflated& t, V3 point, V3& dir) {
     for (int it = 0; it < 64; ++it) {
         if (len2(v) < 1e-10f) { dir = V3{0.0f, 0.0f, 0.0f}; return 0.0f; }
         const V3 w = mink(-v);
-        for (int k = 0; k < s.n; ++k)
-            if (len2(s.p[k] - w) < 1e-12f) { dir = v / len(v); return len2(v); }
+        bool repeat = false;  // the simplex already holds w (constant indices keep s in registers)
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k < s.n && len2(s.p[k] - w) < 1e-12f) repeat = true;
+        if (repeat) { dir = v / len(v); return len2(v); }
         if (s.n >= 4) break;  // unreachable: a kept tetrahedron means v == 0, which returned above
-        s.p[s.n++] = w;
+        switch (s.n) {
+            case 1: s.p[1] = w; break;
+            case 2: s.p[2] = w; break;
+            default: s.p[3] = w; break;
+        }
+        ++s.n;
         v = closest_origin(s);
     }
     if (len2(v) < 1e-10f) { dir = V3{0.0f, 0.0f, 0.0f}; return 0.0f; }
@@ -344,6 +361,7 @@ constexpr int CCD_THREADS = 32;
 constexpr int CCD_CAP = 256;
 constexpr uint32_t CCD_TREE_CAP = 1024;          // tree hits per CCD body before the world scan
 constexpr uint32_t TREE_LEAF_REF = 0x80000000u;  // leaf children in the broad-phase node records
+constexpr uint32_t CCD_WARP_CAST_MAX = 6;        // candidates left for which casts take the whole warp
 
 struct CcdCtx {
     V3 from, to, dir;
@@ -367,6 +385,105 @@ __device__ __forceinline__ float cast_one(const BodyDev& b, const Shape* __restr
     return hit ? f : 1.0f;
 }
 
+// The cast of one candidate by a whole warp, with the same result as sweep_convex: the
+// ternary search's decisions depend only on the probes, so each round evaluates every probe of
+// the next 4 levels of its decision tree at once (15 nodes x 2 probes on lanes 0-29) and then
+// follows the taken path; the bisection likewise 5 levels per round (31 probes). A node's
+// (lo, hi) is replayed from the round's root with the same operations as the sequential loop,
+// so every probe point, and the fraction, is bit-identical to sweep_convex's.
+__device__ __forceinline__ void replay_ternary(float& l, float& h, uint32_t node) {
+    uint32_t path = 0, depth = 0;  // bit t: the branch taken at depth t + 1 (collected leaf first)
+    for (uint32_t x = node; x > 0; x = (x - 1) >> 1) {
+        path = (path << 1) | ((x & 1u) ? 0u : 1u);  // odd child: d(m1) < d(m2) (hi = m2)
+        ++depth;
+    }
+    for (uint32_t t = 0; t < depth; ++t) {
+        const float m1 = l + (h - l) / 3.0f;
+        const float m2 = h - (h - l) / 3.0f;
+        if (((path >> t) & 1u) == 0u) h = m2;
+        else l = m1;
+    }
+}
+
+__device__ __forceinline__ void replay_bisect(float& l, float& h, uint32_t node) {
+    uint32_t path = 0, depth = 0;
+    for (uint32_t x = node; x > 0; x = (x - 1) >> 1) {
+        path = (path << 1) | ((x & 1u) ? 0u : 1u);  // odd child: d(mid) <= 1e-8 (high = mid)
+        ++depth;
+    }
+    for (uint32_t t = 0; t < depth; ++t) {
+        const float mid = (l + h) * 0.5f;
+        if (((path >> t) & 1u) == 0u) h = mid;
+        else l = mid;
+    }
+}
+
+// td / bd: levels of the ternary / bisection decision tree evaluated per round (td <= 4: 2 (2^td
+// - 1) probes; bd <= 5: 2^bd - 1 probes). Deeper trees take fewer rounds but more probes.
+__device__ bool sweep_convex_warp(V3 from, V3 dir, float length, const Inflated& t, float& fraction, uint32_t td,
+                                  uint32_t bd) {
+    const uint32_t lane = threadIdx.x & 31u;
+    float lo = 0.0f, hi = 1.0f;
+    for (uint32_t done = 0; done < 40;) {  // 40 ternary steps
+        const uint32_t depth = min(td, 40u - done);
+        const uint32_t probes = 2u * ((1u << depth) - 1u);
+        float v = 0.0f;
+        if (lane < probes) {
+            float l = lo, h = hi;
+            replay_ternary(l, h, lane >> 1);
+            const float m = (lane & 1u) ? h - (h - l) / 3.0f : l + (h - l) / 3.0f;
+            v = point_distance2(t, from + dir * (m * length));
+        }
+        uint32_t n = 0;
+        for (uint32_t d = 0; d < depth; ++d) {
+            const float d1 = __shfl_sync(0xffffffffu, v, int(2 * n));
+            const float d2 = __shfl_sync(0xffffffffu, v, int(2 * n + 1));
+            const float m1 = lo + (hi - lo) / 3.0f;
+            const float m2 = hi - (hi - lo) / 3.0f;
+            if (d1 < d2) { hi = m2; n = 2 * n + 1; }
+            else { lo = m1; n = 2 * n + 2; }
+        }
+        done += depth;
+    }
+    const float s_min = (lo + hi) * 0.5f;
+    if (point_distance2(t, from + dir * (s_min * length)) > 1e-8f) return false;
+    float low = 0.0f, high = s_min;
+    for (uint32_t done = 0; done < 60;) {  // 60 bisection steps
+        const uint32_t depth = min(bd, 60u - done);
+        float v = 0.0f;
+        if (lane < (1u << depth) - 1u) {
+            float l = low, h = high;
+            replay_bisect(l, h, lane);
+            v = point_distance2(t, from + dir * (((l + h) * 0.5f) * length));
+        }
+        uint32_t n = 0;
+        for (uint32_t d = 0; d < depth; ++d) {
+            const float dm = __shfl_sync(0xffffffffu, v, int(n));
+            const float mid = (low + high) * 0.5f;
+            if (dm <= 1e-8f) { high = mid; n = 2 * n + 1; }
+            else { low = mid; n = 2 * n + 2; }
+        }
+        done += depth;
+    }
+    fraction = (low + high) * 0.5f;
+    return true;
+}
+
+// cast_one for the whole warp (every lane returns the fraction): convex targets through
+// sweep_convex_warp; planes and meshes by lane 0, broadcast.
+__device__ __forceinline__ float cast_warp(const BodyDev& b, const Shape* __restrict__ shapes, const float4* __restrict__ hull,
+                                           const CcdCtx& c, uint32_t j, uint32_t td, uint32_t bd) {
+    const Shape& sj = shapes[b.info[j].x];
+    if (sj.type == SHAPE_PLANE || sj.type == SHAPE_MESH) {
+        float f = 1.0f;
+        if ((threadIdx.x & 31u) == 0u) f = cast_one(b, shapes, hull, c, j);
+        return __shfl_sync(0xffffffffu, f, 0);
+    }
+    Inflated t{sj, from4(b.pos[j]), q4(b.quat[j]), c.radius, hull};
+    float f;
+    return sweep_convex_warp(c.from, c.dir, c.length, t, f, td, bd) ? f : 1.0f;
+}
+
 __device__ __forceinline__ float warp_min(float v) {
     for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
@@ -382,7 +499,8 @@ __global__ void __launch_bounds__(CCD_THREADS) k_ccd_sweep(BodyDev b, const Shap
                                                            float dt, float* clamp, uint32_t* status,
                                                            const float4* __restrict__ tree_rec,
                                                            const uint32_t* __restrict__ tree_leaf, int tree_m,
-                                                           const uint32_t* __restrict__ unb, uint32_t nunb) {
+                                                           const uint32_t* __restrict__ unb, uint32_t nunb,
+                                                           uint32_t depths) {
     __shared__ uint32_t cand[CCD_CAP], sorted[CCD_CAP];
     __shared__ uint32_t tlist[CCD_TREE_CAP];
     __shared__ uint32_t ntl;
@@ -537,8 +655,16 @@ __global__ void __launch_bounds__(CCD_THREADS) k_ccd_sweep(BodyDev b, const Shap
             slb[r] = v;
         }
         __syncthreads();
-        for (uint32_t w0 = 0; w0 < nc; w0 += CCD_THREADS) {
-            if (!(slb[w0] < best)) break;  // every later candidate hits no sooner than best
+        // Few candidates: one at a time with the whole warp (23 probe latencies a cast); many:
+        // a candidate per lane (141 probe latencies for up to 32 casts).
+        uint32_t s0 = 0;
+        while (s0 < nc && nc - s0 <= CCD_WARP_CAST_MAX) {
+            if (!(slb[s0] < best)) break;  // every later candidate hits no sooner than best
+            best = fminf(best, cast_warp(b, shapes, hull, c, sorted[s0], depths & 0xffu, depths >> 8));
+            ++s0;
+        }
+        for (uint32_t w0 = s0; w0 < nc; w0 += CCD_THREADS) {
+            if (!(slb[w0] < best)) break;
             const uint32_t s = w0 + lane;
             float f = 1.0f;
             if (s < nc && slb[s] < best) f = cast_one(b, shapes, hull, c, sorted[s]);
@@ -569,8 +695,20 @@ void launch_ccd_sweep(const BodyDev& b, const Shape* shapes, const float4* hull,
                       const float4* tree_rec, const uint32_t* tree_leaf, int tree_m, const uint32_t* unb,
                       uint32_t nunb, cudaStream_t s) {
     if (m == 0) return;
+    // Speculation depths of the whole-warp casts (ternary | bisection << 8). On ccd_rain (2,048
+    // casting bodies) the deepest trees measured fastest: 14.9 ms per step at (4, 5) against
+    // 16.5 at (3, 4), 18.2 at (2, 3) and 22.2 at (1, 2). BGPU_CCD_DEPTH="t,b" overrides them,
+    // for measurement.
+    uint32_t td = 4u, bd = 5u;
+    static int env_td = -1, env_bd = -1;
+    if (env_td < 0) {
+        env_td = env_bd = 0;
+        if (const char* e = std::getenv("BGPU_CCD_DEPTH")) std::sscanf(e, "%d,%d", &env_td, &env_bd);
+    }
+    if (env_td >= 1 && env_td <= 4) td = uint32_t(env_td);
+    if (env_bd >= 1 && env_bd <= 5) bd = uint32_t(env_bd);
     k_ccd_sweep<<<m, CCD_THREADS, 0, s>>>(b, shapes, hull, ids, par, n, world_off, world_of, suppressed, nsuppressed,
-                                          dt, clamp, status, tree_rec, tree_leaf, tree_m, unb, nunb);
+                                          dt, clamp, status, tree_rec, tree_leaf, tree_m, unb, nunb, td | (bd << 8));
 }
 
 void launch_ccd_apply(const BodyDev& b, const uint32_t* ids, const float* clamp, uint32_t m, float dt, cudaStream_t s) {
