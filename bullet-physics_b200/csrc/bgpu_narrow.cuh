@@ -369,17 +369,27 @@ struct Closest {
     V3 v, pb;
 };
 
-// gjk.rs:479-499
-__device__ __forceinline__ Closest reduce_triangle(SV* buf, int& n) {
-    SV a = buf[2], b = buf[1], c = buf[0];
+// The GJK simplex is four named points B0..B3 (B0 oldest; the array form buf[i] of the
+// reference maps to Bi): with constant indices only, it stays in registers through the loop.
+
+// gjk.rs:479-499: the closest point of triangle (a, b, c) = (B2, B1, B0); the points with a
+// positive barycentric weight are kept, in the order a, b, c, as B0, B1, ...
+__device__ __forceinline__ Closest reduce_triangle(SV& B0, SV& B1, SV& B2, int& n) {
+    const SV a = B2, b = B1, c = B0;
     float w[3];
-    V3 v = closest_triangle_bary(a, b, c, w);
-    SV src[3] = {a, b, c};
-    SV kept[3] = {a, a, a};
-    int k = 0;
-    for (int i = 0; i < 3; ++i) if (w[i] > 0.0f) kept[k++] = src[i];
-    if (k == 0) { k = 1; kept[0] = a; }
-    for (int i = 0; i < k; ++i) buf[i] = kept[i];
+    const V3 v = closest_triangle_bary(a, b, c, w);
+    const bool fa = w[0] > 0.0f, fb = w[1] > 0.0f, fc = w[2] > 0.0f;
+    int k = int(fa) + int(fb) + int(fc);
+    if (k == 0) {
+        k = 1;
+        B0 = a;
+    } else {
+        const SV k0 = fa ? a : (fb ? b : c);
+        const SV k1 = fa ? (fb ? b : c) : c;
+        B0 = k0;
+        if (k > 1) B1 = k1;
+        if (k > 2) B2 = c;
+    }
     n = k;
     Closest r;
     r.inside = false;
@@ -388,55 +398,72 @@ __device__ __forceinline__ Closest reduce_triangle(SV* buf, int& n) {
     return r;
 }
 
+// gjk.rs:354-567, four coplanar points (a, b, c, d) = (B3, B2, B1, B0): the closest of the
+// four faces. Rarely taken, so a call of its own; its kept points come back by value.
+struct CoplanarReduced {
+    SV k[3];
+    int n;
+    Closest r;
+};
+
+static __device__ __noinline__ CoplanarReduced gjk_reduce_coplanar(SV a, SV b, SV c, SV d, SV first) {
+    SV faces[4][3] = {{a, b, c}, {a, b, d}, {a, c, d}, {b, c, d}};
+    int bf = 0;
+    float bw[3];
+    V3 bv = closest_triangle_bary(faces[0][0], faces[0][1], faces[0][2], bw);
+    float best_v2 = INFINITY;
+    for (int f = 1; f < 4; ++f) {
+        float cw[3];
+        V3 cv = closest_triangle_bary(faces[f][0], faces[f][1], faces[f][2], cw);
+        float v2 = len2(cv);
+        if (v2 < best_v2) { best_v2 = v2; bv = cv; bw[0] = cw[0]; bw[1] = cw[1]; bw[2] = cw[2]; bf = f; }
+    }
+    CoplanarReduced out;
+    out.k[0] = out.k[1] = out.k[2] = first;
+    int k = 0;
+    for (int i = 0; i < 3; ++i) if (bw[i] > 0.0f) out.k[k++] = faces[bf][i];
+    if (k == 0) { k = 1; out.k[0] = faces[bf][0]; }
+    out.n = k;
+    out.r.inside = false;
+    out.r.v = bv;
+    out.r.pb = faces[bf][0].pb * bw[0] + faces[bf][1].pb * bw[1] + faces[bf][2].pb * bw[2];
+    return out;
+}
+
 // gjk.rs:354-567
-static __device__ __noinline__ Closest gjk_reduce(SV* buf, int& n) {
+__device__ __forceinline__ Closest gjk_reduce(SV& B0, SV& B1, SV& B2, SV& B3, int& n) {
     Closest r;
     r.inside = false;
-    if (n == 1) { r.v = buf[0].w; r.pb = buf[0].pb; return r; }
+    if (n == 1) { r.v = B0.w; r.pb = B0.pb; return r; }
     if (n == 2) {  // gjk.rs:366-394
-        SV a = buf[1], b = buf[0];
+        const SV a = B1, b = B0;
         V3 ab = b.w - a.w;
         float denom = len2(ab);
-        if (denom < 1e-24f) { n = 1; buf[0] = a; r.v = a.w; r.pb = a.pb; return r; }
+        if (denom < 1e-24f) { n = 1; B0 = a; r.v = a.w; r.pb = a.pb; return r; }
         float t = -dot(a.w, ab) / denom;
-        if (t <= 0.0f) { n = 1; buf[0] = a; r.v = a.w; r.pb = a.pb; }
-        else if (t >= 1.0f) { n = 1; buf[0] = b; r.v = b.w; r.pb = b.pb; }
-        else { n = 2; buf[0] = a; buf[1] = b; r.v = a.w + ab * t; r.pb = a.pb + (b.pb - a.pb) * t; }
+        if (t <= 0.0f) { n = 1; B0 = a; r.v = a.w; r.pb = a.pb; }
+        else if (t >= 1.0f) { n = 1; B0 = b; r.v = b.w; r.pb = b.pb; }
+        else { n = 2; B0 = a; B1 = b; r.v = a.w + ab * t; r.pb = a.pb + (b.pb - a.pb) * t; }
         return r;
     }
-    if (n == 3) return reduce_triangle(buf, n);
-    SV a = buf[3], b = buf[2], c = buf[1], d = buf[0];
+    if (n == 3) return reduce_triangle(B0, B1, B2, n);
+    const SV a = B3, b = B2, c = B1, d = B0;
     V3 ab = b.w - a.w, ac = c.w - a.w, ad = d.w - a.w;
     if (fabsf(dot(cross(ab, ac), ad)) < 1e-12f) {
-        SV faces[4][3] = {{a, b, c}, {a, b, d}, {a, c, d}, {b, c, d}};
-        int bf = 0;
-        float bw[3];
-        V3 bv = closest_triangle_bary(faces[0][0], faces[0][1], faces[0][2], bw);
-        float best_v2 = INFINITY;
-        for (int f = 1; f < 4; ++f) {
-            float cw[3];
-            V3 cv = closest_triangle_bary(faces[f][0], faces[f][1], faces[f][2], cw);
-            float v2 = len2(cv);
-            if (v2 < best_v2) { best_v2 = v2; bv = cv; bw[0] = cw[0]; bw[1] = cw[1]; bw[2] = cw[2]; bf = f; }
-        }
-        SV kept[3] = {buf[0], buf[0], buf[0]};
-        int k = 0;
-        for (int i = 0; i < 3; ++i) if (bw[i] > 0.0f) kept[k++] = faces[bf][i];
-        if (k == 0) { k = 1; kept[0] = faces[bf][0]; }
-        V3 pbv = faces[bf][0].pb * bw[0] + faces[bf][1].pb * bw[1] + faces[bf][2].pb * bw[2];
-        for (int i = 0; i < k; ++i) buf[i] = kept[i];
-        n = k;
-        r.v = bv;
-        r.pb = pbv;
-        return r;
+        const CoplanarReduced cr = gjk_reduce_coplanar(a, b, c, d, B0);
+        B0 = cr.k[0];
+        if (cr.n > 1) B1 = cr.k[1];
+        if (cr.n > 2) B2 = cr.k[2];
+        n = cr.n;
+        return cr.r;
     }
     V3 abc = cross(ab, ac), acd = cross(ac, ad), adb = cross(ad, ab);
     V3 ao = -a.w, bo = -b.w;
     V3 bcd = cross(c.w - b.w, d.w - b.w);
-    if (dot(abc, ao) * dot(abc, ad) < 0.0f) { buf[0] = c; buf[1] = b; buf[2] = a; n = 3; return reduce_triangle(buf, n); }
-    if (dot(acd, ao) * dot(acd, ab) < 0.0f) { buf[0] = d; buf[1] = c; buf[2] = a; n = 3; return reduce_triangle(buf, n); }
-    if (dot(adb, ao) * dot(adb, ac) < 0.0f) { buf[0] = b; buf[1] = d; buf[2] = a; n = 3; return reduce_triangle(buf, n); }
-    if (dot(bcd, bo) * dot(bcd, a.w - b.w) < 0.0f) { buf[0] = d; buf[1] = c; buf[2] = b; n = 3; return reduce_triangle(buf, n); }
+    if (dot(abc, ao) * dot(abc, ad) < 0.0f) { B0 = c; B1 = b; B2 = a; n = 3; return reduce_triangle(B0, B1, B2, n); }
+    if (dot(acd, ao) * dot(acd, ab) < 0.0f) { B0 = d; B1 = c; B2 = a; n = 3; return reduce_triangle(B0, B1, B2, n); }
+    if (dot(adb, ao) * dot(adb, ac) < 0.0f) { B0 = b; B1 = d; B2 = a; n = 3; return reduce_triangle(B0, B1, B2, n); }
+    if (dot(bcd, bo) * dot(bcd, a.w - b.w) < 0.0f) { B0 = d; B1 = c; B2 = b; n = 3; return reduce_triangle(B0, B1, B2, n); }
     r.inside = true;
     return r;
 }
@@ -568,17 +595,20 @@ static __device__ __noinline__ GjkResult gjk_contact(const ConvexPair& cp, bool 
     V3 fallback = len2(cdir) > 1e-12f ? cdir : V3{1.f, 0.f, 0.f};
     V3 init = (has_seed && len2(seed) > 1e-12f) ? seed : fallback;
     SV first = cp.support(init);
-    SV buf[4] = {first, first, first, first};
+    SV B0 = first, B1 = first, B2 = first, B3 = first;
     int n = 1;
     V3 dir = -first.w;
     float touch2 = TOUCH2 * fmaxf(len2(first.w), 1.0f);
     GjkResult out;
     out.kind = 0;
     for (int it = 0; it < 64; ++it) {
-        Closest cl = gjk_reduce(buf, n);
+        Closest cl = gjk_reduce(B0, B1, B2, B3, n);
         if (cl.inside) {
             out.kind = 2;
-            for (int i = 0; i < 4; ++i) out.simplex[i] = buf[i].w;
+            out.simplex[0] = B0.w;
+            out.simplex[1] = B1.w;
+            out.simplex[2] = B2.w;
+            out.simplex[3] = B3.w;
             return out;
         }
         V3 v = cl.v;
@@ -598,8 +628,10 @@ static __device__ __noinline__ GjkResult gjk_contact(const ConvexPair& cp, bool 
         float delta = dot(v, w.w);
         float band = msum + thr;
         if (delta > 0.0f && delta * delta > v2 * band * band) { out.kind = 0; return out; }
-        bool dup = false;
-        for (int i = 0; i < n; ++i) if (absdiff_le(w.w, buf[i].w, 1e-6f)) dup = true;
+        bool dup = absdiff_le(w.w, B0.w, 1e-6f);
+        if (n > 1 && absdiff_le(w.w, B1.w, 1e-6f)) dup = true;
+        if (n > 2 && absdiff_le(w.w, B2.w, 1e-6f)) dup = true;
+        if (n > 3 && absdiff_le(w.w, B3.w, 1e-6f)) dup = true;
         if (dup || delta >= v2 * (1.0f - REL2)) {
             float cd = sqrtf(v2);
             float distance = cd - msum;
@@ -614,7 +646,9 @@ static __device__ __noinline__ GjkResult gjk_contact(const ConvexPair& cp, bool 
             out.kind = 0;
             return out;
         }
-        buf[n] = w;
+        if (n == 1) B1 = w;
+        else if (n == 2) B2 = w;
+        else B3 = w;
         ++n;
     }
     out.kind = 0;
