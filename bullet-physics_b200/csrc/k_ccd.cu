@@ -418,26 +418,30 @@ __device__ __forceinline__ void replay_bisect(float& l, float& h, uint32_t node)
     }
 }
 
-// td / bd: levels of the ternary / bisection decision tree evaluated per round (td <= 4: 2 (2^td
-// - 1) probes; bd <= 5: 2^bd - 1 probes). Deeper trees take fewer rounds but more probes.
-__device__ bool sweep_convex_warp(V3 from, V3 dir, float length, const Inflated& t, float& fraction, uint32_t td,
-                                  uint32_t bd) {
-    const uint32_t lane = threadIdx.x & 31u;
+// td / bd: levels of the ternary / bisection decision tree evaluated per round (td levels:
+// 2 (2^td - 1) probes; bd levels: 2^bd - 1 probes), on a segment of g lanes (the warp split into
+// 32 / g segments that search side by side, each its own target; 2 (2^td - 1) <= g and
+// 2^bd - 1 <= g). Every lane of the warp calls this with the same g, td and bd; the control flow
+// is uniform across the warp (a segment whose closest approach misses still runs the bisection
+// rounds if another segment's hits, and ignores them).
+__device__ bool sweep_convex_seg(V3 from, V3 dir, float length, const Inflated& t, float& fraction, uint32_t td,
+                                 uint32_t bd, uint32_t g) {
+    const uint32_t sl = (threadIdx.x & 31u) % g;  // lane within the segment
     float lo = 0.0f, hi = 1.0f;
     for (uint32_t done = 0; done < 40;) {  // 40 ternary steps
         const uint32_t depth = min(td, 40u - done);
         const uint32_t probes = 2u * ((1u << depth) - 1u);
         float v = 0.0f;
-        if (lane < probes) {
+        if (sl < probes) {
             float l = lo, h = hi;
-            replay_ternary(l, h, lane >> 1);
-            const float m = (lane & 1u) ? h - (h - l) / 3.0f : l + (h - l) / 3.0f;
+            replay_ternary(l, h, sl >> 1);
+            const float m = (sl & 1u) ? h - (h - l) / 3.0f : l + (h - l) / 3.0f;
             v = point_distance2(t, from + dir * (m * length));
         }
         uint32_t n = 0;
         for (uint32_t d = 0; d < depth; ++d) {
-            const float d1 = __shfl_sync(0xffffffffu, v, int(2 * n));
-            const float d2 = __shfl_sync(0xffffffffu, v, int(2 * n + 1));
+            const float d1 = __shfl_sync(0xffffffffu, v, int(2 * n), int(g));
+            const float d2 = __shfl_sync(0xffffffffu, v, int(2 * n + 1), int(g));
             const float m1 = lo + (hi - lo) / 3.0f;
             const float m2 = hi - (hi - lo) / 3.0f;
             if (d1 < d2) { hi = m2; n = 2 * n + 1; }
@@ -446,19 +450,20 @@ __device__ bool sweep_convex_warp(V3 from, V3 dir, float length, const Inflated&
         done += depth;
     }
     const float s_min = (lo + hi) * 0.5f;
-    if (point_distance2(t, from + dir * (s_min * length)) > 1e-8f) return false;
+    const bool hit = !(point_distance2(t, from + dir * (s_min * length)) > 1e-8f);
+    if (!__any_sync(0xffffffffu, hit)) return false;
     float low = 0.0f, high = s_min;
     for (uint32_t done = 0; done < 60;) {  // 60 bisection steps
         const uint32_t depth = min(bd, 60u - done);
         float v = 0.0f;
-        if (lane < (1u << depth) - 1u) {
+        if (sl < (1u << depth) - 1u) {
             float l = low, h = high;
-            replay_bisect(l, h, lane);
+            replay_bisect(l, h, sl);
             v = point_distance2(t, from + dir * (((l + h) * 0.5f) * length));
         }
         uint32_t n = 0;
         for (uint32_t d = 0; d < depth; ++d) {
-            const float dm = __shfl_sync(0xffffffffu, v, int(n));
+            const float dm = __shfl_sync(0xffffffffu, v, int(n), int(g));
             const float mid = (low + high) * 0.5f;
             if (dm <= 1e-8f) { high = mid; n = 2 * n + 1; }
             else { low = mid; n = 2 * n + 2; }
@@ -466,11 +471,11 @@ __device__ bool sweep_convex_warp(V3 from, V3 dir, float length, const Inflated&
         done += depth;
     }
     fraction = (low + high) * 0.5f;
-    return true;
+    return hit;
 }
 
 // cast_one for the whole warp (every lane returns the fraction): convex targets through
-// sweep_convex_warp; planes and meshes by lane 0, broadcast.
+// sweep_convex_seg on the whole warp; planes and meshes by lane 0, broadcast.
 __device__ __forceinline__ float cast_warp(const BodyDev& b, const Shape* __restrict__ shapes, const float4* __restrict__ hull,
                                            const CcdCtx& c, uint32_t j, uint32_t td, uint32_t bd) {
     const Shape& sj = shapes[b.info[j].x];
@@ -481,7 +486,7 @@ __device__ __forceinline__ float cast_warp(const BodyDev& b, const Shape* __rest
     }
     Inflated t{sj, from4(b.pos[j]), q4(b.quat[j]), c.radius, hull};
     float f;
-    return sweep_convex_warp(c.from, c.dir, c.length, t, f, td, bd) ? f : 1.0f;
+    return sweep_convex_seg(c.from, c.dir, c.length, t, f, td, bd, 32u) ? f : 1.0f;
 }
 
 __device__ __forceinline__ float warp_min(float v) {
@@ -657,11 +662,32 @@ __global__ void __launch_bounds__(CCD_THREADS) k_ccd_sweep(BodyDev b, const Shap
         __syncthreads();
         // Few candidates: one at a time with the whole warp (23 probe latencies a cast); many:
         // a candidate per lane (141 probe latencies for up to 32 casts).
+        // Up to 4 candidates whose bounds are below best side by side, one warp segment each (the
+        // extra casts cannot lower best below the sequential result: a cast's fraction is never
+        // below its bound), with shallower trees the narrower the segment.
         uint32_t s0 = 0;
         while (s0 < nc && nc - s0 <= CCD_WARP_CAST_MAX) {
             if (!(slb[s0] < best)) break;  // every later candidate hits no sooner than best
-            best = fminf(best, cast_warp(b, shapes, hull, c, sorted[s0], depths & 0xffu, depths >> 8));
-            ++s0;
+            uint32_t r = 1;
+            bool mesh = shapes[b.info[sorted[s0]].x].type == SHAPE_MESH;
+            while (r < 4 && s0 + r < nc && slb[s0 + r] < best) {
+                mesh = mesh || shapes[b.info[sorted[s0 + r]].x].type == SHAPE_MESH;
+                ++r;
+            }
+            if (mesh || r == 1) {
+                best = fminf(best, cast_warp(b, shapes, hull, c, sorted[s0], depths & 0xffu, depths >> 8));
+                ++s0;
+                continue;
+            }
+            const uint32_t g = r >= 4 ? 8u : 16u, segs = 32u / g, use = min(segs, r);
+            const uint32_t seg = lane / g;
+            const uint32_t j = sorted[s0 + (seg < use ? seg : 0u)];
+            const Shape& sj = shapes[b.info[j].x];
+            Inflated tj{sj, from4(b.pos[j]), q4(b.quat[j]), c.radius, hull};
+            float f = 1.0f;
+            const bool hitj = sweep_convex_seg(c.from, c.dir, c.length, tj, f, g == 8u ? 2u : 3u, g == 8u ? 3u : 4u, g);
+            best = fminf(best, warp_min(hitj && seg < use ? f : 1.0f));
+            s0 += use;
         }
         for (uint32_t w0 = s0; w0 < nc; w0 += CCD_THREADS) {
             if (!(slb[w0] < best)) break;
