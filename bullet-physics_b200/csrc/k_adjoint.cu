@@ -285,7 +285,8 @@ void run_adj_solve_worlds(const AdjStep& st, const WorldPlan& plan, float4* lbar
         throw CudaError{cudaErrorInvalidValue, "the batch's solver launch shape changed between forward and backward"};
     AdjArgs a{st.recs, st.off, st.end, st.ncol, st.iters, st.tab, st.sweeps, lbar, vbar, wbar, mubar, ebar, material,
               st.merge_pos, carry_in, st.row_src, carry_out, restitution_threshold, warm_factor, nullptr, status_dev};
-    k_adj_solve_worlds<<<plan.ncta, plan.block, 0, s>>>(a, plan.dev(), st.off);
+    // A plan of more than 256 threads a CTA has block-mode worlds only, which run on any block size.
+    k_adj_solve_worlds<<<plan.ncta, plan.block > 256 ? 256u : plan.block, 0, s>>>(a, plan.dev(), st.off);
     check_cuda(cudaGetLastError(), "adjoint world solve launch");
 }
 

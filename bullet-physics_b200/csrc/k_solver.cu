@@ -1533,9 +1533,12 @@ __device__ void solve_world(const WorldSolveArgs& A, uint32_t w, uint32_t lane, 
     }
 }
 
-__global__ void __launch_bounds__(256) k_world_solve(WorldSolveArgs A) {
+// MAXT: the launch's largest block. Plans of up to 256 threads a CTA mix block and warp modes;
+// the 512-thread build runs only plans whose worlds are all in block mode (one large world).
+template <int MAXT>
+__global__ void __launch_bounds__(MAXT) k_world_solve(WorldSolveArgs A) {
     extern __shared__ float4 ws_dyn[];
-    __shared__ WorldCtx ctx[WS_MAX_WARPS];
+    __shared__ WorldCtx ctx[MAXT > 256 ? 1 : WS_MAX_WARPS];
     const uint2 c = A.plan.cta[blockIdx.x];
     const bool block_mode = (c.y >> 31) != 0u;
     const uint32_t count = c.y & 0x7fffffffu;
@@ -1543,6 +1546,7 @@ __global__ void __launch_bounds__(256) k_world_solve(WorldSolveArgs A) {
         solve_world<false>(A, A.plan.list[c.x], threadIdx.x, blockDim.x, ws_dyn, ctx[0]);
         return;
     }
+    if (MAXT > 256) return;  // the plan builder gives this build block-mode plans only
     const uint32_t wi = threadIdx.x >> 5;
     if (wi >= count) return;  // warp mode: warps never sync with each other
     uint32_t off = 0;
@@ -1834,7 +1838,8 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
 bool build_world_plan(const std::vector<uint32_t>& world_off, uint32_t block, uint32_t tau, WorldPlan& plan,
                       cudaStream_t s) {
     plan.valid = false;
-    if (block < 32 || block > 32 * WS_MAX_WARPS || block % 32) return false;
+    // Up to 256 threads a CTA; 512 when every world runs in block mode (tau 0).
+    if (block < 32 || block > (tau == 0 ? 512u : 32u * WS_MAX_WARPS) || block % 32) return false;
     const uint32_t nw = world_off.empty() ? 0u : uint32_t(world_off.size() - 1);
     std::vector<uint32_t> order(nw);
     for (uint32_t k = 0; k < nw; ++k) order[k] = k;
@@ -1872,8 +1877,8 @@ bool build_world_plan(const std::vector<uint32_t>& world_off, uint32_t block, ui
     if (nw) check_cuda(cudaMemcpyAsync(plan.list.p, order.data(), nw * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "h2d");
     check_cuda(cudaStreamSynchronize(s), "sync");  // the host vectors go out of scope
     // Without this opt-in, dynamic shared memory is limited to 48 KB minus the kernel's static part.
-    check_cuda(cudaFuncSetAttribute((const void*)k_world_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    int(smem)), "smem attribute");
+    check_cuda(cudaFuncSetAttribute(block > 256 ? (const void*)k_world_solve<512> : (const void*)k_world_solve<256>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem attribute");
     plan.ncta = uint32_t(cta.size());
     plan.block = block;
     plan.tau = tau;
@@ -1936,7 +1941,8 @@ void run_world_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs
     A.push_ang = w.b.push_ang;
     A.status = status_dev;
     A.plan = plan.dev();
-    k_world_solve<<<plan.ncta, plan.block, plan.smem, s>>>(A);
+    if (plan.block > 256) k_world_solve<512><<<plan.ncta, plan.block, plan.smem, s>>>(A);
+    else k_world_solve<256><<<plan.ncta, plan.block, plan.smem, s>>>(A);
     check_cuda(cudaGetLastError(), "world solve launch");
     mark(6);
 }

@@ -149,6 +149,7 @@ struct World {
     DevBuf<uint32_t> wcol;
     DevBuf<uint32_t> plain_off_d;    // a plain world's {0, n}, for the per-world solver
     static constexpr uint32_t PLAIN_WORLD_SOLVER_MAX_BODIES = 2048;
+    static constexpr uint32_t PLAIN_WORLD_SOLVER_THREADS = 512;
     bool last_world_solver = false;  // the last step ran the per-world solver
     float tuned_ms = 0.0f, tuned_global_ms = 0.0f;
     uint32_t tuned_candidates = 0;
@@ -574,14 +575,15 @@ struct World {
         wplan.valid = false;
         if (!batch) {
             // A plain world small enough for one CTA's shared memory is solved as a batch of one
-            // world (one CTA of 256 threads, velocities in shared memory, block-local syncs).
+            // world (one CTA of PLAIN_WORLD_SOLVER_THREADS threads, velocities in shared memory,
+            // block-local syncs).
             if (n == 0 || n > PLAIN_WORLD_SOLVER_MAX_BODIES) return;
             const std::vector<uint32_t> off{0u, n};
             plain_off_d.reserve(2);
             check_cuda(cudaMemcpyAsync(plain_off_d.p, off.data(), 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, stream),
                        "h2d");
             wcol.reserve(WS_STRIDE + 1);
-            build_world_plan(off, 256u, 0u, wplan, stream);
+            build_world_plan(off, PLAIN_WORLD_SOLVER_THREADS, 0u, wplan, stream);
             return;
         }
         if (wplan_block == 0) return;
