@@ -148,7 +148,7 @@ struct World {
     uint32_t wplan_block = 128, wplan_tau = 64;  // 0 threads: the global (all-worlds) solver
     DevBuf<uint32_t> wcol;
     DevBuf<uint32_t> plain_off_d;    // a plain world's {0, n}, for the per-world solver
-    static constexpr uint32_t PLAIN_WORLD_SOLVER_MAX_BODIES = 2048;
+    static constexpr uint32_t PLAIN_WORLD_SOLVER_MAX_BODIES = 1024;
     static constexpr uint32_t PLAIN_WORLD_SOLVER_THREADS = 512;
     bool last_world_solver = false;  // the last step ran the per-world solver
     float tuned_ms = 0.0f, tuned_global_ms = 0.0f;

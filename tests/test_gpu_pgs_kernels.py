@@ -1,6 +1,6 @@
 """The two PGS kernels for worlds without joints give the same trajectory, bit for bit.
 
-A plain world of more than 2,048 bodies without joints is solved by the chunked kernel
+A plain world of more than 1,024 bodies without joints is solved by the chunked kernel
 (Morton-ordered chunks, neighbour waits); BGPU_PGS=team in the environment selects the
 team-barrier kernel instead (read once per process, so each runs in a child process). Both
 solve the groups in the same (colour, pair) order, so the states after every step must be
