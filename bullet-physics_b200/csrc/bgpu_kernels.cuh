@@ -512,7 +512,7 @@ bool build_world_plan(const std::vector<uint32_t>& world_off, uint32_t block, ui
 void run_world_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
                       uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark,
                       const uint32_t* world_off, uint32_t nworlds, const WorldPlan& plan, uint32_t* wcol,
-                      const JointsDev* joints = nullptr);
+                      const JointsDev* joints = nullptr, bool seed_colours = false);
 // One team barrier that nothing completes (2 blocks): the wait gives up after limit_ns and
 // leaves ST_BARRIER_TIMEOUT in *status. ctr and status are device words the caller zeroes.
 void run_wait_selftest(unsigned long long limit_ns, unsigned int* ctr, uint32_t* status, cudaStream_t s);

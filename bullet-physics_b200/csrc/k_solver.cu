@@ -1306,6 +1306,8 @@ struct WorldSolveArgs {
     float4* push_ang;
     uint32_t* status;
     WorldPlanDev plan;
+    float4* entries;                   // the pairs' new manifolds: their meta bits carry the colour
+    uint32_t seed;                     // nonzero: start from the colours the manifolds carry
 };
 
 struct WorldCtx {  // per world being solved by a CTA or a warp
@@ -1362,12 +1364,14 @@ __device__ void solve_world(const WorldSolveArgs& A, uint32_t w, uint32_t lane, 
     unsigned long long* mask = reinterpret_cast<unsigned long long*>(plin);
     unsigned long long* best0 = mask + nb;
     unsigned long long* best1 = best0 + nb;
+    unsigned long long* dup = best1 + nb;  // seeded colours claimed twice at a body
     for (uint32_t i = lane; i < nb; i += nt) {
         lin[i] = __ldcg(&A.linvel[b0 + i]);
         ang[i] = __ldcg(&A.angvel[b0 + i]);
         mask[i] = 0ull;
         best0[i] = 0ull;
         best1[i] = 0ull;
+        dup[i] = 0ull;
     }
     if (lane == 0) {
         const uint32_t K = *A.ngroups;
@@ -1394,7 +1398,42 @@ __device__ void solve_world(const WorldSolveArgs& A, uint32_t w, uint32_t lane, 
     // 1. Jones-Plassmann rounds: an uncoloured group wins when its priority is the largest
     //    among the uncoloured groups at each of its dynamic bodies; a winner takes the lowest
     //    colour free at both bodies (winners of one round share no dynamic body).
-    for (uint32_t g = g0 + lane; g < g1; g += nt) A.colour[g] = NO_COLOUR;
+    auto seed_of = [&](uint32_t g) -> uint32_t {  // last step's colour + 1 (0: none)
+        const uint32_t cs =
+            (__float_as_uint(A.entries[size_t(A.contact_pairs[g]) * ENTRY_F4 + 2].w) >> META_COLOUR_SHIFT) & 0xffu;
+        return cs <= WS_MAX_COLOURS ? cs : 0u;
+    };
+    if (A.seed) {
+        //    Seeds: each group claims last step's colour at its dynamic bodies; a group keeps it
+        //    when no other group claimed the same colour at either body. The others are coloured
+        //    by the rounds below, first fit around every claimed colour.
+        for (uint32_t g = g0 + lane; g < g1; g += nt) {
+            const uint32_t cs = seed_of(g);
+            if (cs == 0u) continue;
+            const unsigned long long bit = 1ull << (cs - 1u);
+            const uint64_t key = A.pairs[A.contact_pairs[g]];
+            const uint32_t ia = key_lo(key), ib = key_hi(key);
+            if (dyn(ia) && (atomicOr(&mask[ia - b0], bit) & bit)) atomicOr(&dup[ia - b0], bit);
+            if (dyn(ib) && (atomicOr(&mask[ib - b0], bit) & bit)) atomicOr(&dup[ib - b0], bit);
+        }
+        ws_sync<WARP>();
+        uint32_t kept = 0;
+        for (uint32_t g = g0 + lane; g < g1; g += nt) {
+            const uint32_t cs = seed_of(g);
+            bool keep = false;
+            if (cs != 0u) {
+                const unsigned long long bit = 1ull << (cs - 1u);
+                const uint64_t key = A.pairs[A.contact_pairs[g]];
+                const uint32_t ia = key_lo(key), ib = key_hi(key);
+                keep = !(dyn(ia) && (dup[ia - b0] & bit)) && !(dyn(ib) && (dup[ib - b0] & bit));
+            }
+            A.colour[g] = keep ? cs - 1u : NO_COLOUR;
+            kept += keep ? 1u : 0u;
+        }
+        if (kept) atomicSub(&C.left, kept);
+    } else {
+        for (uint32_t g = g0 + lane; g < g1; g += nt) A.colour[g] = NO_COLOUR;
+    }
     ws_sync<WARP>();
     for (uint32_t r = 0; C.left != 0; ++r) {
         if (r >= MAX_ROUNDS) {
@@ -1471,6 +1510,9 @@ __device__ void solve_world(const WorldSolveArgs& A, uint32_t w, uint32_t lane, 
         uint32_t nsplit = 0;
         for (uint32_t k = 0; k < cnt; ++k) nsplit += a.rows[(size_t(p) * 4 + k) * ROW_F4 + 5].z != 0.0f ? 1u : 0u;
         A.recs[slot] = make_uint4(key_lo(key), key_hi(key), p | (cnt << 29), nsplit ? 1u : 0u);
+        // The colour rides in the manifold's meta bits to seed next step's colouring.
+        float* mw = &A.entries[size_t(p) * ENTRY_F4 + 2].w;
+        *mw = __uint_as_float((__float_as_uint(*mw) & ~(0xffu << META_COLOUR_SHIFT)) | ((c + 1u) << META_COLOUR_SHIFT));
         my_rows += cnt;
         if (nsplit) {
             ++my_split_groups;
@@ -1890,7 +1932,7 @@ bool build_world_plan(const std::vector<uint32_t>& world_off, uint32_t block, ui
 void run_world_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, PairData& pd, const StepParams& sp,
                       uint32_t* status_dev, cudaStream_t s, const std::function<void(int)>& mark,
                       const uint32_t* world_off, uint32_t nworlds, const WorldPlan& plan, uint32_t* wcol,
-                      const JointsDev* joints) {
+                      const JointsDev* joints, bool seed_colours) {
     const bool with_joints = joints && joints->n && joints->ncol;
     check_cuda(cudaMemsetAsync(pd.scalars.p + 2, 0, 4 * sizeof(uint32_t), s), "memset");
     check_cuda(cudaMemsetAsync(pd.scalars.p + 10, 0, 2 * sizeof(uint32_t), s), "memset");
@@ -1941,6 +1983,8 @@ void run_world_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs
     A.push_ang = w.b.push_ang;
     A.status = status_dev;
     A.plan = plan.dev();
+    A.entries = pd.entries.p;
+    A.seed = seed_colours ? 1u : 0u;
     if (plan.block > 256) k_world_solve<512><<<plan.ncta, plan.block, plan.smem, s>>>(A);
     else k_world_solve<256><<<plan.ncta, plan.block, plan.smem, s>>>(A);
     check_cuda(cudaGetLastError(), "world solve launch");

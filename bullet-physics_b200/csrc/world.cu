@@ -924,7 +924,8 @@ struct World {
         last_world_solver = use_world_solver();
         if (last_world_solver)
             run_world_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); },
-                             world_offsets_dev(), nw, wplan, wcol.p, batch ? nullptr : &jd);
+                             world_offsets_dev(), nw, wplan, wcol.p, batch ? nullptr : &jd,
+                             step_count % RECOLOUR_PERIOD != 0);
         else
             run_solver(wv, pairs.p, npairs, pd, sp, status, stream, [&](int k) { mark(k); },
                        step_count % RECOLOUR_PERIOD != 0, &jd, batch ? nullptr : bp.leaf_body.p,
