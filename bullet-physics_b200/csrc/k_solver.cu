@@ -1685,6 +1685,16 @@ __global__ void k_wait_selftest(unsigned int* ctr, uint32_t* status, unsigned lo
     team_barrier(ctr, gridDim.x + 1u, status, limit_ns);
 }
 
+int device_sms() {
+    static int sms = -1;
+    if (sms < 0) {
+        int dev = 0;
+        check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+        check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "sm count");
+    }
+    return sms;
+}
+
 int coop_grid(const void* fn, int block, size_t smem) {
     static int sms = -1;
     if (sms < 0) {
@@ -1788,8 +1798,10 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
     check_cuda(cudaMemsetAsync(pd.barrier.p, 0, 16 * sizeof(unsigned int), s), "memset barrier");
     ColourArgs ca{pd.scalars.p + 2, pd.contact_pairs.p, pairs, w.b.iw, pd.colour.p, pd.body_prio.p, pd.body_mask.p,
                   pd.body_dup.p, pd.entries.p, seed_colours ? 1u : 0u, pd.barrier.p, status_dev};
+    // Two blocks per SM: enough threads for a pile's groups, and the rounds' grid barriers
+    // are cheaper than with every block the SM could hold.
     static int colour_grid = 0;
-    if (!colour_grid) colour_grid = coop_grid((const void*)k_colour, TB, 0);
+    if (!colour_grid) colour_grid = std::min(coop_grid((const void*)k_colour, TB, 0), 2 * device_sms());
     pd.colour_work.reserve(2 * size_t(npairs) + 2);
     JpList wl{{pd.colour_work.p, pd.colour_work.p + npairs}, {pd.barrier.p + 6, pd.barrier.p + 7}};
     void* cargs[] = {&ca, &wl};
