@@ -291,10 +291,19 @@ __global__ void k_colour(ColourArgs a, JpList wl) {
 
 // Colour histograms of all groups and of the groups with split-active rows,
 // plus the row and split-row totals.
+// With chunk histograms (vhist non-null) the pass also counts each group into its (colour,
+// chunk) bins and records its touch sets (chunk_count, with the chunked PGS's code below).
+__device__ __forceinline__ void chunk_count(const uint64_t* __restrict__ pairs, uint32_t p, uint32_t c, uint32_t rows,
+                                            bool split, const float4* __restrict__ iw,
+                                            const uint32_t* __restrict__ chunk_of, uint32_t P, uint32_t* vhist,
+                                            uint32_t* shist, uint32_t* touch, uint32_t* all_flag);
+
 __global__ void k_colour_hist(const uint32_t* __restrict__ count, const uint32_t* __restrict__ contact_pairs,
                               const uint32_t* __restrict__ colour, const uint32_t* __restrict__ row_count,
                               const float4* __restrict__ rows, uint32_t* hist, uint32_t* split_hist, uint32_t* split_flag,
-                              uint32_t* sub_hist) {
+                              uint32_t* sub_hist, const uint64_t* __restrict__ pairs, const float4* __restrict__ iw,
+                              const uint32_t* __restrict__ chunk_of, uint32_t P, uint32_t* vhist, uint32_t* shist,
+                              uint32_t* touch, uint32_t* all_flag) {
     // Block-local histograms; [MAX_COLOURS] rows, [MAX_COLOURS + 1] split-active rows;
     // shc: groups per (colour, row count - 1).
     __shared__ uint32_t sh[MAX_COLOURS + 2], ssh[MAX_COLOURS], shc[MAX_COLOURS * 4];
@@ -322,6 +331,7 @@ __global__ void k_colour_hist(const uint32_t* __restrict__ count, const uint32_t
             nsplit_rows += nsr;
             atomicAdd(&ssh[c], 1u);
         }
+        if (vhist) chunk_count(pairs, p, c, n, nsr != 0u, iw, chunk_of, P, vhist, shist, touch, all_flag);
     }
     nrows = __reduce_add_sync(0xffffffffu, nrows);
     nsplit_rows = __reduce_add_sync(0xffffffffu, nsplit_rows);
@@ -343,47 +353,81 @@ __global__ void k_colour_hist(const uint32_t* __restrict__ count, const uint32_t
 }
 
 // Offsets of the colour batches; scalars [3] rows [4] colours [5] split groups
-// [10] split rows [11] largest split batch.
+// [10] split rows [11] largest split batch. One warp, four raw colours a lane.
+// Colours without groups are dropped (remap: colour -> dense colour), batches start on
+// multiples of 32 (one warp's slots never straddle two batches), so a batch's start is the sum
+// of the earlier batches' sizes rounded up to 32. Inside a batch the groups with 4 rows come
+// first, then 3, 2, 1 (sub_cursor: the scatter's cursor of each part), so most warps hold
+// groups of one size: their lanes run the same number of contacts and read the table's contact
+// planes without gaps. The split batches keep their cursors; after the scatter they hold the
+// split batch ends. (chunked: the scatter takes per-(colour, chunk) cursors, so the batch ends
+// are written here.)
 __global__ void k_colour_scan(uint32_t* hist, uint32_t* offset, uint32_t* cursor, uint32_t* split_hist,
                               uint32_t* split_offset, uint32_t* split_cursor, const unsigned int* bar, uint32_t* scalars,
                               uint32_t* remap, const uint32_t* sub_hist, uint32_t* sub_cursor, uint32_t chunked) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    static_assert(MAX_COLOURS == 128, "four raw colours a lane");
+    if (blockIdx.x != 0 || threadIdx.x >= 32u) return;
+    const uint32_t lane = threadIdx.x;
     const uint32_t nraw = bar[5];
-    uint32_t acc = 0, sacc = 0, smax = 0, split_groups = 0, d = 0;
-    // Colours without groups are dropped (remap: colour -> dense colour), batches start on
-    // multiples of 32 (one warp's slots never straddle two batches). Inside a batch the
-    // groups with 4 rows come first, then 3, 2, 1 (sub_cursor: the scatter's cursor of each
-    // part), so most warps hold groups of one size: their lanes run the same number of
-    // contacts and read the table's contact planes without gaps. The split batches keep
-    // their cursors; after the scatter they hold the split batch ends. (chunked: the scatter
-    // takes per-(colour, chunk) cursors, so the batch ends are written here.)
-    for (uint32_t c = 0; c < nraw; ++c) {
-        if (hist[c] == 0) continue;
+    uint32_t h[4], sh[4], cnt = 0, pad = 0, spad = 0, smax = 0, sg = 0;
+    for (uint32_t k = 0; k < 4; ++k) {
+        const uint32_t c = 4u * lane + k;
+        h[k] = c < nraw ? hist[c] : 0u;
+        sh[k] = h[k] ? split_hist[c] : 0u;
+        if (h[k]) {
+            ++cnt;
+            pad += (h[k] + 31u) & ~31u;
+            spad += (sh[k] + 31u) & ~31u;
+            smax = max(smax, sh[k]);
+            sg += sh[k];
+        }
+    }
+    uint32_t d = cnt, acc = pad, sacc = spad;  // inclusive scans, then exclusive
+    for (uint32_t o = 1; o < 32; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, d, o), y = __shfl_up_sync(0xffffffffu, acc, o),
+                       z = __shfl_up_sync(0xffffffffu, sacc, o);
+        if (lane >= o) { d += x; acc += y; sacc += z; }
+    }
+    const uint32_t ncol = __shfl_sync(0xffffffffu, d, 31);
+    d -= cnt;
+    acc -= pad;
+    sacc -= spad;
+    for (uint32_t k = 0; k < 4; ++k) {
+        if (!h[k]) continue;
+        const uint32_t c = 4u * lane + k;
         remap[c] = d;
-        acc = (acc + 31u) & ~31u;
         offset[d] = acc;
         uint32_t part = acc;
         for (uint32_t n = 4; n >= 1; --n) {
             sub_cursor[d * 4 + (n - 1)] = part;
             part += sub_hist[c * 4 + (n - 1)];
         }
-        acc += hist[c];
-        cursor[d] = acc;  // the batch end
-        sacc = (sacc + 31u) & ~31u;
+        cursor[d] = acc + h[k];  // the batch end
         split_offset[d] = sacc;
-        split_cursor[d] = chunked ? sacc + split_hist[c] : sacc;
-        sacc += split_hist[c];
-        smax = max(smax, split_hist[c]);
-        split_groups += split_hist[c];
+        split_cursor[d] = chunked ? sacc + sh[k] : sacc;
+        if (d + 1u == ncol) {  // the last batch: the ends, unpadded
+            offset[ncol] = acc + h[k];
+            split_offset[ncol] = sacc + sh[k];
+        }
+        acc += (h[k] + 31u) & ~31u;
+        sacc += (sh[k] + 31u) & ~31u;
         ++d;
     }
-    offset[d] = acc;
-    split_offset[d] = sacc;
-    scalars[3] = hist[MAX_COLOURS + 1];
-    scalars[4] = d;
-    scalars[5] = split_groups;
-    scalars[10] = hist[MAX_COLOURS + 2];
-    scalars[11] = smax;
+    for (uint32_t o = 16; o > 0; o >>= 1) {
+        smax = max(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+        sg += __shfl_xor_sync(0xffffffffu, sg, o);
+    }
+    if (lane == 0) {
+        if (ncol == 0) {
+            offset[0] = 0u;
+            split_offset[0] = 0u;
+        }
+        scalars[3] = hist[MAX_COLOURS + 1];
+        scalars[4] = ncol;
+        scalars[5] = sg;
+        scalars[10] = hist[MAX_COLOURS + 2];
+        scalars[11] = smax;
+    }
 }
 
 // One atomicAdd per distinct colour among the calling lanes of a warp.
@@ -443,25 +487,18 @@ __device__ __forceinline__ void chunk_touch(uint32_t* touch, uint32_t x, uint32_
 }
 
 // Groups per (colour, chunk, row count) and split groups per (colour, chunk), plus the
-// touch sets of the groups' dynamic bodies.
-__global__ void k_chunk_hist(const uint32_t* __restrict__ count, const uint32_t* __restrict__ contact_pairs,
-                             const uint64_t* __restrict__ pairs, const uint32_t* __restrict__ row_count,
-                             const uint32_t* __restrict__ colour, const uint32_t* __restrict__ split_flag,
-                             const float4* __restrict__ iw, const uint32_t* __restrict__ chunk_of, uint32_t P,
-                             uint32_t* vhist, uint32_t* shist, uint32_t* touch, uint32_t* all_flag) {
-    const uint32_t K = *count;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
-        const uint32_t c = colour[k];
-        if (c >= MAX_COLOURS) continue;
-        const uint32_t p = contact_pairs[k];
-        const uint64_t key = pairs[p];
-        const uint32_t ia = key_lo(key), ib = key_hi(key);
-        const uint32_t B = group_owner(ia, ib, iw, chunk_of);
-        atomicAdd(&vhist[(size_t(c) * P + B) * 4 + (row_count[p] - 1)], 1u);
-        if (split_flag[k]) atomicAdd(&shist[size_t(c) * P + B], 1u);
-        if (inv_mass_of(iw, ia) > 0.0f && chunk_of[ia] != B) chunk_touch(touch, ia, B, all_flag);
-        if (inv_mass_of(iw, ib) > 0.0f && chunk_of[ib] != B) chunk_touch(touch, ib, B, all_flag);
-    }
+// touch sets of the groups' dynamic bodies (k_colour_hist's pass, for each group).
+__device__ __forceinline__ void chunk_count(const uint64_t* __restrict__ pairs, uint32_t p, uint32_t c, uint32_t rows,
+                                            bool split, const float4* __restrict__ iw,
+                                            const uint32_t* __restrict__ chunk_of, uint32_t P, uint32_t* vhist,
+                                            uint32_t* shist, uint32_t* touch, uint32_t* all_flag) {
+    const uint64_t key = pairs[p];
+    const uint32_t ia = key_lo(key), ib = key_hi(key);
+    const uint32_t B = group_owner(ia, ib, iw, chunk_of);
+    atomicAdd(&vhist[(size_t(c) * P + B) * 4 + (rows - 1)], 1u);
+    if (split) atomicAdd(&shist[size_t(c) * P + B], 1u);
+    if (inv_mass_of(iw, ia) > 0.0f && chunk_of[ia] != B) chunk_touch(touch, ia, B, all_flag);
+    if (inv_mass_of(iw, ib) > 0.0f && chunk_of[ib] != B) chunk_touch(touch, ib, B, all_flag);
 }
 
 // One block per raw colour: the colour's batch is laid out chunk by chunk (inside a chunk the
@@ -1815,9 +1852,8 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
     uint32_t* sub_cursor = pd.colour_sub.p + 4 * MAX_COLOURS;
     check_cuda(cudaMemsetAsync(sub_hist, 0, 4 * MAX_COLOURS * sizeof(uint32_t), s), "memset");
     uint32_t g = std::min<uint32_t>((npairs + TB - 1) / TB, 148u * 8u);
-    k_colour_hist<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pd.colour.p, pd.row_count.p, pd.rows.p,
-                                   pd.colour_count.p, pd.split_count.p, pd.flags.p, sub_hist);
-    // Chunks: each body's chunk, the (colour, chunk) counts and the touch sets.
+    // Chunks: each body's chunk; the (colour, chunk) counts and the touch sets come with the
+    // colour histograms.
     uint32_t P = 0, W = 0;
     uint32_t *vhist = nullptr, *shist = nullptr, *all_flag = nullptr;
     if (chunked) {
@@ -1840,9 +1876,10 @@ void run_solver(const WorldView& w, const uint64_t* pairs, uint32_t npairs, Pair
         const uint32_t lim = (morton_leaf && tree_m) ? tree_m : n;
         k_chunk_of<<<std::min<uint32_t>((lim + TB - 1) / TB, 148u * 8u), TB, 0, s>>>(
             n, P, (morton_leaf && tree_m) ? morton_leaf : nullptr, tree_m, pd.chunk_of.p);
-        k_chunk_hist<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pairs, pd.row_count.p, pd.colour.p,
-                                      pd.flags.p, w.b.iw, pd.chunk_of.p, P, vhist, shist, pd.chunk_touch.p, all_flag);
     }
+    k_colour_hist<<<g, TB, 0, s>>>(pd.scalars.p + 2, pd.contact_pairs.p, pd.colour.p, pd.row_count.p, pd.rows.p,
+                                   pd.colour_count.p, pd.split_count.p, pd.flags.p, sub_hist, pairs, w.b.iw,
+                                   pd.chunk_of.p, P, vhist, shist, pd.chunk_touch.p, all_flag);
     k_colour_scan<<<1, 32, 0, s>>>(pd.colour_count.p, pd.colour_offset.p, pd.colour_cursor.p, pd.split_count.p,
                                    pd.split_offset.p, pd.split_cursor.p, pd.barrier.p, pd.scalars.p, pd.colour_remap.p,
                                    sub_hist, sub_cursor, chunked ? 1u : 0u);
