@@ -448,8 +448,9 @@ __device__ __forceinline__ uint32_t claim_slot(uint32_t* cursor, uint32_t c) {
 // run of bodies in Morton order (the broad phase's tree leaves), and a group belongs to the
 // chunk of its first dynamic body. Block b solves chunk b's groups of every colour; before
 // a phase it waits only for the blocks whose groups share a dynamic body with its own (its
-// neighbours), not for the whole grid. Two blocks share a body exactly when both appear in
-// the body's touch set, so the neighbour relation is built from the touch sets.
+// neighbours), not for the whole grid. Every block whose groups touch a body appears in the
+// body's touch set (its own chunk plus the foreign chunks recorded by the histogram pass), so
+// making every two chunks of each touch set neighbours covers every shared body.
 constexpr uint32_t CHUNK_TOUCH = 8;          // foreign chunks recorded per body
 constexpr uint32_t CHUNK_EMPTY = 0xffffffffu;
 constexpr uint32_t CHUNK_MAX = 1024;         // blocks of a chunked launch
