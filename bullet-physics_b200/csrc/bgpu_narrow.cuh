@@ -108,7 +108,21 @@ __device__ __forceinline__ void clip_poly(const ClipPoly& src, int axis, float s
     }
 }
 
-static __device__ __noinline__ bool box_box(V3 ha, V3 p1, Q oa, V3 hb, V3 p2, Q ob, Manifold& out) {
+// box_box's arrays (clip polygons, clipped points, cull order), indexed at runtime. The kernels
+// keep one per thread in shared memory, where a runtime index costs no local-memory traffic. 83
+// words: an odd stride puts the 32 lanes' copies of a field in 32 different banks.
+struct BoxBoxScratch {
+    ClipPoly buf, tmp;
+    V3 pts[8];
+    float deps[8];
+    float rd[8];
+    int ri[8];
+    int pad;
+};
+static_assert(sizeof(BoxBoxScratch) % 8 == 4, "odd word stride");
+
+static __device__ __noinline__ bool box_box(V3 ha, V3 p1, Q oa, V3 hb, V3 p2, Q ob, Manifold& out,
+                                            BoxBoxScratch& S) {
     const float EPS = 1e-6f, FUDGE = 1.05f;
     M3 r1 = from_quat(oa), r2 = from_quat(ob);
     V3 p = p2 - p1;
@@ -229,7 +243,8 @@ static __device__ __noinline__ bool box_box(V3 ha, V3 p1, Q oa, V3 hb, V3 p2, Q 
     float m22 = dot(col(ra, code2), col(rb, a2));
     float k1 = m11 * comp(sb, a1), k2 = m21 * comp(sb, a1), k3 = m12 * comp(sb, a2), k4 = m22 * comp(sb, a2);
 
-    ClipPoly buf, tmp;
+    ClipPoly& buf = S.buf;
+    ClipPoly& tmp = S.tmp;
     buf.x[0] = c1 - k1 - k3; buf.y[0] = c2 - k2 - k4;
     buf.x[1] = c1 - k1 + k3; buf.y[1] = c2 - k2 + k4;
     buf.x[2] = c1 + k1 + k3; buf.y[2] = c2 + k2 + k4;
@@ -244,8 +259,8 @@ static __device__ __noinline__ bool box_box(V3 ha, V3 p1, Q oa, V3 hb, V3 p2, Q 
 
     float det1 = 1.0f / (m11 * m22 - m12 * m21);
     m11 *= det1; m12 *= det1; m21 *= det1; m22 *= det1;
-    V3 pts[8];
-    float deps[8];
+    V3* pts = S.pts;
+    float* deps = S.deps;
     int np = 0;
     for (int i = 0; i < buf.n; ++i) {
         float rx = buf.x[i], ry = buf.y[i];
@@ -267,8 +282,8 @@ static __device__ __noinline__ bool box_box(V3 ha, V3 p1, Q oa, V3 hb, V3 p2, Q 
         int i0 = 0;
         float dd = deps[0];
         for (int i = 1; i < np; ++i) if (deps[i] >= dd) { i0 = i; dd = deps[i]; }
-        int ri[8];
-        float rd[8];
+        int* ri = S.ri;
+        float* rd = S.rd;
         int rn = 0;
         for (int i = 0; i < np; ++i) if (i != i0) { ri[rn] = i; rd[rn] = len2(pts[i] - pts[i0]); rn++; }
         for (int j = 1; j < rn; ++j) {

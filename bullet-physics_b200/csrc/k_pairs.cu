@@ -494,7 +494,7 @@ __global__ void k_classify(BodyDev b, const Shape* __restrict__ shapes, const ui
 
 // narrowphase/mod.rs:63-286 for one pair; returns the manifold (positions on B, normals A->B).
 __device__ __forceinline__ void collide_analytic(uint32_t route, const Shape& sa, V3 pa, Q qa, const Shape& sb, V3 pb,
-                                                 Q qb, const float4* __restrict__ hull, Manifold& m) {
+                                                 Q qb, const float4* __restrict__ hull, Manifold& m, BoxBoxScratch& bbs) {
     float thr = fminf(sa.cbt, sb.cbt);
     m.n = 0;
     switch (route) {
@@ -507,7 +507,7 @@ __device__ __forceinline__ void collide_analytic(uint32_t route, const Shape& sa
             if (sphere_box(sa.p0, pa, V3{sb.p0, sb.p1, sb.p2}, pb, qb, thr, m)) mf_flip(m);
             break;
         case NP_BOX_SPHERE: sphere_box(sb.p0, pb, V3{sa.p0, sa.p1, sa.p2}, pa, qa, thr, m); break;
-        case NP_BOX_BOX: box_box(V3{sa.p0, sa.p1, sa.p2}, pa, qa, V3{sb.p0, sb.p1, sb.p2}, pb, qb, m); break;
+        case NP_BOX_BOX: box_box(V3{sa.p0, sa.p1, sa.p2}, pa, qa, V3{sb.p0, sb.p1, sb.p2}, pb, qb, m, bbs); break;
         default: break;
     }
 }
@@ -779,8 +779,11 @@ __device__ __forceinline__ bool entry_seed(const float4* __restrict__ e, V3& s) 
     return false;
 }
 
-__global__ void k_narrow_analytic(BodyDev b, const Shape* __restrict__ shapes, const float4* __restrict__ hull,
+constexpr uint32_t NARROW_ANALYTIC_TB = 128;
+
+__global__ __launch_bounds__(NARROW_ANALYTIC_TB) void k_narrow_analytic(BodyDev b, const Shape* __restrict__ shapes, const float4* __restrict__ hull,
                                   const uint64_t* __restrict__ pairs, uint32_t npairs, PairDataDev pd) {
+    __shared__ BoxBoxScratch s_bbs[NARROW_ANALYTIC_TB];
     uint32_t counts[NP_CONVEX + 1];
     uint32_t cnt = 0;
 #pragma unroll
@@ -797,7 +800,7 @@ __global__ void k_narrow_analytic(BodyDev b, const Shape* __restrict__ shapes, c
         Shape sa = shapes[ia.x], sb = shapes[ib.x];
         Manifold m;
         collide_analytic(pd.status[p] >> 8, sa, from4(b.pred[i]), q4(b.quat[i]), sb, from4(b.pred[j]), q4(b.quat[j]),
-                         hull, m);
+                         hull, m, s_bbs[threadIdx.x]);
         store_detection(pd, p, npairs, m);
     }
 }
@@ -1025,12 +1028,15 @@ __global__ void k_drop_undetectable(uint32_t npairs, PairDataDev pd) {
     if (pd.status[p] == (PS_DETECT | (NP_NONE << 8))) store_meta_only(pd.entries + size_t(p) * ENTRY_F4, 0u);
 }
 
-__global__ void k_collide_queries(const Shape* __restrict__ shapes, const float4* __restrict__ hull, uint32_t n,
+constexpr uint32_t COLLIDE_QUERIES_TB = 64;
+
+__global__ __launch_bounds__(COLLIDE_QUERIES_TB) void k_collide_queries(const Shape* __restrict__ shapes, const float4* __restrict__ hull, uint32_t n,
                                   const uint32_t* __restrict__ sai, const float4* __restrict__ pa4,
                                   const float4* __restrict__ qa4, const uint32_t* __restrict__ sbi,
                                   const float4* __restrict__ pb4, const float4* __restrict__ qb4,
                                   const float4* __restrict__ seeds, int force_convex, float4* out, uint32_t* counts,
                                   uint32_t* status) {
+    __shared__ BoxBoxScratch s_bbs[COLLIDE_QUERIES_TB];
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     Shape sa = shapes[sai[t]], sb = shapes[sbi[t]];
@@ -1047,7 +1053,7 @@ __global__ void k_collide_queries(const Shape* __restrict__ shapes, const float4
         if (route == NP_MESH) collide_mesh_pair(sa, pa, qa, sb, pb, qb, has_seed, seed, hull, scratch, m, status);
         else collide_convex(sa, pa, qa, sb, pb, qb, has_seed, seed, hull, scratch, m, status);
     } else if (route != NP_NONE) {
-        collide_analytic(route, sa, pa, qa, sb, pb, qb, hull, m);
+        collide_analytic(route, sa, pa, qa, sb, pb, qb, hull, m, s_bbs[threadIdx.x]);
     }
     counts[t] = uint32_t(m.n);
     for (int k = 0; k < m.n; ++k) {
@@ -1097,7 +1103,7 @@ void run_pair_pass(const WorldView& w, const uint64_t* pairs, uint32_t npairs, c
                                                      old_cache.entries.p, old_cache.count_dev, sp, d);
     k_drop_undetectable<<<(npairs + 255) / 256, 256, 0, s>>>(npairs, d);
     uint32_t grid = std::min<uint32_t>((npairs + TB - 1) / TB, 148u * 16u);
-    k_narrow_analytic<<<grid, TB, 0, s>>>(w.b, w.shapes, w.hull, pairs, npairs, d);
+    k_narrow_analytic<<<grid, NARROW_ANALYTIC_TB, 0, s>>>(w.b, w.shapes, w.hull, pairs, npairs, d);
     uint32_t cgrid = std::min<uint32_t>((npairs + 63) / 64, 148u * 8u);
     k_narrow_convex<<<cgrid, 64, 0, s>>>(w.b, w.shapes, w.hull, pairs, npairs, d, status_dev);
     if (w.has_mesh) {
@@ -1115,7 +1121,7 @@ void run_collide_queries(const Shape* shapes, const float4* hull, uint32_t n, co
                          const float4* qa, const uint32_t* sb, const float4* pb, const float4* qb, const float4* seeds,
                          int force_convex, float4* out, uint32_t* counts, uint32_t* status_dev, cudaStream_t s) {
     if (n == 0) return;
-    k_collide_queries<<<(n + 63) / 64, 64, 0, s>>>(shapes, hull, n, sa, pa, qa, sb, pb, qb, seeds, force_convex, out,
+    k_collide_queries<<<(n + COLLIDE_QUERIES_TB - 1) / COLLIDE_QUERIES_TB, COLLIDE_QUERIES_TB, 0, s>>>(shapes, hull, n, sa, pa, qa, sb, pb, qb, seeds, force_convex, out,
                                                    counts, status_dev);
 }
 
