@@ -295,12 +295,13 @@ __global__ void k_query(int m, uint32_t n, const uint32_t* __restrict__ is_unb, 
     }
 }
 
-// Stashed segments (at most STASH_SLOTS partners) to their place in the pair list.
+// Stashed segments (at most STASH_SLOTS partners) to their place in the pair list. Slot t
+// belongs to proxy leaf_body[t] (to proxy t when leaf_body is null).
 __global__ void k_stash_copy(int m, const uint32_t* __restrict__ leaf_body, const uint32_t* __restrict__ counts,
                              const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ stash, uint64_t* out) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= uint32_t(m)) return;
-    const uint32_t i = leaf_body[t];
+    const uint32_t i = leaf_body ? leaf_body[t] : t;
     const uint32_t c = counts[i];
     if (c > STASH_SLOTS) return;
     const uint64_t base = offsets[i];
@@ -348,25 +349,26 @@ __global__ void k_set_unbounded(const uint32_t* __restrict__ unb, uint32_t nunb,
 // Batched worlds: world k owns proxies [off[k], off[k + 1]) and pairs only form
 // inside a world. One CTA per world tests every (i < j) of the world against
 // the other proxies staged in shared memory, tile by tile in ascending j, so
-// each proxy's segment comes out sorted, as in the tree query. The count pass
-// (WRITE false) fills counts[i]; the write pass stores at offsets[i].
+// each proxy's partners come out in ascending order, as in the tree query. The
+// pass fills counts[i] and stashes the partners of every proxy with at most
+// STASH_SLOTS of them (stash[a * n + i]); a world with a proxy over that (a
+// ground plane under a pile) sets wover[w] and adds one to *n_over.
 constexpr int WP_TILE = 64;
 
-template <bool WRITE>
 __global__ void __launch_bounds__(WP_TILE) k_world_pairs(const float4* __restrict__ bmin, const float4* __restrict__ bmax,
-                                                           const uint32_t* __restrict__ off, uint32_t n_worlds,
-                                                           uint32_t* counts, const uint32_t* __restrict__ offsets,
-                                                           uint64_t* out) {
+                                                           const uint32_t* __restrict__ off, uint32_t n_worlds, uint32_t n,
+                                                           uint32_t* counts, uint32_t* stash, uint32_t* wover,
+                                                           uint32_t* n_over) {
     __shared__ float4 smin[WP_TILE], smax[WP_TILE];
     for (uint32_t w = blockIdx.x; w < n_worlds; w += gridDim.x) {
         const uint32_t lo = off[w], hi = off[w + 1];
+        bool over = false;
         for (uint32_t ibase = lo; ibase < hi; ibase += WP_TILE) {
             const uint32_t i = ibase + threadIdx.x;
             const bool has = i < hi;
             float4 qmin = make_float4(0.f, 0.f, 0.f, 0.f), qmax = qmin;
             if (has) { qmin = bmin[i]; qmax = bmax[i]; }
             uint32_t cnt = 0;
-            uint64_t pos = (WRITE && has) ? uint64_t(offsets[i]) : 0ull;
             for (uint32_t jbase = ibase; jbase < hi; jbase += WP_TILE) {
                 __syncthreads();
                 const uint32_t j = jbase + threadIdx.x;
@@ -377,12 +379,63 @@ __global__ void __launch_bounds__(WP_TILE) k_world_pairs(const float4* __restric
                 for (uint32_t q = 0; q < jn; ++q) {
                     const uint32_t jj = jbase + q;
                     if (jj > i && overlaps(qmin, qmax, smin[q], smax[q])) {
-                        if (WRITE) out[pos++] = (uint64_t(i) << 32) | jj;
-                        else ++cnt;
+                        if (cnt < STASH_SLOTS) stash[size_t(cnt) * n + i] = jj;
+                        ++cnt;
                     }
                 }
             }
-            if (!WRITE && has) counts[i] = cnt;
+            if (has) {
+                counts[i] = cnt;
+                over |= cnt > STASH_SLOTS;
+            }
+        }
+        const int any = __syncthreads_or(over ? 1 : 0);
+        if (threadIdx.x == 0) {
+            wover[w] = any ? 1u : 0u;
+            if (any) atomicAdd(n_over, 1u);
+        }
+    }
+}
+
+// The segments of the proxies that k_world_pairs could not stash, in the worlds it
+// flagged. The CTA takes those proxies one at a time and tests 64 candidates j at
+// once; a ballot per warp ranks the hits, so the segment is written in ascending j.
+__global__ void __launch_bounds__(WP_TILE) k_world_pairs_write(const float4* __restrict__ bmin,
+                                                                 const float4* __restrict__ bmax,
+                                                                 const uint32_t* __restrict__ off, uint32_t n_worlds,
+                                                                 const uint32_t* __restrict__ counts,
+                                                                 const uint32_t* __restrict__ offsets,
+                                                                 const uint32_t* __restrict__ wover, uint64_t* out) {
+    static_assert(WP_TILE == 64, "two warps a CTA");
+    __shared__ uint32_t s_mask[2], s_hits[2];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (uint32_t w = blockIdx.x; w < n_worlds; w += gridDim.x) {
+        if (!wover[w]) continue;  // uniform across the CTA
+        const uint32_t lo = off[w], hi = off[w + 1];
+        for (uint32_t ibase = lo; ibase < hi; ibase += WP_TILE) {
+            const uint32_t me = ibase + threadIdx.x;
+            const uint32_t m = __ballot_sync(0xffffffffu, me < hi && counts[me] > STASH_SLOTS);
+            __syncthreads();  // the previous tile's readers of s_mask are done
+            if (lane == 0) s_mask[warp] = m;
+            __syncthreads();
+            unsigned long long todo = (static_cast<unsigned long long>(s_mask[1]) << 32) | s_mask[0];
+            while (todo) {
+                const uint32_t i = ibase + uint32_t(__ffsll(static_cast<long long>(todo)) - 1);
+                todo &= todo - 1ull;
+                const float4 qmin = bmin[i], qmax = bmax[i];
+                uint64_t pos = offsets[i];
+                for (uint32_t jbase = i + 1; jbase < hi; jbase += WP_TILE) {
+                    const uint32_t j = jbase + threadIdx.x;
+                    const bool hit = j < hi && overlaps(qmin, qmax, bmin[j], bmax[j]);
+                    const uint32_t b = __ballot_sync(0xffffffffu, hit);
+                    if (lane == 0) s_hits[warp] = __popc(b);
+                    __syncthreads();
+                    const uint32_t h0 = s_hits[0], h1 = s_hits[1];
+                    if (hit) out[pos + (warp ? h0 : 0u) + __popc(b & ((1u << lane) - 1u))] = (uint64_t(i) << 32) | j;
+                    pos += h0 + h1;
+                    __syncthreads();  // s_hits is rewritten next round
+                }
+            }
         }
     }
 }
@@ -395,19 +448,28 @@ uint64_t Broadphase::run_worlds(const float4* aabb_min, const float4* aabb_max, 
     counts.reserve(n);
     offsets.reserve(n);
     scalars.reserve(4);
+    stash.reserve(size_t(STASH_SLOTS) * n);
+    overflow.reserve(n_worlds);
+    check_cuda(cudaMemsetAsync(scalars.p + 1, 0, sizeof(uint32_t), s), "memset");
     const uint32_t grid = std::min<uint32_t>(n_worlds, 148u * 32u);
-    k_world_pairs<false><<<grid, WP_TILE, 0, s>>>(aabb_min, aabb_max, world_off, n_worlds, counts.p, nullptr, nullptr);
+    k_world_pairs<<<grid, WP_TILE, 0, s>>>(aabb_min, aabb_max, world_off, n_worlds, n, counts.p, stash.p, overflow.p,
+                                           scalars.p + 1);
     size_t scan_bytes = 0;
     check_cuda(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, counts.p, offsets.p, int(n), s), "scan size");
     cub_tmp.reserve(scan_bytes);
     check_cuda(cub::DeviceScan::ExclusiveSum(cub_tmp.p, scan_bytes, counts.p, offsets.p, int(n), s), "scan");
     k_total<<<1, 1, 0, s>>>(n, counts.p, offsets.p, scalars.p);
-    check_cuda(cudaMemcpyAsync(host_scalars, scalars.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "total d2h");
+    check_cuda(cudaMemcpyAsync(host_scalars, scalars.p, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "total d2h");
     check_cuda(cudaStreamSynchronize(s), "broadphase sync");
     uint64_t total = host_scalars[0];
+    const uint32_t n_over = host_scalars[1];
     out.reserve(total + 1);
-    if (total)
-        k_world_pairs<true><<<grid, WP_TILE, 0, s>>>(aabb_min, aabb_max, world_off, n_worlds, counts.p, offsets.p, out.p);
+    if (total) {
+        k_stash_copy<<<(n + 255) / 256, 256, 0, s>>>(int(n), nullptr, counts.p, offsets.p, stash.p, out.p);
+        if (n_over)
+            k_world_pairs_write<<<grid, WP_TILE, 0, s>>>(aabb_min, aabb_max, world_off, n_worlds, counts.p, offsets.p,
+                                                         overflow.p, out.p);
+    }
     return total;
 }
 
