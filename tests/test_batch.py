@@ -102,6 +102,52 @@ def test_batch_pairs_never_cross_worlds(gpu):
 
 
 @gpu_only
+def test_batch_pairs_of_crowded_proxies(gpu):
+    """Proxies with more than 32 partners j > i (the ground plane and large static boxes among
+    small spheres) take the broad phase's second, ballot-ranked write pass. The large boxes sit
+    at several positions of a world, two of them in one 64-proxy tile and one in the next, so
+    a tile holds several such proxies. Every world's pairs must equal the oracle's brute force
+    on that world, in ascending order."""
+    import scenes
+
+    rng = np.random.default_rng(21)
+    b = scenes.BatchScene("crowded_proxies", 1.0 / 60.0, 10, 1)
+    plane = b.add_shape(scenes.PLANE, [0.0, 1.0, 0.0, 0.0])
+    big = b.add_shape(scenes.BOX, [2.0, 2.0, 2.0])
+    ball = b.add_shape(scenes.SPHERE, [0.2])
+    for k in range(6):
+        ns = 110 + 10 * k  # at least 40 spheres after the last big box
+        at = sorted({3 + k, 20 + 2 * k, 66 + k})  # the big boxes' indices in the world
+        n = 1 + ns + len(at)
+        shape = np.full(n, ball)
+        shape[0] = plane
+        shape[at] = big
+        pos = rng.uniform(-2.0, 2.0, size=(n, 3)) + np.array([0.0, 3.0, 0.0])
+        pos[0] = 0.0
+        pos[at] = rng.uniform(-0.3, 0.3, size=(len(at), 3)) + np.array([0.0, 3.0, 0.0])
+        mass = np.ones(n)
+        mass[0] = 0.0
+        mass[at] = 0.0
+        b.add_world(shape, pos, np.tile(np.array([0, 0, 0, 1], np.float32), (n, 1)), mass)
+    w = b.build_gpu(gpu)
+    off = w.world_offsets().astype(np.int64)
+    w.step(b.dt)
+    assert w.stats()["device_status"] == 0
+    pairs = w.pairs().astype(np.int64)
+    key = pairs[:, 0] * (1 << 32) + pairs[:, 1]
+    assert np.all(np.diff(key) > 0)
+    for k in range(len(b.worlds)):
+        lo = off[k]
+        mine = pairs[(pairs[:, 0] >= lo) & (pairs[:, 0] < off[k + 1])] - lo
+        crowded = np.bincount(mine[:, 0], minlength=int(off[k + 1] - lo))
+        assert (crowded > 32).sum() >= 4  # the plane and the three boxes
+        o = b.world_scene(k).build_oracle(orc)
+        o.set_brute_force(True)
+        o.step(b.dt)
+        np.testing.assert_array_equal(mine, o.pairs())
+
+
+@gpu_only
 def test_batch_rejects_plain_body_insertion(gpu):
     import bgpu
 
