@@ -545,19 +545,23 @@ def main():
             "gpu_launches_note": f"CUPTI count of one step x steps ({kernel_kinds} kernel kinds)",
             "device_status": st["device_status"],
         }
-        if args.batch_worlds > 0:
+        # The other configurations are single-GPU legs: they run at n_gpus 1 only, so that the
+        # other ranks of a multi-GPU run do not sit in the closing barrier for minutes.
+        if world_size > 1:
+            line["other_legs"] = "measured at n_gpus 1 only; each rank of this run steps a pile replica"
+        if world_size == 1 and args.batch_worlds > 0:
             line["batched_worlds"] = bench_batched(bgpu, scenes, args.batch_worlds, args.batch_steps, args.warmup)
-        if args.adjoint_worlds > 0:
+        if world_size == 1 and args.adjoint_worlds > 0:
             line["adjoint"] = bench_adjoint(bgpu, scenes, args.adjoint_worlds)
-        if args.ccd_spheres > 0:
+        if world_size == 1 and args.ccd_spheres > 0:
             line["ccd_rain"] = bench_ccd(bgpu, scenes, args.ccd_spheres)
-        if args.spring2_counts:
+        if world_size == 1 and args.spring2_counts:
             line["spring2_chains"] = [bench_spring2(bgpu, scenes, int(c)) for c in args.spring2_counts.split(",")]
-        if args.stack_steps > 0:
+        if world_size == 1 and args.stack_steps > 0:
             line["stack_1000"] = bench_stack(bgpu, scenes, args.stack_steps)
-        if args.mixed_steps > 0:
+        if world_size == 1 and args.mixed_steps > 0:
             line["mixed_convex_16384"] = bench_mixed(bgpu, scenes, args.mixed_steps)
-        if args.mesh_frames > 0:
+        if world_size == 1 and args.mesh_frames > 0:
             line["mesh_rain"] = bench_mesh_rain(bgpu, scenes, args.mesh_frames)
         if world_size == 1 and not args.no_cpu_baseline:
             # CPU leg: the oracle timed on the host (the baseline) and run as the f64 checker.
