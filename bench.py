@@ -65,6 +65,13 @@ def parse():
     return a
 
 
+def smi_gpu_id(local_rank):
+    """nvidia-smi's id of this rank's GPU: its entry of CUDA_VISIBLE_DEVICES (an index or a UUID)
+    when that is set, else the local rank (nvidia-smi ignores CUDA_VISIBLE_DEVICES)."""
+    vis = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    return vis[local_rank] if local_rank < len(vis) else str(local_rank)
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle samples during the timed region: the sampler is running
     (its first sample seen, then dropped) before the region starts, samples every 20 ms, and
@@ -458,10 +465,12 @@ def main():
             dist.destroy_process_group()
         return
 
-    if local_rank:
-        os.environ["CUDA_VISIBLE_DEVICES"] = os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank))
     import bgpu
     import scenes
+
+    if world_size > 1:
+        # The library has its own CUDA runtime: make this rank's GPU its current device too.
+        bgpu.set_device(local_rank)
 
     nx, nz, ny = grid_of(args.grid)
     sc = scenes.large_pile_fast(nx, nz, ny, seed=3 + rank)
@@ -475,7 +484,7 @@ def main():
 
         dist.barrier()
         torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clocks:
+    with ClockSampler(smi_gpu_id(local_rank)) as clocks:
         ms = w.step_timed(sc.dt, args.steps)
     st = w.stats()
     w.enable_timing(False)

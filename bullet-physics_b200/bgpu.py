@@ -286,6 +286,7 @@ def lib():
         sig = {
             "bgpu_version": (ctypes.c_char_p, []),
             "bgpu_device_count": (ctypes.c_int, []),
+            "bgpu_set_device": (S, [ctypes.c_int]),
             "bgpu_last_error": (ctypes.c_size_t, [ctypes.c_char_p, ctypes.c_size_t]),
             "bgpu_solver_info_default": (None, [ctypes.POINTER(SolverInfo)]),
             "bgpu_body_desc_default": (None, [ctypes.POINTER(BodyDesc)]),
@@ -387,6 +388,11 @@ def f32(a):
 
 def device_count():
     return lib().bgpu_device_count()
+
+
+def set_device(device):
+    """Makes `device` the calling thread's device for the library (bgpu_set_device)."""
+    check(lib().bgpu_set_device(int(device)), "set_device")
 
 
 def selftest_wait_timeout(limit_ms):

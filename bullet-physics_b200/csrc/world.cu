@@ -1400,6 +1400,22 @@ int bgpu_device_count(void) {
     return c;
 }
 
+bgpu_status bgpu_set_device(int device) {
+    const int n = bgpu_device_count();
+    if (n == 0) {
+        bgpu::g_last_error = "no CUDA device";
+        return BGPU_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= n) {
+        bgpu::g_last_error = "bgpu_set_device: no device with that ordinal";
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&]() -> bgpu_status {
+        bgpu::check_cuda(cudaSetDevice(device), "cudaSetDevice");
+        return BGPU_OK;
+    });
+}
+
 size_t bgpu_last_error(char* buf, size_t len) {
     const std::string& e = bgpu::g_last_error;
     if (buf && len) {

@@ -243,6 +243,12 @@ bgpu_status bgpu_spring2_hinge2(const float* pos_a, const float* quat_a, const f
 const char* bgpu_version(void);
 int bgpu_device_count(void);
 size_t bgpu_last_error(char* buf, size_t len);
+/* Makes `device` (0 .. bgpu_device_count() - 1, in the order this process sees the devices)
+ * the calling thread's device for the library's later calls, as cudaSetDevice does for the
+ * library's own CUDA runtime. A world lives on the device that was current when it was
+ * created; use it from a thread with that device current. One process per GPU calls this
+ * with its local rank before creating its worlds. */
+bgpu_status bgpu_set_device(int device);
 
 /* World lifetime (PhysicsWorld::new; world.rs:406-463). gravity may be NULL (0, -9.81, 0). */
 bgpu_status bgpu_world_create(const bgpu_solver_info* info, const float* gravity, bgpu_world** out);

@@ -53,6 +53,8 @@ def test_no_device_fails_loudly(bgpu_mod):
         bgpu_mod.World()
     with pytest.raises(bgpu_mod.BgpuError):
         bgpu_mod.broadphase_pairs([[0, 0, 0, 1, 1, 1]])
+    with pytest.raises(bgpu_mod.BgpuError, match="no CUDA device"):
+        bgpu_mod.set_device(0)
 
 
 def test_struct_layouts_match_the_header(bgpu_mod):
@@ -61,3 +63,21 @@ def test_struct_layouts_match_the_header(bgpu_mod):
     assert ctypes.sizeof(bgpu_mod.SolverInfo) == 48
     assert ctypes.sizeof(bgpu_mod.JointDesc) == 4 * 4 + 24 * 4 + 35 * 4
     assert ctypes.sizeof(bgpu_mod.StepStats) == 10 * 4 + 7 * 4 + 2 * 4 + 4
+
+
+@pytest.mark.gpu
+def test_set_device_takes_a_visible_ordinal(gpu):
+    """bgpu_set_device selects among the devices the process sees and rejects any other
+    ordinal with an error (no CUDA call is made for it); a world created after it steps."""
+    n = gpu.device_count()
+    assert n >= 1
+    gpu.set_device(0)
+    for bad in (-1, n):
+        with pytest.raises(gpu.BgpuError, match="no device with that ordinal"):
+            gpu.set_device(bad)
+    w = gpu.World()
+    box = w.box([0.5, 0.5, 0.5])
+    w.add_body(box, (0, 2, 0))
+    w.step(1.0 / 60.0)
+    assert w.stats()["device_status"] == 0
+    w.close()
