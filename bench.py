@@ -66,10 +66,19 @@ def parse():
 
 
 def smi_gpu_id(local_rank):
-    """nvidia-smi's id of this rank's GPU: its entry of CUDA_VISIBLE_DEVICES (an index or a UUID)
-    when that is set, else the local rank (nvidia-smi ignores CUDA_VISIBLE_DEVICES)."""
+    """nvidia-smi's id of this rank's GPU. nvidia-smi ignores CUDA_VISIBLE_DEVICES, so the rank's
+    entry there (an index or a UUID) is used when nvidia-smi knows it; otherwise (unset, or a
+    container that shows nvidia-smi only its own GPUs) the local rank."""
     vis = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
-    return vis[local_rank] if local_rank < len(vis) else str(local_rank)
+    if local_rank < len(vis):
+        try:
+            r = subprocess.run(["nvidia-smi", "-i", vis[local_rank], "--query-gpu=index", "--format=csv,noheader"],
+                               capture_output=True, text=True, timeout=20)
+            if r.returncode == 0 and r.stdout.strip():
+                return vis[local_rank]
+        except (OSError, subprocess.TimeoutExpired):
+            pass
+    return str(local_rank)
 
 
 class ClockSampler:
