@@ -63,6 +63,11 @@ uint32_t add_body(World<R>& w, const double* d) {
         b.is_static = false;
         b.flags = uint32_t(d[17]) | CF_KINEMATIC;
         b.activation = ACT_DISABLE_DEACTIVATION;
+        // The filter and damping a caller sets on the built body (collision_filter, set_damping).
+        b.group = uint16_t(d[18]);
+        b.mask = uint16_t(d[19]);
+        b.linear_damping = static_cast<R>(d[20]);
+        b.angular_damping = static_cast<R>(d[21]);
     }
     if (d[22] != 0) b.activation = uint32_t(d[22]);
     return w.add_body(b);
@@ -390,6 +395,33 @@ void orc_world_get_state(void* p, double* out) {
 void orc_world_set_state(void* p, const double* in) {
     Handle* h = static_cast<Handle*>(p);
     DISPATCH(h, { set_state(w, in); });
+}
+
+// body.rs:883-886 apply_force (wakes the body, as activate() at body.rs:562-574) and the
+// torque accumulator beside it; the step clears both (world/step.rs:206, clear_forces).
+void orc_world_apply_force(void* p, uint32_t i, const double* f, const double* t) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, {
+        using R = std::remove_reference_t<decltype(w.gravity.x)>;
+        auto& b = w.bodies.at(i);
+        if (!b.is_static && b.activation != ACT_DISABLE_SIMULATION && b.activation != ACT_DISABLE_DEACTIVATION) {
+            b.activation = ACT_ACTIVE;
+            b.deactivation_time = R(0);
+        }
+        b.force += V3<R>(static_cast<R>(f[0]), static_cast<R>(f[1]), static_cast<R>(f[2]));
+        b.torque += V3<R>(static_cast<R>(t[0]), static_cast<R>(t[1]), static_cast<R>(t[2]));
+    });
+}
+
+// The body's public collision_group / collision_mask fields (body.rs:325-328), written
+// between steps; the broad phase's pair test reads them every step.
+void orc_world_set_filter(void* p, uint32_t i, uint32_t group, uint32_t mask) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, {
+        auto& b = w.bodies.at(i);
+        b.group = uint16_t(group);
+        b.mask = uint16_t(mask);
+    });
 }
 
 void orc_world_get_push(void* p, double* out) {

@@ -47,6 +47,8 @@ def lib():
             "orc_world_get_state": (None, [P, D]),
             "orc_world_set_state": (None, [P, D]),
             "orc_world_get_push": (None, [P, D]),
+            "orc_world_apply_force": (None, [P, ctypes.c_uint32, D, D]),
+            "orc_world_set_filter": (None, [P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
             "orc_world_num_pairs": (U32, [P]),
             "orc_world_get_pairs": (None, [P, ctypes.POINTER(U32)]),
             "orc_world_num_rows": (U32, [P]),
@@ -308,6 +310,13 @@ class OracleWorld:
     def set_state(self, s):
         s = f64(s)
         self.L.orc_world_set_state(self.h, dptr(s))
+
+    def apply_force(self, i, force, torque=(0.0, 0.0, 0.0)):
+        f, t = f64(force), f64(torque)
+        self.L.orc_world_apply_force(self.h, int(i), dptr(f), dptr(t))
+
+    def set_filter(self, i, group, mask):
+        self.L.orc_world_set_filter(self.h, int(i), int(group), int(mask))
 
     def push(self):
         out = np.zeros((self.num_bodies, 6))
