@@ -64,7 +64,7 @@ def test_damping_applied_during_step(gpu):
 
 
 def test_collision_mask_blocks_pair(gpu):
-    # world/step.rs:1327-1350
+    # world/step.rs:1327-1351
     w, o = _both((0.0, -9.81, 0.0))
     for x in (w, o):
         plate, ball = x.box([2.0, 0.5, 2.0]), x.sphere(0.5)
@@ -75,7 +75,7 @@ def test_collision_mask_blocks_pair(gpu):
 
 
 def test_disable_simulation_body_takes_solver_impulses_without_integrating(gpu):
-    # world/step.rs:1729-1757
+    # world/step.rs:1729-1759
     w, o = _both((0.0, 0.0, 0.0))
     for x in (w, o):
         s = x.sphere(0.5)
@@ -87,7 +87,7 @@ def test_disable_simulation_body_takes_solver_impulses_without_integrating(gpu):
 
 
 def test_kinematic_pushes_dynamic_body(gpu):
-    # world/step.rs:2591-2617
+    # world/step.rs:2591-2619
     w, o = _both((0.0, -10.0, 0.0))
     for x in (w, o):
         ground, slab, small = x.plane([0, 1, 0], 0.0), x.box([1.0, 0.5, 1.0]), x.box([0.25, 0.25, 0.25])
@@ -113,7 +113,7 @@ def test_kinematic_ignores_gravity_forces_and_damping(gpu):
 
 
 def test_dynamic_body_rests_and_sleeps_on_idle_kinematic_platform(gpu):
-    # world/step.rs:2655-2676
+    # world/step.rs:2655-2675
     w, o = _both((0.0, -10.0, 0.0))
     for x in (w, o):
         plat, cargo = x.box([2.0, 0.25, 2.0]), x.box([0.25, 0.25, 0.25])
@@ -126,7 +126,7 @@ def test_dynamic_body_rests_and_sleeps_on_idle_kinematic_platform(gpu):
 
 
 def test_kinematic_static_and_kinematic_kinematic_pairs_are_inert(gpu):
-    # world/step.rs:2681-2713
+    # world/step.rs:2681-2711
     w, o = _both((0.0, -10.0, 0.0))
     for x in (w, o):
         ground, cube = x.plane([0, 1, 0], 0.0), x.box([0.5, 0.5, 0.5])

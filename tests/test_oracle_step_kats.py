@@ -34,7 +34,7 @@ def test_damping_applied_during_step(prec):
 
 @pytest.mark.parametrize("prec", PRECISIONS)
 def test_collision_mask_blocks_pair(prec):
-    # world/step.rs:1327-1350: a plate whose mask accepts no group is passed straight through.
+    # world/step.rs:1327-1351: a plate whose mask accepts no group is passed straight through.
     w = OracleWorld(prec)
     plate, ball = w.box([2.0, 0.5, 2.0]), w.sphere(0.5)
     w.add_body(plate, [0, 0, 0], mass=0, group=DEFAULT, mask=0)
@@ -47,7 +47,7 @@ def test_collision_mask_blocks_pair(prec):
 
 @pytest.mark.parametrize("prec", PRECISIONS)
 def test_collision_group_mask_asymmetric(prec):
-    # world/step.rs:1357-1390: the group / mask test needs both directions. A STATIC-group plate
+    # world/step.rs:1357-1391: the group / mask test needs both directions. A STATIC-group plate
     # that accepts every group is still ignored by a ball whose mask accepts DEFAULT only; once
     # the ball's mask widens to ALL and it is put back above the plate (pose only, its fall
     # velocity kept, as set_body_transform does), it lands and rests on the plate.
@@ -70,7 +70,7 @@ def test_collision_group_mask_asymmetric(prec):
 
 @pytest.mark.parametrize("prec", PRECISIONS)
 def test_disable_simulation_body_takes_solver_impulses_without_integrating(prec):
-    # world/step.rs:1729-1757: a DISABLE_SIMULATION body is in the solve (its velocity takes
+    # world/step.rs:1729-1759: a DISABLE_SIMULATION body is in the solve (its velocity takes
     # the contact impulse) but its pose is never integrated.
     w = OracleWorld(prec)
     w.set_gravity((0, 0, 0))
@@ -87,7 +87,7 @@ def test_disable_simulation_body_takes_solver_impulses_without_integrating(prec)
 
 @pytest.mark.parametrize("prec", PRECISIONS)
 def test_kinematic_pushes_dynamic_body(prec):
-    # world/step.rs:2591-2617: a kinematic slab moving at 2 m/s shoves a resting box along
+    # world/step.rs:2591-2619: a kinematic slab moving at 2 m/s shoves a resting box along
     # (its velocity enters the contact rows), and the box stays awake.
     w = OracleWorld(prec)
     w.set_gravity((0, -10, 0))
@@ -125,7 +125,7 @@ def test_kinematic_ignores_gravity_forces_and_damping(prec):
 
 @pytest.mark.parametrize("prec", PRECISIONS)
 def test_dynamic_body_rests_and_sleeps_on_idle_kinematic_platform(prec):
-    # world/step.rs:2655-2676: a box settles on a resting kinematic platform and goes to sleep
+    # world/step.rs:2655-2675: a box settles on a resting kinematic platform and goes to sleep
     # (idle kinematic contacts do not keep it awake); the platform never moves.
     w = OracleWorld(prec)
     w.set_gravity((0, -10, 0))
@@ -142,7 +142,7 @@ def test_dynamic_body_rests_and_sleeps_on_idle_kinematic_platform(prec):
 
 @pytest.mark.parametrize("prec", PRECISIONS)
 def test_kinematic_static_and_kinematic_kinematic_pairs_are_inert(prec):
-    # world/step.rs:2681-2713: kinematic-kinematic and kinematic-static overlaps produce no
+    # world/step.rs:2681-2711: kinematic-kinematic and kinematic-static overlaps produce no
     # solver rows: both kinematic bodies keep their velocities and stay above the ground.
     w = OracleWorld(prec)
     w.set_gravity((0, -10, 0))
