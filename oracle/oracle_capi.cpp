@@ -727,6 +727,32 @@ uint64_t orc_pairs(int f64, const double* aabbs, uint32_t n, int method, uint32_
     return pr.size();
 }
 
+// ContactManifold::reduce (manifold.rs:80-108) on n points (pos3, normal3, penetration); writes
+// the kept points in the same layout and returns their count.
+uint32_t orc_manifold_reduce(int f64, const double* pts, uint32_t n, uint32_t keep, double* out) {
+    uint32_t k = 0;
+    auto run = [&](auto zero) {
+        using R = decltype(zero);
+        Manifold<R> m;
+        for (uint32_t i = 0; i < n; ++i) {
+            const double* c = pts + 7 * i;
+            m.points.push_back(ContactPoint<R>(V3<R>(static_cast<R>(c[0]), static_cast<R>(c[1]), static_cast<R>(c[2])),
+                                               V3<R>(static_cast<R>(c[3]), static_cast<R>(c[4]), static_cast<R>(c[5])),
+                                               static_cast<R>(c[6])));
+        }
+        reduce_manifold(m, keep);
+        for (auto& cp : m.points) {
+            double* d = out + 7 * k;
+            d[0] = cp.position.x; d[1] = cp.position.y; d[2] = cp.position.z;
+            d[3] = cp.normal.x; d[4] = cp.normal.y; d[5] = cp.normal.z;
+            d[6] = cp.penetration;
+            ++k;
+        }
+    };
+    if (f64) run(0.0); else run(0.0f);
+    return k;
+}
+
 // Persistent manifold handle (float or double).
 struct PmHandle { int f64; PersistentManifold<float> f; PersistentManifold<double> d; };
 

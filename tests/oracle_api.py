@@ -69,6 +69,7 @@ def lib():
             "orc_pm_needs_redetect": (ctypes.c_int, [P, D, D]),
             "orc_pm_set_impulse": (None, [P, U32, ctypes.c_double]),
             "orc_pm_points": (U32, [P, D]),
+            "orc_manifold_reduce": (U32, [ctypes.c_int, D, ctypes.c_uint32, ctypes.c_uint32, D]),
             "orc_interpolate_pose": (None, [ctypes.c_int, D, ctypes.c_double, D]),
             "orc_world_add_joint": (U32, [P, D]),
             "orc_world_set_joint_order": (None, [P, ctypes.POINTER(U32), U32]),
@@ -421,6 +422,14 @@ def oracle_pairs(aabbs, method=0, precision="f32"):
         L.orc_pairs(1 if precision == "f64" else 0, dptr(a), len(a), method,
                     out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), n)
     return out
+
+
+def manifold_reduce(points, keep, precision="f32"):
+    """manifold.rs:80-108 ContactManifold::reduce on rows (pos3, normal3, penetration)."""
+    p = f64(np.asarray(points).reshape(-1, 7))
+    out = np.zeros((max(len(p), 1), 7))
+    n = lib().orc_manifold_reduce(1 if precision == "f64" else 0, dptr(p), len(p), keep, dptr(out))
+    return out[:n]
 
 
 class OracleManifold:
