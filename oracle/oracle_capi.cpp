@@ -172,6 +172,22 @@ int gjk_kind_impl(World<R>& w, uint32_t sa, const double* pa, uint32_t sb, const
     return g.kind;
 }
 
+// gjk.rs:171-288 gjk_contact with the caller's threshold and optional seed; out: distance,
+// normal3, point_on_b3 (the band outcome's fields), the overlap simplex's point count. Returns
+// the outcome kind.
+template <class R>
+int gjk_contact_impl(World<R>& w, uint32_t sa, const double* pa, uint32_t sb, const double* pb, const double* seed,
+                     double threshold, double* out) {
+    const V3<R> sd = seed ? V3<R>(static_cast<R>(seed[0]), static_cast<R>(seed[1]), static_cast<R>(seed[2])) : V3<R>();
+    GjkOutcome<R> g = gjk_contact(w.shapes[sa], v_of<R>(pa), q_of<R>(pa), w.shapes[sb], v_of<R>(pb), q_of<R>(pb),
+                                  seed != nullptr, sd, static_cast<R>(threshold));
+    out[0] = g.distance;
+    out[1] = g.normal.x; out[2] = g.normal.y; out[3] = g.normal.z;
+    out[4] = g.point_on_b.x; out[5] = g.point_on_b.y; out[6] = g.point_on_b.z;
+    out[7] = g.simplex_len;
+    return g.kind;
+}
+
 template <class R>
 void pairs_impl(const double* aabbs, uint32_t n, int method, std::vector<std::pair<uint32_t, uint32_t>>& out) {
     std::vector<Aabb<R>> a(n);
@@ -709,6 +725,14 @@ int orc_gjk_kind(void* p, uint32_t sa, const double* pose_a, uint32_t sb, const 
     Handle* h = static_cast<Handle*>(p);
     int r = 0;
     DISPATCH(h, { r = gjk_kind_impl(w, sa, pose_a, sb, pose_b); });
+    return r;
+}
+
+int orc_gjk_contact(void* p, uint32_t sa, const double* pose_a, uint32_t sb, const double* pose_b, const double* seed,
+                    double threshold, double* out) {
+    Handle* h = static_cast<Handle*>(p);
+    int r = 0;
+    DISPATCH(h, { r = gjk_contact_impl(w, sa, pose_a, sb, pose_b, seed, threshold, out); });
     return r;
 }
 

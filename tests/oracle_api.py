@@ -59,6 +59,7 @@ def lib():
             "orc_world_stage_seconds": (None, [P, D]),
             "orc_collide": (ctypes.c_int, [P, U32, D, U32, D, D, D]),
             "orc_gjk_kind": (ctypes.c_int, [P, U32, D, U32, D]),
+            "orc_gjk_contact": (ctypes.c_int, [P, U32, D, U32, D, D, ctypes.c_double, D]),
             "orc_convex_convex": (ctypes.c_int, [P, U32, D, U32, D, D]),
             "orc_solve_contacts": (None, [P, D, U32, ctypes.c_double, D]),
             "orc_pairs": (ctypes.c_uint64, [ctypes.c_int, D, U32, ctypes.c_int, ctypes.POINTER(U32), ctypes.c_uint64]),
@@ -404,6 +405,14 @@ class OracleWorld:
 
     def gjk_kind(self, sa, pa, sb, pb):
         return self.L.orc_gjk_kind(self.h, sa, dptr(f64(pa)), sb, dptr(f64(pb)))
+
+    def gjk_contact(self, sa, pa, sb, pb, threshold, seed=None):
+        """gjk.rs:171-288: (kind 0 separated / 1 band / 2 overlap, distance, normal, point_on_b,
+        overlap simplex point count)."""
+        out = np.zeros(8)
+        sd = dptr(f64(seed)) if seed is not None else None
+        k = self.L.orc_gjk_contact(self.h, sa, dptr(f64(pa)), sb, dptr(f64(pb)), sd, float(threshold), dptr(out))
+        return k, out[0], out[1:4], out[4:7], int(out[7])
 
     def solve_contacts(self, contacts, inv_dt):
         c = f64(np.asarray(contacts).reshape(-1, 10))
