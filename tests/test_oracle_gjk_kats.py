@@ -167,3 +167,38 @@ def test_gjk_elongated_rod_vs_box_stays_finite(prec):
     k, _, _, _, ns = contact(w, rod, (0, 0, 0), b, (0, 1.45, 0), 0.0173)
     assert k == OVERLAP and ns == 4
     assert contact(w, rod, (0, 0, 0), b, (0, 2.5, 0), 0.0173)[0] == SEPARATED
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_gjk_duplicate_support_gate_across_scales(prec):
+    # gjk.rs:1703-1734: a cube hull (corner supports repeat) against a sphere with a face gap of
+    # 0.01 x scale: a band at that distance from 1e-3 to 1e2.
+    for scale in (1e-3, 1e-2, 1.0, 1e2):
+        w = OracleWorld(prec)
+        e = 0.5 * scale
+        hull = w.hull([[x, y, z] for z in (-e, e) for y in (-e, e) for x in (-e, e)])
+        s = w.sphere(0.5 * scale)
+        k, d, n, *_ = contact(w, hull, (0, 0, 0), s, (1.01 * scale, 0, 0), 0.02 * scale)
+        assert k == BAND, scale
+        assert abs(d - 0.01 * scale) < max(1e-4 * scale, 1e-9), (scale, d)
+        assert np.all(np.isfinite(n)) and abs(n[0]) > 0.999
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_gjk_degenerate_segment_hulls_terminate_finitely(prec):
+    # gjk.rs:1816-1875 (its contact-walk assertions): crossing segments overlap (a full finite
+    # simplex) or touch in the band; parallel segments 2 apart are separated; collinear
+    # overlapping segments end with finite output.
+    w = OracleWorld(prec)
+    sx = w.hull([[-1, 0, 0], [1, 0, 0]])
+    sy = w.hull([[0, -1, 0], [0, 1, 0]])
+    k, d, n, _, ns = contact(w, sx, (0, 0, 0), sy, (0, 0, 0), 0.0173)
+    assert k != SEPARATED
+    if k == OVERLAP:
+        assert ns == 4
+    else:
+        assert abs(d) < 1e-3 and np.all(np.isfinite(n))
+    assert contact(w, sx, (0, 0, 0), sx, (0, 2, 0), 0.0173)[0] == SEPARATED
+    k, d, n, *_ = contact(w, sx, (0, 0, 0), sx, (0.5, 0, 0), 0.0173)
+    if k == BAND:
+        assert np.isfinite(d) and np.all(np.isfinite(n))
