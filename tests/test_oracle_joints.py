@@ -518,3 +518,25 @@ def test_universal_bends_only_about_the_joint_axes(precision, spin, free):  # ge
         assert st[12] > 4.0
     else:
         assert abs(st[11]) < 0.05
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_solver_info_damping_scales_the_joint_row_velocity_term(prec):
+    # solver/sequential_impulse.rs:1645-1677: one iteration of a point-to-point joint between a
+    # moving and a resting sphere; with the solver damping at its default 1.0 the pair ends
+    # closer to a common velocity than at 0.5. (Restated through one world step with gravity
+    # off and the joint's pair suppressed, so only the joint rows act.)
+    def run(damping):
+        w = world(prec, gravity=(0.0, 0.0, 0.0))
+        w.set_solver(num_iterations=1, damping=damping)
+        s = w.add_shape(orc.SPHERE, [0.5])
+        a = w.add_body(s, (-0.5, 0, 0), linvel=(1, 0, 0), mass=1.0)
+        b = w.add_body(s, (0.5, 0, 0), mass=1.0)
+        p2p(w, a, b, (0.5, 0, 0), (-0.5, 0, 0))
+        w.step(DT)
+        st = w.state()
+        return st[a, 7], st[b, 7]
+
+    va1, vb1 = run(1.0)
+    va05, vb05 = run(0.5)
+    assert abs(vb1 - va1) < abs(vb05 - va05)
