@@ -170,6 +170,7 @@ struct World {
     bgpu_step_stats last{};
     bool stats_pending = false;
     float accumulator = 0.0f;  // step_simulation_fixed's m_localTime
+    DevBuf<float4> force_keep;   // a fixed-step call's applied forces, kept for its later substeps
     int solved_standalone = 0;  // 1 after bgpu_solve_contacts (read_contacts reports its groups)
     uint32_t standalone_groups = 0;
     DevBuf<uint64_t> standalone_keys;
@@ -1724,6 +1725,7 @@ bgpu_status bgpu_step(bgpu_world* w, float dt, uint32_t nsteps) {
         return BGPU_ERR_INVALID_ARGUMENT;
     }
     return guarded([&]() -> bgpu_status {
+        w->impl.accumulator = 0.0f;  // step_simulation resets the fixed-step accumulator (step.rs:105)
         for (uint32_t k = 0; k < nsteps; ++k) w->impl.step_once(dt);
         return check_device_status(w->impl);
     });
@@ -1752,12 +1754,21 @@ bgpu_status bgpu_step_timed(bgpu_world* w, float dt, uint32_t nsteps, float* dev
     });
 }
 
-// step.rs:136-199 (fixed-timestep accumulator; motion-state interpolation is not modelled).
+// step.rs:136-199 (fixed-timestep accumulator; motion-state interpolation is not modelled, and the
+// accumulator follows the reference's default latency mode). The forces applied before a call
+// act in every substep of it and are cleared once, after the last one; a call that runs no
+// substep drops them (step.rs:117-121, 160-177).
 bgpu_status bgpu_step_simulation_fixed(bgpu_world* w, float dt, uint32_t max_sub_steps, float fixed_dt,
                                        uint32_t* out_substeps) {
     if (!w || (max_sub_steps != 0 && !(fixed_dt > 0.0f))) return BGPU_ERR_INVALID_ARGUMENT;
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
+        const size_t fbytes = size_t(W.n) * sizeof(float4);
+        auto drop_forces = [&]() {
+            if (!fbytes) return;
+            bgpu::check_cuda(cudaMemsetAsync(W.force.p, 0, fbytes, W.stream), "memset forces");
+            bgpu::check_cuda(cudaMemsetAsync(W.torque.p, 0, fbytes, W.stream), "memset torques");
+        };
         uint32_t num = 0;
         float step_dt = fixed_dt;
         if (max_sub_steps != 0) {
@@ -1769,15 +1780,39 @@ bgpu_status bgpu_step_simulation_fixed(bgpu_world* w, float dt, uint32_t max_sub
             }
         } else {
             step_dt = dt;
-            W.accumulator = dt;  // step.rs:156 (latency interpolation off: the remainder is dt)
+            W.accumulator = 0.0f;  // step.rs:156
             if (std::fabs(dt) <= 1.1920929e-7f) {
+                drop_forces();
                 if (out_substeps) *out_substeps = 0;
                 return BGPU_OK;
             }
             num = 1;
         }
-        uint32_t clamped = max_sub_steps ? std::min(num, max_sub_steps) : num;
-        for (uint32_t k = 0; k < clamped; ++k) W.step_once(step_dt);
+        if (num == 0) {  // a frame without a substep: the applied forces expire
+            drop_forces();
+            if (out_substeps) *out_substeps = 0;
+            return BGPU_OK;
+        }
+        const uint32_t clamped = max_sub_steps ? std::min(num, max_sub_steps) : num;
+        // Each substep's position pass clears the forces, so the call's forces are kept aside
+        // and put back before every later substep.
+        const bool keep = clamped > 1 && fbytes;
+        if (keep) {
+            W.force_keep.reserve(2 * size_t(W.n));
+            bgpu::check_cuda(cudaMemcpyAsync(W.force_keep.p, W.force.p, fbytes, cudaMemcpyDeviceToDevice, W.stream),
+                             "keep forces");
+            bgpu::check_cuda(cudaMemcpyAsync(W.force_keep.p + W.n, W.torque.p, fbytes, cudaMemcpyDeviceToDevice,
+                                             W.stream), "keep torques");
+        }
+        for (uint32_t k = 0; k < clamped; ++k) {
+            if (keep && k > 0) {
+                bgpu::check_cuda(cudaMemcpyAsync(W.force.p, W.force_keep.p, fbytes, cudaMemcpyDeviceToDevice,
+                                                 W.stream), "restore forces");
+                bgpu::check_cuda(cudaMemcpyAsync(W.torque.p, W.force_keep.p + W.n, fbytes, cudaMemcpyDeviceToDevice,
+                                                 W.stream), "restore torques");
+            }
+            W.step_once(step_dt);
+        }
         if (out_substeps) *out_substeps = num;
         return check_device_status(W);
     });
