@@ -13,6 +13,7 @@ namespace {
 
 struct Handle {
     int f64 = 0;
+    double accumulator = 0.0;  // step_simulation_fixed's accumulator (a value of the world's precision)
     std::unique_ptr<World<float>> wf;
     std::unique_ptr<World<double>> wd;
 };
@@ -186,6 +187,53 @@ int gjk_contact_impl(World<R>& w, uint32_t sa, const double* pa, uint32_t sb, co
     out[4] = g.point_on_b.x; out[5] = g.point_on_b.y; out[6] = g.point_on_b.z;
     out[7] = g.simplex_len;
     return g.kind;
+}
+
+// step.rs:136-199 (step_simulation_fixed, the default latency mode, motion states left out): the
+// accumulator, at most max_sub_steps substeps of fixed_dt, the unclamped demand returned; the
+// forces applied before the call act in each substep and are cleared once after the last, and a
+// call without a substep drops them.
+template <class R>
+uint32_t step_fixed_impl(World<R>& w, double& accumulator, double dt, uint32_t max_sub_steps, double fixed_dt) {
+    auto drop = [&]() {
+        for (auto& b : w.bodies) {
+            b.force = V3<R>();
+            b.torque = V3<R>();
+        }
+    };
+    uint32_t num = 0;
+    R step_dt = static_cast<R>(fixed_dt);
+    if (max_sub_steps != 0) {
+        R acc = static_cast<R>(accumulator) + static_cast<R>(dt), fx = static_cast<R>(fixed_dt);
+        if (acc >= fx) {
+            num = uint32_t(acc / fx);
+            acc -= static_cast<R>(num) * fx;
+        }
+        accumulator = acc;
+    } else {
+        step_dt = static_cast<R>(dt);
+        accumulator = 0.0;
+        if (std::fabs(static_cast<R>(dt)) > std::numeric_limits<R>::epsilon()) num = 1;
+    }
+    if (num == 0) {
+        drop();
+        return 0;
+    }
+    const uint32_t clamped = max_sub_steps ? std::min(num, max_sub_steps) : num;
+    std::vector<V3<R>> keep_f, keep_t;
+    for (auto& b : w.bodies) {
+        keep_f.push_back(b.force);
+        keep_t.push_back(b.torque);
+    }
+    for (uint32_t k = 0; k < clamped; ++k) {
+        if (k > 0)
+            for (size_t i = 0; i < w.bodies.size(); ++i) {
+                w.bodies[i].force = keep_f[i];
+                w.bodies[i].torque = keep_t[i];
+            }
+        w.step(step_dt);
+    }
+    return num;
 }
 
 template <class R>
@@ -401,6 +449,13 @@ void orc_world_step(void* p, double dt) {
         using R = std::remove_reference_t<decltype(w.gravity.x)>;
         w.step(static_cast<R>(dt));
     });
+}
+
+uint32_t orc_world_step_fixed(void* p, double dt, uint32_t max_sub_steps, double fixed_dt) {
+    Handle* h = static_cast<Handle*>(p);
+    uint32_t num = 0;
+    DISPATCH(h, { num = step_fixed_impl(w, h->accumulator, dt, max_sub_steps, fixed_dt); });
+    return num;
 }
 
 void orc_world_get_state(void* p, double* out) {

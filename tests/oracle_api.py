@@ -48,6 +48,7 @@ def lib():
             "orc_world_set_state": (None, [P, D]),
             "orc_world_get_push": (None, [P, D]),
             "orc_world_apply_force": (None, [P, ctypes.c_uint32, D, D]),
+            "orc_world_step_fixed": (ctypes.c_uint32, [P, ctypes.c_double, ctypes.c_uint32, ctypes.c_double]),
             "orc_world_set_filter": (None, [P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
             "orc_world_num_pairs": (U32, [P]),
             "orc_world_get_pairs": (None, [P, ctypes.POINTER(U32)]),
@@ -303,6 +304,10 @@ class OracleWorld:
 
     def step(self, dt):
         self.L.orc_world_step(self.h, dt)
+
+    def step_fixed(self, dt, max_sub_steps, fixed_dt):
+        """step.rs:136-199; returns the unclamped substep demand."""
+        return self.L.orc_world_step_fixed(self.h, dt, max_sub_steps, fixed_dt)
 
     def state(self):
         out = np.zeros((self.num_bodies, STATE))
