@@ -157,3 +157,26 @@ def test_kinematic_static_and_kinematic_kinematic_pairs_are_inert(prec):
     assert tuple(st[a, 7:10]) == (0.5, 0.0, 0.0)
     assert tuple(st[b, 7:10]) == (-0.5, 0.0, 0.0)
     assert st[a, 1] > 0.0
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_interpolate_pose_branches(prec):
+    # world/step.rs:3622-3684 (body.rs interpolate_pose): pure translation, the small-angle
+    # Taylor branch, the pi/4 clamp of a large turn, an exact moderate turn, a negative span.
+    import math
+
+    from oracle_api import interpolate_pose
+
+    r = interpolate_pose((1, 2, 3), (0, 0, 0, 1), (10, 0, 0), (0, 0, 0), 0.5, prec)
+    assert r[0] == pytest.approx(6.0, abs=1e-6) and r[6] == pytest.approx(1.0, abs=1e-6)
+    w = 5e-4
+    r = interpolate_pose((0, 0, 0), (0, 0, 0, 1), (0, 0, 0), (w, 0, 0), 1.0, prec)
+    assert r[3] == pytest.approx(0.5 * w, abs=1e-6) and abs(r[6] - 1.0) < 1e-4
+    half_pi = float(np.float32(math.pi / 2)) if prec == "f32" else math.pi / 2
+    r = interpolate_pose((0, 0, 0), (0, 0, 0, 1), (0, 0, 0), (half_pi, 0, 0), 1.0, prec)
+    assert r[3] == pytest.approx(0.6379518, abs=1e-5) and r[6] == pytest.approx(0.7700761, abs=1e-5)
+    r = interpolate_pose((0, 0, 0), (0, 0, 0, 1), (0, 0, 0), (0.5, 0, 0), 1.0, prec)
+    assert r[3] == pytest.approx(math.sin(0.25), abs=1e-5) and r[6] == pytest.approx(math.cos(0.25), abs=1e-5)
+    r = interpolate_pose((0, 1, 0), (0, 0, 0, 1), (2, 0, 0), (0, 0, 0), -1.0 / 128.0, prec)
+    assert r[0] == pytest.approx(-2.0 / 128.0, abs=1e-6) and r[1] == pytest.approx(1.0, abs=1e-6)
+    assert r[6] == pytest.approx(1.0, abs=1e-6)
