@@ -1760,7 +1760,10 @@ bgpu_status bgpu_step_timed(bgpu_world* w, float dt, uint32_t nsteps, float* dev
 // substep drops them (step.rs:117-121, 160-177).
 bgpu_status bgpu_step_simulation_fixed(bgpu_world* w, float dt, uint32_t max_sub_steps, float fixed_dt,
                                        uint32_t* out_substeps) {
-    if (!w || (max_sub_steps != 0 && !(fixed_dt > 0.0f))) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || (max_sub_steps != 0 && !(fixed_dt > 0.0f))) {
+        bgpu::g_last_error = "bgpu_step_simulation_fixed: world is NULL or fixed_dt <= 0 with substeps";
+        return BGPU_ERR_INVALID_ARGUMENT;
+    }
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         const size_t fbytes = size_t(W.n) * sizeof(float4);
