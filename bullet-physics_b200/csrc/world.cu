@@ -1337,6 +1337,13 @@ bgpu_status guarded(F&& f) {
     }
 }
 
+// A rejected argument (NULL where data is required, or out of range): the status, with the
+// message bgpu_last_error reports.
+bgpu_status bad_args(const char* fn) {
+    bgpu::g_last_error = std::string(fn) + ": a required argument is NULL or out of range";
+    return BGPU_ERR_INVALID_ARGUMENT;
+}
+
 bgpu_status check_device_status(World& w) {
     w.finish_stats();
     if (w.last.device_status) {
@@ -1518,7 +1525,7 @@ bgpu_status bgpu_world_create(const bgpu_solver_info* info, const float* gravity
 void bgpu_world_destroy(bgpu_world* w) { delete w; }
 
 bgpu_status bgpu_world_set_gravity(bgpu_world* w, const float* g) {
-    if (!w || !g) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || !g) return bad_args("bgpu_world_set_gravity");
     return guarded([&]() -> bgpu_status {
         w->impl.set_gravity(g);
         return BGPU_OK;
@@ -1526,14 +1533,14 @@ bgpu_status bgpu_world_set_gravity(bgpu_world* w, const float* g) {
 }
 
 bgpu_status bgpu_world_set_solver_info(bgpu_world* w, const bgpu_solver_info* info) {
-    if (!w || !info) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || !info) return bad_args("bgpu_world_set_solver_info");
     copy_info(w->impl.info, *info);
     return BGPU_OK;
 }
 
 bgpu_status bgpu_add_shape(bgpu_world* w, uint32_t type, const float* params, const float* pts, uint32_t npts,
                            uint32_t* out) {
-    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w) return bad_args("bgpu_add_shape");
     return guarded([&]() -> bgpu_status {
         uint32_t id = w->impl.add_shape(type, params, pts, npts);
         if (out) *out = id;
@@ -1543,7 +1550,7 @@ bgpu_status bgpu_add_shape(bgpu_world* w, uint32_t type, const float* params, co
 
 bgpu_status bgpu_add_mesh_shape(bgpu_world* w, const float* vertices, uint32_t nverts, const uint32_t* indices,
                                 uint32_t ntris, uint32_t* out) {
-    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w) return bad_args("bgpu_add_mesh_shape");
     return guarded([&]() -> bgpu_status {
         uint32_t id = w->impl.add_mesh(vertices, nverts, indices, ntris);
         if (out) *out = id;
@@ -1553,7 +1560,7 @@ bgpu_status bgpu_add_mesh_shape(bgpu_world* w, const float* vertices, uint32_t n
 
 bgpu_status bgpu_add_heightfield_shape(bgpu_world* w, const float* heights, uint32_t width, uint32_t depth,
                                        const float* cell_size, uint32_t options, uint32_t* out) {
-    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w) return bad_args("bgpu_add_heightfield_shape");
     return guarded([&]() -> bgpu_status {
         uint32_t id = w->impl.add_heightfield(heights, width, depth, cell_size, options);
         if (out) *out = id;
@@ -1562,7 +1569,7 @@ bgpu_status bgpu_add_heightfield_shape(bgpu_world* w, const float* heights, uint
 }
 
 bgpu_status bgpu_add_bodies(bgpu_world* w, uint32_t n, const bgpu_body_desc* d, uint32_t* out_first) {
-    if (!w || (n && !d)) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || (n && !d)) return bad_args("bgpu_add_bodies");
     return guarded([&]() -> bgpu_status {
         w->impl.finish_stats();
         uint32_t f = w->impl.add_bodies(n, d);
@@ -1665,7 +1672,7 @@ bgpu_status bgpu_tape_rewind(bgpu_tape* t) {
 }
 
 bgpu_status bgpu_tape_timing(const bgpu_tape* t, float* forward_ms, float* backward_ms) {
-    if (!t) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!t) return bad_args("bgpu_tape_timing");
     if (forward_ms) *forward_ms = t->impl->forward_ms;
     if (backward_ms) *backward_ms = t->impl->backward_ms;
     return BGPU_OK;
@@ -1674,7 +1681,7 @@ bgpu_status bgpu_tape_timing(const bgpu_tape* t, float* forward_ms, float* backw
 uint32_t bgpu_batch_num_worlds(const bgpu_world* w) { return (w && w->impl.batch) ? w->impl.num_worlds() : 0u; }
 
 bgpu_status bgpu_batch_autotune(bgpu_world* w, float dt, uint32_t steps_per_candidate, bgpu_batch_tuning* out) {
-    if (!w || !(dt > 0.0f)) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || !(dt > 0.0f)) return bad_args("bgpu_batch_autotune");
     bgpu_status st = guarded([&]() -> bgpu_status {
         bgpu::autotune_batch(w->impl, dt, steps_per_candidate);
         return BGPU_OK;
@@ -1684,7 +1691,7 @@ bgpu_status bgpu_batch_autotune(bgpu_world* w, float dt, uint32_t steps_per_cand
 }
 
 bgpu_status bgpu_batch_set_tuning(bgpu_world* w, uint32_t threads_per_cta, uint32_t warp_world_max_bodies) {
-    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w) return bad_args("bgpu_batch_set_tuning");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         if (!W.batch) throw bgpu::InvalidArg{"bgpu_batch_set_tuning needs a batched world"};
@@ -1699,7 +1706,7 @@ bgpu_status bgpu_batch_set_tuning(bgpu_world* w, uint32_t threads_per_cta, uint3
 }
 
 bgpu_status bgpu_batch_get_tuning(bgpu_world* w, bgpu_batch_tuning* out) {
-    if (!w || !out) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || !out) return bad_args("bgpu_batch_get_tuning");
     World& W = w->impl;
     out->threads_per_cta = W.wplan_block;
     out->warp_world_max_bodies = W.wplan_tau;
@@ -1822,7 +1829,7 @@ bgpu_status bgpu_step_simulation_fixed(bgpu_world* w, float dt, uint32_t max_sub
 }
 
 bgpu_status bgpu_read_state(bgpu_world* w, float* state) {
-    if (!w || !state) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || !state) return bad_args("bgpu_read_state");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         uint32_t n = W.n;
@@ -1850,7 +1857,7 @@ bgpu_status bgpu_read_state(bgpu_world* w, float* state) {
 }
 
 bgpu_status bgpu_write_state(bgpu_world* w, const float* state) {
-    if (!w || !state) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || !state) return bad_args("bgpu_write_state");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         W.finish_stats();
@@ -1882,7 +1889,7 @@ bgpu_status bgpu_write_state(bgpu_world* w, const float* state) {
 }
 
 bgpu_status bgpu_read_poses(bgpu_world* w, float* poses) {
-    if (!w || !poses) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || !poses) return bad_args("bgpu_read_poses");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         uint32_t n = W.n;
@@ -1899,7 +1906,7 @@ bgpu_status bgpu_read_poses(bgpu_world* w, float* poses) {
 }
 
 bgpu_status bgpu_apply_forces(bgpu_world* w, const float* force, const float* torque) {
-    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w) return bad_args("bgpu_apply_forces");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         uint32_t n = W.n;
@@ -1922,7 +1929,7 @@ bgpu_status bgpu_apply_forces(bgpu_world* w, const float* force, const float* to
 }
 
 bgpu_status bgpu_read_pairs(bgpu_world* w, uint32_t* out, uint64_t cap, uint64_t* out_n) {
-    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w) return bad_args("bgpu_read_pairs");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         W.finish_stats();
@@ -1989,7 +1996,7 @@ static void gather_solve_order(World& W, uint32_t ngroups, const uint64_t* keys_
 }
 
 bgpu_status bgpu_read_contacts(bgpu_world* w, float* out, uint64_t cap, uint64_t* out_n) {
-    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w) return bad_args("bgpu_read_contacts");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         W.finish_stats();
@@ -2006,7 +2013,7 @@ bgpu_status bgpu_read_contacts(bgpu_world* w, float* out, uint64_t cap, uint64_t
 }
 
 bgpu_status bgpu_read_solve_order(bgpu_world* w, uint64_t* out, uint64_t cap, uint64_t* out_n) {
-    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w) return bad_args("bgpu_read_solve_order");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         W.finish_stats();
@@ -2063,7 +2070,7 @@ bgpu::V3 euler_xyz_host(const bgpu::M3& m) {
 bgpu_status bgpu_spring2_hinge2(const float* pos_a, const float* quat_a, const float* pos_b, const float* quat_b,
                                 const float* anchor, const float* axis1, const float* axis2, uint32_t body_a,
                                 uint32_t body_b, bgpu_spring2_desc* out) {
-    if (!pos_a || !quat_a || !pos_b || !quat_b || !anchor || !axis1 || !axis2 || !out) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!pos_a || !quat_a || !pos_b || !quat_b || !anchor || !axis1 || !axis2 || !out) return bad_args("bgpu_spring2_hinge2");
     using bgpu::V3;
     using bgpu::M3;
     const V3 pa{pos_a[0], pos_a[1], pos_a[2]}, pb{pos_b[0], pos_b[1], pos_b[2]}, an{anchor[0], anchor[1], anchor[2]};
@@ -2112,7 +2119,7 @@ bgpu_status bgpu_spring2_hinge2(const float* pos_a, const float* quat_a, const f
 }
 
 bgpu_status bgpu_add_spring2_joints(bgpu_world* w, uint32_t n, const bgpu_spring2_desc* d, uint32_t* first_id) {
-    if (!w || (n && !d)) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || (n && !d)) return bad_args("bgpu_add_spring2_joints");
     return guarded([&]() -> bgpu_status {
         uint32_t f = w->impl.add_spring2_joints(n, d);
         if (first_id) *first_id = f;
@@ -2121,7 +2128,7 @@ bgpu_status bgpu_add_spring2_joints(bgpu_world* w, uint32_t n, const bgpu_spring
 }
 
 bgpu_status bgpu_add_generic6dof_joints(bgpu_world* w, uint32_t n, const bgpu_spring2_desc* d, uint32_t* first_id) {
-    if (!w || (n && !d)) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || (n && !d)) return bad_args("bgpu_add_generic6dof_joints");
     return guarded([&]() -> bgpu_status {
         uint32_t f = w->impl.add_spring2_joints(n, d, BGPU_JOINT_GENERIC6DOF);
         if (first_id) *first_id = f;
@@ -2132,7 +2139,7 @@ bgpu_status bgpu_add_generic6dof_joints(bgpu_world* w, uint32_t n, const bgpu_sp
 bgpu_status bgpu_generic6dof_universal(const float* pos_a, const float* quat_a, const float* pos_b, const float* quat_b,
                                        const float* anchor, const float* axis1, const float* axis2, uint32_t body_a,
                                        uint32_t body_b, bgpu_spring2_desc* out) {
-    if (!pos_a || !quat_a || !pos_b || !quat_b || !anchor || !axis1 || !axis2 || !out) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!pos_a || !quat_a || !pos_b || !quat_b || !anchor || !axis1 || !axis2 || !out) return bad_args("bgpu_generic6dof_universal");
     using bgpu::V3;
     using bgpu::M3;
     const V3 pa{pos_a[0], pos_a[1], pos_a[2]}, pb{pos_b[0], pos_b[1], pos_b[2]}, an{anchor[0], anchor[1], anchor[2]};
@@ -2167,7 +2174,7 @@ bgpu_status bgpu_generic6dof_universal(const float* pos_a, const float* quat_a, 
 }
 
 bgpu_status bgpu_read_joint_spring2_state(bgpu_world* w, float* state) {
-    if (!w || !state) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || !state) return bad_args("bgpu_read_joint_spring2_state");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         const size_t nj = W.joints_h.size();
@@ -2181,7 +2188,7 @@ bgpu_status bgpu_read_joint_spring2_state(bgpu_world* w, float* state) {
 
 bgpu_status bgpu_set_ccd(bgpu_world* w, uint32_t first, uint32_t n, const float* motion_threshold,
                          const float* swept_sphere_radius) {
-    if (!w || (n && (!motion_threshold || !swept_sphere_radius))) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || (n && (!motion_threshold || !swept_sphere_radius))) return bad_args("bgpu_set_ccd");
     return guarded([&]() -> bgpu_status {
         w->impl.set_ccd(first, n, motion_threshold, swept_sphere_radius);
         return BGPU_OK;
@@ -2189,7 +2196,7 @@ bgpu_status bgpu_set_ccd(bgpu_world* w, uint32_t first, uint32_t n, const float*
 }
 
 bgpu_status bgpu_read_ccd_clamps(bgpu_world* w, float* clamps) {
-    if (!w || !clamps) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || !clamps) return bad_args("bgpu_read_ccd_clamps");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         for (uint32_t i = 0; i < W.n; ++i) clamps[i] = 1.0f;
@@ -2204,7 +2211,7 @@ bgpu_status bgpu_read_ccd_clamps(bgpu_world* w, float* clamps) {
 }
 
 bgpu_status bgpu_add_joints(bgpu_world* w, uint32_t n, const bgpu_joint_desc* d, uint32_t* first_id) {
-    if (!w || (n && !d)) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || (n && !d)) return bad_args("bgpu_add_joints");
     return guarded([&]() -> bgpu_status {
         uint32_t f = w->impl.add_joints(n, d);
         if (first_id) *first_id = f;
@@ -2215,7 +2222,7 @@ bgpu_status bgpu_add_joints(bgpu_world* w, uint32_t n, const bgpu_joint_desc* d,
 uint32_t bgpu_num_joints(bgpu_world* w) { return w ? uint32_t(w->impl.joints_h.size()) : 0u; }
 
 bgpu_status bgpu_read_joint_angles(bgpu_world* w, float* angles) {
-    if (!w || !angles) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || !angles) return bad_args("bgpu_read_joint_angles");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         const size_t nj = W.joints_h.size();
@@ -2228,7 +2235,7 @@ bgpu_status bgpu_read_joint_angles(bgpu_world* w, float* angles) {
 }
 
 bgpu_status bgpu_read_joint_positions(bgpu_world* w, float* positions) {
-    if (!w || !positions) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || !positions) return bad_args("bgpu_read_joint_positions");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         const size_t nj = W.joints_h.size();
@@ -2241,7 +2248,7 @@ bgpu_status bgpu_read_joint_positions(bgpu_world* w, float* positions) {
 }
 
 bgpu_status bgpu_read_joint_order(bgpu_world* w, uint32_t* ids, uint32_t cap, uint32_t* out_n) {
-    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w) return bad_args("bgpu_read_joint_order");
     const auto& o = w->impl.joint_order_h;
     if (out_n) *out_n = uint32_t(o.size());
     const uint32_t k = std::min<uint32_t>(cap, uint32_t(o.size()));
@@ -2250,7 +2257,7 @@ bgpu_status bgpu_read_joint_order(bgpu_world* w, uint32_t* ids, uint32_t cap, ui
 }
 
 bgpu_status bgpu_read_joint_rows(bgpu_world* w, float* rows, uint32_t cap, uint32_t* out_n) {
-    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w) return bad_args("bgpu_read_joint_rows");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         W.finish_stats();
@@ -2283,7 +2290,7 @@ bgpu_status bgpu_read_joint_rows(bgpu_world* w, float* rows, uint32_t cap, uint3
 
 bgpu_status bgpu_read_colour_batches(bgpu_world* w, uint32_t* groups, uint32_t* split_groups, uint32_t cap,
                                      uint32_t* out_n) {
-    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w) return bad_args("bgpu_read_colour_batches");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         W.finish_stats();
@@ -2324,7 +2331,7 @@ bgpu_status bgpu_read_colour_batches(bgpu_world* w, uint32_t* groups, uint32_t* 
 }
 
 bgpu_status bgpu_get_stats(bgpu_world* w, bgpu_step_stats* out) {
-    if (!w || !out) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || !out) return bad_args("bgpu_get_stats");
     return guarded([&]() -> bgpu_status {
         w->impl.finish_stats();
         *out = w->impl.last;
@@ -2333,7 +2340,7 @@ bgpu_status bgpu_get_stats(bgpu_world* w, bgpu_step_stats* out) {
 }
 
 bgpu_status bgpu_enable_step_timing(bgpu_world* w, int on) {
-    if (!w) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w) return bad_args("bgpu_enable_step_timing");
     return guarded([&]() -> bgpu_status {
         w->impl.finish_stats();
         w->impl.timing = on != 0;
@@ -2343,7 +2350,7 @@ bgpu_status bgpu_enable_step_timing(bgpu_world* w, int on) {
 }
 
 bgpu_status bgpu_broadphase_pairs(const float* aabbs, uint32_t n, uint32_t* out, uint64_t cap, uint64_t* out_n) {
-    if (!aabbs && n) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!aabbs && n) return bad_args("bgpu_broadphase_pairs");
     if (bgpu_device_count() == 0) {
         bgpu::g_last_error = "no CUDA device";
         return BGPU_ERR_NO_DEVICE;
@@ -2403,7 +2410,7 @@ bgpu_status bgpu_broadphase_pairs(const float* aabbs, uint32_t n, uint32_t* out,
 
 bgpu_status bgpu_collide(bgpu_world* w, uint32_t n, const uint32_t* sa, const float* pa, const uint32_t* sb,
                          const float* pb, const float* seeds, int force_convex, float* out, uint32_t* counts) {
-    if (!w || (n && (!sa || !pa || !sb || !pb || !out || !counts))) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || (n && (!sa || !pa || !sb || !pb || !out || !counts))) return bad_args("bgpu_collide");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         for (uint32_t i = 0; i < n; ++i)
@@ -2465,7 +2472,7 @@ bgpu_status bgpu_collide(bgpu_world* w, uint32_t n, const uint32_t* sa, const fl
 
 bgpu_status bgpu_solve_contacts(bgpu_world* w, uint32_t n, const float* contacts, float inv_dt, float* rows_out,
                                 uint64_t* order_keys_out) {
-    if (!w || (n && !contacts) || !(inv_dt > 0.0f)) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || (n && !contacts) || !(inv_dt > 0.0f)) return bad_args("bgpu_solve_contacts");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         W.finish_stats();
@@ -2534,7 +2541,7 @@ bgpu_status bgpu_solve_contacts(bgpu_world* w, uint32_t n, const float* contacts
 }
 
 bgpu_status bgpu_read_push(bgpu_world* w, float* out) {
-    if (!w || !out) return BGPU_ERR_INVALID_ARGUMENT;
+    if (!w || !out) return bad_args("bgpu_read_push");
     return guarded([&]() -> bgpu_status {
         World& W = w->impl;
         uint32_t n = W.n;
