@@ -81,3 +81,13 @@ def test_set_device_takes_a_visible_ordinal(gpu):
     w.step(1.0 / 60.0)
     assert w.stats()["device_status"] == 0
     w.close()
+
+
+def test_rejected_arguments_say_why(bgpu_mod):
+    """A NULL world or buffer is rejected before any CUDA call, with a message naming the call
+    (no stale message from an earlier failure)."""
+    L = bgpu_mod.lib()
+    assert L.bgpu_world_set_gravity(None, None) == 1
+    assert "bgpu_world_set_gravity" in bgpu_mod.last_error()
+    assert L.bgpu_read_state(None, None) == 1
+    assert "bgpu_read_state" in bgpu_mod.last_error()
