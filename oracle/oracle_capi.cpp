@@ -35,7 +35,7 @@ Shape<R> make_shape(uint32_t type, const double* p, const double* pts, uint32_t 
 
 // Body descriptor layout (doubles), shared with tests/oracle_api.py:
 //  0 shape, 1-3 pos, 4-7 quat xyzw, 8-10 linvel, 11-13 angvel, 14 mass (0 = static),
-//  15 friction, 16 restitution, 17 flags, 18 group, 19 mask, 20 lin damping,
+//  15 friction, 16 restitution, 17 flags (| 0x10: additional damping), 18 group, 19 mask, 20 lin damping,
 //  21 ang damping, 22 activation override (0 = default), 23 kinematic (0/1)
 constexpr int DESC = 24;
 
@@ -70,6 +70,9 @@ uint32_t add_body(World<R>& w, const double* d) {
         b.linear_damping = static_cast<R>(d[20]);
         b.angular_damping = static_cast<R>(d[21]);
     }
+    // Flag bit 0x10 (not a collision flag): the additional_damping(true) builder (body.rs:1066-1105).
+    b.additional_damping = (b.flags & 0x10u) != 0;
+    b.flags &= ~0x10u;
     if (d[22] != 0) b.activation = uint32_t(d[22]);
     return w.add_body(b);
 }

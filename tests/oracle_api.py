@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(ROOT, "oracle", "liboracle.so")
 SPHERE, BOX, CAPSULE, HULL, PLANE, MESH = 0, 1, 2, 3, 4, 5
 ACTIVE, ISLAND_SLEEPING, WANTS_DEACTIVATION, DISABLE_DEACTIVATION, DISABLE_SIMULATION = 1, 2, 3, 4, 5
 NO_CONTACT_RESPONSE, DISABLE_WORLD_GRAVITY, KINEMATIC = 0x1, 0x2, 0x4
+ADDITIONAL_DAMPING = 0x10  # the additional_damping(true) builder (the library's body flag of that name)
 
 DESC = 24   # body descriptor doubles (oracle_capi.cpp)
 STATE = 15  # body state doubles

@@ -137,3 +137,16 @@ def test_kinematic_static_and_kinematic_kinematic_pairs_are_inert(gpu):
     assert tuple(st[1, 7:10]) == (0.5, 0.0, 0.0)
     assert tuple(st[2, 7:10]) == (-0.5, 0.0, 0.0)
     assert st[1, 1] > 0.0
+
+
+def test_additional_damping_shrinks_low_speeds(gpu):
+    # body.rs:1347-1400 (additional damping): the scale block below the thresholds and the
+    # 0.005 subtraction under the damping factors, in lockstep with the oracle.
+    w, o = _both((0.0, 0.0, 0.0))
+    for x in (w, o):
+        s = x.sphere(0.5)
+        x.add_body(s, (0, 0, 0), linvel=(0.05, 0, 0), angvel=(0, 0.02, 0), mass=1.0, flags=orc.ADDITIONAL_DAMPING)
+        x.add_body(s, (5, 0, 0), linvel=(0.04, 0, 0), angvel=(0, 0, 0.15), mass=1.0, flags=orc.ADDITIONAL_DAMPING,
+                   lin_damping=0.2, ang_damping=0.2)
+    st = _lockstep(w, o, 10)
+    assert st[0, 7] < 0.05 * 0.005 + 1e-9
