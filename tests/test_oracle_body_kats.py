@@ -61,3 +61,16 @@ def test_additional_damping_subtract_block_follows_the_upstream_quirk(prec):
     o, b = lone(prec, (0.002, 0, 0), (0, 0, 0), flags=ADDITIONAL_DAMPING, ld=0.2, ad=0.2)
     o.step(DT)
     np.testing.assert_array_equal(o.state()[b, 7:10], [0.0, 0.0, 0.0])
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_disable_deactivation_never_sleeps(prec):
+    # body.rs:1229-1238: ten seconds at rest leave a DisableDeactivation body in that state.
+    from oracle_api import DISABLE_DEACTIVATION
+
+    o = OracleWorld(prec)
+    o.set_gravity((0, 0, 0))
+    b = o.add_body(o.sphere(0.5), [0, 0, 0], mass=1.0, activation=DISABLE_DEACTIVATION)
+    for _ in range(600):
+        o.step(DT)
+    assert int(o.state()[b, 13]) == DISABLE_DEACTIVATION
