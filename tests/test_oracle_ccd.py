@@ -162,3 +162,19 @@ def test_ccd_clamps_against_every_convex_target(precision, shape):
     w.set_ccd(ball, 0.1, 0.3)
     w.step(DT)
     assert abs(w.state()[ball, 1] - 0.9) <= 0.05
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_ccd_extreme_timestep_stays_finite(precision):  # :2360-2391
+    # dt = 1e-4 moves the ball 0.012, under the 0.1 threshold: plain integration. dt = 0.5 moves
+    # it 60: the sweep clamps it at the wall.
+    w, _, ball = wall_and_ball(precision)
+    w.step(1e-4)
+    st = w.state()[ball]
+    assert np.all(np.isfinite(st[:13]))
+    assert abs(st[1] - (1.0 - 120.0 * 1e-4)) <= 1e-5
+    w, _, ball = wall_and_ball(precision)
+    w.step(0.5)
+    st = w.state()[ball]
+    assert np.all(np.isfinite(st[:13]))
+    assert abs(st[1] - 0.9) <= 0.05
