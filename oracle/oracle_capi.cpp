@@ -646,6 +646,17 @@ uint32_t orc_world_add_joint(void* p, const double* d) {
     return r;
 }
 
+// Constraint::set_enabled / set_disable_collisions between steps (constraint.rs:637-652): flag bit 1
+// suppresses the pair's collisions, bit 2 disables the joint's rows.
+void orc_world_set_joint_flags(void* p, uint32_t j, uint32_t flags) {
+    Handle* h = static_cast<Handle*>(p);
+    DISPATCH(h, {
+        auto& jt = w.joints.at(j);
+        jt.disable_collisions = (flags & 1u) != 0;
+        jt.enabled = (flags & 2u) == 0;
+    });
+}
+
 void orc_world_set_joint_order(void* p, const uint32_t* ids, uint32_t n) {
     Handle* h = static_cast<Handle*>(p);
     DISPATCH(h, { w.joint_order.assign(ids, ids + n); });

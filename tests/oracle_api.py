@@ -76,6 +76,7 @@ def lib():
             "orc_interpolate_pose": (None, [ctypes.c_int, D, ctypes.c_double, D]),
             "orc_world_add_joint": (U32, [P, D]),
             "orc_world_set_joint_order": (None, [P, ctypes.POINTER(U32), U32]),
+            "orc_world_set_joint_flags": (None, [P, U32, U32]),
             "orc_world_joint_angles": (None, [P, D]),
             "orc_world_joint_positions": (None, [P, D]),
             "orc_world_num_joint_rows": (U32, [P]),
@@ -358,6 +359,10 @@ class OracleWorld:
 
     def add_joint(self, desc):
         return self.L.orc_world_add_joint(self.h, dptr(f64(desc)))
+
+    def set_joint_flags(self, j, flags):
+        """JF_DISABLE_COLLISIONS / JF_DISABLED of joint j, between steps."""
+        self.L.orc_world_set_joint_flags(self.h, int(j), int(flags))
 
     def set_joint_order(self, ids):
         a = np.ascontiguousarray(ids, dtype=np.uint32)

@@ -180,3 +180,51 @@ def test_interpolate_pose_branches(prec):
     r = interpolate_pose((0, 1, 0), (0, 0, 0, 1), (2, 0, 0), (0, 0, 0), -1.0 / 128.0, prec)
     assert r[0] == pytest.approx(-2.0 / 128.0, abs=1e-6) and r[1] == pytest.approx(1.0, abs=1e-6)
     assert r[6] == pytest.approx(1.0, abs=1e-6)
+
+
+def _suppression_world(prec, suppress):
+    # world/step.rs:1767-1872's scene: a sphere A that never sleeps, a static sphere B 0.75 away,
+    # and a disabled point-to-point joint between them whose only effect is the suppression.
+    from oracle_api import JF_DISABLE_COLLISIONS, JF_DISABLED, JOINT_POINT2POINT, frame, joint_desc
+
+    w = OracleWorld(prec)
+    w.set_gravity((0, 0, 0))
+    s = w.sphere(0.5)
+    a = w.add_body(s, [0, 0, 0], mass=1.0, activation=DISABLE_DEACTIVATION)
+    b = w.add_body(s, [0.75, 0, 0], mass=0)
+    flags = JF_DISABLED | (JF_DISABLE_COLLISIONS if suppress else 0)
+    j = w.add_joint(joint_desc(JOINT_POINT2POINT, a, b, frame([0, 0, 0]), frame([0, 0, 0]), flags=flags))
+    return w, a, j
+
+
+def _charge_and_run(w, a):
+    st = w.state()
+    st[a, 0:3] = [0.0, 0.0, 0.0]
+    st[a, 7:10] = [3.0, 0.0, 0.0]
+    w.set_state(st)
+    for _ in range(90):
+        w.step(DT)
+    return w.state()[a, 0]
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_constraint_suppression_flips_take_effect_next_step(prec):
+    # world/step.rs:1767-1838: suppression set at build lets A pass through B; cleared between
+    # steps, A is stopped; the other way round likewise.
+    from oracle_api import JF_DISABLE_COLLISIONS, JF_DISABLED
+
+    w, a, j = _suppression_world(prec, True)
+    assert _charge_and_run(w, a) > 1.5
+    w.set_joint_flags(j, JF_DISABLED)
+    assert _charge_and_run(w, a) < 1.5
+    w, a, j = _suppression_world(prec, False)
+    assert _charge_and_run(w, a) < 1.5
+    w.set_joint_flags(j, JF_DISABLED | JF_DISABLE_COLLISIONS)
+    assert _charge_and_run(w, a) > 1.5
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_disabled_constraint_still_suppresses_collisions(prec):
+    # world/step.rs:1844-1872
+    w, a, _ = _suppression_world(prec, True)
+    assert _charge_and_run(w, a) > 1.5
