@@ -322,6 +322,7 @@ def lib():
             "bgpu_set_ccd": (S, [P, U32, U32, F, F]),
             "bgpu_read_ccd_clamps": (S, [P, F]),
             "bgpu_num_joints": (U32, [P]),
+            "bgpu_set_joint_flags": (S, [P, U32, U32]),
             "bgpu_read_joint_angles": (S, [P, F]),
             "bgpu_read_joint_positions": (S, [P, F]),
             "bgpu_read_joint_order": (S, [P, U32P, U32, U32P]),
@@ -697,6 +698,10 @@ class World:
     @property
     def num_joints(self):
         return self.L.bgpu_num_joints(self.h)
+
+    def set_joint_flags(self, joint, flags):
+        """Joint `joint`'s JOINT_DISABLE_COLLISIONS / JOINT_DISABLED bits, from the next step on."""
+        check(self.L.bgpu_set_joint_flags(self.h, int(joint), int(flags)), "set_joint_flags")
 
     def spring2_state(self):
         """Per joint: Euler angles (3), pivot offset in frame A (3), fact_a, has_static_body."""

@@ -800,7 +800,13 @@ struct World {
                                    stream), "upload joint order");
         check_cuda(cudaMemcpyAsync(joint_coff_d.p, joint_coff_h.data(), (ncol + 1) * sizeof(uint32_t),
                                    cudaMemcpyHostToDevice, stream), "upload joint colours");
-        // world.rs:873-880: suppressed pairs (independent of enabled)
+        upload_suppressed();
+        return first;
+    }
+
+    // world.rs:873-880: the pairs a joint keeps from colliding (independent of enabled), sorted.
+    // Synchronises the stream (the keys are pageable host memory).
+    void upload_suppressed() {
         std::vector<uint64_t> keys;
         for (const auto& x : joints_h)
             if (x.flags & BGPU_JOINT_DISABLE_COLLISIONS) {
@@ -816,7 +822,20 @@ struct World {
                                        cudaMemcpyHostToDevice, stream), "upload suppressed pairs");
         }
         check_cuda(cudaStreamSynchronize(stream), "sync");
-        return first;
+    }
+
+    // Constraint::set_enabled / set_disable_collisions between steps (constraint.rs:637-652): the
+    // two bits change in the joint's device descriptor (read by every step's joint rows and island
+    // links) and in the suppressed pair list (read by every step's pair pass and CCD sweep).
+    void set_joint_flags(uint32_t id, uint32_t flags) {
+        if (id >= joints_h.size()) throw InvalidArg{"bgpu_set_joint_flags: no joint with that id"};
+        const uint32_t bits = BGPU_JOINT_DISABLE_COLLISIONS | BGPU_JOINT_DISABLED;
+        if (flags & ~bits) throw InvalidArg{"bgpu_set_joint_flags: only DISABLE_COLLISIONS and DISABLED change"};
+        joints_h[id].flags = (joints_h[id].flags & ~bits) | flags;
+        const float word = __uint_as_float_host(joints_h[id].flags);
+        check_cuda(cudaMemcpyAsync(&joint_desc_d.p[size_t(id) * JOINT_F4].w, &word, sizeof(float),
+                                   cudaMemcpyHostToDevice, stream), "upload joint flags");
+        upload_suppressed();  // synchronises, so `word` outlives the copy
     }
 
     void set_gravity(const float* g) {
@@ -2220,6 +2239,14 @@ bgpu_status bgpu_add_joints(bgpu_world* w, uint32_t n, const bgpu_joint_desc* d,
 }
 
 uint32_t bgpu_num_joints(bgpu_world* w) { return w ? uint32_t(w->impl.joints_h.size()) : 0u; }
+
+bgpu_status bgpu_set_joint_flags(bgpu_world* w, uint32_t id, uint32_t flags) {
+    if (!w) return bad_args("bgpu_set_joint_flags");
+    return guarded([&]() -> bgpu_status {
+        w->impl.set_joint_flags(id, flags);
+        return BGPU_OK;
+    });
+}
 
 bgpu_status bgpu_read_joint_angles(bgpu_world* w, float* angles) {
     if (!w || !angles) return bad_args("bgpu_read_joint_angles");

@@ -416,6 +416,10 @@ bgpu_status bgpu_generic6dof_universal(const float* pos_a, const float* quat_a, 
 /* Spring-2 joints (Constraint::generic_6dof_spring2), in the same id space as bgpu_add_joints. */
 bgpu_status bgpu_add_spring2_joints(bgpu_world* w, uint32_t n, const bgpu_spring2_desc* d, uint32_t* first_id);
 uint32_t bgpu_num_joints(bgpu_world* w);
+/* Constraint::set_enabled / set_disable_collisions between steps (constraint.rs:637-652):
+ * sets joint `id`'s BGPU_JOINT_DISABLE_COLLISIONS and BGPU_JOINT_DISABLED bits to `flags`
+ * (any other bit is rejected); the next step uses them. Synchronises the world's stream. */
+bgpu_status bgpu_set_joint_flags(bgpu_world* w, uint32_t id, uint32_t flags);
 /* Per joint, 8 floats of the last step that built its rows (spring-2 joints; 0 for the other
  * kinds): the relative Euler angles (get_angle 0-2), the pivot offset in frame A
  * (get_relative_pivot_position 0-2), fact_a and has_static_body (0 or 1). */

@@ -150,3 +150,31 @@ def test_additional_damping_shrinks_low_speeds(gpu):
                    lin_damping=0.2, ang_damping=0.2)
     st = _lockstep(w, o, 10)
     assert st[0, 7] < 0.05 * 0.005 + 1e-9
+
+
+def test_constraint_suppression_flips_take_effect_next_step(gpu):
+    # world/step.rs:1767-1838: suppression of a disabled joint's pair set at build and flipped
+    # between steps (bgpu_set_joint_flags), in lockstep with the oracle.
+    for suppress in (True, False):
+        w, o = _both((0.0, 0.0, 0.0))
+        flags = orc.JF_DISABLED | (orc.JF_DISABLE_COLLISIONS if suppress else 0)
+        s = w.sphere(0.5)
+        w.add_body(s, (0, 0, 0), mass=1.0, activation=orc.DISABLE_DEACTIVATION)
+        w.add_body(s, (0.75, 0, 0), mass=0.0)
+        w.add_joint(orc.JOINT_POINT2POINT, 0, 1, orc.frame((0, 0, 0)), orc.frame((0, 0, 0)), flags=flags)
+        so = o.sphere(0.5)
+        o.add_body(so, (0, 0, 0), mass=1.0, activation=orc.DISABLE_DEACTIVATION)
+        o.add_body(so, (0.75, 0, 0), mass=0.0)
+        o.add_joint(orc.joint_desc(orc.JOINT_POINT2POINT, 0, 1, orc.frame((0, 0, 0)), orc.frame((0, 0, 0)),
+                                   flags=flags))
+        for flip in (False, True):
+            if flip:
+                flags ^= orc.JF_DISABLE_COLLISIONS
+                w.set_joint_flags(0, flags)
+                o.set_joint_flags(0, flags)
+            st = w.state()
+            st[0, 0:3] = (0.0, 0.0, 0.0)
+            st[0, 7:10] = (3.0, 0.0, 0.0)
+            w.set_state(st)
+            x = _lockstep(w, o, 90)[0, 0]
+            assert (x > 1.5) == bool(flags & orc.JF_DISABLE_COLLISIONS), (suppress, flip, x)
