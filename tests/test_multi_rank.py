@@ -63,3 +63,34 @@ def test_single_rank_needs_no_process_group():
 
     assert bench.max_over_ranks(None, 12.5) == 12.5
     assert bench.replica_throughput(131072, 60, 1, 0.3) == pytest.approx(131072 * 60 / 0.3)
+
+
+def test_clock_sampler_gpu_id(monkeypatch):
+    """The rank's nvidia-smi id: its CUDA_VISIBLE_DEVICES entry when nvidia-smi knows it,
+    else the local rank (unset variable, or nvidia-smi missing or not knowing the entry)."""
+    import subprocess
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    monkeypatch.delenv("CUDA_VISIBLE_DEVICES", raising=False)
+    assert bench.smi_gpu_id(3) == "3"
+    monkeypatch.setenv("CUDA_VISIBLE_DEVICES", "4,5,6,7")
+
+    def known(cmd, **kw):
+        return subprocess.CompletedProcess(cmd, 0, stdout="5\n", stderr="")
+
+    monkeypatch.setattr(bench.subprocess, "run", known)
+    assert bench.smi_gpu_id(1) == "5"
+
+    def unknown(cmd, **kw):
+        return subprocess.CompletedProcess(cmd, 6, stdout="", stderr="No devices were found")
+
+    monkeypatch.setattr(bench.subprocess, "run", unknown)
+    assert bench.smi_gpu_id(1) == "1"
+
+    def missing(cmd, **kw):
+        raise FileNotFoundError("nvidia-smi")
+
+    monkeypatch.setattr(bench.subprocess, "run", missing)
+    assert bench.smi_gpu_id(2) == "2"
